@@ -1,0 +1,198 @@
+/* mdrt_nb.h: C ABI of the B200 short-range nonbonded + PME term.
+ *
+ * A drop-in for the part of MDIR's device runtime that builds the groups of
+ * neighbors, runs the pair loop of Lennard-Jones + Ewald real space, and the
+ * PME spreading / FFT / gathering.  In MDIR these are emitted kernels called
+ * through the MLIR GPU runtime ABI plus `mdrt*` entries of
+ * runtime/mdrt_cuda.c; here they are one shared library with plain pointers
+ * and sizes (no CUDA or torch types in the signatures: a stream is passed as
+ * `void *`, i.e. a cudaStream_t, NULL for the default stream).
+ *
+ * Units: nm, ps, kJ/mol, e.  Device arrays are marked "device"; everything
+ * else is host memory.  Every entry returns an mdrtNbStatus; none aborts.
+ * A context is not thread-safe; all work goes to the caller's stream.
+ */
+#ifndef MDRT_NB_H
+#define MDRT_NB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDRT_NB_ABI_VERSION 1
+
+typedef struct mdrtNb mdrtNb;
+
+/* Status codes.  MDIR aborts on driver errors (runtime/mdrt_cuda.c:49-71)
+ * and stops a run through a handler (mdrt_cuda.c:2560-2577); this library
+ * returns them instead. */
+enum mdrtNbStatus {
+  MDRT_NB_OK = 0,
+  MDRT_NB_GROW = 1,             /* a buffer was too small; grown, call again */
+  MDRT_NB_NAN_POSITION = 2,     /* positions not finite or far outside the cell */
+  MDRT_NB_INVALID_BOX = 3,      /* reach >= 0.999 of the least edge, or a bad edge */
+  MDRT_NB_CUDA_ERROR = 4,
+  MDRT_NB_TIMEOUT = 5,
+  MDRT_NB_INVALID_ARGUMENT = 6,
+  MDRT_NB_UNSUPPORTED = 7,
+  MDRT_NB_OVERFLOW = 8,         /* fixed-point accumulator out of range */
+  MDRT_NB_NOT_BUILT = 9         /* a force call before the first build */
+};
+
+/* Flags of mdrtNbForce. */
+enum mdrtNbFlags {
+  MDRT_NB_ENERGY = 1u,       /* energies and virial (f64, fixed order) */
+  MDRT_NB_ACCUMULATE = 2u,   /* add into `forces` instead of overwriting */
+  MDRT_NB_POTENTIAL = 4u,    /* also gather dE_rec/dq (mdrtPmePotential) */
+  MDRT_NB_NO_PAIRS = 8u,     /* skip the pair term */
+  MDRT_NB_NO_PME = 16u,      /* skip the reciprocal sum */
+  MDRT_NB_NO_EXCLUDED = 32u  /* skip the excluded-pair correction */
+};
+
+/* Slots of the energies of mdrtNbEnergies (f64). */
+enum mdrtNbEnergySlot {
+  MDRT_NB_E_LJ = 0,
+  MDRT_NB_E_COULOMB = 1,     /* Ewald direct */
+  MDRT_NB_E_EXCLUDED = 2,    /* -f q q erf(beta r)/r over excluded pairs */
+  MDRT_NB_E_RECIPROCAL = 3,
+  MDRT_NB_W_PAIR = 4,        /* 6: xx yy zz xy xz yz of pairs + excluded */
+  MDRT_NB_W_RECIPROCAL = 10, /* 6 */
+  MDRT_NB_E_COUNT = 16
+};
+
+/* Slots of the build's sizes (MDIR's sizes[5] of
+ * mdrt_gpu_build_neighbors_groups, GroupsBuild.cpp:2517-2547, plus three). */
+enum mdrtNbSizeSlot {
+  MDRT_NB_SIZE_PLACES = 0,
+  MDRT_NB_SIZE_LONGEST = 1,
+  MDRT_NB_SIZE_UNITS = 2,   /* MDIR: blocks; here units of 64 entries */
+  MDRT_NB_SIZE_EXCL_WIDE = 3,
+  MDRT_NB_SIZE_NAN = 4,
+  MDRT_NB_SIZE_OVERFLOW = 5,
+  MDRT_NB_SIZE_GROUPS = 6,
+  MDRT_NB_SIZE_ENTRIES = 7,
+  MDRT_NB_SIZE_COUNT = 8
+};
+
+/* Buffer slots of mdrtNbGroupsBuffer, after MDIR's stable slot table
+ * (include/mdir/Runtime/GroupsABI.h:10-44). */
+enum mdrtNbGroupsSlot {
+  MDRT_NB_GROUPS_ORDER = 0,    /* int32 [places]: atom at a place, -1 empty */
+  MDRT_NB_GROUPS_COUNTS = 1,   /* int32 [groups]: entries of each list */
+  MDRT_NB_GROUPS_ENTRIES = 2,  /* int32x2 [groups * capacity]: (place, mask | image << 16) */
+  MDRT_NB_GROUPS_UNITS = 4,    /* int32x2 [units]: (group, ordinal) */
+  MDRT_NB_GROUPS_SHIFTS = 6,   /* int8x4 [places]: whole cells S of each place */
+  MDRT_NB_GROUPS_PLACED = 15,  /* float32x4 [places]: frames (x + S L, q) */
+  MDRT_NB_GROUPS_PLACE_OF = 16 /* int32 [particles]: place of each atom, -1 none */
+};
+
+/* Library and ABI version (MDRT_NB_ABI_VERSION). */
+int32_t mdrtNbVersion(void);
+/* A message for a status code (static storage). */
+const char *mdrtNbStatusString(int32_t status);
+
+/* A context for `particles` atoms on CUDA device `device`.
+ * MDIR: mdrtGroupsCreate(places, blocks), runtime/mdrt_cuda.c:3087. */
+int32_t mdrtNbCreate(mdrtNb **out, int32_t device, int64_t particles);
+int32_t mdrtNbDestroy(mdrtNb *ctx);
+
+/* Charges (e) and LJ types of each atom, and the sigma / epsilon of each
+ * type pair (ntypes x ntypes, nm and kJ/mol), all host arrays.
+ * MDIR: the fields and the folded type-pair table (D96) of the pair loop,
+ * lib/Driver/TermNonbonded.cpp:1423-1557. */
+int32_t mdrtNbSetParticles(mdrtNb *ctx, const double *charges, const int32_t *types,
+                           int32_t ntypes, const double *sigma, const double *epsilon);
+
+/* Excluded pairs as ragged rows in atom order, both directions:
+ * offsets[particles + 1], partners[offsets[particles]] (host).
+ * MDIR: the `excluded` incidence rows of the build,
+ * GroupsBuild.cpp:2517-2547 (include/mdir/Conversion/RaggedRows.h). */
+int32_t mdrtNbSetExclusions(mdrtNb *ctx, const int32_t *offsets, const int32_t *partners);
+
+/* Cutoff r_c, reach R (r_c + skin), Ewald beta (0: no Coulomb direct sum),
+ * Coulomb constant f, the direct-sum shift erfc(beta r_c)/r_c (0/1), and
+ * the LJ switch in r^2 from switch_distance (0/1).
+ * MDIR: TermNonbonded.cpp:378-470 and TermLennardJones.cpp:26-80. */
+int32_t mdrtNbSetInteraction(mdrtNb *ctx, double cutoff, double reach, double beta, double coulomb,
+                             int32_t coulomb_shift, int32_t lj_switch, double switch_distance);
+
+/* Deterministic mode: 64-bit fixed-point force accumulation (2^32 per
+ * kJ/mol/nm) and PME spreading (2^40 per e); bitwise reproducible.
+ * MDIR: deterministic = true (D70, D84; docs/pme.md, Section 3). */
+int32_t mdrtNbSetDeterministic(mdrtNb *ctx, int32_t on);
+
+/* The PME grid k1 x k2 x k3 and the spline order (4, 5, 6 or 8).
+ * MDIR: the PME plan and cuFFT plans, mdrtRetainFFTPlan, mdrt_cuda.c:2765. */
+int32_t mdrtPmeSetup(mdrtNb *ctx, int32_t k1, int32_t k2, int32_t k3, int32_t order);
+
+/* The neighbor build from device positions x (f64 [n, 3], unwrapped) in the
+ * orthorhombic cell box[3].  Grows its buffers and builds again until every
+ * list fits (count-then-grow), then writes MDRT_NB_SIZE_COUNT sizes to
+ * sizes_out (host, may be NULL).  Returns MDRT_NB_NAN_POSITION (after a
+ * complete build that leaves those atoms out) if any position is not finite.
+ * MDIR: mdrt_gpu_build_neighbors_groups(x, box, reach, excluded, order,
+ * placeOf, entries, masks, counts, units, ordinals, shifts, sizes),
+ * lib/Conversion/MDExecKernels/GroupsBuild.cpp:2515-2550, with
+ * mdrtGroupsGrow (mdrt_cuda.c:3185) and the retry loop of
+ * lib/Conversion/MDExecToGPU/MDExecToGPU.cpp:10107-10175. */
+int32_t mdrtNbBuild(mdrtNb *ctx, const double *x, int64_t n, const double box[3], double reach,
+                    void *stream, int32_t *sizes_out);
+
+/* The force term at device positions x (f64 [n, 3]): writes (or adds, with
+ * MDRT_NB_ACCUMULATE) the forces of the pairs, the excluded-pair correction
+ * and PME to `forces` (device f64 [n, 3]).  Needs a build whose lists are
+ * still valid for x.  Asynchronous on `stream`.
+ * MDIR: the emitted pair loop (TraversePairs.cpp:85), the excluded tuple
+ * loop (TermNonbonded.cpp:1615) and the reciprocal stages
+ * (MDExecToGPU/DevicePME.cpp:38-75). */
+int32_t mdrtNbForce(mdrtNb *ctx, const double *x, const double box[3], uint32_t flags,
+                    double *forces, void *stream);
+
+/* Copies the energies and virials of the last MDRT_NB_ENERGY evaluation
+ * (MDRT_NB_E_COUNT f64) to out (host); waits for `stream`.
+ * MDIR: the seven f64 numbers per sum of docs/pme.md, Section 3, and
+ * TraverseHost::finishSums (include/mdir/Conversion/TraversePairs.h:130-137). */
+int32_t mdrtNbEnergies(mdrtNb *ctx, void *stream, double *out);
+
+/* Host constants of the Ewald sum and the LJ tail in the cell box[3]:
+ * out[0] self -f beta/sqrt(pi) sum q^2, out[1] background
+ * -f pi Q^2/(2 V beta^2), out[2] dispersion correction -2 pi N^2 <C6>/(3 V rc^3)
+ * (0 unless `dispersion`), out[3] its virial per diagonal entry (2 E_disp).
+ * MDIR: TermNonbonded.cpp:601-637 and 651-668. */
+int32_t mdrtNbConstants(mdrtNb *ctx, const double box[3], int32_t dispersion, double *out);
+
+/* dE_rec/dq_i of the last evaluation made with MDRT_NB_POTENTIAL, to
+ * potential (device f64 [n]).  MDIR: the PME potential stage (D231). */
+int32_t mdrtPmePotential(mdrtNb *ctx, double *potential, void *stream);
+
+/* A device pointer to a buffer of the neighbor structure and its element
+ * count (a view; invalidated by the next build that grows).
+ * MDIR: _mlir_ciface_mdrtGroupsBuffer(result, handle, slot),
+ * runtime/mdrt_cuda.c:3109. */
+int32_t mdrtNbGroupsBuffer(mdrtNb *ctx, int32_t slot, void **pointer, int64_t *count);
+
+/* The capacity C of a list (entries a group) and the builds / growths so far.
+ * MDIR: mdrtGroupsBuilt, mdrt_cuda.c:3208. */
+int32_t mdrtNbGroupsInfo(mdrtNb *ctx, int64_t *list_capacity, int64_t *builds, int64_t *grows);
+
+/* The device status word (NB_STATUS_* bits: list overflow, fixed-point
+ * overflow, non-finite positions, stale list, timeout); waits for stream.
+ * clear != 0 resets it. */
+int32_t mdrtNbStatus(mdrtNb *ctx, void *stream, int32_t clear, int32_t *status);
+
+/* 3D real FFTs of a grid in f32 on `stream`, plans cached per size.
+ * MDIR: _mlir_ciface_mdrtCudaFFTForward3DF32 / Backward3DF32
+ * (runtime/mdrt_cuda.c:2942-2979), with plain pointers.  The backward
+ * transform is not normalized and overwrites the half-complex grid. */
+int32_t mdrtCudaFFTForward3DF32(const float *real, float *complex_out, int64_t k1, int64_t k2,
+                                int64_t k3, void *stream);
+int32_t mdrtCudaFFTBackward3DF32(float *complex_in, float *real_out, int64_t k1, int64_t k2,
+                                 int64_t k3, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MDRT_NB_H */

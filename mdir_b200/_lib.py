@@ -1,0 +1,77 @@
+"""Loads libmdrt_nb.so (include/mdrt_nb.h) with ctypes.
+
+The library is built in-tree by `python __graft_entry__.py` (build()) or
+`make -C mdir_b200/csrc`.  There is no fallback: a missing library raises."""
+
+import ctypes
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIBRARY = HERE / "libmdrt_nb.so"
+
+# Status codes, flags and slots (include/mdrt_nb.h).
+OK, GROW, NAN_POSITION, INVALID_BOX, CUDA_ERROR, TIMEOUT, INVALID_ARGUMENT, UNSUPPORTED, \
+    OVERFLOW, NOT_BUILT = range(10)
+ENERGY, ACCUMULATE, POTENTIAL, NO_PAIRS, NO_PME, NO_EXCLUDED = 1, 2, 4, 8, 16, 32
+E_LJ, E_COULOMB, E_EXCLUDED, E_RECIPROCAL, W_PAIR, W_RECIPROCAL, E_COUNT = 0, 1, 2, 3, 4, 10, 16
+SIZE_PLACES, SIZE_LONGEST, SIZE_UNITS, SIZE_EXCL_WIDE, SIZE_NAN, SIZE_OVERFLOW, SIZE_GROUPS, \
+    SIZE_ENTRIES, SIZE_COUNT = range(9)
+SLOT_ORDER, SLOT_COUNTS, SLOT_ENTRIES, SLOT_UNITS, SLOT_SHIFTS, SLOT_PLACED, SLOT_PLACE_OF = \
+    0, 1, 2, 4, 6, 15, 16
+
+_lib = None
+
+# name -> (restype, argtypes); every symbol that include/mdrt_nb.h declares
+_i32, _i64, _u32, _d, _p = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p
+SIGNATURES = {
+    "mdrtNbVersion": (_i32, []),
+    "mdrtNbStatusString": (ctypes.c_char_p, [_i32]),
+    "mdrtNbCreate": (_i32, [ctypes.POINTER(_p), _i32, _i64]),
+    "mdrtNbDestroy": (_i32, [_p]),
+    "mdrtNbSetParticles": (_i32, [_p, _p, _p, _i32, _p, _p]),
+    "mdrtNbSetExclusions": (_i32, [_p, _p, _p]),
+    "mdrtNbSetInteraction": (_i32, [_p, _d, _d, _d, _d, _i32, _i32, _d]),
+    "mdrtNbSetDeterministic": (_i32, [_p, _i32]),
+    "mdrtPmeSetup": (_i32, [_p, _i32, _i32, _i32, _i32]),
+    "mdrtNbBuild": (_i32, [_p, _p, _i64, _p, _d, _p, _p]),
+    "mdrtNbForce": (_i32, [_p, _p, _p, _u32, _p, _p]),
+    "mdrtNbEnergies": (_i32, [_p, _p, _p]),
+    "mdrtNbConstants": (_i32, [_p, _p, _i32, _p]),
+    "mdrtPmePotential": (_i32, [_p, _p, _p]),
+    "mdrtNbGroupsBuffer": (_i32, [_p, _i32, ctypes.POINTER(_p), ctypes.POINTER(_i64)]),
+    "mdrtNbGroupsInfo": (_i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "mdrtNbStatus": (_i32, [_p, _p, _i32, ctypes.POINTER(_i32)]),
+    "mdrtCudaFFTForward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
+    "mdrtCudaFFTBackward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
+}
+
+
+class NativeError(RuntimeError):
+    """A status code other than OK from the native library."""
+
+    def __init__(self, status, call):
+        self.status = status
+        msg = lib().mdrtNbStatusString(status).decode() if _lib else str(status)
+        super().__init__(f"{call}: {msg} (status {status})")
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY.exists():
+            raise ImportError(f"{LIBRARY} is missing: build it with `python __graft_entry__.py` or "
+                              "`make -C mdir_b200/csrc` (there is no CPU fallback)")
+        handle = ctypes.CDLL(str(LIBRARY))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(status, call):
+    if status != OK:
+        raise NativeError(status, call)
+    return status

@@ -1,0 +1,431 @@
+// The C ABI of include/mdrt_nb.h over the host context NbCtx.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "../../include/mdrt_nb.h"
+#include "nb_context.h"
+
+struct mdrtNb {
+  NbCtx c;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return MDRT_NB_OK;
+  fprintf(stderr, "mdrt_nb: %s: %s\n", what, cudaGetErrorString(e));
+  return MDRT_NB_CUDA_ERROR;
+}
+
+#define CK(x)                                        \
+  do {                                               \
+    int s_ = cuda_status((x), #x);                   \
+    if (s_) return s_;                               \
+  } while (0)
+
+template <typename T>
+void nb_free(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+int check_box(const NbCtx &c, const double box[3]) {
+  if (!box) return MDRT_NB_INVALID_ARGUMENT;
+  for (int k = 0; k < 3; ++k)
+    if (!(box[k] > 0.0) || !std::isfinite(box[k])) return MDRT_NB_INVALID_BOX;
+  double least = std::min(box[0], std::min(box[1], box[2]));
+  // MDIR refuses a pairlist distance above 0.999 of the least edge
+  // (docs/neighbor-groups.md, Section 5.2) and a cutoff above half of it.
+  if (c.reach >= 0.999 * least || 2.0 * c.cutoff > least) return MDRT_NB_INVALID_BOX;
+  return MDRT_NB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t mdrtNbVersion(void) { return MDRT_NB_ABI_VERSION; }
+
+const char *mdrtNbStatusString(int32_t s) {
+  switch (s) {
+    case MDRT_NB_OK: return "ok";
+    case MDRT_NB_GROW: return "a buffer was too small and has grown; call again";
+    case MDRT_NB_NAN_POSITION: return "positions that are not finite or are far outside the cell";
+    case MDRT_NB_INVALID_BOX: return "the reach is at least 0.999 of the least edge, the cutoff above half of it, or an edge is not positive";
+    case MDRT_NB_CUDA_ERROR: return "a CUDA call failed";
+    case MDRT_NB_TIMEOUT: return "a device wait ran out of time";
+    case MDRT_NB_INVALID_ARGUMENT: return "invalid argument";
+    case MDRT_NB_UNSUPPORTED: return "unsupported";
+    case MDRT_NB_OVERFLOW: return "a fixed-point accumulator went out of range";
+    case MDRT_NB_NOT_BUILT: return "no neighbor build yet";
+  }
+  return "unknown status";
+}
+
+int32_t mdrtNbCreate(mdrtNb **out, int32_t device, int64_t particles) {
+  if (!out || particles <= 0 || particles > (1ll << 26)) return MDRT_NB_INVALID_ARGUMENT;
+  *out = nullptr;
+  CK(cudaSetDevice(device));
+  mdrtNb *ctx = new mdrtNb();
+  NbCtx &c = ctx->c;
+  c.device = device;
+  c.n = particles;
+  if (cudaMalloc(&c.sizes, sizeof(int32_t) * NB_SIZE_COUNT) != cudaSuccess ||
+      cudaMallocHost(&c.h_sizes, sizeof(int32_t) * NB_SIZE_COUNT) != cudaSuccess ||
+      cudaMalloc(&c.status, sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&c.energy, sizeof(double) * NB_E_SLOTS) != cudaSuccess ||
+      cudaMallocHost(&c.h_energy, sizeof(double) * NB_E_SLOTS) != cudaSuccess) {
+    mdrtNbDestroy(ctx);
+    return MDRT_NB_CUDA_ERROR;
+  }
+  cudaMemset(c.sizes, 0, sizeof(int32_t) * NB_SIZE_COUNT);
+  cudaMemset(c.status, 0, sizeof(int32_t));
+  cudaMemset(c.energy, 0, sizeof(double) * NB_E_SLOTS);
+  // default particle table: no charge, one type of no interaction
+  std::vector<double> q(particles, 0.0);
+  std::vector<int32_t> t(particles, 0);
+  double sg = 0.3, ep = 0.0;
+  int32_t s = mdrtNbSetParticles(ctx, q.data(), t.data(), 1, &sg, &ep);
+  if (s) {
+    mdrtNbDestroy(ctx);
+    return s;
+  }
+  *out = ctx;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbDestroy(mdrtNb *ctx) {
+  if (!ctx) return MDRT_NB_OK;
+  NbCtx &c = ctx->c;
+  cudaSetDevice(c.device);
+  nb_pme_release(c);
+  nb_free(c.q); nb_free(c.type); nb_free(c.lj);
+  nb_free(c.excl_off); nb_free(c.excl); nb_free(c.excl_pairs); nb_free(c.excl_partials);
+  nb_free(c.order); nb_free(c.place_of); nb_free(c.shift); nb_free(c.xw);
+  nb_free(c.box_lo); nb_free(c.box_hi); nb_free(c.group_start); nb_free(c.group_col);
+  nb_free(c.slab); nb_free(c.counts); nb_free(c.unit_n); nb_free(c.unit_start); nb_free(c.units);
+  nb_free(c.sizes); nb_free(c.status);
+  nb_free(c.key); nb_free(c.bin_count); nb_free(c.bin_start); nb_free(c.bin_fill);
+  nb_free(c.sorted); nb_free(c.col_groups); nb_free(c.scan_scratch);
+  nb_free(c.atom_xw); nb_free(c.atom_shift);
+  nb_free(c.xq); nb_free(c.typ_p); nb_free(c.acc); nb_free(c.acc_fixed);
+  nb_free(c.unit_partials); nb_free(c.energy);
+  if (c.h_sizes) cudaFreeHost(c.h_sizes);
+  if (c.h_energy) cudaFreeHost(c.h_energy);
+  delete ctx;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbSetParticles(mdrtNb *ctx, const double *charges, const int32_t *types, int32_t ntypes,
+                           const double *sigma, const double *epsilon) {
+  if (!ctx || !charges || !types || ntypes < 1 || ntypes > 32 || !sigma || !epsilon)
+    return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  CK(cudaSetDevice(c.device));
+  for (int64_t i = 0; i < c.n; ++i)
+    if (types[i] < 0 || types[i] >= ntypes || !std::isfinite(charges[i])) return MDRT_NB_INVALID_ARGUMENT;
+  c.h_q.assign(charges, charges + c.n);
+  c.h_type.assign(types, types + c.n);
+  c.h_lj.resize((size_t)ntypes * ntypes);
+  c.h_c6.resize((size_t)ntypes * ntypes);
+  for (int a = 0; a < ntypes * ntypes; ++a) {
+    double s6 = std::pow(sigma[a], 6.0);
+    c.h_c6[a] = 4.0 * epsilon[a] * s6;
+    c.h_lj[a] = make_float2((float)(4.0 * epsilon[a] * s6), (float)(4.0 * epsilon[a] * s6 * s6));
+  }
+  std::vector<float> qf(charges, charges + c.n);
+  if (!c.q) CK(cudaMalloc(&c.q, sizeof(float) * c.n));
+  if (!c.type) CK(cudaMalloc(&c.type, sizeof(int32_t) * c.n));
+  nb_free(c.lj);
+  CK(cudaMalloc(&c.lj, sizeof(float2) * ntypes * ntypes));
+  CK(cudaMemcpy(c.q, qf.data(), sizeof(float) * c.n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c.type, types, sizeof(int32_t) * c.n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c.lj, c.h_lj.data(), sizeof(float2) * ntypes * ntypes, cudaMemcpyHostToDevice));
+  c.ntypes = ntypes;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbSetExclusions(mdrtNb *ctx, const int32_t *offsets, const int32_t *partners) {
+  if (!ctx || !offsets) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  CK(cudaSetDevice(c.device));
+  int64_t total = offsets[c.n];
+  if (offsets[0] != 0 || total < 0 || (total > 0 && !partners)) return MDRT_NB_INVALID_ARGUMENT;
+  std::vector<int32_t> pairs;
+  for (int64_t i = 0; i < c.n; ++i) {
+    if (offsets[i + 1] < offsets[i]) return MDRT_NB_INVALID_ARGUMENT;
+    for (int32_t k = offsets[i]; k < offsets[i + 1]; ++k) {
+      int32_t j = partners[k];
+      if (j < 0 || j >= c.n || j == i) return MDRT_NB_INVALID_ARGUMENT;
+      if (j > i) {
+        pairs.push_back((int32_t)i);
+        pairs.push_back(j);
+      }
+    }
+  }
+  nb_free(c.excl_off);
+  nb_free(c.excl);
+  nb_free(c.excl_pairs);
+  nb_free(c.excl_partials);
+  CK(cudaMalloc(&c.excl_off, sizeof(int32_t) * (c.n + 1)));
+  CK(cudaMemcpy(c.excl_off, offsets, sizeof(int32_t) * (c.n + 1), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&c.excl, sizeof(int32_t) * std::max<int64_t>(total, 1)));
+  if (total > 0) CK(cudaMemcpy(c.excl, partners, sizeof(int32_t) * total, cudaMemcpyHostToDevice));
+  c.n_excl_pairs = (int64_t)pairs.size() / 2;
+  CK(cudaMalloc(&c.excl_pairs, sizeof(int32_t) * std::max<size_t>(pairs.size(), 2)));
+  if (!pairs.empty())
+    CK(cudaMemcpy(c.excl_pairs, pairs.data(), sizeof(int32_t) * pairs.size(), cudaMemcpyHostToDevice));
+  int64_t blocks = std::max<int64_t>(1, (c.n_excl_pairs + 255) / 256);
+  CK(cudaMalloc(&c.excl_partials, sizeof(double) * 8 * blocks));
+  c.built = false;  // the lists depend on the exclusions
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbSetInteraction(mdrtNb *ctx, double cutoff, double reach, double beta, double coulomb,
+                             int32_t coulomb_shift, int32_t lj_switch, double switch_distance) {
+  if (!ctx || !(cutoff > 0) || !(reach >= cutoff) || !(beta >= 0) || !std::isfinite(coulomb))
+    return MDRT_NB_INVALID_ARGUMENT;
+  if (lj_switch && !(switch_distance >= 0 && switch_distance < cutoff)) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  c.cutoff = cutoff;
+  if (reach != c.reach) c.built = false;
+  c.reach = reach;
+  c.beta = beta;
+  c.coulomb = coulomb;
+  c.coulomb_shift = coulomb_shift;
+  c.lj_switch = lj_switch;
+  c.switch_distance = switch_distance;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbSetDeterministic(mdrtNb *ctx, int32_t on) {
+  if (!ctx) return MDRT_NB_INVALID_ARGUMENT;
+  ctx->c.deterministic = on != 0;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtPmeSetup(mdrtNb *ctx, int32_t k1, int32_t k2, int32_t k3, int32_t order) {
+  if (!ctx) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  CK(cudaSetDevice(c.device));
+  if (k1 == 0 && k2 == 0 && k3 == 0) {
+    nb_pme_release(c);
+    return MDRT_NB_OK;
+  }
+  if (k1 < 2 * order || k2 < 2 * order || k3 < 2 * order) return MDRT_NB_INVALID_ARGUMENT;
+  int s = nb_pme_setup(c, k1, k2, k3, order);
+  if (s == -2) return MDRT_NB_UNSUPPORTED;
+  if (s != 0) return MDRT_NB_CUDA_ERROR;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbBuild(mdrtNb *ctx, const double *x, int64_t n, const double box[3], double reach,
+                    void *stream, int32_t *sizes_out) {
+  if (!ctx || !x) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (n != c.n) return MDRT_NB_INVALID_ARGUMENT;
+  if (reach > 0 && reach != c.reach) {
+    if (reach < c.cutoff) return MDRT_NB_INVALID_ARGUMENT;
+    c.reach = reach;
+  }
+  int s = check_box(c, box);
+  if (s) return s;
+  CK(cudaSetDevice(c.device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nb_build_run(c, x, box, st)) return MDRT_NB_CUDA_ERROR;
+  if (sizes_out)
+    for (int k = 0; k < NB_SIZE_COUNT; ++k) sizes_out[k] = c.h_sizes[k];
+  if (c.h_sizes[NB_SIZE_NAN] > 0) return MDRT_NB_NAN_POSITION;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbForce(mdrtNb *ctx, const double *x, const double box[3], uint32_t flags, double *forces,
+                    void *stream) {
+  if (!ctx || !x || !forces) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (!c.built) return MDRT_NB_NOT_BUILT;
+  int s = check_box(c, box);
+  if (s) return s;
+  for (int k = 0; k < 3; ++k)
+    if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;  // a cell change needs a build
+  cudaStream_t st = (cudaStream_t)stream;
+  bool energy = flags & MDRT_NB_ENERGY;
+  bool pairs = !(flags & MDRT_NB_NO_PAIRS);
+  bool excluded = !(flags & MDRT_NB_NO_EXCLUDED);
+  bool pme = c.pme.on && !(flags & MDRT_NB_NO_PME) && c.beta > 0.0;
+  if (!(flags & MDRT_NB_ACCUMULATE)) CK(cudaMemsetAsync(forces, 0, sizeof(double) * 3 * c.n, st));
+  if (energy) CK(cudaMemsetAsync(c.energy, 0, sizeof(double) * NB_E_SLOTS, st));
+  nb_gather_frames(c, x, box, st);
+  if (pairs) nb_pairs_run(c, box, energy, st);
+  if (excluded) nb_excluded_run(c, box, energy, st);
+  if (energy && (pairs || excluded)) nb_reduce_energy(c, pairs, excluded, st);
+  if (pme) {
+    if (nb_pme_run(c, box, energy, (flags & MDRT_NB_POTENTIAL) != 0, st)) return MDRT_NB_CUDA_ERROR;
+  }
+  bool keep_pme = c.pme.on;
+  if (!pme) c.pme.on = false;  // finish without the PME forces of a skipped sum
+  nb_finish_forces(c, forces, 1, st);
+  c.pme.on = keep_pme;
+  CK(cudaGetLastError());
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbEnergies(mdrtNb *ctx, void *stream, double *out) {
+  if (!ctx || !out) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(c.h_energy, c.energy, sizeof(double) * NB_E_SLOTS, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int k = 0; k < NB_E_SLOTS; ++k) out[k] = c.h_energy[k];
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbConstants(mdrtNb *ctx, const double box[3], int32_t dispersion, double *out) {
+  if (!ctx || !box || !out) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  double sq = 0.0, net = 0.0;
+  for (double v : c.h_q) {
+    sq += v * v;
+    net += v;
+  }
+  double V = box[0] * box[1] * box[2];
+  out[0] = c.beta > 0 ? -c.coulomb * c.beta / std::sqrt(M_PI) * sq : 0.0;
+  out[1] = c.beta > 0 ? -c.coulomb * M_PI * net * net / (2.0 * V * c.beta * c.beta) : 0.0;
+  out[2] = out[3] = 0.0;
+  if (dispersion) {
+    int nt = c.ntypes;
+    std::vector<double> cnt(nt, 0.0);
+    for (int32_t t : c.h_type) cnt[t] += 1.0;
+    double sum = 0.0;
+    for (int a = 0; a < nt; ++a)
+      for (int b = 0; b < nt; ++b) sum += cnt[a] * (cnt[b] - (a == b ? 1.0 : 0.0)) * c.h_c6[a * nt + b];
+    // excluded pairs: read back the rows from the device copy
+    int64_t npairs = c.n_excl_pairs;
+    if (npairs > 0) {
+      std::vector<int32_t> pairs(2 * npairs);
+      cudaMemcpy(pairs.data(), c.excl_pairs, sizeof(int32_t) * 2 * npairs, cudaMemcpyDeviceToHost);
+      for (int64_t k = 0; k < npairs; ++k)
+        sum -= 2.0 * c.h_c6[c.h_type[pairs[2 * k]] * nt + c.h_type[pairs[2 * k + 1]]];
+    }
+    double n = (double)c.n;
+    double npair = n * (n - 1.0) - 2.0 * npairs;
+    double mean = npair > 0 ? sum / npair : 0.0;
+    double rc = c.cutoff;
+    out[2] = -2.0 * M_PI / (3.0 * V) * n * n * mean / (rc * rc * rc);
+    out[3] = 2.0 * out[2];
+  }
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbGroupsBuffer(mdrtNb *ctx, int32_t slot, void **pointer, int64_t *count) {
+  if (!ctx || !pointer) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  void *p = nullptr;
+  int64_t k = 0;
+  switch (slot) {
+    case MDRT_NB_GROUPS_ORDER: p = c.order; k = c.places_cap; break;
+    case MDRT_NB_GROUPS_COUNTS: p = c.counts; k = c.groups_cap; break;
+    case MDRT_NB_GROUPS_ENTRIES: p = c.slab; k = c.groups_cap * c.list_cap; break;
+    case MDRT_NB_GROUPS_UNITS: p = c.units; k = c.units_cap; break;
+    case MDRT_NB_GROUPS_SHIFTS: p = c.shift; k = c.places_cap; break;
+    case MDRT_NB_GROUPS_PLACED: p = c.xq; k = c.places_cap; break;
+    case MDRT_NB_GROUPS_PLACE_OF: p = c.place_of; k = c.n; break;
+    default: return MDRT_NB_INVALID_ARGUMENT;
+  }
+  *pointer = p;
+  if (count) *count = k;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbGroupsInfo(mdrtNb *ctx, int64_t *list_capacity, int64_t *builds, int64_t *grows) {
+  if (!ctx) return MDRT_NB_INVALID_ARGUMENT;
+  if (list_capacity) *list_capacity = ctx->c.list_cap;
+  if (builds) *builds = ctx->c.builds;
+  if (grows) *grows = ctx->c.grows;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbStatus(mdrtNb *ctx, void *stream, int32_t clear, int32_t *status) {
+  if (!ctx || !status) return MDRT_NB_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  int32_t v = 0;
+  CK(cudaMemcpyAsync(&v, ctx->c.status, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (clear) CK(cudaMemsetAsync(ctx->c.status, 0, sizeof(int32_t), st));
+  *status = v;
+  return MDRT_NB_OK;
+}
+
+}  // extern "C"
+
+// --------------------------------------------------------------------------
+// FFT entries with cached plans
+// --------------------------------------------------------------------------
+namespace {
+std::mutex g_fft_mutex;
+std::map<std::tuple<int, int64_t, int64_t, int64_t, int>, cufftHandle> g_fft_plans;
+
+cufftHandle fft_plan(int64_t k1, int64_t k2, int64_t k3, bool forward) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_fft_mutex);
+  auto key = std::make_tuple(dev, k1, k2, k3, forward ? 1 : 0);
+  auto it = g_fft_plans.find(key);
+  if (it != g_fft_plans.end()) return it->second;
+  cufftHandle h = 0;
+  if (cufftPlan3d(&h, (int)k1, (int)k2, (int)k3, forward ? CUFFT_R2C : CUFFT_C2R) != CUFFT_SUCCESS) return 0;
+  g_fft_plans[key] = h;
+  return h;
+}
+}  // namespace
+
+extern "C" int32_t mdrtCudaFFTForward3DF32(const float *real, float *complex_out, int64_t k1, int64_t k2,
+                                           int64_t k3, void *stream) {
+  if (!real || !complex_out || k1 < 1 || k2 < 1 || k3 < 1) return MDRT_NB_INVALID_ARGUMENT;
+  cufftHandle h = fft_plan(k1, k2, k3, true);
+  if (!h) return MDRT_NB_CUDA_ERROR;
+  cufftSetStream(h, (cudaStream_t)stream);
+  if (cufftExecR2C(h, (cufftReal *)real, (cufftComplex *)complex_out) != CUFFT_SUCCESS)
+    return MDRT_NB_CUDA_ERROR;
+  return MDRT_NB_OK;
+}
+
+extern "C" int32_t mdrtCudaFFTBackward3DF32(float *complex_in, float *real_out, int64_t k1, int64_t k2,
+                                            int64_t k3, void *stream) {
+  if (!real_out || !complex_in || k1 < 1 || k2 < 1 || k3 < 1) return MDRT_NB_INVALID_ARGUMENT;
+  cufftHandle h = fft_plan(k1, k2, k3, false);
+  if (!h) return MDRT_NB_CUDA_ERROR;
+  cufftSetStream(h, (cudaStream_t)stream);
+  if (cufftExecC2R(h, (cufftComplex *)complex_in, (cufftReal *)real_out) != CUFFT_SUCCESS)
+    return MDRT_NB_CUDA_ERROR;
+  return MDRT_NB_OK;
+}
+
+// The PME potential gathered per place, scattered to atoms in f64.
+namespace {
+__global__ void nb_potential_out(int64_t places, const int32_t *__restrict__ sizes,
+                                 const int32_t *__restrict__ order, const float *__restrict__ pot,
+                                 double *__restrict__ out) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  int a = order[p];
+  if (a >= 0) out[a] = pot[p];
+}
+}  // namespace
+
+extern "C" int32_t mdrtPmePotential(mdrtNb *ctx, double *potential, void *stream) {
+  if (!ctx || !potential) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (!c.pme.on || !c.built) return MDRT_NB_NOT_BUILT;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(potential, 0, sizeof(double) * c.n, st));
+  int blocks = (int)std::max<int64_t>(1, (c.places_cap + 255) / 256);
+  nb_potential_out<<<blocks, 256, 0, st>>>(c.places_cap, c.sizes, c.order, c.pme.potential, potential);
+  CK(cudaGetLastError());
+  return MDRT_NB_OK;
+}

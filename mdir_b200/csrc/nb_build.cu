@@ -1,0 +1,608 @@
+// The cluster-pair neighbor build on sm_100a.
+//
+// Replaces MDIR's emitted groups build (lib/Conversion/MDExecKernels/
+// GroupsBuild.cpp: emitKeys 520, sortByKey 429, emitChunks 741, emitBoxes
+// 912, emitLists 1098) behind the same contract (docs/neighbor-groups.md,
+// Sections 1.1-1.3 and 4-5.2): every image of every non-excluded pair whose
+// f32 distance is within the widened reach R' = R + 3e-6 (Lx+Ly+Lz) has
+// exactly one bit, in the list of the group of the earlier place.
+//
+// The B200 design differs from the reference's: the cell sort is a counting
+// sort into columns of about 16 atoms per column-width of height (so a
+// group of 16 consecutive places of a column is close to a cube, with no
+// sorting network); the search screens whole candidate groups against the
+// group's bounding box, 32 candidates a ballot, then tests the 16 x 16
+// pairs of two candidate groups per warp pass with the f32 test; the
+// exclusion partners of the 16 members are sorted in shared memory and
+// looked up by binary search; and the list of a group is a fixed slab of C
+// entries (grown by the host when a build reports a longer list), so that
+// the units of work come out in group order and every result is
+// deterministic.
+//
+// Kernels (in launch order): nb_keys, scan, nb_scatter, nb_bin_sort,
+// nb_col_groups, scan, nb_group_cols, nb_places, nb_boxes, nb_search,
+// nb_unit_count, scan, nb_unit_write.
+#include <cmath>
+#include <cstdio>
+
+#include "nb_context.h"
+#include "nb_scan.cuh"
+
+#define NB_EXCL_MAX 256
+
+namespace {
+
+__global__ void nb_keys(int64_t n, const double *__restrict__ x, double Lx, double Ly, double Lz,
+                        int Nx, int Ny, int Nz, float inv_wx, float inv_wy, float inv_hz,
+                        int32_t *__restrict__ key, int32_t *__restrict__ bin_count,
+                        float4 *__restrict__ atom_xw, char4 *__restrict__ atom_shift,
+                        int32_t *__restrict__ sizes) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v0 = x[3 * i], v1 = x[3 * i + 1], v2 = x[3 * i + 2];
+  bool ok = isfinite(v0) && isfinite(v1) && isfinite(v2);
+  double S0 = 0, S1 = 0, S2 = 0;
+  if (ok) {
+    S0 = -floor(v0 / Lx);
+    S1 = -floor(v1 / Ly);
+    S2 = -floor(v2 / Lz);
+    ok = fabs(S0) <= 100.0 && fabs(S1) <= 100.0 && fabs(S2) <= 100.0;
+  }
+  if (!ok) {
+    key[i] = Nx * Ny * Nz;  // the bin of the positions that have no key
+    atomicAdd(&bin_count[Nx * Ny * Nz], 1);
+    atomicAdd(&sizes[NB_SIZE_NAN], 1);
+    atom_xw[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    atom_shift[i] = make_char4(0, 0, 0, 0);
+    return;
+  }
+  float w0 = (float)(v0 + S0 * Lx), w1 = (float)(v1 + S1 * Ly), w2 = (float)(v2 + S2 * Lz);
+  int kx = min(max((int)(w0 * inv_wx), 0), Nx - 1);
+  int ky = min(max((int)(w1 * inv_wy), 0), Ny - 1);
+  int kz = min(max((int)(w2 * inv_hz), 0), Nz - 1);
+  int k = (ky * Nx + kx) * Nz + kz;
+  key[i] = k;
+  atomicAdd(&bin_count[k], 1);
+  atom_xw[i] = make_float4(w0, w1, w2, 1.f);
+  atom_shift[i] = make_char4((signed char)S0, (signed char)S1, (signed char)S2, 0);
+}
+
+__global__ void nb_scatter(int64_t n, const int32_t *__restrict__ key,
+                           const int32_t *__restrict__ bin_start, int32_t *__restrict__ bin_fill,
+                           int32_t *__restrict__ sorted) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int k = key[i];
+  int at = bin_start[k] + atomicAdd(&bin_fill[k], 1);
+  sorted[at] = (int32_t)i;
+}
+
+// Each bin's atoms by number, so that the order does not depend on the
+// threads (bins hold about half an atom on average).
+__global__ void nb_bin_sort(int nbins, const int32_t *__restrict__ bin_start,
+                            int32_t *__restrict__ sorted) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbins) return;
+  int s = bin_start[b], e = bin_start[b + 1];
+  for (int i = s + 1; i < e; ++i) {
+    int v = sorted[i];
+    int j = i - 1;
+    while (j >= s && sorted[j] > v) {
+      sorted[j + 1] = sorted[j];
+      --j;
+    }
+    sorted[j + 1] = v;
+  }
+}
+
+__global__ void nb_col_groups(int ncol, int Nz, const int32_t *__restrict__ bin_start,
+                              int32_t *__restrict__ col_groups) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  int nc = bin_start[(c + 1) * Nz] - bin_start[c * Nz];
+  col_groups[c] = (nc + NB_GROUP - 1) / NB_GROUP;
+}
+
+__global__ void nb_group_cols(int ncol, const int32_t *__restrict__ group_start, int64_t groups_cap,
+                              int32_t *__restrict__ group_col, int32_t *__restrict__ sizes) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c == 0) {
+    int g = group_start[ncol];
+    sizes[NB_SIZE_GROUPS] = g;
+    sizes[NB_SIZE_PLACES] = g * NB_GROUP;
+    if (g > groups_cap) atomicOr(&sizes[NB_SIZE_OVERFLOW], 1);
+  }
+  if (c >= ncol) return;
+  for (int g = group_start[c]; g < group_start[c + 1] && g < groups_cap; ++g) group_col[g] = c;
+}
+
+__global__ void nb_places(int nsorted_max, const int32_t *__restrict__ bin_start, int nvalid_bins,
+                          const int32_t *__restrict__ sorted, const int32_t *__restrict__ key, int Nz,
+                          const int32_t *__restrict__ group_start, int64_t places_cap,
+                          const float4 *__restrict__ atom_xw, const char4 *__restrict__ atom_shift,
+                          int32_t *__restrict__ order, int32_t *__restrict__ place_of,
+                          char4 *__restrict__ shift, float4 *__restrict__ xw) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsorted_max) return;
+  int nvalid = bin_start[nvalid_bins];
+  int a = sorted[s];
+  if (s >= nvalid) {  // positions with no key are in no group
+    place_of[a] = -1;
+    return;
+  }
+  int c = key[a] / Nz;
+  int rank = s - bin_start[c * Nz];
+  int64_t p = (int64_t)group_start[c] * NB_GROUP + rank;
+  if (p >= places_cap) {
+    place_of[a] = -1;
+    return;
+  }
+  order[p] = a;
+  place_of[a] = (int32_t)p;
+  shift[p] = atom_shift[a];
+  xw[p] = atom_xw[a];
+}
+
+__global__ void nb_boxes(int64_t groups_cap, const int32_t *__restrict__ sizes,
+                         const int32_t *__restrict__ order, const float4 *__restrict__ xw,
+                         float4 *__restrict__ box_lo, float4 *__restrict__ box_hi) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
+  float lo0 = INFINITY, lo1 = INFINITY, lo2 = INFINITY;
+  float hi0 = -INFINITY, hi1 = -INFINITY, hi2 = -INFINITY;
+  for (int u = 0; u < NB_GROUP; ++u) {
+    int64_t p = g * NB_GROUP + u;
+    if (order[p] < 0) continue;
+    float4 v = xw[p];
+    lo0 = fminf(lo0, v.x);
+    lo1 = fminf(lo1, v.y);
+    lo2 = fminf(lo2, v.z);
+    hi0 = fmaxf(hi0, v.x);
+    hi1 = fmaxf(hi1, v.y);
+    hi2 = fmaxf(hi2, v.z);
+  }
+  box_lo[g] = make_float4(lo0, lo1, lo2, 0.f);
+  box_hi[g] = make_float4(hi0, hi1, hi2, 0.f);
+}
+
+// The f32 distance of the pair test, the same for both orders of the pair:
+// d = (x_B + s L) - x_A with A the atom of the smaller number and s the
+// image of B relative to A; products and sums rounded one at a time.
+__device__ __forceinline__ float nb_pair_r2(float4 xa, float4 xb, float sx, float sy, float sz) {
+  float dx = __fsub_rn(__fadd_rn(xb.x, sx), xa.x);
+  float dy = __fsub_rn(__fadd_rn(xb.y, sy), xa.y);
+  float dz = __fsub_rn(__fadd_rn(xb.z, sz), xa.z);
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+struct SearchParams {
+  float Lx, Ly, Lz;
+  float wx, wy;
+  int Nx, Ny;
+  float R2f;     // (float)(R'^2)
+  float Rbox;    // R' plus a margin, for the conservative box and window tests
+  int64_t groups_cap;
+  int64_t list_cap;
+};
+
+// A warp builds the list of one group.  Lanes 0-15 and 16-31 hold the
+// members; a pass tests two candidate groups, one per half-warp, each lane
+// one candidate place against the 16 members.
+__global__ void __launch_bounds__(128) nb_search(SearchParams P, const int32_t *sizes_in,
+                                                 const int32_t *__restrict__ order,
+                                                 const float4 *__restrict__ xw,
+                                                 const float4 *__restrict__ box_lo,
+                                                 const float4 *__restrict__ box_hi,
+                                                 const int32_t *__restrict__ group_start,
+                                                 const int32_t *__restrict__ excl_off,
+                                                 const int32_t *__restrict__ excl,
+                                                 int2 *__restrict__ slab, int32_t *__restrict__ counts,
+                                                 int32_t *sizes) {
+  __shared__ float4 s_mem[4][NB_GROUP];
+  __shared__ int s_atom[4][NB_GROUP];
+  __shared__ int s_key[4][NB_EXCL_MAX];
+  __shared__ unsigned char s_ku[4][NB_EXCL_MAX];
+  const unsigned FULL = 0xffffffffu;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int u = lane & 15, half = lane >> 4;
+  int64_t g = (int64_t)blockIdx.x * 4 + warp;
+  int ngroups = sizes_in[NB_SIZE_GROUPS];
+  if (g >= ngroups || g >= P.groups_cap) return;
+
+  // members
+  int64_t pi = g * NB_GROUP + u;
+  int ai = order[pi];
+  float4 xi = xw[pi];
+  if (half == 0) {
+    xi.w = ai >= 0 ? 1.f : 0.f;
+    s_mem[warp][u] = xi;
+    s_atom[warp][u] = ai;
+  }
+  // exclusion partners of the members: keys (partner atom, member), sorted
+  int rs = 0, re = 0;
+  if (excl_off && half == 0 && ai >= 0) {
+    rs = excl_off[ai];
+    re = excl_off[ai + 1];
+  }
+  int cnt = re - rs;
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  int nkeys = __shfl_sync(FULL, incl, 31);
+  bool wide = nkeys > NB_EXCL_MAX;
+  if (!wide) {
+    int at = incl - cnt;
+    for (int k = 0; k < cnt; ++k) {
+      s_key[warp][at + k] = excl[rs + k];
+      s_ku[warp][at + k] = (unsigned char)u;
+    }
+  } else if (lane == 0) {
+    atomicAdd(&sizes[NB_SIZE_EXCL_WIDE], 1);
+  }
+  __syncwarp();
+  int kmin = INT_MAX, kmax = INT_MIN;
+  if (!wide && nkeys > 0) {
+    // rank sort of the keys by (partner, member, position)
+    int myk[NB_EXCL_MAX / 32];
+    unsigned char myu[NB_EXCL_MAX / 32];
+    int myr[NB_EXCL_MAX / 32];
+    int mine = 0;
+    for (int k = lane; k < nkeys; k += 32, ++mine) {
+      int kv = s_key[warp][k];
+      unsigned char ku = s_ku[warp][k];
+      int r = 0;
+      for (int t = 0; t < nkeys; ++t) {
+        int tv = s_key[warp][t];
+        r += (tv < kv) || (tv == kv && t < k);
+      }
+      myk[mine] = kv;
+      myu[mine] = ku;
+      myr[mine] = r;
+      kmin = min(kmin, kv);
+      kmax = max(kmax, kv);
+    }
+    __syncwarp();
+    for (int m = 0; m < mine; ++m) {
+      s_key[warp][myr[m]] = myk[m];
+      s_ku[warp][myr[m]] = myu[m];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      kmin = min(kmin, __shfl_xor_sync(FULL, kmin, o));
+      kmax = max(kmax, __shfl_xor_sync(FULL, kmax, o));
+    }
+  }
+  __syncwarp();
+
+  float4 lo = box_lo[g], hi = box_hi[g];
+  float ci0 = 0.5f * (lo.x + hi.x), ci1 = 0.5f * (lo.y + hi.y), ci2 = 0.5f * (lo.z + hi.z);
+  float wi0 = 0.5f * (hi.x - lo.x), wi1 = 0.5f * (hi.y - lo.y), wi2 = 0.5f * (hi.z - lo.z);
+  int kx0 = (int)floorf((lo.x - P.Rbox) / P.wx), kx1 = (int)floorf((hi.x + P.Rbox) / P.wx);
+  int ky0 = (int)floorf((lo.y - P.Rbox) / P.wy), ky1 = (int)floorf((hi.y + P.Rbox) / P.wy);
+  int sz0 = (lo.z - P.Rbox < 0.f) ? -1 : 0;
+  int sz1 = (hi.z + P.Rbox >= P.Lz) ? 1 : 0;
+  float Rb2 = P.Rbox * P.Rbox;
+  int count = 0;
+
+  for (int ky = ky0; ky <= ky1; ++ky) {
+    int cy = ((ky % P.Ny) + P.Ny) % P.Ny;
+    int sy = (ky - cy) / P.Ny;
+    for (int kx = kx0; kx <= kx1; ++kx) {
+      int cx = ((kx % P.Nx) + P.Nx) % P.Nx;
+      int sx = (kx - cx) / P.Nx;
+      int c = cy * P.Nx + cx;
+      int hb = max(group_start[c], (int)g), he = group_start[c + 1];
+      if (hb >= he) continue;
+      for (int sz = sz0; sz <= sz1; ++sz) {
+        float fsx = (float)sx * P.Lx, fsy = (float)sy * P.Ly, fsz = (float)sz * P.Lz;
+        int code = nb_image_code(sx, sy, sz);
+        for (int base = hb; base < he; base += 32) {
+          int hc = base + lane;
+          bool pass = false;
+          if (hc < he) {
+            float4 l2 = box_lo[hc], h2 = box_hi[hc];
+            float d0 = fabsf(0.5f * (l2.x + h2.x) + fsx - ci0) - (wi0 + 0.5f * (h2.x - l2.x));
+            float d1 = fabsf(0.5f * (l2.y + h2.y) + fsy - ci1) - (wi1 + 0.5f * (h2.y - l2.y));
+            float d2 = fabsf(0.5f * (l2.z + h2.z) + fsz - ci2) - (wi2 + 0.5f * (h2.z - l2.z));
+            d0 = fmaxf(d0, 0.f);
+            d1 = fmaxf(d1, 0.f);
+            d2 = fmaxf(d2, 0.f);
+            pass = d0 * d0 + d1 * d1 + d2 * d2 <= Rb2;
+          }
+          unsigned bits = __ballot_sync(FULL, pass);
+          while (bits) {
+            int c0 = __ffs(bits) - 1;
+            bits &= bits - 1;
+            int c1 = -1;
+            if (bits) {
+              c1 = __ffs(bits) - 1;
+              bits &= bits - 1;
+            }
+            int cand = half ? c1 : c0;
+            unsigned mask = 0;
+            int64_t pj = 0;
+            if (cand >= 0) {
+              int64_t h = base + cand;
+              pj = h * NB_GROUP + u;
+              int aj = order[pj];
+              if (aj >= 0) {
+                float4 xj = xw[pj];
+                bool same = (h == g);
+#pragma unroll 4
+                for (int m = 0; m < NB_GROUP; ++m) {
+                  float4 xm = s_mem[warp][m];
+                  int am = s_atom[warp][m];
+                  // canonical orientation: A = smaller atom number
+                  bool jfirst = aj < am;
+                  float4 xa = jfirst ? xj : xm;
+                  float4 xb = jfirst ? xm : xj;
+                  float sgn = jfirst ? -1.f : 1.f;
+                  float r2 = nb_pair_r2(xa, xb, sgn * fsx, sgn * fsy, sgn * fsz);
+                  bool ok = (xm.w != 0.f) && (r2 <= P.R2f) && (!same || m < u);
+                  mask |= ok ? (1u << m) : 0u;
+                }
+                if (mask) {
+                  if (!wide) {
+                    if (nkeys > 0 && aj >= kmin && aj <= kmax) {
+                      int lo_i = 0, hi_i = nkeys;
+                      while (lo_i < hi_i) {
+                        int mid = (lo_i + hi_i) >> 1;
+                        if (s_key[warp][mid] < aj) lo_i = mid + 1; else hi_i = mid;
+                      }
+                      for (int k = lo_i; k < nkeys && s_key[warp][k] == aj; ++k)
+                        mask &= ~(1u << s_ku[warp][k]);
+                    }
+                  } else {
+                    unsigned mm = mask;
+                    while (mm) {
+                      int m = __ffs(mm) - 1;
+                      mm &= mm - 1;
+                      int am = s_atom[warp][m];
+                      for (int k = excl_off[am]; k < excl_off[am + 1]; ++k)
+                        if (excl[k] == aj) mask &= ~(1u << m);
+                    }
+                  }
+                }
+              }
+            }
+            unsigned has = __ballot_sync(FULL, mask != 0);
+            if (mask) {
+              int rank = __popc(has & ((1u << lane) - 1));
+              int at = count + rank;
+              if (at < P.list_cap)
+                slab[g * P.list_cap + at] = make_int2((int)pj, (int)(mask | ((unsigned)code << 16)));
+            }
+            count += __popc(has);
+          }
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    counts[g] = count;
+    atomicMax(&sizes[NB_SIZE_LONGEST], count);
+    if (count > P.list_cap) atomicOr(&sizes[NB_SIZE_OVERFLOW], 2);
+  }
+}
+
+__global__ void nb_unit_count(int64_t groups_cap, const int32_t *__restrict__ sizes,
+                              const int32_t *__restrict__ counts, int64_t list_cap,
+                              int32_t *__restrict__ unit_n) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= groups_cap) return;
+  int c = 0;
+  if (g < sizes[NB_SIZE_GROUPS]) c = (int)min((int64_t)counts[g], list_cap);
+  unit_n[g] = (c + NB_UNIT - 1) / NB_UNIT;
+}
+
+__global__ void nb_unit_write(int64_t groups_cap, const int32_t *__restrict__ unit_n,
+                              const int32_t *__restrict__ unit_start, int64_t units_cap,
+                              int2 *__restrict__ units, int32_t *__restrict__ sizes) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g == 0) {
+    int total = unit_start[groups_cap];
+    sizes[NB_SIZE_UNITS] = total;
+    if (total > units_cap) atomicOr(&sizes[NB_SIZE_OVERFLOW], 4);
+  }
+  if (g >= groups_cap) return;
+  int s = unit_start[g];
+  for (int k = 0; k < unit_n[g]; ++k)
+    if (s + k < units_cap) units[s + k] = make_int2((int)g, k);
+}
+
+__global__ void nb_count_entries(int64_t groups_cap, const int32_t *sizes,
+                                 const int32_t *__restrict__ counts, int32_t *out) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
+  atomicAdd(&out[NB_SIZE_ENTRIES], counts[g]);
+}
+
+inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
+
+}  // namespace
+
+// Grid of the counting sort: columns of about 16 atoms per column-width of
+// height, z bins of about half an atom.
+static NbGrid nb_plan_grid(int64_t n, const double box[3]) {
+  NbGrid G;
+  double V = box[0] * box[1] * box[2];
+  double rho = (n > 0 ? (double)n : 1.0) / V;
+  double dcol = cbrt((double)NB_GROUP / rho);
+  G.Nx = (int)std::min(256.0, std::max(1.0, std::floor(box[0] / dcol)));
+  G.Ny = (int)std::min(256.0, std::max(1.0, std::floor(box[1] / dcol)));
+  int64_t nz = 2 * n / (G.Nx * G.Ny);
+  G.Nz = (int)std::max<int64_t>(1, std::min<int64_t>(nz, 1 << 20));
+  G.wx = (float)(box[0] / G.Nx);
+  G.wy = (float)(box[1] / G.Ny);
+  G.hz = (float)(box[2] / G.Nz);
+  return G;
+}
+
+#define NB_CHECK(x)                                                  \
+  do {                                                               \
+    cudaError_t e_ = (x);                                            \
+    if (e_ != cudaSuccess) {                                         \
+      fprintf(stderr, "mdrt_nb: %s: %s\n", #x, cudaGetErrorString(e_)); \
+      return -1;                                                     \
+    }                                                                \
+  } while (0)
+
+template <typename T>
+static int nb_realloc(T *&p, int64_t count) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  if (count <= 0) count = 1;
+  cudaError_t e = cudaMalloc((void **)&p, sizeof(T) * (size_t)count);
+  return e == cudaSuccess ? 0 : -1;
+}
+
+// Sizes the buffers for n atoms, the grid and the list capacity C.
+static int nb_reserve(NbCtx &c, const NbGrid &G, int64_t list_cap) {
+  int64_t n = c.n;
+  int64_t cols = G.ncol();
+  int64_t groups = (n + NB_GROUP - 1) / NB_GROUP + cols;  // at most one partial group a column
+  int64_t bins = G.nbins() + 1;
+  if (bins > c.bins_cap) {
+    int64_t cap = bins + bins / 4;
+    if (nb_realloc(c.bin_count, cap) || nb_realloc(c.bin_start, cap + 1) || nb_realloc(c.bin_fill, cap))
+      return -1;
+    int64_t scr = cap / NB_SCAN_TILE + 8;
+    int64_t scr2 = (groups + groups / 4) / NB_SCAN_TILE + 8;
+    if (nb_realloc(c.scan_scratch, std::max(scr, std::max<int64_t>(scr2, 64)) + 4096)) return -1;
+    c.bins_cap = cap;
+  }
+  if (cols + 1 > c.cols_cap) {
+    int64_t cap = cols + cols / 4 + 1;
+    if (nb_realloc(c.col_groups, cap) || nb_realloc(c.group_start, cap + 1)) return -1;
+    c.cols_cap = cap;
+  }
+  bool regroup = groups > c.groups_cap;
+  if (regroup) {
+    int64_t cap = groups + groups / 4 + 16;
+    if (nb_realloc(c.order, cap * NB_GROUP) || nb_realloc(c.shift, cap * NB_GROUP) ||
+        nb_realloc(c.xw, cap * NB_GROUP) || nb_realloc(c.box_lo, cap) || nb_realloc(c.box_hi, cap) ||
+        nb_realloc(c.group_col, cap) || nb_realloc(c.counts, cap) || nb_realloc(c.unit_n, cap) ||
+        nb_realloc(c.unit_start, cap + 1) || nb_realloc(c.xq, cap * NB_GROUP) ||
+        nb_realloc(c.typ_p, cap * NB_GROUP) || nb_realloc(c.acc, cap * NB_GROUP) ||
+        nb_realloc(c.acc_fixed, cap * NB_GROUP * 3))
+      return -1;
+    if (c.pme.on) {
+      if (nb_realloc(c.pme.pme_force, cap * NB_GROUP * 4) || nb_realloc(c.pme.potential, cap * NB_GROUP))
+        return -1;
+    }
+    NB_CHECK(cudaMemset(c.acc, 0, sizeof(float4) * cap * NB_GROUP));
+    NB_CHECK(cudaMemset(c.acc_fixed, 0, sizeof(unsigned long long) * cap * NB_GROUP * 3));
+    c.groups_cap = cap;
+    c.places_cap = cap * NB_GROUP;
+  }
+  if (regroup || list_cap != c.list_cap) {
+    if (nb_realloc(c.slab, c.groups_cap * list_cap)) return -1;
+    c.list_cap = list_cap;
+    int64_t units = c.groups_cap * ((list_cap + NB_UNIT - 1) / NB_UNIT);
+    if (units > c.units_cap) {
+      if (nb_realloc(c.units, units) || nb_realloc(c.unit_partials, units * 8)) return -1;
+      c.units_cap = units;
+    }
+  }
+  return 0;
+}
+
+static int64_t nb_initial_list_cap(int64_t n, const double box[3], double reach, const NbGrid &G) {
+  double V = box[0] * box[1] * box[2];
+  double rho = n / V;
+  double R = reach + 3e-6 * (box[0] + box[1] + box[2]);
+  double hz = NB_GROUP / (rho * G.wx * G.wy);
+  double w0 = 0.5 * G.wx, w1 = 0.5 * G.wy, w2 = 0.5 * hz;
+  double VR = 8 * w0 * w1 * w2 + 8 * (w0 * w1 + w1 * w2 + w2 * w0) * R +
+              2 * M_PI * (w0 + w1 + w2) * R * R + 4.0 / 3.0 * M_PI * R * R * R;
+  double est = 0.5 * rho * VR * 1.6 + 64;
+  est = std::min(est, (double)n * 27.0 + 64);
+  return ((int64_t)est + NB_UNIT - 1) / NB_UNIT * NB_UNIT;
+}
+
+// Launches one build on `s`. Returns 0; the sizes are left in c.sizes (device).
+static void nb_build_launch(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
+  const NbGrid &G = c.grid;
+  int64_t n = c.n;
+  int nbins = G.nbins();
+  cudaMemsetAsync(c.sizes, 0, sizeof(int32_t) * NB_SIZE_COUNT, s);
+  cudaMemsetAsync(c.bin_count, 0, sizeof(int32_t) * (nbins + 1), s);
+  cudaMemsetAsync(c.bin_fill, 0, sizeof(int32_t) * (nbins + 1), s);
+  cudaMemsetAsync(c.order, 0xff, sizeof(int32_t) * c.places_cap, s);
+  nb_keys<<<blocks_for(n, 256), 256, 0, s>>>(n, x, box[0], box[1], box[2], G.Nx, G.Ny, G.Nz,
+                                            1.0f / G.wx, 1.0f / G.wy, 1.0f / G.hz, c.key,
+                                            c.bin_count, c.atom_xw, c.atom_shift, c.sizes);
+  nb_scan(c.bin_count, c.bin_start, nbins + 1, nullptr, c.scan_scratch, s);
+  nb_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, c.key, c.bin_start, c.bin_fill, c.sorted);
+  nb_bin_sort<<<blocks_for(nbins + 1, 256), 256, 0, s>>>(nbins + 1, c.bin_start, c.sorted);
+  nb_col_groups<<<blocks_for(G.ncol(), 256), 256, 0, s>>>(G.ncol(), G.Nz, c.bin_start, c.col_groups);
+  nb_scan(c.col_groups, c.group_start, G.ncol(), nullptr, c.scan_scratch, s);
+  nb_group_cols<<<blocks_for(G.ncol(), 256), 256, 0, s>>>(G.ncol(), c.group_start, c.groups_cap,
+                                                         c.group_col, c.sizes);
+  nb_places<<<blocks_for(n, 256), 256, 0, s>>>((int)n, c.bin_start, nbins, c.sorted, c.key, G.Nz,
+                                              c.group_start, c.places_cap, c.atom_xw, c.atom_shift,
+                                              c.order, c.place_of, c.shift, c.xw);
+  nb_boxes<<<blocks_for(c.groups_cap, 128), 128, 0, s>>>(c.groups_cap, c.sizes, c.order, c.xw,
+                                                        c.box_lo, c.box_hi);
+  SearchParams P;
+  P.Lx = (float)box[0];
+  P.Ly = (float)box[1];
+  P.Lz = (float)box[2];
+  P.wx = G.wx;
+  P.wy = G.wy;
+  P.Nx = G.Nx;
+  P.Ny = G.Ny;
+  double Rw = c.reach + 3e-6 * (box[0] + box[1] + box[2]);
+  P.R2f = (float)(Rw * Rw);
+  P.Rbox = (float)(Rw + 2e-5 * (box[0] + box[1] + box[2]) + 1e-6);
+  P.groups_cap = c.groups_cap;
+  P.list_cap = c.list_cap;
+  nb_search<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, c.sizes, c.order, c.xw, c.box_lo, c.box_hi,
+                                                       c.group_start, c.excl_off, c.excl, c.slab,
+                                                       c.counts, c.sizes);
+  nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts,
+                                                             c.list_cap, c.unit_n);
+  nb_scan(c.unit_n, c.unit_start, (int)c.groups_cap, nullptr, c.scan_scratch, s);
+  nb_unit_write<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.unit_n, c.unit_start,
+                                                             c.units_cap, c.units, c.sizes);
+  nb_count_entries<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts,
+                                                                c.sizes);
+}
+
+// One complete build with count-then-grow: the list capacity C grows to a
+// quarter more than the longest list and the build runs again until every
+// list fits (MDIR: mdrtGroupsGrow, runtime/mdrt_cuda.c:3185, and the build
+// loop of lib/Conversion/MDExecToGPU/MDExecToGPU.cpp:10107-10175).
+int nb_build_run(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
+  NbGrid G = nb_plan_grid(c.n, box);
+  int64_t cap = c.list_cap;
+  if (cap == 0) cap = nb_initial_list_cap(c.n, box, c.reach, G);
+  c.grid = G;
+  if (!c.key) {
+    if (nb_realloc(c.key, c.n) || nb_realloc(c.sorted, c.n) || nb_realloc(c.atom_xw, c.n) ||
+        nb_realloc(c.atom_shift, c.n) || nb_realloc(c.place_of, c.n))
+      return -1;
+  }
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    if (nb_reserve(c, G, cap)) return -1;
+    nb_build_launch(c, x, box, s);
+    NB_CHECK(cudaMemcpyAsync(c.h_sizes, c.sizes, sizeof(int32_t) * NB_SIZE_COUNT,
+                             cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaStreamSynchronize(s));
+    NB_CHECK(cudaGetLastError());
+    if (c.h_sizes[NB_SIZE_OVERFLOW] == 0) {
+      c.built = true;
+      c.builds++;
+      for (int k = 0; k < 3; ++k) c.box_built[k] = box[k];
+      return 0;
+    }
+    int64_t longest = c.h_sizes[NB_SIZE_LONGEST];
+    int64_t want = (longest + longest / 4 + NB_UNIT - 1) / NB_UNIT * NB_UNIT;
+    cap = std::max(cap, want);
+    c.grows++;
+  }
+  return -1;
+}

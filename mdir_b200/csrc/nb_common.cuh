@@ -1,0 +1,66 @@
+// Shared definitions of the sm_100a short-range nonbonded + PME library.
+//
+// Layout in HBM (one context = one system on one device):
+//   places     P = 16 * groups; place p holds atom order[p] or -1 (empty).
+//              A group is 16 consecutive places of one column of the grid,
+//              sorted along z (the spatial cell sort of the build).
+//   frames     xq[p] = float4(x + S_p L rounded once to f32, q); S_p is the
+//              whole-cell shift that took the atom into the cell at the
+//              last build (kept per place, three int8 in shift_p).
+//   lists      one slab of C entries per group: entry = int2(q, bits) with
+//              q the partner place, bits 0-15 the members that pair with it
+//              and bits 16-20 the image code 9(sz+1)+3(sy+1)+(sx+1).
+//   units      (group, ordinal) work items of 64 entries each, in group
+//              order, so that every launch sees them in the same order.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define NB_GROUP 16
+#define NB_UNIT 64
+#define NB_WARP 32
+
+// sizes[] slots written by the build (device) and read by the host.
+enum NbSizeSlot {
+  NB_SIZE_PLACES = 0,     // places the build needed (16 * groups)
+  NB_SIZE_LONGEST = 1,    // longest list of a group (entries)
+  NB_SIZE_UNITS = 2,      // units of 64 entries
+  NB_SIZE_EXCL_WIDE = 3,  // groups whose excluded partners did not fit smem
+  NB_SIZE_NAN = 4,        // positions that are not finite or far outside
+  NB_SIZE_OVERFLOW = 5,   // 1 if any buffer was too small (nothing past it written)
+  NB_SIZE_GROUPS = 6,     // groups used
+  NB_SIZE_ENTRIES = 7,    // total entries written
+  NB_SIZE_COUNT = 8
+};
+
+// Device status word bits (mdrtNbStatus).
+enum NbStatusBits {
+  NB_STATUS_LIST_OVERFLOW = 1,
+  NB_STATUS_FIXED_OVERFLOW = 2,
+  NB_STATUS_NAN = 4,
+  NB_STATUS_STALE_LIST = 8,
+  NB_STATUS_TIMEOUT = 16,
+};
+
+struct NbBox {
+  float L[3];      // edges in f32
+  double Ld[3];    // edges in f64
+};
+
+__host__ __device__ inline int nb_image_code(int sx, int sy, int sz) {
+  return 9 * (sz + 1) + 3 * (sy + 1) + (sx + 1);
+}
+
+__device__ __forceinline__ void nb_decode_image(int code, int &sx, int &sy, int &sz) {
+  sz = code / 9 - 1;
+  int r = code - 9 * (sz + 1);
+  sy = r / 3 - 1;
+  sx = r - 3 * (sy + 1) - 1;
+}
+
+// Fixed-point scale of the deterministic force accumulators: 2^32 units
+// per kJ/mol/nm.
+#define NB_FORCE_SCALE 4294967296.0
+#define NB_FORCE_SCALE_INV (1.0 / 4294967296.0)
+// Fixed-point scale of the deterministic PME grid: 2^40 per e.
+#define NB_GRID_SCALE 1099511627776.0

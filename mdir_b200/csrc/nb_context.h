@@ -1,0 +1,114 @@
+// The host-side context of one system on one device: the buffers of the
+// neighbor structure, the particle tables, PME plans and the scratch of the
+// reductions.  Everything here is owned by the library; callers pass their
+// own state (positions, forces) as plain device pointers.
+#pragma once
+#include <cufft.h>
+#include <cstdint>
+#include <vector>
+
+#include "nb_common.cuh"
+
+struct NbGrid {
+  int Nx = 1, Ny = 1, Nz = 1;  // columns along x, y; z bins per column
+  float wx = 1, wy = 1, hz = 1;  // column widths, bin height
+  int ncol() const { return Nx * Ny; }
+  int nbins() const { return Nx * Ny * Nz; }
+};
+
+struct NbPme {
+  int K[3] = {0, 0, 0};
+  int order = 4;
+  bool on = false;
+  cufftHandle fwd = 0, bwd = 0;
+  float *grid = nullptr;        // K0*K1*K2 real grid
+  float2 *spec = nullptr;       // K0*K1*(K2/2+1)
+  unsigned long long *fixed = nullptr;  // deterministic spreading, K0*K1*K2
+  float *moduli = nullptr;      // |b|^2 tables: K0 + K1 + K2 floats
+  float *pme_force = nullptr;   // float4 per place (gather output)
+  float *potential = nullptr;   // f32 per place: dE_rec/dq
+  double *partials = nullptr;   // per-block energy/virial partials of the convolution
+  int conv_blocks = 0;
+  size_t workspace_bytes = 0;
+};
+
+struct NbCtx {
+  int device = 0;
+  int64_t n = 0;
+  // particle tables (atom order)
+  float *q = nullptr;
+  int32_t *type = nullptr;
+  int32_t ntypes = 0;
+  float2 *lj = nullptr;  // (c6, c12) per type pair, c6 = 4 eps sig^6, c12 = 4 eps sig^12
+  std::vector<double> h_q;     // f64 charges for the host constants
+  std::vector<double> h_c6;    // f64 c6 = 4 eps sig^6 per type pair
+  std::vector<int32_t> h_type;
+  std::vector<float2> h_lj;
+  // exclusions: ragged rows (atom order) and the list of pairs i < j
+  int32_t *excl_off = nullptr, *excl = nullptr;
+  int32_t *excl_pairs = nullptr;
+  int64_t n_excl_pairs = 0;
+  // interaction parameters
+  double cutoff = 1.0, reach = 1.1, beta = 0.0, coulomb = 138.935457644;
+  int coulomb_shift = 0, lj_switch = 0;
+  double switch_distance = 0.0;
+  bool deterministic = false;
+  // neighbor structure
+  NbGrid grid;
+  double box_built[3] = {0, 0, 0};
+  int64_t groups_cap = 0, places_cap = 0, bins_cap = 0, cols_cap = 0;
+  int64_t list_cap = 0;    // C: entries per group
+  int64_t units_cap = 0;
+  int32_t *order = nullptr, *place_of = nullptr;
+  char4 *shift = nullptr;  // per place
+  float4 *xw = nullptr;    // per place, f32 wrapped at the build
+  float4 *box_lo = nullptr, *box_hi = nullptr;  // per group
+  int32_t *group_start = nullptr;  // per column + 1
+  int32_t *group_col = nullptr;    // per group
+  int2 *slab = nullptr;            // groups_cap * list_cap entries
+  int32_t *counts = nullptr;       // per group
+  int32_t *unit_n = nullptr, *unit_start = nullptr;  // per group (+1)
+  int2 *units = nullptr;           // (group, ordinal)
+  int32_t *sizes = nullptr;        // NB_SIZE_COUNT ints on the device
+  int32_t *h_sizes = nullptr;      // pinned mirror
+  int32_t *status = nullptr;       // device status word
+  // build scratch
+  int32_t *key = nullptr, *bin_count = nullptr, *bin_start = nullptr, *bin_fill = nullptr;
+  int32_t *sorted = nullptr, *col_groups = nullptr, *scan_scratch = nullptr;
+  float4 *atom_xw = nullptr;
+  char4 *atom_shift = nullptr;
+  // per-step frames and accumulators (place order)
+  float4 *xq = nullptr;
+  int32_t *typ_p = nullptr;
+  float4 *acc = nullptr;                 // pair + excluded forces, f32 atomics
+  unsigned long long *acc_fixed = nullptr;  // 3 per place, deterministic mode
+  double *unit_partials = nullptr;       // 8 doubles per unit
+  double *excl_partials = nullptr;       // 8 doubles per block of the excluded kernel
+  double *energy = nullptr;              // device results: see NbEnergySlot
+  double *h_energy = nullptr;            // pinned mirror
+  NbPme pme;
+  bool built = false;
+  int64_t builds = 0, grows = 0;
+};
+
+// Energy / virial slots of ctx->energy (f64, device).
+enum NbEnergySlot {
+  NB_E_LJ = 0,
+  NB_E_COUL = 1,
+  NB_E_EXCL = 2,
+  NB_E_REC = 3,
+  NB_W_PAIR = 4,   // 6 entries: xx yy zz xy xz yz (pairs + excluded)
+  NB_W_REC = 10,   // 6 entries
+  NB_E_SLOTS = 16
+};
+
+// Launchers implemented in the .cu files.
+int nb_build_run(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
+void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
+void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
+void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
+void nb_finish_forces(NbCtx &c, double *forces, int accumulate, cudaStream_t s);
+void nb_reduce_energy(NbCtx &c, bool pairs, bool excluded, cudaStream_t s);
+int nb_pme_setup(NbCtx &c, int k0, int k1, int k2, int order);
+void nb_pme_release(NbCtx &c);
+int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaStream_t s);

@@ -1,0 +1,460 @@
+// The Lennard-Jones + Ewald real-space pair kernel on sm_100a, the excluded
+// pair correction, the frame gather and the force / energy finish.
+//
+// Replaces MDIR's emitted pair loop (lib/Conversion/MDExecKernels/
+// TraversePairs.cpp:85 emitGroupPairKernel; schedule in
+// docs/neighbor-groups.md:533-594) and the excluded-pair tuple loop
+// (lib/Driver/TermNonbonded.cpp:1615-1671).  Physics as
+// TermNonbonded.cpp:378-466 and TermLennardJones.cpp:26-80: for each
+// unordered pair in the lists with r^2 < rc^2 (strict), LJ from a table of
+// (c6, c12) by type pair and f q_i q_j (erfc(beta r)/r - shift).
+//
+// Schedule (B200 design): a warp takes a unit of <= 64 entries of one group
+// in two rounds of 32.  Each lane keeps its own entry (partner place, mask,
+// image) and its partner's position in registers for the whole round; the
+// 16 members are read from shared memory, lane l taking member (l + k) mod
+// 16 at step k, so the 32 lanes visit 32 different (member, entry) slots
+// per step.  The member's force accumulator travels with the member: after
+// each step it moves one lane down the half-warp (3 shuffles), and after 16
+// steps it is home again.  The partner's force stays in its lane and is
+// added once per entry with one float4 atomic (red.global.add.v4.f32), or
+// three 64-bit integer atomics in fixed point in the deterministic mode.
+// Energies and virial go to a per-unit f64 slot, summed later in a fixed
+// order, so they are bitwise reproducible in every mode.
+#include <cmath>
+#include <cstdio>
+
+#include "nb_context.h"
+
+#define NB_MAX_TYPES 32
+
+namespace {
+
+struct PairParams {
+  float Lx, Ly, Lz;
+  float rc2;
+  float beta;
+  float two_beta_sqrtpi;
+  float coulomb;
+  float coulomb_shift;  // erfc(beta rc)/rc when the direct sum is shifted, else 0
+  float rs2, winv;      // LJ switch in r^2
+  int ntypes;
+  int64_t list_cap;
+  int64_t units_cap;
+};
+
+// erfc(x) for x >= 0 from exp(-x^2): Abramowitz & Stegun 7.1.26
+// (Hastings), |error| <= 1.5e-7.  `ex` is exp(-x^2), computed once and
+// shared with the force.
+__device__ __forceinline__ float nb_erfc_from_exp(float x, float ex) {
+  const float p = 0.3275911f;
+  const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
+              a5 = 1.061405429f;
+  float t = __fdividef(1.0f, fmaf(p, x, 1.0f));
+  float poly = fmaf(fmaf(fmaf(fmaf(a5, t, a4), t, a3), t, a2), t, a1) * t;
+  return poly * ex;
+}
+
+__device__ __forceinline__ void nb_red_add_v4(float4 *addr, float x, float y, float z) {
+  // one vector reduction instead of three (sm_90 and newer)
+  atomicAdd(addr, make_float4(x, y, z, 0.f));
+}
+
+__device__ __forceinline__ void nb_red_fixed(unsigned long long *addr, float x, float y, float z,
+                                             int *status) {
+  if (fabsf(x) > 1e9f || fabsf(y) > 1e9f || fabsf(z) > 1e9f) atomicOr(status, NB_STATUS_FIXED_OVERFLOW);
+  atomicAdd(addr + 0, (unsigned long long)__float2ll_rn(x * 4294967296.0f));
+  atomicAdd(addr + 1, (unsigned long long)__float2ll_rn(y * 4294967296.0f));
+  atomicAdd(addr + 2, (unsigned long long)__float2ll_rn(z * 4294967296.0f));
+}
+
+template <bool ENERGY, bool FIXED, bool SWITCH>
+__global__ void __launch_bounds__(256) nb_pairs(PairParams P, const int32_t *__restrict__ sizes,
+                                                const int2 *__restrict__ units,
+                                                const int2 *__restrict__ slab,
+                                                const int32_t *__restrict__ counts,
+                                                const float4 *__restrict__ xq,
+                                                const int32_t *__restrict__ typ,
+                                                const float2 *__restrict__ lj, float4 *__restrict__ acc,
+                                                unsigned long long *__restrict__ accf,
+                                                double *__restrict__ partials, int *__restrict__ status) {
+  __shared__ float4 s_x[8][NB_GROUP];
+  __shared__ int s_t[8][NB_GROUP];
+  __shared__ float2 s_lj[NB_MAX_TYPES * NB_MAX_TYPES];
+  const unsigned FULL = 0xffffffffu;
+  int nt2 = P.ntypes * P.ntypes;
+  for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = lj[k];
+  __syncthreads();
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int u = lane & 15;
+  int nunits = min((int64_t)sizes[NB_SIZE_UNITS], P.units_cap);
+  int wstride = gridDim.x * 8;
+  for (int unit = blockIdx.x * 8 + warp; unit < nunits; unit += wstride) {
+    int2 uo = units[unit];
+    int g = uo.x;
+    int64_t pi = (int64_t)g * NB_GROUP + u;
+    __syncwarp();
+    if (lane < 16) {
+      float4 xi = xq[pi];
+      xi.w *= P.coulomb;
+      s_x[warp][u] = xi;
+      s_t[warp][u] = typ[pi] * P.ntypes;
+    }
+    __syncwarp();
+    int cnt = (int)min((int64_t)counts[g], P.list_cap);
+    int e0 = uo.y * NB_UNIT;
+    int ne = min(NB_UNIT, cnt - e0);
+    float ax = 0.f, ay = 0.f, az = 0.f;  // the accumulator of member (lane + k) mod 16
+    float elj = 0.f, ecl = 0.f;
+    float vxx = 0.f, vyy = 0.f, vzz = 0.f, vxy = 0.f, vxz = 0.f, vyz = 0.f;
+    for (int r = 0; r < 2; ++r) {
+      if (r * 32 >= ne) break;
+      bool valid = r * 32 + lane < ne;
+      int2 en = valid ? slab[(int64_t)g * P.list_cap + e0 + r * 32 + lane] : make_int2(0, 0);
+      int q = en.x;
+      unsigned mask = valid ? ((unsigned)en.y & 0xffffu) : 0u;
+      int code = ((unsigned)en.y >> 16) & 31;
+      int sx, sy, sz;
+      nb_decode_image(code, sx, sy, sz);
+      float4 xj = xq[q];
+      xj.x += (float)sx * P.Lx;
+      xj.y += (float)sy * P.Ly;
+      xj.z += (float)sz * P.Lz;
+      int tj = typ[q];
+      float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+#pragma unroll
+      for (int k = 0; k < NB_GROUP; ++k) {
+        int m = (lane + k) & 15;
+        float4 xm = s_x[warp][m];
+        float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
+        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        bool inside = ((mask >> m) & 1u) && (r2 < P.rc2);
+        float r2s = inside ? r2 : 1.0f;
+        float2 cc = s_lj[s_t[warp][m] + tj];
+        float rinv = rsqrtf(r2s);
+        float rinv2 = rinv * rinv;
+        float s6 = rinv2 * rinv2 * rinv2;
+        float a12 = cc.y * s6 * s6, a6 = cc.x * s6;
+        float fs = (12.f * a12 - 6.f * a6) * rinv2;
+        float ulj = a12 - a6;
+        if (SWITCH) {
+          float y = fminf(fmaxf((r2s - P.rs2) * P.winv, 0.f), 1.f);
+          float S = (1.f - y) * (1.f - y) * (1.f + 2.f * y);
+          float dSdr2 = -6.f * y * (1.f - y) * P.winv;
+          fs = fs * S - 2.f * ulj * dSdr2;
+          ulj *= S;
+        }
+        float qq = xm.w * xj.w;
+        float rr = r2s * rinv;
+        float bx = P.beta * rr;
+        float ex = __expf(-bx * bx);
+        float erfcv = nb_erfc_from_exp(bx, ex);
+        fs = fmaf(qq * fmaf(erfcv, rinv, P.two_beta_sqrtpi * ex), rinv2, fs);
+        fs = inside ? fs : 0.f;
+        float fx = fs * dx, fy = fs * dy, fz = fs * dz;
+        ax += fx;
+        ay += fy;
+        az += fz;
+        fjx -= fx;
+        fjy -= fy;
+        fjz -= fz;
+        if (ENERGY) {
+          float uc = qq * (erfcv * rinv - P.coulomb_shift);
+          elj += inside ? ulj : 0.f;
+          ecl += inside ? uc : 0.f;
+          vxx = fmaf(dx, fx, vxx);
+          vyy = fmaf(dy, fy, vyy);
+          vzz = fmaf(dz, fz, vzz);
+          vxy = fmaf(dx, fy, vxy);
+          vxz = fmaf(dx, fz, vxz);
+          vyz = fmaf(dy, fz, vyz);
+        }
+        int src = (lane & 16) | ((lane + 1) & 15);
+        ax = __shfl_sync(FULL, ax, src);
+        ay = __shfl_sync(FULL, ay, src);
+        az = __shfl_sync(FULL, az, src);
+      }
+      if (valid && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
+        if (FIXED)
+          nb_red_fixed(accf + 3 * (int64_t)q, fjx, fjy, fjz, status);
+        else
+          nb_red_add_v4(acc + q, fjx, fjy, fjz);
+      }
+    }
+    ax += __shfl_xor_sync(FULL, ax, 16);
+    ay += __shfl_xor_sync(FULL, ay, 16);
+    az += __shfl_xor_sync(FULL, az, 16);
+    if (lane < 16 && (ax != 0.f || ay != 0.f || az != 0.f)) {
+      if (FIXED)
+        nb_red_fixed(accf + 3 * pi, ax, ay, az, status);
+      else
+        nb_red_add_v4(acc + pi, ax, ay, az);
+    }
+    if (ENERGY) {
+      double v[8] = {elj, ecl, vxx, vyy, vzz, vxy, vxz, vyz};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(FULL, v[k], o);
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) partials[(int64_t)unit * 8 + k] = v[k];
+      }
+    }
+  }
+}
+
+// Frames: xq[p] = ((float)(x_a + S_p L), q_a) for the atom a at place p;
+// an empty place gets zeros (no bit names it).
+__global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
+                          const int32_t *__restrict__ order, const char4 *__restrict__ shift,
+                          const double *__restrict__ x, const float *__restrict__ q,
+                          const int32_t *__restrict__ type, double Lx, double Ly, double Lz,
+                          float4 *__restrict__ xq, int32_t *__restrict__ typ_p) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  int a = order[p];
+  if (a < 0) {
+    xq[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    typ_p[p] = 0;
+    return;
+  }
+  char4 s = shift[p];
+  xq[p] = make_float4((float)(x[3 * a] + s.x * Lx), (float)(x[3 * a + 1] + s.y * Ly),
+                      (float)(x[3 * a + 2] + s.z * Lz), q[a]);
+  typ_p[p] = type[a];
+}
+
+// The excluded-pair correction -f q_i q_j erf(beta r)/r in the minimum
+// image, in f64 from the f32 frames (a thread per pair i < j).
+template <bool FIXED>
+__global__ void nb_excluded(int64_t npairs, const int32_t *__restrict__ pairs,
+                            const int32_t *__restrict__ place_of, const float4 *__restrict__ xq,
+                            double Lx, double Ly, double Lz, double beta, double coulomb, bool energy,
+                            float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
+                            double *__restrict__ partials, int *__restrict__ status) {
+  __shared__ double s_part[8][8];
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (k < npairs) {
+    int i = pairs[2 * k], j = pairs[2 * k + 1];
+    int pi = place_of[i], pj = place_of[j];
+    if (pi >= 0 && pj >= 0) {
+      float4 a = xq[pi], b = xq[pj];
+      double d0 = (double)a.x - b.x, d1 = (double)a.y - b.y, d2 = (double)a.z - b.z;
+      d0 -= Lx * rint(d0 / Lx);
+      d1 -= Ly * rint(d1 / Ly);
+      d2 -= Lz * rint(d2 / Lz);
+      double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+      double qq = coulomb * (double)a.w * (double)b.w;
+      if (qq != 0.0 && r2 > 0.0) {
+        double r = sqrt(r2);
+        double ef = erf(beta * r);
+        double g = 2.0 * beta / sqrt(M_PI) * exp(-beta * beta * r2);
+        double fs = qq * (g / r2 - ef / (r2 * r));
+        float fx = (float)(fs * d0), fy = (float)(fs * d1), fz = (float)(fs * d2);
+        if (FIXED) {
+          nb_red_fixed(accf + 3 * (int64_t)pi, fx, fy, fz, status);
+          nb_red_fixed(accf + 3 * (int64_t)pj, -fx, -fy, -fz, status);
+        } else {
+          nb_red_add_v4(acc + pi, fx, fy, fz);
+          nb_red_add_v4(acc + pj, -fx, -fy, -fz);
+        }
+        v[0] = -qq * ef / r;
+        v[1] = d0 * fs * d0;
+        v[2] = d1 * fs * d1;
+        v[3] = d2 * fs * d2;
+        v[4] = d0 * fs * d1;
+        v[5] = d0 * fs * d2;
+        v[6] = d1 * fs * d2;
+      }
+    }
+  }
+  if (!energy) return;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+  }
+  if (lane == 0)
+    for (int c = 0; c < 8; ++c) s_part[warp][c] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += s_part[w][threadIdx.x];
+    partials[(int64_t)blockIdx.x * 8 + threadIdx.x] = s;
+  }
+}
+
+// forces[a] (f64, atom order) = (or +=) the sum of the place accumulators
+// of the pairs, the excluded pairs and PME; the accumulators are cleared
+// for the next evaluation.
+template <bool FIXED>
+__global__ void nb_finish(int64_t places, const int32_t *__restrict__ sizes,
+                          const int32_t *__restrict__ order, float4 *__restrict__ acc,
+                          unsigned long long *__restrict__ accf, const float4 *__restrict__ pme_force,
+                          double *__restrict__ forces, int accumulate) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  int a = order[p];
+  double f0, f1, f2;
+  if (FIXED) {
+    long long x = (long long)accf[3 * p], y = (long long)accf[3 * p + 1], z = (long long)accf[3 * p + 2];
+    accf[3 * p] = 0ull;
+    accf[3 * p + 1] = 0ull;
+    accf[3 * p + 2] = 0ull;
+    f0 = (double)x * NB_FORCE_SCALE_INV;
+    f1 = (double)y * NB_FORCE_SCALE_INV;
+    f2 = (double)z * NB_FORCE_SCALE_INV;
+  } else {
+    float4 v = acc[p];
+    acc[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    f0 = v.x;
+    f1 = v.y;
+    f2 = v.z;
+  }
+  if (pme_force) {
+    float4 w = pme_force[p];
+    f0 += w.x;
+    f1 += w.y;
+    f2 += w.z;
+  }
+  if (a < 0) return;
+  if (accumulate) {
+    forces[3 * a] += f0;
+    forces[3 * a + 1] += f1;
+    forces[3 * a + 2] += f2;
+  } else {
+    forces[3 * a] = f0;
+    forces[3 * a + 1] = f1;
+    forces[3 * a + 2] = f2;
+  }
+}
+
+// Fixed-order sums of per-unit (and per-block) partials: one block, each
+// thread a strided run of rows, then a tree.
+__global__ void nb_sum_partials(const double *__restrict__ unit_partials,
+                                const int32_t *__restrict__ sizes, int64_t units_cap,
+                                const double *__restrict__ excl_partials, int excl_blocks,
+                                int do_pairs, double *__restrict__ energy) {
+  __shared__ double s[256][8];
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (do_pairs) {
+    int64_t nunits = min((int64_t)sizes[NB_SIZE_UNITS], units_cap);
+    for (int64_t u = threadIdx.x; u < nunits; u += blockDim.x)
+      for (int k = 0; k < 8; ++k) v[k] += unit_partials[u * 8 + k];
+  }
+  for (int64_t b = threadIdx.x; b < excl_blocks; b += blockDim.x)
+    for (int k = 0; k < 8; ++k) w[k] += excl_partials[b * 8 + k];
+  // pairs: lj, coul, W(6); excluded: e, W(6): combine W of both in slots
+  for (int k = 0; k < 8; ++k) s[threadIdx.x][k] = v[k];
+  __syncthreads();
+  for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+    if ((int)threadIdx.x < stride)
+      for (int k = 0; k < 8; ++k) s[threadIdx.x][k] += s[threadIdx.x + stride][k];
+    __syncthreads();
+  }
+  double pv[8];
+  for (int k = 0; k < 8; ++k) pv[k] = s[0][k];
+  __syncthreads();
+  for (int k = 0; k < 8; ++k) s[threadIdx.x][k] = w[k];
+  __syncthreads();
+  for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+    if ((int)threadIdx.x < stride)
+      for (int k = 0; k < 8; ++k) s[threadIdx.x][k] += s[threadIdx.x + stride][k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (do_pairs) {
+      energy[NB_E_LJ] = pv[0];
+      energy[NB_E_COUL] = pv[1];
+    }
+    if (excl_blocks > 0) energy[NB_E_EXCL] = s[0][0];
+    for (int k = 0; k < 6; ++k)
+      energy[NB_W_PAIR + k] = (do_pairs ? pv[2 + k] : 0.0) + (excl_blocks > 0 ? s[0][1 + k] : 0.0);
+  }
+}
+
+inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
+
+int g_sm_count = 0;
+
+}  // namespace
+
+void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
+  nb_gather<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.shift, x,
+                                                          c.q, c.type, box[0], box[1], box[2], c.xq,
+                                                          c.typ_p);
+}
+
+void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
+  if (!g_sm_count) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  PairParams P;
+  P.Lx = (float)box[0];
+  P.Ly = (float)box[1];
+  P.Lz = (float)box[2];
+  P.rc2 = (float)(c.cutoff * c.cutoff);
+  P.beta = (float)c.beta;
+  P.two_beta_sqrtpi = (float)(2.0 * c.beta / sqrt(M_PI));
+  P.coulomb = (float)c.coulomb;
+  P.coulomb_shift = c.coulomb_shift ? (float)(erfc(c.beta * c.cutoff) / c.cutoff) : 0.f;
+  double rs2 = c.switch_distance * c.switch_distance;
+  P.rs2 = (float)rs2;
+  P.winv = c.lj_switch ? (float)(1.0 / (c.cutoff * c.cutoff - rs2)) : 0.f;
+  P.ntypes = c.ntypes;
+  P.list_cap = c.list_cap;
+  P.units_cap = c.units_cap;
+  // persistent grid: enough warps for the units, at most 8 blocks per SM
+  int64_t want = (c.units_cap + 7) / 8;
+  int grid = (int)std::min<int64_t>(want, (int64_t)g_sm_count * 8);
+  if (grid < 1) grid = 1;
+#define NB_LAUNCH(E, F, S)                                                                        \
+  nb_pairs<E, F, S><<<grid, 256, 0, s>>>(P, c.sizes, c.units, c.slab, c.counts, c.xq, c.typ_p, c.lj, \
+                                        c.acc, c.acc_fixed, c.unit_partials, c.status)
+  bool F = c.deterministic, S = c.lj_switch != 0;
+  if (energy) {
+    if (F) { if (S) NB_LAUNCH(true, true, true); else NB_LAUNCH(true, true, false); }
+    else { if (S) NB_LAUNCH(true, false, true); else NB_LAUNCH(true, false, false); }
+  } else {
+    if (F) { if (S) NB_LAUNCH(false, true, true); else NB_LAUNCH(false, true, false); }
+    else { if (S) NB_LAUNCH(false, false, true); else NB_LAUNCH(false, false, false); }
+  }
+#undef NB_LAUNCH
+}
+
+void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
+  if (c.n_excl_pairs == 0 || c.beta == 0.0) return;
+  int blocks = blocks_for(c.n_excl_pairs, 256);
+  if (c.deterministic)
+    nb_excluded<true><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, c.place_of, c.xq, box[0],
+                                             box[1], box[2], c.beta, c.coulomb, energy, c.acc,
+                                             c.acc_fixed, c.excl_partials, c.status);
+  else
+    nb_excluded<false><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, c.place_of, c.xq, box[0],
+                                              box[1], box[2], c.beta, c.coulomb, energy, c.acc,
+                                              c.acc_fixed, c.excl_partials, c.status);
+}
+
+void nb_finish_forces(NbCtx &c, double *forces, int accumulate, cudaStream_t s) {
+  const float4 *pf = c.pme.on ? (const float4 *)c.pme.pme_force : nullptr;
+  if (c.deterministic)
+    nb_finish<true><<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.acc,
+                                                                 c.acc_fixed, pf, forces, accumulate);
+  else
+    nb_finish<false><<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.acc,
+                                                                  c.acc_fixed, pf, forces, accumulate);
+}
+
+void nb_reduce_energy(NbCtx &c, bool pairs, bool excluded, cudaStream_t s) {
+  int eb = (excluded && c.n_excl_pairs > 0 && c.beta != 0.0) ? blocks_for(c.n_excl_pairs, 256) : 0;
+  nb_sum_partials<<<1, 256, 0, s>>>(c.unit_partials, c.sizes, c.units_cap, c.excl_partials, eb,
+                                    pairs ? 1 : 0, c.energy);
+}

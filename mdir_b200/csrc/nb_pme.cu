@@ -1,0 +1,419 @@
+// Smooth particle mesh Ewald on sm_100a: B-spline charge spreading, the
+// influence-function convolution with the reciprocal energy and virial, and
+// force / potential gathering; the 3D FFTs stay on cuFFT.
+//
+// Replaces MDIR's PME device stages (lib/Conversion/MDExecToGPU/
+// DevicePME.cpp:38-75; PMEWeights.cpp, PMESpreadBricks.cpp, PMEConvolve.cpp,
+// PMEGather.cpp; the fixed-point spreading of docs/pme.md, Section 3, D70)
+// and its cuFFT entries (runtime/mdrt_cuda.c:2942-2990).  Equations as
+// docs/pme.md, Sections 1 and 1.2: Q(k) = sum_i q_i M_p M_p M_p,
+// E = 1/2 sum_m B(m) C(m) |F Q(m)|^2 with C = f/(pi V) exp(-pi^2 m^2/beta^2)/m^2,
+// W_ab = sum_m E_m (delta_ab - 2 (1/m^2 + pi^2/beta^2) m_a m_b).
+//
+// B200 design: every stage reads the f32 frames of the places (the same
+// array the pair kernel reads), so spreading and gathering walk atoms in the
+// spatial order of the build and the grid lines they touch stay in L2 (a
+// 64^3 grid is 1 MiB of a 126 MB L2).  Spreading uses `order` threads per
+// atom, one per z point, each adding its order^2 products with f32
+// reductions (or 64-bit integer reductions at 2^40 in the deterministic
+// mode); the convolution scales the half-complex spectrum in place and sums
+// energy and virial in f64 per block, summed again in a fixed order.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "nb_context.h"
+
+namespace {
+
+// w[j] = M_p(t + j), dw[j] its slope, j = 0..p-1; weight j belongs to grid
+// point floor(u) - j.  M_n(x) = (x M_{n-1}(x) + (n - x) M_{n-1}(x - 1))/(n - 1).
+template <int P>
+__device__ __forceinline__ void nb_bspline(float t, float *w, float *dw) {
+  float a[P];
+  a[0] = t;
+  a[1] = 1.f - t;
+#pragma unroll
+  for (int j = 2; j < P; ++j) a[j] = 0.f;
+#pragma unroll
+  for (int m = 3; m <= P; ++m) {
+    float prev[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) prev[j] = a[j];
+    if (m == P && dw) {
+#pragma unroll
+      for (int j = 0; j < P; ++j) dw[j] = (j < m - 1 ? prev[j] : 0.f) - (j > 0 ? prev[j - 1] : 0.f);
+    }
+    float inv = 1.f / (float)(m - 1);
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      if (j < m) {
+        float left = j < m - 1 ? prev[j] : 0.f;
+        float right = j > 0 ? prev[j - 1] : 0.f;
+        a[j] = ((t + j) * left + ((float)m - t - j) * right) * inv;
+      }
+    }
+  }
+  if (P == 2 && dw) {
+    dw[0] = 1.f;
+    dw[1] = -1.f;
+  }
+#pragma unroll
+  for (int j = 0; j < P; ++j) w[j] = a[j];
+}
+
+__device__ __forceinline__ void nb_frac(float x, float invL, int K, int &k0, float &t) {
+  float f = x * invL;
+  f -= floorf(f);
+  float u = f * (float)K;
+  float fl = floorf(u);
+  int k = (int)fl;
+  if (k >= K) k -= K;
+  if (k < 0) k += K;
+  k0 = k;
+  t = u - fl;
+  if (t >= 1.f) t = 0.f;
+}
+
+struct GridParams {
+  int K0, K1, K2;
+  float invL0, invL1, invL2;
+};
+
+template <int P, bool FIXED>
+__global__ void __launch_bounds__(256) nb_spread(GridParams G, int64_t places,
+                                                 const int32_t *__restrict__ sizes,
+                                                 const int32_t *__restrict__ order,
+                                                 const float4 *__restrict__ xq, float *__restrict__ grid,
+                                                 unsigned long long *__restrict__ fixed) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t p = t / P;
+  int c = (int)(t - p * P);
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  if (order[p] < 0) return;
+  float4 v = xq[p];
+  if (v.w == 0.f) return;
+  int k0, k1, k2;
+  float t0, t1, t2;
+  nb_frac(v.x, G.invL0, G.K0, k0, t0);
+  nb_frac(v.y, G.invL1, G.K1, k1, t1);
+  nb_frac(v.z, G.invL2, G.K2, k2, t2);
+  float w0[P], w1[P], w2[P];
+  nb_bspline<P>(t0, w0, nullptr);
+  nb_bspline<P>(t1, w1, nullptr);
+  nb_bspline<P>(t2, w2, nullptr);
+  int gz = k2 - c;
+  if (gz < 0) gz += G.K2;
+  float qz = v.w * w2[c];
+#pragma unroll
+  for (int jx = 0; jx < P; ++jx) {
+    int gx = k0 - jx;
+    if (gx < 0) gx += G.K0;
+    float qxz = qz * w0[jx];
+#pragma unroll
+    for (int jy = 0; jy < P; ++jy) {
+      int gy = k1 - jy;
+      if (gy < 0) gy += G.K1;
+      int64_t idx = ((int64_t)gx * G.K1 + gy) * G.K2 + gz;
+      float val = qxz * w1[jy];
+      if (FIXED)
+        atomicAdd(fixed + idx, (unsigned long long)__double2ll_rn((double)val * NB_GRID_SCALE));
+      else
+        atomicAdd(grid + idx, val);
+    }
+  }
+}
+
+__global__ void nb_fixed_to_grid(int64_t total, unsigned long long *__restrict__ fixed,
+                                 float *__restrict__ grid) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= total) return;
+  long long v = (long long)fixed[k];
+  fixed[k] = 0ull;
+  grid[k] = (float)((double)v * (1.0 / NB_GRID_SCALE));
+}
+
+struct ConvParams {
+  int K0, K1, K2, H2;  // H2 = K2/2 + 1
+  double L0, L1, L2;
+  double pref;       // f / (pi V)
+  double pi2_beta2;  // pi^2 / beta^2
+};
+
+// Multiplies the half-complex spectrum by B C and sums E and W in f64.
+template <bool ENERGY>
+__global__ void __launch_bounds__(256) nb_convolve(ConvParams C, const float *__restrict__ moduli,
+                                                   float2 *__restrict__ spec,
+                                                   double *__restrict__ partials) {
+  __shared__ double s_part[8][7];
+  int64_t total = (int64_t)C.K0 * C.K1 * C.H2;
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (k < total) {
+    int i2 = (int)(k % C.H2);
+    int64_t r = k / C.H2;
+    int i1 = (int)(r % C.K1);
+    int i0 = (int)(r / C.K1);
+    double m0 = (i0 <= C.K0 / 2 ? i0 : i0 - C.K0) / C.L0;
+    double m1 = (i1 <= C.K1 / 2 ? i1 : i1 - C.K1) / C.L1;
+    double m2v = (i2 <= C.K2 / 2 ? i2 : i2 - C.K2) / C.L2;
+    double mm = m0 * m0 + m1 * m1 + m2v * m2v;
+    float2 s = spec[k];
+    double bc = 0.0;
+    if (k != 0) {
+      double B = (double)moduli[i0] * (double)moduli[C.K0 + i1] * (double)moduli[C.K0 + C.K1 + i2];
+      bc = B * C.pref * exp(-C.pi2_beta2 * mm) / mm;
+    }
+    spec[k] = make_float2((float)(s.x * bc), (float)(s.y * bc));
+    if (ENERGY && k != 0) {
+      double wgt = (i2 == 0 || (C.K2 % 2 == 0 && i2 == C.K2 / 2)) ? 1.0 : 2.0;
+      double em = 0.5 * wgt * bc * ((double)s.x * s.x + (double)s.y * s.y);
+      double f = -2.0 * (1.0 / mm + C.pi2_beta2);
+      v[0] = em;
+      v[1] = em * (1.0 + f * m0 * m0);
+      v[2] = em * (1.0 + f * m1 * m1);
+      v[3] = em * (1.0 + f * m2v * m2v);
+      v[4] = em * f * m0 * m1;
+      v[5] = em * f * m0 * m2v;
+      v[6] = em * f * m1 * m2v;
+    }
+  }
+  if (!ENERGY) return;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+  }
+  if (lane == 0)
+    for (int c = 0; c < 7; ++c) s_part[warp][c] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += s_part[w][threadIdx.x];
+    partials[(int64_t)blockIdx.x * 7 + threadIdx.x] = s;
+  }
+}
+
+__global__ void nb_pme_sum(const double *__restrict__ partials, int nblocks, double *__restrict__ energy) {
+  __shared__ double s[256][7];
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int k = 0; k < 7; ++k) v[k] += partials[(int64_t)b * 7 + k];
+  for (int k = 0; k < 7; ++k) s[threadIdx.x][k] = v[k];
+  __syncthreads();
+  for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+    if ((int)threadIdx.x < stride)
+      for (int k = 0; k < 7; ++k) s[threadIdx.x][k] += s[threadIdx.x + stride][k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    energy[NB_E_REC] = s[0][0];
+    for (int k = 0; k < 6; ++k) energy[NB_W_REC + k] = s[0][1 + k];
+  }
+}
+
+// F_i = -q_i sum_k phi(k) grad(M M M); optional potential phi_i = sum_k phi(k) M M M.
+template <int P>
+__global__ void __launch_bounds__(128) nb_pme_gather(GridParams G, int64_t places,
+                                                     const int32_t *__restrict__ sizes,
+                                                     const int32_t *__restrict__ order,
+                                                     const float4 *__restrict__ xq,
+                                                     const float *__restrict__ phi,
+                                                     float4 *__restrict__ out, float *__restrict__ pot) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  if (order[p] < 0) {
+    out[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (pot) pot[p] = 0.f;
+    return;
+  }
+  float4 v = xq[p];
+  int k0, k1, k2;
+  float t0, t1, t2;
+  nb_frac(v.x, G.invL0, G.K0, k0, t0);
+  nb_frac(v.y, G.invL1, G.K1, k1, t1);
+  nb_frac(v.z, G.invL2, G.K2, k2, t2);
+  float w0[P], w1[P], w2[P], d0[P], d1[P], d2[P];
+  nb_bspline<P>(t0, w0, d0);
+  nb_bspline<P>(t1, w1, d1);
+  nb_bspline<P>(t2, w2, d2);
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f, e = 0.f;
+  int gzs[P];
+#pragma unroll
+  for (int jz = 0; jz < P; ++jz) {
+    int gz = k2 - jz;
+    gzs[jz] = gz < 0 ? gz + G.K2 : gz;
+  }
+#pragma unroll
+  for (int jx = 0; jx < P; ++jx) {
+    int gx = k0 - jx;
+    if (gx < 0) gx += G.K0;
+#pragma unroll
+    for (int jy = 0; jy < P; ++jy) {
+      int gy = k1 - jy;
+      if (gy < 0) gy += G.K1;
+      const float *row = phi + ((int64_t)gx * G.K1 + gy) * G.K2;
+      float sz = 0.f, sdz = 0.f;
+#pragma unroll
+      for (int jz = 0; jz < P; ++jz) {
+        float f = __ldg(row + gzs[jz]);
+        sz = fmaf(f, w2[jz], sz);
+        sdz = fmaf(f, d2[jz], sdz);
+      }
+      g0 = fmaf(d0[jx] * w1[jy], sz, g0);
+      g1 = fmaf(w0[jx] * d1[jy], sz, g1);
+      g2 = fmaf(w0[jx] * w1[jy], sdz, g2);
+      e = fmaf(w0[jx] * w1[jy], sz, e);
+    }
+  }
+  float q = v.w;
+  out[p] = make_float4(-q * g0 * (float)G.K0 * G.invL0, -q * g1 * (float)G.K1 * G.invL1,
+                       -q * g2 * (float)G.K2 * G.invL2, 0.f);
+  if (pot) pot[p] = e;
+}
+
+inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
+
+// |b(m)|^2 of the SPME B-spline moduli along one edge, in f64 on the host.
+std::vector<double> host_moduli(int K, int order) {
+  std::vector<double> a(order + 1, 0.0), prev(order + 1, 0.0);
+  // M_p at the integers 0..p-1 by the recursion with t = 0
+  a[0] = 0.0;
+  a[1] = 1.0;
+  for (int m = 3; m <= order; ++m) {
+    prev = a;
+    for (int j = 0; j < m; ++j) {
+      double left = j < m - 1 ? prev[j] : 0.0;
+      double right = j > 0 ? prev[j - 1] : 0.0;
+      a[j] = (j * left + (m - j) * right) / (m - 1);
+    }
+  }
+  std::vector<double> out(K);
+  for (int m = 0; m < K; ++m) {
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k <= order - 2; ++k) {
+      double arg = 2.0 * M_PI * m * k / K;
+      re += a[k + 1] * cos(arg);
+      im += a[k + 1] * sin(arg);
+    }
+    double s = re * re + im * im;
+    out[m] = s < 1e-7 ? 0.0 : 1.0 / s;
+  }
+  for (int m = 0; m < K; ++m)
+    if (out[m] == 0.0) out[m] = 0.5 * (out[(m + K - 1) % K] + out[(m + 1) % K]);
+  return out;
+}
+
+}  // namespace
+
+int nb_pme_setup(NbCtx &c, int k0, int k1, int k2, int order) {
+  nb_pme_release(c);
+  NbPme &P = c.pme;
+  if (order != 4 && order != 5 && order != 6 && order != 8) return -2;
+  P.K[0] = k0;
+  P.K[1] = k1;
+  P.K[2] = k2;
+  P.order = order;
+  int64_t total = (int64_t)k0 * k1 * k2;
+  int64_t half = (int64_t)k0 * k1 * (k2 / 2 + 1);
+  if (cudaMalloc(&P.grid, sizeof(float) * total) != cudaSuccess) return -1;
+  if (cudaMalloc(&P.spec, sizeof(float2) * half) != cudaSuccess) return -1;
+  if (cudaMalloc(&P.fixed, sizeof(unsigned long long) * total) != cudaSuccess) return -1;
+  cudaMemset(P.fixed, 0, sizeof(unsigned long long) * total);
+  if (cudaMalloc(&P.moduli, sizeof(float) * (k0 + k1 + k2)) != cudaSuccess) return -1;
+  P.conv_blocks = blocks_for(half, 256);
+  if (cudaMalloc(&P.partials, sizeof(double) * 7 * P.conv_blocks) != cudaSuccess) return -1;
+  std::vector<float> mod;
+  for (int K : {k0, k1, k2}) {
+    std::vector<double> m = host_moduli(K, order);
+    for (double v : m) mod.push_back((float)v);
+  }
+  cudaMemcpy(P.moduli, mod.data(), sizeof(float) * mod.size(), cudaMemcpyHostToDevice);
+  if (cufftPlan3d(&P.fwd, k0, k1, k2, CUFFT_R2C) != CUFFT_SUCCESS) return -3;
+  if (cufftPlan3d(&P.bwd, k0, k1, k2, CUFFT_C2R) != CUFFT_SUCCESS) return -3;
+  if (c.places_cap > 0) {
+    if (cudaMalloc(&P.pme_force, sizeof(float4) * c.places_cap) != cudaSuccess) return -1;
+    if (cudaMalloc(&P.potential, sizeof(float) * c.places_cap) != cudaSuccess) return -1;
+  }
+  P.on = true;
+  return 0;
+}
+
+void nb_pme_release(NbCtx &c) {
+  NbPme &P = c.pme;
+  if (P.fwd) cufftDestroy(P.fwd);
+  if (P.bwd) cufftDestroy(P.bwd);
+  P.fwd = P.bwd = 0;
+  for (void *p : {(void *)P.grid, (void *)P.spec, (void *)P.fixed, (void *)P.moduli,
+                  (void *)P.pme_force, (void *)P.potential, (void *)P.partials})
+    if (p) cudaFree(p);
+  P.grid = nullptr;
+  P.spec = nullptr;
+  P.fixed = nullptr;
+  P.moduli = nullptr;
+  P.pme_force = nullptr;
+  P.potential = nullptr;
+  P.partials = nullptr;
+  P.on = false;
+}
+
+int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaStream_t s) {
+  NbPme &P = c.pme;
+  if (!P.on) return 0;
+  GridParams G;
+  G.K0 = P.K[0];
+  G.K1 = P.K[1];
+  G.K2 = P.K[2];
+  G.invL0 = (float)(1.0 / box[0]);
+  G.invL1 = (float)(1.0 / box[1]);
+  G.invL2 = (float)(1.0 / box[2]);
+  int64_t total = (int64_t)G.K0 * G.K1 * G.K2;
+  int64_t half = (int64_t)G.K0 * G.K1 * (G.K2 / 2 + 1);
+  int64_t threads = c.places_cap * P.order;
+  if (!c.deterministic) cudaMemsetAsync(P.grid, 0, sizeof(float) * total, s);
+#define SPREAD(ORD)                                                                                    \
+  if (c.deterministic)                                                                                 \
+    nb_spread<ORD, true><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order,   \
+                                                                  c.xq, P.grid, P.fixed);              \
+  else                                                                                                 \
+    nb_spread<ORD, false><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order,  \
+                                                                   c.xq, P.grid, P.fixed);
+  switch (P.order) {
+    case 4: SPREAD(4); break;
+    case 5: SPREAD(5); break;
+    case 6: SPREAD(6); break;
+    case 8: SPREAD(8); break;
+  }
+#undef SPREAD
+  if (c.deterministic) nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, P.fixed, P.grid);
+  cufftSetStream(P.fwd, s);
+  cufftSetStream(P.bwd, s);
+  if (cufftExecR2C(P.fwd, P.grid, (cufftComplex *)P.spec) != CUFFT_SUCCESS) return -3;
+  ConvParams C;
+  C.K0 = G.K0;
+  C.K1 = G.K1;
+  C.K2 = G.K2;
+  C.H2 = G.K2 / 2 + 1;
+  C.L0 = box[0];
+  C.L1 = box[1];
+  C.L2 = box[2];
+  C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
+  C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
+  if (energy) {
+    nb_convolve<true><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
+    nb_pme_sum<<<1, 256, 0, s>>>(P.partials, P.conv_blocks, c.energy);
+  } else {
+    nb_convolve<false><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
+  }
+  if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.grid) != CUFFT_SUCCESS) return -3;
+  float *pot = potential ? P.potential : nullptr;
+  int blocks = blocks_for(c.places_cap, 128);
+  switch (P.order) {
+    case 4: nb_pme_gather<4><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, (float4 *)P.pme_force, pot); break;
+    case 5: nb_pme_gather<5><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, (float4 *)P.pme_force, pot); break;
+    case 6: nb_pme_gather<6><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, (float4 *)P.pme_force, pot); break;
+    case 8: nb_pme_gather<8><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, (float4 *)P.pme_force, pot); break;
+  }
+  return 0;
+}

@@ -1,0 +1,222 @@
+"""The nonbonded + PME term over the C ABI (include/mdrt_nb.h).
+
+`NonbondedTerm` owns one native context: the neighbor structure, the
+particle tables and the PME plans of one system on one device.  Device
+arrays are torch CUDA tensors (torch is the allocator and the stream
+source, nothing more); every call goes through libmdrt_nb.so."""
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+COULOMB = float.fromhex("0x1.15def44ac2182p+7")  # kJ mol^-1 nm e^-2 (MDIR COULOMB_NATIVE)
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _host(a, dtype):
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype))
+
+
+def _hp(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _dp(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def exclusion_rows(n, pairs):
+    """Ragged rows (offsets[n+1], partners) of excluded pairs, both ways."""
+    pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+    if len(pairs) == 0:
+        return np.zeros(n + 1, dtype=np.int32), np.zeros(0, dtype=np.int32)
+    both = np.concatenate([pairs, pairs[:, ::-1]])
+    both = both[np.lexsort((both[:, 1], both[:, 0]))]
+    counts = np.bincount(both[:, 0], minlength=n)
+    off = np.zeros(n + 1, dtype=np.int32)
+    off[1:] = np.cumsum(counts)
+    return off, both[:, 1].astype(np.int32)
+
+
+class NonbondedTerm:
+    """One system's short-range nonbonded + PME term on one CUDA device."""
+
+    def __init__(self, particles, device=0):
+        self.n = int(particles)
+        self.device = torch.device("cuda", device)
+        torch.cuda.set_device(self.device)
+        handle = ctypes.c_void_p()
+        L.check(L.lib().mdrtNbCreate(ctypes.byref(handle), device, self.n), "mdrtNbCreate")
+        self._h = handle
+        self.box = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().mdrtNbDestroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- configuration -----------------------------------------------------
+    def set_particles(self, charges, types, sigma, epsilon):
+        q = _host(charges, np.float64)
+        t = _host(types, np.int32)
+        sg = _host(sigma, np.float64)
+        ep = _host(epsilon, np.float64)
+        nt = sg.shape[0]
+        L.check(L.lib().mdrtNbSetParticles(self._h, _hp(q), _hp(t), nt, _hp(sg), _hp(ep)),
+                "mdrtNbSetParticles")
+
+    def set_exclusions(self, pairs=None, rows=None):
+        off, part = rows if rows is not None else exclusion_rows(self.n, pairs if pairs is not None else [])
+        off = _host(off, np.int32)
+        part = _host(part, np.int32)
+        L.check(L.lib().mdrtNbSetExclusions(self._h, _hp(off), _hp(part) if len(part) else None),
+                "mdrtNbSetExclusions")
+
+    def set_interaction(self, cutoff, reach, beta, coulomb=COULOMB, coulomb_shift=False,
+                        lj_switch=False, switch_distance=0.0):
+        L.check(L.lib().mdrtNbSetInteraction(self._h, cutoff, reach, beta, coulomb, int(coulomb_shift),
+                                             int(lj_switch), switch_distance), "mdrtNbSetInteraction")
+
+    def set_pme(self, grid, order=4):
+        k = [0, 0, 0] if grid is None else [int(v) for v in grid]
+        L.check(L.lib().mdrtPmeSetup(self._h, k[0], k[1], k[2], int(order)), "mdrtPmeSetup")
+
+    def set_deterministic(self, on=True):
+        L.check(L.lib().mdrtNbSetDeterministic(self._h, int(bool(on))), "mdrtNbSetDeterministic")
+
+    # -- the path ------------------------------------------------------------
+    def _check_x(self, x):
+        if not (x.is_cuda and x.dtype == torch.float64 and x.shape == (self.n, 3) and x.is_contiguous()):
+            raise ValueError("positions: a contiguous CUDA float64 tensor of shape (n, 3)")
+
+    def build(self, x, box, reach=0.0, stream=None, allow_nan=False):
+        """The neighbor build at device positions x; returns the sizes."""
+        self._check_x(x)
+        b = _host(box, np.float64)
+        sizes = np.zeros(L.SIZE_COUNT, dtype=np.int32)
+        s = L.lib().mdrtNbBuild(self._h, _dp(x), self.n, _hp(b), reach, _stream(stream), _hp(sizes))
+        if not (s == L.NAN_POSITION and allow_nan):
+            L.check(s, "mdrtNbBuild")
+        self.box = b
+        return sizes
+
+    def force(self, x, box=None, energy=False, potential=False, forces=None, accumulate=False,
+              pairs=True, pme=True, excluded=True, stream=None):
+        """Forces (device f64 (n, 3)) of the term at x."""
+        self._check_x(x)
+        b = _host(self.box if box is None else box, np.float64)
+        if forces is None:
+            forces = torch.empty((self.n, 3), dtype=torch.float64, device=x.device)
+        flags = (L.ENERGY if energy else 0) | (L.POTENTIAL if potential else 0) | \
+            (L.ACCUMULATE if accumulate else 0) | (0 if pairs else L.NO_PAIRS) | \
+            (0 if pme else L.NO_PME) | (0 if excluded else L.NO_EXCLUDED)
+        L.check(L.lib().mdrtNbForce(self._h, _dp(x), _hp(b), flags, _dp(forces), _stream(stream)),
+                "mdrtNbForce")
+        return forces
+
+    def energies(self, stream=None):
+        out = np.zeros(L.E_COUNT)
+        L.check(L.lib().mdrtNbEnergies(self._h, _stream(stream), _hp(out)), "mdrtNbEnergies")
+        return {"lj": out[L.E_LJ], "coulomb": out[L.E_COULOMB], "excluded": out[L.E_EXCLUDED],
+                "reciprocal": out[L.E_RECIPROCAL],
+                "virial_pair": _sym(out[L.W_PAIR:L.W_PAIR + 6]),
+                "virial_reciprocal": _sym(out[L.W_RECIPROCAL:L.W_RECIPROCAL + 6])}
+
+    def constants(self, box=None, dispersion=False):
+        b = _host(self.box if box is None else box, np.float64)
+        out = np.zeros(4)
+        L.check(L.lib().mdrtNbConstants(self._h, _hp(b), int(dispersion), _hp(out)), "mdrtNbConstants")
+        return {"self": out[0], "background": out[1], "dispersion": out[2], "dispersion_virial": out[3]}
+
+    def potential(self, stream=None):
+        out = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        L.check(L.lib().mdrtPmePotential(self._h, _dp(out), _stream(stream)), "mdrtPmePotential")
+        return out
+
+    def status(self, clear=False, stream=None):
+        v = ctypes.c_int32()
+        L.check(L.lib().mdrtNbStatus(self._h, _stream(stream), int(clear), ctypes.byref(v)), "mdrtNbStatus")
+        return v.value
+
+    def info(self):
+        cap, builds, grows = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        L.check(L.lib().mdrtNbGroupsInfo(self._h, ctypes.byref(cap), ctypes.byref(builds),
+                                         ctypes.byref(grows)), "mdrtNbGroupsInfo")
+        return {"list_capacity": cap.value, "builds": builds.value, "grows": grows.value}
+
+    def buffer(self, slot, dtype, width=1):
+        """A host copy of a buffer of the neighbor structure."""
+        p, k = ctypes.c_void_p(), ctypes.c_int64()
+        L.check(L.lib().mdrtNbGroupsBuffer(self._h, slot, ctypes.byref(p), ctypes.byref(k)),
+                "mdrtNbGroupsBuffer")
+        itemsize = np.dtype(dtype).itemsize * width
+        out = np.empty(k.value * width, dtype=dtype)
+        torch.cuda.synchronize(self.device)
+        res = _cudart().cudaMemcpy(ctypes.c_void_p(out.ctypes.data), p, ctypes.c_size_t(k.value * itemsize), 2)
+        if int(res) != 0:
+            raise RuntimeError(f"cudaMemcpy failed: {res}")
+        return out.reshape(-1, width) if width > 1 else out
+
+    def pair_set(self, sizes):
+        """The (i, j, image code) of every bit of the lists, i < j by atom
+        number, code = 9(sz+1)+3(sy+1)+(sx+1) of j relative to i."""
+        order = self.buffer(L.SLOT_ORDER, np.int32)
+        counts = self.buffer(L.SLOT_COUNTS, np.int32)
+        cap = self.info()["list_capacity"]
+        entries = self.buffer(L.SLOT_ENTRIES, np.int32, 2)
+        G = int(sizes[L.SIZE_GROUPS])
+        counts = counts[:G]
+        E = entries[: G * cap].reshape(G, cap, 2)
+        valid = np.arange(cap)[None, :] < counts[:, None]
+        g_idx, e_idx = np.nonzero(valid)
+        q = E[g_idx, e_idx, 0]
+        bits = E[g_idx, e_idx, 1].astype(np.uint32)
+        mask = bits & 0xFFFF
+        code = (bits >> 16) & 31
+        m_bits = (mask[:, None] >> np.arange(16)[None, :]) & 1
+        k_idx, m_idx = np.nonzero(m_bits)
+        a = order[16 * g_idx[k_idx] + m_idx]
+        b = order[q[k_idx]]
+        c = code[k_idx].astype(np.int64)
+        sz, r = c // 9 - 1, c % 9
+        sy, sx = r // 3 - 1, r % 3 - 1
+        swap = b < a
+        sx = np.where(swap, -sx, sx)
+        sy = np.where(swap, -sy, sy)
+        sz = np.where(swap, -sz, sz)
+        i = np.minimum(a, b)
+        j = np.maximum(a, b)
+        out = np.stack([i, j, 9 * (sz + 1) + 3 * (sy + 1) + (sx + 1)], axis=1).astype(np.int32)
+        return out
+
+
+_CUDART = None
+
+
+def _cudart():
+    # the CUDA runtime that libmdrt_nb.so loaded (by its soname)
+    global _CUDART
+    if _CUDART is None:
+        L.lib()
+        _CUDART = ctypes.CDLL("libcudart.so.12")
+        _CUDART.cudaMemcpy.restype = ctypes.c_int
+        _CUDART.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    return _CUDART
+
+
+def _sym(v):
+    xx, yy, zz, xy, xz, yz = v
+    return np.array([[xx, xy, xz], [xy, yy, yz], [xz, yz, zz]])

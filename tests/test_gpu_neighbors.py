@@ -1,0 +1,75 @@
+"""The device neighbor build against the oracle's pair sets and MDIR's own
+bit counts (test/Runtime/neighbors-groups-gpu.mlir:508-630): the lists hold
+exactly the oracle's set of (pair, image) bits, bit for bit."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.test_oracle import GROUPS_KAT, lcg_case
+
+pytestmark = pytest.mark.gpu
+
+
+def device_pairs(x, L, R, ex, allow_nan=False):
+    from mdir_b200 import NonbondedTerm
+    n = len(x)
+    t = NonbondedTerm(n)
+    t.set_interaction(cutoff=min(R, 0.49 * L), reach=R, beta=0.0)
+    if ex is not None:
+        t.set_exclusions(rows=ex)
+    xd = torch.tensor(x, dtype=torch.float64, device="cuda")
+    sizes = t.build(xd, [L, L, L], allow_nan=allow_nan)
+    pairs = t.pair_set(sizes)
+    return t, sizes, pairs
+
+
+def canon(p):
+    p = np.asarray(p, dtype=np.int64)
+    return p[np.lexsort((p[:, 2], p[:, 1], p[:, 0]))]
+
+
+@pytest.mark.parametrize("L,R,deg,poison,n,bits", GROUPS_KAT)
+def test_lists_are_the_oracle_set(cuda, L, R, deg, poison, n, bits):
+    x, ex = lcg_case(L, R, deg, poison, n)
+    t, sizes, pairs = device_pairs(x, L, R, ex, allow_nan=poison)
+    assert len(pairs) == bits
+    count, ref = O.pairset(x, [L, L, L], R, ex)
+    assert count == bits
+    np.testing.assert_array_equal(canon(pairs), canon(ref))
+    assert sizes[4] == (1 if poison else 0)
+    t.close()
+
+
+def test_build_is_deterministic(cuda):
+    x, _ = lcg_case(7.0, 1.0, 0, False, 2000)
+    from mdir_b200 import _lib as L
+    t1, s1, p1 = device_pairs(x, 7.0, 1.0, None)
+    e1 = t1.buffer(L.SLOT_ENTRIES, np.int32, 2).copy()
+    o1 = t1.buffer(L.SLOT_ORDER, np.int32).copy()
+    t2, s2, p2 = device_pairs(x, 7.0, 1.0, None)
+    e2 = t2.buffer(L.SLOT_ENTRIES, np.int32, 2)
+    o2 = t2.buffer(L.SLOT_ORDER, np.int32)
+    np.testing.assert_array_equal(o1, o2)
+    G = s1[6]
+    cap = t1.info()["list_capacity"]
+    np.testing.assert_array_equal(e1[: G * cap], e2[: G * cap])
+
+
+def test_capacity_grows_and_retries(cuda):
+    # a reach of 0.975 of the edge needs lists far longer than the first
+    # estimate: the build grows and completes with every bit (D331 growth)
+    x, ex = lcg_case(4.0, 3.9, 0, False, 320)
+    t, sizes, pairs = device_pairs(x, 4.0, 3.9, ex)
+    assert len(pairs) == 198183
+    assert t.info()["list_capacity"] >= sizes[1]
+
+
+def test_reach_beyond_edge_is_refused(cuda):
+    from mdir_b200 import NonbondedTerm, _lib
+    x, _ = lcg_case(4.0, 1.0, 0, False, 320)
+    t = NonbondedTerm(320)
+    t.set_interaction(cutoff=1.0, reach=3.999, beta=0.0)
+    with pytest.raises(_lib.NativeError) as e:
+        t.build(torch.tensor(x, device="cuda"), [4.0, 4.0, 4.0])
+    assert e.value.status == _lib.INVALID_BOX

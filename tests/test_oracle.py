@@ -1,0 +1,113 @@
+"""The oracle against MDIR's own known answers (CPU only)."""
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+# test/Runtime/neighbors-groups-gpu.mlir:508-630: (edge, reach, exclusion
+# degree, poisoned particle 7, particles) -> bits of the lists.
+GROUPS_KAT = [
+    (12.0, 1.5, 0, False, 2000, 16352),
+    (12.0, 1.5, 1, False, 2000, 16337),
+    (12.0, 1.5, 9, False, 2000, 16200),
+    (12.0, 1.5, 0, True, 2000, 16337),
+    (7.0, 1.0, 0, False, 2000, 24389),
+    (5.8, 0.8, 0, False, 2000, 21979),
+    (4.0, 1.9, 0, False, 2000, 896816),
+    (5.8, 3.19, 0, False, 2000, 1392935),
+    (4.0, 2.4, 0, False, 320, 46145),
+    (4.0, 3.0, 0, False, 320, 90433),
+    (4.0, 3.6, 1, False, 320, 154718),
+    (4.0, 3.9, 0, False, 320, 198183),
+]
+
+
+def lcg_case(L, R, deg, poison, n):
+    x = O.lcg_positions(n, L)
+    if poison:
+        x[7, 0] = np.nan
+    ex = O.chain_exclusions(n, deg) if deg else None
+    return x, ex
+
+
+@pytest.mark.parametrize("L,R,deg,poison,n,bits", GROUPS_KAT)
+def test_pairset_matches_groups_kat(L, R, deg, poison, n, bits):
+    x, ex = lcg_case(L, R, deg, poison, n)
+    count, _ = O.pairset(x, [L, L, L], R, ex, want_list=False)
+    assert count == bits
+
+
+def test_pairset_covers_f64_reach():
+    # every image within R in f64 has a bit; the extra bits are within R'
+    L, R, n = 12.0, 1.5, 2000
+    x = O.lcg_positions(n, L)
+    count, pairs = O.pairset(x, [L, L, L], R)
+    xw = x - np.floor(x / L) * L
+    d = xw[pairs[:, 1]] - xw[pairs[:, 0]]
+    code = pairs[:, 2]
+    s = np.stack([code % 3 - 1, (code // 3) % 3 - 1, code // 9 - 1], 1)
+    r = np.linalg.norm(d + s * L, axis=1)
+    assert r.max() <= O.lib().orc_widened_reach(R, np.array([L, L, L]).ctypes.data) + 1e-6
+    assert (r <= R).sum() == 16349  # neighbors-groups-gpu.mlir:37 (in f64)
+
+
+def test_opc_three_waters_pme_kat():
+    fx = json.loads((GOLDEN / "opc_three.json").read_text())
+    x = np.array(fx["positions_nm"])
+    q = np.array(fx["charges_e"])
+    box = np.array(fx["box_nm"])
+    res = np.array(fx["residue"])
+    n = len(q)
+    pairs = [(i, j) for i in range(n) for j in range(i + 1, n) if res[i] == res[j]]
+    beta = fx["beta_per_nm"]
+    exp = fx["expected_kcal"]
+    en, _, _ = O.nonbonded(x, q, np.zeros(n, int), np.full((1, 1), 0.3), np.zeros((1, 1)), box,
+                           fx["cutoff_nm"], beta, O.rows_from_pairs(n, pairs))
+    assert en["coulomb"] / O.KJ_PER_KCAL == pytest.approx(exp["direct"], abs=1e-8)
+    e_ex, _, _ = O.excluded(x, q, pairs, box, beta)
+    assert e_ex / O.KJ_PER_KCAL == pytest.approx(exp["excluded"], abs=1e-7)
+    e_rec, _, _, _ = O.pme(x, q, box, fx["pme_grid"], fx["pme_order"], beta)
+    # pme.test: the reciprocal sum to its six digits with 64 points, order 8
+    assert e_rec / O.KJ_PER_KCAL == pytest.approx(exp["reciprocal"], abs=2e-6)
+    es = O.self_energy(q, beta) + O.background_energy(q, box, beta)
+    assert es / O.KJ_PER_KCAL == pytest.approx(exp["self"], abs=1e-7)
+
+
+def test_pme_matches_ewald_sum_and_forces_are_gradients():
+    rng = np.random.default_rng(0)
+    n, L = 40, 2.0
+    x = rng.uniform(0, L, size=(n, 3))
+    q = rng.normal(size=n)
+    q -= q.mean()
+    box = np.array([L, L, L])
+    beta = 3.0
+    e, f, W, pot = O.pme(x, q, box, [32, 32, 32], 8, beta)
+    assert e == pytest.approx(O.ewald_sum_reciprocal(x, q, box, beta), rel=2e-6)
+    h = 1e-5
+    for i, k in [(0, 0), (3, 1), (7, 2)]:
+        xp, xm = x.copy(), x.copy()
+        xp[i, k] += h
+        xm[i, k] -= h
+        fd = -(O.pme(xp, q, box, [32, 32, 32], 8, beta)[0] - O.pme(xm, q, box, [32, 32, 32], 8, beta)[0]) / (2 * h)
+        assert f[i, k] == pytest.approx(fd, rel=1e-5, abs=1e-6)
+    # dE/dq by differences
+    qp, qm = q.copy(), q.copy()
+    qp[5] += 1e-6
+    qm[5] -= 1e-6
+    fdq = (O.pme(x, qp, box, [32, 32, 32], 8, beta)[0] - O.pme(x, qm, box, [32, 32, 32], 8, beta)[0]) / 2e-6
+    assert pot[5] == pytest.approx(fdq, rel=1e-5)
+
+
+def test_beta_and_grid_of_the_water_box():
+    beta = O.ewald_beta(0.9, 1e-5)
+    assert beta == pytest.approx(3.4705, abs=1e-4)
+    assert math.erfc(beta * 0.9) == pytest.approx(1e-5, rel=1e-9)
+    L = (7850 / 33.4) ** (1 / 3)
+    assert O.pme_grid([L] * 3, 0.1, 4) == [64, 64, 64]
+    assert O.pme_grid([22.008] * 3, 0.1, 4) == [224, 224, 224]
