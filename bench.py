@@ -1,0 +1,321 @@
+"""Throughput of the B200 nonbonded + PME path on the TIP3P water box.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: 7,850 rigid TIP3P waters (23,550 atoms) at 33.4 nm^-3, cutoff
+0.9 nm, reach 1.0 nm, PME order 4 on a 64^3 grid (0.1 nm), SETTLE, NVT at
+300 K (Bussi, 0.1 ps), dt 2 fs, mixed precision: the MD step of the device
+path (neighbor build when the test of validity asks, pair kernel, excluded
+correction, PME with cuFFT, leap-frog + SETTLE + thermostat) as a CUDA
+graph.  One bench step = `--md-steps` MD steps (one replay of the step
+graph); the L2 is flushed between bench steps (a 256 MiB write).  Metric:
+ns/day, the aggregate of N independent replicas (one per GPU: the single
+box does not shard).
+
+The reference arm (--impl reference) times the OpenMP CPU port of MDIR's
+host algorithm for the same workload on the host cores."""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+DT_PS = 0.002
+METRIC = "ns/day water box (TIP3P 23,550 atoms, PME, SETTLE, NVT, 2 fs)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--md-steps", type=int, default=100, help="MD steps per bench step")
+    p.add_argument("--unroll", type=int, default=10, help="MD steps per graph")
+    p.add_argument("--waters", type=int, default=7850)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(args):
+    from mdir_b200 import systems
+    s = systems.tip3p(waters=args.waters)
+    v = systems.maxwell_velocities(s, 300.0, seed=2)
+    return s, v
+
+
+def config(args, s):
+    return {"workload": f"tip3p-{len(s['charges'])}", "atoms": len(s["charges"]),
+            "box_nm": round(float(s["box"][0]), 4), "cutoff_nm": s["cutoff"], "reach_nm": s["reach"],
+            "pme_grid": list(s["grid"]), "pme_order": s["order"], "dt_ps": DT_PS,
+            "md_steps_per_step": args.md_steps, "graph_steps": args.unroll, "ensemble": "NVT Bussi 300 K",
+            "l2": "flushed between timed steps (256 MiB write); each step replays md_steps MD steps",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": reasons}
+
+
+def count_pairs(x, box, rc, excluded_pairs):
+    """Unordered non-excluded pairs with r < r_c (minimum image), counted on
+    the device in chunks: the work units of the pair kernel's roofline."""
+    import torch
+    X = x.to(torch.float64)
+    L = torch.tensor(box, dtype=torch.float64, device=X.device)
+    n = X.shape[0]
+    total = 0
+    chunk = 1024
+    for a in range(0, n, chunk):
+        d = X[a:a + chunk, None, :] - X[None, :, :]
+        d -= L * torch.round(d / L)
+        r2 = (d * d).sum(-1)
+        i = torch.arange(a, min(a + chunk, n), device=X.device)[:, None]
+        j = torch.arange(n, device=X.device)[None, :]
+        total += int(((r2 < rc * rc) & (j > i)).sum())
+    ex = np.asarray(excluded_pairs).reshape(-1, 2)
+    if len(ex):
+        xe = X.cpu().numpy()
+        d = xe[ex[:, 0]] - xe[ex[:, 1]]
+        d -= np.asarray(box) * np.round(d / np.asarray(box))
+        total -= int((np.sum(d * d, 1) < rc * rc).sum())
+    return total
+
+
+def ns_per_day(md_steps, seconds):
+    return md_steps / seconds * DT_PS * 86400.0 / 1000.0
+
+
+def cpu_baseline(s, x, steps=3):
+    from oracle.cpu_port import time_md_steps
+    sec, threads, tb, tf = time_md_steps(s, x, steps)
+    return {"value": round(ns_per_day(1, sec), 4), "unit": "ns/day", "cores": threads, "kind": "port",
+            "sample": f"{steps} force evaluations of the {len(s['charges'])}-atom box after a warm-up "
+                      f"(f32 neighbor matrix, f32 row loop, i64 PME spreading, pocketfft via numpy), one "
+                      f"matrix rebuild every 10 steps amortised: {tf * 1e3:.1f} ms/eval, "
+                      f"{tb * 1e3:.1f} ms/build"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    s, v = workload(args)
+    from oracle.cpu_port import CpuPort
+    cp = CpuPort(s)
+    x = s["positions"].copy()
+    cp.build(x)
+    for _ in range(max(args.warmup, 1)):
+        cp.force(x)
+    times = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        if k % 10 == 0:
+            cp.build(x)
+        cp.force(x)
+        times.append(time.perf_counter() - t0)
+    sec = sum(times) / len(times)
+    value = ns_per_day(1, sec)
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "ns/day",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 pairs / f64 PME", "data": "synthetic",
+           "config": config(args, s),
+           "cpu_baseline": {"value": round(value, 4), "unit": "ns/day", "cores": cp.threads, "kind": "port",
+                            "sample": f"{args.steps} MD-step force evaluations (rebuild every 10) of the "
+                                      f"{len(s['charges'])}-atom box; MDIR's CPU path is MLIR-generated and "
+                                      "cannot be built here, so this is the OpenMP port of its algorithm"},
+           "e2e": {"value": round(value, 4), "unit": "ns/day", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import mdir_b200 as mdir
+    from mdir_b200 import _lib
+    from mdir_b200.md import Integrator
+    from mdir_b200.term import NonbondedTerm, _dp, _hp, _stream
+
+    s, v0 = workload(args)
+    n = len(s["charges"])
+    # ---- device-resident leg -------------------------------------------------
+    term = NonbondedTerm(n, device=local)
+    term.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    term.set_exclusions(pairs=s["excluded_pairs"])
+    term.set_interaction(s["cutoff"], s["reach"], s["beta"])
+    term.set_pme(s["grid"], s["order"])
+    md = Integrator(term, s["masses"], s["waters"])
+    md.thermostat(300.0, 0.1, seed=1 + rank)
+    x = torch.tensor(s["positions"], dtype=torch.float64, device=dev)
+    v = torch.tensor(v0, dtype=torch.float64, device=dev)
+    box = s["box"]
+    md.build(x, box)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        md.run(x, v, box, DT_PS, args.md_steps, unroll=args.unroll)
+    torch.cuda.synchronize(dev)
+    th0 = md.thermo()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        md.run(x, v, box, DT_PS, args.md_steps, unroll=args.unroll)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    th1 = md.thermo()
+    builds = th1["builds"] - th0["builds"]
+    ms_per_step = total_ms / args.steps
+    value = ns_per_day(args.md_steps * args.steps * world, total_ms / 1e3)
+    status = term.status(clear=True)
+    temp = md.temperature()
+
+    # ---- end to end through the public API, host buffers ---------------------
+    system = mdir.System.from_dict(s)
+    st = mdir.InitialState(s["positions"], v0, s["box"])
+    integ, ens, exe, sch = mdir.Integrator(), mdir.Ensemble(), mdir.Execution(), mdir.Schedule()
+    integ.timestep = DT_PS
+    ens.kind, ens.temperature, ens.tau_t = mdir.EnsembleKind.NVT, 300.0, 0.1
+    exe.device, exe.graph_steps = local, args.unroll
+    sim = mdir.Simulation(mdir.compile(system, st, integ, ens, exe, sch))
+    hx = torch.tensor(s["positions"], dtype=torch.float64).pin_memory()
+    hv = torch.tensor(v0, dtype=torch.float64).pin_memory()
+    out_x = torch.empty_like(hx).pin_memory()
+    for _ in range(2):
+        sim.set_state(hx, hv, non_blocking=True)
+        sim.run(args.md_steps)
+    torch.cuda.synchronize(dev)
+    e_steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        sim.set_state(hx, hv, non_blocking=True)
+        sim.run(args.md_steps)
+        out_x.copy_(sim.x, non_blocking=True)
+        torch.cuda.synchronize(dev)
+    e2e_sec = (time.perf_counter() - t0)
+    if world > 1:
+        t = torch.tensor([e2e_sec], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+    e2e = ns_per_day(args.md_steps * e_steps * world, e2e_sec)
+
+    # ---- roofline of the dominant kernel (pair kernel), timed live ------------
+    times = np.zeros(8)
+    _lib.check(_lib.lib().mdrtNbTimeKernels(term._h, _dp(x), _hp(np.asarray(box, dtype=np.float64)), 200,
+                                            _stream(), _hp(times)), "mdrtNbTimeKernels")
+    pairs = count_pairs(x, box, s["cutoff"], s["excluded_pairs"])
+    flop_per_pair = 50
+    props = torch.cuda.get_device_properties(dev)
+    sm_max = clk["sm_max_mhz"] or 1965.0
+    peak_fp32 = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved = pairs * flop_per_pair / (times[1] * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": "nb_pairs", "achieved": round(achieved, 3),
+                "peak": round(peak_fp32, 2), "unit": "TFLOP/s", "frac": round(achieved / peak_fp32, 4),
+                "traffic": None, "pairs_within_cutoff": pairs, "flop_per_pair": flop_per_pair,
+                "launch_ms": round(times[1], 5),
+                "peak_note": "nominal FP32 = SMs x 128 x 2 x max SM clock (no measured FP32 peak exists)",
+                "stage_ms": {"gather": round(times[0], 5), "pairs": round(times[1], 5),
+                             "excluded": round(times[2], 5), "pme": round(times[3], 5),
+                             "finish": round(times[4], 5)}}
+
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "ns/day", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pairs / f64 sums (mixed)", "data": "synthetic (seeded TIP3P box, random orientations)",
+            "config": config(args, s), "clocks": clk,
+            "e2e": {"value": round(e2e, 2), "unit": "ns/day", "h2d_bytes_per_step": 2 * n * 3 * 8,
+                    "d2h_bytes_per_step": n * 3 * 8 + 4},
+            "roofline": roofline,
+            # kernels per MD step: gather, pairs, excluded, spread, convolve,
+            # pme gather, finish, update, thermostat, check (+ 2 memsets);
+            # 14 per build
+            "gpu_launches": int(args.steps * args.md_steps * 10 + builds * 14),
+            "builds": int(builds), "temperature_K": round(temp, 1), "status": status}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(s, s["positions"])
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

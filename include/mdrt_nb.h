@@ -182,6 +182,45 @@ int32_t mdrtNbGroupsInfo(mdrtNb *ctx, int64_t *list_capacity, int64_t *builds, i
  * clear != 0 resets it. */
 int32_t mdrtNbStatus(mdrtNb *ctx, void *stream, int32_t clear, int32_t *status);
 
+/* Average device time (ms, CUDA events on `stream`) of `iterations`
+ * launches of each stage of the force term at device positions x, after a
+ * valid build: out[0] frame gather, out[1] pair kernel, out[2] excluded
+ * correction, out[3] PME (spread, FFTs, convolution, gather), out[4] force
+ * finish.  For the roofline of each kernel; the forces it leaves are not
+ * meaningful.  MDIR: MDRT_WAIT=1 per-kernel timing (runtime/mdrt_cuda.c:600). */
+int32_t mdrtNbTimeKernels(mdrtNb *ctx, const double *x, const double box[3], int32_t iterations,
+                          void *stream, double *out);
+
+/* ---- The MD step (leap-frog, SETTLE, Bussi thermostat) ------------------
+ * MDIR: the compiled step loop that Simulation::run calls
+ * (lib/Compiler/Simulation.cpp:421, 1679) and its replayed step graph
+ * (runtime/mdrt_step_graph.cu), here for the nonbonded + PME system alone. */
+typedef struct mdrtMd mdrtMd;
+
+/* An integrator over the term `nb`: masses (host f64 [n], amu), and
+ * `nwaters` rigid three-site waters (host int32 [nwaters][3]: O, H, H) held
+ * by SETTLE at O-H d_oh and H-H d_hh (nm); the other atoms move freely. */
+int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwaters,
+                     const int32_t *waters, double d_oh, double d_hh);
+int32_t mdrtMdDestroy(mdrtMd *md);
+/* Bussi (CSVR) thermostat at `temperature` K with time constant tau (ps);
+ * tau <= 0 leaves the energy constant (NVE).  `seed` fixes the noise. */
+int32_t mdrtMdSetThermostat(mdrtMd *md, double temperature, double tau, uint64_t seed);
+/* A neighbor build at device positions x that also resets the reference
+ * positions of the test of validity (D80). */
+int32_t mdrtMdBuild(mdrtMd *md, const double *x, const double box[3], void *stream);
+/* `steps` leap-frog steps of dt (ps) on the device state x, v (f64 [n, 3]);
+ * the lists are rebuilt on the device whenever 2 max|x - x_build| > R - r_c.
+ * unroll > 0 replays a CUDA graph of `unroll` steps whose rebuilds are
+ * conditional nodes (no host wait); unroll = 0 runs step by step. */
+int32_t mdrtMdRun(mdrtMd *md, double *x, double *v, const double box[3], double dt, int64_t steps,
+                  int32_t unroll, void *stream);
+/* out[6]: thermostat scaling, kinetic energy of the last two half steps,
+ * steps taken, builds made, degrees of freedom; waits for `stream`. */
+int32_t mdrtMdThermo(mdrtMd *md, void *stream, double *out);
+/* The device array of the forces of the last step (f64 [n, 3]). */
+int32_t mdrtMdForces(mdrtMd *md, double **forces);
+
 /* 3D real FFTs of a grid in f32 on `stream`, plans cached per size.
  * MDIR: _mlir_ciface_mdrtCudaFFTForward3DF32 / Backward3DF32
  * (runtime/mdrt_cuda.c:2942-2979), with plain pointers.  The backward

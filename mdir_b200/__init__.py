@@ -2,7 +2,11 @@
 (vv137/mdir) interface for that path.
 
 The kernels live in libmdrt_nb.so (C ABI: include/mdrt_nb.h); this package
-holds the host-side mirror of MDIR's Python interface for the path."""
+holds the host-side mirror of MDIR's Python interface for the path:
+`compile`, `Simulation`, `FrameEvaluator` and `mdir_b200.torch`."""
 
-from .term import COULOMB, NonbondedTerm, exclusion_rows  # noqa: F401
 from . import systems  # noqa: F401
+from .api import (CompileError, Electrostatics, Ensemble, EnsembleKind, Execution, InitialState,  # noqa: F401
+                  InputError, Integrator, Precision, Program, Schedule, Simulation, SimulationError,
+                  System, Target, Truncation, UnsupportedError, compile)
+from .term import COULOMB, NonbondedTerm, exclusion_rows  # noqa: F401

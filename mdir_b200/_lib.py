@@ -41,6 +41,14 @@ SIGNATURES = {
     "mdrtNbGroupsBuffer": (_i32, [_p, _i32, ctypes.POINTER(_p), ctypes.POINTER(_i64)]),
     "mdrtNbGroupsInfo": (_i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "mdrtNbStatus": (_i32, [_p, _p, _i32, ctypes.POINTER(_i32)]),
+    "mdrtNbTimeKernels": (_i32, [_p, _p, _p, _i32, _p, _p]),
+    "mdrtMdCreate": (_i32, [ctypes.POINTER(_p), _p, _p, _i64, _p, _d, _d]),
+    "mdrtMdDestroy": (_i32, [_p]),
+    "mdrtMdSetThermostat": (_i32, [_p, _d, _d, ctypes.c_uint64]),
+    "mdrtMdBuild": (_i32, [_p, _p, _p, _p]),
+    "mdrtMdRun": (_i32, [_p, _p, _p, _p, _d, _i64, _i32, _p]),
+    "mdrtMdThermo": (_i32, [_p, _p, _p]),
+    "mdrtMdForces": (_i32, [_p, ctypes.POINTER(_p)]),
     "mdrtCudaFFTForward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
     "mdrtCudaFFTBackward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
 }

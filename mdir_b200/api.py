@@ -1,0 +1,328 @@
+"""MDIR's Python interface for the nonbonded + PME path, over the device
+library: `compile(system, state, integrator, ensemble, execution, schedule)`
+returns a `Program`, `Simulation(program)` runs it, and
+`FrameEvaluator(program).evaluate(frames)` gives energies and gradients of
+stored frames.
+
+Names, argument meaning and errors follow MDIR (python/Bindings.cpp:951
+compile, 1625 Simulation, 2230 run; python/mdir/_frames.py:458, 715;
+docs/python-compile.md): snake-case properties on plain objects, typed
+enums, InputError / UnsupportedError / CompileError / SimulationError.  The
+supported subset is the one this library implements: orthorhombic cells,
+Lennard-Jones from a type table (optionally with the r^2 switch), Ewald
+direct + PME or no electrostatics, rigid three-site waters, NVE or NVT
+(Bussi), mixed precision with an optional deterministic mode.  Units: nm,
+ps, kJ/mol, e, K."""
+
+import enum
+import math
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .md import Integrator as _Integrator
+from .term import COULOMB, NonbondedTerm, _dp, _hp
+
+
+class InputError(ValueError):
+    """Invalid inputs (MDIR: mdir.InputError)."""
+
+
+class UnsupportedError(RuntimeError):
+    """A request outside the supported subset (MDIR: mdir.UnsupportedError)."""
+
+
+class CompileError(RuntimeError):
+    """A program that cannot be set up (MDIR: mdir.CompileError)."""
+
+
+class SimulationError(RuntimeError):
+    """A run that stopped (MDIR: mdir.SimulationError, from stopWith)."""
+
+
+class Target(enum.Enum):
+    CPU = "CPU"
+    GPU = "GPU"
+
+
+class Precision(enum.Enum):
+    MIXED = "MIXED"
+    DOUBLE = "DOUBLE"
+
+
+class EnsembleKind(enum.Enum):
+    NVE = "NVE"
+    NVT = "NVT"
+
+
+class Electrostatics(enum.Enum):
+    NONE = "NONE"
+    PME = "PME"
+
+
+class Truncation(enum.Enum):
+    NONE = "NONE"
+    SWITCH = "SWITCH"  # the cubic switch of the potential in r^2 from switch_distance
+
+
+class System:
+    """The model: topology tables and the nonbonded settings.
+
+    `from_dict` takes a dict of mdir_b200.systems (charges, types, sigma,
+    epsilon tables, excluded_pairs, masses, waters, box)."""
+
+    def __init__(self, charges, types, sigma, epsilon, masses, excluded_pairs=(), waters=None):
+        self.charges = np.asarray(charges, dtype=np.float64)
+        self.types = np.asarray(types, dtype=np.int32)
+        self.sigma = np.asarray(sigma, dtype=np.float64)
+        self.epsilon = np.asarray(epsilon, dtype=np.float64)
+        self.masses = np.asarray(masses, dtype=np.float64)
+        self.excluded_pairs = np.asarray(excluded_pairs, dtype=np.int64).reshape(-1, 2)
+        self.water_residues = None if waters is None else np.asarray(waters, dtype=np.int32).reshape(-1, 3)
+        self.periodic = True
+        self.cutoff = 1.0
+        self.pairlist_distance = 1.1
+        self.switch_distance = 0.0
+        self.truncation = Truncation.NONE
+        self.electrostatics = Electrostatics.PME
+        self.dispersion = False
+        self.pme_alpha = 0.0  # beta in nm^-1; 0: from pme_tolerance
+        self.pme_tolerance = 1e-5
+        self.pme_spacing = 0.1
+        self.pme_grid = (0, 0, 0)
+        self.pme_order = 4
+        self.rigid_water = waters is not None
+
+    @property
+    def particle_count(self):
+        return len(self.charges)
+
+    @classmethod
+    def from_dict(cls, d):
+        s = cls(d["charges"], d["types"], d["sigma"], d["epsilon"], d["masses"], d["excluded_pairs"],
+                d.get("waters"))
+        s.cutoff = d["cutoff"]
+        s.pairlist_distance = d["reach"]
+        s.electrostatics = Electrostatics.PME if d["pme"] else Electrostatics.NONE
+        s.dispersion = bool(d.get("dispersion", False))
+        if d["pme"]:
+            s.pme_alpha = d["beta"]
+            s.pme_grid = tuple(d["grid"])
+            s.pme_order = d["order"]
+        if d.get("lj_switch"):
+            s.truncation = Truncation.SWITCH
+            s.switch_distance = d["switch"]
+        return s
+
+
+class InitialState:
+    def __init__(self, positions, velocities=None, cell=None):
+        self.positions = np.asarray(positions, dtype=np.float64)
+        self.velocities = (np.zeros((0, 3)) if velocities is None else np.asarray(velocities, dtype=np.float64))
+        self.cell = None if cell is None else np.asarray(cell, dtype=np.float64)
+
+
+class Integrator:
+    def __init__(self):
+        self.method = "LEAP_FROG"
+        self.timestep = 0.002
+
+
+class Ensemble:
+    def __init__(self):
+        self.kind = EnsembleKind.NVE
+        self.temperature = 300.0
+        self.thermostat = "BUSSI"
+        self.tau_t = 0.1
+        self.seed = 1
+
+
+class Execution:
+    def __init__(self):
+        self.target = Target.GPU
+        self.precision = Precision.MIXED
+        self.device = 0
+        self.deterministic = False
+        self.step_graph = True
+        self.graph_steps = 10
+
+
+class Schedule:
+    def __init__(self):
+        self.steps = 0
+        self.energy_period = 0
+
+
+def _beta(rc, tol):
+    low, high = 0.0, 1.0
+    while math.erfc(high * rc) > tol:
+        high *= 2.0
+    for _ in range(100):
+        mid = 0.5 * (low + high)
+        if math.erfc(mid * rc) > tol:
+            low = mid
+        else:
+            high = mid
+    return 0.5 * (low + high)
+
+
+def _smooth(least):
+    size = max(int(least), 2)
+    while True:
+        if size % 2 == 0:
+            rest = size
+            for f in (2, 3, 5, 7):
+                while rest % f == 0:
+                    rest //= f
+            if rest == 1:
+                return size
+        size += 1
+
+
+class Program:
+    """A validated, immutable plan (MDIR: mdir.Program with `plan`)."""
+
+    def __init__(self, system, state, integrator, ensemble, execution, schedule, plan):
+        self.system, self.state, self.integrator = system, state, integrator
+        self.ensemble, self.execution, self.schedule = ensemble, execution, schedule
+        self.plan = dict(plan)
+
+
+def compile(system, state, integrator, ensemble, execution, schedule):
+    """Validates the inputs and fixes the plan of the run (MDIR
+    python/Bindings.cpp:951): beta by bisection of erfc(beta r_c) = tol, the
+    PME grid as the smallest even 2,3,5,7-smooth size per edge
+    (lib/Driver/TermNonbonded.cpp:755-838, 1104-1130)."""
+    n = system.particle_count
+    x = state.positions
+    if x.shape != (n, 3):
+        raise InputError(f"positions: expected shape ({n}, 3); found {x.shape}")
+    if not np.all(np.isfinite(x)):
+        raise InputError("positions: not finite")
+    if state.velocities.shape not in ((0, 3), (n, 3)):
+        raise InputError(f"velocities: expected shape ({n}, 3) or (0, 3)")
+    if state.cell is None or np.shape(state.cell) != (3,):
+        raise UnsupportedError("an orthorhombic cell of three edges is required (triclinic cells are not supported)")
+    box = np.asarray(state.cell, dtype=np.float64)
+    if execution.target != Target.GPU:
+        raise UnsupportedError("this library runs the GPU target only")
+    if execution.precision != Precision.MIXED:
+        raise UnsupportedError("precision: MIXED (f32 pairs, f64 sums; deterministic=True for fixed point)")
+    if system.sigma.shape != system.epsilon.shape or system.sigma.ndim != 2:
+        raise InputError("sigma and epsilon are type x type tables")
+    if system.types.min(initial=0) < 0 or system.types.max(initial=0) >= system.sigma.shape[0]:
+        raise InputError("a type out of the range of the tables")
+    rc, R = float(system.cutoff), float(system.pairlist_distance)
+    if not (0 < rc <= R):
+        raise InputError("cutoff must be positive and at most pairlist_distance")
+    if R >= 0.999 * box.min() or 2 * rc > box.min():
+        raise InputError("pairlist_distance must be below 0.999 of the least edge and the cutoff at most half of it")
+    if np.any(np.abs(system.charges) >= 100.0):
+        raise InputError("particle mesh Ewald holds charges of less than 100 e")
+    plan = {"particles": n, "cutoff": rc, "reach": R, "box": box.tolist(), "device": execution.device}
+    if system.electrostatics == Electrostatics.PME:
+        beta = system.pme_alpha or _beta(rc, system.pme_tolerance)
+        grid = [int(g) if g else _smooth(math.ceil(L / system.pme_spacing - 1e-9)) for g, L in
+                zip(system.pme_grid, box)]
+        grid = [max(g, 2 * system.pme_order) for g in grid]
+        if system.pme_order not in (4, 5, 6, 8):
+            raise UnsupportedError("pme_order: 4, 5, 6 or 8")
+        plan.update({"beta": beta, "pme_grid": grid, "pme_order": system.pme_order})
+    else:
+        plan.update({"beta": 0.0, "pme_grid": None})
+    if ensemble.kind not in (EnsembleKind.NVE, EnsembleKind.NVT):
+        raise UnsupportedError("ensembles: NVE and NVT")
+    if not integrator.timestep > 0:
+        raise InputError("timestep must be positive")
+    plan["waters"] = 0 if system.water_residues is None else len(system.water_residues)
+    return Program(system, state, integrator, ensemble, execution, schedule, plan)
+
+
+class State:
+    def __init__(self, positions, velocities, step):
+        self.positions, self.velocities, self.step = positions, velocities, step
+
+
+def _make_term(program):
+    s, p = program.system, program.plan
+    t = NonbondedTerm(s.particle_count, device=program.execution.device)
+    t.set_particles(s.charges, s.types, s.sigma, s.epsilon)
+    t.set_exclusions(pairs=s.excluded_pairs)
+    t.set_interaction(p["cutoff"], p["reach"], p["beta"], coulomb=COULOMB,
+                      lj_switch=s.truncation == Truncation.SWITCH, switch_distance=s.switch_distance)
+    if p["pme_grid"]:
+        t.set_pme(p["pme_grid"], p["pme_order"])
+    t.set_deterministic(program.execution.deterministic)
+    return t
+
+
+class Simulation:
+    """A persistent run of a program on its device (MDIR:
+    python/Bindings.cpp:1625 and lib/Compiler/Simulation.cpp:1679)."""
+
+    def __init__(self, program):
+        self.program = program
+        s, p = program.system, program.plan
+        self.device = torch.device("cuda", program.execution.device)
+        self.term = _make_term(program)
+        self.box = np.asarray(p["box"])
+        self.md = _Integrator(self.term, s.masses, s.water_residues if s.rigid_water else None)
+        e = program.ensemble
+        self.md.thermostat(e.temperature, e.tau_t if e.kind == EnsembleKind.NVT else 0.0, e.seed)
+        st = program.state
+        self.x = torch.tensor(st.positions, dtype=torch.float64, device=self.device)
+        v = st.velocities if len(st.velocities) else np.zeros_like(st.positions)
+        self.v = torch.tensor(v, dtype=torch.float64, device=self.device)
+        self.step = 0
+        self._build()
+
+    def _build(self):
+        try:
+            self.md.build(self.x, self.box)
+        except L.NativeError as e:
+            if e.status == L.NAN_POSITION:
+                raise SimulationError("positions that are not numbers or are far outside the cell") from e
+            raise
+
+    def set_state(self, positions, velocities=None, non_blocking=False):
+        """New positions (and velocities) from host or device arrays; the
+        lists are rebuilt at the next run."""
+        self.x.copy_(torch.as_tensor(positions), non_blocking=non_blocking)
+        if velocities is not None:
+            self.v.copy_(torch.as_tensor(velocities), non_blocking=non_blocking)
+        self._stale = True
+
+    def run(self, steps):
+        if steps < 0:
+            raise InputError("steps must be nonnegative")
+        if getattr(self, "_stale", False):
+            self._build()
+            self._stale = False
+        ex = self.program.execution
+        unroll = ex.graph_steps if ex.step_graph else 0
+        self.md.run(self.x, self.v, self.box, self.program.integrator.timestep, steps, unroll=unroll)
+        self.step += steps
+        status = self.term.status(clear=True)
+        if status & 1:
+            raise SimulationError("the lists overflowed their room during the run; rebuild with more room")
+        if status & 4:
+            raise SimulationError("positions that are not numbers or are far outside the cell")
+
+    def state(self):
+        return State(self.x.cpu().numpy(), self.v.cpu().numpy(), self.step)
+
+    def energies(self):
+        """The potential energy terms (kJ/mol) and the kinetic energy at the
+        current positions."""
+        f = self.term.force(self.x, self.box, energy=True)
+        e = self.term.energies()
+        c = self.term.constants(self.box, dispersion=self.program.system.dispersion)
+        terms = {"lj": e["lj"], "coulomb": e["coulomb"], "excluded": e["excluded"],
+                 "reciprocal": e["reciprocal"], "self": c["self"], "background": c["background"],
+                 "dispersion": c["dispersion"]}
+        terms["potential"] = sum(terms.values())
+        t = self.md.thermo()
+        terms["kinetic"] = t["kinetic"]
+        del f
+        return terms

@@ -10,10 +10,6 @@
 #include "../../include/mdrt_nb.h"
 #include "nb_context.h"
 
-struct mdrtNb {
-  NbCtx c;
-};
-
 namespace {
 
 int cuda_status(cudaError_t e, const char *what) {
@@ -426,6 +422,40 @@ extern "C" int32_t mdrtPmePotential(mdrtNb *ctx, double *potential, void *stream
   CK(cudaMemsetAsync(potential, 0, sizeof(double) * c.n, st));
   int blocks = (int)std::max<int64_t>(1, (c.places_cap + 255) / 256);
   nb_potential_out<<<blocks, 256, 0, st>>>(c.places_cap, c.sizes, c.order, c.pme.potential, potential);
+  CK(cudaGetLastError());
+  return MDRT_NB_OK;
+}
+
+extern "C" int32_t mdrtNbTimeKernels(mdrtNb *ctx, const double *x, const double box[3], int32_t iterations,
+                                     void *stream, double *out) {
+  if (!ctx || !x || !box || !out || iterations < 1) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (!c.built) return MDRT_NB_NOT_BUILT;
+  cudaStream_t st = (cudaStream_t)stream;
+  double *scratch = nullptr;
+  CK(cudaMalloc(&scratch, sizeof(double) * 3 * c.n));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto timed = [&](auto &&launch) {
+    launch();  // warm
+    cudaEventRecord(e0, st);
+    for (int k = 0; k < iterations; ++k) launch();
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return (double)ms / iterations;
+  };
+  out[0] = timed([&] { nb_gather_frames(c, x, box, st); });
+  out[1] = timed([&] { nb_pairs_run(c, box, false, st); });
+  out[2] = timed([&] { nb_excluded_run(c, box, false, st); });
+  out[3] = (c.pme.on && c.beta > 0) ? timed([&] { nb_pme_run(c, box, false, false, st); }) : 0.0;
+  out[4] = timed([&] { nb_finish_forces(c, scratch, 0, st); });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(st);
+  cudaFree(scratch);
   CK(cudaGetLastError());
   return MDRT_NB_OK;
 }

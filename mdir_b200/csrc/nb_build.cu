@@ -572,6 +572,10 @@ static void nb_build_launch(NbCtx &c, const double *x, const double box[3], cuda
                                                                 c.sizes);
 }
 
+void nb_build_launch_public(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
+  nb_build_launch(c, x, box, s);
+}
+
 // One complete build with count-then-grow: the list capacity C grows to a
 // quarter more than the longest list and the build runs again until every
 // list fits (MDIR: mdrtGroupsGrow, runtime/mdrt_cuda.c:3185, and the build

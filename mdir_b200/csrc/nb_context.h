@@ -102,8 +102,16 @@ enum NbEnergySlot {
   NB_E_SLOTS = 16
 };
 
+// The opaque handle of the C ABI.
+struct mdrtNb {
+  NbCtx c;
+};
+
 // Launchers implemented in the .cu files.
 int nb_build_run(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
+// One build's launches with the current capacities, no host wait (a graph
+// body); overflow is left in c.sizes.
+void nb_build_launch_public(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
 void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
 void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);

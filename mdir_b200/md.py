@@ -1,0 +1,71 @@
+"""The MD step over the C ABI: leap-frog with SETTLE for rigid waters and the
+Bussi thermostat, replayed as a CUDA graph whose list rebuilds are decided
+on the device (mdrtMd* of include/mdrt_nb.h)."""
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .term import NonbondedTerm, _dp, _host, _hp, _stream
+
+KB = 0.0083144626181532  # kJ/mol/K
+
+
+class Integrator:
+    """Leap-frog MD of one system on the device: `x` and `v` are device f64
+    tensors (n, 3) that the integrator updates in place."""
+
+    def __init__(self, term: NonbondedTerm, masses, waters=None, d_oh=0.09572, d_hh=None):
+        self.term = term
+        m = _host(masses, np.float64)
+        w = np.zeros((0, 3), dtype=np.int32) if waters is None else _host(waters, np.int32).reshape(-1, 3)
+        if d_hh is None:
+            d_hh = 2.0 * d_oh * np.sin(np.radians(104.52) / 2.0)
+        h = ctypes.c_void_p()
+        L.check(L.lib().mdrtMdCreate(ctypes.byref(h), term._h, _hp(m), len(w), _hp(w) if len(w) else None,
+                                     d_oh, d_hh), "mdrtMdCreate")
+        self._h = h
+        self.masses = m
+        self.nwaters = len(w)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().mdrtMdDestroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def thermostat(self, temperature, tau, seed=1):
+        L.check(L.lib().mdrtMdSetThermostat(self._h, temperature, tau, seed), "mdrtMdSetThermostat")
+
+    def build(self, x, box, stream=None):
+        b = _host(box, np.float64)
+        self.term.box = b
+        L.check(L.lib().mdrtMdBuild(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtMdBuild")
+
+    def run(self, x, v, box, dt, steps, unroll=10, stream=None):
+        b = _host(box, np.float64)
+        L.check(L.lib().mdrtMdRun(self._h, _dp(x), _dp(v), _hp(b), dt, int(steps), int(unroll), _stream(stream)),
+                "mdrtMdRun")
+
+    def thermo(self, stream=None):
+        out = np.zeros(8)
+        L.check(L.lib().mdrtMdThermo(self._h, _stream(stream), _hp(out)), "mdrtMdThermo")
+        return {"lambda": out[0], "kinetic_half": out[1], "kinetic_half_before": out[2],
+                "steps": int(out[3]), "builds": int(out[4]), "ndof": int(out[5]),
+                "kinetic": 0.5 * (out[1] + out[2])}
+
+    def forces(self):
+        p = ctypes.c_void_p()
+        L.check(L.lib().mdrtMdForces(self._h, ctypes.byref(p)), "mdrtMdForces")
+        return p.value
+
+    def temperature(self, stream=None):
+        t = self.thermo(stream)
+        return 2.0 * t["kinetic"] / (t["ndof"] * KB)

@@ -32,7 +32,7 @@ _lib = None
 
 
 def build():
-    """Compiles liboracle.so and cpu_port.so beside this file."""
+    """Compiles liboracle.so and libcpu_port.so beside this file."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
 
 

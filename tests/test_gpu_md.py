@@ -1,0 +1,96 @@
+"""The MD step on the device: SETTLE, the CUDA-graph replay with
+conditional rebuilds, energy conservation and the thermostat."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from mdir_b200 import NonbondedTerm, systems
+from mdir_b200.md import Integrator
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(s, deterministic=False, tau=0.0, seed=1):
+    n = len(s["charges"])
+    t = NonbondedTerm(n)
+    t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t.set_exclusions(pairs=s["excluded_pairs"])
+    t.set_interaction(s["cutoff"], s["reach"], s["beta"])
+    t.set_pme(s["grid"], s["order"])
+    t.set_deterministic(deterministic)
+    md = Integrator(t, s["masses"], s["waters"])
+    md.thermostat(300.0, tau, seed)
+    x = torch.tensor(s["positions"], dtype=torch.float64, device="cuda")
+    v = torch.tensor(systems.maxwell_velocities(s, 300.0, seed=2), device="cuda")
+    md.build(x, s["box"])
+    return t, md, x, v
+
+
+def water_geometry(x, waters):
+    x = x.cpu().numpy()
+    o, h1, h2 = x[waters[:, 0]], x[waters[:, 1]], x[waters[:, 2]]
+    return (np.linalg.norm(h1 - o, axis=1), np.linalg.norm(h2 - o, axis=1), np.linalg.norm(h2 - h1, axis=1))
+
+
+def test_settle_keeps_waters_rigid(cuda):
+    s = systems.tip3p(waters=600, seed=21)
+    t, md, x, v = setup(s)
+    md.run(x, v, s["box"], 0.002, 50, unroll=10)
+    d1, d2, d3 = water_geometry(x, s["waters"])
+    dhh = 2 * 0.09572 * np.sin(np.radians(104.52) / 2)
+    assert np.abs(d1 - 0.09572).max() < 1e-9
+    assert np.abs(d2 - 0.09572).max() < 1e-9
+    assert np.abs(d3 - dhh).max() < 1e-9
+
+
+def test_graph_replay_equals_step_by_step_bitwise(cuda):
+    s = systems.tip3p(waters=500, seed=22)
+    t1, md1, x1, v1 = setup(s, deterministic=True, tau=0.1)
+    md1.run(x1, v1, s["box"], 0.002, 60, unroll=10)
+    t2, md2, x2, v2 = setup(s, deterministic=True, tau=0.1)
+    md2.run(x2, v2, s["box"], 0.002, 60, unroll=0)
+    assert md1.thermo()["builds"] == md2.thermo()["builds"]
+    assert torch.equal(x1, x2) and torch.equal(v1, v2)
+
+
+def test_lists_stay_valid_across_device_rebuilds(cuda):
+    s = systems.tip3p(waters=700, seed=23)
+    t, md, x, v = setup(s, tau=0.1)
+    md.run(x, v, s["box"], 0.002, 400, unroll=20)
+    th = md.thermo()
+    assert th["builds"] >= 2  # the test of validity asked for rebuilds on the device
+    assert t.status() == 0
+    f = t.force(x, energy=True).cpu().numpy()
+    ref = O.evaluate(s, x.cpu().numpy())
+    err = np.sqrt(np.mean(np.sum((f - ref["forces"]) ** 2, 1)) / np.mean(np.sum(ref["forces"] ** 2, 1)))
+    assert err < 1e-5
+
+
+def test_nve_energy_is_conserved(cuda):
+    s = systems.tip3p(waters=600, seed=24)
+    t, md, x, v = setup(s, tau=0.0)
+    md.run(x, v, s["box"], 0.001, 300, unroll=10)  # relax the lattice start
+
+    def total():
+        t.force(x, energy=True)
+        e = t.energies()
+        c = t.constants()
+        pot = e["lj"] + e["coulomb"] + e["excluded"] + e["reciprocal"] + c["self"] + c["background"]
+        return pot + md.thermo()["kinetic"], md.thermo()["kinetic"]
+
+    e0, k0 = total()
+    md.run(x, v, s["box"], 0.001, 500, unroll=10)
+    e1, k1 = total()
+    assert abs(e1 - e0) < 2e-3 * k0, (e0, e1, k0)
+
+
+def test_thermostat_holds_the_temperature(cuda):
+    s = systems.tip3p(waters=500, seed=25)
+    t, md, x, v = setup(s, tau=0.05)
+    md.run(x, v, s["box"], 0.002, 1500, unroll=10)
+    temps = []
+    for _ in range(10):
+        md.run(x, v, s["box"], 0.002, 50, unroll=10)
+        temps.append(md.temperature())
+    assert abs(np.mean(temps) - 300.0) < 15.0, temps
