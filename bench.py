@@ -43,6 +43,9 @@ def parse():
     p.add_argument("--md-steps", type=int, default=100, help="MD steps per bench step")
     p.add_argument("--unroll", type=int, default=10, help="MD steps per graph")
     p.add_argument("--waters", type=int, default=7850)
+    p.add_argument("--reach", type=float, default=1.2, help="reach of the outer lists (nm)")
+    p.add_argument("--pruned", type=float, default=1.0, help="reach of the pruned inner lists (nm); 0: one list")
+    p.add_argument("--equilibrate", type=int, default=5000, help="untimed MD steps before warm-up")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
@@ -50,6 +53,8 @@ def parse():
 def workload(args):
     from mdir_b200 import systems
     s = systems.tip3p(waters=args.waters)
+    s["reach"] = args.reach
+    s["pruned"] = args.pruned
     v = systems.maxwell_velocities(s, 300.0, seed=2)
     return s, v
 
@@ -57,6 +62,7 @@ def workload(args):
 def config(args, s):
     return {"workload": f"tip3p-{len(s['charges'])}", "atoms": len(s["charges"]),
             "box_nm": round(float(s["box"][0]), 4), "cutoff_nm": s["cutoff"], "reach_nm": s["reach"],
+            "pruned_reach_nm": s["pruned"],
             "pme_grid": list(s["grid"]), "pme_order": s["order"], "dt_ps": DT_PS,
             "md_steps_per_step": args.md_steps, "graph_steps": args.unroll, "ensemble": "NVT Bussi 300 K",
             "l2": "flushed between timed steps (256 MiB write); each step replays md_steps MD steps",
@@ -206,6 +212,7 @@ def main():
     term.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
     term.set_exclusions(pairs=s["excluded_pairs"])
     term.set_interaction(s["cutoff"], s["reach"], s["beta"])
+    term.set_pruned_reach(s["pruned"])
     term.set_pme(s["grid"], s["order"])
     md = Integrator(term, s["masses"], s["waters"])
     md.thermostat(300.0, 0.1, seed=1 + rank)
@@ -215,6 +222,11 @@ def main():
     md.build(x, box)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # untimed equilibration: the lattice start relaxes and heats; a strong
+    # thermostat brings it to 300 K before the timed steps
+    md.thermostat(300.0, 0.02, seed=7 + rank)
+    md.run(x, v, box, DT_PS, args.equilibrate, unroll=args.unroll)
+    md.thermostat(300.0, 0.1, seed=1 + rank)
     for _ in range(args.warmup):
         md.run(x, v, box, DT_PS, args.md_steps, unroll=args.unroll)
     torch.cuda.synchronize(dev)
@@ -243,6 +255,7 @@ def main():
         total_ms = float(t.item())
     th1 = md.thermo()
     builds = th1["builds"] - th0["builds"]
+    prunes = th1["prunes"] - th0["prunes"]
     ms_per_step = total_ms / args.steps
     value = ns_per_day(args.md_steps * args.steps * world, total_ms / 1e3)
     status = term.status(clear=True)
@@ -250,6 +263,7 @@ def main():
 
     # ---- end to end through the public API, host buffers ---------------------
     system = mdir.System.from_dict(s)
+    system.pruned_distance = s["pruned"]
     st = mdir.InitialState(s["positions"], v0, s["box"])
     integ, ens, exe, sch = mdir.Integrator(), mdir.Ensemble(), mdir.Execution(), mdir.Schedule()
     integ.timestep = DT_PS
@@ -304,11 +318,11 @@ def main():
             "e2e": {"value": round(e2e, 2), "unit": "ns/day", "h2d_bytes_per_step": 2 * n * 3 * 8,
                     "d2h_bytes_per_step": n * 3 * 8 + 4},
             "roofline": roofline,
-            # kernels per MD step: gather, pairs, excluded, spread, convolve,
-            # pme gather, finish, update, thermostat, check (+ 2 memsets);
-            # 14 per build
-            "gpu_launches": int(args.steps * args.md_steps * 10 + builds * 14),
-            "builds": int(builds), "temperature_K": round(temp, 1), "status": status}
+            # this library's kernels per MD step: noise, spread, convolve, PME
+            # gather, pairs, update (cuFFT's own kernels not counted); 16 per
+            # build (with the frames and the references) and 5 per pruning
+            "gpu_launches": int(args.steps * args.md_steps * 6 + builds * 16 + prunes * 5),
+            "builds": int(builds), "prunes": int(prunes), "temperature_K": round(temp, 1), "status": status}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(s, s["positions"])
     if rank == 0:

@@ -118,6 +118,18 @@ int32_t mdrtNbSetExclusions(mdrtNb *ctx, const int32_t *offsets, const int32_t *
 int32_t mdrtNbSetInteraction(mdrtNb *ctx, double cutoff, double reach, double beta, double coulomb,
                              int32_t coulomb_shift, int32_t lj_switch, double switch_distance);
 
+/* The dual list: the lists built at the reach R are pruned to
+ * pruned_distance (r_c <= it < R; 0 or R: one list), and the force term
+ * reads the pruned ones.  MDIR: `pruned_distance` of [energy] (D114,
+ * docs/neighbor-groups.md, Section 6.2). */
+int32_t mdrtNbSetPrunedReach(mdrtNb *ctx, double pruned_distance);
+
+/* Prunes the lists at device positions x (after a build whose lists are
+ * valid for x): inner mask = outer mask and r <= pruned_distance, entries
+ * with no bit left dropped.  MDIR: emitGroupsPrune,
+ * lib/Conversion/MDExecToGPU/MDExecToGPU.cpp:9588. */
+int32_t mdrtNbPrune(mdrtNb *ctx, const double *x, const double box[3], void *stream);
+
 /* Deterministic mode: 64-bit fixed-point force accumulation (2^32 per
  * kJ/mol/nm) and PME spreading (2^40 per e); bitwise reproducible.
  * MDIR: deterministic = true (D70, D84; docs/pme.md, Section 3). */
@@ -215,8 +227,9 @@ int32_t mdrtMdBuild(mdrtMd *md, const double *x, const double box[3], void *stre
  * conditional nodes (no host wait); unroll = 0 runs step by step. */
 int32_t mdrtMdRun(mdrtMd *md, double *x, double *v, const double box[3], double dt, int64_t steps,
                   int32_t unroll, void *stream);
-/* out[6]: thermostat scaling, kinetic energy of the last two half steps,
- * steps taken, builds made, degrees of freedom; waits for `stream`. */
+/* out[7]: thermostat scaling, kinetic energy of the last two half steps,
+ * steps taken, builds made, degrees of freedom, prunings made; waits for
+ * `stream`. */
 int32_t mdrtMdThermo(mdrtMd *md, void *stream, double *out);
 /* The device array of the forces of the last step (f64 [n, 3]). */
 int32_t mdrtMdForces(mdrtMd *md, double **forces);

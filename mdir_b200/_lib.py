@@ -32,6 +32,8 @@ SIGNATURES = {
     "mdrtNbSetExclusions": (_i32, [_p, _p, _p]),
     "mdrtNbSetInteraction": (_i32, [_p, _d, _d, _d, _d, _i32, _i32, _d]),
     "mdrtNbSetDeterministic": (_i32, [_p, _i32]),
+    "mdrtNbSetPrunedReach": (_i32, [_p, _d]),
+    "mdrtNbPrune": (_i32, [_p, _p, _p, _p]),
     "mdrtPmeSetup": (_i32, [_p, _i32, _i32, _i32, _i32]),
     "mdrtNbBuild": (_i32, [_p, _p, _i64, _p, _d, _p, _p]),
     "mdrtNbForce": (_i32, [_p, _p, _p, _u32, _p, _p]),

@@ -83,6 +83,7 @@ class System:
         self.periodic = True
         self.cutoff = 1.0
         self.pairlist_distance = 1.1
+        self.pruned_distance = 0.0  # the dual list's inner reach (D114); 0: one list
         self.switch_distance = 0.0
         self.truncation = Truncation.NONE
         self.electrostatics = Electrostatics.PME
@@ -220,7 +221,11 @@ def compile(system, state, integrator, ensemble, execution, schedule):
         raise InputError("pairlist_distance must be below 0.999 of the least edge and the cutoff at most half of it")
     if np.any(np.abs(system.charges) >= 100.0):
         raise InputError("particle mesh Ewald holds charges of less than 100 e")
-    plan = {"particles": n, "cutoff": rc, "reach": R, "box": box.tolist(), "device": execution.device}
+    Rin = float(system.pruned_distance or 0.0)
+    if Rin and not (rc <= Rin <= R):
+        raise InputError("pruned_distance must lie between the cutoff and pairlist_distance")
+    plan = {"particles": n, "cutoff": rc, "reach": R, "pruned_reach": Rin, "box": box.tolist(),
+            "device": execution.device}
     if system.electrostatics == Electrostatics.PME:
         beta = system.pme_alpha or _beta(rc, system.pme_tolerance)
         grid = [int(g) if g else _smooth(math.ceil(L / system.pme_spacing - 1e-9)) for g, L in
@@ -254,6 +259,8 @@ def _make_term(program):
     if p["pme_grid"]:
         t.set_pme(p["pme_grid"], p["pme_order"])
     t.set_deterministic(program.execution.deterministic)
+    if p["pruned_reach"]:
+        t.set_pruned_reach(p["pruned_reach"])
     return t
 
 

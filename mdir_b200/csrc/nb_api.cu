@@ -111,6 +111,8 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   nb_free(c.atom_xw); nb_free(c.atom_shift);
   nb_free(c.xq); nb_free(c.typ_p); nb_free(c.acc); nb_free(c.acc_fixed);
   nb_free(c.unit_partials); nb_free(c.energy);
+  nb_free(c.slab_in); nb_free(c.counts_in); nb_free(c.unit_n_in); nb_free(c.unit_start_in);
+  nb_free(c.units_in); nb_free(c.sizes_in);
   if (c.h_sizes) cudaFreeHost(c.h_sizes);
   if (c.h_energy) cudaFreeHost(c.h_energy);
   delete ctx;
@@ -196,6 +198,37 @@ int32_t mdrtNbSetInteraction(mdrtNb *ctx, double cutoff, double reach, double be
   c.coulomb_shift = coulomb_shift;
   c.lj_switch = lj_switch;
   c.switch_distance = switch_distance;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbSetPrunedReach(mdrtNb *ctx, double pruned_distance) {
+  if (!ctx || !(pruned_distance == 0.0 || (pruned_distance >= ctx->c.cutoff && pruned_distance <= ctx->c.reach)))
+    return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (pruned_distance >= c.reach) pruned_distance = 0.0;  // no tighter than the outer list: one list
+  c.inner_reach = pruned_distance;
+  c.inner_valid = false;
+  if (c.inner_reach > 0.0 && c.built) {
+    int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap;
+    if (key != c.inner_key || !c.slab_in) {
+      if (nb_reserve_inner(c)) return MDRT_NB_CUDA_ERROR;
+      c.inner_key = key;
+    }
+  }
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbPrune(mdrtNb *ctx, const double *x, const double box[3], void *stream) {
+  if (!ctx || !x || !box) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (!c.built) return MDRT_NB_NOT_BUILT;
+  if (c.inner_reach <= 0.0) return MDRT_NB_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  nb_gather_frames(c, x, box, st);
+  nb_prune_run(c, box, st);
+  c.inner_valid = true;
+  c.prunes++;
+  CK(cudaGetLastError());
   return MDRT_NB_OK;
 }
 

@@ -420,6 +420,57 @@ __global__ void nb_count_entries(int64_t groups_cap, const int32_t *sizes,
   atomicAdd(&out[NB_SIZE_ENTRIES], counts[g]);
 }
 
+// The pruning of the dual list (MDIR: emitGroupsPrune,
+// lib/Conversion/MDExecToGPU/MDExecToGPU.cpp:9588; docs/neighbor-groups.md,
+// Section 6.2): inner mask = outer mask and [r^2 <= R_in'^2] at the current
+// frames, entries whose inner mask is empty dropped, the rest written in
+// their order (a warp per group, ballot compaction), so that the inner list
+// of a group is a deterministic function of the outer one and the frames.
+__global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_t *__restrict__ sizes,
+                                                float Lx, float Ly, float Lz, float rin2, int64_t list_cap,
+                                                const int2 *__restrict__ slab, const int32_t *__restrict__ counts,
+                                                const int32_t *__restrict__ order, const float4 *__restrict__ xq,
+                                                int2 *__restrict__ slab_in, int32_t *__restrict__ counts_in) {
+  __shared__ float4 s_m[4][NB_GROUP];
+  const unsigned FULL = 0xffffffffu;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int64_t g = (int64_t)blockIdx.x * 4 + warp;
+  if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
+  if (lane < NB_GROUP) s_m[warp][lane] = xq[g * NB_GROUP + lane];
+  unsigned live = __ballot_sync(FULL, lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0) & 0xffffu;
+  __syncwarp();
+  int cnt = (int)min((int64_t)counts[g], list_cap);
+  int out = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    int e = base + lane;
+    unsigned inner = 0;
+    int2 en = make_int2(0, 0);
+    if (e < cnt) {
+      en = slab[g * list_cap + e];
+      unsigned mm = (unsigned)en.y & live & 0xffffu;
+      int sx, sy, sz;
+      nb_decode_image(((unsigned)en.y >> 16) & 31, sx, sy, sz);
+      float4 xj = xq[en.x];
+      float jx = xj.x + (float)sx * Lx, jy = xj.y + (float)sy * Ly, jz = xj.z + (float)sz * Lz;
+      while (mm) {
+        int m = __ffs(mm) - 1;
+        mm &= mm - 1;
+        float4 xm = s_m[warp][m];
+        float dx = xm.x - jx, dy = xm.y - jy, dz = xm.z - jz;
+        float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= rin2) inner |= 1u << m;
+      }
+    }
+    unsigned has = __ballot_sync(FULL, inner != 0);
+    if (inner) {
+      int at = out + __popc(has & ((1u << lane) - 1));
+      slab_in[g * list_cap + at] = make_int2(en.x, (int)(inner | ((unsigned)en.y & 0xffff0000u)));
+    }
+    out += __popc(has);
+  }
+  if (lane == 0) counts_in[g] = out;
+}
+
 inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
 
 }  // namespace
@@ -576,6 +627,32 @@ void nb_build_launch_public(NbCtx &c, const double *x, const double box[3], cuda
   nb_build_launch(c, x, box, s);
 }
 
+int nb_reserve_inner(NbCtx &c) {
+  // the inner buffers follow the outer capacities
+  int64_t G = c.groups_cap, C = c.list_cap, U = c.units_cap;
+  if (nb_realloc(c.slab_in, G * C) || nb_realloc(c.counts_in, G) || nb_realloc(c.unit_n_in, G) ||
+      nb_realloc(c.unit_start_in, G + 1) || nb_realloc(c.units_in, U))
+    return -1;
+  if (!c.sizes_in) {
+    if (cudaMalloc(&c.sizes_in, sizeof(int32_t) * NB_SIZE_COUNT) != cudaSuccess) return -1;
+  }
+  cudaMemset(c.sizes_in, 0, sizeof(int32_t) * NB_SIZE_COUNT);
+  c.inner_valid = false;
+  return 0;
+}
+
+void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s) {
+  double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2]);
+  nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
+                                                      (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+                                                      c.counts, c.order, c.xq, c.slab_in, c.counts_in);
+  nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts_in, c.list_cap,
+                                                             c.unit_n_in);
+  nb_scan(c.unit_n_in, c.unit_start_in, (int)c.groups_cap, nullptr, c.scan_scratch, s);
+  nb_unit_write<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.unit_n_in, c.unit_start_in,
+                                                             c.units_cap, c.units_in, c.sizes_in);
+}
+
 // One complete build with count-then-grow: the list capacity C grows to a
 // quarter more than the longest list and the build runs again until every
 // list fits (MDIR: mdrtGroupsGrow, runtime/mdrt_cuda.c:3185, and the build
@@ -601,6 +678,14 @@ int nb_build_run(NbCtx &c, const double *x, const double box[3], cudaStream_t s)
       c.built = true;
       c.builds++;
       for (int k = 0; k < 3; ++k) c.box_built[k] = box[k];
+      c.inner_valid = false;
+      if (c.inner_reach > 0.0) {
+        int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap;
+        if (key != c.inner_key || !c.slab_in) {
+          if (nb_reserve_inner(c)) return -1;
+          c.inner_key = key;
+        }
+      }
       return 0;
     }
     int64_t longest = c.h_sizes[NB_SIZE_LONGEST];

@@ -89,6 +89,20 @@ struct NbCtx {
   NbPme pme;
   bool built = false;
   int64_t builds = 0, grows = 0;
+  // the inner list of the dual list (MDIR D114): the outer lists pruned to
+  // `inner_reach` at the positions of the last pruning; same layout, same
+  // capacity per group.  inner_reach = 0: one list.
+  double inner_reach = 0.0;
+  bool inner_valid = false;
+  int64_t inner_key = -1;  // the outer capacities the inner buffers were sized for
+  int2 *slab_in = nullptr;
+  int32_t *counts_in = nullptr;
+  int32_t *unit_n_in = nullptr, *unit_start_in = nullptr;
+  int2 *units_in = nullptr;
+  int32_t *sizes_in = nullptr;  // NB_SIZE_UNITS of the inner list (device)
+  int64_t prunes = 0;
+  // tuning (mdrtNbSetTuning): blocks of 8 warps per SM of the pair kernel
+  int pair_blocks_per_sm = 3;
 };
 
 // Energy / virial slots of ctx->energy (f64, device).
@@ -112,9 +126,17 @@ int nb_build_run(NbCtx &c, const double *x, const double box[3], cudaStream_t s)
 // One build's launches with the current capacities, no host wait (a graph
 // body); overflow is left in c.sizes.
 void nb_build_launch_public(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
+// The pruning of the outer lists into the inner ones at the current frames
+// xq (gathered by the caller), and the inner units; no host wait.
+void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s);
+// Allocates the inner lists to the outer capacities (host, between launches).
+int nb_reserve_inner(NbCtx &c);
 void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
 void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
+// The correction over a given list of pairs (i < j), forces only.
+void nb_excluded_list_run(NbCtx &c, const double box[3], const int32_t *pairs, int64_t npairs,
+                          cudaStream_t s);
 void nb_finish_forces(NbCtx &c, double *forces, int accumulate, cudaStream_t s);
 void nb_reduce_energy(NbCtx &c, bool pairs, bool excluded, cudaStream_t s);
 int nb_pme_setup(NbCtx &c, int k0, int k1, int k2, int order);

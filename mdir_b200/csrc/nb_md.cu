@@ -9,6 +9,17 @@
 // water rigid by M-SHAKE below double precision (D112); SETTLE
 // (Miyamoto & Kollman, J. Comput. Chem. 13 (1992) 952) is the analytic
 // solution of the same constraints for a rigid three-site water.
+//
+// One step (B200 design):
+//   fork:  PME (spread, R2C, convolve, C2R, gather) on a high-priority side
+//          stream  ||  pair kernel (+ excluded pairs outside waters)
+//   join:  md_update, a thread per water: reads the place accumulators of its
+//          three atoms (pairs + PME), adds the three intra-water excluded
+//          Ewald corrections in f64, integrates, applies SETTLE, writes x, v,
+//          the f32 frames of the next step and clears the accumulators
+//          md_thermostat: kinetic energy (fixed-order f64), Bussi scaling, and
+//          the test of validity that sets the conditional rebuild
+//   if rebuild: the neighbor build, the frames, the reference positions
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -24,16 +35,23 @@ struct mdrtMd {
   double *mass = nullptr;          // device f64 [n]
   int32_t *waters = nullptr;       // device [nw][3] (O, H1, H2)
   int32_t *free_atoms = nullptr;   // device [nfree]
+  int32_t *excl_other = nullptr;   // excluded pairs not inside one water (i < j)
+  int64_t n_excl_other = 0;
+  bool water_excl = false;         // the three pairs of each water are excluded
   double dOH = 0.09572, dHH = 0.15139, mO = 15.9994, mH = 1.008;
-  double *force = nullptr;         // device f64 [n, 3]
+  double *force = nullptr;         // device f64 [n, 3]: the forces of the last step
   double *x_ref = nullptr;         // positions at the last build
+  double *x_prune = nullptr;       // positions at the last pruning (dual list)
   double *ke_part = nullptr;       // per-block kinetic partials
   int ke_blocks = 0;
-  unsigned int *maxd2 = nullptr;   // float bits of max |x - x_ref|^2
-  double *thermo = nullptr;        // [0] lambda, [1] KE of the last half step, [2] KE before, [3] steps, [4] builds
+  unsigned int *maxd2 = nullptr;   // [0] float bits of max |x - x_ref|^2, [1] of max |x - x_prune|^2, [2] blocks done
+  double *thermo = nullptr;        // [0] lambda, [1] KE, [2] KE before, [3] steps, [4] builds, [5] prunes, [6..7] noise
+  int *flag = nullptr;             // [0] rebuild, [1] prune: flags for the step-by-step path
   double temperature = 300.0, tau = 0.0;
   int64_t ndof = 0;
   unsigned long long seed = 1;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // graph
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -50,7 +68,6 @@ namespace {
 struct Vec3 {
   double x, y, z;
 };
-__device__ __forceinline__ Vec3 v3(double x, double y, double z) { return {x, y, z}; }
 __device__ __forceinline__ Vec3 operator-(Vec3 a, Vec3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 __device__ __forceinline__ Vec3 operator+(Vec3 a, Vec3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 __device__ __forceinline__ Vec3 operator*(double s, Vec3 a) { return {s * a.x, s * a.y, s * a.z}; }
@@ -70,17 +87,16 @@ struct SettleParams {
   double mO, mH, ra, rb, rc;  // canonical triangle: O at ra from the centre of mass, H pair at rb, half HH rc
 };
 
-// SETTLE: the constrained positions a3, b3, c3 of one water from its
-// constrained old positions a0, b0, c0 and unconstrained new a1, b1, c1.
+// SETTLE: the constrained positions of one water from its constrained old
+// positions a0, b0, c0 and unconstrained new a1, b1, c1 (overwritten).
 __device__ void settle(const SettleParams &P, Vec3 a0, Vec3 b0, Vec3 c0, Vec3 &a1, Vec3 &b1, Vec3 &c1) {
   double M = P.mO + 2.0 * P.mH;
   Vec3 d = (1.0 / M) * (P.mO * a1 + P.mH * b1 + P.mH * c1);  // centre of mass of the new positions
   Vec3 A1 = a1 - d, B1 = b1 - d, C1 = c1 - d;
   Vec3 B0 = b0 - a0, C0 = c0 - a0;
-  Vec3 ez = unit(cross(B0, C0));      // normal of the old plane
-  Vec3 ex = unit(cross(A1, ez));      // perpendicular to it and to the new O
+  Vec3 ez = unit(cross(B0, C0));  // normal of the old plane
+  Vec3 ex = unit(cross(A1, ez));  // perpendicular to it and to the new O
   Vec3 ey = cross(ez, ex);
-  // the old and new sites in the frame (ex, ey, ez)
   double xb0 = dot(B0, ex), yb0 = dot(B0, ey);
   double xc0 = dot(C0, ex), yc0 = dot(C0, ey);
   double za1 = dot(A1, ez);
@@ -112,28 +128,114 @@ __device__ __forceinline__ void atomic_max_float(unsigned int *addr, float v) {
   atomicMax(addr, __float_as_uint(fmaxf(v, 0.f)));  // non-negative floats order as integers
 }
 
-// One leap-frog step with SETTLE: v += lambda-scaled, f/m dt; x += v dt;
-// constrain; v = (x_new - x_old)/dt.  A thread per water, then per free atom.
-__global__ void md_update(int64_t nwaters, int64_t nfree, const int32_t *__restrict__ waters,
-                          const int32_t *__restrict__ free_atoms, SettleParams S,
-                          const double *__restrict__ inv_mass, const double *__restrict__ mass,
-                          const double *__restrict__ f, double *__restrict__ x, double *__restrict__ v,
-                          const double *__restrict__ x_ref, const double *__restrict__ thermo, double dt,
-                          double *__restrict__ ke_part, unsigned int *__restrict__ maxd2) {
-  __shared__ double s_ke[8];
-  __shared__ float s_d2[8];
+struct UpdateParams {
+  SettleParams S;
+  double dt;
+  double L[3];
+  double beta, coulomb, two_beta_sqrtpi;
+  int water_excl;
+  int fixed;
+  // thermostat and the tests of validity, done by the last block
+  double tau, temperature, ndof;
+  double build_half2, prune_half2;  // ((R - r_c)/2)^2 and ((R_in - r_c)/2)^2 (0: no dual list)
+  cudaGraphConditionalHandle h_build, h_prune;
+  int use_graph;
+  int *flag;
+};
+
+// The force on atom a: the pair / excluded accumulator of its place and the
+// PME force; clears the accumulator for the next step.
+__device__ __forceinline__ Vec3 take_force(int a, const int32_t *__restrict__ place_of, float4 *acc,
+                                           unsigned long long *accf, const float4 *__restrict__ pme, int fixed) {
+  int p = place_of[a];
+  if (p < 0) return {0.0, 0.0, 0.0};
+  Vec3 f;
+  if (fixed) {
+    long long x = (long long)accf[3 * p], y = (long long)accf[3 * p + 1], z = (long long)accf[3 * p + 2];
+    accf[3 * p] = 0ull;
+    accf[3 * p + 1] = 0ull;
+    accf[3 * p + 2] = 0ull;
+    f = {(double)x * NB_FORCE_SCALE_INV, (double)y * NB_FORCE_SCALE_INV, (double)z * NB_FORCE_SCALE_INV};
+  } else {
+    float4 v = acc[p];
+    acc[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    f = {v.x, v.y, v.z};
+  }
+  if (pme) {
+    float4 w = pme[p];
+    f.x += w.x;
+    f.y += w.y;
+    f.z += w.z;
+  }
+  return f;
+}
+
+// The excluded Ewald correction -f q_i q_j erf(beta r)/r of one pair in f64;
+// adds its force to fi and subtracts it from fj.
+__device__ __forceinline__ void excl_pair(const UpdateParams &U, Vec3 xi, Vec3 xj, double qq, Vec3 &fi, Vec3 &fj) {
+  Vec3 d = xi - xj;
+  d.x -= U.L[0] * rint(d.x / U.L[0]);
+  d.y -= U.L[1] * rint(d.y / U.L[1]);
+  d.z -= U.L[2] * rint(d.z / U.L[2]);
+  double r2 = dot(d, d);
+  if (qq == 0.0 || r2 <= 0.0) return;
+  double r = sqrt(r2);
+  double fs = qq * (U.two_beta_sqrtpi * exp(-U.beta * U.beta * r2) / r2 - erf(U.beta * r) / (r2 * r));
+  fi = fi + fs * d;
+  fj = fj - fs * d;
+}
+
+__device__ __forceinline__ void write_frame(int a, Vec3 x, const int32_t *__restrict__ place_of,
+                                            const char4 *__restrict__ shift, const double *L, float4 *xq) {
+  int p = place_of[a];
+  if (p < 0) return;
+  char4 s = shift[p];
+  float4 o = xq[p];
+  xq[p] = make_float4((float)(x.x + s.x * L[0]), (float)(x.y + s.y * L[1]), (float)(x.z + s.z * L[2]), o.w);
+}
+
+#define MD_UPDATE_THREADS 64
+
+__device__ void md_last_block(const UpdateParams &U, const double *ke_part, int nblocks, double *thermo,
+                              unsigned int *maxd2);
+
+// One leap-frog step with SETTLE: v = lambda v + f/m dt; x += v dt;
+// constrain; v = (x_new - x_old)/dt.  A thread per water, then per free
+// atom, in small blocks so that the f64 work spreads over the SMs.  The
+// last block to finish sums the kinetic energy in a fixed order and runs
+// the thermostat and the tests of validity (md_last_block).
+__global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
+    int64_t nwaters, int64_t nfree, const int32_t *__restrict__ waters, const int32_t *__restrict__ free_atoms,
+    UpdateParams U, const double *__restrict__ inv_mass, const double *__restrict__ mass,
+    const float *__restrict__ charge, const int32_t *__restrict__ place_of, const char4 *__restrict__ shift,
+    float4 *acc, unsigned long long *accf, const float4 *__restrict__ pme, float4 *xq, double *__restrict__ x,
+    double *__restrict__ v, double *__restrict__ fout, const double *__restrict__ x_ref,
+    const double *__restrict__ x_prune, double *thermo, double *ke_part, unsigned int *maxd2) {
+  __shared__ double s_ke[MD_UPDATE_THREADS / 32];
+  __shared__ float s_d2[MD_UPDATE_THREADS / 32], s_p2[MD_UPDATE_THREADS / 32];
+  __shared__ int s_last;
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double lambda = thermo[0];
+  double dt = U.dt;
   double ke = 0.0;
-  float d2max = 0.f;
+  float d2max = 0.f, p2max = 0.f;
   if (t < nwaters) {
     int ia = waters[3 * t], ib = waters[3 * t + 1], ic = waters[3 * t + 2];
     Vec3 a0 = load3(x, ia), b0 = load3(x, ib), c0 = load3(x, ic);
-    Vec3 va = lambda * load3(v, ia) + (dt * inv_mass[ia]) * load3(f, ia);
-    Vec3 vb = lambda * load3(v, ib) + (dt * inv_mass[ib]) * load3(f, ib);
-    Vec3 vc = lambda * load3(v, ic) + (dt * inv_mass[ic]) * load3(f, ic);
+    Vec3 fa = take_force(ia, place_of, acc, accf, pme, U.fixed);
+    Vec3 fb = take_force(ib, place_of, acc, accf, pme, U.fixed);
+    Vec3 fc = take_force(ic, place_of, acc, accf, pme, U.fixed);
+    if (U.water_excl) {
+      double qa = charge[ia], qb = charge[ib], qc = charge[ic];
+      excl_pair(U, a0, b0, U.coulomb * qa * qb, fa, fb);
+      excl_pair(U, a0, c0, U.coulomb * qa * qc, fa, fc);
+      excl_pair(U, b0, c0, U.coulomb * qb * qc, fb, fc);
+    }
+    Vec3 va = lambda * load3(v, ia) + (dt * inv_mass[ia]) * fa;
+    Vec3 vb = lambda * load3(v, ib) + (dt * inv_mass[ib]) * fb;
+    Vec3 vc = lambda * load3(v, ic) + (dt * inv_mass[ic]) * fc;
     Vec3 a1 = a0 + dt * va, b1 = b0 + dt * vb, c1 = c0 + dt * vc;
-    settle(S, a0, b0, c0, a1, b1, c1);
+    settle(U.S, a0, b0, c0, a1, b1, c1);
     double inv_dt = 1.0 / dt;
     va = inv_dt * (a1 - a0);
     vb = inv_dt * (b1 - b0);
@@ -144,40 +246,68 @@ __global__ void md_update(int64_t nwaters, int64_t nfree, const int32_t *__restr
     store3(v, ia, va);
     store3(v, ib, vb);
     store3(v, ic, vc);
+    store3(fout, ia, fa);
+    store3(fout, ib, fb);
+    store3(fout, ic, fc);
+    write_frame(ia, a1, place_of, shift, U.L, xq);
+    write_frame(ib, b1, place_of, shift, U.L, xq);
+    write_frame(ic, c1, place_of, shift, U.L, xq);
     ke = 0.5 * (mass[ia] * dot(va, va) + mass[ib] * dot(vb, vb) + mass[ic] * dot(vc, vc));
     Vec3 da = a1 - load3(x_ref, ia), db = b1 - load3(x_ref, ib), dc = c1 - load3(x_ref, ic);
     d2max = (float)fmax(dot(da, da), fmax(dot(db, db), dot(dc, dc)));
+    if (U.prune_half2 > 0.0) {
+      da = a1 - load3(x_prune, ia);
+      db = b1 - load3(x_prune, ib);
+      dc = c1 - load3(x_prune, ic);
+      p2max = (float)fmax(dot(da, da), fmax(dot(db, db), dot(dc, dc)));
+    }
   } else if (t < nwaters + nfree) {
     int i = free_atoms[t - nwaters];
-    Vec3 vi = lambda * load3(v, i) + (dt * inv_mass[i]) * load3(f, i);
+    Vec3 fi = take_force(i, place_of, acc, accf, pme, U.fixed);
+    Vec3 vi = lambda * load3(v, i) + (dt * inv_mass[i]) * fi;
     Vec3 xi = load3(x, i) + dt * vi;
     store3(x, i, xi);
     store3(v, i, vi);
+    store3(fout, i, fi);
+    write_frame(i, xi, place_of, shift, U.L, xq);
     ke = 0.5 * mass[i] * dot(vi, vi);
     Vec3 di = xi - load3(x_ref, i);
     d2max = (float)dot(di, di);
+    if (U.prune_half2 > 0.0) {
+      di = xi - load3(x_prune, i);
+      p2max = (float)dot(di, di);
+    }
   }
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     ke += __shfl_xor_sync(0xffffffffu, ke, o);
     d2max = fmaxf(d2max, __shfl_xor_sync(0xffffffffu, d2max, o));
+    p2max = fmaxf(p2max, __shfl_xor_sync(0xffffffffu, p2max, o));
   }
   if (lane == 0) {
     s_ke[warp] = ke;
     s_d2[warp] = d2max;
+    s_p2[warp] = p2max;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0.0;
-    float m = 0.f;
+    float m = 0.f, mp = 0.f;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
       s += s_ke[w];
       m = fmaxf(m, s_d2[w]);
+      mp = fmaxf(mp, s_p2[w]);
     }
     ke_part[blockIdx.x] = s;
     atomic_max_float(maxd2, m);
+    atomic_max_float(maxd2 + 1, mp);
+    __threadfence();
+    unsigned done = atomicAdd(maxd2 + 2, 1u);
+    s_last = done == gridDim.x - 1;
   }
+  __syncthreads();
+  if (s_last) md_last_block(U, ke_part, gridDim.x, thermo, maxd2);
 }
 
 // splitmix64 (Steele, Lea & Flood 2014) as a counter-based generator.
@@ -193,7 +323,7 @@ __device__ __forceinline__ double uniform01(unsigned long long &ctr, unsigned lo
 }
 __device__ __forceinline__ double normal01(unsigned long long &ctr, unsigned long long seed) {
   double u1 = uniform01(ctr, seed), u2 = uniform01(ctr, seed);
-  return sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2);
+  return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
 }
 // Gamma(a, 1), a >= 1, by Marsaglia & Tsang (ACM TOMS 26 (2000) 363); the
 // loop is bounded and falls back to the mean.
@@ -211,15 +341,27 @@ __device__ double gamma_draw(double a, unsigned long long &ctr, unsigned long lo
   return a;
 }
 
-// The kinetic energy of the half step (fixed-order sum) and the Bussi
-// (CSVR; Bussi, Donadio & Parrinello, J. Chem. Phys. 126 (2007) 014101)
-// scaling for the next update.  thermo: [0] lambda, [1] KE, [2] KE before,
-// [3] steps, [4] builds.
-__global__ void md_thermostat(const double *__restrict__ ke_part, int nblocks, double *thermo, double dt,
-                              double tau, double temperature, double ndof, unsigned long long seed) {
-  __shared__ double s[256];
+// The noise of the Bussi thermostat for the coming update: a normal R1 and
+// the sum of ndof - 1 squared normals (2 Gamma((ndof - 1)/2)), from the step
+// counter; off the critical path, on the side stream beside the pair kernel.
+__global__ void md_noise(double *thermo, double ndof, unsigned long long seed) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long ctr = (unsigned long long)thermo[3] * 1024ull;
+  thermo[6] = normal01(ctr, seed);
+  thermo[7] = ndof > 1.0 ? 2.0 * gamma_draw(0.5 * (ndof - 1.0), ctr, seed) : 0.0;
+}
+
+// The last block of md_update: the kinetic energy of the half step
+// (fixed-order f64 sum), the Bussi (CSVR; Bussi, Donadio & Parrinello,
+// J. Chem. Phys. 126 (2007) 014101) scaling for the next update, and the
+// tests of validity (D80 and D114, the cell unchanged):
+// rebuild when 2 max|x - x_build| > R - r_c, prune when rebuilt or
+// 2 max|x - x_prune| > R_in - r_c; they set the conditional nodes.
+__device__ void md_last_block(const UpdateParams &U, const double *ke_part, int nblocks, double *thermo,
+                              unsigned int *maxd2) {
+  __shared__ double s[MD_UPDATE_THREADS];
   double v = 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += ke_part[b];
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += __ldcg(ke_part + b);
   s[threadIdx.x] = v;
   __syncthreads();
   for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
@@ -230,43 +372,52 @@ __global__ void md_thermostat(const double *__restrict__ ke_part, int nblocks, d
   double K = s[0];
   thermo[2] = thermo[1];
   thermo[1] = K;
-  double step = thermo[3];
-  thermo[3] = step + 1.0;
+  thermo[3] += 1.0;
   double lambda = 1.0;
-  if (tau > 0.0 && K > 0.0 && ndof > 1.0) {
+  if (U.tau > 0.0 && K > 0.0 && U.ndof > 1.0) {
     const double kB = 0.0083144626181532;
-    double Kt = 0.5 * ndof * kB * temperature;
-    double c = exp(-dt / tau);
-    unsigned long long ctr = (unsigned long long)step * 1024ull;
-    double r1 = normal01(ctr, seed);
-    double sum = 2.0 * gamma_draw(0.5 * (ndof - 1.0), ctr, seed);
-    double Knew = K + (1.0 - c) * (Kt * (r1 * r1 + sum) / ndof - K) + 2.0 * r1 * sqrt(c * (1.0 - c) * K * Kt / ndof);
+    double Kt = 0.5 * U.ndof * kB * U.temperature;
+    double c = exp(-U.dt / U.tau);
+    double r1 = thermo[6], sum = thermo[7];
+    double Knew = K + (1.0 - c) * (Kt * (r1 * r1 + sum) / U.ndof - K) + 2.0 * r1 * sqrt(c * (1.0 - c) * K * Kt / U.ndof);
     lambda = sqrt(fmax(Knew, 0.0) / K);
   }
   thermo[0] = lambda;
-}
-
-// Sets the conditional of the rebuild: 2 max|x - x_ref| > R - r_c (D80, in
-// a cell that does not change).
-__global__ void md_check(unsigned int *maxd2, double half_skin2, cudaGraphConditionalHandle h, int use_graph,
-                         int *flag) {
-  float d2 = __uint_as_float(*maxd2);
-  int rebuild = (double)d2 > half_skin2 ? 1 : 0;
-  if (flag) *flag = rebuild;
-  if (use_graph) cudaGraphSetConditional(h, rebuild);
+  float d2 = __uint_as_float(atomicAdd(maxd2, 0u));
+  float p2 = __uint_as_float(atomicAdd(maxd2 + 1, 0u));
+  int rebuild = (double)d2 > U.build_half2 ? 1 : 0;
+  int prune = (U.prune_half2 > 0.0 && (rebuild || (double)p2 > U.prune_half2)) ? 1 : 0;
+  maxd2[0] = 0u;
+  maxd2[1] = 0u;
+  maxd2[2] = 0u;
+  if (U.flag) {
+    U.flag[0] = rebuild;
+    U.flag[1] = prune;
+  }
+  if (U.use_graph) {
+    cudaGraphSetConditional(U.h_build, rebuild);
+    if (U.prune_half2 > 0.0) cudaGraphSetConditional(U.h_prune, prune);
+  }
 }
 
 // After a build: the reference positions and the counters.
 __global__ void md_after_build(int64_t n3, const double *__restrict__ x, double *__restrict__ x_ref,
-                               unsigned int *maxd2, double *thermo, const int32_t *sizes, int *status) {
+                               double *thermo, const int32_t *sizes, int *status) {
   int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n3) x_ref[k] = x[k];
   if (k == 0) {
-    *maxd2 = 0u;
     thermo[4] += 1.0;
     if (sizes[NB_SIZE_OVERFLOW] != 0) atomicOr(status, NB_STATUS_LIST_OVERFLOW);
     if (sizes[NB_SIZE_NAN] != 0) atomicOr(status, NB_STATUS_NAN);
   }
+}
+
+// After a pruning: the reference positions of the inner list.
+__global__ void md_after_prune(int64_t n3, const double *__restrict__ x, double *__restrict__ x_prune,
+                               double *thermo) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n3) x_prune[k] = x[k];
+  if (k == 0) thermo[5] += 1.0;
 }
 
 inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
@@ -284,41 +435,77 @@ static SettleParams settle_params(const mdrtMd &m) {
   return S;
 }
 
-// One step on `s`: forces at x, update, thermostat, the test of validity;
-// with a graph the rebuild is a conditional node added by the caller.
+// One step on `s` from the frames xq of the current positions x.
 static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], double dt, cudaStream_t s,
-                         cudaGraphConditionalHandle h, int use_graph, int *flag) {
+                         cudaGraphConditionalHandle h_build, cudaGraphConditionalHandle h_prune, int use_graph,
+                         int *flag) {
   NbCtx &c = *m.nb;
-  nb_gather_frames(c, x, box, s);
+  bool pme = c.pme.on && c.beta > 0.0;
+  cudaEventRecord(m.ev_fork, s);
+  cudaStreamWaitEvent(m.side, m.ev_fork, 0);
+  md_noise<<<1, 32, 0, m.side>>>(m.thermo, (double)m.ndof, m.seed);
+  if (pme) nb_pme_run(c, box, false, false, m.side);
   nb_pairs_run(c, box, false, s);
-  nb_excluded_run(c, box, false, s);
-  if (c.pme.on && c.beta > 0.0) nb_pme_run(c, box, false, false, s);
-  nb_finish_forces(c, m.force, 0, s);
-  int64_t units = m.nwaters + m.nfree;
-  cudaMemsetAsync(m.maxd2, 0, sizeof(unsigned int), s);
-  md_update<<<m.ke_blocks, 256, 0, s>>>(m.nwaters, m.nfree, m.waters, m.free_atoms, settle_params(m),
-                                       m.inv_mass, m.mass, m.force, x, v, m.x_ref, m.thermo, dt, m.ke_part,
-                                       m.maxd2);
-  (void)units;
-  md_thermostat<<<1, 256, 0, s>>>(m.ke_part, m.ke_blocks, m.thermo, dt, m.tau, m.temperature, (double)m.ndof,
-                                  m.seed);
+  if (m.n_excl_other > 0) nb_excluded_list_run(c, box, m.excl_other, m.n_excl_other, s);
+  cudaEventRecord(m.ev_join, m.side);
+  cudaStreamWaitEvent(s, m.ev_join, 0);
+  UpdateParams U;
+  U.S = settle_params(m);
+  U.dt = dt;
+  for (int k = 0; k < 3; ++k) U.L[k] = box[k];
+  U.beta = c.beta;
+  U.coulomb = c.coulomb;
+  U.two_beta_sqrtpi = 2.0 * c.beta / sqrt(M_PI);
+  U.water_excl = (m.water_excl && c.beta > 0.0) ? 1 : 0;
+  U.fixed = c.deterministic ? 1 : 0;
+  U.tau = m.tau;
+  U.temperature = m.temperature;
+  U.ndof = (double)m.ndof;
   double half = 0.5 * (c.reach - c.cutoff);
-  md_check<<<1, 1, 0, s>>>(m.maxd2, half * half, h, use_graph, flag);
+  U.build_half2 = half * half;
+  double half_in = 0.5 * (c.inner_reach - c.cutoff);
+  U.prune_half2 = c.inner_reach > 0.0 ? half_in * half_in : 0.0;
+  U.h_build = h_build;
+  U.h_prune = h_prune;
+  U.use_graph = use_graph;
+  U.flag = flag;
+  md_update<<<m.ke_blocks, MD_UPDATE_THREADS, 0, s>>>(
+      m.nwaters, m.nfree, m.waters, m.free_atoms, U, m.inv_mass, m.mass, c.q, c.place_of, c.shift, c.acc,
+      c.acc_fixed, pme ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref, m.x_prune,
+      m.thermo, m.ke_part, m.maxd2);
 }
 
+// A pruning at x on `s` (frames current): the inner lists and their units.
+static void md_prune_body(mdrtMd &m, const double *x, const double box[3], cudaStream_t s) {
+  NbCtx &c = *m.nb;
+  nb_prune_run(c, box, s);
+  md_after_prune<<<blocks_for(3 * m.n, 256), 256, 0, s>>>(3 * m.n, x, m.x_prune, m.thermo);
+}
+
+// A build at x on `s` without a host wait (the body of the conditional node).
 static void md_rebuild_body(mdrtMd &m, const double *x, const double box[3], cudaStream_t s) {
   NbCtx &c = *m.nb;
   nb_build_launch_public(c, x, box, s);
-  md_after_build<<<blocks_for(3 * m.n, 256), 256, 0, s>>>(3 * m.n, x, m.x_ref, m.maxd2, m.thermo, c.sizes,
-                                                         c.status);
+  nb_gather_frames(c, x, box, s);
+  md_after_build<<<blocks_for(3 * m.n, 256), 256, 0, s>>>(3 * m.n, x, m.x_ref, m.thermo, c.sizes, c.status);
+}
+
+static void md_drop_graph(mdrtMd *m) {
+  if (m->exec) cudaGraphExecDestroy(m->exec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  m->exec = nullptr;
+  m->graph = nullptr;
 }
 
 static void md_free(mdrtMd *m) {
   if (!m) return;
-  if (m->exec) cudaGraphExecDestroy(m->exec);
-  if (m->graph) cudaGraphDestroy(m->graph);
+  md_drop_graph(m);
+  if (m->ev_fork) cudaEventDestroy(m->ev_fork);
+  if (m->ev_join) cudaEventDestroy(m->ev_join);
+  if (m->side) cudaStreamDestroy(m->side);
   for (void *p : {(void *)m->inv_mass, (void *)m->mass, (void *)m->waters, (void *)m->free_atoms,
-                  (void *)m->force, (void *)m->x_ref, (void *)m->ke_part, (void *)m->maxd2, (void *)m->thermo})
+                  (void *)m->excl_other, (void *)m->force, (void *)m->x_ref, (void *)m->x_prune,
+                  (void *)m->ke_part, (void *)m->maxd2, (void *)m->thermo, (void *)m->flag})
     if (p) cudaFree(p);
   delete m;
 }
@@ -337,15 +524,15 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
   m->nwaters = nwaters;
   m->dOH = d_oh;
   m->dHH = d_hh;
-  std::vector<char> in_water(c.n, 0);
+  std::vector<int64_t> water_of(c.n, -1);
   for (int64_t w = 0; w < nwaters; ++w)
     for (int k = 0; k < 3; ++k) {
       int32_t a = waters[3 * w + k];
-      if (a < 0 || a >= c.n || in_water[a]) {
+      if (a < 0 || a >= c.n || water_of[a] >= 0) {
         md_free(m);
         return MDRT_NB_INVALID_ARGUMENT;
       }
-      in_water[a] = 1;
+      water_of[a] = w;
     }
   if (nwaters > 0) {
     m->mO = masses[waters[0]];
@@ -357,9 +544,32 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
         return MDRT_NB_UNSUPPORTED;  // one water model per system
       }
   }
+  // Excluded pairs: those inside one water go to the update kernel, if every
+  // water has all three; the others keep the excluded-pair kernel.
+  std::vector<int32_t> pairs(2 * c.n_excl_pairs);
+  if (c.n_excl_pairs > 0)
+    cudaMemcpy(pairs.data(), c.excl_pairs, sizeof(int32_t) * pairs.size(), cudaMemcpyDeviceToHost);
+  std::vector<int> per_water(nwaters, 0);
+  std::vector<int32_t> other;
+  for (int64_t k = 0; k < c.n_excl_pairs; ++k) {
+    int32_t i = pairs[2 * k], j = pairs[2 * k + 1];
+    if (water_of[i] >= 0 && water_of[i] == water_of[j])
+      per_water[water_of[i]]++;
+    else {
+      other.push_back(i);
+      other.push_back(j);
+    }
+  }
+  bool all = nwaters > 0;
+  for (int64_t w = 0; w < nwaters; ++w) all = all && per_water[w] == 3;
+  if (!all) {  // keep every pair in the kernel
+    other = pairs;
+  }
+  m->water_excl = all;
+  m->n_excl_other = (int64_t)other.size() / 2;
   std::vector<int32_t> fr;
   for (int64_t i = 0; i < c.n; ++i)
-    if (!in_water[i]) fr.push_back((int32_t)i);
+    if (water_of[i] < 0) fr.push_back((int32_t)i);
   m->nfree = (int64_t)fr.size();
   std::vector<double> inv(c.n);
   for (int64_t i = 0; i < c.n; ++i) {
@@ -370,16 +580,24 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
     inv[i] = 1.0 / masses[i];
   }
   m->ndof = 3 * c.n - 3 * nwaters - 3;
-  m->ke_blocks = blocks_for(nwaters + m->nfree, 256);
+  m->ke_blocks = blocks_for(nwaters + m->nfree, MD_UPDATE_THREADS);
+  int lo = 0, hi = 0;
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
   bool ok = cudaMalloc(&m->inv_mass, sizeof(double) * c.n) == cudaSuccess &&
             cudaMalloc(&m->mass, sizeof(double) * c.n) == cudaSuccess &&
             cudaMalloc(&m->waters, sizeof(int32_t) * std::max<int64_t>(3 * nwaters, 1)) == cudaSuccess &&
             cudaMalloc(&m->free_atoms, sizeof(int32_t) * std::max<int64_t>(m->nfree, 1)) == cudaSuccess &&
+            cudaMalloc(&m->excl_other, sizeof(int32_t) * std::max<size_t>(other.size(), 2)) == cudaSuccess &&
             cudaMalloc(&m->force, sizeof(double) * 3 * c.n) == cudaSuccess &&
             cudaMalloc(&m->x_ref, sizeof(double) * 3 * c.n) == cudaSuccess &&
+            cudaMalloc(&m->x_prune, sizeof(double) * 3 * c.n) == cudaSuccess &&
             cudaMalloc(&m->ke_part, sizeof(double) * m->ke_blocks) == cudaSuccess &&
-            cudaMalloc(&m->maxd2, sizeof(unsigned int)) == cudaSuccess &&
-            cudaMalloc(&m->thermo, sizeof(double) * 8) == cudaSuccess;
+            cudaMalloc(&m->maxd2, sizeof(unsigned int) * 4) == cudaSuccess &&
+            cudaMalloc(&m->thermo, sizeof(double) * 8) == cudaSuccess &&
+            cudaMalloc(&m->flag, sizeof(int) * 2) == cudaSuccess &&
+            cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, hi) == cudaSuccess &&
+            cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     md_free(m);
     return MDRT_NB_CUDA_ERROR;
@@ -388,9 +606,12 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
   cudaMemcpy(m->mass, masses, sizeof(double) * c.n, cudaMemcpyHostToDevice);
   if (nwaters > 0) cudaMemcpy(m->waters, waters, sizeof(int32_t) * 3 * nwaters, cudaMemcpyHostToDevice);
   if (m->nfree > 0) cudaMemcpy(m->free_atoms, fr.data(), sizeof(int32_t) * m->nfree, cudaMemcpyHostToDevice);
+  if (!other.empty())
+    cudaMemcpy(m->excl_other, other.data(), sizeof(int32_t) * other.size(), cudaMemcpyHostToDevice);
   double th[8] = {1.0, 0, 0, 0, 0, 0, 0, 0};
   cudaMemcpy(m->thermo, th, sizeof(th), cudaMemcpyHostToDevice);
-  cudaMemset(m->maxd2, 0, sizeof(unsigned int));
+  cudaMemset(m->maxd2, 0, sizeof(unsigned int) * 4);
+  cudaMemset(m->force, 0, sizeof(double) * 3 * c.n);
   *out = m;
   return MDRT_NB_OK;
 }
@@ -408,97 +629,112 @@ int32_t mdrtMdSetThermostat(mdrtMd *m, double temperature, double tau, uint64_t 
   m->temperature = temperature;
   m->tau = tau;
   m->seed = seed;
-  if (m->exec) {  // parameters are baked into the graph
-    cudaGraphExecDestroy(m->exec);
-    cudaGraphDestroy(m->graph);
-    m->exec = nullptr;
-    m->graph = nullptr;
-  }
+  md_drop_graph(m);  // parameters are baked into the graph
   return MDRT_NB_OK;
 }
 
-// A build at x that also resets the reference positions of the test of validity.
+// A build at x that also writes the frames and resets the reference
+// positions of the test of validity.
 int32_t mdrtMdBuild(mdrtMd *m, const double *x, const double box[3], void *stream) {
   if (!m || !x || !box) return MDRT_NB_INVALID_ARGUMENT;
   int32_t sizes[NB_SIZE_COUNT];
   int32_t s = mdrtNbBuild(m->handle, x, m->n, box, 0.0, stream, sizes);
   if (s) return s;
   cudaStream_t st = (cudaStream_t)stream;
-  md_after_build<<<blocks_for(3 * m->n, 256), 256, 0, st>>>(3 * m->n, x, m->x_ref, m->maxd2, m->thermo,
-                                                           m->nb->sizes, m->nb->status);
+  NbCtx &c = *m->nb;
+  nb_gather_frames(c, x, box, st);
+  md_after_build<<<blocks_for(3 * m->n, 256), 256, 0, st>>>(3 * m->n, x, m->x_ref, m->thermo, c.sizes, c.status);
+  if (c.inner_reach > 0.0) {
+    md_prune_body(*m, x, box, st);
+    c.inner_valid = true;
+    c.prunes++;
+  }
   return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
 }
+
+}  // extern "C"
+
+// Captures one conditional node (IF) after the current capture point of
+// `cap` and the launches of `fill` on `body` into its body graph.
+template <typename F>
+static cudaError_t md_capture_if(cudaStream_t cap, cudaStream_t body, cudaGraphConditionalHandle h, F &&fill) {
+  cudaStreamCaptureStatus status;
+  cudaGraph_t g;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, &deps, &ndeps);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamUpdateCaptureDependencies(cap, &node, 1, cudaStreamSetCaptureDependencies);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamBeginCaptureToGraph(body, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  fill(body);
+  return cudaStreamEndCapture(body, nullptr);
+}
+
+extern "C" {
 
 int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
                   int32_t unroll, void *stream) {
   if (!m || !x || !v || !box || !(dt > 0) || steps < 0) return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = *m->nb;
   if (!c.built) return MDRT_NB_NOT_BUILT;
+  for (int k = 0; k < 3; ++k)
+    if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;
   cudaSetDevice(c.device);
   cudaStream_t st = (cudaStream_t)stream;
   if (unroll <= 0) {
-    // step by step, the host reading the test of validity after each step
-    int *flag = nullptr;
-    if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
-    int h_flag = 0;
+    // step by step, the host reading the tests of validity after each step
+    int h_flag[2] = {0, 0};
     for (int64_t k = 0; k < steps; ++k) {
-      md_step_body(*m, x, v, box, dt, st, 0, 0, flag);
-      cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+      md_step_body(*m, x, v, box, dt, st, 0, 0, 0, m->flag);
+      cudaMemcpyAsync(h_flag, m->flag, sizeof(h_flag), cudaMemcpyDeviceToHost, st);
       cudaStreamSynchronize(st);
-      if (h_flag) {
+      if (h_flag[0]) {
         int32_t s = mdrtMdBuild(m, x, box, stream);
-        if (s) {
-          cudaFree(flag);
-          return s;
-        }
+        if (s) return s;
+      } else if (h_flag[1]) {
+        md_prune_body(*m, x, box, st);
+        c.prunes++;
       }
     }
-    cudaFree(flag);
     return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
   }
   // a graph of `unroll` steps, each ending in a conditional rebuild
-  int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap;
+  int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap + (int64_t)(c.inner_reach * 1e9) +
+                (c.inner_valid ? 1 : 0) + (c.deterministic ? 2 : 0);
   bool stale = !m->exec || m->gx != x || m->gv != v || m->gdt != dt || m->gunroll != unroll ||
                m->gbox[0] != box[0] || m->gbox[1] != box[1] || m->gbox[2] != box[2] || m->gcap_key != key;
   if (stale) {
-    if (m->exec) cudaGraphExecDestroy(m->exec);
-    if (m->graph) cudaGraphDestroy(m->graph);
-    m->exec = nullptr;
-    m->graph = nullptr;
-    cudaStream_t cap;
+    md_drop_graph(m);
+    cudaStream_t cap, body;
     cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-    cudaStream_t body;
     cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking);
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return MDRT_NB_CUDA_ERROR;
-    m->handles.assign(unroll, 0);
+    bool dual = c.inner_reach > 0.0;
+    m->handles.assign(2 * unroll, 0);
     for (int k = 0; k < unroll && e == cudaSuccess; ++k) {
       cudaStreamCaptureStatus status;
       cudaGraph_t g;
-      const cudaGraphNode_t *deps = nullptr;
-      size_t ndeps = 0;
-      e = cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, &deps, &ndeps);
+      e = cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, nullptr, nullptr);
       if (e != cudaSuccess) break;
-      e = cudaGraphConditionalHandleCreate(&m->handles[k], g, 0, cudaGraphCondAssignDefault);
+      e = cudaGraphConditionalHandleCreate(&m->handles[2 * k], g, 0, cudaGraphCondAssignDefault);
+      if (e == cudaSuccess && dual)
+        e = cudaGraphConditionalHandleCreate(&m->handles[2 * k + 1], g, 0, cudaGraphCondAssignDefault);
       if (e != cudaSuccess) break;
-      md_step_body(*m, x, v, box, dt, cap, m->handles[k], 1, nullptr);
-      e = cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, &deps, &ndeps);
-      if (e != cudaSuccess) break;
-      cudaGraphNodeParams cp = {};
-      cp.type = cudaGraphNodeTypeConditional;
-      cp.conditional.handle = m->handles[k];
-      cp.conditional.type = cudaGraphCondTypeIf;
-      cp.conditional.size = 1;
-      cudaGraphNode_t node;
-      e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
-      if (e != cudaSuccess) break;
-      e = cudaStreamUpdateCaptureDependencies(cap, &node, 1, cudaStreamSetCaptureDependencies);
-      if (e != cudaSuccess) break;
-      cudaGraph_t bodyGraph = cp.conditional.phGraph_out[0];
-      e = cudaStreamBeginCaptureToGraph(body, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-      if (e != cudaSuccess) break;
-      md_rebuild_body(*m, x, box, body);
-      e = cudaStreamEndCapture(body, nullptr);
+      md_step_body(*m, x, v, box, dt, cap, m->handles[2 * k], m->handles[2 * k + 1], 1, nullptr);
+      e = md_capture_if(cap, body, m->handles[2 * k], [&](cudaStream_t b) { md_rebuild_body(*m, x, box, b); });
+      if (e == cudaSuccess && dual)
+        e = md_capture_if(cap, body, m->handles[2 * k + 1], [&](cudaStream_t b) { md_prune_body(*m, x, box, b); });
     }
     cudaGraph_t graph = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
@@ -510,7 +746,7 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
       cudaGetLastError();
       return MDRT_NB_CUDA_ERROR;
     }
-    e = cudaGraphInstantiate(&m->exec, graph, 0);
+    e = cudaGraphInstantiate(&m->exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     if (e != cudaSuccess) {
       fprintf(stderr, "mdrt_nb: step graph instantiate: %s\n", cudaGetErrorString(e));
       cudaGraphDestroy(graph);
@@ -542,6 +778,7 @@ int32_t mdrtMdThermo(mdrtMd *m, void *stream, double *out) {
   if (cudaStreamSynchronize(st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
   for (int k = 0; k < 5; ++k) out[k] = h[k];
   out[5] = (double)m->ndof;
+  out[6] = h[5];
   return MDRT_NB_OK;
 }
 

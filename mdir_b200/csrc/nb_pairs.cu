@@ -69,7 +69,7 @@ __device__ __forceinline__ void nb_red_fixed(unsigned long long *addr, float x, 
 }
 
 template <bool ENERGY, bool FIXED, bool SWITCH>
-__global__ void __launch_bounds__(256) nb_pairs(PairParams P, const int32_t *__restrict__ sizes,
+__global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const int32_t *__restrict__ sizes,
                                                 const int2 *__restrict__ units,
                                                 const int2 *__restrict__ slab,
                                                 const int32_t *__restrict__ counts,
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256) nb_pairs(PairParams P, const int32_t *__r
       xj.z += (float)sz * P.Lz;
       int tj = typ[q];
       float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-#pragma unroll
+#pragma unroll 4
       for (int k = 0; k < NB_GROUP; ++k) {
         int m = (lane + k) & 15;
         float4 xm = s_x[warp][m];
@@ -412,13 +412,21 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
   P.ntypes = c.ntypes;
   P.list_cap = c.list_cap;
   P.units_cap = c.units_cap;
-  // persistent grid: enough warps for the units, at most 8 blocks per SM
+  // persistent grid: enough warps for the units, `pair_blocks_per_sm`
+  // blocks of 8 warps per SM (4 fit at 64 registers; fewer leave room for
+  // the PME kernels that run beside it on another stream)
   int64_t want = (c.units_cap + 7) / 8;
-  int grid = (int)std::min<int64_t>(want, (int64_t)g_sm_count * 8);
+  int grid = (int)std::min<int64_t>(want, (int64_t)g_sm_count * std::max(1, c.pair_blocks_per_sm));
   if (grid < 1) grid = 1;
-#define NB_LAUNCH(E, F, S)                                                                        \
-  nb_pairs<E, F, S><<<grid, 256, 0, s>>>(P, c.sizes, c.units, c.slab, c.counts, c.xq, c.typ_p, c.lj, \
-                                        c.acc, c.acc_fixed, c.unit_partials, c.status)
+  // the inner list of the dual list once it has been pruned, else the outer
+  bool inner = c.inner_reach > 0.0 && c.inner_valid;
+  const int32_t *lsizes = inner ? c.sizes_in : c.sizes;
+  const int2 *lunits = inner ? c.units_in : c.units;
+  const int2 *lslab = inner ? c.slab_in : c.slab;
+  const int32_t *lcounts = inner ? c.counts_in : c.counts;
+#define NB_LAUNCH(E, F, S)                                                                          \
+  nb_pairs<E, F, S><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, c.acc, \
+                                        c.acc_fixed, c.unit_partials, c.status)
   bool F = c.deterministic, S = c.lj_switch != 0;
   if (energy) {
     if (F) { if (S) NB_LAUNCH(true, true, true); else NB_LAUNCH(true, true, false); }
@@ -428,6 +436,18 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
     else { if (S) NB_LAUNCH(false, false, true); else NB_LAUNCH(false, false, false); }
   }
 #undef NB_LAUNCH
+}
+
+void nb_excluded_list_run(NbCtx &c, const double box[3], const int32_t *pairs, int64_t npairs,
+                          cudaStream_t s) {
+  if (npairs == 0 || c.beta == 0.0) return;
+  int blocks = blocks_for(npairs, 256);
+  if (c.deterministic)
+    nb_excluded<true><<<blocks, 256, 0, s>>>(npairs, pairs, c.place_of, c.xq, box[0], box[1], box[2], c.beta,
+                                             c.coulomb, false, c.acc, c.acc_fixed, nullptr, c.status);
+  else
+    nb_excluded<false><<<blocks, 256, 0, s>>>(npairs, pairs, c.place_of, c.xq, box[0], box[1], box[2], c.beta,
+                                              c.coulomb, false, c.acc, c.acc_fixed, nullptr, c.status);
 }
 
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
@@ -455,6 +475,7 @@ void nb_finish_forces(NbCtx &c, double *forces, int accumulate, cudaStream_t s) 
 
 void nb_reduce_energy(NbCtx &c, bool pairs, bool excluded, cudaStream_t s) {
   int eb = (excluded && c.n_excl_pairs > 0 && c.beta != 0.0) ? blocks_for(c.n_excl_pairs, 256) : 0;
-  nb_sum_partials<<<1, 256, 0, s>>>(c.unit_partials, c.sizes, c.units_cap, c.excl_partials, eb,
-                                    pairs ? 1 : 0, c.energy);
+  bool inner = c.inner_reach > 0.0 && c.inner_valid;
+  nb_sum_partials<<<1, 256, 0, s>>>(c.unit_partials, inner ? c.sizes_in : c.sizes, c.units_cap, c.excl_partials,
+                                    eb, pairs ? 1 : 0, c.energy);
 }

@@ -273,6 +273,77 @@ __global__ void __launch_bounds__(128) nb_pme_gather(GridParams G, int64_t place
   if (pot) pot[p] = e;
 }
 
+// The same gather with P threads per atom, one z point each (P a power of
+// two dividing 32), summed over the P lanes by shuffles: four times the
+// threads of a thread per atom, for a kernel that waits on L2 reads.
+template <int P>
+__global__ void __launch_bounds__(128) nb_pme_gather_split(GridParams G, int64_t places,
+                                                           const int32_t *__restrict__ sizes,
+                                                           const int32_t *__restrict__ order,
+                                                           const float4 *__restrict__ xq,
+                                                           const float *__restrict__ phi,
+                                                           float4 *__restrict__ out, float *__restrict__ pot) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t p = t / P;
+  int c = (int)(t & (P - 1));
+  bool live = p < places && p < sizes[NB_SIZE_PLACES];
+  bool atom = live && order[p] >= 0;
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f, e = 0.f;
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (atom) {
+    v = xq[p];
+    int k0, k1, k2;
+    float t0, t1, t2;
+    nb_frac(v.x, G.invL0, G.K0, k0, t0);
+    nb_frac(v.y, G.invL1, G.K1, k1, t1);
+    nb_frac(v.z, G.invL2, G.K2, k2, t2);
+    float w0[P], w1[P], w2[P], d0[P], d1[P], d2[P];
+    nb_bspline<P>(t0, w0, d0);
+    nb_bspline<P>(t1, w1, d1);
+    nb_bspline<P>(t2, w2, d2);
+    int gz = k2 - c;
+    if (gz < 0) gz += G.K2;
+    float wz = w2[c], dz = d2[c];
+#pragma unroll
+    for (int jx = 0; jx < P; ++jx) {
+      int gx = k0 - jx;
+      if (gx < 0) gx += G.K0;
+#pragma unroll
+      for (int jy = 0; jy < P; ++jy) {
+        int gy = k1 - jy;
+        if (gy < 0) gy += G.K1;
+        float f = __ldg(phi + ((int64_t)gx * G.K1 + gy) * G.K2 + gz);
+        float wxy = w0[jx] * w1[jy];
+        g0 = fmaf(d0[jx] * w1[jy], f, g0);
+        g1 = fmaf(w0[jx] * d1[jy], f, g1);
+        e = fmaf(wxy, f, e);
+        g2 = fmaf(wxy, f, g2);
+      }
+    }
+    g0 *= wz;
+    g1 *= wz;
+    g2 *= dz;
+    e *= wz;
+  }
+#pragma unroll
+  for (int o = P / 2; o > 0; o >>= 1) {
+    g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+    g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+    g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+    e += __shfl_xor_sync(0xffffffffu, e, o);
+  }
+  if (!live || c != 0) return;
+  if (!atom) {
+    out[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (pot) pot[p] = 0.f;
+    return;
+  }
+  float q = v.w;
+  out[p] = make_float4(-q * g0 * (float)G.K0 * G.invL0, -q * g1 * (float)G.K1 * G.invL1,
+                       -q * g2 * (float)G.K2 * G.invL2, 0.f);
+  if (pot) pot[p] = e;
+}
+
 inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
 
 // |b(m)|^2 of the SPME B-spline moduli along one edge, in f64 on the host.
@@ -409,11 +480,12 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
   if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.grid) != CUFFT_SUCCESS) return -3;
   float *pot = potential ? P.potential : nullptr;
   int blocks = blocks_for(c.places_cap, 128);
+  float4 *pf = (float4 *)P.pme_force;
   switch (P.order) {
-    case 4: nb_pme_gather<4><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, (float4 *)P.pme_force, pot); break;
-    case 5: nb_pme_gather<5><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, (float4 *)P.pme_force, pot); break;
-    case 6: nb_pme_gather<6><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, (float4 *)P.pme_force, pot); break;
-    case 8: nb_pme_gather<8><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, (float4 *)P.pme_force, pot); break;
+    case 4: nb_pme_gather_split<4><<<blocks_for(c.places_cap * 4, 128), 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, pf, pot); break;
+    case 5: nb_pme_gather<5><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, pf, pot); break;
+    case 6: nb_pme_gather<6><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, pf, pot); break;
+    case 8: nb_pme_gather_split<8><<<blocks_for(c.places_cap * 8, 128), 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, pf, pot); break;
   }
   return 0;
 }

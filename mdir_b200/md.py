@@ -58,7 +58,7 @@ class Integrator:
         out = np.zeros(8)
         L.check(L.lib().mdrtMdThermo(self._h, _stream(stream), _hp(out)), "mdrtMdThermo")
         return {"lambda": out[0], "kinetic_half": out[1], "kinetic_half_before": out[2],
-                "steps": int(out[3]), "builds": int(out[4]), "ndof": int(out[5]),
+                "steps": int(out[3]), "builds": int(out[4]), "ndof": int(out[5]), "prunes": int(out[6]),
                 "kinetic": 0.5 * (out[1] + out[2])}
 
     def forces(self):

@@ -94,6 +94,14 @@ class NonbondedTerm:
         k = [0, 0, 0] if grid is None else [int(v) for v in grid]
         L.check(L.lib().mdrtPmeSetup(self._h, k[0], k[1], k[2], int(order)), "mdrtPmeSetup")
 
+    def set_pruned_reach(self, pruned_distance):
+        """The dual list: prune the lists to this reach (0: one list)."""
+        L.check(L.lib().mdrtNbSetPrunedReach(self._h, float(pruned_distance)), "mdrtNbSetPrunedReach")
+
+    def prune(self, x, box=None, stream=None):
+        b = _host(self.box if box is None else box, np.float64)
+        L.check(L.lib().mdrtNbPrune(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtNbPrune")
+
     def set_deterministic(self, on=True):
         L.check(L.lib().mdrtNbSetDeterministic(self._h, int(bool(on))), "mdrtNbSetDeterministic")
 

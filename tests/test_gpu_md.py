@@ -85,6 +85,43 @@ def test_nve_energy_is_conserved(cuda):
     assert abs(e1 - e0) < 2e-3 * k0, (e0, e1, k0)
 
 
+def test_dual_list_keeps_every_pair_within_the_cutoff(cuda):
+    # outer lists at 1.2 nm rebuilt rarely, inner lists pruned to 1.0 nm on
+    # the device whenever the positions moved half of the inner skin
+    s = systems.tip3p(waters=700, seed=26)
+    s["reach"] = 1.2
+    t, md, x, v = setup(s, tau=0.1)
+    t.set_pruned_reach(1.0)
+    md.build(x, s["box"])
+    md.run(x, v, s["box"], 0.002, 400, unroll=20)
+    th = md.thermo()
+    assert th["prunes"] > th["builds"] >= 1
+    assert t.status() == 0
+    ref = O.evaluate(s, x.cpu().numpy())
+    f = md.forces()
+    # the forces of the next evaluation at these positions, over the inner lists
+    got = t.force(x, energy=True).cpu().numpy()
+    err = np.sqrt(np.mean(np.sum((got - ref["forces"]) ** 2, 1)) / np.mean(np.sum(ref["forces"] ** 2, 1)))
+    assert err < 1e-5
+    e = t.energies()
+    assert abs(e["coulomb"] - ref["terms"]["coulomb"]) < 1e-6 * sum(abs(v) for v in ref["terms"].values())
+    del f
+
+
+def test_dual_list_step_by_step_equals_graph(cuda):
+    s = systems.tip3p(waters=500, seed=27)
+    s["reach"] = 1.15
+    runs = []
+    for unroll in (10, 0):
+        t, md, x, v = setup(s, deterministic=True, tau=0.1)
+        t.set_pruned_reach(1.0)
+        md.build(x, s["box"])
+        md.run(x, v, s["box"], 0.002, 80, unroll=unroll)
+        runs.append((x.clone(), md.thermo()))
+    assert torch.equal(runs[0][0], runs[1][0])
+    assert runs[0][1]["prunes"] == runs[1][1]["prunes"] > 0
+
+
 def test_thermostat_holds_the_temperature(cuda):
     s = systems.tip3p(waters=500, seed=25)
     t, md, x, v = setup(s, tau=0.05)
