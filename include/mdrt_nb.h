@@ -130,6 +130,15 @@ int32_t mdrtNbSetPrunedReach(mdrtNb *ctx, double pruned_distance);
  * lib/Conversion/MDExecToGPU/MDExecToGPU.cpp:9588. */
 int32_t mdrtNbPrune(mdrtNb *ctx, const double *x, const double box[3], void *stream);
 
+/* Launch-shape tuning of the kernels (the autotuner's knobs; results do not
+ * depend on them): MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM, the resident blocks of 8
+ * warps per SM of the pair kernel (1-4; fewer leave room for the PME
+ * kernels beside it).  Returns MDRT_NB_INVALID_ARGUMENT for an unknown key
+ * or value.  No MDIR counterpart: MDIR fixes these in its emitters
+ * (lib/Dialect/MDExec/DevicePolicy.cpp:72-99). */
+enum mdrtNbTuneKey { MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM = 0 };
+int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value);
+
 /* Deterministic mode: 64-bit fixed-point force accumulation (2^32 per
  * kJ/mol/nm) and PME spreading (2^40 per e); bitwise reproducible.
  * MDIR: deterministic = true (D70, D84; docs/pme.md, Section 3). */
@@ -198,8 +207,11 @@ int32_t mdrtNbStatus(mdrtNb *ctx, void *stream, int32_t clear, int32_t *status);
  * launches of each stage of the force term at device positions x, after a
  * valid build: out[0] frame gather, out[1] pair kernel, out[2] excluded
  * correction, out[3] PME (spread, FFTs, convolution, gather), out[4] force
- * finish.  For the roofline of each kernel; the forces it leaves are not
- * meaningful.  MDIR: MDRT_WAIT=1 per-kernel timing (runtime/mdrt_cuda.c:600). */
+ * finish, out[5] neighbor build (launches only), out[6] pruning (0 without
+ * a dual list); out holds 8 doubles.  The launches of a stage are replayed
+ * from a CUDA graph, so the host's launch rate does not enter the numbers.
+ * For the roofline of each kernel; the forces it leaves are not meaningful.
+ * MDIR: MDRT_WAIT=1 per-kernel timing (runtime/mdrt_cuda.c:600). */
 int32_t mdrtNbTimeKernels(mdrtNb *ctx, const double *x, const double box[3], int32_t iterations,
                           void *stream, double *out);
 

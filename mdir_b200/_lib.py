@@ -33,6 +33,7 @@ SIGNATURES = {
     "mdrtNbSetInteraction": (_i32, [_p, _d, _d, _d, _d, _i32, _i32, _d]),
     "mdrtNbSetDeterministic": (_i32, [_p, _i32]),
     "mdrtNbSetPrunedReach": (_i32, [_p, _d]),
+    "mdrtNbSetTuning": (_i32, [_p, _i32, _i32]),
     "mdrtNbPrune": (_i32, [_p, _p, _p, _p]),
     "mdrtPmeSetup": (_i32, [_p, _i32, _i32, _i32, _i32]),
     "mdrtNbBuild": (_i32, [_p, _p, _i64, _p, _d, _p, _p]),

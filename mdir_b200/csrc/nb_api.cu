@@ -201,6 +201,17 @@ int32_t mdrtNbSetInteraction(mdrtNb *ctx, double cutoff, double reach, double be
   return MDRT_NB_OK;
 }
 
+int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value) {
+  if (!ctx) return MDRT_NB_INVALID_ARGUMENT;
+  switch (key) {
+    case MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM:
+      if (value < 1 || value > 4) return MDRT_NB_INVALID_ARGUMENT;
+      ctx->c.pair_blocks_per_sm = value;
+      return MDRT_NB_OK;
+  }
+  return MDRT_NB_INVALID_ARGUMENT;
+}
+
 int32_t mdrtNbSetPrunedReach(mdrtNb *ctx, double pruned_distance) {
   if (!ctx || !(pruned_distance == 0.0 || (pruned_distance >= ctx->c.cutoff && pruned_distance <= ctx->c.reach)))
     return MDRT_NB_INVALID_ARGUMENT;
@@ -464,7 +475,12 @@ extern "C" int32_t mdrtNbTimeKernels(mdrtNb *ctx, const double *x, const double 
   if (!ctx || !x || !box || !out || iterations < 1) return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = ctx->c;
   if (!c.built) return MDRT_NB_NOT_BUILT;
-  cudaStream_t st = (cudaStream_t)stream;
+  // The launches of each stage are captured into a CUDA graph on a stream
+  // of our own and the graph is timed, so that the host's launch rate does
+  // not bound the numbers of short kernels.
+  (void)stream;
+  cudaStream_t st;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   double *scratch = nullptr;
   CK(cudaMalloc(&scratch, sizeof(double) * 3 * c.n));
   cudaEvent_t e0, e1;
@@ -472,12 +488,23 @@ extern "C" int32_t mdrtNbTimeKernels(mdrtNb *ctx, const double *x, const double 
   cudaEventCreate(&e1);
   auto timed = [&](auto &&launch) {
     launch();  // warm
-    cudaEventRecord(e0, st);
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -1.0;
     for (int k = 0; k < iterations; ++k) launch();
+    if (cudaStreamEndCapture(st, &g) != cudaSuccess || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return -1.0;
+    }
+    cudaGraphLaunch(ge, st);
+    cudaEventRecord(e0, st);
+    cudaGraphLaunch(ge, st);
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
+    cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
     return (double)ms / iterations;
   };
   out[0] = timed([&] { nb_gather_frames(c, x, box, st); });
@@ -485,9 +512,15 @@ extern "C" int32_t mdrtNbTimeKernels(mdrtNb *ctx, const double *x, const double 
   out[2] = timed([&] { nb_excluded_run(c, box, false, st); });
   out[3] = (c.pme.on && c.beta > 0) ? timed([&] { nb_pme_run(c, box, false, false, st); }) : 0.0;
   out[4] = timed([&] { nb_finish_forces(c, scratch, 0, st); });
+  // the neighbor build with its present capacities (no host wait) and the
+  // pruning; the lists they leave are those of x again
+  out[5] = timed([&] { nb_build_launch_public(c, x, box, st); });
+  nb_gather_frames(c, x, box, st);
+  out[6] = c.inner_reach > 0.0 ? timed([&] { nb_prune_run(c, box, st); }) : 0.0;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
   cudaFree(scratch);
   CK(cudaGetLastError());
   return MDRT_NB_OK;

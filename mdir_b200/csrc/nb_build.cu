@@ -185,112 +185,139 @@ struct SearchParams {
   int64_t list_cap;
 };
 
-// A warp builds the list of one group.  Lanes 0-15 and 16-31 hold the
+// W warps build the list of one group (W = 1: a warp a group, four groups
+// a block; W = 4: a block a group).  Lanes 0-15 and 16-31 of a warp hold the
 // members; a pass tests two candidate groups, one per half-warp, each lane
-// one candidate place against the 16 members.
-__global__ void __launch_bounds__(128) nb_search(SearchParams P, const int32_t *sizes_in,
-                                                 const int32_t *__restrict__ order,
-                                                 const float4 *__restrict__ xw,
-                                                 const float4 *__restrict__ box_lo,
-                                                 const float4 *__restrict__ box_hi,
-                                                 const int32_t *__restrict__ group_start,
-                                                 const int32_t *__restrict__ excl_off,
-                                                 const int32_t *__restrict__ excl,
-                                                 int2 *__restrict__ slab, int32_t *__restrict__ counts,
-                                                 int32_t *sizes) {
-  __shared__ float4 s_mem[4][NB_GROUP];
-  __shared__ int s_atom[4][NB_GROUP];
-  __shared__ int s_key[4][NB_EXCL_MAX];
-  __shared__ unsigned char s_ku[4][NB_EXCL_MAX];
+// one candidate place against the 16 members.  With W > 1 the columns of the
+// window are cut into W contiguous shares, each warp stages its entries in
+// shared memory (list_cap each) and the block writes them in warp order, so
+// a list is the same for every W.
+template <int W>
+__global__ void __launch_bounds__(128) nb_search_t(SearchParams P, const int32_t *sizes_in,
+                                                   const int32_t *__restrict__ order,
+                                                   const float4 *__restrict__ xw,
+                                                   const float4 *__restrict__ box_lo,
+                                                   const float4 *__restrict__ box_hi,
+                                                   const int32_t *__restrict__ group_start,
+                                                   const int32_t *__restrict__ excl_off,
+                                                   const int32_t *__restrict__ excl,
+                                                   int2 *__restrict__ slab, int32_t *__restrict__ counts,
+                                                   int32_t *sizes) {
+  constexpr int GPB = 4 / W;  // groups per block
+  extern __shared__ int2 s_stage[];
+  __shared__ float4 s_mem[GPB][NB_GROUP];
+  __shared__ int s_atom[GPB][NB_GROUP];
+  __shared__ int s_key[GPB][NB_EXCL_MAX];
+  __shared__ unsigned char s_ku[GPB][NB_EXCL_MAX];
+  __shared__ int s_meta[GPB][4];  // nkeys, wide, kmin, kmax
+  __shared__ int s_count[4];
   const unsigned FULL = 0xffffffffu;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int u = lane & 15, half = lane >> 4;
-  int64_t g = (int64_t)blockIdx.x * 4 + warp;
+  int gi = warp / W, part = warp % W;
+  int64_t g = (int64_t)blockIdx.x * GPB + gi;
   int ngroups = sizes_in[NB_SIZE_GROUPS];
-  if (g >= ngroups || g >= P.groups_cap) return;
+  bool live = g < ngroups && g < P.groups_cap;
+  if (W == 1 && !live) return;
 
-  // members
-  int64_t pi = g * NB_GROUP + u;
-  int ai = order[pi];
-  float4 xi = xw[pi];
-  if (half == 0) {
-    xi.w = ai >= 0 ? 1.f : 0.f;
-    s_mem[warp][u] = xi;
-    s_atom[warp][u] = ai;
-  }
-  // exclusion partners of the members: keys (partner atom, member), sorted
-  int rs = 0, re = 0;
-  if (excl_off && half == 0 && ai >= 0) {
-    rs = excl_off[ai];
-    re = excl_off[ai + 1];
-  }
-  int cnt = re - rs;
-  int incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(FULL, incl, o);
-    if (lane >= o) incl += y;
-  }
-  int nkeys = __shfl_sync(FULL, incl, 31);
-  bool wide = nkeys > NB_EXCL_MAX;
-  if (!wide) {
-    int at = incl - cnt;
-    for (int k = 0; k < cnt; ++k) {
-      s_key[warp][at + k] = excl[rs + k];
-      s_ku[warp][at + k] = (unsigned char)u;
+  // members and the exclusion partners of the members: keys (partner atom,
+  // member), sorted; by the first warp of the group
+  if (live && part == 0) {
+    int64_t pi = g * NB_GROUP + u;
+    int ai = order[pi];
+    float4 xi = xw[pi];
+    if (half == 0) {
+      xi.w = ai >= 0 ? 1.f : 0.f;
+      s_mem[gi][u] = xi;
+      s_atom[gi][u] = ai;
     }
-  } else if (lane == 0) {
-    atomicAdd(&sizes[NB_SIZE_EXCL_WIDE], 1);
-  }
-  __syncwarp();
-  int kmin = INT_MAX, kmax = INT_MIN;
-  if (!wide && nkeys > 0) {
-    // rank sort of the keys by (partner, member, position)
-    int myk[NB_EXCL_MAX / 32];
-    unsigned char myu[NB_EXCL_MAX / 32];
-    int myr[NB_EXCL_MAX / 32];
-    int mine = 0;
-    for (int k = lane; k < nkeys; k += 32, ++mine) {
-      int kv = s_key[warp][k];
-      unsigned char ku = s_ku[warp][k];
-      int r = 0;
-      for (int t = 0; t < nkeys; ++t) {
-        int tv = s_key[warp][t];
-        r += (tv < kv) || (tv == kv && t < k);
+    int rs = 0, re = 0;
+    if (excl_off && half == 0 && ai >= 0) {
+      rs = excl_off[ai];
+      re = excl_off[ai + 1];
+    }
+    int cnt = re - rs;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    int nkeys = __shfl_sync(FULL, incl, 31);
+    bool wide = nkeys > NB_EXCL_MAX;
+    if (!wide) {
+      int at = incl - cnt;
+      for (int k = 0; k < cnt; ++k) {
+        s_key[gi][at + k] = excl[rs + k];
+        s_ku[gi][at + k] = (unsigned char)u;
       }
-      myk[mine] = kv;
-      myu[mine] = ku;
-      myr[mine] = r;
-      kmin = min(kmin, kv);
-      kmax = max(kmax, kv);
+    } else if (lane == 0) {
+      atomicAdd(&sizes[NB_SIZE_EXCL_WIDE], 1);
     }
     __syncwarp();
-    for (int m = 0; m < mine; ++m) {
-      s_key[warp][myr[m]] = myk[m];
-      s_ku[warp][myr[m]] = myu[m];
-    }
+    int kmin = INT_MAX, kmax = INT_MIN;
+    if (!wide && nkeys > 0) {
+      // rank sort of the keys by (partner, member, position)
+      int myk[NB_EXCL_MAX / 32];
+      unsigned char myu[NB_EXCL_MAX / 32];
+      int myr[NB_EXCL_MAX / 32];
+      int mine = 0;
+      for (int k = lane; k < nkeys; k += 32, ++mine) {
+        int kv = s_key[gi][k];
+        unsigned char ku = s_ku[gi][k];
+        int r = 0;
+        for (int t = 0; t < nkeys; ++t) {
+          int tv = s_key[gi][t];
+          r += (tv < kv) || (tv == kv && t < k);
+        }
+        myk[mine] = kv;
+        myu[mine] = ku;
+        myr[mine] = r;
+        kmin = min(kmin, kv);
+        kmax = max(kmax, kv);
+      }
+      __syncwarp();
+      for (int m = 0; m < mine; ++m) {
+        s_key[gi][myr[m]] = myk[m];
+        s_ku[gi][myr[m]] = myu[m];
+      }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      kmin = min(kmin, __shfl_xor_sync(FULL, kmin, o));
-      kmax = max(kmax, __shfl_xor_sync(FULL, kmax, o));
+      for (int o = 16; o > 0; o >>= 1) {
+        kmin = min(kmin, __shfl_xor_sync(FULL, kmin, o));
+        kmax = max(kmax, __shfl_xor_sync(FULL, kmax, o));
+      }
     }
+    if (lane == 0) {
+      s_meta[gi][0] = nkeys;
+      s_meta[gi][1] = wide;
+      s_meta[gi][2] = kmin;
+      s_meta[gi][3] = kmax;
+    }
+    __syncwarp();
   }
-  __syncwarp();
-
-  float4 lo = box_lo[g], hi = box_hi[g];
-  float ci0 = 0.5f * (lo.x + hi.x), ci1 = 0.5f * (lo.y + hi.y), ci2 = 0.5f * (lo.z + hi.z);
-  float wi0 = 0.5f * (hi.x - lo.x), wi1 = 0.5f * (hi.y - lo.y), wi2 = 0.5f * (hi.z - lo.z);
-  int kx0 = (int)floorf((lo.x - P.Rbox) / P.wx), kx1 = (int)floorf((hi.x + P.Rbox) / P.wx);
-  int ky0 = (int)floorf((lo.y - P.Rbox) / P.wy), ky1 = (int)floorf((hi.y + P.Rbox) / P.wy);
-  int sz0 = (lo.z - P.Rbox < 0.f) ? -1 : 0;
-  int sz1 = (hi.z + P.Rbox >= P.Lz) ? 1 : 0;
-  float Rb2 = P.Rbox * P.Rbox;
+  if (W > 1) __syncthreads();
+  else __syncwarp();
   int count = 0;
+  int2 *stage = W > 1 ? s_stage + (size_t)warp * P.list_cap : nullptr;
+  if (live) {
+    int nkeys = s_meta[gi][0];
+    bool wide = s_meta[gi][1] != 0;
+    int kmin = s_meta[gi][2], kmax = s_meta[gi][3];
+    float4 lo = box_lo[g], hi = box_hi[g];
+    float ci0 = 0.5f * (lo.x + hi.x), ci1 = 0.5f * (lo.y + hi.y), ci2 = 0.5f * (lo.z + hi.z);
+    float wi0 = 0.5f * (hi.x - lo.x), wi1 = 0.5f * (hi.y - lo.y), wi2 = 0.5f * (hi.z - lo.z);
+    int kx0 = (int)floorf((lo.x - P.Rbox) / P.wx), kx1 = (int)floorf((hi.x + P.Rbox) / P.wx);
+    int ky0 = (int)floorf((lo.y - P.Rbox) / P.wy), ky1 = (int)floorf((hi.y + P.Rbox) / P.wy);
+    int sz0 = (lo.z - P.Rbox < 0.f) ? -1 : 0;
+    int sz1 = (hi.z + P.Rbox >= P.Lz) ? 1 : 0;
+    float Rb2 = P.Rbox * P.Rbox;
+    int nx = kx1 - kx0 + 1, nwin = (ky1 - ky0 + 1) * nx;
+    int w0 = (int)((int64_t)nwin * part / W), w1 = (int)((int64_t)nwin * (part + 1) / W);
 
-  for (int ky = ky0; ky <= ky1; ++ky) {
-    int cy = ((ky % P.Ny) + P.Ny) % P.Ny;
-    int sy = (ky - cy) / P.Ny;
-    for (int kx = kx0; kx <= kx1; ++kx) {
+    for (int wi = w0; wi < w1; ++wi) {
+      int ky = ky0 + wi / nx, kx = kx0 + wi % nx;
+      int cy = ((ky % P.Ny) + P.Ny) % P.Ny;
+      int sy = (ky - cy) / P.Ny;
       int cx = ((kx % P.Nx) + P.Nx) % P.Nx;
       int sx = (kx - cx) / P.Nx;
       int c = cy * P.Nx + cx;
@@ -333,8 +360,8 @@ __global__ void __launch_bounds__(128) nb_search(SearchParams P, const int32_t *
                 bool same = (h == g);
 #pragma unroll 4
                 for (int m = 0; m < NB_GROUP; ++m) {
-                  float4 xm = s_mem[warp][m];
-                  int am = s_atom[warp][m];
+                  float4 xm = s_mem[gi][m];
+                  int am = s_atom[gi][m];
                   // canonical orientation: A = smaller atom number
                   bool jfirst = aj < am;
                   float4 xa = jfirst ? xj : xm;
@@ -350,17 +377,17 @@ __global__ void __launch_bounds__(128) nb_search(SearchParams P, const int32_t *
                       int lo_i = 0, hi_i = nkeys;
                       while (lo_i < hi_i) {
                         int mid = (lo_i + hi_i) >> 1;
-                        if (s_key[warp][mid] < aj) lo_i = mid + 1; else hi_i = mid;
+                        if (s_key[gi][mid] < aj) lo_i = mid + 1; else hi_i = mid;
                       }
-                      for (int k = lo_i; k < nkeys && s_key[warp][k] == aj; ++k)
-                        mask &= ~(1u << s_ku[warp][k]);
+                      for (int k = lo_i; k < nkeys && s_key[gi][k] == aj; ++k)
+                        mask &= ~(1u << s_ku[gi][k]);
                     }
                   } else {
                     unsigned mm = mask;
                     while (mm) {
                       int m = __ffs(mm) - 1;
                       mm &= mm - 1;
-                      int am = s_atom[warp][m];
+                      int am = s_atom[gi][m];
                       for (int k = excl_off[am]; k < excl_off[am + 1]; ++k)
                         if (excl[k] == aj) mask &= ~(1u << m);
                     }
@@ -370,10 +397,14 @@ __global__ void __launch_bounds__(128) nb_search(SearchParams P, const int32_t *
             }
             unsigned has = __ballot_sync(FULL, mask != 0);
             if (mask) {
-              int rank = __popc(has & ((1u << lane) - 1));
-              int at = count + rank;
-              if (at < P.list_cap)
-                slab[g * P.list_cap + at] = make_int2((int)pj, (int)(mask | ((unsigned)code << 16)));
+              int at = count + __popc(has & ((1u << lane) - 1));
+              int2 en = make_int2((int)pj, (int)(mask | ((unsigned)code << 16)));
+              if (at < P.list_cap) {
+                if (W > 1)
+                  stage[at] = en;
+                else
+                  slab[g * P.list_cap + at] = en;
+              }
             }
             count += __popc(has);
           }
@@ -381,10 +412,29 @@ __global__ void __launch_bounds__(128) nb_search(SearchParams P, const int32_t *
       }
     }
   }
-  if (lane == 0) {
-    counts[g] = count;
-    atomicMax(&sizes[NB_SIZE_LONGEST], count);
-    if (count > P.list_cap) atomicOr(&sizes[NB_SIZE_OVERFLOW], 2);
+  if (W == 1) {
+    if (lane == 0) {
+      counts[g] = count;
+      atomicMax(&sizes[NB_SIZE_LONGEST], count);
+      if (count > P.list_cap) atomicOr(&sizes[NB_SIZE_OVERFLOW], 2);
+    }
+    return;
+  }
+  if (lane == 0) s_count[warp] = count;
+  __syncthreads();
+  if (!live) return;
+  int at = 0, total = 0;
+  for (int w = gi * W; w < gi * W + W; ++w) {
+    if (w < warp) at += s_count[w];
+    total += s_count[w];
+  }
+  int keep = (int)min((int64_t)count, P.list_cap);
+  for (int i = lane; i < keep; i += 32)
+    if (at + i < P.list_cap) slab[g * P.list_cap + at + i] = stage[i];
+  if (part == 0 && lane == 0) {
+    counts[g] = total;
+    atomicMax(&sizes[NB_SIZE_LONGEST], total);
+    if (total > P.list_cap) atomicOr(&sizes[NB_SIZE_OVERFLOW], 2);
   }
 }
 
@@ -469,6 +519,72 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
     out += __popc(has);
   }
   if (lane == 0) counts_in[g] = out;
+}
+
+// The same pruning with a block of NB_PRUNE_WARPS warps per group: warp w
+// takes the w-th contiguous share of the outer entries, stages what
+// survives in shared memory, and the block writes the shares in warp order,
+// so the inner list is the one of the warp-per-group kernel, in a quarter of
+// the dependent rounds.  Dynamic shared memory: list_cap entries.
+#define NB_PRUNE_WARPS 4
+__global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
+    nb_prune_block(int64_t groups_cap, const int32_t *__restrict__ sizes, float Lx, float Ly, float Lz, float rin2,
+                   int64_t list_cap, const int2 *__restrict__ slab, const int32_t *__restrict__ counts,
+                   const int32_t *__restrict__ order, const float4 *__restrict__ xq, int2 *__restrict__ slab_in,
+                   int32_t *__restrict__ counts_in) {
+  extern __shared__ int2 s_stage[];
+  __shared__ float4 s_m[NB_GROUP];
+  __shared__ int s_cnt[NB_PRUNE_WARPS];
+  __shared__ unsigned s_live;
+  const unsigned FULL = 0xffffffffu;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int64_t g = blockIdx.x;
+  if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
+  if (warp == 0) {
+    if (lane < NB_GROUP) s_m[lane] = xq[g * NB_GROUP + lane];
+    unsigned live = __ballot_sync(FULL, lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0) & 0xffffu;
+    if (lane == 0) s_live = live;
+  }
+  __syncthreads();
+  unsigned live = s_live;
+  int cnt = (int)min((int64_t)counts[g], list_cap);
+  int share = ((cnt + NB_PRUNE_WARPS - 1) / NB_PRUNE_WARPS + 31) / 32 * 32;
+  int lo = min(cnt, warp * share), hi = min(cnt, lo + share);
+  int2 *stage = s_stage + lo;  // a warp's survivors never outnumber its share
+  int out = 0;
+  for (int base = lo; base < hi; base += 32) {
+    int e = base + lane;
+    unsigned inner = 0;
+    int2 en = make_int2(0, 0);
+    if (e < hi) {
+      en = slab[g * list_cap + e];
+      unsigned mm = (unsigned)en.y & live & 0xffffu;
+      int sx, sy, sz;
+      nb_decode_image(((unsigned)en.y >> 16) & 31, sx, sy, sz);
+      float4 xj = xq[en.x];
+      float jx = xj.x + (float)sx * Lx, jy = xj.y + (float)sy * Ly, jz = xj.z + (float)sz * Lz;
+      while (mm) {
+        int m = __ffs(mm) - 1;
+        mm &= mm - 1;
+        float4 xm = s_m[m];
+        float dx = xm.x - jx, dy = xm.y - jy, dz = xm.z - jz;
+        float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= rin2) inner |= 1u << m;
+      }
+    }
+    unsigned has = __ballot_sync(FULL, inner != 0);
+    if (inner) stage[out + __popc(has & ((1u << lane) - 1))] = make_int2(en.x, (int)(inner | ((unsigned)en.y & 0xffff0000u)));
+    out += __popc(has);
+  }
+  if (lane == 0) s_cnt[warp] = out;
+  __syncthreads();
+  int at = 0, total = 0;
+  for (int w = 0; w < NB_PRUNE_WARPS; ++w) {
+    if (w < warp) at += s_cnt[w];
+    total += s_cnt[w];
+  }
+  for (int i = lane; i < out; i += 32) slab_in[g * list_cap + at + i] = stage[i];
+  if (threadIdx.x == 0) counts_in[g] = total;
 }
 
 inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
@@ -611,9 +727,22 @@ static void nb_build_launch(NbCtx &c, const double *x, const double box[3], cuda
   P.Rbox = (float)(Rw + 2e-5 * (box[0] + box[1] + box[2]) + 1e-6);
   P.groups_cap = c.groups_cap;
   P.list_cap = c.list_cap;
-  nb_search<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, c.sizes, c.order, c.xw, c.box_lo, c.box_hi,
-                                                       c.group_start, c.excl_off, c.excl, c.slab,
-                                                       c.counts, c.sizes);
+  // four warps a group when their staging fits in shared memory, else one
+  size_t stage = sizeof(int2) * 4 * (size_t)c.list_cap;
+  if (stage <= 200 * 1024) {
+    static size_t configured = 0;
+    if (stage > 48 * 1024 && configured < stage) {
+      cudaFuncSetAttribute(nb_search_t<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+      configured = stage;
+    }
+    nb_search_t<4><<<(int)c.groups_cap, 128, stage, s>>>(P, c.sizes, c.order, c.xw, c.box_lo, c.box_hi,
+                                                         c.group_start, c.excl_off, c.excl, c.slab, c.counts,
+                                                         c.sizes);
+  } else {
+    nb_search_t<1><<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, c.sizes, c.order, c.xw, c.box_lo, c.box_hi,
+                                                               c.group_start, c.excl_off, c.excl, c.slab,
+                                                               c.counts, c.sizes);
+  }
   nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts,
                                                              c.list_cap, c.unit_n);
   nb_scan(c.unit_n, c.unit_start, (int)c.groups_cap, nullptr, c.scan_scratch, s);
@@ -643,9 +772,21 @@ int nb_reserve_inner(NbCtx &c) {
 
 void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s) {
   double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2]);
-  nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
-                                                      (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
-                                                      c.counts, c.order, c.xq, c.slab_in, c.counts_in);
+  size_t stage = sizeof(int2) * (size_t)c.list_cap;
+  if (stage <= 200 * 1024) {
+    static int configured = 0;
+    if (stage > 48 * 1024 && configured < (int)stage) {
+      cudaFuncSetAttribute(nb_prune_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+      configured = (int)stage;
+    }
+    nb_prune_block<<<(int)c.groups_cap, NB_PRUNE_WARPS * 32, stage, s>>>(
+        c.groups_cap, c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+        c.counts, c.order, c.xq, c.slab_in, c.counts_in);
+  } else {
+    nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
+                                                        (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+                                                        c.counts, c.order, c.xq, c.slab_in, c.counts_in);
+  }
   nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts_in, c.list_cap,
                                                              c.unit_n_in);
   nb_scan(c.unit_n_in, c.unit_start_in, (int)c.groups_cap, nullptr, c.scan_scratch, s);

@@ -27,6 +27,8 @@
 #include "../../include/mdrt_nb.h"
 #include "nb_context.h"
 
+#define MD_MAX_UNROLL 256  // steps of one replayed graph
+
 struct mdrtMd {
   NbCtx *nb = nullptr;
   mdrtNb *handle = nullptr;
@@ -45,7 +47,8 @@ struct mdrtMd {
   double *ke_part = nullptr;       // per-block kinetic partials
   int ke_blocks = 0;
   unsigned int *maxd2 = nullptr;   // [0] float bits of max |x - x_ref|^2, [1] of max |x - x_prune|^2, [2] blocks done
-  double *thermo = nullptr;        // [0] lambda, [1] KE, [2] KE before, [3] steps, [4] builds, [5] prunes, [6..7] noise
+  double *thermo = nullptr;        // [0] lambda, [1] KE, [2] KE before, [3] steps, [4] builds, [5] prunes
+  double *noise = nullptr;         // thermostat draws of the steps of one launch (2 a step)
   int *flag = nullptr;             // [0] rebuild, [1] prune: flags for the step-by-step path
   double temperature = 300.0, tau = 0.0;
   int64_t ndof = 0;
@@ -138,9 +141,11 @@ struct UpdateParams {
   // thermostat and the tests of validity, done by the last block
   double tau, temperature, ndof;
   double build_half2, prune_half2;  // ((R - r_c)/2)^2 and ((R_in - r_c)/2)^2 (0: no dual list)
-  cudaGraphConditionalHandle h_build, h_prune;
+  cudaGraphConditionalHandle h_any;  // the step's conditional node: a rebuild or a pruning is due
   int use_graph;
-  int *flag;
+  int *flag;  // [0] rebuild, [1] prune (device)
+  const double *noise;  // the thermostat's draws of the steps of this launch
+  int k;                // this step's index among them
 };
 
 // The force on atom a: the pair / excluded accumulator of its place and the
@@ -170,21 +175,6 @@ __device__ __forceinline__ Vec3 take_force(int a, const int32_t *__restrict__ pl
   return f;
 }
 
-// The excluded Ewald correction -f q_i q_j erf(beta r)/r of one pair in f64;
-// adds its force to fi and subtracts it from fj.
-__device__ __forceinline__ void excl_pair(const UpdateParams &U, Vec3 xi, Vec3 xj, double qq, Vec3 &fi, Vec3 &fj) {
-  Vec3 d = xi - xj;
-  d.x -= U.L[0] * rint(d.x / U.L[0]);
-  d.y -= U.L[1] * rint(d.y / U.L[1]);
-  d.z -= U.L[2] * rint(d.z / U.L[2]);
-  double r2 = dot(d, d);
-  if (qq == 0.0 || r2 <= 0.0) return;
-  double r = sqrt(r2);
-  double fs = qq * (U.two_beta_sqrtpi * exp(-U.beta * U.beta * r2) / r2 - erf(U.beta * r) / (r2 * r));
-  fi = fi + fs * d;
-  fj = fj - fs * d;
-}
-
 __device__ __forceinline__ void write_frame(int a, Vec3 x, const int32_t *__restrict__ place_of,
                                             const char4 *__restrict__ shift, const double *L, float4 *xq) {
   int p = place_of[a];
@@ -199,11 +189,23 @@ __device__ __forceinline__ void write_frame(int a, Vec3 x, const int32_t *__rest
 __device__ void md_last_block(const UpdateParams &U, const double *ke_part, int nblocks, double *thermo,
                               unsigned int *maxd2);
 
+__device__ __forceinline__ Vec3 shfl3(Vec3 a, int src) {
+  return {__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src), __shfl_sync(0xffffffffu, a.z, src)};
+}
+
 // One leap-frog step with SETTLE: v = lambda v + f/m dt; x += v dt;
-// constrain; v = (x_new - x_old)/dt.  A thread per water, then per free
-// atom, in small blocks so that the f64 work spreads over the SMs.  The
-// last block to finish sums the kinetic energy in a fixed order and runs
-// the thermostat and the tests of validity (md_last_block).
+// constrain; v = (x_new - x_old)/dt.
+//
+// Waters: a lane per atom, three neighbouring lanes per water (10 waters a
+// warp, lanes 30 and 31 idle), so that the loads of every atom are issued
+// at once and coalesced: the step is bound by two memory round trips (the
+// place of the atom, then its accumulators), not by a chain of them.  Lane k
+// of a water computes the excluded Ewald correction of the pair (k, k+1) in
+// f64, the lanes exchange positions and forces by shuffles, and each
+// evaluates SETTLE for its water (the same inputs, so the same result) and
+// writes its own atom.  Blocks past the waters take the free atoms, a thread
+// each.  The last block to finish sums the kinetic energy in a fixed order
+// and runs the thermostat and the tests of validity (md_last_block).
 __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     int64_t nwaters, int64_t nfree, const int32_t *__restrict__ waters, const int32_t *__restrict__ free_atoms,
     UpdateParams U, const double *__restrict__ inv_mass, const double *__restrict__ mass,
@@ -214,55 +216,102 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
   __shared__ double s_ke[MD_UPDATE_THREADS / 32];
   __shared__ float s_d2[MD_UPDATE_THREADS / 32], s_p2[MD_UPDATE_THREADS / 32];
   __shared__ int s_last;
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int WPB = MD_UPDATE_THREADS / 32 * 10;  // waters per block
+  int64_t water_blocks = (nwaters + WPB - 1) / WPB;
   double lambda = thermo[0];
   double dt = U.dt;
   double ke = 0.0;
   float d2max = 0.f, p2max = 0.f;
-  if (t < nwaters) {
-    int ia = waters[3 * t], ib = waters[3 * t + 1], ic = waters[3 * t + 2];
-    Vec3 a0 = load3(x, ia), b0 = load3(x, ib), c0 = load3(x, ic);
-    Vec3 fa = take_force(ia, place_of, acc, accf, pme, U.fixed);
-    Vec3 fb = take_force(ib, place_of, acc, accf, pme, U.fixed);
-    Vec3 fc = take_force(ic, place_of, acc, accf, pme, U.fixed);
-    if (U.water_excl) {
-      double qa = charge[ia], qb = charge[ib], qc = charge[ic];
-      excl_pair(U, a0, b0, U.coulomb * qa * qb, fa, fb);
-      excl_pair(U, a0, c0, U.coulomb * qa * qc, fa, fc);
-      excl_pair(U, b0, c0, U.coulomb * qb * qc, fb, fc);
+  if (blockIdx.x < water_blocks) {
+    int lane = threadIdx.x & 31, wl = lane / 3, k = lane - 3 * (lane / 3);
+    int64_t w = ((int64_t)blockIdx.x * (MD_UPDATE_THREADS / 32) + (threadIdx.x >> 5)) * 10 + wl;
+    bool act = lane < 30 && w < nwaters;
+    int a = act ? waters[3 * w + k] : 0;
+    int base = 3 * wl, s1 = base + (k + 1) % 3, s2 = base + (k + 2) % 3;
+    if (lane >= 30) s1 = s2 = base = lane;
+    // every independent load first
+    Vec3 x0 = load3(x, a), v0 = load3(v, a);
+    int p = act ? place_of[a] : -1;
+    double q = charge[a], im = inv_mass[a], ms = mass[a];
+    Vec3 xr = load3(x_ref, a);
+    Vec3 xpr = U.prune_half2 > 0.0 ? load3(x_prune, a) : xr;
+    Vec3 f = {0.0, 0.0, 0.0};
+    char4 sh = make_char4(0, 0, 0, 0);
+    float qw = 0.f;
+    if (p >= 0) {
+      if (U.fixed) {
+        long long fx = (long long)accf[3 * p], fy = (long long)accf[3 * p + 1], fz = (long long)accf[3 * p + 2];
+        f = {(double)fx * NB_FORCE_SCALE_INV, (double)fy * NB_FORCE_SCALE_INV, (double)fz * NB_FORCE_SCALE_INV};
+      } else {
+        float4 f4 = acc[p];
+        f = {f4.x, f4.y, f4.z};
+      }
+      if (pme) {
+        float4 w4 = pme[p];
+        f.x += w4.x;
+        f.y += w4.y;
+        f.z += w4.z;
+      }
+      sh = shift[p];
+      qw = xq[p].w;
     }
-    Vec3 va = lambda * load3(v, ia) + (dt * inv_mass[ia]) * fa;
-    Vec3 vb = lambda * load3(v, ib) + (dt * inv_mass[ib]) * fb;
-    Vec3 vc = lambda * load3(v, ic) + (dt * inv_mass[ic]) * fc;
-    Vec3 a1 = a0 + dt * va, b1 = b0 + dt * vb, c1 = c0 + dt * vc;
-    settle(U.S, a0, b0, c0, a1, b1, c1);
-    double inv_dt = 1.0 / dt;
-    va = inv_dt * (a1 - a0);
-    vb = inv_dt * (b1 - b0);
-    vc = inv_dt * (c1 - c0);
-    store3(x, ia, a1);
-    store3(x, ib, b1);
-    store3(x, ic, c1);
-    store3(v, ia, va);
-    store3(v, ib, vb);
-    store3(v, ic, vc);
-    store3(fout, ia, fa);
-    store3(fout, ib, fb);
-    store3(fout, ic, fc);
-    write_frame(ia, a1, place_of, shift, U.L, xq);
-    write_frame(ib, b1, place_of, shift, U.L, xq);
-    write_frame(ic, c1, place_of, shift, U.L, xq);
-    ke = 0.5 * (mass[ia] * dot(va, va) + mass[ib] * dot(vb, vb) + mass[ic] * dot(vc, vc));
-    Vec3 da = a1 - load3(x_ref, ia), db = b1 - load3(x_ref, ib), dc = c1 - load3(x_ref, ic);
-    d2max = (float)fmax(dot(da, da), fmax(dot(db, db), dot(dc, dc)));
-    if (U.prune_half2 > 0.0) {
-      da = a1 - load3(x_prune, ia);
-      db = b1 - load3(x_prune, ib);
-      dc = c1 - load3(x_prune, ic);
-      p2max = (float)fmax(dot(da, da), fmax(dot(db, db), dot(dc, dc)));
+    // the excluded pair (k, k+1) of this water
+    Vec3 x1 = shfl3(x0, s1);
+    double q1 = __shfl_sync(0xffffffffu, q, s1);
+    Vec3 fp = {0.0, 0.0, 0.0};
+    if (U.water_excl && act) {
+      Vec3 d = x0 - x1;
+      d.x -= U.L[0] * rint(d.x / U.L[0]);
+      d.y -= U.L[1] * rint(d.y / U.L[1]);
+      d.z -= U.L[2] * rint(d.z / U.L[2]);
+      double r2 = dot(d, d), qq = U.coulomb * q * q1;
+      if (qq != 0.0 && r2 > 0.0) {
+        double r = sqrt(r2);
+        double fs = qq * (U.two_beta_sqrtpi * exp(-U.beta * U.beta * r2) / r2 - erf(U.beta * r) / (r2 * r));
+        fp = fs * d;
+      }
     }
-  } else if (t < nwaters + nfree) {
-    int i = free_atoms[t - nwaters];
+    // this atom: + its own pair, - the pair (k-1, k) of the lane before
+    f = f + fp - shfl3(fp, s2);
+    // the three atoms of the water, in O, H, H order
+    Vec3 xa = shfl3(x0, base), xb = shfl3(x0, base + 1), xc = shfl3(x0, base + 2);
+    Vec3 va = shfl3(v0, base), vb = shfl3(v0, base + 1), vc = shfl3(v0, base + 2);
+    Vec3 fa = shfl3(f, base), fb = shfl3(f, base + 1), fc = shfl3(f, base + 2);
+    double ima = __shfl_sync(0xffffffffu, im, base), imb = __shfl_sync(0xffffffffu, im, base + 1),
+           imc = __shfl_sync(0xffffffffu, im, base + 2);
+    va = lambda * va + (dt * ima) * fa;
+    vb = lambda * vb + (dt * imb) * fb;
+    vc = lambda * vc + (dt * imc) * fc;
+    Vec3 a1 = xa + dt * va, b1 = xb + dt * vb, c1 = xc + dt * vc;
+    settle(U.S, xa, xb, xc, a1, b1, c1);
+    Vec3 xn = k == 0 ? a1 : (k == 1 ? b1 : c1);
+    if (act) {
+      Vec3 vn = (1.0 / dt) * (xn - x0);
+      store3(x, a, xn);
+      store3(v, a, vn);
+      store3(fout, a, f);
+      if (p >= 0) {
+        xq[p] = make_float4((float)(xn.x + sh.x * U.L[0]), (float)(xn.y + sh.y * U.L[1]),
+                            (float)(xn.z + sh.z * U.L[2]), qw);
+        if (U.fixed) {
+          accf[3 * p] = 0ull;
+          accf[3 * p + 1] = 0ull;
+          accf[3 * p + 2] = 0ull;
+        } else {
+          acc[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+      ke = 0.5 * ms * dot(vn, vn);
+      Vec3 dr = xn - xr;
+      d2max = (float)dot(dr, dr);
+      if (U.prune_half2 > 0.0) {
+        dr = xn - xpr;
+        p2max = (float)dot(dr, dr);
+      }
+    }
+  } else if ((int64_t)(blockIdx.x - water_blocks) * blockDim.x + threadIdx.x < nfree) {
+    int64_t t = (int64_t)(blockIdx.x - water_blocks) * blockDim.x + threadIdx.x;
+    int i = free_atoms[t];
     Vec3 fi = take_force(i, place_of, acc, accf, pme, U.fixed);
     Vec3 vi = lambda * load3(v, i) + (dt * inv_mass[i]) * fi;
     Vec3 xi = load3(x, i) + dt * vi;
@@ -341,14 +390,17 @@ __device__ double gamma_draw(double a, unsigned long long &ctr, unsigned long lo
   return a;
 }
 
-// The noise of the Bussi thermostat for the coming update: a normal R1 and
-// the sum of ndof - 1 squared normals (2 Gamma((ndof - 1)/2)), from the step
-// counter; off the critical path, on the side stream beside the pair kernel.
-__global__ void md_noise(double *thermo, double ndof, unsigned long long seed) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  unsigned long long ctr = (unsigned long long)thermo[3] * 1024ull;
-  thermo[6] = normal01(ctr, seed);
-  thermo[7] = ndof > 1.0 ? 2.0 * gamma_draw(0.5 * (ndof - 1.0), ctr, seed) : 0.0;
+// The noise of the Bussi thermostat for the next `count` steps, a thread
+// per step: a normal R1 and the sum of ndof - 1 squared normals
+// (2 Gamma((ndof - 1)/2)), from the step counter and the seed, so that a
+// step draws the same numbers however the steps are launched.  One launch
+// at the head of a replayed graph serves all its steps.
+__global__ void md_noise(const double *thermo, double *noise, int count, double ndof, unsigned long long seed) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  unsigned long long ctr = ((unsigned long long)thermo[3] + (unsigned long long)k) * 1024ull;
+  noise[2 * k] = normal01(ctr, seed);
+  noise[2 * k + 1] = ndof > 1.0 ? 2.0 * gamma_draw(0.5 * (ndof - 1.0), ctr, seed) : 0.0;
 }
 
 // The last block of md_update: the kinetic energy of the half step
@@ -378,7 +430,7 @@ __device__ void md_last_block(const UpdateParams &U, const double *ke_part, int 
     const double kB = 0.0083144626181532;
     double Kt = 0.5 * U.ndof * kB * U.temperature;
     double c = exp(-U.dt / U.tau);
-    double r1 = thermo[6], sum = thermo[7];
+    double r1 = U.noise[2 * U.k], sum = U.noise[2 * U.k + 1];
     double Knew = K + (1.0 - c) * (Kt * (r1 * r1 + sum) / U.ndof - K) + 2.0 * r1 * sqrt(c * (1.0 - c) * K * Kt / U.ndof);
     lambda = sqrt(fmax(Knew, 0.0) / K);
   }
@@ -390,14 +442,17 @@ __device__ void md_last_block(const UpdateParams &U, const double *ke_part, int 
   maxd2[0] = 0u;
   maxd2[1] = 0u;
   maxd2[2] = 0u;
-  if (U.flag) {
-    U.flag[0] = rebuild;
-    U.flag[1] = prune;
-  }
-  if (U.use_graph) {
-    cudaGraphSetConditional(U.h_build, rebuild);
-    if (U.prune_half2 > 0.0) cudaGraphSetConditional(U.h_prune, prune);
-  }
+  U.flag[0] = rebuild;
+  U.flag[1] = prune;
+  if (U.use_graph) cudaGraphSetConditional(U.h_any, rebuild | prune);
+}
+
+// The first node of the body of a step's conditional node: which of the
+// rebuild and the pruning it runs.
+__global__ void md_set_inner(const int *flag, cudaGraphConditionalHandle h_build, cudaGraphConditionalHandle h_prune,
+                             int dual) {
+  cudaGraphSetConditional(h_build, flag[0]);
+  if (dual) cudaGraphSetConditional(h_prune, flag[1]);
 }
 
 // After a build: the reference positions and the counters.
@@ -437,19 +492,23 @@ static SettleParams settle_params(const mdrtMd &m) {
 
 // One step on `s` from the frames xq of the current positions x.
 static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], double dt, cudaStream_t s,
-                         cudaGraphConditionalHandle h_build, cudaGraphConditionalHandle h_prune, int use_graph,
-                         int *flag) {
+                         cudaGraphConditionalHandle h_any, int use_graph, int *flag, int k) {
   NbCtx &c = *m.nb;
   bool pme = c.pme.on && c.beta > 0.0;
-  cudaEventRecord(m.ev_fork, s);
-  cudaStreamWaitEvent(m.side, m.ev_fork, 0);
-  md_noise<<<1, 32, 0, m.side>>>(m.thermo, (double)m.ndof, m.seed);
-  if (pme) nb_pme_run(c, box, false, false, m.side);
+  if (pme) {
+    cudaEventRecord(m.ev_fork, s);
+    cudaStreamWaitEvent(m.side, m.ev_fork, 0);
+    nb_pme_run(c, box, false, false, m.side);
+  }
   nb_pairs_run(c, box, false, s);
   if (m.n_excl_other > 0) nb_excluded_list_run(c, box, m.excl_other, m.n_excl_other, s);
-  cudaEventRecord(m.ev_join, m.side);
-  cudaStreamWaitEvent(s, m.ev_join, 0);
+  if (pme) {
+    cudaEventRecord(m.ev_join, m.side);
+    cudaStreamWaitEvent(s, m.ev_join, 0);
+  }
   UpdateParams U;
+  U.noise = m.noise;
+  U.k = k;
   U.S = settle_params(m);
   U.dt = dt;
   for (int k = 0; k < 3; ++k) U.L[k] = box[k];
@@ -465,8 +524,7 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
   U.build_half2 = half * half;
   double half_in = 0.5 * (c.inner_reach - c.cutoff);
   U.prune_half2 = c.inner_reach > 0.0 ? half_in * half_in : 0.0;
-  U.h_build = h_build;
-  U.h_prune = h_prune;
+  U.h_any = h_any;
   U.use_graph = use_graph;
   U.flag = flag;
   md_update<<<m.ke_blocks, MD_UPDATE_THREADS, 0, s>>>(
@@ -505,7 +563,8 @@ static void md_free(mdrtMd *m) {
   if (m->side) cudaStreamDestroy(m->side);
   for (void *p : {(void *)m->inv_mass, (void *)m->mass, (void *)m->waters, (void *)m->free_atoms,
                   (void *)m->excl_other, (void *)m->force, (void *)m->x_ref, (void *)m->x_prune,
-                  (void *)m->ke_part, (void *)m->maxd2, (void *)m->thermo, (void *)m->flag})
+                  (void *)m->ke_part, (void *)m->maxd2, (void *)m->thermo, (void *)m->flag,
+                  (void *)m->noise})
     if (p) cudaFree(p);
   delete m;
 }
@@ -580,7 +639,10 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
     inv[i] = 1.0 / masses[i];
   }
   m->ndof = 3 * c.n - 3 * nwaters - 3;
-  m->ke_blocks = blocks_for(nwaters + m->nfree, MD_UPDATE_THREADS);
+  // blocks of waters (10 a warp), then blocks of free atoms (one a thread)
+  m->ke_blocks = (int)((nwaters + MD_UPDATE_THREADS / 32 * 10 - 1) / (MD_UPDATE_THREADS / 32 * 10) +
+                       (m->nfree + MD_UPDATE_THREADS - 1) / MD_UPDATE_THREADS);
+  if (m->ke_blocks < 1) m->ke_blocks = 1;
   int lo = 0, hi = 0;
   cudaDeviceGetStreamPriorityRange(&lo, &hi);
   bool ok = cudaMalloc(&m->inv_mass, sizeof(double) * c.n) == cudaSuccess &&
@@ -594,6 +656,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
             cudaMalloc(&m->ke_part, sizeof(double) * m->ke_blocks) == cudaSuccess &&
             cudaMalloc(&m->maxd2, sizeof(unsigned int) * 4) == cudaSuccess &&
             cudaMalloc(&m->thermo, sizeof(double) * 8) == cudaSuccess &&
+            cudaMalloc(&m->noise, sizeof(double) * 2 * MD_MAX_UNROLL) == cudaSuccess &&
             cudaMalloc(&m->flag, sizeof(int) * 2) == cudaSuccess &&
             cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, hi) == cudaSuccess &&
             cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
@@ -685,7 +748,7 @@ extern "C" {
 
 int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
                   int32_t unroll, void *stream) {
-  if (!m || !x || !v || !box || !(dt > 0) || steps < 0) return MDRT_NB_INVALID_ARGUMENT;
+  if (!m || !x || !v || !box || !(dt > 0) || steps < 0 || unroll > MD_MAX_UNROLL) return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = *m->nb;
   if (!c.built) return MDRT_NB_NOT_BUILT;
   for (int k = 0; k < 3; ++k)
@@ -696,7 +759,8 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
     // step by step, the host reading the tests of validity after each step
     int h_flag[2] = {0, 0};
     for (int64_t k = 0; k < steps; ++k) {
-      md_step_body(*m, x, v, box, dt, st, 0, 0, 0, m->flag);
+      md_noise<<<1, 32, 0, st>>>(m->thermo, m->noise, 1, (double)m->ndof, m->seed);
+      md_step_body(*m, x, v, box, dt, st, 0, 0, m->flag, 0);
       cudaMemcpyAsync(h_flag, m->flag, sizeof(h_flag), cudaMemcpyDeviceToHost, st);
       cudaStreamSynchronize(st);
       if (h_flag[0]) {
@@ -716,28 +780,45 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
                m->gbox[0] != box[0] || m->gbox[1] != box[1] || m->gbox[2] != box[2] || m->gcap_key != key;
   if (stale) {
     md_drop_graph(m);
-    cudaStream_t cap, body;
+    // Each step ends in one conditional node, taken when a rebuild or a
+    // pruning is due (about one step in three); its body sets and runs two
+    // nested ones, the rebuild and the pruning.
+    cudaStream_t cap, body, inner;
     cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
     cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&inner, cudaStreamNonBlocking);
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     bool dual = c.inner_reach > 0.0;
-    m->handles.assign(2 * unroll, 0);
+    m->handles.assign(unroll, 0);
+    if (e == cudaSuccess)
+      md_noise<<<(unroll + 31) / 32, 32, 0, cap>>>(m->thermo, m->noise, unroll, (double)m->ndof, m->seed);
     for (int k = 0; k < unroll && e == cudaSuccess; ++k) {
       cudaStreamCaptureStatus status;
       cudaGraph_t g;
       e = cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, nullptr, nullptr);
       if (e != cudaSuccess) break;
-      e = cudaGraphConditionalHandleCreate(&m->handles[2 * k], g, 0, cudaGraphCondAssignDefault);
-      if (e == cudaSuccess && dual)
-        e = cudaGraphConditionalHandleCreate(&m->handles[2 * k + 1], g, 0, cudaGraphCondAssignDefault);
+      e = cudaGraphConditionalHandleCreate(&m->handles[k], g, 0, cudaGraphCondAssignDefault);
       if (e != cudaSuccess) break;
-      md_step_body(*m, x, v, box, dt, cap, m->handles[2 * k], m->handles[2 * k + 1], 1, nullptr);
-      e = md_capture_if(cap, body, m->handles[2 * k], [&](cudaStream_t b) { md_rebuild_body(*m, x, box, b); });
-      if (e == cudaSuccess && dual)
-        e = md_capture_if(cap, body, m->handles[2 * k + 1], [&](cudaStream_t b) { md_prune_body(*m, x, box, b); });
+      md_step_body(*m, x, v, box, dt, cap, m->handles[k], 1, m->flag, k);
+      cudaError_t ei = cudaSuccess;
+      e = md_capture_if(cap, body, m->handles[k], [&](cudaStream_t b) {
+        cudaStreamCaptureStatus bs;
+        cudaGraph_t bg;
+        cudaGraphConditionalHandle hb = 0, hp = 0;
+        ei = cudaStreamGetCaptureInfo(b, &bs, nullptr, &bg, nullptr, nullptr);
+        if (ei == cudaSuccess) ei = cudaGraphConditionalHandleCreate(&hb, bg, 0, cudaGraphCondAssignDefault);
+        if (ei == cudaSuccess && dual) ei = cudaGraphConditionalHandleCreate(&hp, bg, 0, cudaGraphCondAssignDefault);
+        if (ei != cudaSuccess) return;
+        md_set_inner<<<1, 1, 0, b>>>(m->flag, hb, hp, dual ? 1 : 0);
+        ei = md_capture_if(b, inner, hb, [&](cudaStream_t ib) { md_rebuild_body(*m, x, box, ib); });
+        if (ei == cudaSuccess && dual)
+          ei = md_capture_if(b, inner, hp, [&](cudaStream_t ib) { md_prune_body(*m, x, box, ib); });
+      });
+      if (e == cudaSuccess) e = ei;
     }
     cudaGraph_t graph = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+    cudaStreamDestroy(inner);
     cudaStreamDestroy(body);
     cudaStreamDestroy(cap);
     if (e != cudaSuccess || e2 != cudaSuccess) {

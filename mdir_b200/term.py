@@ -102,6 +102,11 @@ class NonbondedTerm:
         b = _host(self.box if box is None else box, np.float64)
         L.check(L.lib().mdrtNbPrune(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtNbPrune")
 
+    def set_tuning(self, pair_blocks_per_sm=None):
+        """Launch shapes (the autotuner's knobs); results do not depend on them."""
+        if pair_blocks_per_sm is not None:
+            L.check(L.lib().mdrtNbSetTuning(self._h, 0, int(pair_blocks_per_sm)), "mdrtNbSetTuning")
+
     def set_deterministic(self, on=True):
         L.check(L.lib().mdrtNbSetDeterministic(self._h, int(bool(on))), "mdrtNbSetDeterministic")
 
