@@ -100,7 +100,7 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   NbCtx &c = ctx->c;
   cudaSetDevice(c.device);
   nb_pme_release(c);
-  nb_free(c.q); nb_free(c.type); nb_free(c.lj);
+  nb_free(c.q); nb_free(c.type); nb_free(c.lj); nb_free(c.ljf);
   nb_free(c.excl_off); nb_free(c.excl); nb_free(c.excl_pairs); nb_free(c.excl_partials);
   nb_free(c.order); nb_free(c.place_of); nb_free(c.shift); nb_free(c.xw);
   nb_free(c.box_lo); nb_free(c.box_hi); nb_free(c.group_start); nb_free(c.group_col);
@@ -136,10 +136,32 @@ int32_t mdrtNbSetParticles(mdrtNb *ctx, const double *charges, const int32_t *ty
     c.h_c6[a] = 4.0 * epsilon[a] * s6;
     c.h_lj[a] = make_float2((float)(4.0 * epsilon[a] * s6), (float)(4.0 * epsilon[a] * s6 * s6));
   }
+  // Does the table factorize, c_ab = sqrt(c_aa c_bb) for both c6 and c12
+  // (one LJ type, or geometric mixing)?  Then the pair kernel multiplies
+  // per-type factors instead of looking the pair up.
+  std::vector<float2> factors(ntypes);
+  bool geom = true;
+  for (int a = 0; a < ntypes; ++a) {
+    double c6 = c.h_c6[a * ntypes + a], c12 = 4.0 * epsilon[a * ntypes + a] * std::pow(sigma[a * ntypes + a], 12.0);
+    if (c6 < 0 || c12 < 0) geom = false;
+    factors[a] = make_float2((float)std::sqrt(std::max(c6, 0.0)), (float)std::sqrt(std::max(c12, 0.0)));
+  }
+  for (int a = 0; a < ntypes && geom; ++a)
+    for (int b = 0; b < ntypes && geom; ++b) {
+      double c6 = c.h_c6[a * ntypes + b];
+      double c12 = 4.0 * epsilon[a * ntypes + b] * std::pow(sigma[a * ntypes + b], 12.0);
+      double g6 = (double)factors[a].x * factors[b].x, g12 = (double)factors[a].y * factors[b].y;
+      if (std::fabs(c6 - g6) > 1e-6 * std::fabs(c6) + 1e-30 || std::fabs(c12 - g12) > 1e-6 * std::fabs(c12) + 1e-30)
+        geom = false;
+    }
+  c.lj_geom = geom;
   std::vector<float> qf(charges, charges + c.n);
   if (!c.q) CK(cudaMalloc(&c.q, sizeof(float) * c.n));
   if (!c.type) CK(cudaMalloc(&c.type, sizeof(int32_t) * c.n));
   nb_free(c.lj);
+  nb_free(c.ljf);
+  CK(cudaMalloc(&c.ljf, sizeof(float2) * ntypes));
+  CK(cudaMemcpy(c.ljf, factors.data(), sizeof(float2) * ntypes, cudaMemcpyHostToDevice));
   CK(cudaMalloc(&c.lj, sizeof(float2) * ntypes * ntypes));
   CK(cudaMemcpy(c.q, qf.data(), sizeof(float) * c.n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c.type, types, sizeof(int32_t) * c.n, cudaMemcpyHostToDevice));

@@ -40,6 +40,8 @@ struct NbCtx {
   int32_t *type = nullptr;
   int32_t ntypes = 0;
   float2 *lj = nullptr;  // (c6, c12) per type pair, c6 = 4 eps sig^6, c12 = 4 eps sig^12
+  float2 *ljf = nullptr;  // per type (sqrt c6, sqrt c12) when the table factorizes
+  bool lj_geom = false;   // c6_ab = f_a f_b and c12_ab = g_a g_b for every pair of types
   std::vector<double> h_q;     // f64 charges for the host constants
   std::vector<double> h_c6;    // f64 c6 = 4 eps sig^6 per type pair
   std::vector<int32_t> h_type;

@@ -68,25 +68,39 @@ __device__ __forceinline__ void nb_red_fixed(unsigned long long *addr, float x, 
   atomicAdd(addr + 2, (unsigned long long)__float2ll_rn(z * 4294967296.0f));
 }
 
-template <bool ENERGY, bool FIXED, bool SWITCH>
+// LJM selects the Lennard-Jones coefficients: 0, a (c6, c12) table by type
+// pair in shared memory; 1, the product of per-type factors (sqrt c6,
+// sqrt c12), exact when the table factorizes (one LJ type, or geometric
+// mixing), which needs no dependent lookup.  The members live twice in
+// shared memory (slots u and u + 16), so that lane l reads member
+// (l + k) mod 16 at slot l mod 16 + k: an immediate offset in the unrolled
+// loop, no index arithmetic.
+template <bool ENERGY, bool FIXED, bool SWITCH, int LJM>
 __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const int32_t *__restrict__ sizes,
                                                 const int2 *__restrict__ units,
                                                 const int2 *__restrict__ slab,
                                                 const int32_t *__restrict__ counts,
                                                 const float4 *__restrict__ xq,
                                                 const int32_t *__restrict__ typ,
-                                                const float2 *__restrict__ lj, float4 *__restrict__ acc,
-                                                unsigned long long *__restrict__ accf,
+                                                const float2 *__restrict__ lj, const float2 *__restrict__ ljf,
+                                                float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
                                                 double *__restrict__ partials, int *__restrict__ status) {
-  __shared__ float4 s_x[8][NB_GROUP];
-  __shared__ int s_t[8][NB_GROUP];
-  __shared__ float2 s_lj[NB_MAX_TYPES * NB_MAX_TYPES];
+  __shared__ float4 s_x[8][2 * NB_GROUP];
+  __shared__ float2 s_f[8][2 * NB_GROUP];  // LJM 1: member factors
+  __shared__ int s_t[8][2 * NB_GROUP];     // LJM 0: member row offsets in s_lj
+  __shared__ float2 s_lj[LJM == 0 ? NB_MAX_TYPES * NB_MAX_TYPES : 1];
   const unsigned FULL = 0xffffffffu;
-  int nt2 = P.ntypes * P.ntypes;
-  for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = lj[k];
-  __syncthreads();
+  if (LJM == 0) {
+    int nt2 = P.ntypes * P.ntypes;
+    for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = lj[k];
+    __syncthreads();
+  }
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int u = lane & 15;
+  const int src = (lane & 16) | ((lane + 1) & 15);  // the lane the member accumulators come from
+  const float4 *px = &s_x[warp][u];
+  const float2 *pf = &s_f[warp][u];
+  const int *pt = &s_t[warp][u];
   int nunits = min((int64_t)sizes[NB_SIZE_UNITS], P.units_cap);
   int wstride = gridDim.x * 8;
   for (int unit = blockIdx.x * 8 + warp; unit < nunits; unit += wstride) {
@@ -94,11 +108,15 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const int32_t *
     int g = uo.x;
     int64_t pi = (int64_t)g * NB_GROUP + u;
     __syncwarp();
-    if (lane < 16) {
+    {
       float4 xi = xq[pi];
       xi.w *= P.coulomb;
-      s_x[warp][u] = xi;
-      s_t[warp][u] = typ[pi] * P.ntypes;
+      int ti = typ[pi];
+      s_x[warp][lane] = xi;
+      if (LJM == 1)
+        s_f[warp][lane] = ljf[ti];
+      else
+        s_t[warp][lane] = ti * P.ntypes;
     }
     __syncwarp();
     int cnt = (int)min((int64_t)counts[g], P.list_cap);
@@ -121,16 +139,24 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const int32_t *
       xj.y += (float)sy * P.Ly;
       xj.z += (float)sz * P.Lz;
       int tj = typ[q];
+      float2 fj = LJM == 1 ? ljf[tj] : make_float2(0.f, 0.f);
+      // bit k of mrot: the pair of this lane's entry with member (lane + k) mod 16
+      unsigned mrot = ((mask >> u) | (mask << (16 - u))) & 0xffffu;
       float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-#pragma unroll 4
+#pragma unroll
       for (int k = 0; k < NB_GROUP; ++k) {
-        int m = (lane + k) & 15;
-        float4 xm = s_x[warp][m];
+        float4 xm = px[k];
         float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
         float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        bool inside = ((mask >> m) & 1u) && (r2 < P.rc2);
+        bool inside = (mrot & (1u << k)) && (r2 < P.rc2);
         float r2s = inside ? r2 : 1.0f;
-        float2 cc = s_lj[s_t[warp][m] + tj];
+        float2 cc;
+        if (LJM == 1) {
+          float2 fm = pf[k];
+          cc = make_float2(fm.x * fj.x, fm.y * fj.y);
+        } else {
+          cc = s_lj[pt[k] + tj];
+        }
         float rinv = rsqrtf(r2s);
         float rinv2 = rinv * rinv;
         float s6 = rinv2 * rinv2 * rinv2;
@@ -169,7 +195,6 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const int32_t *
           vxz = fmaf(dx, fz, vxz);
           vyz = fmaf(dy, fz, vyz);
         }
-        int src = (lane & 16) | ((lane + 1) & 15);
         ax = __shfl_sync(FULL, ax, src);
         ay = __shfl_sync(FULL, ay, src);
         az = __shfl_sync(FULL, az, src);
@@ -424,9 +449,16 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
   const int2 *lunits = inner ? c.units_in : c.units;
   const int2 *lslab = inner ? c.slab_in : c.slab;
   const int32_t *lcounts = inner ? c.counts_in : c.counts;
-#define NB_LAUNCH(E, F, S)                                                                          \
-  nb_pairs<E, F, S><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, c.acc, \
-                                        c.acc_fixed, c.unit_partials, c.status)
+#define NB_LAUNCH2(E, F, S, M)                                                                      \
+  nb_pairs<E, F, S, M><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, c.ljf, \
+                                           c.acc, c.acc_fixed, c.unit_partials, c.status)
+#define NB_LAUNCH(E, F, S)      \
+  do {                          \
+    if (c.lj_geom)              \
+      NB_LAUNCH2(E, F, S, 1);   \
+    else                        \
+      NB_LAUNCH2(E, F, S, 0);   \
+  } while (0)
   bool F = c.deterministic, S = c.lj_switch != 0;
   if (energy) {
     if (F) { if (S) NB_LAUNCH(true, true, true); else NB_LAUNCH(true, true, false); }
@@ -436,6 +468,7 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
     else { if (S) NB_LAUNCH(false, false, true); else NB_LAUNCH(false, false, false); }
   }
 #undef NB_LAUNCH
+#undef NB_LAUNCH2
 }
 
 void nb_excluded_list_run(NbCtx &c, const double box[3], const int32_t *pairs, int64_t npairs,
