@@ -246,6 +246,32 @@ int32_t mdrtMdThermo(mdrtMd *md, void *stream, double *out);
 /* The device array of the forces of the last step (f64 [n, 3]). */
 int32_t mdrtMdForces(mdrtMd *md, double **forces);
 
+/* ---- An entry point that allocates nothing -------------------------------
+ * mdrtNbExcludedNoAlloc: the excluded-pair Ewald correction
+ * -f q_i q_j erf(beta r)/r over `npairs` pairs (device int32 [npairs][2],
+ * i < j), in f64 from device positions x (f64 [n, 3]) and charges (f64 [n]),
+ * in the orthorhombic cell box[3] (host).  Adds the forces to `forces`
+ * (device f64 [n, 3]) and writes the energy and the virial (xx yy zz xy xz
+ * yz) to energy_virial (device f64 [7]); asynchronous on `stream`.
+ *
+ * For callers that cannot allocate device memory: code recording a CUDA
+ * graph by stream capture (cudaMalloc cannot be captured), hosts that own all
+ * device memory through a fixed pool, and loops that must not pay the device
+ * synchronization of cudaFree.  It calls no cudaMalloc, cudaFree or
+ * allocating library routine: its scratch (the per-block partial sums) is a
+ * fixed __device__ array of the library, held on every GPU that loads it
+ * until the process exits.  More than MDRT_NB_NOALLOC_MAX_PAIRS pairs is
+ * refused with MDRT_NB_INVALID_ARGUMENT (and a message on stderr).  The
+ * first call on a device looks up the array's device address (a runtime
+ * query, no allocation); make that first call before any stream capture.
+ * Calls share the array: two calls that overlap on the GPU race.
+ * No counterpart in MDIR; the allocating path is mdrtNbForce with
+ * MDRT_NB_NO_PAIRS | MDRT_NB_NO_PME. */
+#define MDRT_NB_NOALLOC_MAX_PAIRS (1 << 20)
+int32_t mdrtNbExcludedNoAlloc(const double *x, const double *charges, const int32_t *pairs, int64_t npairs,
+                              const double box[3], double beta, double coulomb, double *forces,
+                              double *energy_virial, void *stream);
+
 /* 3D real FFTs of a grid in f32 on `stream`, plans cached per size.
  * MDIR: _mlir_ciface_mdrtCudaFFTForward3DF32 / Backward3DF32
  * (runtime/mdrt_cuda.c:2942-2979), with plain pointers.  The backward

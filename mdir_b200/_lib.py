@@ -52,6 +52,7 @@ SIGNATURES = {
     "mdrtMdRun": (_i32, [_p, _p, _p, _p, _d, _i64, _i32, _p]),
     "mdrtMdThermo": (_i32, [_p, _p, _p]),
     "mdrtMdForces": (_i32, [_p, ctypes.POINTER(_p)]),
+    "mdrtNbExcludedNoAlloc": (_i32, [_p, _p, _p, _i64, _p, _d, _d, _p, _p, _p]),
     "mdrtCudaFFTForward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
     "mdrtCudaFFTBackward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
 }
