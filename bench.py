@@ -31,6 +31,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 DT_PS = 0.002
+PAIRS_TRAFFIC_BYTES = 6.19e6  # ncu dram__bytes_read.sum + dram__bytes_write.sum of nb_pairs, 23,550 atoms
 METRIC = "ns/day water box (TIP3P 23,550 atoms, PME, SETTLE, NVT, 2 fs)"
 
 
@@ -303,7 +304,10 @@ def main():
     achieved = pairs * flop_per_pair / (times[1] * 1e-3) / 1e12
     roofline = {"bound": "fp32", "kernel": "nb_pairs", "achieved": round(achieved, 3),
                 "peak": round(peak_fp32, 2), "unit": "TFLOP/s", "frac": round(achieved / peak_fp32, 4),
-                "traffic": None, "pairs_within_cutoff": pairs, "flop_per_pair": flop_per_pair,
+                # DRAM bytes read + written per launch of nb_pairs on this
+                # workload, from one ncu capture (profiles/nb_pairs_tip3p23550.md)
+                "traffic": PAIRS_TRAFFIC_BYTES if args.waters == 7850 else None,
+                "pairs_within_cutoff": pairs, "flop_per_pair": flop_per_pair,
                 "launch_ms": round(times[1], 5),
                 "peak_note": "nominal FP32 = SMs x 128 x 2 x max SM clock (no measured FP32 peak exists)",
                 "stage_ms": {"gather": round(times[0], 5), "pairs": round(times[1], 5),

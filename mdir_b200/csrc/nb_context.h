@@ -104,7 +104,7 @@ struct NbCtx {
   int32_t *sizes_in = nullptr;  // NB_SIZE_UNITS of the inner list (device)
   int64_t prunes = 0;
   // tuning (mdrtNbSetTuning): blocks of 8 warps per SM of the pair kernel
-  int pair_blocks_per_sm = 3;
+  int pair_blocks_per_sm = 4;
 };
 
 // Energy / virial slots of ctx->energy (f64, device).
