@@ -188,6 +188,43 @@ int32_t mdrtNbConstants(mdrtNb *ctx, const double box[3], int32_t dispersion, do
  * potential (device f64 [n]).  MDIR: the PME potential stage (D231). */
 int32_t mdrtPmePotential(mdrtNb *ctx, double *potential, void *stream);
 
+/* The largest displacement (nm, minimum image) of each of `count` frames
+ * (device f64 [count, n, 3]) from the positions of the last build, to out
+ * (host f64 [count]); +inf for a frame with a coordinate that is not
+ * finite.  The lists of the build serve a frame while 2 out[f] stays below
+ * reach - cutoff.  Waits for `stream`.
+ * MDIR: the skin test of the drift (ExposeValidity.cpp;
+ * docs/neighbor-groups.md, Section 7.1), here over a batch of frames. */
+int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, const double box[3],
+                           double *out, void *stream);
+
+/* Modes of mdrtNbParameterGradient. */
+enum mdrtNbGradientMode {
+  MDRT_NB_GRAD_PRODUCT = 0,  /* sum_k g_k . dF_k/dtheta for a cotangent g on the forces */
+  MDRT_NB_GRAD_ENERGY = 1    /* dE/dtheta (pairs, excluded, reciprocal, self, background) */
+};
+
+/* The gradient of the term in its parameters at device positions x (f64
+ * [n, 3]) with the lists of the last build (valid for x, box unchanged):
+ * the charges of the atoms and the sigma / epsilon entries of the type-pair
+ * table.  Adds dq_i to dq (device f64 [n], atom order) and d/dsigma_ab,
+ * d/depsilon_ab to dtable (device f64 [2 ntypes^2]: the ntypes^2 sigma
+ * entries, row-major by type pair, then the epsilon entries); both are
+ * accumulated, so that frames add up.  MDRT_NB_GRAD_PRODUCT reads the
+ * cotangent g (device f64 [n, 3], on the forces F = -dE/dx); for a loss
+ * (1/K) sum |F - F_ref|^2, g = (2/K)(F - F_ref).  MDRT_NB_GRAD_ENERGY
+ * ignores it and leaves out the dispersion correction, a host function of
+ * the table.  The pair geometry is recomputed, not stored.  Refuses the
+ * switched LJ form (MDRT_NB_UNSUPPORTED).  Asynchronous on `stream`.
+ * MDIR: the force-matching product FrameEnergies.vjp(positions=)
+ * (python/mdir/_frames.py:327, docs/python-frames.md:203-260, D381; its
+ * cotangent is on dE/dx = -F) and the gradient in the tunables
+ * (docs/python-gradient.md, D376), whose product refuses per-atom charges
+ * with PME (D379); here they are given. */
+int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3],
+                                const double *cotangent, int32_t mode, double *dq,
+                                double *dtable, void *stream);
+
 /* A device pointer to a buffer of the neighbor structure and its element
  * count (a view; invalidated by the next build that grows).
  * MDIR: _mlir_ciface_mdrtGroupsBuffer(result, handle, slot),

@@ -9,4 +9,5 @@ from . import systems  # noqa: F401
 from .api import (CompileError, Electrostatics, Ensemble, EnsembleKind, Execution, InitialState,  # noqa: F401
                   InputError, Integrator, Precision, Program, Schedule, Simulation, SimulationError,
                   System, Target, Truncation, UnsupportedError, compile)
+from .frames import FrameEnergies, FrameEvaluator  # noqa: F401
 from .term import COULOMB, NonbondedTerm, exclusion_rows  # noqa: F401

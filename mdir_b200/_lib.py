@@ -18,6 +18,7 @@ SIZE_PLACES, SIZE_LONGEST, SIZE_UNITS, SIZE_EXCL_WIDE, SIZE_NAN, SIZE_OVERFLOW, 
     SIZE_ENTRIES, SIZE_COUNT = range(9)
 SLOT_ORDER, SLOT_COUNTS, SLOT_ENTRIES, SLOT_UNITS, SLOT_SHIFTS, SLOT_PLACED, SLOT_PLACE_OF = \
     0, 1, 2, 4, 6, 15, 16
+GRAD_PRODUCT, GRAD_ENERGY = 0, 1
 
 _lib = None
 
@@ -41,6 +42,8 @@ SIGNATURES = {
     "mdrtNbEnergies": (_i32, [_p, _p, _p]),
     "mdrtNbConstants": (_i32, [_p, _p, _i32, _p]),
     "mdrtPmePotential": (_i32, [_p, _p, _p]),
+    "mdrtNbDisplacement": (_i32, [_p, _p, _i64, _p, _p, _p]),
+    "mdrtNbParameterGradient": (_i32, [_p, _p, _p, _p, _i32, _p, _p, _p]),
     "mdrtNbGroupsBuffer": (_i32, [_p, _i32, ctypes.POINTER(_p), ctypes.POINTER(_i64)]),
     "mdrtNbGroupsInfo": (_i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "mdrtNbStatus": (_i32, [_p, _p, _i32, ctypes.POINTER(_i32)]),

@@ -41,6 +41,26 @@ int check_box(const NbCtx &c, const double box[3]) {
   return MDRT_NB_OK;
 }
 
+// The squared largest displacement of frame blockIdx.y from the positions of
+// the last build, under the minimum image, as the bits of a non-negative
+// double (which order like the integers); a coordinate that is not finite
+// counts as infinitely far.
+__global__ void nb_frame_drift(int64_t n, const double *__restrict__ frames, const double *__restrict__ ref,
+                               double Lx, double Ly, double Lz, unsigned long long *__restrict__ out) {
+  const double *x = frames + (int64_t)blockIdx.y * 3 * n;
+  double m = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double d0 = x[3 * i] - ref[3 * i], d1 = x[3 * i + 1] - ref[3 * i + 1], d2 = x[3 * i + 2] - ref[3 * i + 2];
+    d0 -= Lx * rint(d0 / Lx);
+    d1 -= Ly * rint(d1 / Ly);
+    d2 -= Lz * rint(d2 / Lz);
+    double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+    m = r2 == r2 ? fmax(m, r2) : INFINITY;
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out + blockIdx.y, (unsigned long long)__double_as_longlong(m));
+}
+
 }  // namespace
 
 extern "C" {
@@ -100,7 +120,8 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   NbCtx &c = ctx->c;
   cudaSetDevice(c.device);
   nb_pme_release(c);
-  nb_free(c.q); nb_free(c.type); nb_free(c.lj); nb_free(c.ljf);
+  nb_free(c.q); nb_free(c.type); nb_free(c.lj); nb_free(c.ljf); nb_free(c.sigeps);
+  nb_free(c.adj_g); nb_free(c.adj_q); nb_free(c.adj_types); nb_free(c.x_build); nb_free(c.drift);
   nb_free(c.excl_off); nb_free(c.excl); nb_free(c.excl_pairs); nb_free(c.excl_partials);
   nb_free(c.order); nb_free(c.place_of); nb_free(c.shift); nb_free(c.xw);
   nb_free(c.box_lo); nb_free(c.box_hi); nb_free(c.group_start); nb_free(c.group_col);
@@ -131,7 +152,9 @@ int32_t mdrtNbSetParticles(mdrtNb *ctx, const double *charges, const int32_t *ty
   c.h_type.assign(types, types + c.n);
   c.h_lj.resize((size_t)ntypes * ntypes);
   c.h_c6.resize((size_t)ntypes * ntypes);
+  std::vector<float2> se((size_t)ntypes * ntypes);
   for (int a = 0; a < ntypes * ntypes; ++a) {
+    se[a] = make_float2((float)sigma[a], (float)epsilon[a]);
     double s6 = std::pow(sigma[a], 6.0);
     c.h_c6[a] = 4.0 * epsilon[a] * s6;
     c.h_lj[a] = make_float2((float)(4.0 * epsilon[a] * s6), (float)(4.0 * epsilon[a] * s6 * s6));
@@ -163,6 +186,9 @@ int32_t mdrtNbSetParticles(mdrtNb *ctx, const double *charges, const int32_t *ty
   CK(cudaMalloc(&c.ljf, sizeof(float2) * ntypes));
   CK(cudaMemcpy(c.ljf, factors.data(), sizeof(float2) * ntypes, cudaMemcpyHostToDevice));
   CK(cudaMalloc(&c.lj, sizeof(float2) * ntypes * ntypes));
+  nb_free(c.sigeps);
+  CK(cudaMalloc(&c.sigeps, sizeof(float2) * ntypes * ntypes));
+  CK(cudaMemcpy(c.sigeps, se.data(), sizeof(float2) * ntypes * ntypes, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c.q, qf.data(), sizeof(float) * c.n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c.type, types, sizeof(int32_t) * c.n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c.lj, c.h_lj.data(), sizeof(float2) * ntypes * ntypes, cudaMemcpyHostToDevice));
@@ -300,6 +326,8 @@ int32_t mdrtNbBuild(mdrtNb *ctx, const double *x, int64_t n, const double box[3]
   CK(cudaSetDevice(c.device));
   cudaStream_t st = (cudaStream_t)stream;
   if (nb_build_run(c, x, box, st)) return MDRT_NB_CUDA_ERROR;
+  if (!c.x_build) CK(cudaMalloc(&c.x_build, sizeof(double) * 3 * c.n));
+  CK(cudaMemcpyAsync(c.x_build, x, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToDevice, st));
   if (sizes_out)
     for (int k = 0; k < NB_SIZE_COUNT; ++k) sizes_out[k] = c.h_sizes[k];
   if (c.h_sizes[NB_SIZE_NAN] > 0) return MDRT_NB_NAN_POSITION;
@@ -333,6 +361,59 @@ int32_t mdrtNbForce(mdrtNb *ctx, const double *x, const double box[3], uint32_t 
   if (!pme) c.pme.on = false;  // finish without the PME forces of a skipped sum
   nb_finish_forces(c, forces, 1, st);
   c.pme.on = keep_pme;
+  CK(cudaGetLastError());
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, const double box[3], double *out,
+                           void *stream) {
+  if (!ctx || !box || count < 0 || (count > 0 && (!frames || !out))) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (!c.built || !c.x_build) return MDRT_NB_NOT_BUILT;
+  if (count == 0) return MDRT_NB_OK;
+  CK(cudaSetDevice(c.device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (c.drift_cap < count) {
+    nb_free(c.drift);
+    c.drift_cap = 0;
+    CK(cudaMalloc(&c.drift, sizeof(unsigned long long) * count));
+    c.drift_cap = count;
+  }
+  CK(cudaMemsetAsync(c.drift, 0, sizeof(unsigned long long) * count, st));
+  int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (c.n + 255) / 256));
+  for (int64_t f0 = 0; f0 < count; f0 += 65535) {
+    int64_t nf = std::min<int64_t>(65535, count - f0);
+    nb_frame_drift<<<dim3(bx, (unsigned)nf), 256, 0, st>>>(c.n, frames + f0 * 3 * c.n, c.x_build, box[0], box[1],
+                                                         box[2], c.drift + f0);
+  }
+  CK(cudaGetLastError());
+  std::vector<unsigned long long> bits(count);
+  CK(cudaMemcpyAsync(bits.data(), c.drift, sizeof(unsigned long long) * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int64_t f = 0; f < count; ++f) {
+    double d2;
+    std::memcpy(&d2, &bits[f], sizeof(double));
+    out[f] = std::sqrt(d2);
+  }
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3], const double *cotangent,
+                                int32_t mode, double *dq, double *dtable, void *stream) {
+  if (!ctx || !x || !box || !dq || !dtable) return MDRT_NB_INVALID_ARGUMENT;
+  if (mode != MDRT_NB_GRAD_PRODUCT && mode != MDRT_NB_GRAD_ENERGY) return MDRT_NB_INVALID_ARGUMENT;
+  if (mode == MDRT_NB_GRAD_PRODUCT && !cotangent) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (!c.built) return MDRT_NB_NOT_BUILT;
+  int s = check_box(c, box);
+  if (s) return s;
+  for (int k = 0; k < 3; ++k)
+    if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;
+  // the switched Lennard-Jones form has no adjoint here
+  if (c.lj_switch) return MDRT_NB_UNSUPPORTED;
+  CK(cudaSetDevice(c.device));
+  if (nb_adjoint_reserve(c)) return MDRT_NB_CUDA_ERROR;
+  if (nb_adjoint_run(c, x, box, cotangent, mode, dq, dtable, (cudaStream_t)stream)) return MDRT_NB_CUDA_ERROR;
   CK(cudaGetLastError());
   return MDRT_NB_OK;
 }

@@ -28,6 +28,7 @@ struct NbPme {
   float *pme_force = nullptr;   // float4 per place (gather output)
   float *potential = nullptr;   // f32 per place: dE_rec/dq
   double *partials = nullptr;   // per-block energy/virial partials of the convolution
+  float *adj_grid = nullptr;    // K0*K1*K2: the dipole grid V, then psi (the adjoint)
   int conv_blocks = 0;
   size_t workspace_bytes = 0;
 };
@@ -46,6 +47,7 @@ struct NbCtx {
   std::vector<double> h_c6;    // f64 c6 = 4 eps sig^6 per type pair
   std::vector<int32_t> h_type;
   std::vector<float2> h_lj;
+  float2 *sigeps = nullptr;    // (sigma, epsilon) per type pair, for the parameter gradient
   // exclusions: ragged rows (atom order) and the list of pairs i < j
   int32_t *excl_off = nullptr, *excl = nullptr;
   int32_t *excl_pairs = nullptr;
@@ -105,6 +107,17 @@ struct NbCtx {
   int64_t prunes = 0;
   // tuning (mdrtNbSetTuning): blocks of 8 warps per SM of the pair kernel
   int pair_blocks_per_sm = 4;
+  // parameter gradient scratch (mdrtNbParameterGradient), allocated at the first call
+  float4 *adj_g = nullptr;        // per place: the cotangent on the forces (f32)
+  double *adj_q = nullptr;        // per place: the charge gradient, kept zero between calls
+  double *adj_types = nullptr;    // per block of the adjoint kernel: 2 ntypes^2 partials
+  int64_t adj_places = 0;         // places_cap the per-place arrays were sized for
+  int adj_blocks = 0;
+  // the f64 positions of the last build (atom order) and the per-frame
+  // displacement maxima of mdrtNbDisplacement
+  double *x_build = nullptr;
+  unsigned long long *drift = nullptr;
+  int64_t drift_cap = 0;
 };
 
 // Energy / virial slots of ctx->energy (f64, device).
@@ -144,3 +157,13 @@ void nb_reduce_energy(NbCtx &c, bool pairs, bool excluded, cudaStream_t s);
 int nb_pme_setup(NbCtx &c, int k0, int k1, int k2, int order);
 void nb_pme_release(NbCtx &c);
 int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaStream_t s);
+// The parameter gradient (mdrtNbParameterGradient).  mode 0: the product
+// sum_k g_k . dF_k/dtheta for the cotangent g (f64 [n,3], atom order); mode 1:
+// dE/dtheta.  Adds the charge gradient to dq (f64 [n], atom order) and the
+// type-pair gradient to dtable (f64, ntypes^2 sigma entries then ntypes^2
+// epsilon entries).  Needs the adjoint scratch (nb_adjoint_reserve).
+int nb_adjoint_reserve(NbCtx &c);
+int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double *cotangent, int mode,
+                   double *dq, double *dtable, cudaStream_t s);
+// The reciprocal part of the charge gradient, added per place into c.adj_q.
+int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s);

@@ -403,25 +403,233 @@ __global__ void nb_sum_partials(const double *__restrict__ unit_partials,
   }
 }
 
+// ---------------------------------------------------------------------------
+// The parameter gradient (the differentiation form).
+//
+// MODE 0, the force-matching product.  With g_i the cotangent on the forces
+// (for a loss (1/K) sum |F - F^ref|^2, g = (2/K)(F - F^ref)) and u(r; theta)
+// the energy of a pair, F_i = -sum_j u'(r_ij) d_ij / r_ij, so that
+//   G_theta = sum_i g_i . dF_i/dtheta = -sum_pairs h_ij du'/dtheta,
+//   h_ij = (g_i - g_j) . d_ij / r_ij,
+// which gives, with D = d/dr [erfc(beta r)/r] and u_LJ = 4 eps ((sigma/r)^12 - (sigma/r)^6),
+//   G_q[i] -= h f q_j D,  G_q[j] -= h f q_i D,
+//   G_sigma[ab] -= h 4 eps (36 s6 - 144 s12)/(sigma r),  G_eps[ab] -= h 4 (6 s6 - 12 s12)/r.
+// MODE 1, the gradient of the energy:
+//   G_q[i] += f q_j (erfc(beta r)/r - shift),  G_sigma[ab] += 4 eps (12 s12 - 6 s6)/sigma,
+//   G_eps[ab] += 4 (s12 - s6).
+// The kernel walks the same lists and slots as nb_pairs and recomputes the
+// geometry (nothing of the forward pass is stored).  The member's G_q
+// travels with it like its force accumulator; the partner's stays in its
+// lane and is added once per entry (f64 atomics); the type-pair sums go to
+// shared memory and per-block partials, summed later in a fixed order.
+// MDIR's counterpart is the IR-derived product of md-differentiate (D381,
+// docs/python-frames.md:203-260), which walks the neighbor matrix.
+template <int MODE>
+__global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
+    PairParams P, const int32_t *__restrict__ sizes, const int2 *__restrict__ units, const int2 *__restrict__ slab,
+    const int32_t *__restrict__ counts, const float4 *__restrict__ xq, const int32_t *__restrict__ typ,
+    const float2 *__restrict__ sigeps, const float4 *__restrict__ gp, double *__restrict__ gq,
+    double *__restrict__ type_partials) {
+  __shared__ float4 s_x[8][2 * NB_GROUP];
+  __shared__ float4 s_g[8][2 * NB_GROUP];
+  __shared__ int s_t[8][2 * NB_GROUP];
+  __shared__ float2 s_se[NB_MAX_TYPES * NB_MAX_TYPES];
+  __shared__ float s_acc[2 * NB_MAX_TYPES * NB_MAX_TYPES];
+  const unsigned FULL = 0xffffffffu;
+  int nt2 = P.ntypes * P.ntypes;
+  for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+    s_se[k] = sigeps[k];
+    s_acc[k] = 0.f;
+    s_acc[nt2 + k] = 0.f;
+  }
+  __syncthreads();
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int u = lane & 15;
+  const int src = (lane & 16) | ((lane + 1) & 15);
+  const float4 *px = &s_x[warp][u];
+  const float4 *pg = &s_g[warp][u];
+  const int *pt = &s_t[warp][u];
+  int nunits = min((int64_t)sizes[NB_SIZE_UNITS], P.units_cap);
+  int wstride = gridDim.x * 8;
+  for (int unit = blockIdx.x * 8 + warp; unit < nunits; unit += wstride) {
+    int2 uo = units[unit];
+    int g = uo.x;
+    int64_t pi = (int64_t)g * NB_GROUP + u;
+    __syncwarp();
+    {
+      float4 xi = xq[pi];
+      xi.w *= P.coulomb;
+      s_x[warp][lane] = xi;
+      s_g[warp][lane] = MODE == 0 ? gp[pi] : make_float4(0.f, 0.f, 0.f, 0.f);
+      s_t[warp][lane] = typ[pi] * P.ntypes;
+    }
+    __syncwarp();
+    int cnt = (int)min((int64_t)counts[g], P.list_cap);
+    int e0 = uo.y * NB_UNIT;
+    int ne = min(NB_UNIT, cnt - e0);
+    float ai = 0.f;  // G_q of member (lane + k) mod 16
+    for (int r = 0; r < 2; ++r) {
+      if (r * 32 >= ne) break;
+      bool valid = r * 32 + lane < ne;
+      int2 en = valid ? slab[(int64_t)g * P.list_cap + e0 + r * 32 + lane] : make_int2(0, 0);
+      int q = en.x;
+      unsigned mask = valid ? ((unsigned)en.y & 0xffffu) : 0u;
+      int code = ((unsigned)en.y >> 16) & 31;
+      int sx, sy, sz;
+      nb_decode_image(code, sx, sy, sz);
+      float4 xj = xq[q];
+      xj.x += (float)sx * P.Lx;
+      xj.y += (float)sy * P.Ly;
+      xj.z += (float)sz * P.Lz;
+      float4 gj = MODE == 0 ? gp[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      int tj = typ[q];
+      float fqj = xj.w * P.coulomb;
+      unsigned mrot = ((mask >> u) | (mask << (16 - u))) & 0xffffu;
+      float aj = 0.f;
+#pragma unroll 4
+      for (int k = 0; k < NB_GROUP; ++k) {
+        float4 xm = px[k];
+        float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
+        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        bool inside = ((mrot >> k) & 1u) && (r2 < P.rc2);
+        float r2s = inside ? r2 : 1.0f;
+        float rinv = rsqrtf(r2s);
+        float rinv2 = rinv * rinv;
+        float rr = r2s * rinv;
+        float bx = P.beta * rr;
+        float ex = __expf(-bx * bx);
+        float erfcv = nb_erfc_from_exp(bx, ex);
+        // w: the factor of the pair's term; cq: its Coulomb part per unit f q_i q_j
+        float w, cq;
+        if (MODE == 0) {
+          float4 gm = pg[k];
+          float h = ((gm.x - gj.x) * dx + (gm.y - gj.y) * dy + (gm.z - gj.z) * dz) * rinv;
+          w = inside ? h : 0.f;
+          // -h D, D = -(erfc(beta r)/r^2 + 2 beta/sqrt(pi) exp(-beta^2 r^2)/r)
+          cq = w * fmaf(erfcv, rinv2, P.two_beta_sqrtpi * ex * rinv);
+        } else {
+          w = inside ? 1.f : 0.f;
+          cq = w * (erfcv * rinv - P.coulomb_shift);
+        }
+        ai = fmaf(cq, fqj, ai);
+        aj = fmaf(cq, xm.w, aj);
+        int tp = pt[k] + tj;
+        float2 se = s_se[tp];
+        if (w != 0.f && se.y != 0.f) {
+          float s1 = se.x * rinv;
+          float s2 = s1 * s1;
+          float s6 = s2 * s2 * s2;
+          float s12 = s6 * s6;
+          float ds, de;
+          if (MODE == 0) {
+            de = -w * 4.f * (6.f * s6 - 12.f * s12) * rinv;
+            ds = -w * 4.f * se.y * (36.f * s6 - 144.f * s12) * rinv / se.x;
+          } else {
+            de = 4.f * (s12 - s6);
+            ds = 4.f * se.y * (12.f * s12 - 6.f * s6) / se.x;
+          }
+          atomicAdd(&s_acc[tp], ds);
+          atomicAdd(&s_acc[nt2 + tp], de);
+        }
+        ai = __shfl_sync(FULL, ai, src);
+      }
+      if (valid && aj != 0.f) atomicAdd(gq + q, (double)aj);
+    }
+    ai += __shfl_xor_sync(FULL, ai, 16);
+    if (lane < 16 && ai != 0.f) atomicAdd(gq + pi, (double)ai);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < 2 * nt2; k += blockDim.x)
+    type_partials[(int64_t)blockIdx.x * 2 * nt2 + k] = (double)s_acc[k];
+}
+
+// g of each place (f32), gathered from the atom-order cotangent (f64).
+__global__ void nb_gather_cotangent(int64_t places, const int32_t *__restrict__ sizes,
+                                    const int32_t *__restrict__ order, const double *__restrict__ g,
+                                    float4 *__restrict__ gp) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  int a = order[p];
+  gp[p] = a < 0 ? make_float4(0.f, 0.f, 0.f, 0.f)
+                : make_float4((float)g[3 * a], (float)g[3 * a + 1], (float)g[3 * a + 2], 0.f);
+}
+
+// The per-place charge gradient (f64) added to atom order; the place
+// values are zeroed for the next call.
+__global__ void nb_scatter_place_values(int64_t places, const int32_t *__restrict__ sizes,
+                                        const int32_t *__restrict__ order, double *__restrict__ vp,
+                                        double *__restrict__ out) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= places) return;
+  double v = vp[p];
+  if (v != 0.0) {
+    int a = p < sizes[NB_SIZE_PLACES] ? order[p] : -1;
+    if (a >= 0) out[a] += v;
+    vp[p] = 0.0;
+  }
+}
+
+// The excluded pairs, u = -f q_i q_j erf(beta r)/r, in f64 and atom order.
+// MODE 0: G_q[i] += h f q_j X, X = d/dr [erf(beta r)/r]; MODE 1: G_q[i] -= f q_j erf(beta r)/r.
+template <int MODE>
+__global__ void nb_excluded_adjoint(int64_t npairs, const int32_t *__restrict__ pairs, const double *__restrict__ x,
+                                    const float *__restrict__ q, const double *__restrict__ g, double Lx, double Ly,
+                                    double Lz, double beta, double coulomb, double *__restrict__ gq) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npairs) return;
+  int i = pairs[2 * k], j = pairs[2 * k + 1];
+  double d0 = x[3 * i] - x[3 * j], d1 = x[3 * i + 1] - x[3 * j + 1], d2 = x[3 * i + 2] - x[3 * j + 2];
+  d0 -= Lx * rint(d0 / Lx);
+  d1 -= Ly * rint(d1 / Ly);
+  d2 -= Lz * rint(d2 / Lz);
+  double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+  if (r2 <= 0.0) return;
+  double r = sqrt(r2);
+  double c;
+  if (MODE == 0) {
+    double h = ((g[3 * i] - g[3 * j]) * d0 + (g[3 * i + 1] - g[3 * j + 1]) * d1 + (g[3 * i + 2] - g[3 * j + 2]) * d2) / r;
+    double X = 2.0 * beta / sqrt(M_PI) * exp(-beta * beta * r2) / r - erf(beta * r) / r2;
+    c = h * coulomb * X;
+  } else {
+    c = -coulomb * erf(beta * r) / r;
+  }
+  atomicAdd(gq + i, c * (double)q[j]);
+  atomicAdd(gq + j, c * (double)q[i]);
+}
+
+// The charge terms of the energy without a pair: the Ewald self term
+// -f beta/sqrt(pi) sum q^2 and the neutralizing background -f pi Q^2/(2 V beta^2).
+__global__ void nb_charge_terms(int64_t n, const float *__restrict__ q, double self2, double background,
+                                double *__restrict__ gq) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  gq[i] += self2 * (double)q[i] + background;
+}
+
+// Fixed-order sum of the per-block type-pair partials, added into out.
+__global__ void nb_sum_type_partials(const double *__restrict__ partials, int nblocks, int width,
+                                     double *__restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= width) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * width + k];
+  out[k] += s;
+}
+
 inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
 
 int g_sm_count = 0;
 
-}  // namespace
-
-void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
-  nb_gather<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.shift, x,
-                                                          c.q, c.type, box[0], box[1], box[2], c.xq,
-                                                          c.typ_p);
-}
-
-void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
+void ensure_sm_count() {
   if (!g_sm_count) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
     if (g_sm_count <= 0) g_sm_count = 148;
   }
+}
+
+PairParams pair_params(const NbCtx &c, const double box[3]) {
   PairParams P;
   P.Lx = (float)box[0];
   P.Ly = (float)box[1];
@@ -437,6 +645,20 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
   P.ntypes = c.ntypes;
   P.list_cap = c.list_cap;
   P.units_cap = c.units_cap;
+  return P;
+}
+
+}  // namespace
+
+void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
+  nb_gather<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.shift, x,
+                                                          c.q, c.type, box[0], box[1], box[2], c.xq,
+                                                          c.typ_p);
+}
+
+void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
+  ensure_sm_count();
+  PairParams P = pair_params(c, box);
   // persistent grid: enough warps for the units, `pair_blocks_per_sm`
   // blocks of 8 warps per SM (4 fit at 64 registers; fewer leave room for
   // the PME kernels that run beside it on another stream)
@@ -511,4 +733,70 @@ void nb_reduce_energy(NbCtx &c, bool pairs, bool excluded, cudaStream_t s) {
   bool inner = c.inner_reach > 0.0 && c.inner_valid;
   nb_sum_partials<<<1, 256, 0, s>>>(c.unit_partials, inner ? c.sizes_in : c.sizes, c.units_cap, c.excl_partials,
                                     eb, pairs ? 1 : 0, c.energy);
+}
+
+int nb_adjoint_reserve(NbCtx &c) {
+  ensure_sm_count();
+  if (!c.adj_types) {
+    c.adj_blocks = g_sm_count * 4;
+    if (cudaMalloc(&c.adj_types, sizeof(double) * c.adj_blocks * 2 * NB_MAX_TYPES * NB_MAX_TYPES) != cudaSuccess)
+      return -1;
+  }
+  if (c.adj_places < c.places_cap) {
+    if (c.adj_g) cudaFree(c.adj_g);
+    if (c.adj_q) cudaFree(c.adj_q);
+    c.adj_g = nullptr;
+    c.adj_q = nullptr;
+    c.adj_places = 0;
+    if (cudaMalloc(&c.adj_g, sizeof(float4) * c.places_cap) != cudaSuccess) return -1;
+    if (cudaMalloc(&c.adj_q, sizeof(double) * c.places_cap) != cudaSuccess) return -1;
+    if (cudaMemset(c.adj_q, 0, sizeof(double) * c.places_cap) != cudaSuccess) return -1;
+    c.adj_places = c.places_cap;
+  }
+  return 0;
+}
+
+int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double *cot, int mode, double *dq,
+                   double *dtable, cudaStream_t s) {
+  PairParams P = pair_params(c, box);
+  nb_gather_frames(c, x, box, s);
+  if (mode == 0)
+    nb_gather_cotangent<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, cot, c.adj_g);
+  bool inner = c.inner_reach > 0.0 && c.inner_valid;
+  const int32_t *lsizes = inner ? c.sizes_in : c.sizes;
+  const int2 *lunits = inner ? c.units_in : c.units;
+  const int2 *lslab = inner ? c.slab_in : c.slab;
+  const int32_t *lcounts = inner ? c.counts_in : c.counts;
+  int64_t want = (c.units_cap + 7) / 8;
+  int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, c.adj_blocks));
+  if (mode == 0)
+    nb_pairs_adjoint<0><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
+                                             c.adj_q, c.adj_types);
+  else
+    nb_pairs_adjoint<1><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
+                                             c.adj_q, c.adj_types);
+  int width = 2 * c.ntypes * c.ntypes;
+  nb_sum_type_partials<<<blocks_for(width, 256), 256, 0, s>>>(c.adj_types, grid, width, dtable);
+  int rc = nb_pme_adjoint_run(c, box, mode, s);
+  if (rc) return rc;
+  nb_scatter_place_values<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.adj_q,
+                                                                        dq);
+  if (c.n_excl_pairs > 0 && c.beta != 0.0) {
+    int blocks = blocks_for(c.n_excl_pairs, 256);
+    if (mode == 0)
+      nb_excluded_adjoint<0><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, x, c.q, cot, box[0], box[1],
+                                                    box[2], c.beta, c.coulomb, dq);
+    else
+      nb_excluded_adjoint<1><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, x, c.q, cot, box[0], box[1],
+                                                    box[2], c.beta, c.coulomb, dq);
+  }
+  if (mode == 1 && c.beta > 0.0) {
+    double net = 0.0;
+    for (double v : c.h_q) net += v;
+    double V = box[0] * box[1] * box[2];
+    double self2 = -2.0 * c.coulomb * c.beta / sqrt(M_PI);
+    double background = -c.coulomb * M_PI * net / (V * c.beta * c.beta);
+    nb_charge_terms<<<blocks_for(c.n, 256), 256, 0, s>>>(c.n, c.q, self2, background, dq);
+  }
+  return 0;
 }

@@ -344,6 +344,106 @@ __global__ void __launch_bounds__(128) nb_pme_gather_split(GridParams G, int64_t
   if (pot) pot[p] = e;
 }
 
+// The adjoint of the reciprocal forces for the force-matching product.
+// With Q = sum_j q_j W_j, phi = Psi * Q and F_i = -q_i sum_k phi(k) grad W_i(k):
+//   sum_i g_i . dF_i/dq_m = -g_m . sum_k phi(k) grad W_m(k) - sum_k W_m(k) psi(k),
+//   psi = Psi * V,  V(k) = sum_i q_i g_i . grad W_i(k)   (Psi symmetric).
+// nb_spread_dipole builds V; psi comes from the same FFTs and influence;
+// nb_pme_adjoint_gather forms the two terms per atom.
+template <int P>
+__global__ void __launch_bounds__(256) nb_spread_dipole(GridParams G, int64_t places,
+                                                        const int32_t *__restrict__ sizes,
+                                                        const int32_t *__restrict__ order,
+                                                        const float4 *__restrict__ xq, const float4 *__restrict__ gp,
+                                                        float *__restrict__ grid) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t p = t / P;
+  int c = (int)(t - p * P);
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  if (order[p] < 0) return;
+  float4 v = xq[p];
+  float4 g = gp[p];
+  if (v.w == 0.f) return;
+  int k0, k1, k2;
+  float t0, t1, t2;
+  nb_frac(v.x, G.invL0, G.K0, k0, t0);
+  nb_frac(v.y, G.invL1, G.K1, k1, t1);
+  nb_frac(v.z, G.invL2, G.K2, k2, t2);
+  float w0[P], w1[P], w2[P], d0[P], d1[P], d2[P];
+  nb_bspline<P>(t0, w0, d0);
+  nb_bspline<P>(t1, w1, d1);
+  nb_bspline<P>(t2, w2, d2);
+  float a0 = v.w * g.x * (float)G.K0 * G.invL0, a1 = v.w * g.y * (float)G.K1 * G.invL1,
+        a2 = v.w * g.z * (float)G.K2 * G.invL2;
+  int gz = k2 - c;
+  if (gz < 0) gz += G.K2;
+  float wz = w2[c], dz = d2[c];
+#pragma unroll
+  for (int jx = 0; jx < P; ++jx) {
+    int gx = k0 - jx;
+    if (gx < 0) gx += G.K0;
+#pragma unroll
+    for (int jy = 0; jy < P; ++jy) {
+      int gy = k1 - jy;
+      if (gy < 0) gy += G.K1;
+      float val = (a0 * d0[jx] * w1[jy] + a1 * w0[jx] * d1[jy]) * wz + a2 * w0[jx] * w1[jy] * dz;
+      atomicAdd(grid + ((int64_t)gx * G.K1 + gy) * G.K2 + gz, val);
+    }
+  }
+}
+
+// MODE 0: the two terms above; MODE 1: dE/dq_m = sum_k W_m(k) phi(k).
+template <int P, int MODE>
+__global__ void __launch_bounds__(128) nb_pme_adjoint_gather(GridParams G, int64_t places,
+                                                             const int32_t *__restrict__ sizes,
+                                                             const int32_t *__restrict__ order,
+                                                             const float4 *__restrict__ xq,
+                                                             const float4 *__restrict__ gp,
+                                                             const float *__restrict__ phi,
+                                                             const float *__restrict__ psi,
+                                                             double *__restrict__ out) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  if (order[p] < 0) return;
+  float4 v = xq[p];
+  float4 g = MODE == 0 ? gp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+  int k0, k1, k2;
+  float t0, t1, t2;
+  nb_frac(v.x, G.invL0, G.K0, k0, t0);
+  nb_frac(v.y, G.invL1, G.K1, k1, t1);
+  nb_frac(v.z, G.invL2, G.K2, k2, t2);
+  float w0[P], w1[P], w2[P], d0[P], d1[P], d2[P];
+  nb_bspline<P>(t0, w0, d0);
+  nb_bspline<P>(t1, w1, d1);
+  nb_bspline<P>(t2, w2, d2);
+  const float *sgrid = MODE == 0 ? psi : phi;
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0, s = 0.0;
+  for (int jx = 0; jx < P; ++jx) {
+    int gx = k0 - jx;
+    if (gx < 0) gx += G.K0;
+    for (int jy = 0; jy < P; ++jy) {
+      int gy = k1 - jy;
+      if (gy < 0) gy += G.K1;
+      for (int jz = 0; jz < P; ++jz) {
+        int gz = k2 - jz;
+        if (gz < 0) gz += G.K2;
+        int64_t idx = ((int64_t)gx * G.K1 + gy) * G.K2 + gz;
+        double f = phi[idx], y = sgrid[idx];
+        g0 += f * d0[jx] * w1[jy] * w2[jz];
+        g1 += f * w0[jx] * d1[jy] * w2[jz];
+        g2 += f * w0[jx] * w1[jy] * d2[jz];
+        s += y * w0[jx] * w1[jy] * w2[jz];
+      }
+    }
+  }
+  if (MODE == 1) {
+    out[p] += s;
+    return;
+  }
+  double grad = g.x * g0 * G.K0 * G.invL0 + g.y * g1 * G.K1 * G.invL1 + g.z * g2 * G.K2 * G.invL2;
+  out[p] += -grad - s;
+}
+
 inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
 
 // |b(m)|^2 of the SPME B-spline moduli along one edge, in f64 on the host.
@@ -417,8 +517,9 @@ void nb_pme_release(NbCtx &c) {
   if (P.bwd) cufftDestroy(P.bwd);
   P.fwd = P.bwd = 0;
   for (void *p : {(void *)P.grid, (void *)P.spec, (void *)P.fixed, (void *)P.moduli,
-                  (void *)P.pme_force, (void *)P.potential, (void *)P.partials})
+                  (void *)P.pme_force, (void *)P.potential, (void *)P.partials, (void *)P.adj_grid})
     if (p) cudaFree(p);
+  P.adj_grid = nullptr;
   P.grid = nullptr;
   P.spec = nullptr;
   P.fixed = nullptr;
@@ -486,6 +587,66 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
     case 5: nb_pme_gather<5><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, pf, pot); break;
     case 6: nb_pme_gather<6><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, pf, pot); break;
     case 8: nb_pme_gather_split<8><<<blocks_for(c.places_cap * 8, 128), 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, P.grid, pf, pot); break;
+  }
+  return 0;
+}
+
+// The reciprocal part of the parameter gradient in the charges, added per
+// place into c.adj_q.  phi is recomputed by the forward stages (spread, FFT,
+// influence, inverse FFT); in mode 0 the dipole grid V goes through the same
+// FFT pair and influence to give psi.  The dipole spread uses f32 atomics
+// in both modes of the forward (deterministic or not).
+int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s) {
+  NbPme &P = c.pme;
+  if (!P.on) return 0;
+  GridParams G;
+  G.K0 = P.K[0];
+  G.K1 = P.K[1];
+  G.K2 = P.K[2];
+  G.invL0 = (float)(1.0 / box[0]);
+  G.invL1 = (float)(1.0 / box[1]);
+  G.invL2 = (float)(1.0 / box[2]);
+  int64_t total = (int64_t)G.K0 * G.K1 * G.K2;
+  int64_t half = (int64_t)G.K0 * G.K1 * (G.K2 / 2 + 1);
+  if (!P.adj_grid && cudaMalloc(&P.adj_grid, sizeof(float) * total) != cudaSuccess) return -2;
+  int rc = nb_pme_run(c, box, false, false, s);  // phi in P.grid
+  if (rc) return rc;
+  int blocks = blocks_for(c.places_cap, 128);
+  if (mode == 1) {
+    switch (P.order) {
+      case 4: nb_pme_adjoint_gather<4, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, P.grid, nullptr, c.adj_q); break;
+      case 5: nb_pme_adjoint_gather<5, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, P.grid, nullptr, c.adj_q); break;
+      case 6: nb_pme_adjoint_gather<6, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, P.grid, nullptr, c.adj_q); break;
+      case 8: nb_pme_adjoint_gather<8, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, P.grid, nullptr, c.adj_q); break;
+    }
+    return 0;
+  }
+  cudaMemsetAsync(P.adj_grid, 0, sizeof(float) * total, s);
+  int64_t threads = c.places_cap * P.order;
+  switch (P.order) {
+    case 4: nb_spread_dipole<4><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.adj_grid); break;
+    case 5: nb_spread_dipole<5><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.adj_grid); break;
+    case 6: nb_spread_dipole<6><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.adj_grid); break;
+    case 8: nb_spread_dipole<8><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.adj_grid); break;
+  }
+  if (cufftExecR2C(P.fwd, P.adj_grid, (cufftComplex *)P.spec) != CUFFT_SUCCESS) return -3;
+  ConvParams C;
+  C.K0 = G.K0;
+  C.K1 = G.K1;
+  C.K2 = G.K2;
+  C.H2 = G.K2 / 2 + 1;
+  C.L0 = box[0];
+  C.L1 = box[1];
+  C.L2 = box[2];
+  C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
+  C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
+  nb_convolve<false><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
+  if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.adj_grid) != CUFFT_SUCCESS) return -3;
+  switch (P.order) {
+    case 4: nb_pme_adjoint_gather<4, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
+    case 5: nb_pme_adjoint_gather<5, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
+    case 6: nb_pme_adjoint_gather<6, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
+    case 8: nb_pme_adjoint_gather<8, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
   }
   return 0;
 }

@@ -1,0 +1,294 @@
+"""Frames of one system on the device: energies, forces, and the gradients
+in the parameters (per-type LJ sigma / epsilon and per-atom charges).
+
+Mirrors MDIR's frame evaluator (python/mdir/_frames.py:467-715,
+docs/python-frames.md): `FrameEvaluator(system).evaluate(positions,
+gradients=("tunables", "positions"))` returns `FrameEnergies` with
+`.energy`, `.gradients` and `.vjp(cotangent, positions=)`, the product of
+force matching (D381), whose cotangent is on dU/dx = -F.  The tunables are
+named "sigma", "epsilon" (one per LJ type, mixed by Lorentz-Berthelot) and
+"charges" (one per atom).  MDIR refuses the product in per-atom charges
+with PME (D379); here it is given by the adjoint of the reciprocal sum.
+
+Frames of a batch share one neighbor build while they stay within half
+the skin of the positions it was made at (one displacement test per batch
+on the device, `mdrtNbDisplacement`); a frame that moved further is
+evaluated after a new build.  Every evaluation goes through libmdrt_nb.so."""
+
+import numpy as np
+import torch
+
+from .api import UnsupportedError
+from .term import NonbondedTerm
+
+TUNABLES = ("sigma", "epsilon", "charges")
+
+
+def lorentz_berthelot(sigma, epsilon):
+    """The (ntypes, ntypes) tables sigma_ab = (sigma_a + sigma_b)/2 and
+    epsilon_ab = sqrt(epsilon_a epsilon_b)."""
+    s = np.asarray(sigma, dtype=np.float64)
+    e = np.asarray(epsilon, dtype=np.float64)
+    return 0.5 * (s[:, None] + s[None, :]), np.sqrt(e[:, None] * e[None, :])
+
+
+def lorentz_berthelot_chain(dtable, sigma, epsilon):
+    """The gradient in the per-type values from the gradient in the tables
+    (dtable[0]: d/dsigma_ab, dtable[1]: d/depsilon_ab, each pair counted
+    once in each order).  A type with epsilon 0 has no LJ term and gets no
+    epsilon gradient (sqrt is not differentiable there)."""
+    T = np.asarray(dtable, dtype=np.float64)
+    S = T + np.swapaxes(T, 1, 2)
+    s_grad = 0.5 * S[0].sum(axis=1)
+    e = np.asarray(epsilon, dtype=np.float64)
+    eab = np.sqrt(e[:, None] * e[None, :])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        w = np.where(e[:, None] > 0, eab / (2.0 * e[:, None]), 0.0)
+    e_grad = (S[1] * w).sum(axis=1)
+    return s_grad, e_grad
+
+
+def diagonal_types(system):
+    """Per-type sigma and epsilon of a system whose tables are the
+    Lorentz-Berthelot mixtures of their diagonals; raises otherwise."""
+    sg = np.asarray(system["sigma"], dtype=np.float64)
+    ep = np.asarray(system["epsilon"], dtype=np.float64)
+    s, e = np.diag(sg).copy(), np.diag(ep).copy()
+    ms, me = lorentz_berthelot(s, e)
+    if not (np.allclose(ms, sg, rtol=1e-12, atol=0) and np.allclose(me, ep, rtol=1e-12, atol=1e-300)):
+        raise UnsupportedError("the LJ tables are not Lorentz-Berthelot mixtures of per-type values")
+    return s, e
+
+
+def dispersion_table_gradient(system, sigma_table, epsilon_table, box):
+    """d E_disp / d(sigma_ab, epsilon_ab) of the long-range dispersion
+    correction E_disp = -(2 pi / 3V) N^2 <C6> / rc^3, <C6> over the distinct
+    non-excluded pairs (MDIR TermNonbonded.cpp:601-637), C6_ab = 4 eps sig^6."""
+    types = np.asarray(system["types"])
+    nt = sigma_table.shape[0]
+    n = len(types)
+    cnt = np.bincount(types, minlength=nt).astype(np.float64)
+    M = cnt[:, None] * cnt[None, :] - np.diag(cnt)
+    pairs = np.asarray(system["excluded_pairs"]).reshape(-1, 2)
+    # an excluded pair (i < j) leaves the sum as 2 C6[type_i, type_j], the
+    # form of the library's constant (mdrtNbConstants)
+    np.subtract.at(M, (types[pairs[:, 0]], types[pairs[:, 1]]), 2.0)
+    npair = n * (n - 1.0) - 2.0 * len(pairs)
+    V = float(np.prod(box))
+    rc = system["cutoff"]
+    dE_dc6 = -2.0 * np.pi / (3.0 * V) * n * n / (npair * rc ** 3) * M
+    out = np.zeros((2, nt, nt))
+    out[0] = dE_dc6 * 24.0 * epsilon_table * sigma_table ** 5
+    out[1] = dE_dc6 * 4.0 * sigma_table ** 6
+    return out
+
+
+class FrameEnergies:
+    """The result of `FrameEvaluator.evaluate` (MDIR _frames.py:281)."""
+
+    def __init__(self, evaluator, positions, energy, gradients):
+        self._evaluator = evaluator
+        self._positions = positions
+        self._version = evaluator.version
+        self.energy = energy
+        self.gradients = gradients
+
+    def vjp(self, cotangent=None, *, positions=None):
+        """sum_n [g_n dU_n/dtheta + sum_i Gbar_ni . d^2 U_n / dx_i dtheta]
+        with g = cotangent (K,) and Gbar = positions (K, n, 3), a cotangent on
+        dU/dx = -F (MDIR FrameEnergies.vjp, docs/python-frames.md:203-260);
+        returns {"sigma", "epsilon", "charges"} (numpy f64)."""
+        ev = self._evaluator
+        if ev.version != self._version:
+            raise RuntimeError("the parameters changed since this evaluation")
+        X = self._positions
+        K = X.shape[0]
+        dq = torch.zeros(ev.n, dtype=torch.float64, device=ev.device)
+        dt = torch.zeros((2, ev.ntypes, ev.ntypes), dtype=torch.float64, device=ev.device)
+        if positions is not None:
+            Gbar = torch.as_tensor(positions, dtype=torch.float64, device=ev.device).reshape(K, ev.n, 3)
+            ev.product(X, -Gbar, dq=dq, dtable=dt)
+        if cotangent is not None:
+            g = np.broadcast_to(np.asarray(cotangent, dtype=np.float64), (K,))
+            for k in ev.schedule(X):
+                if g[k] != 0.0:
+                    q1, t1 = ev.term.parameter_gradient(X[k])
+                    dq += g[k] * q1
+                    dt += g[k] * t1
+                    if ev.system.get("dispersion", False):
+                        dt += g[k] * torch.as_tensor(ev.dispersion_gradient(), device=ev.device)
+        return ev.per_type(dq, dt)
+
+
+class FrameEvaluator:
+    """Energies, forces and parameter gradients of frames of one system."""
+
+    def __init__(self, system, device=0, sigma=None, epsilon=None, charges=None):
+        self.system = system
+        self.n = len(system["charges"])
+        self.device = torch.device("cuda", device)
+        self.box = np.asarray(system["box"], dtype=np.float64)
+        self.types = np.asarray(system["types"], dtype=np.int32)
+        s0, e0 = (sigma, epsilon) if sigma is not None else diagonal_types(system)
+        self.sigma = np.asarray(s0, dtype=np.float64).copy()
+        self.epsilon = np.asarray(e0, dtype=np.float64).copy()
+        self.charges = np.asarray(system["charges"] if charges is None else charges, dtype=np.float64).copy()
+        self.ntypes = len(self.sigma)
+        self.cutoff = float(system["cutoff"])
+        self.reach = float(system["reach"])
+        term = NonbondedTerm(self.n, device)
+        term.set_exclusions(system["excluded_pairs"])
+        pme = system.get("pme", True)
+        term.set_interaction(self.cutoff, self.reach, system["beta"] if pme else 0.0,
+                             coulomb_shift=system.get("coulomb_shift", False),
+                             lj_switch=system.get("lj_switch", False), switch_distance=system.get("switch", 0.0))
+        if pme:
+            term.set_pme(system["grid"], system["order"])
+        self.term = term
+        self.version = 0
+        self._uploaded = -1
+        self._built = False
+        self.builds = 0
+
+    # -- parameters ------------------------------------------------------------
+    def set_parameters(self, sigma=None, epsilon=None, charges=None):
+        """New values of the tunables (host arrays); the next evaluation uses them."""
+        changed = False
+        for name, value in (("sigma", sigma), ("epsilon", epsilon), ("charges", charges)):
+            if value is None:
+                continue
+            v = np.asarray(value, dtype=np.float64).reshape(getattr(self, name).shape)
+            if not np.array_equal(v, getattr(self, name)):
+                setattr(self, name, v.copy())
+                changed = True
+        if changed:
+            self.version += 1
+
+    def tables(self):
+        return lorentz_berthelot(self.sigma, self.epsilon)
+
+    def _upload(self):
+        if self._uploaded != self.version:
+            sg, ep = self.tables()
+            self.term.set_particles(self.charges, self.types, sg, ep)
+            self._uploaded = self.version
+
+    def per_type(self, dq, dtable):
+        """{"sigma", "epsilon", "charges"} from the table gradient."""
+        ds, de = lorentz_berthelot_chain(dtable.cpu().numpy(), self.sigma, self.epsilon)
+        return {"sigma": ds, "epsilon": de, "charges": dq.cpu().numpy()}
+
+    def dispersion_gradient(self):
+        sg, ep = self.tables()
+        return dispersion_table_gradient(self.system, sg, ep, self.box)
+
+    # -- frames ----------------------------------------------------------------
+    def frames(self, positions):
+        """(K, n, 3) contiguous f64 device frames from a tensor or an array."""
+        X = torch.as_tensor(positions, dtype=torch.float64, device=self.device)
+        if X.dim() == 2:
+            X = X.unsqueeze(0)
+        if X.dim() != 3 or X.shape[1:] != (self.n, 3):
+            raise ValueError(f"positions: (K, {self.n}, 3)")
+        return X.contiguous()
+
+    def schedule(self, X):
+        """Yields the frame numbers in order, each with a build whose lists
+        serve it: the frames ahead are tested against the positions of the
+        current build in one launch, and a frame that moved more than half
+        the skin gets a new build first."""
+        self._upload()
+        K = X.shape[0]
+        half_skin = 0.5 * (self.reach - self.cutoff)
+        k = 0
+        while k < K:
+            if not self._built:
+                self._build(X[k])
+            d = self.term.displacement(X[k:])
+            bad = np.nonzero(~(d < half_skin))[0]
+            run = int(bad[0]) if len(bad) else K - k
+            if run == 0:
+                self._build(X[k])
+                continue
+            for j in range(k, k + run):
+                yield j
+            k += run
+
+    def _build(self, x):
+        self.term.build(x, self.box, self.reach)
+        self._built = True
+        self.builds += 1
+
+    def forces(self, positions, energy=False, out=None):
+        """Forces (K, n, 3) of every frame (and, with `energy`, the
+        potential energies (K,) as a host array)."""
+        X = self.frames(positions)
+        F = torch.empty_like(X) if out is None else out
+        E = np.zeros(X.shape[0]) if energy else None
+        for k in self.schedule(X):
+            self.term.force(X[k], energy=energy, forces=F[k])
+            if energy:
+                E[k] = self._energy()
+        return (F, E) if energy else F
+
+    def _energy(self):
+        e = self.term.energies()
+        c = self.term.constants(dispersion=self.system.get("dispersion", False))
+        return (e["lj"] + e["coulomb"] + e["excluded"] + e["reciprocal"] + c["self"] + c["background"]
+                + c["dispersion"])
+
+    def product(self, positions, cotangent, dq=None, dtable=None):
+        """sum over frames of sum_i g_ni . dF_ni/dtheta for a cotangent g
+        (K, n, 3) on the forces: the charge gradient (n,) and the table
+        gradient (2, ntypes, ntypes), device f64, accumulated into dq and
+        dtable when given."""
+        X = self.frames(positions)
+        G = torch.as_tensor(cotangent, dtype=torch.float64, device=self.device).reshape(X.shape).contiguous()
+        if dq is None:
+            dq = torch.zeros(self.n, dtype=torch.float64, device=self.device)
+        if dtable is None:
+            dtable = torch.zeros((2, self.ntypes, self.ntypes), dtype=torch.float64, device=self.device)
+        for k in self.schedule(X):
+            self.term.parameter_gradient(X[k], cotangent=G[k], dq=dq, dtable=dtable)
+        return dq, dtable
+
+    def energy_gradient(self, positions):
+        """dU_n/dtheta per frame: charges (K, n) and tables (K, 2, nt, nt)."""
+        X = self.frames(positions)
+        K = X.shape[0]
+        dq = torch.zeros((K, self.n), dtype=torch.float64, device=self.device)
+        dt = torch.zeros((K, 2, self.ntypes, self.ntypes), dtype=torch.float64, device=self.device)
+        disp = None
+        if self.system.get("dispersion", False):
+            disp = torch.as_tensor(self.dispersion_gradient(), device=self.device)
+        for k in self.schedule(X):
+            self.term.parameter_gradient(X[k], dq=dq[k], dtable=dt[k])
+            if disp is not None:
+                dt[k] += disp
+        return dq, dt
+
+    def evaluate(self, positions, cells=None, tilts=None, *, gradients=("tunables",)):
+        """Energies of the frames and the gradients asked for: "positions"
+        (dU/dx, (K, n, 3)) and "tunables" (per frame: sigma (K, nt),
+        epsilon (K, nt), charges (K, n)).  MDIR: FrameEvaluator.evaluate,
+        python/mdir/_frames.py:715.  The cell is the system's (orthorhombic);
+        another cell or tilts are refused."""
+        if tilts is not None:
+            raise UnsupportedError("triclinic cells are not implemented")
+        if cells is not None and not np.allclose(np.asarray(cells, dtype=np.float64).reshape(-1, 3), self.box):
+            raise UnsupportedError("frames in another cell than the system's")
+        for g in gradients:
+            if g not in ("tunables", "positions"):
+                raise ValueError(f"unknown gradient {g!r}")
+        X = self.frames(positions)
+        F, E = self.forces(X, energy=True)
+        out = {}
+        if "positions" in gradients:
+            out["positions"] = -F
+        if "tunables" in gradients:
+            dq, dt = self.energy_gradient(X)
+            tab = dt.cpu().numpy()
+            per = [lorentz_berthelot_chain(tab[k], self.sigma, self.epsilon) for k in range(X.shape[0])]
+            out["tunables"] = {"sigma": np.stack([p[0] for p in per]), "epsilon": np.stack([p[1] for p in per]),
+                               "charges": dq.cpu().numpy()}
+        return FrameEnergies(self, X, E, out)

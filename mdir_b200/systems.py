@@ -184,6 +184,35 @@ def batch_frames(count=256, low=1000, high=8000, seed=4, **kw):
     return [solvated_frame(int(a), seed=int(rng.integers(1 << 30)), **kw) for a in sizes]
 
 
+def force_matching(frames=64, waters=7850, types=8, seed=5, jitter=0.005, perturb=0.02, perturb_seed=6, **kw):
+    """The force-matching workload: `frames` copies of the TIP3P box with
+    every coordinate jittered by N(0, jitter) nm, the oxygens assigned
+    round-robin to `types` LJ types (all at the TIP3P oxygen values,
+    Lorentz-Berthelot tables) and the hydrogens to one more type with
+    epsilon 0.  Returns (system, positions (frames, n, 3), target), where
+    target holds the per-type sigma / epsilon and the charges of the target
+    forces: each value times (1 + perturb s), s a seeded sign pattern."""
+    base = tip3p(waters=waters, **kw)
+    n = 3 * waters
+    t = np.empty(n, dtype=np.int32)
+    t[0::3] = np.arange(waters) % types
+    t[1::3] = types
+    t[2::3] = types
+    sig = np.array([SIG_O] * types + [0.1])
+    eps = np.array([EPS_O] * types + [0.0])
+    sigma, epsilon = _lb_tables(sig, eps)
+    system = dict(base)
+    system.update({"name": f"tip3p-{n}-fm{types}", "types": t, "sigma": sigma, "epsilon": epsilon,
+                   "type_sigma": sig, "type_epsilon": eps})
+    rng = np.random.default_rng(seed)
+    X = base["positions"][None, :, :] + rng.normal(0.0, jitter, size=(frames, n, 3))
+    rs = np.random.default_rng(perturb_seed)
+    target = {"sigma": sig * (1.0 + perturb * rs.choice([-1.0, 1.0], size=sig.shape)),
+              "epsilon": eps * (1.0 + perturb * rs.choice([-1.0, 1.0], size=eps.shape)),
+              "charges": base["charges"] * (1.0 + perturb * rs.choice([-1.0, 1.0], size=n))}
+    return system, X, target
+
+
 def maxwell_velocities(system, temperature, seed=2):
     rng = np.random.default_rng(seed)
     m = np.asarray(system["masses"])

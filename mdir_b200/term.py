@@ -56,6 +56,7 @@ class NonbondedTerm:
         L.check(L.lib().mdrtNbCreate(ctypes.byref(handle), device, self.n), "mdrtNbCreate")
         self._h = handle
         self.box = None
+        self.ntypes = 1
 
     def close(self):
         if getattr(self, "_h", None):
@@ -77,6 +78,7 @@ class NonbondedTerm:
         nt = sg.shape[0]
         L.check(L.lib().mdrtNbSetParticles(self._h, _hp(q), _hp(t), nt, _hp(sg), _hp(ep)),
                 "mdrtNbSetParticles")
+        self.ntypes = nt
 
     def set_exclusions(self, pairs=None, rows=None):
         off, part = rows if rows is not None else exclusion_rows(self.n, pairs if pairs is not None else [])
@@ -158,6 +160,43 @@ class NonbondedTerm:
         out = torch.empty(self.n, dtype=torch.float64, device=self.device)
         L.check(L.lib().mdrtPmePotential(self._h, _dp(out), _stream(stream)), "mdrtPmePotential")
         return out
+
+    def displacement(self, frames, box=None, stream=None):
+        """The largest displacement of each frame (device f64 (K, n, 3))
+        from the positions of the last build (host f64 (K,))."""
+        if not (frames.is_cuda and frames.dtype == torch.float64 and frames.is_contiguous()
+                and frames.shape[-2:] == (self.n, 3)):
+            raise ValueError("frames: a contiguous CUDA float64 tensor of shape (K, n, 3)")
+        count = frames.numel() // (3 * self.n)
+        b = _host(self.box if box is None else box, np.float64)
+        out = np.zeros(count)
+        L.check(L.lib().mdrtNbDisplacement(self._h, _dp(frames), count, _hp(b), _hp(out), _stream(stream)),
+                "mdrtNbDisplacement")
+        return out
+
+    def parameter_gradient(self, x, cotangent=None, box=None, dq=None, dtable=None, ntypes=None,
+                           stream=None):
+        """The gradient in the charges and the sigma / epsilon table at x:
+        with a cotangent g (device f64 (n, 3)) on the forces, the product
+        sum_k g_k . dF_k/dtheta, else dE/dtheta (without the dispersion
+        correction).  Adds into dq (device f64 (n,)) and dtable (device f64
+        (2, ntypes, ntypes)), created as zeros when not given; returns both."""
+        self._check_x(x)
+        b = _host(self.box if box is None else box, np.float64)
+        if dq is None:
+            dq = torch.zeros(self.n, dtype=torch.float64, device=x.device)
+        if dtable is None:
+            nt = self.ntypes if ntypes is None else ntypes
+            dtable = torch.zeros((2, nt, nt), dtype=torch.float64, device=x.device)
+        mode = L.GRAD_ENERGY
+        g = None
+        if cotangent is not None:
+            self._check_x(cotangent)
+            mode = L.GRAD_PRODUCT
+            g = _dp(cotangent)
+        L.check(L.lib().mdrtNbParameterGradient(self._h, _dp(x), _hp(b), g, mode, _dp(dq), _dp(dtable),
+                                                _stream(stream)), "mdrtNbParameterGradient")
+        return dq, dtable
 
     def status(self, clear=False, stream=None):
         v = ctypes.c_int32()

@@ -1,0 +1,101 @@
+"""The frame evaluator as operations of PyTorch (the differentiation form).
+
+`forces(evaluator, sigma, epsilon, charges, positions)` returns the forces
+(K, n, 3) of the frames; autograd differentiates them in the per-type LJ
+sigma / epsilon and the per-atom charges through the hand-written adjoint
+of libmdrt_nb.so (`mdrtNbParameterGradient`, the product mode), which
+recomputes the pair geometry and the reciprocal grids instead of storing
+them.  A force-matching loss (1/K) sum |F - F_ref|^2 therefore costs one
+forward and one adjoint pass per frame.
+
+`evaluate(evaluator, theta, positions)` returns the energies (K,),
+differentiable in theta = {"sigma", "epsilon", "charges"} (the energy mode)
+and in the positions (dU/dx = -F).  MDIR: mdir.torch.evaluate
+(python/mdir/torch.py), a custom op whose backward is the vector-Jacobian
+product of the evaluator.  Forward mode is not implemented, and a second
+derivative in the positions (forces that require a gradient in the
+positions) is refused, as MDIR refuses it for the reciprocal sum."""
+
+import numpy as np
+import torch
+
+from .frames import UnsupportedError, lorentz_berthelot_chain
+
+__all__ = ["forces", "evaluate"]
+
+
+def _host(t):
+    return t.detach().to("cpu", torch.float64).numpy()
+
+
+class _Forces(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, evaluator, positions, sigma, epsilon, charges):
+        evaluator.set_parameters(_host(sigma), _host(epsilon), _host(charges))
+        X = evaluator.frames(positions.detach())
+        F = evaluator.forces(X)
+        ctx.evaluator = evaluator
+        ctx.params = (_host(sigma), _host(epsilon), _host(charges))
+        ctx.save_for_backward(X)
+        return F.reshape(positions.shape)
+
+    @staticmethod
+    def backward(ctx, grad):
+        if ctx.needs_input_grad[1]:
+            raise UnsupportedError("the derivative of the forces in the positions is not implemented")
+        ev = ctx.evaluator
+        (X,) = ctx.saved_tensors
+        ev.set_parameters(*ctx.params)
+        dq, dt = ev.product(X, grad.reshape(X.shape))
+        ds, de = lorentz_berthelot_chain(dt.cpu().numpy(), ev.sigma, ev.epsilon)
+        dev = grad.device
+        return (None, None, torch.as_tensor(ds, device=dev) if ctx.needs_input_grad[2] else None,
+                torch.as_tensor(de, device=dev) if ctx.needs_input_grad[3] else None,
+                dq if ctx.needs_input_grad[4] else None)
+
+
+def forces(evaluator, sigma, epsilon, charges, positions):
+    """Forces (K, n, 3) at the given per-type sigma / epsilon (nt,) and
+    charges (n,), differentiable in the three."""
+    return _Forces.apply(evaluator, positions, sigma, epsilon, charges)
+
+
+class _Energies(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, evaluator, positions, sigma, epsilon, charges):
+        evaluator.set_parameters(_host(sigma), _host(epsilon), _host(charges))
+        X = evaluator.frames(positions.detach())
+        F, E = evaluator.forces(X, energy=True)
+        ctx.evaluator = evaluator
+        ctx.params = (_host(sigma), _host(epsilon), _host(charges))
+        ctx.save_for_backward(X, F)
+        ctx.shape = positions.shape
+        return torch.as_tensor(E, dtype=torch.float64, device=X.device)
+
+    @staticmethod
+    def backward(ctx, grad):
+        ev = ctx.evaluator
+        X, F = ctx.saved_tensors
+        ev.set_parameters(*ctx.params)
+        g = grad.detach().to(torch.float64)
+        out_x = (-(g[:, None, None] * F)).reshape(ctx.shape) if ctx.needs_input_grad[1] else None
+        ds = de = dq = None
+        if any(ctx.needs_input_grad[2:]):
+            q, t = ev.energy_gradient(X)
+            gq = (g[:, None] * q).sum(0)
+            gt = (g[:, None, None, None] * t).sum(0)
+            s_, e_ = lorentz_berthelot_chain(gt.cpu().numpy(), ev.sigma, ev.epsilon)
+            ds = torch.as_tensor(s_, device=grad.device)
+            de = torch.as_tensor(e_, device=grad.device)
+            dq = gq
+        return None, out_x, ds, de, dq
+
+
+def evaluate(evaluator, theta, positions):
+    """Energies (K,) of the frames at theta = {"sigma", "epsilon",
+    "charges"} (tensors; missing entries take the evaluator's values)."""
+    dev = evaluator.device
+    sigma = theta.get("sigma", torch.as_tensor(evaluator.sigma, device=dev))
+    epsilon = theta.get("epsilon", torch.as_tensor(evaluator.epsilon, device=dev))
+    charges = theta.get("charges", torch.as_tensor(evaluator.charges, device=dev))
+    return _Energies.apply(evaluator, positions, sigma, epsilon, charges)
