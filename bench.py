@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--pruned", type=float, default=1.0, help="reach of the pruned inner lists (nm); 0: one list")
     p.add_argument("--equilibrate", type=int, default=5000, help="untimed MD steps before warm-up")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the force-matching gradient leg")
     return p.parse_args()
 
 
@@ -150,6 +151,112 @@ def cpu_baseline(s, x, steps=3):
                       f"(f32 neighbor matrix, f32 row loop, i64 PME spreading, pocketfft via numpy), one "
                       f"matrix rebuild every 10 steps amortised: {tf * 1e3:.1f} ms/eval, "
                       f"{tb * 1e3:.1f} ms/build"}
+
+
+def adjoint_leg(args, dev, flush, world=1, frames=64, reps=5, warmup=3):
+    """Frames/s of the force-matching gradient of the differentiation form:
+    a loss (1/K) sum |F - F_ref|^2 over `frames` jittered copies of the box
+    (8 oxygen LJ types, N(0, 0.005 nm)), differentiated in the 8 sigma, 8
+    epsilon and all charges through mdir_b200.torch.forces (forward, loss,
+    adjoint backward), against the plain per-frame forward plus central
+    differences, 2 forwards per parameter (timed forward x (2P + 1)).
+    With N ranks each takes its own `frames` (weak scaling) and the
+    gradients are summed over the ranks (one f64 all-reduce per batch)."""
+    import torch
+    import torch.distributed as dist
+    from mdir_b200 import FrameEvaluator, systems
+    from mdir_b200 import torch as mtorch
+    s, X, target = systems.force_matching(frames=frames, waters=args.waters)
+    n = X.shape[1]
+    ev = FrameEvaluator(s, device=dev.index)
+    Xd = torch.tensor(X, device=dev)
+    # target forces: the device forward at the perturbed parameters (untimed)
+    ev.set_parameters(target["sigma"], target["epsilon"], target["charges"])
+    F_ref = ev.forces(Xd).clone()
+    sig = torch.tensor(s["type_sigma"], device=dev, requires_grad=True)
+    eps = torch.tensor(s["type_epsilon"], device=dev, requires_grad=True)
+    q = torch.tensor(s["charges"], device=dev, requires_grad=True)
+    hX = torch.tensor(X).pin_memory()
+    host_grad = torch.empty(n + 2 * len(s["type_sigma"]), dtype=torch.float64).pin_memory()
+
+    def step(x):
+        for t in (sig, eps, q):
+            t.grad = None
+        F = mtorch.forces(ev, sig, eps, q, x)
+        loss = ((F - F_ref) ** 2).sum() / frames
+        loss.backward()
+        if world > 1:
+            flat = torch.cat([sig.grad, eps.grad, q.grad])
+            dist.all_reduce(flat)
+        return loss
+
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        step(Xd)
+    torch.cuda.synchronize(dev)
+    builds0 = ev.builds
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step(Xd)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(a.elapsed_time(b))
+    dev_ms = statistics.median(ms)
+    if world > 1:
+        t = torch.tensor([dev_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    # end to end: the frames from pinned host memory, the gradients back
+    e2e = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        x = hX.to(dev, non_blocking=True)
+        step(x)
+        host_grad[:n].copy_(q.grad, non_blocking=True)
+        host_grad[n:n + len(sig)].copy_(sig.grad, non_blocking=True)
+        host_grad[n + len(sig):].copy_(eps.grad, non_blocking=True)
+        torch.cuda.synchronize(dev)
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e)
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    # the plain forward of one frame with the same lists, for the differences
+    Fb = torch.empty_like(Xd)
+    fw = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ev.forces(Xd, out=Fb)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        fw.append(a.elapsed_time(b) / frames)
+    fwd_ms = statistics.median(fw)
+    n_lj = 2 * 8
+    p_all = n_lj + n
+    adj_fps = frames * world / (dev_ms / 1e3)
+    fd_all = 1.0 / (fwd_ms / 1e3 * (2 * p_all + 1))
+    fd_lj = 1.0 / (fwd_ms / 1e3 * (2 * n_lj + 1))
+    return {"metric": "force-matching gradient frames/s (8 sigma + 8 epsilon + all charges)",
+            "frames": frames, "atoms": n, "parameters": p_all,
+            "value": round(adj_fps, 1), "unit": "frames/s", "ms_per_batch": round(dev_ms, 3),
+            "e2e": {"value": round(frames * world / e2e_s, 1), "unit": "frames/s",
+                    "h2d_bytes_per_step": int(X.nbytes), "d2h_bytes_per_step": int(host_grad.numel() * 8)},
+            "forward_ms_per_frame": round(fwd_ms, 4),
+            "fd_frames_per_s": round(fd_all, 4), "fd_frames_per_s_lj_only": round(fd_lj, 2),
+            "speedup_vs_fd": round(adj_fps / fd_all, 1), "speedup_vs_fd_lj_only": round(adj_fps / fd_lj, 2),
+            "builds_in_timed": int(ev.builds - builds0),
+            "gradient_error": "adjoint vs FP64 central differences (h = 1e-5) <= 1e-4 per element "
+                              "(tests/test_gpu_adjoint.py, 23,550 atoms)",
+            "targets": "device forward at parameters x (1 +- 2%)",
+            "l2": "flushed before each timed batch (256 MiB write)"}
 
 
 def run_reference(args):
@@ -257,6 +364,7 @@ def main():
     th1 = md.thermo()
     builds = th1["builds"] - th0["builds"]
     prunes = th1["prunes"] - th0["prunes"]
+    regrows = th1["regrows"] - th0["regrows"]
     ms_per_step = total_ms / args.steps
     value = ns_per_day(args.md_steps * args.steps * world, total_ms / 1e3)
     status = term.status(clear=True)
@@ -326,7 +434,10 @@ def main():
             # gather, pairs, update (cuFFT's own kernels not counted); 16 per
             # build (with the frames and the references) and 5 per pruning
             "gpu_launches": int(args.steps * args.md_steps * 6 + builds * 16 + prunes * 5),
-            "builds": int(builds), "prunes": int(prunes), "temperature_K": round(temp, 1), "status": status}
+            "builds": int(builds), "prunes": int(prunes), "regrows": int(regrows), "regrows_total": th1["regrows"],
+            "temperature_K": round(temp, 1), "status": status}
+    if not args.no_adjoint:
+        line["adjoint"] = adjoint_leg(args, dev, flush, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(s, s["positions"])
     if rank == 0:

@@ -273,12 +273,18 @@ int32_t mdrtMdBuild(mdrtMd *md, const double *x, const double box[3], void *stre
 /* `steps` leap-frog steps of dt (ps) on the device state x, v (f64 [n, 3]);
  * the lists are rebuilt on the device whenever 2 max|x - x_build| > R - r_c.
  * unroll > 0 replays a CUDA graph of `unroll` steps whose rebuilds are
- * conditional nodes (no host wait); unroll = 0 runs step by step. */
+ * conditional nodes (no host wait inside the graphs); the run of graphs
+ * starts from a checkpoint of x, v and the thermostat state and ends in one
+ * host wait that reads what its rebuilds saw: after a list that outgrew its
+ * capacity the run is redone from the checkpoint with grown lists
+ * (count-then-grow, MDIR MDExecToGPU.cpp:10107-10175), and positions that
+ * are not finite return MDRT_NB_NAN_POSITION.  unroll = 0 runs step by step,
+ * the host reading the test of validity after each step. */
 int32_t mdrtMdRun(mdrtMd *md, double *x, double *v, const double box[3], double dt, int64_t steps,
                   int32_t unroll, void *stream);
-/* out[7]: thermostat scaling, kinetic energy of the last two half steps,
- * steps taken, builds made, degrees of freedom, prunings made; waits for
- * `stream`. */
+/* out[8]: thermostat scaling, kinetic energy of the last two half steps,
+ * steps taken, builds made, degrees of freedom, prunings made, runs of step
+ * graphs redone after a list overflow; waits for `stream`. */
 int32_t mdrtMdThermo(mdrtMd *md, void *stream, double *out);
 /* The device array of the forces of the last step (f64 [n, 3]). */
 int32_t mdrtMdForces(mdrtMd *md, double **forces);

@@ -320,8 +320,10 @@ class Simulation:
         return State(self.x.cpu().numpy(), self.v.cpu().numpy(), self.step)
 
     def energies(self):
-        """The potential energy terms (kJ/mol) and the kinetic energy at the
-        current positions."""
+        """The potential energy terms (kJ/mol) at the current positions and
+        the kinetic energy of leap-frog, the mean of the last two half steps
+        (centred one step behind the positions; `Integrator.total_energy`
+        pairs them at the same time, by one more step)."""
         f = self.term.force(self.x, self.box, energy=True)
         e = self.term.energies()
         c = self.term.constants(self.box, dispersion=self.program.system.dispersion)

@@ -836,3 +836,10 @@ int nb_build_run(NbCtx &c, const double *x, const double box[3], cudaStream_t s)
   }
   return -1;
 }
+
+int nb_grow_lists(NbCtx &c, int64_t longest) {
+  int64_t want = (longest + longest / 4 + NB_UNIT - 1) / NB_UNIT * NB_UNIT;
+  if (want <= c.list_cap) return 0;
+  c.grows++;
+  return nb_reserve(c, c.grid, want);
+}

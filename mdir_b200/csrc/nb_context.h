@@ -146,6 +146,9 @@ void nb_build_launch_public(NbCtx &c, const double *x, const double box[3], cuda
 void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s);
 // Allocates the inner lists to the outer capacities (host, between launches).
 int nb_reserve_inner(NbCtx &c);
+// Grows the list capacity for lists of up to `longest` entries (+25%), as
+// the count of a build that overflowed asks (host, between launches).
+int nb_grow_lists(NbCtx &c, int64_t longest);
 void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
 void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);

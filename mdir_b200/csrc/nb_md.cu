@@ -50,6 +50,13 @@ struct mdrtMd {
   double *thermo = nullptr;        // [0] lambda, [1] KE, [2] KE before, [3] steps, [4] builds, [5] prunes
   double *noise = nullptr;         // thermostat draws of the steps of one launch (2 a step)
   int *flag = nullptr;             // [0] rebuild, [1] prune: flags for the step-by-step path
+  // The checkpoint of a run of step graphs (positions, velocities, thermo)
+  // and what its builds saw: [0] the longest list, [1] capacity overflow
+  // bits, [2] builds that met positions that are not finite.
+  double *x_ck = nullptr, *v_ck = nullptr, *thermo_ck = nullptr;
+  double *xref_ck = nullptr, *xprune_ck = nullptr;  // the reference positions of the lists in force
+  int32_t *peak = nullptr, *h_peak = nullptr;
+  int64_t regrows = 0;             // runs redone after an overflow inside the graphs
   double temperature = 300.0, tau = 0.0;
   int64_t ndof = 0;
   unsigned long long seed = 1;
@@ -455,17 +462,28 @@ __global__ void md_set_inner(const int *flag, cudaGraphConditionalHandle h_build
   if (dual) cudaGraphSetConditional(h_prune, flag[1]);
 }
 
-// After a build: the reference positions and the counters.
+// After a build: the reference positions, the counters, and what the build
+// saw (the longest list, overflow, positions that are not finite), for the
+// host check at the end of a run of step graphs.
 __global__ void md_after_build(int64_t n3, const double *__restrict__ x, double *__restrict__ x_ref,
-                               double *thermo, const int32_t *sizes, int *status) {
+                               double *thermo, const int32_t *sizes, int *status, int32_t *peak) {
   int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n3) x_ref[k] = x[k];
   if (k == 0) {
     thermo[4] += 1.0;
-    if (sizes[NB_SIZE_OVERFLOW] != 0) atomicOr(status, NB_STATUS_LIST_OVERFLOW);
-    if (sizes[NB_SIZE_NAN] != 0) atomicOr(status, NB_STATUS_NAN);
+    atomicMax(&peak[0], sizes[NB_SIZE_LONGEST]);
+    if (sizes[NB_SIZE_OVERFLOW] != 0) {
+      atomicOr(status, NB_STATUS_LIST_OVERFLOW);
+      atomicOr(&peak[1], sizes[NB_SIZE_OVERFLOW]);
+    }
+    if (sizes[NB_SIZE_NAN] != 0) {
+      atomicOr(status, NB_STATUS_NAN);
+      atomicAdd(&peak[2], 1);
+    }
   }
 }
+
+__global__ void md_clear_status(int *status, int bits) { atomicAnd(status, ~bits); }
 
 // After a pruning: the reference positions of the inner list.
 __global__ void md_after_prune(int64_t n3, const double *__restrict__ x, double *__restrict__ x_prune,
@@ -545,7 +563,8 @@ static void md_rebuild_body(mdrtMd &m, const double *x, const double box[3], cud
   NbCtx &c = *m.nb;
   nb_build_launch_public(c, x, box, s);
   nb_gather_frames(c, x, box, s);
-  md_after_build<<<blocks_for(3 * m.n, 256), 256, 0, s>>>(3 * m.n, x, m.x_ref, m.thermo, c.sizes, c.status);
+  md_after_build<<<blocks_for(3 * m.n, 256), 256, 0, s>>>(3 * m.n, x, m.x_ref, m.thermo, c.sizes, c.status,
+                                                          m.peak);
 }
 
 static void md_drop_graph(mdrtMd *m) {
@@ -564,8 +583,10 @@ static void md_free(mdrtMd *m) {
   for (void *p : {(void *)m->inv_mass, (void *)m->mass, (void *)m->waters, (void *)m->free_atoms,
                   (void *)m->excl_other, (void *)m->force, (void *)m->x_ref, (void *)m->x_prune,
                   (void *)m->ke_part, (void *)m->maxd2, (void *)m->thermo, (void *)m->flag,
-                  (void *)m->noise})
+                  (void *)m->noise, (void *)m->x_ck, (void *)m->v_ck, (void *)m->thermo_ck, (void *)m->peak,
+                  (void *)m->xref_ck, (void *)m->xprune_ck})
     if (p) cudaFree(p);
+  if (m->h_peak) cudaFreeHost(m->h_peak);
   delete m;
 }
 
@@ -658,6 +679,13 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
             cudaMalloc(&m->thermo, sizeof(double) * 8) == cudaSuccess &&
             cudaMalloc(&m->noise, sizeof(double) * 2 * MD_MAX_UNROLL) == cudaSuccess &&
             cudaMalloc(&m->flag, sizeof(int) * 2) == cudaSuccess &&
+            cudaMalloc(&m->x_ck, sizeof(double) * 3 * c.n) == cudaSuccess &&
+            cudaMalloc(&m->v_ck, sizeof(double) * 3 * c.n) == cudaSuccess &&
+            cudaMalloc(&m->thermo_ck, sizeof(double) * 8) == cudaSuccess &&
+            cudaMalloc(&m->xref_ck, sizeof(double) * 3 * c.n) == cudaSuccess &&
+            cudaMalloc(&m->xprune_ck, sizeof(double) * 3 * c.n) == cudaSuccess &&
+            cudaMalloc(&m->peak, sizeof(int32_t) * 4) == cudaSuccess &&
+            cudaMallocHost(&m->h_peak, sizeof(int32_t) * 4) == cudaSuccess &&
             cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, hi) == cudaSuccess &&
             cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming) == cudaSuccess;
@@ -674,6 +702,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
   double th[8] = {1.0, 0, 0, 0, 0, 0, 0, 0};
   cudaMemcpy(m->thermo, th, sizeof(th), cudaMemcpyHostToDevice);
   cudaMemset(m->maxd2, 0, sizeof(unsigned int) * 4);
+  cudaMemset(m->peak, 0, sizeof(int32_t) * 4);
   cudaMemset(m->force, 0, sizeof(double) * 3 * c.n);
   *out = m;
   return MDRT_NB_OK;
@@ -706,7 +735,8 @@ int32_t mdrtMdBuild(mdrtMd *m, const double *x, const double box[3], void *strea
   cudaStream_t st = (cudaStream_t)stream;
   NbCtx &c = *m->nb;
   nb_gather_frames(c, x, box, st);
-  md_after_build<<<blocks_for(3 * m->n, 256), 256, 0, st>>>(3 * m->n, x, m->x_ref, m->thermo, c.sizes, c.status);
+  md_after_build<<<blocks_for(3 * m->n, 256), 256, 0, st>>>(3 * m->n, x, m->x_ref, m->thermo, c.sizes, c.status,
+                                                            m->peak);
   if (c.inner_reach > 0.0) {
     md_prune_body(*m, x, box, st);
     c.inner_valid = true;
@@ -744,36 +774,10 @@ static cudaError_t md_capture_if(cudaStream_t cap, cudaStream_t body, cudaGraphC
   return cudaStreamEndCapture(body, nullptr);
 }
 
-extern "C" {
-
-int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
-                  int32_t unroll, void *stream) {
-  if (!m || !x || !v || !box || !(dt > 0) || steps < 0 || unroll > MD_MAX_UNROLL) return MDRT_NB_INVALID_ARGUMENT;
+// The graph of `unroll` steps, each ending in a conditional rebuild,
+// captured again when its arguments or the capacities changed.
+static int32_t md_prepare_graph(mdrtMd *m, double *x, double *v, const double box[3], double dt, int32_t unroll) {
   NbCtx &c = *m->nb;
-  if (!c.built) return MDRT_NB_NOT_BUILT;
-  for (int k = 0; k < 3; ++k)
-    if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;
-  cudaSetDevice(c.device);
-  cudaStream_t st = (cudaStream_t)stream;
-  if (unroll <= 0) {
-    // step by step, the host reading the tests of validity after each step
-    int h_flag[2] = {0, 0};
-    for (int64_t k = 0; k < steps; ++k) {
-      md_noise<<<1, 32, 0, st>>>(m->thermo, m->noise, 1, (double)m->ndof, m->seed);
-      md_step_body(*m, x, v, box, dt, st, 0, 0, m->flag, 0);
-      cudaMemcpyAsync(h_flag, m->flag, sizeof(h_flag), cudaMemcpyDeviceToHost, st);
-      cudaStreamSynchronize(st);
-      if (h_flag[0]) {
-        int32_t s = mdrtMdBuild(m, x, box, stream);
-        if (s) return s;
-      } else if (h_flag[1]) {
-        md_prune_body(*m, x, box, st);
-        c.prunes++;
-      }
-    }
-    return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
-  }
-  // a graph of `unroll` steps, each ending in a conditional rebuild
   int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap + (int64_t)(c.inner_reach * 1e9) +
                 (c.inner_valid ? 1 : 0) + (c.deterministic ? 2 : 0);
   bool stale = !m->exec || m->gx != x || m->gv != v || m->gdt != dt || m->gunroll != unroll ||
@@ -841,9 +845,88 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
     m->gcap_key = key;
     for (int k = 0; k < 3; ++k) m->gbox[k] = box[k];
   }
+  return MDRT_NB_OK;
+}
+
+extern "C" {
+
+int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
+                  int32_t unroll, void *stream) {
+  if (!m || !x || !v || !box || !(dt > 0) || steps < 0 || unroll > MD_MAX_UNROLL) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = *m->nb;
+  if (!c.built) return MDRT_NB_NOT_BUILT;
+  for (int k = 0; k < 3; ++k)
+    if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;
+  cudaSetDevice(c.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (unroll <= 0) {
+    // step by step, the host reading the tests of validity after each step
+    int h_flag[2] = {0, 0};
+    for (int64_t k = 0; k < steps; ++k) {
+      md_noise<<<1, 32, 0, st>>>(m->thermo, m->noise, 1, (double)m->ndof, m->seed);
+      md_step_body(*m, x, v, box, dt, st, 0, 0, m->flag, 0);
+      cudaMemcpyAsync(h_flag, m->flag, sizeof(h_flag), cudaMemcpyDeviceToHost, st);
+      cudaStreamSynchronize(st);
+      if (h_flag[0]) {
+        int32_t s = mdrtMdBuild(m, x, box, stream);
+        if (s) return s;
+      } else if (h_flag[1]) {
+        md_prune_body(*m, x, box, st);
+        c.prunes++;
+      }
+    }
+    return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
+  }
+  // Runs of step graphs.  A rebuild inside a graph that overflows a list
+  // leaves the following steps with incomplete lists, so each run starts
+  // from a checkpoint (positions, velocities, thermostat state, and the
+  // positions the lists in force were built and pruned at) and ends in one
+  // read of what its builds saw.  After an overflow the run goes back to the
+  // checkpoint, grows the lists to the longest count (+25%), builds and
+  // prunes them again where they were built and pruned (the same lists and
+  // the same schedule of rebuilds, with room), and runs again.  Positions
+  // that are not finite end the run.
   int64_t launches = steps / unroll;
-  for (int64_t k = 0; k < launches; ++k)
-    if (cudaGraphLaunch(m->exec, st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
+  size_t bytes = sizeof(double) * 3 * m->n;
+  bool dual = c.inner_reach > 0.0 && c.inner_valid;
+  for (int attempt = 0; launches > 0; ++attempt) {
+    int32_t s = md_prepare_graph(m, x, v, box, dt, unroll);
+    if (s) return s;
+    if (cudaMemcpyAsync(m->x_ck, x, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(m->v_ck, v, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(m->xref_ck, m->x_ref, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        (dual && cudaMemcpyAsync(m->xprune_ck, m->x_prune, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) ||
+        cudaMemcpyAsync(m->thermo_ck, m->thermo, sizeof(double) * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(m->peak, 0, sizeof(int32_t) * 4, st) != cudaSuccess)
+      return MDRT_NB_CUDA_ERROR;
+    for (int64_t k = 0; k < launches; ++k)
+      if (cudaGraphLaunch(m->exec, st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
+    if (cudaMemcpyAsync(m->h_peak, m->peak, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return MDRT_NB_CUDA_ERROR;
+    if (m->h_peak[2] > 0) return MDRT_NB_NAN_POSITION;
+    if (m->h_peak[1] == 0) break;
+    if (attempt >= 8) return MDRT_NB_GROW;
+    if (cudaMemcpyAsync(x, m->x_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(v, m->v_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return MDRT_NB_CUDA_ERROR;
+    md_clear_status<<<1, 1, 0, st>>>(c.status, NB_STATUS_LIST_OVERFLOW);
+    if (nb_grow_lists(c, m->h_peak[0])) return MDRT_NB_CUDA_ERROR;
+    s = mdrtNbBuild(m->handle, m->xref_ck, m->n, box, 0.0, stream, nullptr);
+    if (s) return s;
+    if (cudaMemcpyAsync(m->x_ref, m->xref_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return MDRT_NB_CUDA_ERROR;
+    if (dual) {
+      nb_gather_frames(c, m->xprune_ck, box, st);
+      md_prune_body(*m, m->xprune_ck, box, st);
+      c.inner_valid = true;
+    }
+    nb_gather_frames(c, x, box, st);
+    // the counters of the checkpoint: the build and pruning above redo ones it had
+    if (cudaMemcpyAsync(m->thermo, m->thermo_ck, sizeof(double) * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return MDRT_NB_CUDA_ERROR;
+    m->regrows++;
+  }
   int64_t rest = steps - launches * unroll;
   if (rest > 0) return mdrtMdRun(m, x, v, box, dt, rest, 0, stream);
   return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
@@ -860,6 +943,7 @@ int32_t mdrtMdThermo(mdrtMd *m, void *stream, double *out) {
   for (int k = 0; k < 5; ++k) out[k] = h[k];
   out[5] = (double)m->ndof;
   out[6] = h[5];
+  out[7] = (double)m->regrows;
   return MDRT_NB_OK;
 }
 

@@ -59,6 +59,7 @@ class Integrator:
         L.check(L.lib().mdrtMdThermo(self._h, _stream(stream), _hp(out)), "mdrtMdThermo")
         return {"lambda": out[0], "kinetic_half": out[1], "kinetic_half_before": out[2],
                 "steps": int(out[3]), "builds": int(out[4]), "ndof": int(out[5]), "prunes": int(out[6]),
+                "regrows": int(out[7]),
                 "kinetic": 0.5 * (out[1] + out[2])}
 
     def forces(self):
@@ -69,3 +70,21 @@ class Integrator:
     def temperature(self, stream=None):
         t = self.thermo(stream)
         return 2.0 * t["kinetic"] / (t["ndof"] * KB)
+
+    def total_energy(self, x, v, box, dt, dispersion=False, stream=None):
+        """The total energy at the current positions x_N, for energy
+        conservation: the potential at x_N and the kinetic energy centred at
+        N, the mean of the half steps N - 1/2 and N + 1/2 of leap-frog.  The
+        half step N + 1/2 is one more MD step, so this advances the state by
+        one step.  (The kinetic energy of `thermo` is centred one step behind
+        the positions; paired with the potential at x_N it is off by O(dt).)
+        Returns (total, potential, kinetic)."""
+        t = self.term
+        t.force(x, box, energy=True, stream=stream)
+        e = t.energies(stream)
+        c = t.constants(box, dispersion=dispersion)
+        pot = e["lj"] + e["coulomb"] + e["excluded"] + e["reciprocal"] + c["self"] + c["background"] + \
+            c["dispersion"]
+        self.run(x, v, box, dt, 1, unroll=0, stream=stream)
+        kin = self.thermo(stream)["kinetic"]
+        return pot + kin, pot, kin
