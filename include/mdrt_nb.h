@@ -48,7 +48,8 @@ enum mdrtNbFlags {
   MDRT_NB_POTENTIAL = 4u,    /* also gather dE_rec/dq (mdrtPmePotential) */
   MDRT_NB_NO_PAIRS = 8u,     /* skip the pair term */
   MDRT_NB_NO_PME = 16u,      /* skip the reciprocal sum */
-  MDRT_NB_NO_EXCLUDED = 32u  /* skip the excluded-pair correction */
+  MDRT_NB_NO_EXCLUDED = 32u, /* skip the excluded-pair correction */
+  MDRT_NB_GRAPH = 64u        /* mdrtNbBatchForce: replay the launches as a CUDA graph */
 };
 
 /* Slots of the energies of mdrtNbEnergies (f64). */
@@ -136,7 +137,7 @@ int32_t mdrtNbPrune(mdrtNb *ctx, const double *x, const double box[3], void *str
  * kernels beside it).  Returns MDRT_NB_INVALID_ARGUMENT for an unknown key
  * or value.  No MDIR counterpart: MDIR fixes these in its emitters
  * (lib/Dialect/MDExec/DevicePolicy.cpp:72-99). */
-enum mdrtNbTuneKey { MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM = 0 };
+enum mdrtNbTuneKey { MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM = 0, MDRT_NB_TUNE_SEARCH_WARPS = 1 };
 int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value);
 
 /* Deterministic mode: 64-bit fixed-point force accumulation (2^32 per
@@ -323,6 +324,62 @@ int32_t mdrtCudaFFTForward3DF32(const float *real, float *complex_out, int64_t k
                                 int64_t k3, void *stream);
 int32_t mdrtCudaFFTBackward3DF32(float *complex_in, float *real_out, int64_t k1, int64_t k2,
                                  int64_t k3, void *stream);
+
+/* ---- Batches of frames (the batching form) --------------------------------
+ * Many independent systems ("frames") of uneven sizes, each with its own
+ * orthorhombic cell and PME grid, evaluated together: the atoms of frame f
+ * are atoms atom0[f] .. atom0[f+1]-1 of the batch (frames one after the
+ * other), and every stage (the build, the pair kernel, the excluded pairs,
+ * PME) is one launch over all frames, the pair kernel one persistent grid
+ * over the units of every frame.  The frames share the interaction (cutoff,
+ * reach, beta), the LJ type table and the spline order.  Deterministic mode,
+ * the dual list and the switched LJ form are not offered for batches.
+ * MDIR: frames are evaluated one after another (D251,
+ * docs/python-frames.md:1178), its device batch (D386, docs/driver.md:
+ * 1655-1700; python/mdir/_frames.py:769) loops over frames of one program. */
+typedef struct mdrtNbBatch mdrtNbBatch;
+
+/* A batch of `frames` frames with atoms[f] atoms each (host). */
+int32_t mdrtNbBatchCreate(mdrtNbBatch **out, int32_t device, int32_t frames, const int64_t *atoms);
+int32_t mdrtNbBatchDestroy(mdrtNbBatch *batch);
+/* As mdrtNbSetParticles over all atoms of the batch; one type table. */
+int32_t mdrtNbBatchSetParticles(mdrtNbBatch *batch, const double *charges, const int32_t *types,
+                                int32_t ntypes, const double *sigma, const double *epsilon);
+/* As mdrtNbSetExclusions in the batch's numbering; every pair inside one
+ * frame (else MDRT_NB_INVALID_ARGUMENT). */
+int32_t mdrtNbBatchSetExclusions(mdrtNbBatch *batch, const int32_t *offsets, const int32_t *partners);
+int32_t mdrtNbBatchSetInteraction(mdrtNbBatch *batch, double cutoff, double reach, double beta,
+                                  double coulomb);
+/* The PME grid of each frame, grids[3 f + k] (host), and the spline order
+ * (4 or 8).  Frames of one shape share one batched cuFFT plan pair. */
+int32_t mdrtNbBatchPmeSetup(mdrtNbBatch *batch, const int32_t *grids, int32_t order);
+/* MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM (1-4) and MDRT_NB_TUNE_SEARCH_WARPS (1 or
+ * 4 warps a group in the search); results do not depend on them. */
+int32_t mdrtNbBatchSetTuning(mdrtNbBatch *batch, int32_t key, int32_t value);
+/* The build of all frames at device positions x (f64 [n, 3], the batch's
+ * numbering) in the cells boxes[3 f + k] (host); grows and builds again
+ * until every list fits (host wait), as mdrtNbBuild. */
+int32_t mdrtNbBatchBuild(mdrtNbBatch *batch, const double *x, const double *boxes, void *stream,
+                         int32_t *sizes_out);
+/* Forces of all frames (device f64 [n, 3]); flags as mdrtNbForce, plus
+ * MDRT_NB_GRAPH: the launches captured once as a CUDA graph and replayed
+ * (captured again when the buffers, pointers or flags change).  With
+ * MDRT_NB_ENERGY the energies of each frame are summed in a fixed order. */
+int32_t mdrtNbBatchForce(mdrtNbBatch *batch, const double *x, uint32_t flags, double *forces, void *stream);
+/* out[f * MDRT_NB_E_COUNT + slot]: the energies and virials of each frame
+ * (slots of mdrtNbEnergySlot) of the last MDRT_NB_ENERGY evaluation; waits. */
+int32_t mdrtNbBatchEnergies(mdrtNbBatch *batch, void *stream, double *out);
+/* out[2 f]: the Ewald self term of frame f, out[2 f + 1] its background
+ * term (host, f64), in the cells of the last build. */
+int32_t mdrtNbBatchConstants(mdrtNbBatch *batch, double *out);
+/* The project's autotuner: times a build and an evaluation with energies
+ * for every search width (4, 1 warps a group) and pair-kernel occupancy
+ * (4..1 blocks per SM), keeps the fastest, and writes it to choice[2] =
+ * {search warps, pair blocks per SM}.  Needs a build (for the cells);
+ * `forces` is scratch (device f64 [n, 3]).  No MDIR counterpart: MDIR's
+ * launch shapes are fixed by its emitters (DevicePolicy.cpp:72-99). */
+int32_t mdrtNbBatchAutotune(mdrtNbBatch *batch, const double *x, double *forces, void *stream,
+                            int32_t *choice);
 
 #ifdef __cplusplus
 }

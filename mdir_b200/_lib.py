@@ -12,7 +12,8 @@ LIBRARY = HERE / "libmdrt_nb.so"
 # Status codes, flags and slots (include/mdrt_nb.h).
 OK, GROW, NAN_POSITION, INVALID_BOX, CUDA_ERROR, TIMEOUT, INVALID_ARGUMENT, UNSUPPORTED, \
     OVERFLOW, NOT_BUILT = range(10)
-ENERGY, ACCUMULATE, POTENTIAL, NO_PAIRS, NO_PME, NO_EXCLUDED = 1, 2, 4, 8, 16, 32
+ENERGY, ACCUMULATE, POTENTIAL, NO_PAIRS, NO_PME, NO_EXCLUDED, GRAPH = 1, 2, 4, 8, 16, 32, 64
+TUNE_PAIR_BLOCKS_PER_SM, TUNE_SEARCH_WARPS = 0, 1
 E_LJ, E_COULOMB, E_EXCLUDED, E_RECIPROCAL, W_PAIR, W_RECIPROCAL, E_COUNT = 0, 1, 2, 3, 4, 10, 16
 SIZE_PLACES, SIZE_LONGEST, SIZE_UNITS, SIZE_EXCL_WIDE, SIZE_NAN, SIZE_OVERFLOW, SIZE_GROUPS, \
     SIZE_ENTRIES, SIZE_COUNT = range(9)
@@ -56,6 +57,18 @@ SIGNATURES = {
     "mdrtMdThermo": (_i32, [_p, _p, _p]),
     "mdrtMdForces": (_i32, [_p, ctypes.POINTER(_p)]),
     "mdrtNbExcludedNoAlloc": (_i32, [_p, _p, _p, _i64, _p, _d, _d, _p, _p, _p]),
+    "mdrtNbBatchCreate": (_i32, [ctypes.POINTER(_p), _i32, _i32, _p]),
+    "mdrtNbBatchDestroy": (_i32, [_p]),
+    "mdrtNbBatchSetParticles": (_i32, [_p, _p, _p, _i32, _p, _p]),
+    "mdrtNbBatchSetExclusions": (_i32, [_p, _p, _p]),
+    "mdrtNbBatchSetInteraction": (_i32, [_p, _d, _d, _d, _d]),
+    "mdrtNbBatchPmeSetup": (_i32, [_p, _p, _i32]),
+    "mdrtNbBatchSetTuning": (_i32, [_p, _i32, _i32]),
+    "mdrtNbBatchBuild": (_i32, [_p, _p, _p, _p, _p]),
+    "mdrtNbBatchForce": (_i32, [_p, _p, _u32, _p, _p]),
+    "mdrtNbBatchEnergies": (_i32, [_p, _p, _p]),
+    "mdrtNbBatchConstants": (_i32, [_p, _p]),
+    "mdrtNbBatchAutotune": (_i32, [_p, _p, _p, _p, _p]),
     "mdrtCudaFFTForward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
     "mdrtCudaFFTBackward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
 }

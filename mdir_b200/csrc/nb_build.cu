@@ -192,8 +192,10 @@ struct SearchParams {
 // window are cut into W contiguous shares, each warp stages its entries in
 // shared memory (list_cap each) and the block writes them in warp order, so
 // a list is the same for every W.
-template <int W>
-__global__ void __launch_bounds__(128) nb_search_t(SearchParams P, const int32_t *sizes_in,
+template <int W, bool BATCH>
+__global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFrameDev *__restrict__ frames,
+                                                   const int32_t *__restrict__ group_frame,
+                                                   const int32_t *sizes_in,
                                                    const int32_t *__restrict__ order,
                                                    const float4 *__restrict__ xw,
                                                    const float4 *__restrict__ box_lo,
@@ -217,8 +219,24 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P, const int32_t
   int gi = warp / W, part = warp % W;
   int64_t g = (int64_t)blockIdx.x * GPB + gi;
   int ngroups = sizes_in[NB_SIZE_GROUPS];
-  bool live = g < ngroups && g < P.groups_cap;
+  bool live = g < ngroups && g < P0.groups_cap;
   if (W == 1 && !live) return;
+  // a frame of a batch: its cell, grid, reach and first column
+  SearchParams P = P0;
+  int col0 = 0;
+  if (BATCH && live) {
+    const NbFrameDev &F = frames[group_frame[g]];
+    P.Lx = F.Lf0;
+    P.Ly = F.Lf1;
+    P.Lz = F.Lf2;
+    P.wx = F.wx;
+    P.wy = F.wy;
+    P.Nx = F.Nx;
+    P.Ny = F.Ny;
+    P.R2f = F.R2f;
+    P.Rbox = F.Rbox;
+    col0 = F.col0;
+  }
 
   // members and the exclusion partners of the members: keys (partner atom,
   // member), sorted; by the first warp of the group
@@ -320,7 +338,7 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P, const int32_t
       int sy = (ky - cy) / P.Ny;
       int cx = ((kx % P.Nx) + P.Nx) % P.Nx;
       int sx = (kx - cx) / P.Nx;
-      int c = cy * P.Nx + cx;
+      int c = col0 + cy * P.Nx + cx;
       int hb = max(group_start[c], (int)g), he = group_start[c + 1];
       if (hb >= he) continue;
       for (int sz = sz0; sz <= sz1; ++sz) {
@@ -626,12 +644,13 @@ static int nb_realloc(T *&p, int64_t count) {
   return e == cudaSuccess ? 0 : -1;
 }
 
-// Sizes the buffers for n atoms, the grid and the list capacity C.
-static int nb_reserve(NbCtx &c, const NbGrid &G, int64_t list_cap) {
+// Sizes the buffers for n atoms, the planned columns and bins
+// (c.plan_cols, c.plan_bins) and the list capacity C.
+static int nb_reserve(NbCtx &c, int64_t list_cap) {
   int64_t n = c.n;
-  int64_t cols = G.ncol();
+  int64_t cols = c.plan_cols;
   int64_t groups = (n + NB_GROUP - 1) / NB_GROUP + cols;  // at most one partial group a column
-  int64_t bins = G.nbins() + 1;
+  int64_t bins = c.plan_bins + 1;
   if (bins > c.bins_cap) {
     int64_t cap = bins + bins / 4;
     if (nb_realloc(c.bin_count, cap) || nb_realloc(c.bin_start, cap + 1) || nb_realloc(c.bin_fill, cap))
@@ -732,16 +751,17 @@ static void nb_build_launch(NbCtx &c, const double *x, const double box[3], cuda
   if (stage <= 200 * 1024) {
     static size_t configured = 0;
     if (stage > 48 * 1024 && configured < stage) {
-      cudaFuncSetAttribute(nb_search_t<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+      cudaFuncSetAttribute(nb_search_t<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
       configured = stage;
     }
-    nb_search_t<4><<<(int)c.groups_cap, 128, stage, s>>>(P, c.sizes, c.order, c.xw, c.box_lo, c.box_hi,
-                                                         c.group_start, c.excl_off, c.excl, c.slab, c.counts,
-                                                         c.sizes);
+    nb_search_t<4, false><<<(int)c.groups_cap, 128, stage, s>>>(P, nullptr, nullptr, c.sizes, c.order, c.xw,
+                                                                c.box_lo, c.box_hi, c.group_start, c.excl_off,
+                                                                c.excl, c.slab, c.counts, c.sizes);
   } else {
-    nb_search_t<1><<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, c.sizes, c.order, c.xw, c.box_lo, c.box_hi,
-                                                               c.group_start, c.excl_off, c.excl, c.slab,
-                                                               c.counts, c.sizes);
+    nb_search_t<1, false><<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, nullptr, nullptr, c.sizes, c.order, c.xw,
+                                                                      c.box_lo, c.box_hi, c.group_start,
+                                                                      c.excl_off, c.excl, c.slab, c.counts,
+                                                                      c.sizes);
   }
   nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts,
                                                              c.list_cap, c.unit_n);
@@ -803,13 +823,15 @@ int nb_build_run(NbCtx &c, const double *x, const double box[3], cudaStream_t s)
   int64_t cap = c.list_cap;
   if (cap == 0) cap = nb_initial_list_cap(c.n, box, c.reach, G);
   c.grid = G;
+  c.plan_cols = G.ncol();
+  c.plan_bins = G.nbins();
   if (!c.key) {
     if (nb_realloc(c.key, c.n) || nb_realloc(c.sorted, c.n) || nb_realloc(c.atom_xw, c.n) ||
         nb_realloc(c.atom_shift, c.n) || nb_realloc(c.place_of, c.n))
       return -1;
   }
   for (int attempt = 0; attempt < 8; ++attempt) {
-    if (nb_reserve(c, G, cap)) return -1;
+    if (nb_reserve(c, cap)) return -1;
     nb_build_launch(c, x, box, s);
     NB_CHECK(cudaMemcpyAsync(c.h_sizes, c.sizes, sizeof(int32_t) * NB_SIZE_COUNT,
                              cudaMemcpyDeviceToHost, s));
@@ -841,5 +863,262 @@ int nb_grow_lists(NbCtx &c, int64_t longest) {
   int64_t want = (longest + longest / 4 + NB_UNIT - 1) / NB_UNIT * NB_UNIT;
   if (want <= c.list_cap) return 0;
   c.grows++;
-  return nb_reserve(c, c.grid, want);
+  return nb_reserve(c, want);
+}
+
+// ---------------------------------------------------------------------------
+// The build of a batch of frames (mdrtNbBatch).  The same stages as one
+// system's, each one launch over all frames: the bins and columns of frame
+// f start at F.bin0 and F.col0, so that the counting sort, the scans and
+// the groups are those of one grid laid end to end, and the search of a
+// group reads its frame's cell, grid and reach.
+
+namespace {
+
+__global__ void nb_batch_keys(int64_t n, const double *__restrict__ x, const int32_t *__restrict__ atom_frame,
+                              const NbFrameDev *__restrict__ frames, int nbins, int32_t *__restrict__ key,
+                              int32_t *__restrict__ atom_col, int32_t *__restrict__ bin_count,
+                              float4 *__restrict__ atom_xw, char4 *__restrict__ atom_shift,
+                              int32_t *__restrict__ sizes) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const NbFrameDev &F = frames[atom_frame[i]];
+  double v0 = x[3 * i], v1 = x[3 * i + 1], v2 = x[3 * i + 2];
+  bool ok = isfinite(v0) && isfinite(v1) && isfinite(v2);
+  double S0 = 0, S1 = 0, S2 = 0;
+  if (ok) {
+    S0 = -floor(v0 / F.L0);
+    S1 = -floor(v1 / F.L1);
+    S2 = -floor(v2 / F.L2);
+    ok = fabs(S0) <= 100.0 && fabs(S1) <= 100.0 && fabs(S2) <= 100.0;
+  }
+  if (!ok) {
+    key[i] = nbins;
+    atom_col[i] = -1;
+    atomicAdd(&bin_count[nbins], 1);
+    atomicAdd(&sizes[NB_SIZE_NAN], 1);
+    atom_xw[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    atom_shift[i] = make_char4(0, 0, 0, 0);
+    return;
+  }
+  float w0 = (float)(v0 + S0 * F.L0), w1 = (float)(v1 + S1 * F.L1), w2 = (float)(v2 + S2 * F.L2);
+  int kx = min(max((int)(w0 * F.inv_wx), 0), F.Nx - 1);
+  int ky = min(max((int)(w1 * F.inv_wy), 0), F.Ny - 1);
+  int kz = min(max((int)(w2 * F.inv_hz), 0), F.Nz - 1);
+  int col = ky * F.Nx + kx;
+  int k = F.bin0 + col * F.Nz + kz;
+  key[i] = k;
+  atom_col[i] = F.col0 + col;
+  atomicAdd(&bin_count[k], 1);
+  atom_xw[i] = make_float4(w0, w1, w2, 1.f);
+  atom_shift[i] = make_char4((signed char)S0, (signed char)S1, (signed char)S2, 0);
+}
+
+__global__ void nb_batch_col_groups(int ncol, const int32_t *__restrict__ col_frame,
+                                    const NbFrameDev *__restrict__ frames, const int32_t *__restrict__ bin_start,
+                                    int32_t *__restrict__ col_groups) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const NbFrameDev &F = frames[col_frame[c]];
+  int b0 = F.bin0 + (c - F.col0) * F.Nz;
+  int nc = bin_start[b0 + F.Nz] - bin_start[b0];
+  col_groups[c] = (nc + NB_GROUP - 1) / NB_GROUP;
+}
+
+__global__ void nb_batch_places(int nsorted_max, const int32_t *__restrict__ bin_start, int nvalid_bins,
+                                const int32_t *__restrict__ sorted, const int32_t *__restrict__ atom_col,
+                                const int32_t *__restrict__ col_frame, const NbFrameDev *__restrict__ frames,
+                                const int32_t *__restrict__ group_start, int64_t places_cap,
+                                const float4 *__restrict__ atom_xw, const char4 *__restrict__ atom_shift,
+                                int32_t *__restrict__ order, int32_t *__restrict__ place_of,
+                                char4 *__restrict__ shift, float4 *__restrict__ xw) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsorted_max) return;
+  int nvalid = bin_start[nvalid_bins];
+  int a = sorted[s];
+  if (s >= nvalid) {
+    place_of[a] = -1;
+    return;
+  }
+  int c = atom_col[a];
+  const NbFrameDev &F = frames[col_frame[c]];
+  int rank = s - bin_start[F.bin0 + (c - F.col0) * F.Nz];
+  int64_t p = (int64_t)group_start[c] * NB_GROUP + rank;
+  if (p >= places_cap) {
+    place_of[a] = -1;
+    return;
+  }
+  order[p] = a;
+  place_of[a] = (int32_t)p;
+  shift[p] = atom_shift[a];
+  xw[p] = atom_xw[a];
+}
+
+__global__ void nb_batch_group_frames(int64_t groups_cap, const int32_t *__restrict__ sizes,
+                                      const int32_t *__restrict__ group_col, const int32_t *__restrict__ col_frame,
+                                      const NbFrameDev *__restrict__ frames, int32_t *__restrict__ group_frame,
+                                      float4 *__restrict__ group_L) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
+  int f = col_frame[group_col[g]];
+  group_frame[g] = f;
+  group_L[g] = make_float4(frames[f].Lf0, frames[f].Lf1, frames[f].Lf2, 0.f);
+}
+
+// The units of frame f: [frame_units[2f], frame_units[2f + 1]).
+__global__ void nb_batch_frame_units(int nframes, const NbFrameDev *__restrict__ frames,
+                                     const int32_t *__restrict__ group_start, const int32_t *__restrict__ unit_start,
+                                     int32_t *__restrict__ frame_units) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nframes) return;
+  const NbFrameDev &F = frames[f];
+  int g0 = group_start[F.col0], g1 = group_start[F.col0 + F.ncol];
+  frame_units[2 * f] = unit_start[g0];
+  frame_units[2 * f + 1] = unit_start[g1];
+}
+
+}  // namespace
+
+// The grids of the frames (host): columns and bins end to end, the widened
+// reach of each cell; uploads the frames and the column -> frame map.
+static int nb_batch_plan(mdrtNbBatch &b, int64_t *list_cap_hint) {
+  NbCtx &c = b.nb->c;
+  int64_t bins = 0, cols = 0, cap = 0;
+  std::vector<int32_t> col_frame;
+  for (int f = 0; f < b.frames; ++f) {
+    NbFrameDev &F = b.h_frames[f];
+    const double *L = &b.h_boxes[3 * f];
+    int64_t nf = b.atom0[f + 1] - b.atom0[f];
+    NbGrid G = nb_plan_grid(std::max<int64_t>(nf, 1), L);
+    F.L0 = L[0];
+    F.L1 = L[1];
+    F.L2 = L[2];
+    F.Lf0 = (float)L[0];
+    F.Lf1 = (float)L[1];
+    F.Lf2 = (float)L[2];
+    F.Nx = G.Nx;
+    F.Ny = G.Ny;
+    F.Nz = G.Nz;
+    F.wx = G.wx;
+    F.wy = G.wy;
+    F.inv_wx = 1.0f / G.wx;
+    F.inv_wy = 1.0f / G.wy;
+    F.inv_hz = 1.0f / G.hz;
+    F.bin0 = (int)bins;
+    F.col0 = (int)cols;
+    F.ncol = G.ncol();
+    F.atom0 = (int)b.atom0[f];
+    F.natoms = (int)nf;
+    double Rw = c.reach + 3e-6 * (L[0] + L[1] + L[2]);
+    F.R2f = (float)(Rw * Rw);
+    F.Rbox = (float)(Rw + 2e-5 * (L[0] + L[1] + L[2]) + 1e-6);
+    F.pref = c.coulomb / (M_PI * L[0] * L[1] * L[2]);
+    F.pi2_beta2 = c.beta > 0 ? M_PI * M_PI / (c.beta * c.beta) : 0.0;
+    bins += G.nbins();
+    cols += G.ncol();
+    col_frame.insert(col_frame.end(), G.ncol(), f);
+    cap = std::max(cap, nb_initial_list_cap(std::max<int64_t>(nf, 1), L, c.reach, G));
+  }
+  if (bins >= (1ll << 31) - 2 || cols >= (1ll << 31) - 2) return -1;
+  c.plan_cols = cols;
+  c.plan_bins = bins;
+  if (list_cap_hint) *list_cap_hint = cap;
+  if (!b.frames_dev && nb_realloc(b.frames_dev, b.frames)) return -1;
+  NB_CHECK(cudaMemcpy(b.frames_dev, b.h_frames.data(), sizeof(NbFrameDev) * b.frames, cudaMemcpyHostToDevice));
+  if (cols > b.cols_alloc) {
+    if (nb_realloc(b.col_frame, cols)) return -1;
+    b.cols_alloc = cols;
+  }
+  NB_CHECK(cudaMemcpy(b.col_frame, col_frame.data(), sizeof(int32_t) * cols, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+static void nb_batch_build_launch(mdrtNbBatch &b, const double *x, cudaStream_t s) {
+  NbCtx &c = b.nb->c;
+  int64_t n = c.n;
+  int nbins = (int)c.plan_bins;
+  int ncol = (int)c.plan_cols;
+  cudaMemsetAsync(c.sizes, 0, sizeof(int32_t) * NB_SIZE_COUNT, s);
+  cudaMemsetAsync(c.bin_count, 0, sizeof(int32_t) * (nbins + 1), s);
+  cudaMemsetAsync(c.bin_fill, 0, sizeof(int32_t) * (nbins + 1), s);
+  cudaMemsetAsync(c.order, 0xff, sizeof(int32_t) * c.places_cap, s);
+  nb_batch_keys<<<blocks_for(n, 256), 256, 0, s>>>(n, x, b.atom_frame, b.frames_dev, nbins, c.key, b.atom_col,
+                                                  c.bin_count, c.atom_xw, c.atom_shift, c.sizes);
+  nb_scan(c.bin_count, c.bin_start, nbins + 1, nullptr, c.scan_scratch, s);
+  nb_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, c.key, c.bin_start, c.bin_fill, c.sorted);
+  nb_bin_sort<<<blocks_for(nbins + 1, 256), 256, 0, s>>>(nbins + 1, c.bin_start, c.sorted);
+  nb_batch_col_groups<<<blocks_for(ncol, 256), 256, 0, s>>>(ncol, b.col_frame, b.frames_dev, c.bin_start,
+                                                           c.col_groups);
+  nb_scan(c.col_groups, c.group_start, ncol, nullptr, c.scan_scratch, s);
+  nb_group_cols<<<blocks_for(ncol, 256), 256, 0, s>>>(ncol, c.group_start, c.groups_cap, c.group_col, c.sizes);
+  nb_batch_places<<<blocks_for(n, 256), 256, 0, s>>>((int)n, c.bin_start, nbins, c.sorted, b.atom_col,
+                                                    b.col_frame, b.frames_dev, c.group_start, c.places_cap,
+                                                    c.atom_xw, c.atom_shift, c.order, c.place_of, c.shift, c.xw);
+  nb_boxes<<<blocks_for(c.groups_cap, 128), 128, 0, s>>>(c.groups_cap, c.sizes, c.order, c.xw, c.box_lo,
+                                                        c.box_hi);
+  nb_batch_group_frames<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.group_col,
+                                                                     b.col_frame, b.frames_dev, b.group_frame,
+                                                                     b.group_L);
+  SearchParams P = {};
+  P.groups_cap = c.groups_cap;
+  P.list_cap = c.list_cap;
+  size_t stage = sizeof(int2) * 4 * (size_t)c.list_cap;
+  if (b.search_warps == 4 && stage <= 200 * 1024) {
+    static size_t configured = 0;
+    if (stage > 48 * 1024 && configured < stage) {
+      cudaFuncSetAttribute(nb_search_t<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+      configured = stage;
+    }
+    nb_search_t<4, true><<<(int)c.groups_cap, 128, stage, s>>>(P, b.frames_dev, b.group_frame, c.sizes, c.order,
+                                                               c.xw, c.box_lo, c.box_hi, c.group_start, c.excl_off,
+                                                               c.excl, c.slab, c.counts, c.sizes);
+  } else {
+    nb_search_t<1, true><<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, b.frames_dev, b.group_frame, c.sizes,
+                                                                     c.order, c.xw, c.box_lo, c.box_hi,
+                                                                     c.group_start, c.excl_off, c.excl, c.slab,
+                                                                     c.counts, c.sizes);
+  }
+  nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts, c.list_cap,
+                                                             c.unit_n);
+  nb_scan(c.unit_n, c.unit_start, (int)c.groups_cap, nullptr, c.scan_scratch, s);
+  nb_unit_write<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.unit_n, c.unit_start, c.units_cap,
+                                                             c.units, c.sizes);
+  nb_count_entries<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts, c.sizes);
+  nb_batch_frame_units<<<blocks_for(b.frames, 128), 128, 0, s>>>(b.frames, b.frames_dev, c.group_start,
+                                                                c.unit_start, b.frame_units);
+}
+
+int nb_batch_build_run(mdrtNbBatch &b, const double *x, cudaStream_t s) {
+  NbCtx &c = b.nb->c;
+  int64_t hint = 0;
+  if (nb_batch_plan(b, &hint)) return -1;
+  int64_t cap = std::max<int64_t>(c.list_cap, hint);
+  if (!c.key) {
+    if (nb_realloc(c.key, c.n) || nb_realloc(c.sorted, c.n) || nb_realloc(c.atom_xw, c.n) ||
+        nb_realloc(c.atom_shift, c.n) || nb_realloc(c.place_of, c.n) || nb_realloc(b.atom_col, c.n))
+      return -1;
+  }
+  if (!b.frame_units && nb_realloc(b.frame_units, 2 * (int64_t)b.frames)) return -1;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    if (nb_reserve(c, cap)) return -1;
+    if (c.groups_cap > b.groups_alloc) {
+      if (nb_realloc(b.group_frame, c.groups_cap) || nb_realloc(b.group_L, c.groups_cap)) return -1;
+      b.groups_alloc = c.groups_cap;
+    }
+    nb_batch_build_launch(b, x, s);
+    NB_CHECK(cudaMemcpyAsync(c.h_sizes, c.sizes, sizeof(int32_t) * NB_SIZE_COUNT, cudaMemcpyDeviceToHost, s));
+    NB_CHECK(cudaStreamSynchronize(s));
+    NB_CHECK(cudaGetLastError());
+    if (c.h_sizes[NB_SIZE_OVERFLOW] == 0) {
+      c.built = true;
+      c.builds++;
+      c.inner_valid = false;
+      return 0;
+    }
+    int64_t longest = c.h_sizes[NB_SIZE_LONGEST];
+    int64_t want = (longest + longest / 4 + NB_UNIT - 1) / NB_UNIT * NB_UNIT;
+    cap = std::max(cap, want);
+    c.grows++;
+  }
+  return -1;
 }

@@ -113,6 +113,9 @@ struct NbCtx {
   double *adj_types = nullptr;    // per block of the adjoint kernel: 2 ntypes^2 partials
   int64_t adj_places = 0;         // places_cap the per-place arrays were sized for
   int adj_blocks = 0;
+  // the columns and bins the buffers are planned for (one grid, or the
+  // frames of a batch laid end to end)
+  int64_t plan_cols = 0, plan_bins = 0;
   // the f64 positions of the last build (atom order) and the per-frame
   // displacement maxima of mdrtNbDisplacement
   double *x_build = nullptr;
@@ -134,6 +137,76 @@ enum NbEnergySlot {
 // The opaque handle of the C ABI.
 struct mdrtNb {
   NbCtx c;
+};
+
+// One frame of a batch, as the kernels read it: the cell, its grid of
+// columns and bins and where they sit among the batch's, the widened
+// reach, and its PME grid.
+struct NbFrameDev {
+  double L0, L1, L2;
+  float Lf0, Lf1, Lf2;
+  float inv_wx, inv_wy, inv_hz;
+  float wx, wy;
+  int Nx, Ny, Nz;
+  int bin0, col0, ncol;
+  float R2f, Rbox;
+  int K0, K1, K2, mod0;
+  long long grid0, spec0;
+  double pref, pi2_beta2;  // the influence function: f/(pi V), pi^2/beta^2
+  int atom0, natoms;
+};
+
+// Many independent systems (frames) evaluated together: the atoms of all
+// frames are numbered one after the other, and one NbCtx holds the places,
+// groups, lists, units and accumulators of all of them.  The grids of the
+// frames lie end to end (bins and columns), so that every stage of the
+// build, the pair kernel and PME is one launch over all frames; a group,
+// a column and an atom know their frame.
+struct mdrtNbBatch {
+  mdrtNb *nb = nullptr;  // the shared context, n = all atoms
+  int32_t frames = 0;
+  std::vector<int64_t> atom0;  // frames + 1
+  std::vector<NbFrameDev> h_frames;
+  NbFrameDev *frames_dev = nullptr;
+  int32_t *atom_frame = nullptr;  // per atom
+  int32_t *atom_col = nullptr;    // per atom: its column at the build
+  int32_t *col_frame = nullptr;   // per column
+  int32_t *group_frame = nullptr; // per group
+  float4 *group_L = nullptr;      // per group: the frame's cell
+  int64_t groups_alloc = 0, cols_alloc = 0;
+  int32_t *frame_units = nullptr; // per frame: first unit, one past the last
+  std::vector<double> h_boxes;    // frames x 3 of the last build
+  // excluded pairs: blocks of 256 pairs that never straddle two frames
+  int32_t *excl_blk_frame = nullptr, *excl_blk_first = nullptr, *excl_frame_end = nullptr;
+  std::vector<int32_t> h_excl_blk0;  // frames + 1
+  int excl_blocks = 0;
+  double *excl_part = nullptr;
+  // PME: frames sorted by grid shape; one batched cuFFT plan pair a shape
+  int order = 4;
+  bool pme = false;
+  struct Shape {
+    int K[3];
+    int count;
+    long long grid0, spec0;
+    cufftHandle fwd, bwd;
+  };
+  std::vector<Shape> shapes;
+  long long grid_points = 0;  // real grid points of all frames
+  int32_t *conv_blk_frame = nullptr;
+  std::vector<int32_t> h_conv_blk0;  // frames + 1
+  int conv_blocks = 0;
+  double *conv_part = nullptr;
+  int32_t *d_excl_blk0 = nullptr, *d_conv_blk0 = nullptr;
+  // energies: frames x NB_E_SLOTS (device) and a pinned mirror
+  double *frame_energy = nullptr, *h_frame_energy = nullptr;
+  int search_warps = 4;  // tuning: warps a group of the search (1 or 4)
+  // the force evaluation as a CUDA graph
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  const double *gx = nullptr;
+  double *gf = nullptr;
+  uint32_t gflags = 0;
+  int64_t gkey = -1;
 };
 
 // Launchers implemented in the .cu files.
@@ -170,3 +243,15 @@ int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double 
                    double *dq, double *dtable, cudaStream_t s);
 // The reciprocal part of the charge gradient, added per place into c.adj_q.
 int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s);
+
+// The batch (mdrtNbBatch): the build of all frames (grows and builds again
+// until every list fits; host wait), the frames of the places, the pair
+// kernel, the excluded pairs, PME, and the per-frame energy sums.
+int nb_batch_build_run(mdrtNbBatch &b, const double *x, cudaStream_t s);
+void nb_batch_gather_frames(mdrtNbBatch &b, const double *x, cudaStream_t s);
+void nb_batch_pairs_run(mdrtNbBatch &b, bool energy, cudaStream_t s);
+void nb_batch_excluded_run(mdrtNbBatch &b, bool energy, cudaStream_t s);
+int nb_batch_pme_setup(mdrtNbBatch &b, const int32_t *grids, int order);
+void nb_batch_pme_release(mdrtNbBatch &b);
+int nb_batch_pme_run(mdrtNbBatch &b, bool energy, cudaStream_t s);
+void nb_batch_energy_sums(mdrtNbBatch &b, bool pairs, bool excluded, bool pme, cudaStream_t s);

@@ -75,8 +75,9 @@ __device__ __forceinline__ void nb_red_fixed(unsigned long long *addr, float x, 
 // shared memory (slots u and u + 16), so that lane l reads member
 // (l + k) mod 16 at slot l mod 16 + k: an immediate offset in the unrolled
 // loop, no index arithmetic.
-template <bool ENERGY, bool FIXED, bool SWITCH, int LJM>
-__global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const int32_t *__restrict__ sizes,
+template <bool ENERGY, bool FIXED, bool SWITCH, int LJM, bool BATCH = false>
+__global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *__restrict__ group_L,
+                                                const int32_t *__restrict__ sizes,
                                                 const int2 *__restrict__ units,
                                                 const int2 *__restrict__ slab,
                                                 const int32_t *__restrict__ counts,
@@ -122,6 +123,13 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const int32_t *
     int cnt = (int)min((int64_t)counts[g], P.list_cap);
     int e0 = uo.y * NB_UNIT;
     int ne = min(NB_UNIT, cnt - e0);
+    float Lx = P.Lx, Ly = P.Ly, Lz = P.Lz;
+    if (BATCH) {  // the cell of the group's frame
+      float4 Lg = group_L[g];
+      Lx = Lg.x;
+      Ly = Lg.y;
+      Lz = Lg.z;
+    }
     float ax = 0.f, ay = 0.f, az = 0.f;  // the accumulator of member (lane + k) mod 16
     float elj = 0.f, ecl = 0.f;
     float vxx = 0.f, vyy = 0.f, vzz = 0.f, vxy = 0.f, vxz = 0.f, vyz = 0.f;
@@ -135,9 +143,9 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const int32_t *
       int sx, sy, sz;
       nb_decode_image(code, sx, sy, sz);
       float4 xj = xq[q];
-      xj.x += (float)sx * P.Lx;
-      xj.y += (float)sy * P.Ly;
-      xj.z += (float)sz * P.Lz;
+      xj.x += (float)sx * Lx;
+      xj.y += (float)sy * Ly;
+      xj.z += (float)sz * Lz;
       int tj = typ[q];
       float2 fj = LJM == 1 ? ljf[tj] : make_float2(0.f, 0.f);
       // bit k of mrot: the pair of this lane's entry with member (lane + k) mod 16
@@ -251,52 +259,49 @@ __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
   typ_p[p] = type[a];
 }
 
-// The excluded-pair correction -f q_i q_j erf(beta r)/r in the minimum
-// image, in f64 from the f32 frames (a thread per pair i < j).
+// One excluded pair (i < j): the correction -f q_i q_j erf(beta r)/r in the
+// minimum image, in f64 from the f32 frames; adds the forces and returns the
+// energy and virial in v[0..6].
 template <bool FIXED>
-__global__ void nb_excluded(int64_t npairs, const int32_t *__restrict__ pairs,
-                            const int32_t *__restrict__ place_of, const float4 *__restrict__ xq,
-                            double Lx, double Ly, double Lz, double beta, double coulomb, bool energy,
-                            float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
-                            double *__restrict__ partials, int *__restrict__ status) {
-  __shared__ double s_part[8][8];
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (k < npairs) {
-    int i = pairs[2 * k], j = pairs[2 * k + 1];
-    int pi = place_of[i], pj = place_of[j];
-    if (pi >= 0 && pj >= 0) {
-      float4 a = xq[pi], b = xq[pj];
-      double d0 = (double)a.x - b.x, d1 = (double)a.y - b.y, d2 = (double)a.z - b.z;
-      d0 -= Lx * rint(d0 / Lx);
-      d1 -= Ly * rint(d1 / Ly);
-      d2 -= Lz * rint(d2 / Lz);
-      double r2 = d0 * d0 + d1 * d1 + d2 * d2;
-      double qq = coulomb * (double)a.w * (double)b.w;
-      if (qq != 0.0 && r2 > 0.0) {
-        double r = sqrt(r2);
-        double ef = erf(beta * r);
-        double g = 2.0 * beta / sqrt(M_PI) * exp(-beta * beta * r2);
-        double fs = qq * (g / r2 - ef / (r2 * r));
-        float fx = (float)(fs * d0), fy = (float)(fs * d1), fz = (float)(fs * d2);
-        if (FIXED) {
-          nb_red_fixed(accf + 3 * (int64_t)pi, fx, fy, fz, status);
-          nb_red_fixed(accf + 3 * (int64_t)pj, -fx, -fy, -fz, status);
-        } else {
-          nb_red_add_v4(acc + pi, fx, fy, fz);
-          nb_red_add_v4(acc + pj, -fx, -fy, -fz);
-        }
-        v[0] = -qq * ef / r;
-        v[1] = d0 * fs * d0;
-        v[2] = d1 * fs * d1;
-        v[3] = d2 * fs * d2;
-        v[4] = d0 * fs * d1;
-        v[5] = d0 * fs * d2;
-        v[6] = d1 * fs * d2;
-      }
-    }
+__device__ __forceinline__ void nb_excluded_pair(int i, int j, const int32_t *__restrict__ place_of,
+                                                 const float4 *__restrict__ xq, double Lx, double Ly, double Lz,
+                                                 double beta, double coulomb, float4 *__restrict__ acc,
+                                                 unsigned long long *__restrict__ accf, int *__restrict__ status,
+                                                 double *v) {
+  int pi = place_of[i], pj = place_of[j];
+  if (pi < 0 || pj < 0) return;
+  float4 a = xq[pi], b = xq[pj];
+  double d0 = (double)a.x - b.x, d1 = (double)a.y - b.y, d2 = (double)a.z - b.z;
+  d0 -= Lx * rint(d0 / Lx);
+  d1 -= Ly * rint(d1 / Ly);
+  d2 -= Lz * rint(d2 / Lz);
+  double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+  double qq = coulomb * (double)a.w * (double)b.w;
+  if (qq == 0.0 || r2 <= 0.0) return;
+  double r = sqrt(r2);
+  double ef = erf(beta * r);
+  double g = 2.0 * beta / sqrt(M_PI) * exp(-beta * beta * r2);
+  double fs = qq * (g / r2 - ef / (r2 * r));
+  float fx = (float)(fs * d0), fy = (float)(fs * d1), fz = (float)(fs * d2);
+  if (FIXED) {
+    nb_red_fixed(accf + 3 * (int64_t)pi, fx, fy, fz, status);
+    nb_red_fixed(accf + 3 * (int64_t)pj, -fx, -fy, -fz, status);
+  } else {
+    nb_red_add_v4(acc + pi, fx, fy, fz);
+    nb_red_add_v4(acc + pj, -fx, -fy, -fz);
   }
-  if (!energy) return;
+  v[0] = -qq * ef / r;
+  v[1] = d0 * fs * d0;
+  v[2] = d1 * fs * d1;
+  v[3] = d2 * fs * d2;
+  v[4] = d0 * fs * d1;
+  v[5] = d0 * fs * d2;
+  v[6] = d1 * fs * d2;
+}
+
+// The block's sums of v[0..6] to partials[blockIdx.x * 8 + c].
+__device__ __forceinline__ void nb_block_partials8(double *v, double *__restrict__ partials) {
+  __shared__ double s_part[8][8];
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
@@ -310,6 +315,120 @@ __global__ void nb_excluded(int64_t npairs, const int32_t *__restrict__ pairs,
     double s = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += s_part[w][threadIdx.x];
     partials[(int64_t)blockIdx.x * 8 + threadIdx.x] = s;
+  }
+}
+
+// The excluded-pair correction, a thread per pair i < j.
+template <bool FIXED>
+__global__ void nb_excluded(int64_t npairs, const int32_t *__restrict__ pairs,
+                            const int32_t *__restrict__ place_of, const float4 *__restrict__ xq,
+                            double Lx, double Ly, double Lz, double beta, double coulomb, bool energy,
+                            float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
+                            double *__restrict__ partials, int *__restrict__ status) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (k < npairs)
+    nb_excluded_pair<FIXED>(pairs[2 * k], pairs[2 * k + 1], place_of, xq, Lx, Ly, Lz, beta, coulomb, acc, accf,
+                            status, v);
+  if (!energy) return;
+  nb_block_partials8(v, partials);
+}
+
+// The same over the frames of a batch: block b takes pairs
+// [blk_first[b], frame_end[f]) of one frame f = blk_frame[b] (at most 256),
+// so that its partial sums belong to one frame.
+__global__ void nb_batch_excluded(const int32_t *__restrict__ blk_frame, const int32_t *__restrict__ blk_first,
+                                  const int32_t *__restrict__ frame_end, const int32_t *__restrict__ pairs,
+                                  const int32_t *__restrict__ place_of, const float4 *__restrict__ xq,
+                                  const NbFrameDev *__restrict__ frames, double beta, double coulomb, bool energy,
+                                  float4 *__restrict__ acc, double *__restrict__ partials) {
+  int f = blk_frame[blockIdx.x];
+  int64_t k = (int64_t)blk_first[blockIdx.x] + threadIdx.x;
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (k < frame_end[f]) {
+    const NbFrameDev &F = frames[f];
+    nb_excluded_pair<false>(pairs[2 * k], pairs[2 * k + 1], place_of, xq, F.L0, F.L1, F.L2, beta, coulomb, acc,
+                            nullptr, nullptr, v);
+  }
+  if (!energy) return;
+  nb_block_partials8(v, partials);
+}
+
+// Frames of a batch: each place's atom in its frame's cell.
+__global__ void nb_batch_gather(int64_t places, const int32_t *__restrict__ sizes,
+                                const int32_t *__restrict__ order, const char4 *__restrict__ shift,
+                                const double *__restrict__ x, const float *__restrict__ q,
+                                const int32_t *__restrict__ type, const int32_t *__restrict__ atom_frame,
+                                const NbFrameDev *__restrict__ frames, float4 *__restrict__ xq,
+                                int32_t *__restrict__ typ_p) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  int a = order[p];
+  if (a < 0) {
+    xq[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    typ_p[p] = 0;
+    return;
+  }
+  const NbFrameDev &F = frames[atom_frame[a]];
+  char4 s = shift[p];
+  xq[p] = make_float4((float)(x[3 * a] + s.x * F.L0), (float)(x[3 * a + 1] + s.y * F.L1),
+                      (float)(x[3 * a + 2] + s.z * F.L2), q[a]);
+  typ_p[p] = type[a];
+}
+
+// The energies and virials of each frame (a block a frame), summed in a
+// fixed order: the units of its pairs, the blocks of its excluded pairs and
+// of its convolution.
+__global__ void nb_batch_sums(int nframes, const int32_t *__restrict__ frame_units,
+                              const double *__restrict__ unit_partials, int pairs,
+                              const int32_t *__restrict__ excl_blk0, const double *__restrict__ excl_part,
+                              int excluded, const int32_t *__restrict__ conv_blk0,
+                              const double *__restrict__ conv_part, int pme, double *__restrict__ frame_energy) {
+  __shared__ double s[128][8];
+  int f = blockIdx.x;
+  if (f >= nframes) return;
+  double *out = frame_energy + (int64_t)f * NB_E_SLOTS;
+  for (int part = 0; part < 3; ++part) {
+    int width = part == 2 ? 7 : 8;
+    const double *src = part == 0 ? unit_partials : part == 1 ? excl_part : conv_part;
+    bool on = part == 0 ? pairs : part == 1 ? excluded : pme;
+    int lo = 0, hi = 0;
+    if (on) {
+      if (part == 0) {
+        lo = frame_units[2 * f];
+        hi = frame_units[2 * f + 1];
+      } else if (part == 1) {
+        lo = excl_blk0[f];
+        hi = excl_blk0[f + 1];
+      } else {
+        lo = conv_blk0[f];
+        hi = conv_blk0[f + 1];
+      }
+    }
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int r = lo + (int)threadIdx.x; r < hi; r += blockDim.x)
+      for (int k = 0; k < width; ++k) v[k] += src[(int64_t)r * width + k];
+    for (int k = 0; k < 8; ++k) s[threadIdx.x][k] = v[k];
+    __syncthreads();
+    for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+      if ((int)threadIdx.x < stride)
+        for (int k = 0; k < 8; ++k) s[threadIdx.x][k] += s[threadIdx.x + stride][k];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      if (part == 0) {
+        out[NB_E_LJ] = s[0][0];
+        out[NB_E_COUL] = s[0][1];
+        for (int k = 0; k < 6; ++k) out[NB_W_PAIR + k] = s[0][2 + k];
+      } else if (part == 1) {
+        out[NB_E_EXCL] = s[0][0];
+        for (int k = 0; k < 6; ++k) out[NB_W_PAIR + k] += s[0][1 + k];
+      } else {
+        out[NB_E_REC] = s[0][0];
+        for (int k = 0; k < 6; ++k) out[NB_W_REC + k] = s[0][1 + k];
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -671,9 +790,9 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
   const int2 *lunits = inner ? c.units_in : c.units;
   const int2 *lslab = inner ? c.slab_in : c.slab;
   const int32_t *lcounts = inner ? c.counts_in : c.counts;
-#define NB_LAUNCH2(E, F, S, M)                                                                      \
-  nb_pairs<E, F, S, M><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, c.ljf, \
-                                           c.acc, c.acc_fixed, c.unit_partials, c.status)
+#define NB_LAUNCH2(E, F, S, M)                                                                         \
+  nb_pairs<E, F, S, M><<<grid, 256, 0, s>>>(P, nullptr, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, \
+                                           c.ljf, c.acc, c.acc_fixed, c.unit_partials, c.status)
 #define NB_LAUNCH(E, F, S)      \
   do {                          \
     if (c.lj_geom)              \
@@ -799,4 +918,49 @@ int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double 
     nb_charge_terms<<<blocks_for(c.n, 256), 256, 0, s>>>(c.n, c.q, self2, background, dq);
   }
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// The batch (mdrtNbBatch): one launch of each kernel over all frames.
+
+void nb_batch_gather_frames(mdrtNbBatch &b, const double *x, cudaStream_t s) {
+  NbCtx &c = b.nb->c;
+  nb_batch_gather<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.shift, x, c.q,
+                                                                c.type, b.atom_frame, b.frames_dev, c.xq, c.typ_p);
+}
+
+void nb_batch_pairs_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
+  NbCtx &c = b.nb->c;
+  ensure_sm_count();
+  double unit_box[3] = {1.0, 1.0, 1.0};  // the cells come from group_L
+  PairParams P = pair_params(c, unit_box);
+  int64_t want = (c.units_cap + 7) / 8;
+  int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)g_sm_count * std::max(1, c.pair_blocks_per_sm)));
+#define NB_BATCH_LAUNCH(E, M)                                                                                \
+  nb_pairs<E, false, false, M, true><<<grid, 256, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq, \
+                                                         c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed, c.unit_partials, \
+                                                         c.status)
+  if (energy) {
+    if (c.lj_geom) NB_BATCH_LAUNCH(true, 1); else NB_BATCH_LAUNCH(true, 0);
+  } else {
+    if (c.lj_geom) NB_BATCH_LAUNCH(false, 1); else NB_BATCH_LAUNCH(false, 0);
+  }
+#undef NB_BATCH_LAUNCH
+}
+
+void nb_batch_excluded_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
+  NbCtx &c = b.nb->c;
+  if (b.excl_blocks == 0 || c.beta == 0.0) return;
+  nb_batch_excluded<<<b.excl_blocks, 256, 0, s>>>(b.excl_blk_frame, b.excl_blk_first, b.excl_frame_end,
+                                                  c.excl_pairs, c.place_of, c.xq, b.frames_dev, c.beta, c.coulomb,
+                                                  energy, c.acc, b.excl_part);
+}
+
+void nb_batch_energy_sums(mdrtNbBatch &b, bool pairs, bool excluded, bool pme, cudaStream_t s) {
+  NbCtx &c = b.nb->c;
+  bool ex = excluded && b.excl_blocks > 0 && c.beta != 0.0;
+  cudaMemsetAsync(b.frame_energy, 0, sizeof(double) * NB_E_SLOTS * b.frames, s);
+  nb_batch_sums<<<b.frames, 128, 0, s>>>(b.frames, b.frame_units, c.unit_partials, pairs ? 1 : 0, b.d_excl_blk0,
+                                         b.excl_part, ex ? 1 : 0, b.d_conv_blk0, b.conv_part, pme ? 1 : 0,
+                                         b.frame_energy);
 }

@@ -650,3 +650,343 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s) 
   }
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// PME over the frames of a batch (mdrtNbBatch).  The grids of the frames lie
+// end to end, frames of one shape next to each other, so that one batched
+// cuFFT plan pair per shape transforms them all; spreading, the influence
+// function and gathering are one launch each, every atom or spectrum point
+// reading its frame's grid, cell and moduli.
+
+#include <algorithm>
+#include <map>
+
+namespace {
+
+__device__ __forceinline__ GridParams nb_frame_grid(const NbFrameDev &F) {
+  GridParams G;
+  G.K0 = F.K0;
+  G.K1 = F.K1;
+  G.K2 = F.K2;
+  G.invL0 = (float)(1.0 / F.L0);
+  G.invL1 = (float)(1.0 / F.L1);
+  G.invL2 = (float)(1.0 / F.L2);
+  return G;
+}
+
+template <int P>
+__global__ void __launch_bounds__(256) nb_batch_spread(int64_t places, const int32_t *__restrict__ sizes,
+                                                       const int32_t *__restrict__ order,
+                                                       const int32_t *__restrict__ atom_frame,
+                                                       const NbFrameDev *__restrict__ frames,
+                                                       const float4 *__restrict__ xq, float *__restrict__ grid) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t p = t / P;
+  int c = (int)(t - p * P);
+  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
+  int a = order[p];
+  if (a < 0) return;
+  float4 v = xq[p];
+  if (v.w == 0.f) return;
+  const NbFrameDev &F = frames[atom_frame[a]];
+  GridParams G = nb_frame_grid(F);
+  float *fg = grid + F.grid0;
+  int k0, k1, k2;
+  float t0, t1, t2;
+  nb_frac(v.x, G.invL0, G.K0, k0, t0);
+  nb_frac(v.y, G.invL1, G.K1, k1, t1);
+  nb_frac(v.z, G.invL2, G.K2, k2, t2);
+  float w0[P], w1[P], w2[P];
+  nb_bspline<P>(t0, w0, nullptr);
+  nb_bspline<P>(t1, w1, nullptr);
+  nb_bspline<P>(t2, w2, nullptr);
+  int gz = k2 - c;
+  if (gz < 0) gz += G.K2;
+  float qz = v.w * w2[c];
+#pragma unroll
+  for (int jx = 0; jx < P; ++jx) {
+    int gx = k0 - jx;
+    if (gx < 0) gx += G.K0;
+    float qxz = qz * w0[jx];
+#pragma unroll
+    for (int jy = 0; jy < P; ++jy) {
+      int gy = k1 - jy;
+      if (gy < 0) gy += G.K1;
+      atomicAdd(fg + ((int64_t)gx * G.K1 + gy) * G.K2 + gz, qxz * w1[jy]);
+    }
+  }
+}
+
+// Block b of the spectrum of frame f = blk_frame[b] (256 points of it).
+template <bool ENERGY>
+__global__ void __launch_bounds__(256) nb_batch_convolve(const int32_t *__restrict__ blk_frame,
+                                                         const int32_t *__restrict__ blk0,
+                                                         const NbFrameDev *__restrict__ frames,
+                                                         const float *__restrict__ moduli, float2 *__restrict__ spec,
+                                                         double *__restrict__ partials) {
+  __shared__ double s_part[8][7];
+  int f = blk_frame[blockIdx.x];
+  const NbFrameDev &F = frames[f];
+  int H2 = F.K2 / 2 + 1;
+  int64_t total = (int64_t)F.K0 * F.K1 * H2;
+  int64_t k = (int64_t)(blockIdx.x - blk0[f]) * blockDim.x + threadIdx.x;
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (k < total) {
+    int i2 = (int)(k % H2);
+    int64_t r = k / H2;
+    int i1 = (int)(r % F.K1);
+    int i0 = (int)(r / F.K1);
+    double m0 = (i0 <= F.K0 / 2 ? i0 : i0 - F.K0) / F.L0;
+    double m1 = (i1 <= F.K1 / 2 ? i1 : i1 - F.K1) / F.L1;
+    double m2v = (i2 <= F.K2 / 2 ? i2 : i2 - F.K2) / F.L2;
+    double mm = m0 * m0 + m1 * m1 + m2v * m2v;
+    float2 *sp = spec + F.spec0;
+    const float *md = moduli + F.mod0;
+    float2 s = sp[k];
+    double bc = 0.0;
+    if (k != 0) {
+      double B = (double)md[i0] * (double)md[F.K0 + i1] * (double)md[F.K0 + F.K1 + i2];
+      bc = B * F.pref * exp(-F.pi2_beta2 * mm) / mm;
+    }
+    sp[k] = make_float2((float)(s.x * bc), (float)(s.y * bc));
+    if (ENERGY && k != 0) {
+      double wgt = (i2 == 0 || (F.K2 % 2 == 0 && i2 == F.K2 / 2)) ? 1.0 : 2.0;
+      double em = 0.5 * wgt * bc * ((double)s.x * s.x + (double)s.y * s.y);
+      double fm = -2.0 * (1.0 / mm + F.pi2_beta2);
+      v[0] = em;
+      v[1] = em * (1.0 + fm * m0 * m0);
+      v[2] = em * (1.0 + fm * m1 * m1);
+      v[3] = em * (1.0 + fm * m2v * m2v);
+      v[4] = em * fm * m0 * m1;
+      v[5] = em * fm * m0 * m2v;
+      v[6] = em * fm * m1 * m2v;
+    }
+  }
+  if (!ENERGY) return;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+  }
+  if (lane == 0)
+    for (int c = 0; c < 7; ++c) s_part[warp][c] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += s_part[w][threadIdx.x];
+    partials[(int64_t)blockIdx.x * 7 + threadIdx.x] = s;
+  }
+}
+
+// P lanes an atom, one z point each (P a power of two dividing 32).
+template <int P>
+__global__ void __launch_bounds__(128) nb_batch_gather_split(int64_t places, const int32_t *__restrict__ sizes,
+                                                             const int32_t *__restrict__ order,
+                                                             const int32_t *__restrict__ atom_frame,
+                                                             const NbFrameDev *__restrict__ frames,
+                                                             const float4 *__restrict__ xq,
+                                                             const float *__restrict__ grid,
+                                                             float4 *__restrict__ out) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t p = t / P;
+  int c = (int)(t & (P - 1));
+  bool live = p < places && p < sizes[NB_SIZE_PLACES];
+  int a = live ? order[p] : -1;
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  GridParams G = {1, 1, 1, 1.f, 1.f, 1.f};
+  if (a >= 0) {
+    const NbFrameDev &F = frames[atom_frame[a]];
+    G = nb_frame_grid(F);
+    const float *phi = grid + F.grid0;
+    v = xq[p];
+    int k0, k1, k2;
+    float t0, t1, t2;
+    nb_frac(v.x, G.invL0, G.K0, k0, t0);
+    nb_frac(v.y, G.invL1, G.K1, k1, t1);
+    nb_frac(v.z, G.invL2, G.K2, k2, t2);
+    float w0[P], w1[P], w2[P], d0[P], d1[P], d2[P];
+    nb_bspline<P>(t0, w0, d0);
+    nb_bspline<P>(t1, w1, d1);
+    nb_bspline<P>(t2, w2, d2);
+    int gz = k2 - c;
+    if (gz < 0) gz += G.K2;
+    float wz = w2[c], dz = d2[c];
+#pragma unroll
+    for (int jx = 0; jx < P; ++jx) {
+      int gx = k0 - jx;
+      if (gx < 0) gx += G.K0;
+#pragma unroll
+      for (int jy = 0; jy < P; ++jy) {
+        int gy = k1 - jy;
+        if (gy < 0) gy += G.K1;
+        float f = __ldg(phi + ((int64_t)gx * G.K1 + gy) * G.K2 + gz);
+        g0 = fmaf(d0[jx] * w1[jy], f, g0);
+        g1 = fmaf(w0[jx] * d1[jy], f, g1);
+        g2 = fmaf(w0[jx] * w1[jy], f, g2);
+      }
+    }
+    g0 *= wz;
+    g1 *= wz;
+    g2 *= dz;
+  }
+#pragma unroll
+  for (int o = P / 2; o > 0; o >>= 1) {
+    g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+    g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+    g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+  }
+  if (!live || c != 0) return;
+  if (a < 0) {
+    out[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
+  float q = v.w;
+  out[p] = make_float4(-q * g0 * (float)G.K0 * G.invL0, -q * g1 * (float)G.K1 * G.invL1,
+                       -q * g2 * (float)G.K2 * G.invL2, 0.f);
+}
+
+}  // namespace
+
+void nb_batch_pme_release(mdrtNbBatch &b) {
+  for (auto &sh : b.shapes) {
+    if (sh.fwd) cufftDestroy(sh.fwd);
+    if (sh.bwd) cufftDestroy(sh.bwd);
+  }
+  b.shapes.clear();
+  for (void *p : {(void *)b.conv_blk_frame, (void *)b.d_conv_blk0, (void *)b.conv_part})
+    if (p) cudaFree(p);
+  b.conv_blk_frame = nullptr;
+  b.d_conv_blk0 = nullptr;
+  b.conv_part = nullptr;
+  b.conv_blocks = 0;
+  b.pme = false;
+  nb_pme_release(b.nb->c);
+}
+
+int nb_batch_pme_setup(mdrtNbBatch &b, const int32_t *grids, int order) {
+  nb_batch_pme_release(b);
+  if (order != 4 && order != 8) return -2;  // the split gather: a power of two dividing 32
+  NbCtx &c = b.nb->c;
+  NbPme &P = c.pme;
+  // frames grouped by shape, in order of first appearance
+  std::map<std::tuple<int, int, int>, std::vector<int>> by_shape;
+  std::vector<std::tuple<int, int, int>> shape_order;
+  for (int f = 0; f < b.frames; ++f) {
+    auto key = std::make_tuple(grids[3 * f], grids[3 * f + 1], grids[3 * f + 2]);
+    if (!by_shape.count(key)) shape_order.push_back(key);
+    by_shape[key].push_back(f);
+  }
+  long long grid0 = 0, spec0 = 0;
+  std::vector<float> mod;
+  std::vector<int32_t> blk_frame, blk0(b.frames + 1, 0);
+  std::vector<int> mod_of_shape;
+  for (auto &key : shape_order) {
+    int K0 = std::get<0>(key), K1 = std::get<1>(key), K2 = std::get<2>(key);
+    int mod0 = (int)mod.size();
+    for (int K : {K0, K1, K2}) {
+      std::vector<double> m = host_moduli(K, order);
+      for (double v : m) mod.push_back((float)v);
+    }
+    const std::vector<int> &fr = by_shape[key];
+    mdrtNbBatch::Shape sh;
+    sh.K[0] = K0;
+    sh.K[1] = K1;
+    sh.K[2] = K2;
+    sh.count = (int)fr.size();
+    sh.grid0 = grid0;
+    sh.spec0 = spec0;
+    sh.fwd = sh.bwd = 0;
+    long long total = (long long)K0 * K1 * K2, half = (long long)K0 * K1 * (K2 / 2 + 1);
+    for (int f : fr) {
+      NbFrameDev &F = b.h_frames[f];
+      F.K0 = K0;
+      F.K1 = K1;
+      F.K2 = K2;
+      F.mod0 = mod0;
+      F.grid0 = grid0;
+      F.spec0 = spec0;
+      grid0 += total;
+      spec0 += half;
+    }
+    int n[3] = {K0, K1, K2};
+    if (cufftPlanMany(&sh.fwd, 3, n, nullptr, 1, (int)total, nullptr, 1, (int)half, CUFFT_R2C, sh.count) !=
+            CUFFT_SUCCESS ||
+        cufftPlanMany(&sh.bwd, 3, n, nullptr, 1, (int)half, nullptr, 1, (int)total, CUFFT_C2R, sh.count) !=
+            CUFFT_SUCCESS) {
+      b.shapes.push_back(sh);
+      return -3;
+    }
+    b.shapes.push_back(sh);
+  }
+  // the convolution's blocks, frame by frame
+  for (int f = 0; f < b.frames; ++f) {
+    const NbFrameDev &F = b.h_frames[f];
+    long long half = (long long)F.K0 * F.K1 * (F.K2 / 2 + 1);
+    int nb = (int)((half + 255) / 256);
+    blk0[f] = (int)blk_frame.size();
+    blk_frame.insert(blk_frame.end(), nb, f);
+  }
+  blk0[b.frames] = (int)blk_frame.size();
+  b.conv_blocks = (int)blk_frame.size();
+  b.h_conv_blk0 = blk0;
+  if (cudaMalloc(&P.grid, sizeof(float) * std::max<long long>(grid0, 1)) != cudaSuccess ||
+      cudaMalloc(&P.spec, sizeof(float2) * std::max<long long>(spec0, 1)) != cudaSuccess ||
+      cudaMalloc(&P.moduli, sizeof(float) * mod.size()) != cudaSuccess ||
+      cudaMalloc(&b.conv_part, sizeof(double) * 7 * std::max(b.conv_blocks, 1)) != cudaSuccess ||
+      cudaMalloc(&b.conv_blk_frame, sizeof(int32_t) * std::max(b.conv_blocks, 1)) != cudaSuccess ||
+      cudaMalloc(&b.d_conv_blk0, sizeof(int32_t) * (b.frames + 1)) != cudaSuccess)
+    return -1;
+  cudaMemcpy(P.moduli, mod.data(), sizeof(float) * mod.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(b.conv_blk_frame, blk_frame.data(), sizeof(int32_t) * b.conv_blocks, cudaMemcpyHostToDevice);
+  cudaMemcpy(b.d_conv_blk0, blk0.data(), sizeof(int32_t) * (b.frames + 1), cudaMemcpyHostToDevice);
+  b.grid_points = grid0;
+  if (c.places_cap > 0) {
+    if (cudaMalloc(&P.pme_force, sizeof(float4) * c.places_cap) != cudaSuccess) return -1;
+    if (cudaMalloc(&P.potential, sizeof(float) * c.places_cap) != cudaSuccess) return -1;
+  }
+  P.order = order;
+  P.on = true;
+  b.order = order;
+  b.pme = true;
+  if (b.frames_dev)
+    cudaMemcpy(b.frames_dev, b.h_frames.data(), sizeof(NbFrameDev) * b.frames, cudaMemcpyHostToDevice);
+  return 0;
+}
+
+int nb_batch_pme_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
+  NbCtx &c = b.nb->c;
+  NbPme &P = c.pme;
+  if (!b.pme || c.beta <= 0.0) return 0;
+  cudaMemsetAsync(P.grid, 0, sizeof(float) * b.grid_points, s);
+  int64_t threads = c.places_cap * b.order;
+  if (b.order == 4)
+    nb_batch_spread<4><<<blocks_for(threads, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, b.atom_frame,
+                                                               b.frames_dev, c.xq, P.grid);
+  else
+    nb_batch_spread<8><<<blocks_for(threads, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, b.atom_frame,
+                                                               b.frames_dev, c.xq, P.grid);
+  for (auto &sh : b.shapes) {
+    cufftSetStream(sh.fwd, s);
+    if (cufftExecR2C(sh.fwd, P.grid + sh.grid0, (cufftComplex *)P.spec + sh.spec0) != CUFFT_SUCCESS) return -3;
+  }
+  if (energy)
+    nb_batch_convolve<true><<<b.conv_blocks, 256, 0, s>>>(b.conv_blk_frame, b.d_conv_blk0, b.frames_dev, P.moduli,
+                                                          P.spec, b.conv_part);
+  else
+    nb_batch_convolve<false><<<b.conv_blocks, 256, 0, s>>>(b.conv_blk_frame, b.d_conv_blk0, b.frames_dev, P.moduli,
+                                                           P.spec, b.conv_part);
+  for (auto &sh : b.shapes) {
+    cufftSetStream(sh.bwd, s);
+    if (cufftExecC2R(sh.bwd, (cufftComplex *)P.spec + sh.spec0, P.grid + sh.grid0) != CUFFT_SUCCESS) return -3;
+  }
+  float4 *pf = (float4 *)P.pme_force;
+  if (b.order == 4)
+    nb_batch_gather_split<4><<<blocks_for(c.places_cap * 4, 128), 128, 0, s>>>(
+        c.places_cap, c.sizes, c.order, b.atom_frame, b.frames_dev, c.xq, P.grid, pf);
+  else
+    nb_batch_gather_split<8><<<blocks_for(c.places_cap * 8, 128), 128, 0, s>>>(
+        c.places_cap, c.sizes, c.order, b.atom_frame, b.frames_dev, c.xq, P.grid, pf);
+  return 0;
+}

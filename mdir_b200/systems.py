@@ -143,10 +143,12 @@ def tip3p(waters=7850, density=33.4, seed=3, jitter=0.02, cutoff=0.9, skin=0.1, 
 
 
 def solvated_frame(atoms, seed, solute_fraction=0.05, solute_types=7, cutoff=0.9, skin=0.1,
-                   tol=1e-5, spacing=0.1, order=4, water_density=100.2):
+                   tol=1e-5, spacing=0.1, order=4, water_density=100.2, table=None):
     """A cubic box at water density holding `atoms` atoms (a multiple of 3):
     waters, of which 5% of the atoms are replaced by solute atoms with
-    random charges (zero net) and LJ types 1..solute_types."""
+    random charges (zero net) and LJ types 1..solute_types.  `table`
+    (per-type sigma, epsilon of the solute types) is drawn from the frame's
+    seed when not given."""
     rng = np.random.default_rng(seed)
     assert atoms % 3 == 0
     waters = atoms // 3
@@ -166,8 +168,10 @@ def solvated_frame(atoms, seed, solute_fraction=0.05, solute_types=7, cutoff=0.9
     qs -= qs.mean()
     q[sol_atoms] = qs
     types[sol_atoms] = rng.integers(1, solute_types + 1, size=len(sol_atoms))
-    sig = np.concatenate([[SIG_O], rng.uniform(0.25, 0.40, solute_types), [0.1]])
-    eps = np.concatenate([[EPS_O], rng.uniform(0.2, 1.0, solute_types), [0.0]])
+    if table is None:
+        table = (rng.uniform(0.25, 0.40, solute_types), rng.uniform(0.2, 1.0, solute_types))
+    sig = np.concatenate([[SIG_O], table[0], [0.1]])
+    eps = np.concatenate([[EPS_O], table[1], [0.0]])
     sigma, epsilon = _lb_tables(sig, eps)
     q -= q.mean()  # exact zero net charge of the frame
     s = dict(sysw)
@@ -176,12 +180,15 @@ def solvated_frame(atoms, seed, solute_fraction=0.05, solute_types=7, cutoff=0.9
     return s
 
 
-def batch_frames(count=256, low=1000, high=8000, seed=4, **kw):
+def batch_frames(count=256, low=1000, high=8000, seed=4, solute_types=7, **kw):
     """`count` solvated frames with atom counts uniform in [low, high],
-    multiples of 3."""
+    multiples of 3, sharing one LJ type table (8 types with LJ: the water
+    oxygen and `solute_types` solute types drawn once for the batch)."""
     rng = np.random.default_rng(seed)
     sizes = 3 * rng.integers(low // 3, high // 3 + 1, size=count)
-    return [solvated_frame(int(a), seed=int(rng.integers(1 << 30)), **kw) for a in sizes]
+    table = (rng.uniform(0.25, 0.40, solute_types), rng.uniform(0.2, 1.0, solute_types))
+    return [solvated_frame(int(a), seed=int(rng.integers(1 << 30)), solute_types=solute_types, table=table, **kw)
+            for a in sizes]
 
 
 def force_matching(frames=64, waters=7850, types=8, seed=5, jitter=0.005, perturb=0.02, perturb_seed=6, **kw):
