@@ -160,3 +160,16 @@ class BatchEvaluator:
         terms["virial_pair"] = out[:, L.W_PAIR:L.W_PAIR + 6]
         terms["virial_reciprocal"] = out[:, L.W_RECIPROCAL:L.W_RECIPROCAL + 6]
         return terms
+
+
+def shard(atoms, ranks):
+    """Frames assigned to ranks by greedy bin-packing on their atom counts
+    (largest first, each to the least loaded rank): a list of frame-number
+    lists, each in increasing order."""
+    load = [0] * ranks
+    out = [[] for _ in range(ranks)]
+    for f in sorted(range(len(atoms)), key=lambda k: (-int(atoms[k]), k)):
+        r = min(range(ranks), key=lambda q: (load[q], q))
+        out[r].append(f)
+        load[r] += int(atoms[f])
+    return [sorted(o) for o in out]

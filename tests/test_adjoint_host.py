@@ -76,3 +76,14 @@ def test_force_matching_workload_shapes():
     # the same seeds give the same workload
     s2, X2, _ = systems.force_matching(frames=3, waters=300, types=8)
     assert np.array_equal(X, X2)
+
+
+def test_batch_shards_balance_atoms():
+    from mdir_b200.batch import shard
+    rng = np.random.default_rng(4)
+    atoms = 3 * rng.integers(333, 2667, size=256)
+    for ranks in (1, 2, 4, 8):
+        parts = shard(atoms, ranks)
+        assert sorted(f for p in parts for f in p) == list(range(256))
+        loads = [int(atoms[p].sum()) for p in parts]
+        assert max(loads) - min(loads) <= int(atoms.max())
