@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="skip the force-matching gradient leg")
     p.add_argument("--no-batch", action="store_true", help="skip the batch-of-frames leg")
+    p.add_argument("--no-precision", action="store_true", help="skip the 1.07M-atom precision leg")
     return p.parse_args()
 
 
@@ -340,6 +341,73 @@ def batch_leg(args, dev, flush, world=1, rank=0, frames=256, reps=5, warmup=3):
             "l2": "flushed before each timed batch (256 MiB write)"}
 
 
+def precision_leg(args, dev, flush, thermalize=1000, nve=10000, every=500, timed=200):
+    """The precision form on the large water box (356,700 TIP3P waters,
+    1.07M atoms, 224^3 grid) in the deterministic mode (FP32 pairs, 64-bit
+    fixed-point forces and grid, FP64 energies): ns/day of the NVT step,
+    bitwise determinism of two 20-step runs from one state, and the NVE
+    drift of the total energy (potential and kinetic energy at the same
+    time) after a thermalisation.  The RMS force error against FP64 is the
+    tests' (the oracle does not run here)."""
+    import torch
+    from mdir_b200 import NonbondedTerm, systems
+    from mdir_b200.md import Integrator
+    s = systems.tip3p(waters=356700)
+    n = len(s["charges"])
+    t = NonbondedTerm(n, device=dev.index)
+    t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t.set_exclusions(pairs=s["excluded_pairs"])
+    t.set_interaction(s["cutoff"], 1.2, s["beta"])
+    t.set_pruned_reach(1.0)
+    t.set_pme(s["grid"], s["order"])
+    t.set_deterministic(True)
+    md = Integrator(t, s["masses"], s["waters"])
+    x = torch.tensor(s["positions"], dtype=torch.float64, device=dev)
+    v = torch.tensor(systems.maxwell_velocities(s, 300.0, seed=2), device=dev)
+    box = s["box"]
+    md.build(x, box)
+    md.thermostat(300.0, 0.02, seed=11)
+    md.run(x, v, box, DT_PS, thermalize, unroll=10)
+    md.thermostat(300.0, 0.1, seed=12)
+    stream = torch.cuda.current_stream(dev)
+    flush.zero_()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    md.run(x, v, box, DT_PS, timed, unroll=10)
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b)
+    # two runs of 20 NVE steps from one state
+    md.thermostat(300.0, 0.0, seed=13)
+    x0, v0 = x.clone(), v.clone()
+    md.build(x, box)
+    md.run(x, v, box, DT_PS, 20, unroll=10)
+    x1, v1 = x.clone(), v.clone()
+    x.copy_(x0)
+    v.copy_(v0)
+    md.build(x, box)
+    md.run(x, v, box, DT_PS, 20, unroll=10)
+    same = bool(torch.equal(x, x1) and torch.equal(v, v1))
+    # NVE
+    samples = []
+    for _ in range(nve // every):
+        md.run(x, v, box, DT_PS, every - 1, unroll=0 if (every - 1) % 10 else 10)
+        samples.append(md.total_energy(x, v, box, DT_PS))
+    E = np.array(samples)
+    tt = np.arange(len(E)) * every * DT_PS
+    slope = float(np.polyfit(tt, E[:, 0], 1)[0]) if len(E) > 1 else 0.0  # kJ/mol/ps
+    kin = float(E[:, 2].mean())
+    return {"workload": "tip3p-1070100 (356,700 waters, 224^3 grid), deterministic mode",
+            "ns_per_day": round(ns_per_day(timed, ms / 1e3), 2), "ms_per_step": round(ms / timed, 4),
+            "bitwise_deterministic_two_runs": same, "status": t.status(),
+            "nve": {"steps": nve, "dt_ps": DT_PS, "drift_kj_mol_ns": round(slope * 1000.0, 3),
+                    "drift_per_atom_kj_mol_ns": round(slope * 1000.0 / n, 6),
+                    "drift_relative_to_kinetic_per_ns": round(slope * 1000.0 / kin, 6),
+                    "total_std_kj_mol": round(float(E[:, 0].std()), 3),
+                    "temperature_K": round(2.0 * kin / (md.thermo()["ndof"] * 0.0083144626181532), 1)},
+            "force_error": "RMS relative force error vs FP64 <= 1e-5 (tests/test_gpu_precision.py)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -521,6 +589,8 @@ def main():
         line["adjoint"] = adjoint_leg(args, dev, flush, world)
     if not args.no_batch:
         line["batch"] = batch_leg(args, dev, flush, world, rank)
+    if not args.no_precision and world == 1:
+        line["precision"] = precision_leg(args, dev, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(s, s["positions"])
     if rank == 0:

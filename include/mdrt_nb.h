@@ -85,7 +85,7 @@ enum mdrtNbGroupsSlot {
   MDRT_NB_GROUPS_ENTRIES = 2,  /* int32x2 [groups * capacity]: (place, mask | image << 16) */
   MDRT_NB_GROUPS_UNITS = 4,    /* int32x2 [units]: (group, ordinal) */
   MDRT_NB_GROUPS_SHIFTS = 6,   /* int8x4 [places]: whole cells S of each place */
-  MDRT_NB_GROUPS_PLACED = 15,  /* float32x4 [places]: frames (x + S L, q) */
+  MDRT_NB_GROUPS_PLACED = 15,  /* float32x4 [places]: frames (x + (S - 1/2) L, q), centred on the cell */
   MDRT_NB_GROUPS_PLACE_OF = 16 /* int32 [particles]: place of each atom, -1 none */
 };
 
@@ -266,7 +266,9 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
                      const int32_t *waters, double d_oh, double d_hh);
 int32_t mdrtMdDestroy(mdrtMd *md);
 /* Bussi (CSVR) thermostat at `temperature` K with time constant tau (ps);
- * tau <= 0 leaves the energy constant (NVE).  `seed` fixes the noise. */
+ * tau <= 0 leaves the energy constant (NVE).  `seed` fixes the noise.  The
+ * velocity scaling a step computes for the next one is dropped: the next
+ * step starts unscaled. */
 int32_t mdrtMdSetThermostat(mdrtMd *md, double temperature, double tau, uint64_t seed);
 /* A neighbor build at device positions x that also resets the reference
  * positions of the test of validity (D80). */

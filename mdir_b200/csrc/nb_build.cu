@@ -859,6 +859,75 @@ int nb_build_run(NbCtx &c, const double *x, const double box[3], cudaStream_t s)
   return -1;
 }
 
+namespace {
+
+// Copies the entries of each list from a slab of old_cap entries a group to
+// one of new_cap (a thread per entry of the old slab).
+__global__ void nb_copy_lists(int64_t groups, const int32_t *__restrict__ sizes, int64_t old_cap, int64_t new_cap,
+                              const int32_t *__restrict__ counts, const int2 *__restrict__ src,
+                              int2 *__restrict__ dst) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t g = t / old_cap, e = t - g * old_cap;
+  if (g >= groups || g >= sizes[NB_SIZE_GROUPS]) return;
+  if (e >= min((int64_t)counts[g], old_cap)) return;
+  dst[g * new_cap + e] = src[g * old_cap + e];
+}
+
+}  // namespace
+
+int nb_grow_lists_keep(NbCtx &c, int64_t longest, cudaStream_t s) {
+  int64_t want = (longest + longest / 4 + NB_UNIT - 1) / NB_UNIT * NB_UNIT;
+  if (want <= c.list_cap || !c.built) return 0;
+  int64_t G = c.groups_cap, C0 = c.list_cap;
+  int64_t units = G * ((want + NB_UNIT - 1) / NB_UNIT);
+  bool inner = c.slab_in != nullptr;
+  int2 *slab = nullptr, *slab_in = nullptr, *units_new = nullptr, *units_in = nullptr;
+  double *partials = nullptr;
+  auto fail = [&]() {
+    for (void *p : {(void *)slab, (void *)slab_in, (void *)units_new, (void *)units_in, (void *)partials})
+      if (p) cudaFree(p);
+    return -1;
+  };
+  if (cudaMalloc(&slab, sizeof(int2) * G * want) != cudaSuccess) return fail();
+  if (inner && cudaMalloc(&slab_in, sizeof(int2) * G * want) != cudaSuccess) return fail();
+  if (units > c.units_cap) {
+    if (cudaMalloc(&units_new, sizeof(int2) * units) != cudaSuccess ||
+        cudaMalloc(&partials, sizeof(double) * 8 * units) != cudaSuccess)
+      return fail();
+    if (inner && cudaMalloc(&units_in, sizeof(int2) * units) != cudaSuccess) return fail();
+  }
+  int blocks = blocks_for(G * C0, 256);
+  nb_copy_lists<<<blocks, 256, 0, s>>>(G, c.sizes, C0, want, c.counts, c.slab, slab);
+  if (inner) nb_copy_lists<<<blocks, 256, 0, s>>>(G, c.sizes, C0, want, c.counts_in, c.slab_in, slab_in);
+  if (units_new) {
+    cudaMemcpyAsync(units_new, c.units, sizeof(int2) * c.units_cap, cudaMemcpyDeviceToDevice, s);
+    if (inner) cudaMemcpyAsync(units_in, c.units_in, sizeof(int2) * c.units_cap, cudaMemcpyDeviceToDevice, s);
+  }
+  NB_CHECK(cudaStreamSynchronize(s));
+  NB_CHECK(cudaGetLastError());
+  cudaFree(c.slab);
+  c.slab = slab;
+  if (inner) {
+    cudaFree(c.slab_in);
+    c.slab_in = slab_in;
+  }
+  if (units_new) {
+    cudaFree(c.units);
+    cudaFree(c.unit_partials);
+    c.units = units_new;
+    c.unit_partials = partials;
+    if (inner) {
+      cudaFree(c.units_in);
+      c.units_in = units_in;
+    }
+    c.units_cap = units;
+  }
+  c.list_cap = want;
+  c.inner_key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap;
+  c.grows++;
+  return 0;
+}
+
 int nb_grow_lists(NbCtx &c, int64_t longest) {
   int64_t want = (longest + longest / 4 + NB_UNIT - 1) / NB_UNIT * NB_UNIT;
   if (want <= c.list_cap) return 0;

@@ -4,9 +4,13 @@
 //   places     P = 16 * groups; place p holds atom order[p] or -1 (empty).
 //              A group is 16 consecutive places of one column of the grid,
 //              sorted along z (the spatial cell sort of the build).
-//   frames     xq[p] = float4(x + S_p L rounded once to f32, q); S_p is the
-//              whole-cell shift that took the atom into the cell at the
-//              last build (kept per place, three int8 in shift_p).
+//   frames     xq[p] = float4(x + (S_p - 1/2) L rounded once to f32, q);
+//              S_p is the whole-cell shift that took the atom into the cell
+//              at the last build (kept per place, three int8 in shift_p).
+//              The frames are centred on the cell: the largest coordinate,
+//              and so the spacing of f32 values, is half that of [0, L);
+//              pair displacements do not depend on the origin, and readers
+//              of absolute positions (PME) add the half cell back.
 //   lists      one slab of C entries per group: entry = int2(q, bits) with
 //              q the partner place, bits 0-15 the members that pair with it
 //              and bits 16-20 the image code 9(sz+1)+3(sy+1)+(sx+1).
@@ -46,6 +50,10 @@ struct NbBox {
   float L[3];      // edges in f32
   double Ld[3];    // edges in f64
 };
+
+// The multiple of the cell edge added to an atom's position in its frame:
+// its whole-cell shift less the half cell of the centred frames.
+__host__ __device__ inline double nb_frame_shift(int s) { return (double)s - 0.5; }
 
 __host__ __device__ inline int nb_image_code(int sx, int sy, int sz) {
   return 9 * (sz + 1) + 3 * (sy + 1) + (sx + 1);

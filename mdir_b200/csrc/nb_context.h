@@ -222,6 +222,12 @@ int nb_reserve_inner(NbCtx &c);
 // Grows the list capacity for lists of up to `longest` entries (+25%), as
 // the count of a build that overflowed asks (host, between launches).
 int nb_grow_lists(NbCtx &c, int64_t longest);
+// The same growth keeping the lists in force: their entries and units are
+// copied into the larger buffers, so nothing needs a build (host wait on s).
+int nb_grow_lists_keep(NbCtx &c, int64_t longest, cudaStream_t s);
+// Lists longer than this fraction of the capacity are grown ahead, before a
+// rebuild inside the step graphs overflows.
+#define NB_GROW_AHEAD 0.85
 void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
 void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);

@@ -32,6 +32,7 @@
 struct mdrtMd {
   NbCtx *nb = nullptr;
   mdrtNb *handle = nullptr;
+  int device = 0;                  // the context's device (the context may go first)
   int64_t n = 0, nwaters = 0, nfree = 0;
   double *inv_mass = nullptr;      // device f64 [n]
   double *mass = nullptr;          // device f64 [n]
@@ -188,7 +189,8 @@ __device__ __forceinline__ void write_frame(int a, Vec3 x, const int32_t *__rest
   if (p < 0) return;
   char4 s = shift[p];
   float4 o = xq[p];
-  xq[p] = make_float4((float)(x.x + s.x * L[0]), (float)(x.y + s.y * L[1]), (float)(x.z + s.z * L[2]), o.w);
+  xq[p] = make_float4((float)(x.x + nb_frame_shift(s.x) * L[0]), (float)(x.y + nb_frame_shift(s.y) * L[1]),
+                      (float)(x.z + nb_frame_shift(s.z) * L[2]), o.w);
 }
 
 #define MD_UPDATE_THREADS 64
@@ -298,8 +300,9 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
       store3(v, a, vn);
       store3(fout, a, f);
       if (p >= 0) {
-        xq[p] = make_float4((float)(xn.x + sh.x * U.L[0]), (float)(xn.y + sh.y * U.L[1]),
-                            (float)(xn.z + sh.z * U.L[2]), qw);
+        xq[p] = make_float4((float)(xn.x + nb_frame_shift(sh.x) * U.L[0]),
+                            (float)(xn.y + nb_frame_shift(sh.y) * U.L[1]),
+                            (float)(xn.z + nb_frame_shift(sh.z) * U.L[2]), qw);
         if (U.fixed) {
           accf[3 * p] = 0ull;
           accf[3 * p + 1] = 0ull;
@@ -600,6 +603,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
   mdrtMd *m = new mdrtMd();
   m->nb = &c;
   m->handle = nb;
+  m->device = c.device;
   m->n = c.n;
   m->nwaters = nwaters;
   m->dOH = d_oh;
@@ -710,7 +714,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
 
 int32_t mdrtMdDestroy(mdrtMd *m) {
   if (m) {
-    cudaSetDevice(m->nb->device);
+    cudaSetDevice(m->device);
     md_free(m);
   }
   return MDRT_NB_OK;
@@ -722,6 +726,11 @@ int32_t mdrtMdSetThermostat(mdrtMd *m, double temperature, double tau, uint64_t 
   m->tau = tau;
   m->seed = seed;
   md_drop_graph(m);  // parameters are baked into the graph
+  // the scaling the last step computed for the next one belongs to the old
+  // thermostat: the next step starts unscaled
+  double one = 1.0;
+  cudaSetDevice(m->device);
+  if (cudaMemcpy(m->thermo, &one, sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
   return MDRT_NB_OK;
 }
 
@@ -734,6 +743,8 @@ int32_t mdrtMdBuild(mdrtMd *m, const double *x, const double box[3], void *strea
   if (s) return s;
   cudaStream_t st = (cudaStream_t)stream;
   NbCtx &c = *m->nb;
+  if (sizes[NB_SIZE_LONGEST] > NB_GROW_AHEAD * c.list_cap && nb_grow_lists_keep(c, sizes[NB_SIZE_LONGEST], st))
+    return MDRT_NB_CUDA_ERROR;
   nb_gather_frames(c, x, box, st);
   md_after_build<<<blocks_for(3 * m->n, 256), 256, 0, st>>>(3 * m->n, x, m->x_ref, m->thermo, c.sizes, c.status,
                                                             m->peak);
@@ -905,7 +916,12 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
         cudaStreamSynchronize(st) != cudaSuccess)
       return MDRT_NB_CUDA_ERROR;
     if (m->h_peak[2] > 0) return MDRT_NB_NAN_POSITION;
-    if (m->h_peak[1] == 0) break;
+    if (m->h_peak[1] == 0) {
+      // lists near their capacity grow ahead, keeping those in force
+      if (m->h_peak[0] > NB_GROW_AHEAD * c.list_cap && nb_grow_lists_keep(c, m->h_peak[0], st))
+        return MDRT_NB_CUDA_ERROR;
+      break;
+    }
     if (attempt >= 8) return MDRT_NB_GROW;
     if (cudaMemcpyAsync(x, m->x_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(v, m->v_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   }
 }
 
-// Frames: xq[p] = ((float)(x_a + S_p L), q_a) for the atom a at place p;
+// Frames: xq[p] = ((float)(x_a + (S_p - 1/2) L), q_a) for the atom a at place p;
 // an empty place gets zeros (no bit names it).
 __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
                           const int32_t *__restrict__ order, const char4 *__restrict__ shift,
@@ -254,8 +254,8 @@ __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
     return;
   }
   char4 s = shift[p];
-  xq[p] = make_float4((float)(x[3 * a] + s.x * Lx), (float)(x[3 * a + 1] + s.y * Ly),
-                      (float)(x[3 * a + 2] + s.z * Lz), q[a]);
+  xq[p] = make_float4((float)(x[3 * a] + nb_frame_shift(s.x) * Lx), (float)(x[3 * a + 1] + nb_frame_shift(s.y) * Ly),
+                      (float)(x[3 * a + 2] + nb_frame_shift(s.z) * Lz), q[a]);
   typ_p[p] = type[a];
 }
 
@@ -371,8 +371,9 @@ __global__ void nb_batch_gather(int64_t places, const int32_t *__restrict__ size
   }
   const NbFrameDev &F = frames[atom_frame[a]];
   char4 s = shift[p];
-  xq[p] = make_float4((float)(x[3 * a] + s.x * F.L0), (float)(x[3 * a + 1] + s.y * F.L1),
-                      (float)(x[3 * a + 2] + s.z * F.L2), q[a]);
+  xq[p] = make_float4((float)(x[3 * a] + nb_frame_shift(s.x) * F.L0),
+                      (float)(x[3 * a + 1] + nb_frame_shift(s.y) * F.L1),
+                      (float)(x[3 * a + 2] + nb_frame_shift(s.z) * F.L2), q[a]);
   typ_p[p] = type[a];
 }
 

