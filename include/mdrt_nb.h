@@ -137,7 +137,11 @@ int32_t mdrtNbPrune(mdrtNb *ctx, const double *x, const double box[3], void *str
  * kernels beside it).  Returns MDRT_NB_INVALID_ARGUMENT for an unknown key
  * or value.  No MDIR counterpart: MDIR fixes these in its emitters
  * (lib/Dialect/MDExec/DevicePolicy.cpp:72-99). */
-enum mdrtNbTuneKey { MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM = 0, MDRT_NB_TUNE_SEARCH_WARPS = 1 };
+enum mdrtNbTuneKey {
+  MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM = 0,
+  MDRT_NB_TUNE_SEARCH_WARPS = 1,  /* batches only */
+  MDRT_NB_TUNE_PAIR_SMS = 2       /* SMs the pair grid spans (0: all); the others stay free for PME */
+};
 int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value);
 
 /* Deterministic mode: 64-bit fixed-point force accumulation (2^32 per

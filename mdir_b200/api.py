@@ -147,6 +147,7 @@ class Execution:
         self.deterministic = False
         self.step_graph = True
         self.graph_steps = 10
+        self.pair_sms = 0  # SMs the pair kernel spans (0: all); the others are left to PME
 
 
 class Schedule:
@@ -261,6 +262,8 @@ def _make_term(program):
     t.set_deterministic(program.execution.deterministic)
     if p["pruned_reach"]:
         t.set_pruned_reach(p["pruned_reach"])
+    if program.execution.pair_sms:
+        t.set_tuning(pair_sms=program.execution.pair_sms)
     return t
 
 
@@ -291,6 +294,12 @@ class Simulation:
             if e.status == L.NAN_POSITION:
                 raise SimulationError("positions that are not numbers or are far outside the cell") from e
             raise
+
+    def tune(self, **kw):
+        """Times short runs over outer and pruned reaches and spans of the
+        pair grid and keeps the fastest (Integrator.tune; MDIR's skins
+        search, D281); the state is put back.  Returns the choice."""
+        return self.md.tune(self.x, self.v, self.box, self.program.integrator.timestep, **kw)
 
     def set_state(self, positions, velocities=None, non_blocking=False):
         """New positions (and velocities) from host or device arrays; the

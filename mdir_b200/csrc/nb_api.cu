@@ -256,6 +256,10 @@ int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value) {
       if (value < 1 || value > 4) return MDRT_NB_INVALID_ARGUMENT;
       ctx->c.pair_blocks_per_sm = value;
       return MDRT_NB_OK;
+    case MDRT_NB_TUNE_PAIR_SMS:
+      if (value < 0 || value > 4096) return MDRT_NB_INVALID_ARGUMENT;
+      ctx->c.pair_sms = value;
+      return MDRT_NB_OK;
   }
   return MDRT_NB_INVALID_ARGUMENT;
 }

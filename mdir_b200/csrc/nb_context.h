@@ -107,6 +107,7 @@ struct NbCtx {
   int64_t prunes = 0;
   // tuning (mdrtNbSetTuning): blocks of 8 warps per SM of the pair kernel
   int pair_blocks_per_sm = 4;
+  int pair_sms = 0;  // SMs the persistent pair grid spans (0: all); the rest are left to PME
   // parameter gradient scratch (mdrtNbParameterGradient), allocated at the first call
   float4 *adj_g = nullptr;        // per place: the cotangent on the forces (f32)
   double *adj_q = nullptr;        // per place: the charge gradient, kept zero between calls

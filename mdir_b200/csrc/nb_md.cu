@@ -790,7 +790,8 @@ static cudaError_t md_capture_if(cudaStream_t cap, cudaStream_t body, cudaGraphC
 static int32_t md_prepare_graph(mdrtMd *m, double *x, double *v, const double box[3], double dt, int32_t unroll) {
   NbCtx &c = *m->nb;
   int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap + (int64_t)(c.inner_reach * 1e9) +
-                (c.inner_valid ? 1 : 0) + (c.deterministic ? 2 : 0);
+                (c.inner_valid ? 1 : 0) + (c.deterministic ? 2 : 0) + ((int64_t)c.pair_blocks_per_sm << 40) +
+                ((int64_t)c.pair_sms << 44);
   bool stale = !m->exec || m->gx != x || m->gv != v || m->gdt != dt || m->gunroll != unroll ||
                m->gbox[0] != box[0] || m->gbox[1] != box[1] || m->gbox[2] != box[2] || m->gcap_key != key;
   if (stale) {

@@ -783,7 +783,8 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
   // blocks of 8 warps per SM (4 fit at 64 registers; fewer leave room for
   // the PME kernels that run beside it on another stream)
   int64_t want = (c.units_cap + 7) / 8;
-  int grid = (int)std::min<int64_t>(want, (int64_t)g_sm_count * std::max(1, c.pair_blocks_per_sm));
+  int sms = c.pair_sms > 0 ? std::min(c.pair_sms, g_sm_count) : g_sm_count;
+  int grid = (int)std::min<int64_t>(want, (int64_t)sms * std::max(1, c.pair_blocks_per_sm));
   if (grid < 1) grid = 1;
   // the inner list of the dual list once it has been pruned, else the outer
   bool inner = c.inner_reach > 0.0 && c.inner_valid;

@@ -67,6 +67,55 @@ class Integrator:
         L.check(L.lib().mdrtMdForces(self._h, ctypes.byref(p)), "mdrtMdForces")
         return p.value
 
+    def tune(self, x, v, box, dt, reaches=(1.2, 1.3, 1.4, 1.5), pruned=(1.0, 1.025), pair_sms=(0, 128),
+             steps=200, reps=3, stream=None):
+        """The autotuner of the step: times `reps` runs of `steps` steps for
+        every outer reach, pruned reach and span of the pair grid (SMs; the
+        others are left to the PME kernels beside it), keeps the fastest and
+        builds for it.  x and v are put back; the step counter and the
+        thermostat's noise move on.  MDIR searches its reaches the same way
+        (the skins search, D281, lib/Compiler/Skins.cpp).  Returns the choice
+        with its time per step (µs)."""
+        t = self.term
+        cutoff = t.interaction["cutoff"]
+        least = float(np.min(np.asarray(box, dtype=np.float64)))
+        keep_x, keep_v = x.clone(), v.clone()
+        st = stream if stream is not None else torch.cuda.current_stream(x.device)
+        trials = []
+        for R in reaches:
+            if not R < 0.999 * least:
+                continue
+            for Rin in pruned:
+                if not cutoff <= Rin < R:
+                    continue
+                for sms in pair_sms:
+                    t.set_reach(R)
+                    t.set_pruned_reach(Rin)
+                    t.set_tuning(pair_sms=sms)
+                    x.copy_(keep_x)
+                    v.copy_(keep_v)
+                    self.build(x, box, stream=st)
+                    self.run(x, v, box, dt, steps // 2, unroll=10, stream=st)
+                    ms = []
+                    for _ in range(reps):
+                        a = torch.cuda.Event(enable_timing=True)
+                        b = torch.cuda.Event(enable_timing=True)
+                        a.record(st)
+                        self.run(x, v, box, dt, steps, unroll=10, stream=st)
+                        b.record(st)
+                        b.synchronize()
+                        ms.append(a.elapsed_time(b) / steps)
+                    trials.append((float(np.median(ms)) * 1e3, R, Rin, sms))
+        us, R, Rin, sms = min(trials)
+        t.set_reach(R)
+        t.set_pruned_reach(Rin)
+        t.set_tuning(pair_sms=sms)
+        x.copy_(keep_x)
+        v.copy_(keep_v)
+        self.build(x, box, stream=st)
+        return {"reach": R, "pruned_reach": Rin, "pair_sms": sms, "us_per_step": round(us, 2),
+                "trials": len(trials)}
+
     def temperature(self, stream=None):
         t = self.thermo(stream)
         return 2.0 * t["kinetic"] / (t["ndof"] * KB)

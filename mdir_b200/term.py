@@ -57,6 +57,9 @@ class NonbondedTerm:
         self._h = handle
         self.box = None
         self.ntypes = 1
+        self.interaction = None
+        self.pruned = 0.0
+        self.pair_sms = 0
 
     def close(self):
         if getattr(self, "_h", None):
@@ -91,6 +94,15 @@ class NonbondedTerm:
                         lj_switch=False, switch_distance=0.0):
         L.check(L.lib().mdrtNbSetInteraction(self._h, cutoff, reach, beta, coulomb, int(coulomb_shift),
                                              int(lj_switch), switch_distance), "mdrtNbSetInteraction")
+        self.interaction = {"cutoff": cutoff, "reach": reach, "beta": beta, "coulomb": coulomb,
+                            "coulomb_shift": coulomb_shift, "lj_switch": lj_switch,
+                            "switch_distance": switch_distance}
+
+    def set_reach(self, reach):
+        """A new reach of the lists (the next build uses it)."""
+        kw = dict(self.interaction)
+        kw["reach"] = reach
+        self.set_interaction(**kw)
 
     def set_pme(self, grid, order=4):
         k = [0, 0, 0] if grid is None else [int(v) for v in grid]
@@ -99,15 +111,20 @@ class NonbondedTerm:
     def set_pruned_reach(self, pruned_distance):
         """The dual list: prune the lists to this reach (0: one list)."""
         L.check(L.lib().mdrtNbSetPrunedReach(self._h, float(pruned_distance)), "mdrtNbSetPrunedReach")
+        self.pruned = float(pruned_distance)
 
     def prune(self, x, box=None, stream=None):
         b = _host(self.box if box is None else box, np.float64)
         L.check(L.lib().mdrtNbPrune(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtNbPrune")
 
-    def set_tuning(self, pair_blocks_per_sm=None):
+    def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None):
         """Launch shapes (the autotuner's knobs); results do not depend on them."""
         if pair_blocks_per_sm is not None:
-            L.check(L.lib().mdrtNbSetTuning(self._h, 0, int(pair_blocks_per_sm)), "mdrtNbSetTuning")
+            L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_BLOCKS_PER_SM, int(pair_blocks_per_sm)),
+                    "mdrtNbSetTuning")
+        if pair_sms is not None:
+            L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_SMS, int(pair_sms)), "mdrtNbSetTuning")
+            self.pair_sms = int(pair_sms)
 
     def set_deterministic(self, on=True):
         L.check(L.lib().mdrtNbSetDeterministic(self._h, int(bool(on))), "mdrtNbSetDeterministic")

@@ -1,0 +1,150 @@
+"""Precision of the device path against the FP64 oracle on every workload:
+the RMS relative force error, and the NVE energy drift with the total energy
+taken both from the device potential and from the oracle's potential at the
+same positions.  Needs a CUDA device; prints one JSON object per workload.
+
+    python tests/precision_report.py [--quick]
+
+Workloads: argon (864 atoms, 1.0 nm cutoff, dispersion correction), the
+TIP3P box (23,550 atoms), the large TIP3P box (1,070,100 atoms, the
+deterministic mode), the 256 solvated frames of the batch, and the frames
+of the force-matching workload."""
+
+import argparse
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
+
+from oracle import oracle as O  # noqa: E402
+from mdir_b200 import NonbondedTerm, systems  # noqa: E402
+from mdir_b200.batch import BatchEvaluator  # noqa: E402
+from mdir_b200.md import Integrator  # noqa: E402
+
+KB = 0.0083144626181532
+
+
+def rms_rel(a, b):
+    return float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
+
+
+def term_for(s, deterministic=False, reach=None, pruned=None):
+    n = len(s["charges"])
+    t = NonbondedTerm(n)
+    t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t.set_exclusions(pairs=s["excluded_pairs"])
+    pme = s.get("pme", True)
+    t.set_interaction(s["cutoff"], reach or s["reach"], s["beta"] if pme else 0.0,
+                      lj_switch=s.get("lj_switch", False), switch_distance=s.get("switch", 0.0))
+    if pruned:
+        t.set_pruned_reach(pruned)
+    if pme:
+        t.set_pme(s["grid"], s["order"])
+    t.set_deterministic(deterministic)
+    return t
+
+
+def force_error(s, x=None, deterministic=False):
+    x = s["positions"] if x is None else x
+    t = term_for(s, deterministic)
+    xd = torch.tensor(x, dtype=torch.float64, device="cuda")
+    t.build(xd, s["box"])
+    F = t.force(xd).cpu().numpy()
+    t.close()
+    return rms_rel(F, O.evaluate(s, x)["forces"])
+
+
+def nve(s, dt, thermalize, steps, every, oracle_samples, deterministic=False, reach=None, pruned=None,
+        temperature=300.0):
+    """Total energy along an NVE run after a thermalisation: slope (kJ/mol/ns)
+    from the device potential, and from the oracle's at `oracle_samples`
+    evenly spaced samples."""
+    t = term_for(s, deterministic, reach, pruned)
+    md = Integrator(t, s["masses"], s.get("waters"))
+    x = torch.tensor(s["positions"], dtype=torch.float64, device="cuda")
+    v = torch.tensor(systems.maxwell_velocities(s, temperature, seed=2), device="cuda")
+    md.build(x, s["box"])
+    if thermalize:
+        md.thermostat(temperature, 0.02 if s.get("waters") is not None else 0.1, seed=3)
+        md.run(x, v, s["box"], dt, thermalize, unroll=10)
+    md.thermostat(temperature, 0.0, seed=4)
+    disp = bool(s.get("dispersion", False))
+    dev, ora, times = [], [], []
+    pick = set(np.linspace(0, steps // every - 1, oracle_samples).round().astype(int).tolist())
+    for k in range(steps // every):
+        md.run(x, v, s["box"], dt, every - 1, unroll=10 if (every - 1) % 10 == 0 else 0)
+        xk = x.cpu().numpy()
+        tot, pot, kin = md.total_energy(x, v, s["box"], dt, dispersion=disp)
+        dev.append(tot)
+        times.append((k + 1) * every * dt)
+        if k in pick:
+            ora.append((times[-1], O.evaluate(s, xk)["energy"] + kin))
+    dev = np.array(dev)
+    coef, cov = np.polyfit(times, dev, 1, cov=True)
+    slope = float(coef[0]) * 1000.0
+    slope_se = float(np.sqrt(cov[0, 0])) * 1000.0
+    oslope = float(np.polyfit([a for a, _ in ora], [b for _, b in ora], 1)[0]) * 1000.0 if len(ora) > 1 else None
+    kin = md.thermo()["kinetic"]
+    n = len(s["charges"])
+    out = {"steps": steps, "dt_ps": dt, "deterministic": deterministic,
+           "drift_kj_mol_ns": round(slope, 3), "drift_stderr_kj_mol_ns": round(slope_se, 3),
+           "drift_per_atom_kj_mol_ns": round(slope / n, 6),
+           "relative_change": round(float((dev[-1] - dev[0]) / abs(dev.mean())), 9),
+           "drift_oracle_kj_mol_ns": None if oslope is None else round(oslope, 3),
+           "total_std_kj_mol": round(float(dev.std()), 4), "kinetic_kj_mol": round(kin, 2),
+           "temperature_K": round(2 * kin / (md.thermo()["ndof"] * KB), 1),
+           "device_minus_oracle_total_kj_mol": [round(float(dev[int(round((a / dt) / every)) - 1] - b), 4)
+                                                for a, b in ora]}
+    md.close()
+    t.close()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--quick", action="store_true", help="shorter runs, no large box")
+    args = ap.parse_args()
+    q = args.quick
+    t0 = time.time()
+    # argon: reference argon.test checks drift over 2000 x 5 fs; here 2 fs
+    s = systems.argon()
+    print(json.dumps({"workload": "argon-864", "force_rms_rel": force_error(s),
+                      "nve": nve(s, 0.002, 0, 2000 if not q else 400, 101, 5, temperature=120.0)}), flush=True)
+    # MDIR's argon.test settings: LJ switched from 0.75 to 0.85 nm, 2000 x 5 fs
+    # (its bound: a relative drift of at most 1e-5)
+    s = dict(systems.argon(cutoff=0.85, skin=0.1))
+    s.update({"lj_switch": True, "switch": 0.75})
+    print(json.dumps({"workload": "argon-864-switched", "force_rms_rel": force_error(s),
+                      "nve": nve(s, 0.005, 0, 2000 if not q else 400, 101, 5, temperature=120.0)}), flush=True)
+    s = systems.tip3p()
+    print(json.dumps({"workload": "tip3p-23550",
+                      "force_rms_rel": force_error(s),
+                      "force_rms_rel_deterministic": force_error(s, deterministic=True),
+                      "nve": nve(s, 0.002, 3000, 100000 if not q else 1000, 501, 6, reach=1.5, pruned=1.025)}),
+          flush=True)
+    if not q:
+        s = systems.tip3p(waters=356700)
+        print(json.dumps({"workload": "tip3p-1070100", "force_rms_rel_deterministic": force_error(s, deterministic=True),
+                          "nve": nve(s, 0.002, 1000, 10000, 1001, 2, deterministic=True, reach=1.5, pruned=1.025)}),
+              flush=True)
+    frames = systems.batch_frames(count=256 if not q else 16)
+    ev = BatchEvaluator(frames)
+    F = ev.force(energy=False).cpu().numpy()
+    errs = [rms_rel(ev.frame(k, F), O.evaluate(f, f["positions"])["forces"]) for k, f in enumerate(frames)]
+    print(json.dumps({"workload": f"batch-{len(frames)}-frames", "force_rms_rel_median": float(np.median(errs)),
+                      "force_rms_rel_max": float(np.max(errs)), "atoms": int(ev.n)}), flush=True)
+    ev.close()
+    s, X, _ = systems.force_matching(frames=2)
+    errs = [force_error(s, X[k]) for k in range(2)]
+    print(json.dumps({"workload": "force-matching-frames", "force_rms_rel": errs}), flush=True)
+    print(json.dumps({"seconds": round(time.time() - t0, 1)}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
