@@ -49,6 +49,10 @@ def parse():
     p.add_argument("--equilibrate", type=int, default=5000, help="untimed MD steps before warm-up")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-tune", action="store_true", help="keep --reach/--pruned instead of the autotuner's choice")
+    p.add_argument("--pair-sms", type=int, default=0, help="span of the pair grid with --no-tune (0: all SMs)")
+    p.add_argument("--only", choices=["adjoint", "batch", "precision"], help="run one leg alone (profiling)")
+    p.add_argument("--adjoint-frames", type=int, default=64)
+    p.add_argument("--batch-frames", type=int, default=256)
     p.add_argument("--no-adjoint", action="store_true", help="skip the force-matching gradient leg")
     p.add_argument("--no-batch", action="store_true", help="skip the batch-of-frames leg")
     p.add_argument("--no-precision", action="store_true", help="skip the 1.07M-atom precision leg")
@@ -166,9 +170,9 @@ def adjoint_leg(args, dev, flush, world=1, frames=64, reps=5, warmup=3):
     With N ranks each takes its own `frames` (weak scaling) and the
     gradients are summed over the ranks (one f64 all-reduce per batch)."""
     import torch
-    import torch.distributed as dist
     from mdir_b200 import FrameEvaluator, systems
     from mdir_b200 import torch as mtorch
+    from mdir_b200.ranks import max_over_ranks, sum_gradients
     s, X, target = systems.force_matching(frames=frames, waters=args.waters)
     n = X.shape[1]
     ev = FrameEvaluator(s, device=dev.index)
@@ -188,9 +192,7 @@ def adjoint_leg(args, dev, flush, world=1, frames=64, reps=5, warmup=3):
         F = mtorch.forces(ev, sig, eps, q, x)
         loss = ((F - F_ref) ** 2).sum() / frames
         loss.backward()
-        if world > 1:
-            flat = torch.cat([sig.grad, eps.grad, q.grad])
-            dist.all_reduce(flat)
+        sum_gradients(sig.grad, eps.grad, q.grad)
         return loss
 
     stream = torch.cuda.current_stream(dev)
@@ -207,11 +209,7 @@ def adjoint_leg(args, dev, flush, world=1, frames=64, reps=5, warmup=3):
         b.record(stream)
         torch.cuda.synchronize(dev)
         ms.append(a.elapsed_time(b))
-    dev_ms = statistics.median(ms)
-    if world > 1:
-        t = torch.tensor([dev_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
+    dev_ms = max_over_ranks(statistics.median(ms), dev)
     # end to end: the frames from pinned host memory, the gradients back
     e2e = []
     for _ in range(reps):
@@ -225,11 +223,7 @@ def adjoint_leg(args, dev, flush, world=1, frames=64, reps=5, warmup=3):
         host_grad[n + len(sig):].copy_(eps.grad, non_blocking=True)
         torch.cuda.synchronize(dev)
         e2e.append(time.perf_counter() - t0)
-    e2e_s = statistics.median(e2e)
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(statistics.median(e2e), dev)
     # the plain forward of one frame with the same lists, for the differences
     Fb = torch.empty_like(Xd)
     fw = []
@@ -273,9 +267,9 @@ def batch_leg(args, dev, flush, world=1, rank=0, frames=256, reps=5, warmup=3):
     ranks the frames are shared by bin-packing on atom counts and the
     per-frame energies all-gathered."""
     import torch
-    import torch.distributed as dist
     from mdir_b200 import systems
     from mdir_b200.batch import BatchEvaluator, shard
+    from mdir_b200.ranks import gather_frame_values, max_over_ranks
     allf = systems.batch_frames(count=frames)
     mine = shard([len(f["charges"]) for f in allf], world)[rank] if world > 1 else list(range(frames))
     fr = [allf[k] for k in mine]
@@ -298,12 +292,7 @@ def batch_leg(args, dev, flush, world=1, rank=0, frames=256, reps=5, warmup=3):
             b.record(stream)
             torch.cuda.synchronize(dev)
             ms.append(a.elapsed_time(b))
-        m = statistics.median(ms)
-        if world > 1:
-            t = torch.tensor([m], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            m = float(t.item())
-        return m
+        return max_over_ranks(statistics.median(ms), dev)
 
     def build_and_force():
         ev.build()
@@ -322,13 +311,8 @@ def batch_leg(args, dev, flush, world=1, rank=0, frames=256, reps=5, warmup=3):
         ev.force(energy=True, graph=True)
         e = ev.energies()
         e2e.append(time.perf_counter() - t0)
-    e2e_s = statistics.median(e2e)
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-        got = [None] * world
-        dist.all_gather_object(got, (mine, e["potential"].tolist()))
+    e2e_s = max_over_ranks(statistics.median(e2e), dev)
+    gather_frame_values(frames, mine, e["potential"])
     atoms = int(ev.n)
     return {"metric": "batched frames/s (forces + per-frame energies, build included)",
             "frames": frames, "atoms_this_rank": atoms, "value": round(frames / (full_ms / 1e3), 1),
@@ -464,6 +448,21 @@ def main():
     from mdir_b200.md import Integrator
     from mdir_b200.term import NonbondedTerm, _dp, _hp, _stream
 
+    if args.only:
+        # one leg alone (profiling): its object as the JSON line
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        if args.only == "adjoint":
+            out = adjoint_leg(args, dev, flush, world, frames=args.adjoint_frames)
+        elif args.only == "batch":
+            out = batch_leg(args, dev, flush, world, rank, frames=args.batch_frames)
+        else:
+            out = precision_leg(args, dev, flush)
+        if rank == 0:
+            print(json.dumps({args.only: out}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
     s, v0 = workload(args)
     n = len(s["charges"])
     # ---- device-resident leg -------------------------------------------------
@@ -473,6 +472,8 @@ def main():
     term.set_interaction(s["cutoff"], s["reach"], s["beta"])
     term.set_pruned_reach(s["pruned"])
     term.set_pme(s["grid"], s["order"])
+    if args.no_tune and args.pair_sms:
+        term.set_tuning(pair_sms=args.pair_sms)
     md = Integrator(term, s["masses"], s["waters"])
     md.thermostat(300.0, 0.1, seed=1 + rank)
     x = torch.tensor(s["positions"], dtype=torch.float64, device=dev)
@@ -534,7 +535,7 @@ def main():
     integ.timestep = DT_PS
     ens.kind, ens.temperature, ens.tau_t = mdir.EnsembleKind.NVT, 300.0, 0.1
     exe.device, exe.graph_steps = local, args.unroll
-    exe.pair_sms = tuned["pair_sms"] if tuned else 0
+    exe.pair_sms = tuned["pair_sms"] if tuned else args.pair_sms
     sim = mdir.Simulation(mdir.compile(system, st, integ, ens, exe, sch))
     hx = torch.tensor(s["positions"], dtype=torch.float64).pin_memory()
     hv = torch.tensor(v0, dtype=torch.float64).pin_memory()
