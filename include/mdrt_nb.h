@@ -274,13 +274,29 @@ int32_t mdrtMdDestroy(mdrtMd *md);
  * velocity scaling a step computes for the next one is dropped: the next
  * step starts unscaled. */
 int32_t mdrtMdSetThermostat(mdrtMd *md, double temperature, double tau, uint64_t seed);
+/* The look-ahead of the rebuild decision: the drift's growth over the window
+ * that ended is extrapolated `factor` times (default 1; 0: none).  A drift
+ * past half the skin before the next decision stops the step (the steps
+ * after it do nothing) and the host rebuilds there, so a smaller factor
+ * costs stops, never a missed pair.  No MDIR counterpart: MDIR tests every
+ * step on the device and rebuilds in its host loop (ExposeValidity.cpp). */
+int32_t mdrtMdSetLookahead(mdrtMd *md, double factor);
 /* A neighbor build at device positions x that also resets the reference
  * positions of the test of validity (D80). */
 int32_t mdrtMdBuild(mdrtMd *md, const double *x, const double box[3], void *stream);
-/* `steps` leap-frog steps of dt (ps) on the device state x, v (f64 [n, 3]);
- * the lists are rebuilt on the device whenever 2 max|x - x_build| > R - r_c.
- * unroll > 0 replays a CUDA graph of `unroll` steps whose rebuilds are
- * conditional nodes (no host wait inside the graphs); the run of graphs
+/* `steps` leap-frog steps of dt (ps) on the device state x, v (f64 [n, 3]).
+ * The lists are pruned on the device whenever 2 max|x - x_prune| > R_in - r_c
+ * (gated launches in every step) and rebuilt at the end of each window of
+ * steps (`unroll` steps in a graph, 10 step by step) when the drift could
+ * pass half the skin before the next decision: 2 (d + factor (d - d_last)
+ * + 0.002 nm) > R - r_c, d = max|x - x_build| (mdrtMdSetLookahead).  A drift
+ * past half the skin inside a window stops the step there (the later steps
+ * of the graphs do nothing); the host rebuilds at that step and runs the
+ * steps left.  unroll > 0 replays a CUDA graph of `unroll` steps
+ * (one conditional node, the rebuild; no host wait inside); unroll < 0 runs
+ * step by step with a decision every -unroll steps (10 for unroll = 0); the
+ * steps after the last whole graph run step by step with the graph's window;
+ * the run of graphs
  * starts from a checkpoint of x, v and the thermostat state and ends in one
  * host wait that reads what its rebuilds saw: after a list that outgrew its
  * capacity the run is redone from the checkpoint with grown lists
@@ -289,9 +305,10 @@ int32_t mdrtMdBuild(mdrtMd *md, const double *x, const double box[3], void *stre
  * the host reading the test of validity after each step. */
 int32_t mdrtMdRun(mdrtMd *md, double *x, double *v, const double box[3], double dt, int64_t steps,
                   int32_t unroll, void *stream);
-/* out[8]: thermostat scaling, kinetic energy of the last two half steps,
+/* out[9]: thermostat scaling, kinetic energy of the last two half steps,
  * steps taken, builds made, degrees of freedom, prunings made, runs of step
- * graphs redone after a list overflow; waits for `stream`. */
+ * graphs redone after a list overflow, stops at a drift past half the skin
+ * between two rebuild decisions; waits for `stream`. */
 int32_t mdrtMdThermo(mdrtMd *md, void *stream, double *out);
 /* The device array of the forces of the last step (f64 [n, 3]). */
 int32_t mdrtMdForces(mdrtMd *md, double **forces);

@@ -52,6 +52,7 @@ SIGNATURES = {
     "mdrtMdCreate": (_i32, [ctypes.POINTER(_p), _p, _p, _i64, _p, _d, _d]),
     "mdrtMdDestroy": (_i32, [_p]),
     "mdrtMdSetThermostat": (_i32, [_p, _d, _d, ctypes.c_uint64]),
+    "mdrtMdSetLookahead": (_i32, [_p, _d]),
     "mdrtMdBuild": (_i32, [_p, _p, _p, _p]),
     "mdrtMdRun": (_i32, [_p, _p, _p, _p, _d, _i64, _i32, _p]),
     "mdrtMdThermo": (_i32, [_p, _p, _p]),

@@ -498,12 +498,21 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
                                                 float Lx, float Ly, float Lz, float rin2, int64_t list_cap,
                                                 const int2 *__restrict__ slab, const int32_t *__restrict__ counts,
                                                 const int32_t *__restrict__ order, const float4 *__restrict__ xq,
-                                                int2 *__restrict__ slab_in, int32_t *__restrict__ counts_in) {
+                                                int2 *__restrict__ slab_in, int32_t *__restrict__ counts_in,
+                                                const int *gate, const double *__restrict__ x,
+                                                double *__restrict__ x_prune) {
   __shared__ float4 s_m[4][NB_GROUP];
   const unsigned FULL = 0xffffffffu;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int64_t g = (int64_t)blockIdx.x * 4 + warp;
+  if (gate && *gate == 0) return;
   if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
+  if (x_prune) {
+    for (int k = lane; k < 3 * NB_GROUP; k += 32) {
+      int a = order[g * NB_GROUP + k / 3];
+      if (a >= 0) x_prune[3 * a + k % 3] = x[3 * a + k % 3];
+    }
+  }
   if (lane < NB_GROUP) s_m[warp][lane] = xq[g * NB_GROUP + lane];
   unsigned live = __ballot_sync(FULL, lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0) & 0xffffu;
   __syncwarp();
@@ -549,7 +558,8 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
     nb_prune_block(int64_t groups_cap, const int32_t *__restrict__ sizes, float Lx, float Ly, float Lz, float rin2,
                    int64_t list_cap, const int2 *__restrict__ slab, const int32_t *__restrict__ counts,
                    const int32_t *__restrict__ order, const float4 *__restrict__ xq, int2 *__restrict__ slab_in,
-                   int32_t *__restrict__ counts_in) {
+                   int32_t *__restrict__ counts_in, const int *gate, const double *__restrict__ x,
+                   double *__restrict__ x_prune) {
   extern __shared__ int2 s_stage[];
   __shared__ float4 s_m[NB_GROUP];
   __shared__ int s_cnt[NB_PRUNE_WARPS];
@@ -557,7 +567,12 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
   const unsigned FULL = 0xffffffffu;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int64_t g = blockIdx.x;
+  if (gate && *gate == 0) return;  // no pruning due (decided on the device)
   if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
+  if (x_prune && threadIdx.x < 3 * NB_GROUP) {  // the positions of the pruning, for its test of validity
+    int a = order[g * NB_GROUP + threadIdx.x / 3];
+    if (a >= 0) x_prune[3 * a + threadIdx.x % 3] = x[3 * a + threadIdx.x % 3];
+  }
   if (warp == 0) {
     if (lane < NB_GROUP) s_m[lane] = xq[g * NB_GROUP + lane];
     unsigned live = __ballot_sync(FULL, lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0) & 0xffffu;
@@ -801,17 +816,84 @@ void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s) {
     }
     nb_prune_block<<<(int)c.groups_cap, NB_PRUNE_WARPS * 32, stage, s>>>(
         c.groups_cap, c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
-        c.counts, c.order, c.xq, c.slab_in, c.counts_in);
+        c.counts, c.order, c.xq, c.slab_in, c.counts_in, nullptr, nullptr, nullptr);
   } else {
     nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
                                                         (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
-                                                        c.counts, c.order, c.xq, c.slab_in, c.counts_in);
+                                                        c.counts, c.order, c.xq, c.slab_in, c.counts_in, nullptr,
+                                                        nullptr, nullptr);
   }
   nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts_in, c.list_cap,
                                                              c.unit_n_in);
   nb_scan(c.unit_n_in, c.unit_start_in, (int)c.groups_cap, nullptr, c.scan_scratch, s);
   nb_unit_write<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.unit_n_in, c.unit_start_in,
                                                              c.units_cap, c.units_in, c.sizes_in);
+}
+
+namespace {
+
+// The units of the lists in one block: a scan of the groups' unit counts,
+// then the units (group, ordinal) in group order, the same as the
+// three-kernel path; with a gate, nothing unless it is set.  Counts one
+// more pruning in *prunes.
+__global__ void __launch_bounds__(1024) nb_units_one_block(int64_t groups_cap, const int32_t *__restrict__ sizes,
+                                                           const int32_t *__restrict__ counts, int64_t list_cap,
+                                                           int64_t units_cap, int32_t *__restrict__ unit_start,
+                                                           int2 *__restrict__ units, int32_t *__restrict__ sizes_out,
+                                                           const int *gate, double *prunes) {
+  __shared__ int s_part[1024];
+  if (gate && *gate == 0) return;
+  int G = (int)min((int64_t)sizes[NB_SIZE_GROUPS], groups_cap);
+  int t = threadIdx.x;
+  int per = (G + (int)blockDim.x - 1) / (int)blockDim.x;
+  int g0 = min(G, t * per), g1 = min(G, g0 + per);
+  int local = 0;
+  for (int g = g0; g < g1; ++g) local += ((int)min((int64_t)counts[g], list_cap) + NB_UNIT - 1) / NB_UNIT;
+  s_part[t] = local;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+    int y = t >= o ? s_part[t - o] : 0;
+    __syncthreads();
+    s_part[t] += y;
+    __syncthreads();
+  }
+  int at = s_part[t] - local;
+  for (int g = g0; g < g1; ++g) {
+    int n = ((int)min((int64_t)counts[g], list_cap) + NB_UNIT - 1) / NB_UNIT;
+    unit_start[g] = at;
+    for (int k = 0; k < n; ++k)
+      if (at + k < units_cap) units[at + k] = make_int2(g, k);
+    at += n;
+  }
+  if (t == (int)blockDim.x - 1) {
+    sizes_out[NB_SIZE_UNITS] = s_part[t];
+    if (prunes) *prunes += 1.0;
+  }
+}
+
+}  // namespace
+
+void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double *x, double *x_prune,
+                    double *prunes, cudaStream_t s) {
+  double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2]);
+  size_t stage = sizeof(int2) * (size_t)c.list_cap;
+  if (stage <= 200 * 1024) {
+    static int configured = 0;
+    if (stage > 48 * 1024 && configured < (int)stage) {
+      cudaFuncSetAttribute(nb_prune_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+      configured = (int)stage;
+    }
+    nb_prune_block<<<(int)c.groups_cap, NB_PRUNE_WARPS * 32, stage, s>>>(
+        c.groups_cap, c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+        c.counts, c.order, c.xq, c.slab_in, c.counts_in, gate, x, x_prune);
+  } else {
+    nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
+                                                        (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+                                                        c.counts, c.order, c.xq, c.slab_in, c.counts_in, gate, x,
+                                                        x_prune);
+  }
+  nb_units_one_block<<<1, 1024, 0, s>>>(c.groups_cap, c.sizes, c.counts_in, c.list_cap, c.units_cap, c.unit_start_in,
+                                       c.units_in, c.sizes_in, gate, prunes);
 }
 
 // One complete build with count-then-grow: the list capacity C grows to a

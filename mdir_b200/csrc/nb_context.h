@@ -218,6 +218,12 @@ void nb_build_launch_public(NbCtx &c, const double *x, const double box[3], cuda
 // The pruning of the outer lists into the inner ones at the current frames
 // xq (gathered by the caller), and the inner units; no host wait.
 void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s);
+// The same pruning as two launches that do nothing unless *gate (device) is
+// set: the inner lists with the positions of the pruning copied to x_prune,
+// then the inner units in one block, counting the pruning in *prunes.  The
+// per-step pruning of the MD step, which needs no conditional node.
+void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double *x, double *x_prune,
+                    double *prunes, cudaStream_t s);
 // Allocates the inner lists to the outer capacities (host, between launches).
 int nb_reserve_inner(NbCtx &c);
 // Grows the list capacity for lists of up to `longest` entries (+25%), as
@@ -230,7 +236,8 @@ int nb_grow_lists_keep(NbCtx &c, int64_t longest, cudaStream_t s);
 // rebuild inside the step graphs overflows.
 #define NB_GROW_AHEAD 0.85
 void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
-void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
+// With `halt` (device), nothing when *halt is set (the MD step's stop).
+void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt = nullptr);
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
 // The correction over a given list of pairs (i < j), forces only.
 void nb_excluded_list_run(NbCtx &c, const double box[3], const int32_t *pairs, int64_t npairs,
@@ -250,6 +257,12 @@ int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double 
                    double *dq, double *dtable, cudaStream_t s);
 // The reciprocal part of the charge gradient, added per place into c.adj_q.
 int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s);
+
+// The MD step's reciprocal chain when the update gathers (order 4): the
+// frames spread into qgrid (through qfixed, empty, in the deterministic
+// mode) -> spec -> phi, on the integrator's own buffers.
+int nb_pme_md_chain(NbCtx &c, const double box[3], float *qgrid, unsigned long long *qfixed, float2 *spec,
+                    float *phi, cudaStream_t s);
 
 // The batch (mdrtNbBatch): the build of all frames (grows and builds again
 // until every list fits; host wait), the frames of the places, the pair

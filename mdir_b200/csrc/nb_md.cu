@@ -26,6 +26,7 @@
 
 #include "../../include/mdrt_nb.h"
 #include "nb_context.h"
+#include "nb_spline.cuh"
 
 #define MD_MAX_UNROLL 256  // steps of one replayed graph
 
@@ -57,7 +58,17 @@ struct mdrtMd {
   double *x_ck = nullptr, *v_ck = nullptr, *thermo_ck = nullptr;
   double *xref_ck = nullptr, *xprune_ck = nullptr;  // the reference positions of the lists in force
   int32_t *peak = nullptr, *h_peak = nullptr;
+  double *h_steps = nullptr;       // pinned: the step counter at the checkpoint and after the run
   int64_t regrows = 0;             // runs redone after an overflow inside the graphs
+  int64_t redone = 0;              // stops at a drift past half the skin between two decisions
+  double lookahead = 1.0;          // mdrtMdSetLookahead
+  // PME gathered by the update (order 4): the step's side stream spreads the
+  // frames into qgrid (through qfixed in the deterministic mode) and
+  // transforms qgrid -> spec -> phi; the update gathers each atom's PME force
+  float *qgrid = nullptr, *phi = nullptr;
+  unsigned long long *qfixed = nullptr;
+  float2 *spec = nullptr;
+  int64_t pme_points = 0;          // K0 K1 K2 the buffers were sized for
   double temperature = 300.0, tau = 0.0;
   int64_t ndof = 0;
   unsigned long long seed = 1;
@@ -154,6 +165,19 @@ struct UpdateParams {
   int *flag;  // [0] rebuild, [1] prune (device)
   const double *noise;  // the thermostat's draws of the steps of this launch
   int k;                // this step's index among them
+  // the rebuild is decided ahead, at the last step of each window of steps
+  // (check_build), from the drift and its growth over the window; at the
+  // other steps a drift past half the skin marks the lists stale (status),
+  // and the run is redone
+  int check_build;
+  double lookahead;  // the growth of the last window extrapolated this many times
+  int *status;
+  int32_t *peak;
+  // PME inside the update (order 4): the potential to gather from (0: the
+  // PME forces come in `pme`)
+  int pme_fused;
+  GridParams G;
+  const float *phi;
 };
 
 // The force on atom a: the pair / excluded accumulator of its place and the
@@ -183,14 +207,61 @@ __device__ __forceinline__ Vec3 take_force(int a, const int32_t *__restrict__ pl
   return f;
 }
 
-__device__ __forceinline__ void write_frame(int a, Vec3 x, const int32_t *__restrict__ place_of,
-                                            const char4 *__restrict__ shift, const double *L, float4 *xq) {
+__device__ __forceinline__ float4 write_frame(int a, Vec3 x, const int32_t *__restrict__ place_of,
+                                              const char4 *__restrict__ shift, const double *L, float4 *xq) {
   int p = place_of[a];
-  if (p < 0) return;
+  if (p < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
   char4 s = shift[p];
   float4 o = xq[p];
-  xq[p] = make_float4((float)(x.x + nb_frame_shift(s.x) * L[0]), (float)(x.y + nb_frame_shift(s.y) * L[1]),
-                      (float)(x.z + nb_frame_shift(s.z) * L[2]), o.w);
+  float4 nf = make_float4((float)(x.x + nb_frame_shift(s.x) * L[0]), (float)(x.y + nb_frame_shift(s.y) * L[1]),
+                          (float)(x.z + nb_frame_shift(s.z) * L[2]), o.w);
+  xq[p] = nf;
+  return nf;
+}
+
+// The PME force on the atom at frame fr (charge fr.w), gathered from the
+// potential grid with order-4 B-splines: F = -q sum_k phi(k) grad W(k).
+__device__ __forceinline__ Vec3 md_pme_gather(float4 fr, const float *__restrict__ phi, const GridParams &G) {
+  int k0, k1, k2;
+  float t0, t1, t2;
+  nb_frac(fr.x, G.invL0, G.K0, k0, t0);
+  nb_frac(fr.y, G.invL1, G.K1, k1, t1);
+  nb_frac(fr.z, G.invL2, G.K2, k2, t2);
+  float w0[4], w1[4], w2[4], d0[4], d1[4], d2[4];
+  nb_bspline<4>(t0, w0, d0);
+  nb_bspline<4>(t1, w1, d1);
+  nb_bspline<4>(t2, w2, d2);
+  int gzs[4];
+#pragma unroll
+  for (int jz = 0; jz < 4; ++jz) {
+    int gz = k2 - jz;
+    gzs[jz] = gz < 0 ? gz + G.K2 : gz;
+  }
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+#pragma unroll
+  for (int jx = 0; jx < 4; ++jx) {
+    int gx = k0 - jx;
+    if (gx < 0) gx += G.K0;
+#pragma unroll
+    for (int jy = 0; jy < 4; ++jy) {
+      int gy = k1 - jy;
+      if (gy < 0) gy += G.K1;
+      const float *row = phi + ((int64_t)gx * G.K1 + gy) * G.K2;
+      float sz = 0.f, sdz = 0.f;
+#pragma unroll
+      for (int jz = 0; jz < 4; ++jz) {
+        float f = __ldg(row + gzs[jz]);
+        sz = fmaf(f, w2[jz], sz);
+        sdz = fmaf(f, d2[jz], sdz);
+      }
+      g0 = fmaf(d0[jx] * w1[jy], sz, g0);
+      g1 = fmaf(w0[jx] * d1[jy], sz, g1);
+      g2 = fmaf(w0[jx] * w1[jy], sdz, g2);
+    }
+  }
+  float q = fr.w;
+  return {(double)(-q * g0 * (float)G.K0 * G.invL0), (double)(-q * g1 * (float)G.K1 * G.invL1),
+          (double)(-q * g2 * (float)G.K2 * G.invL2)};
 }
 
 #define MD_UPDATE_THREADS 64
@@ -225,6 +296,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
   __shared__ double s_ke[MD_UPDATE_THREADS / 32];
   __shared__ float s_d2[MD_UPDATE_THREADS / 32], s_p2[MD_UPDATE_THREADS / 32];
   __shared__ int s_last;
+  if (U.flag[3]) return;  // stopped at a stale list: the state stays at that step
   const int WPB = MD_UPDATE_THREADS / 32 * 10;  // waters per block
   int64_t water_blocks = (nwaters + WPB - 1) / WPB;
   double lambda = thermo[0];
@@ -247,6 +319,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     Vec3 f = {0.0, 0.0, 0.0};
     char4 sh = make_char4(0, 0, 0, 0);
     float qw = 0.f;
+    float4 fr = make_float4(0.f, 0.f, 0.f, 0.f);
     if (p >= 0) {
       if (U.fixed) {
         long long fx = (long long)accf[3 * p], fy = (long long)accf[3 * p + 1], fz = (long long)accf[3 * p + 2];
@@ -262,7 +335,14 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
         f.z += w4.z;
       }
       sh = shift[p];
-      qw = xq[p].w;
+      fr = xq[p];
+      qw = fr.w;
+      if (U.pme_fused && qw != 0.f) {
+        Vec3 fg = md_pme_gather(fr, U.phi, U.G);
+        f.x += fg.x;
+        f.y += fg.y;
+        f.z += fg.z;
+      }
     }
     // the excluded pair (k, k+1) of this water
     Vec3 x1 = shfl3(x0, s1);
@@ -300,9 +380,10 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
       store3(v, a, vn);
       store3(fout, a, f);
       if (p >= 0) {
-        xq[p] = make_float4((float)(xn.x + nb_frame_shift(sh.x) * U.L[0]),
-                            (float)(xn.y + nb_frame_shift(sh.y) * U.L[1]),
-                            (float)(xn.z + nb_frame_shift(sh.z) * U.L[2]), qw);
+        float4 nf = make_float4((float)(xn.x + nb_frame_shift(sh.x) * U.L[0]),
+                                (float)(xn.y + nb_frame_shift(sh.y) * U.L[1]),
+                                (float)(xn.z + nb_frame_shift(sh.z) * U.L[2]), qw);
+        xq[p] = nf;
         if (U.fixed) {
           accf[3 * p] = 0ull;
           accf[3 * p + 1] = 0ull;
@@ -323,6 +404,11 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     int64_t t = (int64_t)(blockIdx.x - water_blocks) * blockDim.x + threadIdx.x;
     int i = free_atoms[t];
     Vec3 fi = take_force(i, place_of, acc, accf, pme, U.fixed);
+    int pi = place_of[i];
+    if (U.pme_fused && pi >= 0) {
+      float4 fr = xq[pi];
+      if (fr.w != 0.f) fi = fi + md_pme_gather(fr, U.phi, U.G);
+    }
     Vec3 vi = lambda * load3(v, i) + (dt * inv_mass[i]) * fi;
     Vec3 xi = load3(x, i) + dt * vi;
     store3(x, i, xi);
@@ -447,22 +533,37 @@ __device__ void md_last_block(const UpdateParams &U, const double *ke_part, int 
   thermo[0] = lambda;
   float d2 = __uint_as_float(atomicAdd(maxd2, 0u));
   float p2 = __uint_as_float(atomicAdd(maxd2 + 1, 0u));
-  int rebuild = (double)d2 > U.build_half2 ? 1 : 0;
+  int stale = (double)d2 > U.build_half2 ? 1 : 0;
+  int rebuild = 0;
+  if (U.check_build) {
+    // the drift the lists may reach before the next decision: its growth
+    // over the window just ended, once more (thermo[6] holds the drift at
+    // the last decision, 0 after a build; the largest drift grows slower
+    // than the first, ballistic, window); a wrong guess is caught by the test
+    // of every step and costs a redo, not a missed pair
+    double d = sqrt((double)d2);
+    double ahead = d + U.lookahead * fmax(d - thermo[6], 0.0) + 0.002;
+    rebuild = (stale || ahead * ahead > U.build_half2) ? 1 : 0;
+    thermo[6] = d;
+    stale = 0;
+  }
+  if (stale && U.use_graph) {
+    // the lists of the next step are not sure: the steps after this one do
+    // nothing (flag[3]), and the host rebuilds here and runs the rest
+    atomicOr(U.status, NB_STATUS_STALE_LIST);
+    atomicAdd(&U.peak[3], 1);
+    U.flag[3] = 1;
+  }
   int prune = (U.prune_half2 > 0.0 && (rebuild || (double)p2 > U.prune_half2)) ? 1 : 0;
+  // the host's build after a stale list (or, step by step, after a rebuild) prunes too
+  if (stale || (!U.use_graph && rebuild)) prune = 0;
   maxd2[0] = 0u;
   maxd2[1] = 0u;
   maxd2[2] = 0u;
   U.flag[0] = rebuild;
   U.flag[1] = prune;
-  if (U.use_graph) cudaGraphSetConditional(U.h_any, rebuild | prune);
-}
-
-// The first node of the body of a step's conditional node: which of the
-// rebuild and the pruning it runs.
-__global__ void md_set_inner(const int *flag, cudaGraphConditionalHandle h_build, cudaGraphConditionalHandle h_prune,
-                             int dual) {
-  cudaGraphSetConditional(h_build, flag[0]);
-  if (dual) cudaGraphSetConditional(h_prune, flag[1]);
+  U.flag[2] = stale;
+  if (U.use_graph && U.check_build) cudaGraphSetConditional(U.h_any, rebuild);
 }
 
 // After a build: the reference positions, the counters, and what the build
@@ -474,6 +575,7 @@ __global__ void md_after_build(int64_t n3, const double *__restrict__ x, double 
   if (k < n3) x_ref[k] = x[k];
   if (k == 0) {
     thermo[4] += 1.0;
+    thermo[6] = 0.0;  // the drift at the last rebuild decision
     atomicMax(&peak[0], sizes[NB_SIZE_LONGEST]);
     if (sizes[NB_SIZE_OVERFLOW] != 0) {
       atomicOr(status, NB_STATUS_LIST_OVERFLOW);
@@ -513,15 +615,20 @@ static SettleParams settle_params(const mdrtMd &m) {
 
 // One step on `s` from the frames xq of the current positions x.
 static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], double dt, cudaStream_t s,
-                         cudaGraphConditionalHandle h_any, int use_graph, int *flag, int k) {
+                         cudaGraphConditionalHandle h_any, int use_graph, int *flag, int k, int check_build,
+                         int window) {
   NbCtx &c = *m.nb;
   bool pme = c.pme.on && c.beta > 0.0;
+  bool fused = pme && m.qgrid != nullptr;
   if (pme) {
     cudaEventRecord(m.ev_fork, s);
     cudaStreamWaitEvent(m.side, m.ev_fork, 0);
-    nb_pme_run(c, box, false, false, m.side);
+    if (fused)
+      nb_pme_md_chain(c, box, m.qgrid, m.qfixed, m.spec, m.phi, m.side);
+    else
+      nb_pme_run(c, box, false, false, m.side);
   }
-  nb_pairs_run(c, box, false, s);
+  nb_pairs_run(c, box, false, s, flag + 3);
   if (m.n_excl_other > 0) nb_excluded_list_run(c, box, m.excl_other, m.n_excl_other, s);
   if (pme) {
     cudaEventRecord(m.ev_join, m.side);
@@ -548,10 +655,22 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
   U.h_any = h_any;
   U.use_graph = use_graph;
   U.flag = flag;
+  U.check_build = check_build;
+  U.lookahead = m.lookahead;
+  U.status = c.status;
+  U.peak = m.peak;
+  U.pme_fused = fused ? 1 : 0;
+  U.G.K0 = c.pme.K[0];
+  U.G.K1 = c.pme.K[1];
+  U.G.K2 = c.pme.K[2];
+  U.G.invL0 = (float)(1.0 / box[0]);
+  U.G.invL1 = (float)(1.0 / box[1]);
+  U.G.invL2 = (float)(1.0 / box[2]);
+  U.phi = m.phi;
   md_update<<<m.ke_blocks, MD_UPDATE_THREADS, 0, s>>>(
       m.nwaters, m.nfree, m.waters, m.free_atoms, U, m.inv_mass, m.mass, c.q, c.place_of, c.shift, c.acc,
-      c.acc_fixed, pme ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref, m.x_prune,
-      m.thermo, m.ke_part, m.maxd2);
+      c.acc_fixed, (pme && !fused) ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref,
+      m.x_prune, m.thermo, m.ke_part, m.maxd2);
 }
 
 // A pruning at x on `s` (frames current): the inner lists and their units.
@@ -559,6 +678,13 @@ static void md_prune_body(mdrtMd &m, const double *x, const double box[3], cudaS
   NbCtx &c = *m.nb;
   nb_prune_run(c, box, s);
   md_after_prune<<<blocks_for(3 * m.n, 256), 256, 0, s>>>(3 * m.n, x, m.x_prune, m.thermo);
+}
+
+// The pruning of a step when the update asked for it (flag[1], on the
+// device): two launches that do nothing otherwise, no conditional node.
+static void md_prune_step(mdrtMd &m, const double *x, const double box[3], cudaStream_t s) {
+  NbCtx &c = *m.nb;
+  if (c.inner_reach > 0.0) nb_prune_gated(c, box, m.flag + 1, x, m.x_prune, m.thermo + 5, s);
 }
 
 // A build at x on `s` without a host wait (the body of the conditional node).
@@ -577,6 +703,31 @@ static void md_drop_graph(mdrtMd *m) {
   m->graph = nullptr;
 }
 
+// The integrator's PME buffers when the update gathers (order 4 with a
+// reciprocal sum), sized for the context's grid; none otherwise.
+static int md_pme_buffers(mdrtMd *m) {
+  NbCtx &c = *m->nb;
+  bool want = c.pme.on && c.beta > 0.0 && c.pme.order == 4;
+  int64_t pts = want ? (int64_t)c.pme.K[0] * c.pme.K[1] * c.pme.K[2] : 0;
+  if (pts == m->pme_points) return 0;
+  for (void **p : {(void **)&m->qgrid, (void **)&m->phi, (void **)&m->qfixed, (void **)&m->spec}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  m->pme_points = 0;
+  if (!want) return 0;
+  int64_t half = (int64_t)c.pme.K[0] * c.pme.K[1] * (c.pme.K[2] / 2 + 1);
+  if (cudaMalloc(&m->qgrid, sizeof(float) * pts) != cudaSuccess ||
+      cudaMalloc(&m->phi, sizeof(float) * pts) != cudaSuccess ||
+      cudaMalloc(&m->qfixed, sizeof(unsigned long long) * pts) != cudaSuccess ||
+      cudaMalloc(&m->spec, sizeof(float2) * half) != cudaSuccess)
+    return -1;
+  // the fixed-point grid starts empty; each step's conversion empties it again
+  if (cudaMemset(m->qfixed, 0, sizeof(unsigned long long) * pts) != cudaSuccess) return -1;
+  m->pme_points = pts;
+  return 0;
+}
+
 static void md_free(mdrtMd *m) {
   if (!m) return;
   md_drop_graph(m);
@@ -587,9 +738,11 @@ static void md_free(mdrtMd *m) {
                   (void *)m->excl_other, (void *)m->force, (void *)m->x_ref, (void *)m->x_prune,
                   (void *)m->ke_part, (void *)m->maxd2, (void *)m->thermo, (void *)m->flag,
                   (void *)m->noise, (void *)m->x_ck, (void *)m->v_ck, (void *)m->thermo_ck, (void *)m->peak,
-                  (void *)m->xref_ck, (void *)m->xprune_ck})
+                  (void *)m->xref_ck, (void *)m->xprune_ck, (void *)m->qgrid, (void *)m->phi, (void *)m->qfixed,
+                  (void *)m->spec})
     if (p) cudaFree(p);
   if (m->h_peak) cudaFreeHost(m->h_peak);
+  if (m->h_steps) cudaFreeHost(m->h_steps);
   delete m;
 }
 
@@ -682,7 +835,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
             cudaMalloc(&m->maxd2, sizeof(unsigned int) * 4) == cudaSuccess &&
             cudaMalloc(&m->thermo, sizeof(double) * 8) == cudaSuccess &&
             cudaMalloc(&m->noise, sizeof(double) * 2 * MD_MAX_UNROLL) == cudaSuccess &&
-            cudaMalloc(&m->flag, sizeof(int) * 2) == cudaSuccess &&
+            cudaMalloc(&m->flag, sizeof(int) * 4) == cudaSuccess &&
             cudaMalloc(&m->x_ck, sizeof(double) * 3 * c.n) == cudaSuccess &&
             cudaMalloc(&m->v_ck, sizeof(double) * 3 * c.n) == cudaSuccess &&
             cudaMalloc(&m->thermo_ck, sizeof(double) * 8) == cudaSuccess &&
@@ -690,6 +843,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
             cudaMalloc(&m->xprune_ck, sizeof(double) * 3 * c.n) == cudaSuccess &&
             cudaMalloc(&m->peak, sizeof(int32_t) * 4) == cudaSuccess &&
             cudaMallocHost(&m->h_peak, sizeof(int32_t) * 4) == cudaSuccess &&
+            cudaMallocHost(&m->h_steps, sizeof(double) * 2) == cudaSuccess &&
             cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, hi) == cudaSuccess &&
             cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming) == cudaSuccess;
@@ -707,6 +861,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
   cudaMemcpy(m->thermo, th, sizeof(th), cudaMemcpyHostToDevice);
   cudaMemset(m->maxd2, 0, sizeof(unsigned int) * 4);
   cudaMemset(m->peak, 0, sizeof(int32_t) * 4);
+  cudaMemset(m->flag, 0, sizeof(int) * 4);
   cudaMemset(m->force, 0, sizeof(double) * 3 * c.n);
   *out = m;
   return MDRT_NB_OK;
@@ -717,6 +872,13 @@ int32_t mdrtMdDestroy(mdrtMd *m) {
     cudaSetDevice(m->device);
     md_free(m);
   }
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtMdSetLookahead(mdrtMd *m, double factor) {
+  if (!m || !(factor >= 0.0) || !(factor <= 100.0)) return MDRT_NB_INVALID_ARGUMENT;
+  m->lookahead = factor;
+  md_drop_graph(m);  // parameters are baked into the graph
   return MDRT_NB_OK;
 }
 
@@ -746,6 +908,7 @@ int32_t mdrtMdBuild(mdrtMd *m, const double *x, const double box[3], void *strea
   if (sizes[NB_SIZE_LONGEST] > NB_GROW_AHEAD * c.list_cap && nb_grow_lists_keep(c, sizes[NB_SIZE_LONGEST], st))
     return MDRT_NB_CUDA_ERROR;
   nb_gather_frames(c, x, box, st);
+  if (md_pme_buffers(m)) return MDRT_NB_CUDA_ERROR;
   md_after_build<<<blocks_for(3 * m->n, 256), 256, 0, st>>>(3 * m->n, x, m->x_ref, m->thermo, c.sizes, c.status,
                                                             m->peak);
   if (c.inner_reach > 0.0) {
@@ -785,56 +948,102 @@ static cudaError_t md_capture_if(cudaStream_t cap, cudaStream_t body, cudaGraphC
   return cudaStreamEndCapture(body, nullptr);
 }
 
-// The graph of `unroll` steps, each ending in a conditional rebuild,
-// captured again when its arguments or the capacities changed.
+// Steps between the rebuild decisions of the step-by-step path by default
+// (the graph path decides at the end of each graph, every `unroll` steps).
+#define MD_WINDOW 10
+
+// Step by step, the host reading the flags after each step: a rebuild
+// decided ahead at the end of each window of MD_WINDOW steps, or forced by
+// a drift past half the skin; the pruning is decided on the device.
+static int32_t md_run_steps(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
+                            int window, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  int h_flag[3] = {0, 0, 0};
+  int64_t kw = 0;  // the step in the window; a forced rebuild starts a new window, as in the graphs
+  for (int64_t k = 0; k < steps; ++k) {
+    md_noise<<<1, 32, 0, st>>>(m->thermo, m->noise, 1, (double)m->ndof, m->seed);
+    int check = (kw + 1) % window == 0 ? 1 : 0;
+    md_step_body(*m, x, v, box, dt, st, 0, 0, m->flag, 0, check, window);
+    md_prune_step(*m, x, box, st);
+    cudaMemcpyAsync(h_flag, m->flag, sizeof(h_flag), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
+    ++kw;
+    if (h_flag[0] || h_flag[2]) {
+      int32_t s = mdrtMdBuild(m, x, box, stream);
+      if (s) return s;
+      if (h_flag[2]) {
+        kw = 0;
+        m->redone++;
+      }
+    }
+  }
+  return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
+}
+
+// Back to the checkpoint of a run: positions, velocities, the lists built
+// and pruned where those in force were (no host build of its own: the
+// capacities are the caller's), the frames, the thermostat state.
+static int32_t md_restore(mdrtMd *m, double *x, double *v, const double box[3], bool dual, void *stream) {
+  NbCtx &c = *m->nb;
+  cudaStream_t st = (cudaStream_t)stream;
+  size_t bytes = sizeof(double) * 3 * m->n;
+  if (cudaMemcpyAsync(x, m->x_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(v, m->v_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MDRT_NB_CUDA_ERROR;
+  int32_t s = mdrtNbBuild(m->handle, m->xref_ck, m->n, box, 0.0, stream, nullptr);
+  if (s) return s;
+  if (cudaMemcpyAsync(m->x_ref, m->xref_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MDRT_NB_CUDA_ERROR;
+  if (dual) {
+    nb_gather_frames(c, m->xprune_ck, box, st);
+    md_prune_body(*m, m->xprune_ck, box, st);
+    c.inner_valid = true;
+  }
+  nb_gather_frames(c, x, box, st);
+  // the counters of the checkpoint: the build and pruning above redo ones it had
+  if (cudaMemcpyAsync(m->thermo, m->thermo_ck, sizeof(double) * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MDRT_NB_CUDA_ERROR;
+  return MDRT_NB_OK;
+}
+
+// The graph of `unroll` steps (gated prunings, one conditional rebuild at
+// the end), captured again when its arguments or the capacities changed.
 static int32_t md_prepare_graph(mdrtMd *m, double *x, double *v, const double box[3], double dt, int32_t unroll) {
   NbCtx &c = *m->nb;
   int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap + (int64_t)(c.inner_reach * 1e9) +
                 (c.inner_valid ? 1 : 0) + (c.deterministic ? 2 : 0) + ((int64_t)c.pair_blocks_per_sm << 40) +
-                ((int64_t)c.pair_sms << 44);
+                ((int64_t)c.pair_sms << 44) + (int64_t)(uintptr_t)m->qgrid;
   bool stale = !m->exec || m->gx != x || m->gv != v || m->gdt != dt || m->gunroll != unroll ||
                m->gbox[0] != box[0] || m->gbox[1] != box[1] || m->gbox[2] != box[2] || m->gcap_key != key;
   if (stale) {
     md_drop_graph(m);
-    // Each step ends in one conditional node, taken when a rebuild or a
-    // pruning is due (about one step in three); its body sets and runs two
-    // nested ones, the rebuild and the pruning.
-    cudaStream_t cap, body, inner;
+    // A window of `unroll` steps: each step prunes when its update asks
+    // (gated launches, no conditional node), and the last step decides the
+    // rebuild for the window ahead in the graph's one conditional node (an
+    // untaken conditional node costs about as much as a short kernel chain,
+    // so there is one per window, not one per step).
+    cudaStream_t cap, body;
     cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
     cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking);
-    cudaStreamCreateWithFlags(&inner, cudaStreamNonBlocking);
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-    bool dual = c.inner_reach > 0.0;
-    m->handles.assign(unroll, 0);
+    m->handles.assign(1, 0);
     if (e == cudaSuccess)
       md_noise<<<(unroll + 31) / 32, 32, 0, cap>>>(m->thermo, m->noise, unroll, (double)m->ndof, m->seed);
     for (int k = 0; k < unroll && e == cudaSuccess; ++k) {
-      cudaStreamCaptureStatus status;
-      cudaGraph_t g;
-      e = cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, nullptr, nullptr);
-      if (e != cudaSuccess) break;
-      e = cudaGraphConditionalHandleCreate(&m->handles[k], g, 0, cudaGraphCondAssignDefault);
-      if (e != cudaSuccess) break;
-      md_step_body(*m, x, v, box, dt, cap, m->handles[k], 1, m->flag, k);
-      cudaError_t ei = cudaSuccess;
-      e = md_capture_if(cap, body, m->handles[k], [&](cudaStream_t b) {
-        cudaStreamCaptureStatus bs;
-        cudaGraph_t bg;
-        cudaGraphConditionalHandle hb = 0, hp = 0;
-        ei = cudaStreamGetCaptureInfo(b, &bs, nullptr, &bg, nullptr, nullptr);
-        if (ei == cudaSuccess) ei = cudaGraphConditionalHandleCreate(&hb, bg, 0, cudaGraphCondAssignDefault);
-        if (ei == cudaSuccess && dual) ei = cudaGraphConditionalHandleCreate(&hp, bg, 0, cudaGraphCondAssignDefault);
-        if (ei != cudaSuccess) return;
-        md_set_inner<<<1, 1, 0, b>>>(m->flag, hb, hp, dual ? 1 : 0);
-        ei = md_capture_if(b, inner, hb, [&](cudaStream_t ib) { md_rebuild_body(*m, x, box, ib); });
-        if (ei == cudaSuccess && dual)
-          ei = md_capture_if(b, inner, hp, [&](cudaStream_t ib) { md_prune_body(*m, x, box, ib); });
-      });
-      if (e == cudaSuccess) e = ei;
+      bool last = k == unroll - 1;
+      if (last) {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t g;
+        e = cudaStreamGetCaptureInfo(cap, &status, nullptr, &g, nullptr, nullptr);
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&m->handles[0], g, 0, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) break;
+      }
+      md_step_body(*m, x, v, box, dt, cap, m->handles[0], 1, m->flag, k, last ? 1 : 0, unroll);
+      if (last) e = md_capture_if(cap, body, m->handles[0], [&](cudaStream_t b) { md_rebuild_body(*m, x, box, b); });
+      if (e == cudaSuccess) md_prune_step(*m, x, box, cap);
     }
     cudaGraph_t graph = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
-    cudaStreamDestroy(inner);
     cudaStreamDestroy(body);
     cudaStreamDestroy(cap);
     if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -864,44 +1073,30 @@ extern "C" {
 
 int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
                   int32_t unroll, void *stream) {
-  if (!m || !x || !v || !box || !(dt > 0) || steps < 0 || unroll > MD_MAX_UNROLL) return MDRT_NB_INVALID_ARGUMENT;
+  if (!m || !x || !v || !box || !(dt > 0) || steps < 0 || unroll > MD_MAX_UNROLL || unroll < -MD_MAX_UNROLL)
+    return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = *m->nb;
   if (!c.built) return MDRT_NB_NOT_BUILT;
   for (int k = 0; k < 3; ++k)
     if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;
   cudaSetDevice(c.device);
   cudaStream_t st = (cudaStream_t)stream;
-  if (unroll <= 0) {
-    // step by step, the host reading the tests of validity after each step
-    int h_flag[2] = {0, 0};
-    for (int64_t k = 0; k < steps; ++k) {
-      md_noise<<<1, 32, 0, st>>>(m->thermo, m->noise, 1, (double)m->ndof, m->seed);
-      md_step_body(*m, x, v, box, dt, st, 0, 0, m->flag, 0);
-      cudaMemcpyAsync(h_flag, m->flag, sizeof(h_flag), cudaMemcpyDeviceToHost, st);
-      cudaStreamSynchronize(st);
-      if (h_flag[0]) {
-        int32_t s = mdrtMdBuild(m, x, box, stream);
-        if (s) return s;
-      } else if (h_flag[1]) {
-        md_prune_body(*m, x, box, st);
-        c.prunes++;
-      }
-    }
-    return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
-  }
-  // Runs of step graphs.  A rebuild inside a graph that overflows a list
-  // leaves the following steps with incomplete lists, so each run starts
-  // from a checkpoint (positions, velocities, thermostat state, and the
-  // positions the lists in force were built and pruned at) and ends in one
-  // read of what its builds saw.  After an overflow the run goes back to the
-  // checkpoint, grows the lists to the longest count (+25%), builds and
-  // prunes them again where they were built and pruned (the same lists and
-  // the same schedule of rebuilds, with room), and runs again.  Positions
+  if (unroll <= 0) return md_run_steps(m, x, v, box, dt, steps, unroll < 0 ? -unroll : MD_WINDOW, stream);
+  // Runs of step graphs.  Each run starts from a checkpoint (positions,
+  // velocities, thermostat state, and the positions the lists in force were
+  // built and pruned at) and ends in one read of what its steps saw.  A
+  // rebuild inside a graph that overflowed a list: back to the checkpoint,
+  // the lists grown to the longest count (+25%), built and pruned again
+  // where they were (the same lists and schedule, with room), and the run
+  // again.  A drift past half the skin between two rebuild decisions (the
+  // decision looks ahead, so this is rare): the steps after it did nothing,
+  // so the host rebuilds at that step and runs the steps left.  Positions
   // that are not finite end the run.
-  int64_t launches = steps / unroll;
   size_t bytes = sizeof(double) * 3 * m->n;
   bool dual = c.inner_reach > 0.0 && c.inner_valid;
-  for (int attempt = 0; launches > 0; ++attempt) {
+  int64_t left = steps;
+  for (int attempt = 0; left >= unroll;) {
+    int64_t launches = left / unroll;
     int32_t s = md_prepare_graph(m, x, v, box, dt, unroll);
     if (s) return s;
     if (cudaMemcpyAsync(m->x_ck, x, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
@@ -914,38 +1109,38 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
     for (int64_t k = 0; k < launches; ++k)
       if (cudaGraphLaunch(m->exec, st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
     if (cudaMemcpyAsync(m->h_peak, m->peak, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(m->h_steps, m->thermo_ck + 3, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(m->h_steps + 1, m->thermo + 3, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
       return MDRT_NB_CUDA_ERROR;
     if (m->h_peak[2] > 0) return MDRT_NB_NAN_POSITION;
-    if (m->h_peak[1] == 0) {
-      // lists near their capacity grow ahead, keeping those in force
-      if (m->h_peak[0] > NB_GROW_AHEAD * c.list_cap && nb_grow_lists_keep(c, m->h_peak[0], st))
-        return MDRT_NB_CUDA_ERROR;
-      break;
+    if (m->h_peak[1] != 0) {
+      if (++attempt > 8) return MDRT_NB_GROW;
+      md_clear_status<<<1, 1, 0, st>>>(c.status, NB_STATUS_LIST_OVERFLOW | NB_STATUS_STALE_LIST);
+      if (cudaMemsetAsync(m->flag + 3, 0, sizeof(int), st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
+      if (nb_grow_lists(c, m->h_peak[0])) return MDRT_NB_CUDA_ERROR;
+      s = md_restore(m, x, v, box, dual, stream);
+      if (s) return s;
+      m->regrows++;
+      continue;
     }
-    if (attempt >= 8) return MDRT_NB_GROW;
-    if (cudaMemcpyAsync(x, m->x_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(v, m->v_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-      return MDRT_NB_CUDA_ERROR;
-    md_clear_status<<<1, 1, 0, st>>>(c.status, NB_STATUS_LIST_OVERFLOW);
-    if (nb_grow_lists(c, m->h_peak[0])) return MDRT_NB_CUDA_ERROR;
-    s = mdrtNbBuild(m->handle, m->xref_ck, m->n, box, 0.0, stream, nullptr);
-    if (s) return s;
-    if (cudaMemcpyAsync(m->x_ref, m->xref_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-      return MDRT_NB_CUDA_ERROR;
-    if (dual) {
-      nb_gather_frames(c, m->xprune_ck, box, st);
-      md_prune_body(*m, m->xprune_ck, box, st);
-      c.inner_valid = true;
+    if (m->h_peak[3] != 0) {
+      // stopped at a stale list: rebuild there and go on with the steps left
+      int64_t done = (int64_t)(m->h_steps[1] - m->h_steps[0]);
+      md_clear_status<<<1, 1, 0, st>>>(c.status, NB_STATUS_STALE_LIST);
+      if (cudaMemsetAsync(m->flag + 3, 0, sizeof(int), st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
+      s = mdrtMdBuild(m, x, box, stream);
+      if (s) return s;
+      m->redone++;
+      left -= done;
+      continue;
     }
-    nb_gather_frames(c, x, box, st);
-    // the counters of the checkpoint: the build and pruning above redo ones it had
-    if (cudaMemcpyAsync(m->thermo, m->thermo_ck, sizeof(double) * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    // lists near their capacity grow ahead, keeping those in force
+    if (m->h_peak[0] > NB_GROW_AHEAD * c.list_cap && nb_grow_lists_keep(c, m->h_peak[0], st))
       return MDRT_NB_CUDA_ERROR;
-    m->regrows++;
+    left -= launches * unroll;
   }
-  int64_t rest = steps - launches * unroll;
-  if (rest > 0) return mdrtMdRun(m, x, v, box, dt, rest, 0, stream);
+  if (left > 0) return md_run_steps(m, x, v, box, dt, left, unroll, stream);
   return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
 }
 
@@ -961,6 +1156,7 @@ int32_t mdrtMdThermo(mdrtMd *m, void *stream, double *out) {
   out[5] = (double)m->ndof;
   out[6] = h[5];
   out[7] = (double)m->regrows;
+  out[8] = (double)m->redone;
   return MDRT_NB_OK;
 }
 

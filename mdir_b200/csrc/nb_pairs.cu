@@ -85,7 +85,9 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
                                                 const int32_t *__restrict__ typ,
                                                 const float2 *__restrict__ lj, const float2 *__restrict__ ljf,
                                                 float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
-                                                double *__restrict__ partials, int *__restrict__ status) {
+                                                double *__restrict__ partials, int *__restrict__ status,
+                                                const int *halt) {
+  if (halt && *halt) return;  // the MD step stopped at a stale list (its host rebuilds)
   __shared__ float4 s_x[8][2 * NB_GROUP];
   __shared__ float2 s_f[8][2 * NB_GROUP];  // LJM 1: member factors
   __shared__ int s_t[8][2 * NB_GROUP];     // LJM 0: member row offsets in s_lj
@@ -776,7 +778,7 @@ void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream
                                                           c.typ_p);
 }
 
-void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
+void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt) {
   ensure_sm_count();
   PairParams P = pair_params(c, box);
   // persistent grid: enough warps for the units, `pair_blocks_per_sm`
@@ -794,7 +796,7 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s) {
   const int32_t *lcounts = inner ? c.counts_in : c.counts;
 #define NB_LAUNCH2(E, F, S, M)                                                                         \
   nb_pairs<E, F, S, M><<<grid, 256, 0, s>>>(P, nullptr, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, \
-                                           c.ljf, c.acc, c.acc_fixed, c.unit_partials, c.status)
+                                           c.ljf, c.acc, c.acc_fixed, c.unit_partials, c.status, halt)
 #define NB_LAUNCH(E, F, S)      \
   do {                          \
     if (c.lj_geom)              \
@@ -941,7 +943,7 @@ void nb_batch_pairs_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
 #define NB_BATCH_LAUNCH(E, M)                                                                                \
   nb_pairs<E, false, false, M, true><<<grid, 256, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq, \
                                                          c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed, c.unit_partials, \
-                                                         c.status)
+                                                         c.status, nullptr)
   if (energy) {
     if (c.lj_geom) NB_BATCH_LAUNCH(true, 1); else NB_BATCH_LAUNCH(true, 0);
   } else {

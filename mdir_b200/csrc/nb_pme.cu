@@ -23,64 +23,11 @@
 #include <vector>
 
 #include "nb_context.h"
+#include "nb_spline.cuh"
 
 namespace {
 
-// w[j] = M_p(t + j), dw[j] its slope, j = 0..p-1; weight j belongs to grid
-// point floor(u) - j.  M_n(x) = (x M_{n-1}(x) + (n - x) M_{n-1}(x - 1))/(n - 1).
-template <int P>
-__device__ __forceinline__ void nb_bspline(float t, float *w, float *dw) {
-  float a[P];
-  a[0] = t;
-  a[1] = 1.f - t;
-#pragma unroll
-  for (int j = 2; j < P; ++j) a[j] = 0.f;
-#pragma unroll
-  for (int m = 3; m <= P; ++m) {
-    float prev[P];
-#pragma unroll
-    for (int j = 0; j < P; ++j) prev[j] = a[j];
-    if (m == P && dw) {
-#pragma unroll
-      for (int j = 0; j < P; ++j) dw[j] = (j < m - 1 ? prev[j] : 0.f) - (j > 0 ? prev[j - 1] : 0.f);
-    }
-    float inv = 1.f / (float)(m - 1);
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-      if (j < m) {
-        float left = j < m - 1 ? prev[j] : 0.f;
-        float right = j > 0 ? prev[j - 1] : 0.f;
-        a[j] = ((t + j) * left + ((float)m - t - j) * right) * inv;
-      }
-    }
-  }
-  if (P == 2 && dw) {
-    dw[0] = 1.f;
-    dw[1] = -1.f;
-  }
-#pragma unroll
-  for (int j = 0; j < P; ++j) w[j] = a[j];
-}
 
-// The grid point and fraction of a frame coordinate x (centred on the
-// cell: the fractional coordinate is x / L + 1/2).
-__device__ __forceinline__ void nb_frac(float x, float invL, int K, int &k0, float &t) {
-  float f = fmaf(x, invL, 0.5f);
-  f -= floorf(f);
-  float u = f * (float)K;
-  float fl = floorf(u);
-  int k = (int)fl;
-  if (k >= K) k -= K;
-  if (k < 0) k += K;
-  k0 = k;
-  t = u - fl;
-  if (t >= 1.f) t = 0.f;
-}
-
-struct GridParams {
-  int K0, K1, K2;
-  float invL0, invL1, invL2;
-};
 
 template <int P, bool FIXED>
 __global__ void __launch_bounds__(256) nb_spread(GridParams G, int64_t places,
@@ -990,5 +937,53 @@ int nb_batch_pme_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
   else
     nb_batch_gather_split<8><<<blocks_for(c.places_cap * 8, 128), 128, 0, s>>>(
         c.places_cap, c.sizes, c.order, b.atom_frame, b.frames_dev, c.xq, P.grid, pf);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// The reciprocal chain of the MD step when the update gathers (order 4): the
+// integrator owns a charge grid (and its fixed-point form), a spectrum and a
+// potential grid, so that force calls between runs leave them alone; the
+// chain spreads the step's frames, transforms and applies the influence
+// function, and the update gathers each atom's PME force from the potential.
+
+int nb_pme_md_chain(NbCtx &c, const double box[3], float *qgrid, unsigned long long *qfixed, float2 *spec,
+                    float *phi, cudaStream_t s) {
+  NbPme &P = c.pme;
+  GridParams G;
+  G.K0 = P.K[0];
+  G.K1 = P.K[1];
+  G.K2 = P.K[2];
+  G.invL0 = (float)(1.0 / box[0]);
+  G.invL1 = (float)(1.0 / box[1]);
+  G.invL2 = (float)(1.0 / box[2]);
+  int64_t total = (int64_t)G.K0 * G.K1 * G.K2;
+  int64_t half = (int64_t)G.K0 * G.K1 * (G.K2 / 2 + 1);
+  int64_t threads = c.places_cap * 4;
+  if (c.deterministic) {
+    // the fixed-point grid is empty: its conversion empties it
+    nb_spread<4, true><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, qgrid,
+                                                                qfixed);
+    nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, qfixed, qgrid);
+  } else {
+    cudaMemsetAsync(qgrid, 0, sizeof(float) * total, s);
+    nb_spread<4, false><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, qgrid,
+                                                                 qfixed);
+  }
+  cufftSetStream(P.fwd, s);
+  cufftSetStream(P.bwd, s);
+  if (cufftExecR2C(P.fwd, qgrid, (cufftComplex *)spec) != CUFFT_SUCCESS) return -3;
+  ConvParams C;
+  C.K0 = G.K0;
+  C.K1 = G.K1;
+  C.K2 = G.K2;
+  C.H2 = G.K2 / 2 + 1;
+  C.L0 = box[0];
+  C.L1 = box[1];
+  C.L2 = box[2];
+  C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
+  C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
+  nb_convolve<false><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, spec, P.partials);
+  if (cufftExecC2R(P.bwd, (cufftComplex *)spec, phi) != CUFFT_SUCCESS) return -3;
   return 0;
 }

@@ -44,6 +44,10 @@ class Integrator:
     def thermostat(self, temperature, tau, seed=1):
         L.check(L.lib().mdrtMdSetThermostat(self._h, temperature, tau, seed), "mdrtMdSetThermostat")
 
+    def lookahead(self, factor):
+        """The rebuild decision's extrapolation of the drift (default 1)."""
+        L.check(L.lib().mdrtMdSetLookahead(self._h, float(factor)), "mdrtMdSetLookahead")
+
     def build(self, x, box, stream=None):
         b = _host(box, np.float64)
         self.term.box = b
@@ -55,11 +59,11 @@ class Integrator:
                 "mdrtMdRun")
 
     def thermo(self, stream=None):
-        out = np.zeros(8)
+        out = np.zeros(9)
         L.check(L.lib().mdrtMdThermo(self._h, _stream(stream), _hp(out)), "mdrtMdThermo")
         return {"lambda": out[0], "kinetic_half": out[1], "kinetic_half_before": out[2],
                 "steps": int(out[3]), "builds": int(out[4]), "ndof": int(out[5]), "prunes": int(out[6]),
-                "regrows": int(out[7]),
+                "regrows": int(out[7]), "redone": int(out[8]),
                 "kinetic": 0.5 * (out[1] + out[2])}
 
     def forces(self):
@@ -67,7 +71,7 @@ class Integrator:
         L.check(L.lib().mdrtMdForces(self._h, ctypes.byref(p)), "mdrtMdForces")
         return p.value
 
-    def tune(self, x, v, box, dt, reaches=(1.2, 1.3, 1.4, 1.5), pruned=(1.0, 1.025), pair_sms=(0, 128),
+    def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(1.025, 1.05), pair_sms=(0, 128),
              steps=200, reps=3, stream=None):
         """The autotuner of the step: times `reps` runs of `steps` steps for
         every outer reach, pruned reach and span of the pair grid (SMs; the

@@ -140,7 +140,7 @@ def test_lists_that_outgrow_their_capacity_inside_the_graphs_are_redone(cuda):
     the first build, and a rebuild inside the step graphs overflows.  The
     run goes back to its checkpoint with grown lists; the result is the
     step-by-step run's, bit for bit (deterministic mode)."""
-    s = systems.argon(length=5.57)
+    s = systems.argon(length=5.57, skin=0.4)  # a wide skin: no stops at stale lists
     L = s["box"][0]
     v0 = -1.5 * (s["positions"] - 0.5 * L)
 
@@ -152,6 +152,7 @@ def test_lists_that_outgrow_their_capacity_inside_the_graphs_are_redone(cuda):
         t.set_deterministic(True)
         md = Integrator(t, s["masses"], None)
         md.thermostat(120.0, 0.0, 1)
+        md.lookahead(100.0)  # a rebuild at the end of every window: the growth comes inside the graphs
         x = torch.tensor(s["positions"], dtype=torch.float64, device="cuda")
         v = torch.tensor(v0, dtype=torch.float64, device="cuda")
         md.build(x, s["box"])
@@ -159,11 +160,31 @@ def test_lists_that_outgrow_their_capacity_inside_the_graphs_are_redone(cuda):
         md.run(x, v, s["box"], 0.002, 150, unroll=unroll)
         return t, md, x, v, cap0
 
-    t1, md1, x1, v1, cap0 = run(10)
+    t1, md1, x1, v1, cap0 = run(5)
     th = md1.thermo()
     assert th["regrows"] >= 1
     assert t1.info()["list_capacity"] > cap0
     assert t1.status() & 1 == 0  # no overflow left behind
-    t2, md2, x2, v2, _ = run(0)
+    t2, md2, x2, v2, _ = run(-5)
     assert md2.thermo()["builds"] == th["builds"]
+    assert torch.equal(x1, x2) and torch.equal(v1, v2)
+
+
+def test_stops_at_a_stale_list_equal_the_host_rebuilding_at_once(cuda):
+    """With no look-ahead (factor 0) the drift passes half the skin inside
+    windows again and again: the graphs stop at that step and the host
+    rebuilds there, which must give the step-by-step run (the host testing
+    every step) bit for bit, a stale list never used."""
+    s = systems.tip3p(waters=500, seed=28)
+    s["reach"] = 1.0
+    runs = []
+    for unroll in (10, 0):
+        t, md, x, v = setup(s, deterministic=True, tau=0.1)
+        md.lookahead(0.0)
+        md.build(x, s["box"])
+        md.run(x, v, s["box"], 0.002, 200, unroll=unroll)
+        runs.append((x.clone(), v.clone(), md.thermo()))
+    (x1, v1, th1), (x2, v2, th2) = runs
+    assert th1["redone"] > 0 and th1["redone"] == th2["redone"]
+    assert th1["builds"] == th2["builds"]
     assert torch.equal(x1, x2) and torch.equal(v1, v2)
