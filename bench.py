@@ -326,7 +326,7 @@ def batch_leg(args, dev, flush, world=1, rank=0, frames=256, reps=5, warmup=3):
             "l2": "flushed before each timed batch (256 MiB write)"}
 
 
-def precision_leg(args, dev, flush, thermalize=1000, nve=10000, every=500, timed=200):
+def precision_leg(args, dev, flush, reach=1.6, pruned=1.05, thermalize=1000, nve=10000, every=500, timed=200):
     """The precision form on the large water box (356,700 TIP3P waters,
     1.07M atoms, 224^3 grid) in the deterministic mode (FP32 pairs, 64-bit
     fixed-point forces and grid, FP64 energies): ns/day of the NVT step,
@@ -342,8 +342,8 @@ def precision_leg(args, dev, flush, thermalize=1000, nve=10000, every=500, timed
     t = NonbondedTerm(n, device=dev.index)
     t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
     t.set_exclusions(pairs=s["excluded_pairs"])
-    t.set_interaction(s["cutoff"], 1.2, s["beta"])
-    t.set_pruned_reach(1.0)
+    t.set_interaction(s["cutoff"], reach, s["beta"])
+    t.set_pruned_reach(pruned)
     t.set_pme(s["grid"], s["order"])
     t.set_deterministic(True)
     md = Integrator(t, s["masses"], s["waters"])
@@ -383,6 +383,7 @@ def precision_leg(args, dev, flush, thermalize=1000, nve=10000, every=500, timed
     slope = float(np.polyfit(tt, E[:, 0], 1)[0]) if len(E) > 1 else 0.0  # kJ/mol/ps
     kin = float(E[:, 2].mean())
     return {"workload": "tip3p-1070100 (356,700 waters, 224^3 grid), deterministic mode",
+            "reach_nm": reach, "pruned_reach_nm": pruned,
             "ns_per_day": round(ns_per_day(timed, ms / 1e3), 2), "ms_per_step": round(ms / timed, 4),
             "bitwise_deterministic_two_runs": same, "status": t.status(),
             "nve": {"steps": nve, "dt_ps": DT_PS, "drift_kj_mol_ns": round(slope * 1000.0, 3),
@@ -522,6 +523,7 @@ def main():
     builds = th1["builds"] - th0["builds"]
     prunes = th1["prunes"] - th0["prunes"]
     regrows = th1["regrows"] - th0["regrows"]
+    stops = th1["redone"] - th0["redone"]
     ms_per_step = total_ms / args.steps
     value = ns_per_day(args.md_steps * args.steps * world, total_ms / 1e3)
     status = term.status(clear=True)
@@ -594,13 +596,14 @@ def main():
             "gpu_launches": int(args.steps * args.md_steps * 6 + builds * 16 + prunes * 5),
             "tuned": tuned,
             "builds": int(builds), "prunes": int(prunes), "regrows": int(regrows), "regrows_total": th1["regrows"],
+            "stale_stops": int(stops),
             "temperature_K": round(temp, 1), "status": status}
     if not args.no_adjoint:
         line["adjoint"] = adjoint_leg(args, dev, flush, world)
     if not args.no_batch:
         line["batch"] = batch_leg(args, dev, flush, world, rank)
     if not args.no_precision and world == 1:
-        line["precision"] = precision_leg(args, dev, flush)
+        line["precision"] = precision_leg(args, dev, flush, s["reach"], s["pruned"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(s, s["positions"])
     if rank == 0:
