@@ -488,6 +488,34 @@ __global__ void nb_count_entries(int64_t groups_cap, const int32_t *sizes,
   atomicAdd(&out[NB_SIZE_ENTRIES], counts[g]);
 }
 
+// The box of a group's live members, reduced over a warp whose lanes
+// 0..15 hold the members (dead lanes and lanes 16..31 give nothing).
+__device__ __forceinline__ void nb_live_box(float4 xm, bool on, float3 &lo, float3 &hi) {
+  const unsigned FULL = 0xffffffffu;
+  lo = on ? make_float3(xm.x, xm.y, xm.z) : make_float3(3.0e38f, 3.0e38f, 3.0e38f);
+  hi = on ? make_float3(xm.x, xm.y, xm.z) : make_float3(-3.0e38f, -3.0e38f, -3.0e38f);
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = fminf(lo.x, __shfl_xor_sync(FULL, lo.x, o));
+    lo.y = fminf(lo.y, __shfl_xor_sync(FULL, lo.y, o));
+    lo.z = fminf(lo.z, __shfl_xor_sync(FULL, lo.z, o));
+    hi.x = fmaxf(hi.x, __shfl_xor_sync(FULL, hi.x, o));
+    hi.y = fmaxf(hi.y, __shfl_xor_sync(FULL, hi.y, o));
+    hi.z = fmaxf(hi.z, __shfl_xor_sync(FULL, hi.z, o));
+  }
+}
+
+// True when the point lies farther than the pruned reach from the whole box,
+// so that no member can pass the member test.  Each axis gap is one member's
+// own difference (the box corner is a member coordinate), never more than any
+// member's; `far2` = R_in'^2 (1 + 1e-4) covers the rounding of the squares and
+// their sum, so the test only drops what the member loop would drop.
+__device__ __forceinline__ bool nb_beyond_box(float3 lo, float3 hi, float jx, float jy, float jz, float far2) {
+  float gx = fmaxf(fmaxf(lo.x - jx, jx - hi.x), 0.f);
+  float gy = fmaxf(fmaxf(lo.y - jy, jy - hi.y), 0.f);
+  float gz = fmaxf(fmaxf(lo.z - jz, jz - hi.z), 0.f);
+  return gx * gx + gy * gy + gz * gz > far2;
+}
+
 // The pruning of the dual list (MDIR: emitGroupsPrune,
 // lib/Conversion/MDExecToGPU/MDExecToGPU.cpp:9588; docs/neighbor-groups.md,
 // Section 6.2): inner mask = outer mask and [r^2 <= R_in'^2] at the current
@@ -513,8 +541,13 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
       if (a >= 0) x_prune[3 * a + k % 3] = x[3 * a + k % 3];
     }
   }
-  if (lane < NB_GROUP) s_m[warp][lane] = xq[g * NB_GROUP + lane];
-  unsigned live = __ballot_sync(FULL, lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0) & 0xffffu;
+  float4 xme = xq[g * NB_GROUP + (lane & 15)];
+  if (lane < NB_GROUP) s_m[warp][lane] = xme;
+  bool on = lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0;
+  unsigned live = __ballot_sync(FULL, on) & 0xffffu;
+  float3 box_lo, box_hi;
+  nb_live_box(xme, on, box_lo, box_hi);
+  const float far2 = rin2 * 1.0001f;
   __syncwarp();
   int cnt = (int)min((int64_t)counts[g], list_cap);
   int out = 0;
@@ -529,6 +562,7 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
       nb_decode_image(((unsigned)en.y >> 16) & 31, sx, sy, sz);
       float4 xj = xq[en.x];
       float jx = xj.x + (float)sx * Lx, jy = xj.y + (float)sy * Ly, jz = xj.z + (float)sz * Lz;
+      if (nb_beyond_box(box_lo, box_hi, jx, jy, jz, far2)) mm = 0;
       while (mm) {
         int m = __ffs(mm) - 1;
         mm &= mm - 1;
@@ -564,6 +598,7 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
   __shared__ float4 s_m[NB_GROUP];
   __shared__ int s_cnt[NB_PRUNE_WARPS];
   __shared__ unsigned s_live;
+  __shared__ float3 s_lo, s_hi;
   const unsigned FULL = 0xffffffffu;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int64_t g = blockIdx.x;
@@ -574,12 +609,22 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
     if (a >= 0) x_prune[3 * a + threadIdx.x % 3] = x[3 * a + threadIdx.x % 3];
   }
   if (warp == 0) {
-    if (lane < NB_GROUP) s_m[lane] = xq[g * NB_GROUP + lane];
-    unsigned live = __ballot_sync(FULL, lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0) & 0xffffu;
-    if (lane == 0) s_live = live;
+    float4 xme = xq[g * NB_GROUP + (lane & 15)];
+    if (lane < NB_GROUP) s_m[lane] = xme;
+    bool on = lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0;
+    unsigned live = __ballot_sync(FULL, on) & 0xffffu;
+    float3 blo, bhi;
+    nb_live_box(xme, on, blo, bhi);
+    if (lane == 0) {
+      s_live = live;
+      s_lo = blo;
+      s_hi = bhi;
+    }
   }
   __syncthreads();
   unsigned live = s_live;
+  const float3 box_lo = s_lo, box_hi = s_hi;
+  const float far2 = rin2 * 1.0001f;
   int cnt = (int)min((int64_t)counts[g], list_cap);
   int share = ((cnt + NB_PRUNE_WARPS - 1) / NB_PRUNE_WARPS + 31) / 32 * 32;
   int lo = min(cnt, warp * share), hi = min(cnt, lo + share);
@@ -596,6 +641,7 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
       nb_decode_image(((unsigned)en.y >> 16) & 31, sx, sy, sz);
       float4 xj = xq[en.x];
       float jx = xj.x + (float)sx * Lx, jy = xj.y + (float)sy * Ly, jz = xj.z + (float)sz * Lz;
+      if (nb_beyond_box(box_lo, box_hi, jx, jy, jz, far2)) mm = 0;
       while (mm) {
         int m = __ffs(mm) - 1;
         mm &= mm - 1;

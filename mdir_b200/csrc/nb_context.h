@@ -262,7 +262,8 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s);
 // frames spread into qgrid (through qfixed, empty, in the deterministic
 // mode) -> spec -> phi, on the integrator's own buffers.
 int nb_pme_md_chain(NbCtx &c, const double box[3], float *qgrid, unsigned long long *qfixed, float2 *spec,
-                    float *phi, cudaStream_t s);
+                    float *phi, const float *influence, const int *halt, cudaStream_t s);
+int nb_pme_influence(NbCtx &c, const double box[3], float *influence, cudaStream_t s);
 
 // The batch (mdrtNbBatch): the build of all frames (grows and builds again
 // until every list fits; host wait), the frames of the places, the pair

@@ -29,6 +29,7 @@
 #include "nb_spline.cuh"
 
 #define MD_MAX_UNROLL 256  // steps of one replayed graph
+#define MD_IN_FLIGHT 2     // step graphs queued ahead of the one the host checks
 
 struct mdrtMd {
   NbCtx *nb = nullptr;
@@ -68,7 +69,15 @@ struct mdrtMd {
   float *qgrid = nullptr, *phi = nullptr;
   unsigned long long *qfixed = nullptr;
   float2 *spec = nullptr;
+  float *influence = nullptr;      // B C, f32 per half-complex point, of influence_key
+  double influence_key[7] = {0, 0, 0, 0, 0, 0, 0};  // cell, beta, f, grid
   int64_t pme_points = 0;          // K0 K1 K2 the buffers were sized for
+  // A stop at a stale list, seen by the host while step graphs are queued:
+  // the update writes 1 into mapped pinned memory, and the host, which keeps
+  // at most MD_IN_FLIGHT graphs queued beyond the one it waits for, stops
+  // launching (the graphs after a stop would do nothing).
+  int *h_halt = nullptr, *d_halt = nullptr;
+  cudaEvent_t ev_run[MD_IN_FLIGHT + 1] = {};
   double temperature = 300.0, tau = 0.0;
   int64_t ndof = 0;
   unsigned long long seed = 1;
@@ -178,6 +187,7 @@ struct UpdateParams {
   int pme_fused;
   GridParams G;
   const float *phi;
+  int *host_halt;  // mapped pinned memory: 1 when a stale list stopped the steps
 };
 
 // The force on atom a: the pair / excluded accumulator of its place and the
@@ -553,6 +563,7 @@ __device__ void md_last_block(const UpdateParams &U, const double *ke_part, int 
     atomicOr(U.status, NB_STATUS_STALE_LIST);
     atomicAdd(&U.peak[3], 1);
     U.flag[3] = 1;
+    if (U.host_halt) *(volatile int *)U.host_halt = 1;
   }
   int prune = (U.prune_half2 > 0.0 && (rebuild || (double)p2 > U.prune_half2)) ? 1 : 0;
   // the host's build after a stale list (or, step by step, after a rebuild) prunes too
@@ -624,7 +635,7 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
     cudaEventRecord(m.ev_fork, s);
     cudaStreamWaitEvent(m.side, m.ev_fork, 0);
     if (fused)
-      nb_pme_md_chain(c, box, m.qgrid, m.qfixed, m.spec, m.phi, m.side);
+      nb_pme_md_chain(c, box, m.qgrid, m.qfixed, m.spec, m.phi, m.influence, flag + 3, m.side);
     else
       nb_pme_run(c, box, false, false, m.side);
   }
@@ -667,6 +678,7 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
   U.G.invL1 = (float)(1.0 / box[1]);
   U.G.invL2 = (float)(1.0 / box[2]);
   U.phi = m.phi;
+  U.host_halt = use_graph ? m.d_halt : nullptr;
   md_update<<<m.ke_blocks, MD_UPDATE_THREADS, 0, s>>>(
       m.nwaters, m.nfree, m.waters, m.free_atoms, U, m.inv_mass, m.mass, c.q, c.place_of, c.shift, c.acc,
       c.acc_fixed, (pme && !fused) ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref,
@@ -710,21 +722,40 @@ static int md_pme_buffers(mdrtMd *m) {
   bool want = c.pme.on && c.beta > 0.0 && c.pme.order == 4;
   int64_t pts = want ? (int64_t)c.pme.K[0] * c.pme.K[1] * c.pme.K[2] : 0;
   if (pts == m->pme_points) return 0;
-  for (void **p : {(void **)&m->qgrid, (void **)&m->phi, (void **)&m->qfixed, (void **)&m->spec}) {
+  for (void **p : {(void **)&m->qgrid, (void **)&m->phi, (void **)&m->qfixed, (void **)&m->spec,
+                   (void **)&m->influence}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
   m->pme_points = 0;
+  for (double &k : m->influence_key) k = 0.0;
   if (!want) return 0;
   int64_t half = (int64_t)c.pme.K[0] * c.pme.K[1] * (c.pme.K[2] / 2 + 1);
   if (cudaMalloc(&m->qgrid, sizeof(float) * pts) != cudaSuccess ||
       cudaMalloc(&m->phi, sizeof(float) * pts) != cudaSuccess ||
       cudaMalloc(&m->qfixed, sizeof(unsigned long long) * pts) != cudaSuccess ||
-      cudaMalloc(&m->spec, sizeof(float2) * half) != cudaSuccess)
+      cudaMalloc(&m->spec, sizeof(float2) * half) != cudaSuccess ||
+      cudaMalloc(&m->influence, sizeof(float) * half) != cudaSuccess)
     return -1;
   // the fixed-point grid starts empty; each step's conversion empties it again
   if (cudaMemset(m->qfixed, 0, sizeof(unsigned long long) * pts) != cudaSuccess) return -1;
   m->pme_points = pts;
+  return 0;
+}
+
+// The influence table for the MD step's PME chain, made again when the
+// cell, the Ewald parameter, the Coulomb factor or the grid differ from
+// those it was made for.
+static int md_influence(mdrtMd *m, const double box[3], cudaStream_t s) {
+  if (!m->influence) return 0;
+  const NbCtx &c = *m->nb;
+  double key[7] = {box[0], box[1], box[2], c.beta, c.coulomb, (double)c.pme.K[0],
+                   (double)c.pme.K[1] * 65536.0 + (double)c.pme.K[2]};
+  bool same = true;
+  for (int k = 0; k < 7; ++k) same = same && key[k] == m->influence_key[k];
+  if (same) return 0;
+  if (nb_pme_influence(*m->nb, box, m->influence, s)) return -1;
+  for (int k = 0; k < 7; ++k) m->influence_key[k] = key[k];
   return 0;
 }
 
@@ -733,13 +764,16 @@ static void md_free(mdrtMd *m) {
   md_drop_graph(m);
   if (m->ev_fork) cudaEventDestroy(m->ev_fork);
   if (m->ev_join) cudaEventDestroy(m->ev_join);
+  for (cudaEvent_t e : m->ev_run)
+    if (e) cudaEventDestroy(e);
+  if (m->h_halt) cudaFreeHost(m->h_halt);
   if (m->side) cudaStreamDestroy(m->side);
   for (void *p : {(void *)m->inv_mass, (void *)m->mass, (void *)m->waters, (void *)m->free_atoms,
                   (void *)m->excl_other, (void *)m->force, (void *)m->x_ref, (void *)m->x_prune,
                   (void *)m->ke_part, (void *)m->maxd2, (void *)m->thermo, (void *)m->flag,
                   (void *)m->noise, (void *)m->x_ck, (void *)m->v_ck, (void *)m->thermo_ck, (void *)m->peak,
                   (void *)m->xref_ck, (void *)m->xprune_ck, (void *)m->qgrid, (void *)m->phi, (void *)m->qfixed,
-                  (void *)m->spec})
+                  (void *)m->spec, (void *)m->influence})
     if (p) cudaFree(p);
   if (m->h_peak) cudaFreeHost(m->h_peak);
   if (m->h_steps) cudaFreeHost(m->h_steps);
@@ -846,7 +880,11 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
             cudaMallocHost(&m->h_steps, sizeof(double) * 2) == cudaSuccess &&
             cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, hi) == cudaSuccess &&
             cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
-            cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming) == cudaSuccess;
+            cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming) == cudaSuccess &&
+            cudaHostAlloc(&m->h_halt, sizeof(int), cudaHostAllocMapped) == cudaSuccess &&
+            cudaHostGetDevicePointer(&m->d_halt, m->h_halt, 0) == cudaSuccess;
+  for (int k = 0; ok && k <= MD_IN_FLIGHT; ++k)
+    ok = cudaEventCreateWithFlags(&m->ev_run[k], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     md_free(m);
     return MDRT_NB_CUDA_ERROR;
@@ -1081,6 +1119,7 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
     if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;
   cudaSetDevice(c.device);
   cudaStream_t st = (cudaStream_t)stream;
+  if (md_influence(m, box, st)) return MDRT_NB_CUDA_ERROR;
   if (unroll <= 0) return md_run_steps(m, x, v, box, dt, steps, unroll < 0 ? -unroll : MD_WINDOW, stream);
   // Runs of step graphs.  Each run starts from a checkpoint (positions,
   // velocities, thermostat state, and the positions the lists in force were
@@ -1106,8 +1145,19 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
         cudaMemcpyAsync(m->thermo_ck, m->thermo, sizeof(double) * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
         cudaMemsetAsync(m->peak, 0, sizeof(int32_t) * 4, st) != cudaSuccess)
       return MDRT_NB_CUDA_ERROR;
-    for (int64_t k = 0; k < launches; ++k)
-      if (cudaGraphLaunch(m->exec, st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
+    // the previous run ended in a synchronize: nothing writes the word now
+    *(volatile int *)m->h_halt = 0;
+    for (int64_t k = 0; k < launches; ++k) {
+      cudaEvent_t &done = m->ev_run[k % (MD_IN_FLIGHT + 1)];
+      if (k > MD_IN_FLIGHT) {
+        // the graph launched MD_IN_FLIGHT + 1 launches ago has finished
+        // (the ones after it keep the device busy meanwhile)
+        if (cudaEventSynchronize(done) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
+        if (*(volatile int *)m->h_halt) break;
+      }
+      if (cudaGraphLaunch(m->exec, st) != cudaSuccess || cudaEventRecord(done, st) != cudaSuccess)
+        return MDRT_NB_CUDA_ERROR;
+    }
     if (cudaMemcpyAsync(m->h_peak, m->peak, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(m->h_steps, m->thermo_ck + 3, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(m->h_steps + 1, m->thermo + 3, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||

@@ -34,6 +34,8 @@ struct PairParams {
   float Lx, Ly, Lz;
   float rc2;
   float beta;
+  float beta_p;         // p beta, p of the erfc approximation below
+  float nb2_log2e;      // -beta^2 log2(e): exp(-beta^2 r^2) = 2^(r^2 nb2_log2e)
   float two_beta_sqrtpi;
   float coulomb;
   float coulomb_shift;  // erfc(beta rc)/rc when the direct sum is shifted, else 0
@@ -43,14 +45,35 @@ struct PairParams {
   int64_t units_cap;
 };
 
-// erfc(x) for x >= 0 from exp(-x^2): Abramowitz & Stegun 7.1.26
-// (Hastings), |error| <= 1.5e-7.  `ex` is exp(-x^2), computed once and
-// shared with the force.
-__device__ __forceinline__ float nb_erfc_from_exp(float x, float ex) {
-  const float p = 0.3275911f;
+// The special-function unit's approximations with denormals flushed
+// (PTX rsqrt/ex2/rcp .approx.ftz).  The flush touches only arguments or
+// results below 2^-126: r^2 that small means two sites at one point, and
+// 2^(r^2 nb2_log2e) stays above 2^-40 within any cutoff for which the real
+// space sum is accurate (beta r_c <= 5), so no value changes and the
+// denormal scaling of the non-ftz forms is dropped.
+__device__ __forceinline__ float nb_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float nb_ex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float nb_rcp(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// erfc(beta r) from exp(-beta^2 r^2): Abramowitz & Stegun 7.1.26
+// (Hastings), |error| <= 1.5e-7, with t = 1 / (1 + p beta r).  `pbr` is
+// p beta r; `ex` is exp(-beta^2 r^2), computed once and shared with the force.
+__device__ __forceinline__ float nb_erfc_from_exp(float pbr, float ex) {
   const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
               a5 = 1.061405429f;
-  float t = __fdividef(1.0f, fmaf(p, x, 1.0f));
+  float t = nb_rcp(1.0f + pbr);
   float poly = fmaf(fmaf(fmaf(fmaf(a5, t, a4), t, a3), t, a2), t, a1) * t;
   return poly * ex;
 }
@@ -167,7 +190,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
         } else {
           cc = s_lj[pt[k] + tj];
         }
-        float rinv = rsqrtf(r2s);
+        float rinv = nb_rsqrt(r2s);
         float rinv2 = rinv * rinv;
         float s6 = rinv2 * rinv2 * rinv2;
         float a12 = cc.y * s6 * s6, a6 = cc.x * s6;
@@ -182,9 +205,8 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
         }
         float qq = xm.w * xj.w;
         float rr = r2s * rinv;
-        float bx = P.beta * rr;
-        float ex = __expf(-bx * bx);
-        float erfcv = nb_erfc_from_exp(bx, ex);
+        float ex = nb_ex2(r2s * P.nb2_log2e);
+        float erfcv = nb_erfc_from_exp(P.beta_p * rr, ex);
         fs = fmaf(qq * fmaf(erfcv, rinv, P.two_beta_sqrtpi * ex), rinv2, fs);
         fs = inside ? fs : 0.f;
         float fx = fs * dx, fy = fs * dy, fz = fs * dz;
@@ -615,12 +637,11 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
         float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         bool inside = ((mrot >> k) & 1u) && (r2 < P.rc2);
         float r2s = inside ? r2 : 1.0f;
-        float rinv = rsqrtf(r2s);
+        float rinv = nb_rsqrt(r2s);
         float rinv2 = rinv * rinv;
         float rr = r2s * rinv;
-        float bx = P.beta * rr;
-        float ex = __expf(-bx * bx);
-        float erfcv = nb_erfc_from_exp(bx, ex);
+        float ex = nb_ex2(r2s * P.nb2_log2e);
+        float erfcv = nb_erfc_from_exp(P.beta_p * rr, ex);
         // w: the factor of the pair's term; cq: its Coulomb part per unit f q_i q_j
         float w, cq;
         if (MODE == 0) {
@@ -758,6 +779,8 @@ PairParams pair_params(const NbCtx &c, const double box[3]) {
   P.Lz = (float)box[2];
   P.rc2 = (float)(c.cutoff * c.cutoff);
   P.beta = (float)c.beta;
+  P.beta_p = (float)(0.3275911 * c.beta);
+  P.nb2_log2e = (float)(-c.beta * c.beta / log(2.0));
   P.two_beta_sqrtpi = (float)(2.0 * c.beta / sqrt(M_PI));
   P.coulomb = (float)c.coulomb;
   P.coulomb_shift = c.coulomb_shift ? (float)(erfc(c.beta * c.cutoff) / c.cutoff) : 0.f;

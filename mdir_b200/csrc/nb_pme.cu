@@ -34,7 +34,8 @@ __global__ void __launch_bounds__(256) nb_spread(GridParams G, int64_t places,
                                                  const int32_t *__restrict__ sizes,
                                                  const int32_t *__restrict__ order,
                                                  const float4 *__restrict__ xq, float *__restrict__ grid,
-                                                 unsigned long long *__restrict__ fixed) {
+                                                 unsigned long long *__restrict__ fixed, const int *halt) {
+  if (halt && *halt) return;  // the MD step stopped at a stale list
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int64_t p = t / P;
   int c = (int)(t - p * P);
@@ -89,6 +90,43 @@ struct ConvParams {
   double pi2_beta2;  // pi^2 / beta^2
 };
 
+// B C at half-complex point k: the B-spline moduli product times the Ewald
+// reciprocal kernel f exp(-pi^2 m^2 / beta^2) / (pi V m^2); 0 at m = 0.
+__device__ __forceinline__ double nb_bc(const ConvParams &C, const float *__restrict__ moduli, int64_t k,
+                                        double &m0, double &m1, double &m2v, double &mm) {
+  int i2 = (int)(k % C.H2);
+  int64_t r = k / C.H2;
+  int i1 = (int)(r % C.K1);
+  int i0 = (int)(r / C.K1);
+  m0 = (i0 <= C.K0 / 2 ? i0 : i0 - C.K0) / C.L0;
+  m1 = (i1 <= C.K1 / 2 ? i1 : i1 - C.K1) / C.L1;
+  m2v = (i2 <= C.K2 / 2 ? i2 : i2 - C.K2) / C.L2;
+  mm = m0 * m0 + m1 * m1 + m2v * m2v;
+  if (k == 0) return 0.0;
+  double B = (double)moduli[i0] * (double)moduli[C.K0 + i1] * (double)moduli[C.K0 + C.K1 + i2];
+  return B * C.pref * exp(-C.pi2_beta2 * mm) / mm;
+}
+
+__global__ void nb_influence(ConvParams C, const float *__restrict__ moduli, float *__restrict__ out) {
+  int64_t total = (int64_t)C.K0 * C.K1 * C.H2;
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= total) return;
+  double m0, m1, m2v, mm;
+  out[k] = (float)nb_bc(C, moduli, k, m0, m1, m2v, mm);
+}
+
+// The convolution of the MD step: the spectrum times the influence table
+// (forces only, no energy sums).
+__global__ void nb_scale_spectrum(int64_t half, const float *__restrict__ influence, float2 *__restrict__ spec,
+                                  const int *halt) {
+  if (halt && *halt) return;  // the MD step stopped at a stale list
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= half) return;
+  float2 v = spec[k];
+  float b = influence[k];
+  spec[k] = make_float2(v.x * b, v.y * b);
+}
+
 // Multiplies the half-complex spectrum by B C and sums E and W in f64.
 template <bool ENERGY>
 __global__ void __launch_bounds__(256) nb_convolve(ConvParams C, const float *__restrict__ moduli,
@@ -100,19 +138,9 @@ __global__ void __launch_bounds__(256) nb_convolve(ConvParams C, const float *__
   double v[7] = {0, 0, 0, 0, 0, 0, 0};
   if (k < total) {
     int i2 = (int)(k % C.H2);
-    int64_t r = k / C.H2;
-    int i1 = (int)(r % C.K1);
-    int i0 = (int)(r / C.K1);
-    double m0 = (i0 <= C.K0 / 2 ? i0 : i0 - C.K0) / C.L0;
-    double m1 = (i1 <= C.K1 / 2 ? i1 : i1 - C.K1) / C.L1;
-    double m2v = (i2 <= C.K2 / 2 ? i2 : i2 - C.K2) / C.L2;
-    double mm = m0 * m0 + m1 * m1 + m2v * m2v;
+    double m0, m1, m2v, mm;
+    double bc = nb_bc(C, moduli, k, m0, m1, m2v, mm);
     float2 s = spec[k];
-    double bc = 0.0;
-    if (k != 0) {
-      double B = (double)moduli[i0] * (double)moduli[C.K0 + i1] * (double)moduli[C.K0 + C.K1 + i2];
-      bc = B * C.pref * exp(-C.pi2_beta2 * mm) / mm;
-    }
     spec[k] = make_float2((float)(s.x * bc), (float)(s.y * bc));
     if (ENERGY && k != 0) {
       double wgt = (i2 == 0 || (C.K2 % 2 == 0 && i2 == C.K2 / 2)) ? 1.0 : 2.0;
@@ -496,10 +524,10 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
 #define SPREAD(ORD)                                                                                    \
   if (c.deterministic)                                                                                 \
     nb_spread<ORD, true><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order,   \
-                                                                  c.xq, P.grid, P.fixed);              \
+                                                                  c.xq, P.grid, P.fixed, nullptr);     \
   else                                                                                                 \
     nb_spread<ORD, false><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order,  \
-                                                                   c.xq, P.grid, P.fixed);
+                                                                   c.xq, P.grid, P.fixed, nullptr);
   switch (P.order) {
     case 4: SPREAD(4); break;
     case 5: SPREAD(5); break;
@@ -948,7 +976,7 @@ int nb_batch_pme_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
 // function, and the update gathers each atom's PME force from the potential.
 
 int nb_pme_md_chain(NbCtx &c, const double box[3], float *qgrid, unsigned long long *qfixed, float2 *spec,
-                    float *phi, cudaStream_t s) {
+                    float *phi, const float *influence, const int *halt, cudaStream_t s) {
   NbPme &P = c.pme;
   GridParams G;
   G.K0 = P.K[0];
@@ -963,27 +991,37 @@ int nb_pme_md_chain(NbCtx &c, const double box[3], float *qgrid, unsigned long l
   if (c.deterministic) {
     // the fixed-point grid is empty: its conversion empties it
     nb_spread<4, true><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, qgrid,
-                                                                qfixed);
+                                                                qfixed, halt);
     nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, qfixed, qgrid);
   } else {
     cudaMemsetAsync(qgrid, 0, sizeof(float) * total, s);
     nb_spread<4, false><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, qgrid,
-                                                                 qfixed);
+                                                                 qfixed, halt);
   }
   cufftSetStream(P.fwd, s);
   cufftSetStream(P.bwd, s);
   if (cufftExecR2C(P.fwd, qgrid, (cufftComplex *)spec) != CUFFT_SUCCESS) return -3;
+  nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, influence, spec, halt);
+  if (cufftExecC2R(P.bwd, (cufftComplex *)spec, phi) != CUFFT_SUCCESS) return -3;
+  return 0;
+}
+
+// The influence function B C of the cell `box` at every half-complex point,
+// in f32 (the factor nb_convolve forms each time), for a chain that runs
+// many times at one cell.
+int nb_pme_influence(NbCtx &c, const double box[3], float *influence, cudaStream_t s) {
+  NbPme &P = c.pme;
   ConvParams C;
-  C.K0 = G.K0;
-  C.K1 = G.K1;
-  C.K2 = G.K2;
-  C.H2 = G.K2 / 2 + 1;
+  C.K0 = P.K[0];
+  C.K1 = P.K[1];
+  C.K2 = P.K[2];
+  C.H2 = P.K[2] / 2 + 1;
   C.L0 = box[0];
   C.L1 = box[1];
   C.L2 = box[2];
   C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
   C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
-  nb_convolve<false><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, spec, P.partials);
-  if (cufftExecC2R(P.bwd, (cufftComplex *)spec, phi) != CUFFT_SUCCESS) return -3;
-  return 0;
+  int64_t half = (int64_t)C.K0 * C.K1 * C.H2;
+  nb_influence<<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, influence);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
