@@ -586,17 +586,31 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
 // takes the w-th contiguous share of the outer entries, stages what
 // survives in shared memory, and the block writes the shares in warp order,
 // so the inner list is the one of the warp-per-group kernel, in a quarter of
-// the dependent rounds.  Dynamic shared memory: list_cap entries.
+// the dependent rounds.  A lane takes four entries a round, their loads and
+// their partners' frames all issued before the first test, so a round costs
+// two memory latencies for 128 entries.  Dynamic shared memory: list_cap
+// entries.
+//
+// With `units`, each block also claims the units of its inner list from
+// *unit_counter (zeroed by whoever decided the pruning) and writes them, so
+// that no second launch scans the counts; the units then come in the order
+// the blocks finish, which changes no force (each unit's work is the same)
+// but the order of the per-unit energy partials: the deterministic mode keeps
+// the scan.  Block 0 counts the pruning in *prunes.
 #define NB_PRUNE_WARPS 4
 __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
     nb_prune_block(int64_t groups_cap, const int32_t *__restrict__ sizes, float Lx, float Ly, float Lz, float rin2,
                    int64_t list_cap, const int2 *__restrict__ slab, const int32_t *__restrict__ counts,
                    const int32_t *__restrict__ order, const float4 *__restrict__ xq, int2 *__restrict__ slab_in,
                    int32_t *__restrict__ counts_in, const int *gate, const double *__restrict__ x,
-                   double *__restrict__ x_prune) {
+                   double *__restrict__ x_prune, int32_t *unit_counter, int2 *__restrict__ units,
+                   int64_t units_cap, double *prunes) {
   extern __shared__ int2 s_stage[];
   __shared__ float4 s_m[NB_GROUP];
   __shared__ int s_cnt[NB_PRUNE_WARPS];
+  __shared__ int s_unit0, s_nunits;
+  __shared__ int2 s_qe[NB_PRUNE_WARPS][64];    // a warp's queue of entries that pass the box test
+  __shared__ float4 s_qx[NB_PRUNE_WARPS][64];  // and their partners' images
   __shared__ unsigned s_live;
   __shared__ float3 s_lo, s_hi;
   const unsigned FULL = 0xffffffffu;
@@ -626,35 +640,82 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
   const float3 box_lo = s_lo, box_hi = s_hi;
   const float far2 = rin2 * 1.0001f;
   int cnt = (int)min((int64_t)counts[g], list_cap);
-  int share = ((cnt + NB_PRUNE_WARPS - 1) / NB_PRUNE_WARPS + 31) / 32 * 32;
+  int share = ((cnt + NB_PRUNE_WARPS - 1) / NB_PRUNE_WARPS + 127) / 128 * 128;
   int lo = min(cnt, warp * share), hi = min(cnt, lo + share);
   int2 *stage = s_stage + lo;  // a warp's survivors never outnumber its share
-  int out = 0;
-  for (int base = lo; base < hi; base += 32) {
-    int e = base + lane;
+  const int2 *src = slab + g * list_cap;
+  int2 *qe = s_qe[warp];
+  float4 *qx = s_qx[warp];
+  int out = 0, qn = 0;  // survivors staged; entries queued (warp-uniform)
+  // The member tests of the first `take` queued entries, a lane each, in
+  // queue order (the order of the outer list): no lane idles on an entry
+  // that the box test dropped.
+  auto drain = [&](int take) {
+    __syncwarp();
     unsigned inner = 0;
     int2 en = make_int2(0, 0);
-    if (e < hi) {
-      en = slab[g * list_cap + e];
-      unsigned mm = (unsigned)en.y & live & 0xffffu;
-      int sx, sy, sz;
-      nb_decode_image(((unsigned)en.y >> 16) & 31, sx, sy, sz);
-      float4 xj = xq[en.x];
-      float jx = xj.x + (float)sx * Lx, jy = xj.y + (float)sy * Ly, jz = xj.z + (float)sz * Lz;
-      if (nb_beyond_box(box_lo, box_hi, jx, jy, jz, far2)) mm = 0;
-      while (mm) {
-        int m = __ffs(mm) - 1;
-        mm &= mm - 1;
+    if (lane < take) {
+      en = qe[lane];
+      float4 xj = qx[lane];
+      unsigned mm = (unsigned)en.y & live;
+#pragma unroll
+      for (int m = 0; m < NB_GROUP; ++m) {
         float4 xm = s_m[m];
-        float dx = xm.x - jx, dy = xm.y - jy, dz = xm.z - jz;
+        float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
         float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 <= rin2) inner |= 1u << m;
+        if (((mm >> m) & 1u) && r2 <= rin2) inner |= 1u << m;
       }
     }
     unsigned has = __ballot_sync(FULL, inner != 0);
-    if (inner) stage[out + __popc(has & ((1u << lane) - 1))] = make_int2(en.x, (int)(inner | ((unsigned)en.y & 0xffff0000u)));
+    if (inner)
+      stage[out + __popc(has & ((1u << lane) - 1))] = make_int2(en.x, (int)(inner | ((unsigned)en.y & 0xffff0000u)));
     out += __popc(has);
+    // the rest of the queue to its front
+    __syncwarp();
+    int2 re = make_int2(0, 0);
+    float4 rx = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool move = take + lane < qn;
+    if (move) {
+      re = qe[take + lane];
+      rx = qx[take + lane];
+    }
+    __syncwarp();
+    if (move) {
+      qe[lane] = re;
+      qx[lane] = rx;
+    }
+    qn -= take;
+  };
+  for (int base = lo; base < hi; base += 128) {
+    int2 en[4];
+    float4 xj[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) en[j] = base + 32 * j + lane < hi ? src[base + 32 * j + lane] : make_int2(0, 0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) xj[j] = base + 32 * j + lane < hi ? xq[en[j].x] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      bool pass = false;
+      float jx = 0.f, jy = 0.f, jz = 0.f;
+      if (base + 32 * j + lane < hi && ((unsigned)en[j].y & live & 0xffffu)) {
+        int sx, sy, sz;
+        nb_decode_image(((unsigned)en[j].y >> 16) & 31, sx, sy, sz);
+        jx = xj[j].x + (float)sx * Lx;
+        jy = xj[j].y + (float)sy * Ly;
+        jz = xj[j].z + (float)sz * Lz;
+        pass = !nb_beyond_box(box_lo, box_hi, jx, jy, jz, far2);
+      }
+      unsigned pb = __ballot_sync(FULL, pass);
+      if (pass) {
+        int at = qn + __popc(pb & ((1u << lane) - 1));
+        qe[at] = en[j];
+        qx[at] = make_float4(jx, jy, jz, 0.f);
+      }
+      qn += __popc(pb);
+      if (qn >= 32) drain(32);
+    }
   }
+  if (qn > 0) drain(qn);
   if (lane == 0) s_cnt[warp] = out;
   __syncthreads();
   int at = 0, total = 0;
@@ -663,7 +724,20 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
     total += s_cnt[w];
   }
   for (int i = lane; i < out; i += 32) slab_in[g * list_cap + at + i] = stage[i];
-  if (threadIdx.x == 0) counts_in[g] = total;
+  if (threadIdx.x == 0) {
+    counts_in[g] = total;
+    if (units) {
+      int nu = (total + NB_UNIT - 1) / NB_UNIT;
+      s_nunits = nu;
+      s_unit0 = nu > 0 ? atomicAdd(unit_counter, nu) : 0;
+      if (g == 0 && prunes) *prunes += 1.0;
+    }
+  }
+  if (units) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < s_nunits; k += blockDim.x)
+      if (s_unit0 + k < units_cap) units[s_unit0 + k] = make_int2((int)g, k);
+  }
 }
 
 inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); }
@@ -862,7 +936,7 @@ void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s) {
     }
     nb_prune_block<<<(int)c.groups_cap, NB_PRUNE_WARPS * 32, stage, s>>>(
         c.groups_cap, c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
-        c.counts, c.order, c.xq, c.slab_in, c.counts_in, nullptr, nullptr, nullptr);
+        c.counts, c.order, c.xq, c.slab_in, c.counts_in, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr);
   } else {
     nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
                                                         (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
@@ -920,7 +994,7 @@ __global__ void __launch_bounds__(1024) nb_units_one_block(int64_t groups_cap, c
 }  // namespace
 
 void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double *x, double *x_prune,
-                    double *prunes, cudaStream_t s) {
+                    double *prunes, int32_t *unit_counter, cudaStream_t s) {
   double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2]);
   size_t stage = sizeof(int2) * (size_t)c.list_cap;
   if (stage <= 200 * 1024) {
@@ -929,9 +1003,14 @@ void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double
       cudaFuncSetAttribute(nb_prune_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
       configured = (int)stage;
     }
+    // outside the deterministic mode the blocks claim their units themselves
+    // (the counter is zeroed by the update that asked for the pruning)
+    bool claim = !c.deterministic && unit_counter;
     nb_prune_block<<<(int)c.groups_cap, NB_PRUNE_WARPS * 32, stage, s>>>(
         c.groups_cap, c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
-        c.counts, c.order, c.xq, c.slab_in, c.counts_in, gate, x, x_prune);
+        c.counts, c.order, c.xq, c.slab_in, c.counts_in, gate, x, x_prune, claim ? unit_counter : nullptr,
+        claim ? c.units_in : nullptr, c.units_cap, claim ? prunes : nullptr);
+    if (claim) return;
   } else {
     nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
                                                         (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,

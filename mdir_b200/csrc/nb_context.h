@@ -223,7 +223,7 @@ void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s);
 // then the inner units in one block, counting the pruning in *prunes.  The
 // per-step pruning of the MD step, which needs no conditional node.
 void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double *x, double *x_prune,
-                    double *prunes, cudaStream_t s);
+                    double *prunes, int32_t *unit_counter, cudaStream_t s);
 // Allocates the inner lists to the outer capacities (host, between launches).
 int nb_reserve_inner(NbCtx &c);
 // Grows the list capacity for lists of up to `longest` entries (+25%), as

@@ -188,6 +188,7 @@ struct UpdateParams {
   GridParams G;
   const float *phi;
   int *host_halt;  // mapped pinned memory: 1 when a stale list stopped the steps
+  int32_t *unit_counter;  // zeroed with a pruning due: the pruning's blocks claim their units from it
 };
 
 // The force on atom a: the pair / excluded accumulator of its place and the
@@ -573,6 +574,7 @@ __device__ void md_last_block(const UpdateParams &U, const double *ke_part, int 
   maxd2[2] = 0u;
   U.flag[0] = rebuild;
   U.flag[1] = prune;
+  if (prune && U.unit_counter) *U.unit_counter = 0;
   U.flag[2] = stale;
   if (U.use_graph && U.check_build) cudaGraphSetConditional(U.h_any, rebuild);
 }
@@ -622,6 +624,13 @@ static SettleParams settle_params(const mdrtMd &m) {
   S.ra = 2.0 * m.mH * h / (m.mO + 2.0 * m.mH);
   S.rb = h - S.ra;
   return S;
+}
+
+// The count of inner units that the gated pruning's blocks claim from (the
+// deterministic mode keeps the ordered scan: none).
+static int32_t *md_unit_counter(mdrtMd &m) {
+  NbCtx &c = *m.nb;
+  return (c.deterministic || !c.sizes_in) ? nullptr : c.sizes_in + NB_SIZE_UNITS;
 }
 
 // One step on `s` from the frames xq of the current positions x.
@@ -679,6 +688,7 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
   U.G.invL2 = (float)(1.0 / box[2]);
   U.phi = m.phi;
   U.host_halt = use_graph ? m.d_halt : nullptr;
+  U.unit_counter = c.inner_reach > 0.0 ? md_unit_counter(m) : nullptr;
   md_update<<<m.ke_blocks, MD_UPDATE_THREADS, 0, s>>>(
       m.nwaters, m.nfree, m.waters, m.free_atoms, U, m.inv_mass, m.mass, c.q, c.place_of, c.shift, c.acc,
       c.acc_fixed, (pme && !fused) ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref,
@@ -696,7 +706,8 @@ static void md_prune_body(mdrtMd &m, const double *x, const double box[3], cudaS
 // device): two launches that do nothing otherwise, no conditional node.
 static void md_prune_step(mdrtMd &m, const double *x, const double box[3], cudaStream_t s) {
   NbCtx &c = *m.nb;
-  if (c.inner_reach > 0.0) nb_prune_gated(c, box, m.flag + 1, x, m.x_prune, m.thermo + 5, s);
+  if (c.inner_reach > 0.0)
+    nb_prune_gated(c, box, m.flag + 1, x, m.x_prune, m.thermo + 5, md_unit_counter(m), s);
 }
 
 // A build at x on `s` without a host wait (the body of the conditional node).
