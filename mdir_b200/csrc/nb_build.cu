@@ -189,9 +189,14 @@ struct SearchParams {
 // a block; W = 4: a block a group).  Lanes 0-15 and 16-31 of a warp hold the
 // members; a pass tests two candidate groups, one per half-warp, each lane
 // one candidate place against the 16 members.  With W > 1 the columns of the
-// window are cut into W contiguous shares, each warp stages its entries in
-// shared memory (list_cap each) and the block writes them in warp order, so
-// a list is the same for every W.
+// window are cut into W contiguous shares, each warp stages its entries and
+// the block writes them in warp order, so a list is the same for every W.
+// The staging is shared memory (list_cap entries a warp) without `scratch`;
+// with it, a ring of 64 entries a warp in shared memory whose full runs of
+// 32 go to chunks claimed in the group's row of `scratch` (groups_cap x
+// list_cap entries, the inner slab, which a build invalidates anyway), so
+// that a block needs a few KB, not 4 list_cap x 8 B, and many blocks fit on
+// an SM.
 template <int W, bool BATCH>
 __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFrameDev *__restrict__ frames,
                                                    const int32_t *__restrict__ group_frame,
@@ -204,9 +209,11 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
                                                    const int32_t *__restrict__ excl_off,
                                                    const int32_t *__restrict__ excl,
                                                    int2 *__restrict__ slab, int32_t *__restrict__ counts,
-                                                   int32_t *sizes) {
+                                                   int32_t *sizes, int2 *__restrict__ scratch) {
   constexpr int GPB = 4 / W;  // groups per block
   extern __shared__ int2 s_stage[];
+  __shared__ int2 s_ring[W > 1 ? W : 1][64];
+  __shared__ int s_fill;
   __shared__ float4 s_mem[GPB][NB_GROUP];
   __shared__ int s_atom[GPB][NB_GROUP];
   __shared__ int s_key[GPB][NB_EXCL_MAX];
@@ -313,10 +320,16 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
     }
     __syncwarp();
   }
+  const bool chunked = W > 1 && scratch != nullptr;
+  const int chunk_cap = (int)(P.list_cap / 32) + 1;  // chunk offsets a warp
+  int *chunk_at = chunked ? (int *)s_stage + warp * chunk_cap : nullptr;
+  int2 *ring = s_ring[W > 1 ? warp : 0];
+  int rhead = 0, rn = 0, nchunks = 0;  // the ring's first entry and size; chunks written
+  if (chunked && threadIdx.x == 0) s_fill = 0;
   if (W > 1) __syncthreads();
   else __syncwarp();
   int count = 0;
-  int2 *stage = W > 1 ? s_stage + (size_t)warp * P.list_cap : nullptr;
+  int2 *stage = (W > 1 && !chunked) ? s_stage + (size_t)warp * P.list_cap : nullptr;
   if (live) {
     int nkeys = s_meta[gi][0];
     bool wide = s_meta[gi][1] != 0;
@@ -414,7 +427,24 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
               }
             }
             unsigned has = __ballot_sync(FULL, mask != 0);
-            if (mask) {
+            if (chunked) {
+              if (mask)
+                ring[(rhead + rn + __popc(has & ((1u << lane) - 1))) & 63] =
+                    make_int2((int)pj, (int)(mask | ((unsigned)code << 16)));
+              rn += __popc(has);
+              if (rn >= 32) {  // a full run of 32 to a chunk of the group's scratch row
+                __syncwarp();
+                int claim = 0;
+                if (lane == 0) claim = atomicAdd(&s_fill, 32);
+                claim = __shfl_sync(FULL, claim, 0);
+                if (claim + 32 <= P.list_cap) scratch[g * P.list_cap + claim + lane] = ring[(rhead + lane) & 63];
+                if (lane == 0 && nchunks < chunk_cap) chunk_at[nchunks] = claim + 32 <= P.list_cap ? claim : -1;
+                ++nchunks;
+                rhead = (rhead + 32) & 63;
+                rn -= 32;
+                __syncwarp();
+              }
+            } else if (mask) {
               int at = count + __popc(has & ((1u << lane) - 1));
               int2 en = make_int2((int)pj, (int)(mask | ((unsigned)code << 16)));
               if (at < P.list_cap) {
@@ -446,9 +476,20 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
     if (w < warp) at += s_count[w];
     total += s_count[w];
   }
-  int keep = (int)min((int64_t)count, P.list_cap);
-  for (int i = lane; i < keep; i += 32)
-    if (at + i < P.list_cap) slab[g * P.list_cap + at + i] = stage[i];
+  if (chunked) {
+    // this warp's chunks in the order written, then what its ring holds
+    for (int k = 0; k < nchunks && k < chunk_cap; ++k) {
+      int from = chunk_at[k];
+      int to = at + 32 * k + lane;
+      if (from >= 0 && to < P.list_cap) slab[g * P.list_cap + to] = scratch[g * P.list_cap + from + lane];
+    }
+    int to = at + 32 * nchunks + lane;
+    if (lane < rn && to < P.list_cap) slab[g * P.list_cap + to] = ring[(rhead + lane) & 63];
+  } else {
+    int keep = (int)min((int64_t)count, P.list_cap);
+    for (int i = lane; i < keep; i += 32)
+      if (at + i < P.list_cap) slab[g * P.list_cap + at + i] = stage[i];
+  }
   if (part == 0 && lane == 0) {
     counts[g] = total;
     atomicMax(&sizes[NB_SIZE_LONGEST], total);
@@ -844,6 +885,20 @@ static int64_t nb_initial_list_cap(int64_t n, const double box[3], double reach,
   return ((int64_t)est + NB_UNIT - 1) / NB_UNIT * NB_UNIT;
 }
 
+// Lets `kernel` take `bytes` of dynamic shared memory on the current device
+// beside its static shared memory (the default cap is 48 KB for both
+// together); once per device and size.
+#define NB_MAX_DEVICES 64
+template <typename K>
+static void nb_allow_smem(K kernel, size_t bytes, size_t (&configured)[NB_MAX_DEVICES]) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (bytes > 16 * 1024 && dev >= 0 && dev < NB_MAX_DEVICES && configured[dev] < bytes) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    configured[dev] = bytes;
+  }
+}
+
 // Launches one build on `s`. Returns 0; the sizes are left in c.sizes (device).
 static void nb_build_launch(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
   const NbGrid &G = c.grid;
@@ -881,22 +936,22 @@ static void nb_build_launch(NbCtx &c, const double *x, const double box[3], cuda
   P.Rbox = (float)(Rw + 2e-5 * (box[0] + box[1] + box[2]) + 1e-6);
   P.groups_cap = c.groups_cap;
   P.list_cap = c.list_cap;
-  // four warps a group when their staging fits in shared memory, else one
-  size_t stage = sizeof(int2) * 4 * (size_t)c.list_cap;
+  // four warps a group staging in chunks of the inner slab when it is there
+  // (a dual list), else in shared memory when that fits, else one warp
+  bool chunked = c.slab_in && c.slab_in_entries >= c.groups_cap * c.list_cap;
+  size_t stage = chunked ? sizeof(int) * 4 * (size_t)(c.list_cap / 32 + 1) : sizeof(int2) * 4 * (size_t)c.list_cap;
   if (stage <= 200 * 1024) {
-    static size_t configured = 0;
-    if (stage > 48 * 1024 && configured < stage) {
-      cudaFuncSetAttribute(nb_search_t<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
-      configured = stage;
-    }
+    static size_t configured[NB_MAX_DEVICES] = {};
+    nb_allow_smem(nb_search_t<4, false>, stage, configured);
     nb_search_t<4, false><<<(int)c.groups_cap, 128, stage, s>>>(P, nullptr, nullptr, c.sizes, c.order, c.xw,
                                                                 c.box_lo, c.box_hi, c.group_start, c.excl_off,
-                                                                c.excl, c.slab, c.counts, c.sizes);
+                                                                c.excl, c.slab, c.counts, c.sizes,
+                                                                chunked ? c.slab_in : nullptr);
   } else {
     nb_search_t<1, false><<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, nullptr, nullptr, c.sizes, c.order, c.xw,
                                                                       c.box_lo, c.box_hi, c.group_start,
                                                                       c.excl_off, c.excl, c.slab, c.counts,
-                                                                      c.sizes);
+                                                                      c.sizes, nullptr);
   }
   nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts,
                                                              c.list_cap, c.unit_n);
@@ -914,9 +969,11 @@ void nb_build_launch_public(NbCtx &c, const double *x, const double box[3], cuda
 int nb_reserve_inner(NbCtx &c) {
   // the inner buffers follow the outer capacities
   int64_t G = c.groups_cap, C = c.list_cap, U = c.units_cap;
+  c.slab_in_entries = 0;
   if (nb_realloc(c.slab_in, G * C) || nb_realloc(c.counts_in, G) || nb_realloc(c.unit_n_in, G) ||
       nb_realloc(c.unit_start_in, G + 1) || nb_realloc(c.units_in, U))
     return -1;
+  c.slab_in_entries = G * C;
   if (!c.sizes_in) {
     if (cudaMalloc(&c.sizes_in, sizeof(int32_t) * NB_SIZE_COUNT) != cudaSuccess) return -1;
   }
@@ -929,11 +986,8 @@ void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s) {
   double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2]);
   size_t stage = sizeof(int2) * (size_t)c.list_cap;
   if (stage <= 200 * 1024) {
-    static int configured = 0;
-    if (stage > 48 * 1024 && configured < (int)stage) {
-      cudaFuncSetAttribute(nb_prune_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
-      configured = (int)stage;
-    }
+    static size_t configured[NB_MAX_DEVICES] = {};
+    nb_allow_smem(nb_prune_block, stage, configured);
     nb_prune_block<<<(int)c.groups_cap, NB_PRUNE_WARPS * 32, stage, s>>>(
         c.groups_cap, c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
         c.counts, c.order, c.xq, c.slab_in, c.counts_in, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr);
@@ -998,11 +1052,8 @@ void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double
   double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2]);
   size_t stage = sizeof(int2) * (size_t)c.list_cap;
   if (stage <= 200 * 1024) {
-    static int configured = 0;
-    if (stage > 48 * 1024 && configured < (int)stage) {
-      cudaFuncSetAttribute(nb_prune_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
-      configured = (int)stage;
-    }
+    static size_t configured[NB_MAX_DEVICES] = {};
+    nb_allow_smem(nb_prune_block, stage, configured);
     // outside the deterministic mode the blocks claim their units themselves
     // (the counter is zeroed by the update that asked for the pruning)
     bool claim = !c.deterministic && unit_counter;
@@ -1117,6 +1168,7 @@ int nb_grow_lists_keep(NbCtx &c, int64_t longest, cudaStream_t s) {
   if (inner) {
     cudaFree(c.slab_in);
     c.slab_in = slab_in;
+    c.slab_in_entries = G * want;
   }
   if (units_new) {
     cudaFree(c.units);
@@ -1340,19 +1392,16 @@ static void nb_batch_build_launch(mdrtNbBatch &b, const double *x, cudaStream_t 
   P.list_cap = c.list_cap;
   size_t stage = sizeof(int2) * 4 * (size_t)c.list_cap;
   if (b.search_warps == 4 && stage <= 200 * 1024) {
-    static size_t configured = 0;
-    if (stage > 48 * 1024 && configured < stage) {
-      cudaFuncSetAttribute(nb_search_t<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
-      configured = stage;
-    }
+    static size_t configured[NB_MAX_DEVICES] = {};
+    nb_allow_smem(nb_search_t<4, true>, stage, configured);
     nb_search_t<4, true><<<(int)c.groups_cap, 128, stage, s>>>(P, b.frames_dev, b.group_frame, c.sizes, c.order,
                                                                c.xw, c.box_lo, c.box_hi, c.group_start, c.excl_off,
-                                                               c.excl, c.slab, c.counts, c.sizes);
+                                                               c.excl, c.slab, c.counts, c.sizes, nullptr);
   } else {
     nb_search_t<1, true><<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, b.frames_dev, b.group_frame, c.sizes,
                                                                      c.order, c.xw, c.box_lo, c.box_hi,
                                                                      c.group_start, c.excl_off, c.excl, c.slab,
-                                                                     c.counts, c.sizes);
+                                                                     c.counts, c.sizes, nullptr);
   }
   nb_unit_count<<<blocks_for(c.groups_cap, 256), 256, 0, s>>>(c.groups_cap, c.sizes, c.counts, c.list_cap,
                                                              c.unit_n);

@@ -100,6 +100,7 @@ struct NbCtx {
   bool inner_valid = false;
   int64_t inner_key = -1;  // the outer capacities the inner buffers were sized for
   int2 *slab_in = nullptr;
+  int64_t slab_in_entries = 0;  // the allocation of slab_in (the search stages in it)
   int32_t *counts_in = nullptr;
   int32_t *unit_n_in = nullptr, *unit_start_in = nullptr;
   int2 *units_in = nullptr;

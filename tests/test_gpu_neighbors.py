@@ -73,3 +73,39 @@ def test_reach_beyond_edge_is_refused(cuda):
     with pytest.raises(_lib.NativeError) as e:
         t.build(torch.tensor(x, device="cuda"), [4.0, 4.0, 4.0])
     assert e.value.status == _lib.INVALID_BOX
+
+
+@pytest.mark.parametrize("case", [0, 4, 5, 6, 8, 11])
+def test_lists_staged_in_chunks_are_the_same(cuda, case):
+    """With a dual list the search stages its entries in chunks of the inner
+    slab (from the second build on): the outer lists must be the oracle's
+    set and, entry for entry, the lists of the shared-memory staging."""
+    from mdir_b200 import NonbondedTerm
+    from mdir_b200 import _lib as Lb
+    L, R, deg, poison, n, bits = GROUPS_KAT[case]
+    x, ex = lcg_case(L, R, deg, poison, n)
+    xd = torch.tensor(x, dtype=torch.float64, device="cuda")
+    lists = []
+    for dual in (False, True):
+        t = NonbondedTerm(len(x))
+        t.set_interaction(cutoff=0.5 * R, reach=R, beta=0.0)
+        if ex is not None:
+            t.set_exclusions(rows=ex)
+        if dual:
+            t.set_pruned_reach(0.75 * R)
+        t.build(xd, [L, L, L], allow_nan=poison)
+        sizes = t.build(xd, [L, L, L], allow_nan=poison)  # the second build stages in chunks
+        pairs = t.pair_set(sizes)
+        assert len(pairs) == bits
+        G = sizes[6]
+        cap = t.info()["list_capacity"]
+        e = t.buffer(Lb.SLOT_ENTRIES, np.int32, 2)[: G * cap].copy()
+        c = t.buffer(Lb.SLOT_COUNTS, np.int32)[:G].copy()
+        lists.append((canon(pairs), e, c, cap))
+        t.close()
+    (p1, e1, c1, cap1), (p2, e2, c2, cap2) = lists
+    np.testing.assert_array_equal(p1, p2)
+    np.testing.assert_array_equal(c1, c2)
+    assert cap1 == cap2
+    for g in range(len(c1)):
+        np.testing.assert_array_equal(e1[g * cap1: g * cap1 + c1[g]], e2[g * cap2: g * cap2 + c2[g]])
