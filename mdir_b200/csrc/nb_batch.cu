@@ -133,6 +133,7 @@ int32_t mdrtNbBatchDestroy(mdrtNbBatch *b) {
   bfree(b->group_frame);
   bfree(b->group_L);
   bfree(b->frame_units);
+  bfree(b->search_scratch);
   bfree(b->excl_blk_frame);
   bfree(b->excl_blk_first);
   bfree(b->excl_frame_end);
@@ -365,6 +366,10 @@ int32_t mdrtNbBatchAutotune(mdrtNbBatch *b, const double *x, double *forces, voi
   cudaEventDestroy(e1);
   b->search_warps = best_w;
   c.pair_blocks_per_sm = best_p;
+  if (best_w == 1) {  // a warp a group stages nothing
+    bfree(b->search_scratch);
+    b->search_scratch_entries = 0;
+  }
   drop_graph(b);
   if (choice) {
     choice[0] = best_w;

@@ -1390,13 +1390,16 @@ static void nb_batch_build_launch(mdrtNbBatch &b, const double *x, cudaStream_t 
   SearchParams P = {};
   P.groups_cap = c.groups_cap;
   P.list_cap = c.list_cap;
-  size_t stage = sizeof(int2) * 4 * (size_t)c.list_cap;
+  // four warps a group stage in chunks of the batch's scratch rows
+  bool chunked = b.search_scratch && b.search_scratch_entries >= c.groups_cap * c.list_cap;
+  size_t stage = chunked ? sizeof(int) * 4 * (size_t)(c.list_cap / 32 + 1) : sizeof(int2) * 4 * (size_t)c.list_cap;
   if (b.search_warps == 4 && stage <= 200 * 1024) {
     static size_t configured[NB_MAX_DEVICES] = {};
     nb_allow_smem(nb_search_t<4, true>, stage, configured);
     nb_search_t<4, true><<<(int)c.groups_cap, 128, stage, s>>>(P, b.frames_dev, b.group_frame, c.sizes, c.order,
                                                                c.xw, c.box_lo, c.box_hi, c.group_start, c.excl_off,
-                                                               c.excl, c.slab, c.counts, c.sizes, nullptr);
+                                                               c.excl, c.slab, c.counts, c.sizes,
+                                                               chunked ? b.search_scratch : nullptr);
   } else {
     nb_search_t<1, true><<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(P, b.frames_dev, b.group_frame, c.sizes,
                                                                      c.order, c.xw, c.box_lo, c.box_hi,
@@ -1429,6 +1432,11 @@ int nb_batch_build_run(mdrtNbBatch &b, const double *x, cudaStream_t s) {
     if (c.groups_cap > b.groups_alloc) {
       if (nb_realloc(b.group_frame, c.groups_cap) || nb_realloc(b.group_L, c.groups_cap)) return -1;
       b.groups_alloc = c.groups_cap;
+    }
+    if (b.search_warps == 4 && b.search_scratch_entries < c.groups_cap * c.list_cap) {
+      b.search_scratch_entries = 0;
+      if (nb_realloc(b.search_scratch, c.groups_cap * c.list_cap)) return -1;
+      b.search_scratch_entries = c.groups_cap * c.list_cap;
     }
     nb_batch_build_launch(b, x, s);
     NB_CHECK(cudaMemcpyAsync(c.h_sizes, c.sizes, sizeof(int32_t) * NB_SIZE_COUNT, cudaMemcpyDeviceToHost, s));

@@ -177,6 +177,8 @@ struct mdrtNbBatch {
   float4 *group_L = nullptr;      // per group: the frame's cell
   int64_t groups_alloc = 0, cols_alloc = 0;
   int32_t *frame_units = nullptr; // per frame: first unit, one past the last
+  int2 *search_scratch = nullptr; // the search's chunks with four warps a group (groups_cap x list_cap)
+  int64_t search_scratch_entries = 0;
   std::vector<double> h_boxes;    // frames x 3 of the last build
   // excluded pairs: blocks of 256 pairs that never straddle two frames
   int32_t *excl_blk_frame = nullptr, *excl_blk_first = nullptr, *excl_frame_end = nullptr;
