@@ -49,7 +49,10 @@ struct mdrtMd {
   double *x_prune = nullptr;       // positions at the last pruning (dual list)
   double *ke_part = nullptr;       // per-block kinetic partials
   int ke_blocks = 0;
-  unsigned int *maxd2 = nullptr;   // [0] float bits of max |x - x_ref|^2, [1] of max |x - x_prune|^2, [2] blocks done
+  unsigned int *done_blocks = nullptr;  // blocks of md_update finished (the last one reduces)
+  float2 *blk_max = nullptr;       // per block of md_update: max |x - x_ref|^2, max |x - x_prune|^2
+  int32_t *wplace = nullptr;       // the place of each water atom, by slot 3 w + k (after each build)
+  int32_t *fplace = nullptr;       // the place of each free atom, by its slot
   double *thermo = nullptr;        // [0] lambda, [1] KE, [2] KE before, [3] steps, [4] builds, [5] prunes
   double *noise = nullptr;         // thermostat draws of the steps of one launch (2 a step)
   int *flag = nullptr;             // [0] rebuild, [1] prune: flags for the step-by-step path
@@ -155,10 +158,6 @@ __device__ void settle(const SettleParams &P, Vec3 a0, Vec3 b0, Vec3 c0, Vec3 &a
   c1 = d + (xc3 * ex + yc3 * ey + zc1 * ez);
 }
 
-__device__ __forceinline__ void atomic_max_float(unsigned int *addr, float v) {
-  atomicMax(addr, __float_as_uint(fmaxf(v, 0.f)));  // non-negative floats order as integers
-}
-
 struct UpdateParams {
   SettleParams S;
   double dt;
@@ -193,9 +192,8 @@ struct UpdateParams {
 
 // The force on atom a: the pair / excluded accumulator of its place and the
 // PME force; clears the accumulator for the next step.
-__device__ __forceinline__ Vec3 take_force(int a, const int32_t *__restrict__ place_of, float4 *acc,
-                                           unsigned long long *accf, const float4 *__restrict__ pme, int fixed) {
-  int p = place_of[a];
+__device__ __forceinline__ Vec3 take_force(int p, float4 *acc, unsigned long long *accf,
+                                           const float4 *__restrict__ pme, int fixed) {
   if (p < 0) return {0.0, 0.0, 0.0};
   Vec3 f;
   if (fixed) {
@@ -218,9 +216,8 @@ __device__ __forceinline__ Vec3 take_force(int a, const int32_t *__restrict__ pl
   return f;
 }
 
-__device__ __forceinline__ float4 write_frame(int a, Vec3 x, const int32_t *__restrict__ place_of,
-                                              const char4 *__restrict__ shift, const double *L, float4 *xq) {
-  int p = place_of[a];
+__device__ __forceinline__ float4 write_frame(int p, Vec3 x, const char4 *__restrict__ shift, const double *L,
+                                              float4 *xq) {
   if (p < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
   char4 s = shift[p];
   float4 o = xq[p];
@@ -277,8 +274,8 @@ __device__ __forceinline__ Vec3 md_pme_gather(float4 fr, const float *__restrict
 
 #define MD_UPDATE_THREADS 64
 
-__device__ void md_last_block(const UpdateParams &U, const double *ke_part, int nblocks, double *thermo,
-                              unsigned int *maxd2);
+__device__ void md_last_block(const UpdateParams &U, const double *ke_part, const float2 *blk_max, int nblocks,
+                              double *thermo, unsigned int *counter);
 
 __device__ __forceinline__ Vec3 shfl3(Vec3 a, int src) {
   return {__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src), __shfl_sync(0xffffffffu, a.z, src)};
@@ -300,14 +297,16 @@ __device__ __forceinline__ Vec3 shfl3(Vec3 a, int src) {
 __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     int64_t nwaters, int64_t nfree, const int32_t *__restrict__ waters, const int32_t *__restrict__ free_atoms,
     UpdateParams U, const double *__restrict__ inv_mass, const double *__restrict__ mass,
-    const float *__restrict__ charge, const int32_t *__restrict__ place_of, const char4 *__restrict__ shift,
-    float4 *acc, unsigned long long *accf, const float4 *__restrict__ pme, float4 *xq, double *__restrict__ x,
-    double *__restrict__ v, double *__restrict__ fout, const double *__restrict__ x_ref,
-    const double *__restrict__ x_prune, double *thermo, double *ke_part, unsigned int *maxd2) {
+    const float *__restrict__ charge, const int32_t *__restrict__ wplace, const int32_t *__restrict__ fplace,
+    const char4 *__restrict__ shift, float4 *acc, unsigned long long *accf, const float4 *__restrict__ pme,
+    float4 *xq, double *__restrict__ x, double *__restrict__ v, double *__restrict__ fout,
+    const double *__restrict__ x_ref, const double *__restrict__ x_prune, double *thermo, double *ke_part,
+    float2 *blk_max, unsigned int *counter) {
   __shared__ double s_ke[MD_UPDATE_THREADS / 32];
   __shared__ float s_d2[MD_UPDATE_THREADS / 32], s_p2[MD_UPDATE_THREADS / 32];
   __shared__ int s_last;
-  if (U.flag[3]) return;  // stopped at a stale list: the state stays at that step
+  // read beside the first loads; the state stays at a step that a stale list stopped
+  const int halt = U.flag[3];
   const int WPB = MD_UPDATE_THREADS / 32 * 10;  // waters per block
   int64_t water_blocks = (nwaters + WPB - 1) / WPB;
   double lambda = thermo[0];
@@ -318,12 +317,15 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     int lane = threadIdx.x & 31, wl = lane / 3, k = lane - 3 * (lane / 3);
     int64_t w = ((int64_t)blockIdx.x * (MD_UPDATE_THREADS / 32) + (threadIdx.x >> 5)) * 10 + wl;
     bool act = lane < 30 && w < nwaters;
+    // the atom and its place, both by the water's slot: one memory round
+    // trip before the loads by atom and by place
     int a = act ? waters[3 * w + k] : 0;
+    int p = act ? wplace[3 * w + k] : -1;
+    if (halt) return;
     int base = 3 * wl, s1 = base + (k + 1) % 3, s2 = base + (k + 2) % 3;
     if (lane >= 30) s1 = s2 = base = lane;
     // every independent load first
     Vec3 x0 = load3(x, a), v0 = load3(v, a);
-    int p = act ? place_of[a] : -1;
     double q = charge[a], im = inv_mass[a], ms = mass[a];
     Vec3 xr = load3(x_ref, a);
     Vec3 xpr = U.prune_half2 > 0.0 ? load3(x_prune, a) : xr;
@@ -414,8 +416,9 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
   } else if ((int64_t)(blockIdx.x - water_blocks) * blockDim.x + threadIdx.x < nfree) {
     int64_t t = (int64_t)(blockIdx.x - water_blocks) * blockDim.x + threadIdx.x;
     int i = free_atoms[t];
-    Vec3 fi = take_force(i, place_of, acc, accf, pme, U.fixed);
-    int pi = place_of[i];
+    int pi = fplace[t];
+    if (halt) return;
+    Vec3 fi = take_force(pi, acc, accf, pme, U.fixed);
     if (U.pme_fused && pi >= 0) {
       float4 fr = xq[pi];
       if (fr.w != 0.f) fi = fi + md_pme_gather(fr, U.phi, U.G);
@@ -425,7 +428,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     store3(x, i, xi);
     store3(v, i, vi);
     store3(fout, i, fi);
-    write_frame(i, xi, place_of, shift, U.L, xq);
+    write_frame(pi, xi, shift, U.L, xq);
     ke = 0.5 * mass[i] * dot(vi, vi);
     Vec3 di = xi - load3(x_ref, i);
     d2max = (float)dot(di, di);
@@ -434,6 +437,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
       p2max = (float)dot(di, di);
     }
   }
+  if (halt) return;  // every thread of the grid, the idle ones too: no barrier is reached
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -456,14 +460,13 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
       mp = fmaxf(mp, s_p2[w]);
     }
     ke_part[blockIdx.x] = s;
-    atomic_max_float(maxd2, m);
-    atomic_max_float(maxd2 + 1, mp);
+    blk_max[blockIdx.x] = make_float2(m, mp);  // no contended atomics: the last block reduces them
     __threadfence();
-    unsigned done = atomicAdd(maxd2 + 2, 1u);
+    unsigned done = atomicAdd(counter, 1u);
     s_last = done == gridDim.x - 1;
   }
   __syncthreads();
-  if (s_last) md_last_block(U, ke_part, gridDim.x, thermo, maxd2);
+  if (s_last) md_last_block(U, ke_part, blk_max, gridDim.x, thermo, counter);
 }
 
 // splitmix64 (Steele, Lea & Flood 2014) as a counter-based generator.
@@ -516,19 +519,38 @@ __global__ void md_noise(const double *thermo, double *noise, int count, double 
 // tests of validity (D80 and D114, the cell unchanged):
 // rebuild when 2 max|x - x_build| > R - r_c, prune when rebuilt or
 // 2 max|x - x_prune| > R_in - r_c; they set the conditional nodes.
-__device__ void md_last_block(const UpdateParams &U, const double *ke_part, int nblocks, double *thermo,
-                              unsigned int *maxd2) {
-  __shared__ double s[MD_UPDATE_THREADS];
+__device__ void md_last_block(const UpdateParams &U, const double *ke_part, const float2 *blk_max, int nblocks,
+                              double *thermo, unsigned int *counter) {
+  __shared__ double s_k[MD_UPDATE_THREADS / 32];
+  __shared__ float s_m[MD_UPDATE_THREADS / 32][2];
   double v = 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += __ldcg(ke_part + b);
-  s[threadIdx.x] = v;
-  __syncthreads();
-  for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
-    if ((int)threadIdx.x < stride) s[threadIdx.x] += s[threadIdx.x + stride];
-    __syncthreads();
+  float dmax = 0.f, pmax = 0.f;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    v += __ldcg(ke_part + b);
+    float2 mb = __ldcg(blk_max + b);
+    dmax = fmaxf(dmax, mb.x);
+    pmax = fmaxf(pmax, mb.y);
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+    dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    pmax = fmaxf(pmax, __shfl_xor_sync(0xffffffffu, pmax, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    s_k[threadIdx.x >> 5] = v;
+    s_m[threadIdx.x >> 5][0] = dmax;
+    s_m[threadIdx.x >> 5][1] = pmax;
+  }
+  __syncthreads();
   if (threadIdx.x != 0) return;
-  double K = s[0];
+  double K = 0.0;
+  float d2 = 0.f, p2 = 0.f;
+  for (int w = 0; w < MD_UPDATE_THREADS / 32; ++w) {
+    K += s_k[w];
+    d2 = fmaxf(d2, s_m[w][0]);
+    p2 = fmaxf(p2, s_m[w][1]);
+  }
   thermo[2] = thermo[1];
   thermo[1] = K;
   thermo[3] += 1.0;
@@ -542,8 +564,6 @@ __device__ void md_last_block(const UpdateParams &U, const double *ke_part, int 
     lambda = sqrt(fmax(Knew, 0.0) / K);
   }
   thermo[0] = lambda;
-  float d2 = __uint_as_float(atomicAdd(maxd2, 0u));
-  float p2 = __uint_as_float(atomicAdd(maxd2 + 1, 0u));
   int stale = (double)d2 > U.build_half2 ? 1 : 0;
   int rebuild = 0;
   if (U.check_build) {
@@ -569,14 +589,25 @@ __device__ void md_last_block(const UpdateParams &U, const double *ke_part, int 
   int prune = (U.prune_half2 > 0.0 && (rebuild || (double)p2 > U.prune_half2)) ? 1 : 0;
   // the host's build after a stale list (or, step by step, after a rebuild) prunes too
   if (stale || (!U.use_graph && rebuild)) prune = 0;
-  maxd2[0] = 0u;
-  maxd2[1] = 0u;
-  maxd2[2] = 0u;
+  *counter = 0u;
   U.flag[0] = rebuild;
   U.flag[1] = prune;
   if (prune && U.unit_counter) *U.unit_counter = 0;
   U.flag[2] = stale;
   if (U.use_graph && U.check_build) cudaGraphSetConditional(U.h_any, rebuild);
+}
+
+// After a build: the place of every atom by its slot in the integrator's
+// lists (waters 3 w + k, then the free atoms), which md_update reads beside
+// the slots' atom numbers instead of after them.
+__global__ void md_places(int64_t nw3, int64_t nfree, const int32_t *__restrict__ waters,
+                          const int32_t *__restrict__ free_atoms, const int32_t *__restrict__ place_of,
+                          int32_t *__restrict__ wplace, int32_t *__restrict__ fplace) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nw3)
+    wplace[k] = place_of[waters[k]];
+  else if (k - nw3 < nfree)
+    fplace[k - nw3] = place_of[free_atoms[k - nw3]];
 }
 
 // After a build: the reference positions, the counters, and what the build
@@ -690,9 +721,9 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
   U.host_halt = use_graph ? m.d_halt : nullptr;
   U.unit_counter = c.inner_reach > 0.0 ? md_unit_counter(m) : nullptr;
   md_update<<<m.ke_blocks, MD_UPDATE_THREADS, 0, s>>>(
-      m.nwaters, m.nfree, m.waters, m.free_atoms, U, m.inv_mass, m.mass, c.q, c.place_of, c.shift, c.acc,
+      m.nwaters, m.nfree, m.waters, m.free_atoms, U, m.inv_mass, m.mass, c.q, m.wplace, m.fplace, c.shift, c.acc,
       c.acc_fixed, (pme && !fused) ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref,
-      m.x_prune, m.thermo, m.ke_part, m.maxd2);
+      m.x_prune, m.thermo, m.ke_part, m.blk_max, m.done_blocks);
 }
 
 // A pruning at x on `s` (frames current): the inner lists and their units.
@@ -710,11 +741,20 @@ static void md_prune_step(mdrtMd &m, const double *x, const double box[3], cudaS
     nb_prune_gated(c, box, m.flag + 1, x, m.x_prune, m.thermo + 5, md_unit_counter(m), s);
 }
 
+// The places by slot after a build (md_places).
+static void md_refresh_places(mdrtMd &m, cudaStream_t s) {
+  int64_t total = 3 * m.nwaters + m.nfree;
+  if (total > 0)
+    md_places<<<blocks_for(total, 256), 256, 0, s>>>(3 * m.nwaters, m.nfree, m.waters, m.free_atoms,
+                                                    m.nb->place_of, m.wplace, m.fplace);
+}
+
 // A build at x on `s` without a host wait (the body of the conditional node).
 static void md_rebuild_body(mdrtMd &m, const double *x, const double box[3], cudaStream_t s) {
   NbCtx &c = *m.nb;
   nb_build_launch_public(c, x, box, s);
   nb_gather_frames(c, x, box, s);
+  md_refresh_places(m, s);
   md_after_build<<<blocks_for(3 * m.n, 256), 256, 0, s>>>(3 * m.n, x, m.x_ref, m.thermo, c.sizes, c.status,
                                                           m.peak);
 }
@@ -781,7 +821,8 @@ static void md_free(mdrtMd *m) {
   if (m->side) cudaStreamDestroy(m->side);
   for (void *p : {(void *)m->inv_mass, (void *)m->mass, (void *)m->waters, (void *)m->free_atoms,
                   (void *)m->excl_other, (void *)m->force, (void *)m->x_ref, (void *)m->x_prune,
-                  (void *)m->ke_part, (void *)m->maxd2, (void *)m->thermo, (void *)m->flag,
+                  (void *)m->ke_part, (void *)m->done_blocks, (void *)m->blk_max,
+                  (void *)m->wplace, (void *)m->fplace, (void *)m->thermo, (void *)m->flag,
                   (void *)m->noise, (void *)m->x_ck, (void *)m->v_ck, (void *)m->thermo_ck, (void *)m->peak,
                   (void *)m->xref_ck, (void *)m->xprune_ck, (void *)m->qgrid, (void *)m->phi, (void *)m->qfixed,
                   (void *)m->spec, (void *)m->influence})
@@ -877,7 +918,10 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
             cudaMalloc(&m->x_ref, sizeof(double) * 3 * c.n) == cudaSuccess &&
             cudaMalloc(&m->x_prune, sizeof(double) * 3 * c.n) == cudaSuccess &&
             cudaMalloc(&m->ke_part, sizeof(double) * m->ke_blocks) == cudaSuccess &&
-            cudaMalloc(&m->maxd2, sizeof(unsigned int) * 4) == cudaSuccess &&
+            cudaMalloc(&m->done_blocks, sizeof(unsigned int)) == cudaSuccess &&
+            cudaMalloc(&m->blk_max, sizeof(float2) * m->ke_blocks) == cudaSuccess &&
+            cudaMalloc(&m->wplace, sizeof(int32_t) * std::max<int64_t>(3 * nwaters, 1)) == cudaSuccess &&
+            cudaMalloc(&m->fplace, sizeof(int32_t) * std::max<int64_t>(m->nfree, 1)) == cudaSuccess &&
             cudaMalloc(&m->thermo, sizeof(double) * 8) == cudaSuccess &&
             cudaMalloc(&m->noise, sizeof(double) * 2 * MD_MAX_UNROLL) == cudaSuccess &&
             cudaMalloc(&m->flag, sizeof(int) * 4) == cudaSuccess &&
@@ -908,7 +952,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
     cudaMemcpy(m->excl_other, other.data(), sizeof(int32_t) * other.size(), cudaMemcpyHostToDevice);
   double th[8] = {1.0, 0, 0, 0, 0, 0, 0, 0};
   cudaMemcpy(m->thermo, th, sizeof(th), cudaMemcpyHostToDevice);
-  cudaMemset(m->maxd2, 0, sizeof(unsigned int) * 4);
+  cudaMemset(m->done_blocks, 0, sizeof(unsigned int));
   cudaMemset(m->peak, 0, sizeof(int32_t) * 4);
   cudaMemset(m->flag, 0, sizeof(int) * 4);
   cudaMemset(m->force, 0, sizeof(double) * 3 * c.n);
@@ -957,6 +1001,7 @@ int32_t mdrtMdBuild(mdrtMd *m, const double *x, const double box[3], void *strea
   if (sizes[NB_SIZE_LONGEST] > NB_GROW_AHEAD * c.list_cap && nb_grow_lists_keep(c, sizes[NB_SIZE_LONGEST], st))
     return MDRT_NB_CUDA_ERROR;
   nb_gather_frames(c, x, box, st);
+  md_refresh_places(*m, st);
   if (md_pme_buffers(m)) return MDRT_NB_CUDA_ERROR;
   md_after_build<<<blocks_for(3 * m->n, 256), 256, 0, st>>>(3 * m->n, x, m->x_ref, m->thermo, c.sizes, c.status,
                                                             m->peak);
@@ -1041,6 +1086,7 @@ static int32_t md_restore(mdrtMd *m, double *x, double *v, const double box[3], 
     return MDRT_NB_CUDA_ERROR;
   int32_t s = mdrtNbBuild(m->handle, m->xref_ck, m->n, box, 0.0, stream, nullptr);
   if (s) return s;
+  md_refresh_places(*m, st);
   if (cudaMemcpyAsync(m->x_ref, m->xref_ck, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
     return MDRT_NB_CUDA_ERROR;
   if (dual) {
@@ -1131,6 +1177,7 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
   cudaSetDevice(c.device);
   cudaStream_t st = (cudaStream_t)stream;
   if (md_influence(m, box, st)) return MDRT_NB_CUDA_ERROR;
+  md_refresh_places(*m, st);  // the term may have been built without the integrator
   if (unroll <= 0) return md_run_steps(m, x, v, box, dt, steps, unroll < 0 ? -unroll : MD_WINDOW, stream);
   // Runs of step graphs.  Each run starts from a checkpoint (positions,
   // velocities, thermostat state, and the positions the lists in force were
