@@ -275,7 +275,7 @@ int32_t mdrtMdDestroy(mdrtMd *md);
  * step starts unscaled. */
 int32_t mdrtMdSetThermostat(mdrtMd *md, double temperature, double tau, uint64_t seed);
 /* The look-ahead of the rebuild decision: the drift's growth over the window
- * that ended is extrapolated `factor` times (default 1; 0: none).  A drift
+ * that ended is extrapolated `factor` times (default 1.5; 0: none).  A drift
  * past half the skin before the next decision stops the step (the steps
  * after it do nothing) and the host rebuilds there, so a smaller factor
  * costs stops, never a missed pair.  No MDIR counterpart: MDIR tests every

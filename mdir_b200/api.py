@@ -148,6 +148,7 @@ class Execution:
         self.step_graph = True
         self.graph_steps = 10
         self.pair_sms = 0  # SMs the pair kernel spans (0: all); the others are left to PME
+        self.pair_blocks_per_sm = 0  # blocks of the pair kernel an SM (0: the library's default, 4)
 
 
 class Schedule:
@@ -264,6 +265,8 @@ def _make_term(program):
         t.set_pruned_reach(p["pruned_reach"])
     if program.execution.pair_sms:
         t.set_tuning(pair_sms=program.execution.pair_sms)
+    if program.execution.pair_blocks_per_sm:
+        t.set_tuning(pair_blocks_per_sm=program.execution.pair_blocks_per_sm)
     return t
 
 

@@ -65,7 +65,7 @@ struct mdrtMd {
   double *h_steps = nullptr;       // pinned: the step counter at the checkpoint and after the run
   int64_t regrows = 0;             // runs redone after an overflow inside the graphs
   int64_t redone = 0;              // stops at a drift past half the skin between two decisions
-  double lookahead = 1.0;          // mdrtMdSetLookahead
+  double lookahead = 1.5;          // mdrtMdSetLookahead
   // PME gathered by the update (order 4): the step's side stream spreads the
   // frames into qgrid (through qfixed in the deterministic mode) and
   // transforms qgrid -> spec -> phi; the update gathers each atom's PME force
@@ -664,6 +664,15 @@ static int32_t *md_unit_counter(mdrtMd &m) {
   return (c.deterministic || !c.sizes_in) ? nullptr : c.sizes_in + NB_SIZE_UNITS;
 }
 
+// The pruning of a step when the update before it asked for it (flag[1],
+// on the device): one launch (two in the deterministic mode) that does
+// nothing otherwise, no conditional node.
+static void md_prune_step(mdrtMd &m, const double *x, const double box[3], cudaStream_t s) {
+  NbCtx &c = *m.nb;
+  if (c.inner_reach > 0.0)
+    nb_prune_gated(c, box, m.flag + 1, x, m.x_prune, m.thermo + 5, md_unit_counter(m), s);
+}
+
 // One step on `s` from the frames xq of the current positions x.
 static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], double dt, cudaStream_t s,
                          cudaGraphConditionalHandle h_any, int use_graph, int *flag, int k, int check_build,
@@ -679,6 +688,9 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
     else
       nb_pme_run(c, box, false, false, m.side);
   }
+  // the pruning that the last update asked for, beside the PME chain (it
+  // needs only the frames, and the pair kernel after it needs its lists)
+  md_prune_step(m, x, box, s);
   nb_pairs_run(c, box, false, s, flag + 3);
   if (m.n_excl_other > 0) nb_excluded_list_run(c, box, m.excl_other, m.n_excl_other, s);
   if (pme) {
@@ -733,12 +745,13 @@ static void md_prune_body(mdrtMd &m, const double *x, const double box[3], cudaS
   md_after_prune<<<blocks_for(3 * m.n, 256), 256, 0, s>>>(3 * m.n, x, m.x_prune, m.thermo);
 }
 
-// The pruning of a step when the update asked for it (flag[1], on the
-// device): two launches that do nothing otherwise, no conditional node.
-static void md_prune_step(mdrtMd &m, const double *x, const double box[3], cudaStream_t s) {
-  NbCtx &c = *m.nb;
-  if (c.inner_reach > 0.0)
-    nb_prune_gated(c, box, m.flag + 1, x, m.x_prune, m.thermo + 5, md_unit_counter(m), s);
+
+// The pruning that the last step asked for, at the end of a run, so that
+// the lists in force are valid at the positions the run leaves; no step
+// after it prunes again.
+static void md_flush_prune(mdrtMd &m, const double *x, const double box[3], cudaStream_t s) {
+  md_prune_step(m, x, box, s);
+  cudaMemsetAsync(m.flag + 1, 0, sizeof(int), s);
 }
 
 // The places by slot after a build (md_places).
@@ -788,8 +801,11 @@ static int md_pme_buffers(mdrtMd *m) {
       cudaMalloc(&m->spec, sizeof(float2) * half) != cudaSuccess ||
       cudaMalloc(&m->influence, sizeof(float) * half) != cudaSuccess)
     return -1;
-  // the fixed-point grid starts empty; each step's conversion empties it again
-  if (cudaMemset(m->qfixed, 0, sizeof(unsigned long long) * pts) != cudaSuccess) return -1;
+  // the grids start empty; each chain empties them again (the fixed-point
+  // grid by its conversion, the f32 grid by the spectrum scaling)
+  if (cudaMemset(m->qfixed, 0, sizeof(unsigned long long) * pts) != cudaSuccess ||
+      cudaMemset(m->qgrid, 0, sizeof(float) * pts) != cudaSuccess)
+    return -1;
   m->pme_points = pts;
   return 0;
 }
@@ -1010,6 +1026,7 @@ int32_t mdrtMdBuild(mdrtMd *m, const double *x, const double box[3], void *strea
     c.inner_valid = true;
     c.prunes++;
   }
+  cudaMemsetAsync(m->flag + 1, 0, sizeof(int), st);  // pruned here: none due
   return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
 }
 
@@ -1058,7 +1075,6 @@ static int32_t md_run_steps(mdrtMd *m, double *x, double *v, const double box[3]
     md_noise<<<1, 32, 0, st>>>(m->thermo, m->noise, 1, (double)m->ndof, m->seed);
     int check = (kw + 1) % window == 0 ? 1 : 0;
     md_step_body(*m, x, v, box, dt, st, 0, 0, m->flag, 0, check, window);
-    md_prune_step(*m, x, box, st);
     cudaMemcpyAsync(h_flag, m->flag, sizeof(h_flag), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return MDRT_NB_CUDA_ERROR;
     ++kw;
@@ -1071,6 +1087,7 @@ static int32_t md_run_steps(mdrtMd *m, double *x, double *v, const double box[3]
       }
     }
   }
+  md_flush_prune(*m, x, box, st);
   return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
 }
 
@@ -1094,6 +1111,7 @@ static int32_t md_restore(mdrtMd *m, double *x, double *v, const double box[3], 
     md_prune_body(*m, m->xprune_ck, box, st);
     c.inner_valid = true;
   }
+  cudaMemsetAsync(m->flag + 1, 0, sizeof(int), st);  // a run starts with no pruning due
   nb_gather_frames(c, x, box, st);
   // the counters of the checkpoint: the build and pruning above redo ones it had
   if (cudaMemcpyAsync(m->thermo, m->thermo_ck, sizeof(double) * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
@@ -1135,7 +1153,6 @@ static int32_t md_prepare_graph(mdrtMd *m, double *x, double *v, const double bo
       }
       md_step_body(*m, x, v, box, dt, cap, m->handles[0], 1, m->flag, k, last ? 1 : 0, unroll);
       if (last) e = md_capture_if(cap, body, m->handles[0], [&](cudaStream_t b) { md_rebuild_body(*m, x, box, b); });
-      if (e == cudaSuccess) md_prune_step(*m, x, box, cap);
     }
     cudaGraph_t graph = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
@@ -1248,6 +1265,7 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
       return MDRT_NB_CUDA_ERROR;
     left -= launches * unroll;
   }
+  md_flush_prune(*m, x, box, st);
   if (left > 0) return md_run_steps(m, x, v, box, dt, left, unroll, stream);
   return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
 }

@@ -116,11 +116,15 @@ __global__ void nb_influence(ConvParams C, const float *__restrict__ moduli, flo
 }
 
 // The convolution of the MD step: the spectrum times the influence table
-// (forces only, no energy sums).
+// (forces only, no energy sums).  With `grid`, it also empties the charge
+// grid that the forward transform has read (total points), for the next
+// step's spreading: no memset launch on the chain.
 __global__ void nb_scale_spectrum(int64_t half, const float *__restrict__ influence, float2 *__restrict__ spec,
-                                  const int *halt) {
-  if (halt && *halt) return;  // the MD step stopped at a stale list
+                                  float *__restrict__ grid, int64_t total, const int *halt) {
+  if (halt && *halt) return;  // the MD step stopped at a stale list (it spread nothing either)
   int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (grid)
+    for (int64_t i = k; i < total; i += half) grid[i] = 0.f;
   if (k >= half) return;
   float2 v = spec[k];
   float b = influence[k];
@@ -994,14 +998,15 @@ int nb_pme_md_chain(NbCtx &c, const double box[3], float *qgrid, unsigned long l
                                                                 qfixed, halt);
     nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, qfixed, qgrid);
   } else {
-    cudaMemsetAsync(qgrid, 0, sizeof(float) * total, s);
+    // the grid is empty: the spectrum scaling of the last chain emptied it
     nb_spread<4, false><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, qgrid,
                                                                  qfixed, halt);
   }
   cufftSetStream(P.fwd, s);
   cufftSetStream(P.bwd, s);
   if (cufftExecR2C(P.fwd, qgrid, (cufftComplex *)spec) != CUFFT_SUCCESS) return -3;
-  nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, influence, spec, halt);
+  nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, influence, spec,
+                                                          c.deterministic ? nullptr : qgrid, total, halt);
   if (cufftExecC2R(P.bwd, (cufftComplex *)spec, phi) != CUFFT_SUCCESS) return -3;
   return 0;
 }

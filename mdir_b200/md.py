@@ -45,7 +45,7 @@ class Integrator:
         L.check(L.lib().mdrtMdSetThermostat(self._h, temperature, tau, seed), "mdrtMdSetThermostat")
 
     def lookahead(self, factor):
-        """The rebuild decision's extrapolation of the drift (default 1)."""
+        """The rebuild decision's extrapolation of the drift (default 1.5)."""
         L.check(L.lib().mdrtMdSetLookahead(self._h, float(factor)), "mdrtMdSetLookahead")
 
     def build(self, x, box, stream=None):
@@ -71,54 +71,66 @@ class Integrator:
         L.check(L.lib().mdrtMdForces(self._h, ctypes.byref(p)), "mdrtMdForces")
         return p.value
 
-    def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(1.025, 1.05), pair_sms=(0, 128),
-             steps=200, reps=3, stream=None):
-        """The autotuner of the step: times `reps` runs of `steps` steps for
-        every outer reach, pruned reach and span of the pair grid (SMs; the
-        others are left to the PME kernels beside it), keeps the fastest and
-        builds for it.  x and v are put back; the step counter and the
-        thermostat's noise move on.  MDIR searches its reaches the same way
-        (the skins search, D281, lib/Compiler/Skins.cpp).  Returns the choice
-        with its time per step (µs)."""
+    def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(1.025, 1.05),
+             pair_sms=(0, 112, 128, 136), pair_blocks=(4, 3), steps=400, reps=3, stream=None):
+        """The autotuner of the step, in two stages: the outer and pruned
+        reaches first (the launch shapes as set), then the span of the pair
+        grid (SMs; the others are left to the PME kernels beside it) and its
+        blocks per SM at the reaches kept.  Each choice is timed as `reps`
+        runs of `steps` steps after a build and half as many untimed steps;
+        the fastest is kept and built for.  x and v are put back; the step
+        counter and the thermostat's noise move on.  MDIR searches its
+        reaches the same way (the skins search, D281,
+        lib/Compiler/Skins.cpp).  Returns the choice with its time per step
+        (µs)."""
         t = self.term
         cutoff = t.interaction["cutoff"]
         least = float(np.min(np.asarray(box, dtype=np.float64)))
         keep_x, keep_v = x.clone(), v.clone()
         st = stream if stream is not None else torch.cuda.current_stream(x.device)
+
+        def trial(R, Rin, sms, blocks):
+            t.set_reach(R)
+            t.set_pruned_reach(Rin)
+            t.set_tuning(pair_sms=sms, pair_blocks_per_sm=blocks)
+            x.copy_(keep_x)
+            v.copy_(keep_v)
+            self.build(x, box, stream=st)
+            self.run(x, v, box, dt, steps // 2, unroll=10, stream=st)
+            ms = []
+            for _ in range(reps):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                self.run(x, v, box, dt, steps, unroll=10, stream=st)
+                b.record(st)
+                b.synchronize()
+                ms.append(a.elapsed_time(b) / steps)
+            return float(np.median(ms)) * 1e3
+
+        sms0 = getattr(t, "pair_sms", 0)
+        blocks0 = getattr(t, "pair_blocks_per_sm", 4)
         trials = []
         for R in reaches:
             if not R < 0.999 * least:
                 continue
             for Rin in pruned:
-                if not cutoff <= Rin < R:
-                    continue
-                for sms in pair_sms:
-                    t.set_reach(R)
-                    t.set_pruned_reach(Rin)
-                    t.set_tuning(pair_sms=sms)
-                    x.copy_(keep_x)
-                    v.copy_(keep_v)
-                    self.build(x, box, stream=st)
-                    self.run(x, v, box, dt, steps // 2, unroll=10, stream=st)
-                    ms = []
-                    for _ in range(reps):
-                        a = torch.cuda.Event(enable_timing=True)
-                        b = torch.cuda.Event(enable_timing=True)
-                        a.record(st)
-                        self.run(x, v, box, dt, steps, unroll=10, stream=st)
-                        b.record(st)
-                        b.synchronize()
-                        ms.append(a.elapsed_time(b) / steps)
-                    trials.append((float(np.median(ms)) * 1e3, R, Rin, sms))
-        us, R, Rin, sms = min(trials)
+                if cutoff <= Rin < R:
+                    trials.append((trial(R, Rin, sms0, blocks0), R, Rin, sms0, blocks0))
+        _, R, Rin, _, _ = min(trials)
+        for sms in pair_sms:
+            for blocks in pair_blocks:
+                if (sms, blocks) != (sms0, blocks0):
+                    trials.append((trial(R, Rin, sms, blocks), R, Rin, sms, blocks))
+        us, R, Rin, sms, blocks = min(t_ for t_ in trials if t_[1] == R and t_[2] == Rin)
         t.set_reach(R)
         t.set_pruned_reach(Rin)
-        t.set_tuning(pair_sms=sms)
+        t.set_tuning(pair_sms=sms, pair_blocks_per_sm=blocks)
         x.copy_(keep_x)
         v.copy_(keep_v)
         self.build(x, box, stream=st)
-        return {"reach": R, "pruned_reach": Rin, "pair_sms": sms, "us_per_step": round(us, 2),
-                "trials": len(trials)}
+        return {"reach": R, "pruned_reach": Rin, "pair_sms": sms, "pair_blocks_per_sm": blocks,
+                "us_per_step": round(us, 2), "trials": len(trials)}
 
     def temperature(self, stream=None):
         t = self.thermo(stream)

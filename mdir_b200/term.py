@@ -60,6 +60,7 @@ class NonbondedTerm:
         self.interaction = None
         self.pruned = 0.0
         self.pair_sms = 0
+        self.pair_blocks_per_sm = 4
 
     def close(self):
         if getattr(self, "_h", None):
@@ -122,6 +123,7 @@ class NonbondedTerm:
         if pair_blocks_per_sm is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_BLOCKS_PER_SM, int(pair_blocks_per_sm)),
                     "mdrtNbSetTuning")
+            self.pair_blocks_per_sm = int(pair_blocks_per_sm)
         if pair_sms is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_SMS, int(pair_sms)), "mdrtNbSetTuning")
             self.pair_sms = int(pair_sms)

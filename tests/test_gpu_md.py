@@ -188,3 +188,31 @@ def test_stops_at_a_stale_list_equal_the_host_rebuilding_at_once(cuda):
     assert th1["redone"] > 0 and th1["redone"] == th2["redone"]
     assert th1["builds"] == th2["builds"]
     assert torch.equal(x1, x2) and torch.equal(v1, v2)
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_forces_of_a_step_are_the_oracle_forces(cuda, deterministic):
+    """The forces that a step of the graphs used (pairs over the pruned
+    lists, the excluded correction inside the update, PME through the step's
+    own chain and the update's gather), at the positions the step started
+    from, against the FP64 oracle there."""
+    import ctypes
+    from mdir_b200.term import _cudart
+    s = systems.tip3p(waters=700, seed=29)
+    s["reach"] = 1.3
+    t, md, x, v = setup(s, deterministic=deterministic, tau=0.1)
+    t.set_pruned_reach(1.0)
+    md.build(x, s["box"])
+    md.run(x, v, s["box"], 0.002, 200, unroll=10)  # rebuilds and prunings inside the graphs
+    x0 = x.cpu().numpy()
+    md.run(x, v, s["box"], 0.002, 1, unroll=0)  # one step from x0
+    n = len(s["charges"])
+    f = np.empty((n, 3))
+    torch.cuda.synchronize()
+    res = _cudart().cudaMemcpy(ctypes.c_void_p(f.ctypes.data), ctypes.c_void_p(md.forces()),
+                               ctypes.c_size_t(f.nbytes), 2)
+    assert int(res) == 0
+    ref = O.evaluate(s, x0)["forces"]
+    err = np.sqrt(np.mean(np.sum((f - ref) ** 2, 1)) / np.mean(np.sum(ref ** 2, 1)))
+    assert err < 1e-5, err
+    assert md.thermo()["prunes"] > 0 and t.status() == 0
