@@ -559,7 +559,9 @@ def main():
         hv.copy_(sim.v, non_blocking=True)
         torch.cuda.synchronize(dev)
 
-    for _ in range(2):
+    # warm-up: the first runs of a new context capture its step graph and may
+    # grow its lists once ahead of need
+    for _ in range(5):
         e2e_step()
     e_steps = max(3, args.steps // 2)
     t0 = time.perf_counter()

@@ -657,6 +657,7 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
   const unsigned FULL = 0xffffffffu;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int64_t g = blockIdx.x;
+  nb_grid_wait();  // the gate and the frames of the kernels before (a chained launch)
   if (gate && *gate == 0) return;  // no pruning due (decided on the device)
   if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
   if (x_prune && threadIdx.x < 3 * NB_GROUP) {  // the positions of the pruning, for its test of validity
@@ -1057,10 +1058,11 @@ void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double
     // outside the deterministic mode the blocks claim their units themselves
     // (the counter is zeroed by the update that asked for the pruning)
     bool claim = !c.deterministic && unit_counter;
-    nb_prune_block<<<(int)c.groups_cap, NB_PRUNE_WARPS * 32, stage, s>>>(
-        c.groups_cap, c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
-        c.counts, c.order, c.xq, c.slab_in, c.counts_in, gate, x, x_prune, claim ? unit_counter : nullptr,
-        claim ? c.units_in : nullptr, c.units_cap, claim ? prunes : nullptr);
+    nb_launch_chained(nb_prune_block, dim3((int)c.groups_cap), dim3(NB_PRUNE_WARPS * 32), stage, s, c.groups_cap,
+                      c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+                      c.counts, c.order, c.xq, c.slab_in, c.counts_in, gate, x, x_prune,
+                      claim ? unit_counter : nullptr, claim ? c.units_in : nullptr, c.units_cap,
+                      claim ? prunes : nullptr);
     if (claim) return;
   } else {
     nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],

@@ -72,3 +72,29 @@ __device__ __forceinline__ void nb_decode_image(int code, int &sx, int &sy, int 
 #define NB_FORCE_SCALE_INV (1.0 / 4294967296.0)
 // Fixed-point scale of the deterministic PME grid: 2^40 per e.
 #define NB_GRID_SCALE 1099511627776.0
+
+// Programmatic dependent launch (sm_90 and newer): a kernel launched with
+// nb_launch_chained may start while the kernel before it on its stream is
+// finishing; it calls nb_grid_wait() before it reads anything that kernel
+// (or one before it) writes, and every such kernel waits in at least one
+// thread, so that its completion still implies theirs.  The wait is a no-op
+// for a kernel launched the ordinary way.  In a captured graph the launch
+// becomes a programmatic edge, which hides most of the launch gap between
+// the dependent kernels of the MD step.
+__device__ __forceinline__ void nb_grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+static inline cudaError_t nb_launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                            cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}

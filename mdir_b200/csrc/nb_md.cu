@@ -321,18 +321,20 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     // trip before the loads by atom and by place
     int a = act ? waters[3 * w + k] : 0;
     int p = act ? wplace[3 * w + k] : -1;
-    if (halt) return;
     int base = 3 * wl, s1 = base + (k + 1) % 3, s2 = base + (k + 2) % 3;
     if (lane >= 30) s1 = s2 = base = lane;
-    // every independent load first
+    // every load that the pair kernel before does not write first (on a
+    // chained launch they overlap its last blocks), then the wait
     Vec3 x0 = load3(x, a), v0 = load3(v, a);
     double q = charge[a], im = inv_mass[a], ms = mass[a];
     Vec3 xr = load3(x_ref, a);
     Vec3 xpr = U.prune_half2 > 0.0 ? load3(x_prune, a) : xr;
+    char4 sh = p >= 0 ? shift[p] : make_char4(0, 0, 0, 0);
+    float4 fr = p >= 0 ? xq[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    nb_grid_wait();
+    if (halt) return;
     Vec3 f = {0.0, 0.0, 0.0};
-    char4 sh = make_char4(0, 0, 0, 0);
     float qw = 0.f;
-    float4 fr = make_float4(0.f, 0.f, 0.f, 0.f);
     if (p >= 0) {
       if (U.fixed) {
         long long fx = (long long)accf[3 * p], fy = (long long)accf[3 * p + 1], fz = (long long)accf[3 * p + 2];
@@ -347,8 +349,6 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
         f.y += w4.y;
         f.z += w4.z;
       }
-      sh = shift[p];
-      fr = xq[p];
       qw = fr.w;
       if (U.pme_fused && qw != 0.f) {
         Vec3 fg = md_pme_gather(fr, U.phi, U.G);
@@ -417,6 +417,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     int64_t t = (int64_t)(blockIdx.x - water_blocks) * blockDim.x + threadIdx.x;
     int i = free_atoms[t];
     int pi = fplace[t];
+    nb_grid_wait();
     if (halt) return;
     Vec3 fi = take_force(pi, acc, accf, pme, U.fixed);
     if (U.pme_fused && pi >= 0) {
@@ -437,6 +438,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
       p2max = (float)dot(di, di);
     }
   }
+  nb_grid_wait();
   if (halt) return;  // every thread of the grid, the idle ones too: no barrier is reached
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -732,10 +734,10 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
   U.phi = m.phi;
   U.host_halt = use_graph ? m.d_halt : nullptr;
   U.unit_counter = c.inner_reach > 0.0 ? md_unit_counter(m) : nullptr;
-  md_update<<<m.ke_blocks, MD_UPDATE_THREADS, 0, s>>>(
-      m.nwaters, m.nfree, m.waters, m.free_atoms, U, m.inv_mass, m.mass, c.q, m.wplace, m.fplace, c.shift, c.acc,
-      c.acc_fixed, (pme && !fused) ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref,
-      m.x_prune, m.thermo, m.ke_part, m.blk_max, m.done_blocks);
+  nb_launch_chained(md_update, dim3(m.ke_blocks), dim3(MD_UPDATE_THREADS), 0, s, m.nwaters, m.nfree, m.waters,
+                    m.free_atoms, U, m.inv_mass, m.mass, c.q, m.wplace, m.fplace, c.shift, c.acc, c.acc_fixed,
+                    (pme && !fused) ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref,
+                    m.x_prune, m.thermo, m.ke_part, m.blk_max, m.done_blocks);
 }
 
 // A pruning at x on `s` (frames current): the inner lists and their units.

@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
                                                 float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
                                                 double *__restrict__ partials, int *__restrict__ status,
                                                 const int *halt) {
+  nb_grid_wait();  // the lists and frames of the kernels before (a chained launch)
   if (halt && *halt) return;  // the MD step stopped at a stale list (its host rebuilds)
   __shared__ float4 s_x[8][2 * NB_GROUP];
   __shared__ float2 s_f[8][2 * NB_GROUP];  // LJM 1: member factors
@@ -817,9 +818,10 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, co
   const int2 *lunits = inner ? c.units_in : c.units;
   const int2 *lslab = inner ? c.slab_in : c.slab;
   const int32_t *lcounts = inner ? c.counts_in : c.counts;
-#define NB_LAUNCH2(E, F, S, M)                                                                         \
-  nb_pairs<E, F, S, M><<<grid, 256, 0, s>>>(P, nullptr, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, \
-                                           c.ljf, c.acc, c.acc_fixed, c.unit_partials, c.status, halt)
+#define NB_LAUNCH2(E, F, S, M)                                                                            \
+  nb_launch_chained(nb_pairs<E, F, S, M>, dim3(grid), dim3(256), 0, s, P, (const float4 *)nullptr, lsizes,  \
+                    lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed, c.unit_partials, \
+                    c.status, halt)
 #define NB_LAUNCH(E, F, S)      \
   do {                          \
     if (c.lj_geom)              \
