@@ -214,6 +214,8 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
   extern __shared__ int2 s_stage[];
   __shared__ int2 s_ring[W > 1 ? W : 1][64];
   __shared__ int s_fill;
+  __shared__ int4 s_qi[4][64];    // a warp's queue: place, atom, image code, member bound | same group
+  __shared__ float4 s_qx[4][64];  // and the place's frame
   __shared__ float4 s_mem[GPB][NB_GROUP];
   __shared__ int s_atom[GPB][NB_GROUP];
   __shared__ int s_key[GPB][NB_EXCL_MAX];
@@ -345,6 +347,99 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
     int nx = kx1 - kx0 + 1, nwin = (ky1 - ky0 + 1) * nx;
     int w0 = (int)((int64_t)nwin * part / W), w1 = (int)((int64_t)nwin * (part + 1) / W);
 
+    // Places of the candidate groups that pass the test against this
+    // group's box wait in a queue of 64 a warp; the member tests then run a
+    // place a lane over 32 of them at once, in queue order (the order of the
+    // window, so the list is the one of testing every place), and no lane
+    // idles on a place that the box test dropped.
+    int4 *qi = s_qi[warp];
+    float4 *qx = s_qx[warp];
+    int qh = 0, qn = 0;  // the queue's first entry and size (warp-uniform)
+    auto drain = [&](int take) {
+      __syncwarp();
+      unsigned mask = 0;
+      int pj = 0, code = 0;
+      if (lane < take) {
+        int4 e = qi[(qh + lane) & 63];
+        float4 xj = qx[(qh + lane) & 63];
+        pj = e.x;
+        int aj = e.y;
+        code = e.z;
+        int uu = e.w & 15;
+        bool same = ((e.w >> 4) & 1) != 0;
+        int sx, sy, sz;
+        nb_decode_image(code, sx, sy, sz);
+        float fsx = (float)sx * P.Lx, fsy = (float)sy * P.Ly, fsz = (float)sz * P.Lz;
+#pragma unroll 4
+        for (int m = 0; m < NB_GROUP; ++m) {
+          float4 xm = s_mem[gi][m];
+          int am = s_atom[gi][m];
+          // canonical orientation: A = smaller atom number
+          bool jfirst = aj < am;
+          float4 xa = jfirst ? xj : xm;
+          float4 xb = jfirst ? xm : xj;
+          float sgn = jfirst ? -1.f : 1.f;
+          float r2 = nb_pair_r2(xa, xb, sgn * fsx, sgn * fsy, sgn * fsz);
+          bool ok = (xm.w != 0.f) && (r2 <= P.R2f) && (!same || m < uu);
+          mask |= ok ? (1u << m) : 0u;
+        }
+        if (mask) {
+          if (!wide) {
+            if (nkeys > 0 && aj >= kmin && aj <= kmax) {
+              int lo_i = 0, hi_i = nkeys;
+              while (lo_i < hi_i) {
+                int mid = (lo_i + hi_i) >> 1;
+                if (s_key[gi][mid] < aj) lo_i = mid + 1; else hi_i = mid;
+              }
+              for (int k = lo_i; k < nkeys && s_key[gi][k] == aj; ++k)
+                mask &= ~(1u << s_ku[gi][k]);
+            }
+          } else {
+            unsigned mm = mask;
+            while (mm) {
+              int m = __ffs(mm) - 1;
+              mm &= mm - 1;
+              int am = s_atom[gi][m];
+              for (int k = excl_off[am]; k < excl_off[am + 1]; ++k)
+                if (excl[k] == aj) mask &= ~(1u << m);
+            }
+          }
+        }
+      }
+      unsigned has = __ballot_sync(FULL, mask != 0);
+      if (chunked) {
+        if (mask)
+          ring[(rhead + rn + __popc(has & ((1u << lane) - 1))) & 63] =
+              make_int2(pj, (int)(mask | ((unsigned)code << 16)));
+        rn += __popc(has);
+        if (rn >= 32) {  // a full run of 32 to a chunk of the group's scratch row
+          __syncwarp();
+          int claim = 0;
+          if (lane == 0) claim = atomicAdd(&s_fill, 32);
+          claim = __shfl_sync(FULL, claim, 0);
+          if (claim + 32 <= P.list_cap) scratch[g * P.list_cap + claim + lane] = ring[(rhead + lane) & 63];
+          if (lane == 0 && nchunks < chunk_cap) chunk_at[nchunks] = claim + 32 <= P.list_cap ? claim : -1;
+          ++nchunks;
+          rhead = (rhead + 32) & 63;
+          rn -= 32;
+          __syncwarp();
+        }
+      } else if (mask) {
+        int at = count + __popc(has & ((1u << lane) - 1));
+        int2 en = make_int2(pj, (int)(mask | ((unsigned)code << 16)));
+        if (at < P.list_cap) {
+          if (W > 1)
+            stage[at] = en;
+          else
+            slab[g * P.list_cap + at] = en;
+        }
+      }
+      count += __popc(has);
+      qh = (qh + take) & 63;
+      qn -= take;
+      __syncwarp();
+    };
+
     for (int wi = w0; wi < w1; ++wi) {
       int ky = ky0 + wi / nx, kx = kx0 + wi % nx;
       int cy = ((ky % P.Ny) + P.Ny) % P.Ny;
@@ -380,85 +475,38 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
               bits &= bits - 1;
             }
             int cand = half ? c1 : c0;
-            unsigned mask = 0;
-            int64_t pj = 0;
+            bool keep = false;
+            int pj = 0, aj = -1;
+            float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
+            bool same = false;
             if (cand >= 0) {
               int64_t h = base + cand;
-              pj = h * NB_GROUP + u;
-              int aj = order[pj];
+              pj = (int)(h * NB_GROUP + u);
+              aj = order[pj];
               if (aj >= 0) {
-                float4 xj = xw[pj];
-                bool same = (h == g);
-#pragma unroll 4
-                for (int m = 0; m < NB_GROUP; ++m) {
-                  float4 xm = s_mem[gi][m];
-                  int am = s_atom[gi][m];
-                  // canonical orientation: A = smaller atom number
-                  bool jfirst = aj < am;
-                  float4 xa = jfirst ? xj : xm;
-                  float4 xb = jfirst ? xm : xj;
-                  float sgn = jfirst ? -1.f : 1.f;
-                  float r2 = nb_pair_r2(xa, xb, sgn * fsx, sgn * fsy, sgn * fsz);
-                  bool ok = (xm.w != 0.f) && (r2 <= P.R2f) && (!same || m < u);
-                  mask |= ok ? (1u << m) : 0u;
-                }
-                if (mask) {
-                  if (!wide) {
-                    if (nkeys > 0 && aj >= kmin && aj <= kmax) {
-                      int lo_i = 0, hi_i = nkeys;
-                      while (lo_i < hi_i) {
-                        int mid = (lo_i + hi_i) >> 1;
-                        if (s_key[gi][mid] < aj) lo_i = mid + 1; else hi_i = mid;
-                      }
-                      for (int k = lo_i; k < nkeys && s_key[gi][k] == aj; ++k)
-                        mask &= ~(1u << s_ku[gi][k]);
-                    }
-                  } else {
-                    unsigned mm = mask;
-                    while (mm) {
-                      int m = __ffs(mm) - 1;
-                      mm &= mm - 1;
-                      int am = s_atom[gi][m];
-                      for (int k = excl_off[am]; k < excl_off[am + 1]; ++k)
-                        if (excl[k] == aj) mask &= ~(1u << m);
-                    }
-                  }
-                }
+                xj = xw[pj];
+                same = h == g;
+                // the place against this group's box, with the margin of the window
+                float xs = xj.x + fsx, ys = xj.y + fsy, zs = xj.z + fsz;
+                float gx = fmaxf(fmaxf(lo.x - xs, xs - hi.x), 0.f);
+                float gy = fmaxf(fmaxf(lo.y - ys, ys - hi.y), 0.f);
+                float gz = fmaxf(fmaxf(lo.z - zs, zs - hi.z), 0.f);
+                keep = gx * gx + gy * gy + gz * gz <= Rb2;
               }
             }
-            unsigned has = __ballot_sync(FULL, mask != 0);
-            if (chunked) {
-              if (mask)
-                ring[(rhead + rn + __popc(has & ((1u << lane) - 1))) & 63] =
-                    make_int2((int)pj, (int)(mask | ((unsigned)code << 16)));
-              rn += __popc(has);
-              if (rn >= 32) {  // a full run of 32 to a chunk of the group's scratch row
-                __syncwarp();
-                int claim = 0;
-                if (lane == 0) claim = atomicAdd(&s_fill, 32);
-                claim = __shfl_sync(FULL, claim, 0);
-                if (claim + 32 <= P.list_cap) scratch[g * P.list_cap + claim + lane] = ring[(rhead + lane) & 63];
-                if (lane == 0 && nchunks < chunk_cap) chunk_at[nchunks] = claim + 32 <= P.list_cap ? claim : -1;
-                ++nchunks;
-                rhead = (rhead + 32) & 63;
-                rn -= 32;
-                __syncwarp();
-              }
-            } else if (mask) {
-              int at = count + __popc(has & ((1u << lane) - 1));
-              int2 en = make_int2((int)pj, (int)(mask | ((unsigned)code << 16)));
-              if (at < P.list_cap) {
-                if (W > 1)
-                  stage[at] = en;
-                else
-                  slab[g * P.list_cap + at] = en;
-              }
+            unsigned kb = __ballot_sync(FULL, keep);
+            if (keep) {
+              int at = (qh + qn + __popc(kb & ((1u << lane) - 1))) & 63;
+              qi[at] = make_int4(pj, aj, code, u | (same ? 16 : 0));
+              qx[at] = xj;
             }
-            count += __popc(has);
+            qn += __popc(kb);
+            if (qn >= 32) drain(32);
           }
         }
       }
     }
+    if (qn > 0) drain(qn);
   }
   if (W == 1) {
     if (lane == 0) {

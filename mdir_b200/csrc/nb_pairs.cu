@@ -117,9 +117,12 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   __shared__ int s_t[8][2 * NB_GROUP];     // LJM 0: member row offsets in s_lj
   __shared__ float2 s_lj[LJM == 0 ? NB_MAX_TYPES * NB_MAX_TYPES : 1];
   const unsigned FULL = 0xffffffffu;
-  if (LJM == 0) {
+  if (LJM == 0) {  // (6 c6, 12 c12): the force's factors
     int nt2 = P.ntypes * P.ntypes;
-    for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = lj[k];
+    for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+      float2 c = lj[k];
+      s_lj[k] = make_float2(6.f * c.x, 12.f * c.y);
+    }
     __syncthreads();
   }
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -140,9 +143,10 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
       xi.w *= P.coulomb;
       int ti = typ[pi];
       s_x[warp][lane] = xi;
-      if (LJM == 1)
-        s_f[warp][lane] = ljf[ti];
-      else
+      if (LJM == 1) {  // the member's factors times 6 and 12: the force's factors
+        float2 f = ljf[ti];
+        s_f[warp][lane] = make_float2(6.f * f.x, 12.f * f.y);
+      } else
         s_t[warp][lane] = ti * P.ntypes;
     }
     __syncwarp();
@@ -183,8 +187,10 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
         float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
         float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         bool inside = (mrot & (1u << k)) && (r2 < P.rc2);
-        float r2s = inside ? r2 : 1.0f;
-        float2 cc;
+        // a slot outside (masked, or beyond r_c) computes on its own r^2,
+        // finite or not, and its force and energies are dropped below
+        float r2s = r2;
+        float2 cc;  // (6 c6, 12 c12)
         if (LJM == 1) {
           float2 fm = pf[k];
           cc = make_float2(fm.x * fj.x, fm.y * fj.y);
@@ -194,9 +200,9 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
         float rinv = nb_rsqrt(r2s);
         float rinv2 = rinv * rinv;
         float s6 = rinv2 * rinv2 * rinv2;
-        float a12 = cc.y * s6 * s6, a6 = cc.x * s6;
-        float fs = (12.f * a12 - 6.f * a6) * rinv2;
-        float ulj = a12 - a6;
+        float a12 = cc.y * s6 * s6, a6 = cc.x * s6;  // 12 c12 / r^12, 6 c6 / r^6
+        float fs = (a12 - a6) * rinv2;
+        float ulj = (ENERGY || SWITCH) ? a12 * (1.f / 12.f) - a6 * (1.f / 6.f) : 0.f;
         if (SWITCH) {
           float y = fminf(fmaxf((r2s - P.rs2) * P.winv, 0.f), 1.f);
           float S = (1.f - y) * (1.f - y) * (1.f + 2.f * y);
