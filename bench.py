@@ -575,9 +575,21 @@ def main():
     e2e = ns_per_day(args.md_steps * e_steps * world, e2e_sec)
 
     # ---- roofline of the dominant kernel (pair kernel), timed live ------------
-    times = np.zeros(8)
-    _lib.check(_lib.lib().mdrtNbTimeKernels(term._h, _dp(x), _hp(np.asarray(box, dtype=np.float64)), 200,
-                                            _stream(), _hp(times)), "mdrtNbTimeKernels")
+    # on the whole GPU at its faster block count (the kernel alone), and at
+    # the span the step uses (beside PME) for reference
+    def stage_times():
+        t_ = np.zeros(8)
+        _lib.check(_lib.lib().mdrtNbTimeKernels(term._h, _dp(x), _hp(np.asarray(box, dtype=np.float64)), 200,
+                                                _stream(), _hp(t_)), "mdrtNbTimeKernels")
+        return t_
+    step_shape = (term.pair_sms, term.pair_blocks_per_sm)
+    step_times = stage_times()
+    alone = []
+    for blocks in (4, 3):
+        term.set_tuning(pair_sms=0, pair_blocks_per_sm=blocks)
+        alone.append((stage_times(), blocks))
+    times, alone_blocks = min(alone, key=lambda tb: tb[0][1])
+    term.set_tuning(pair_sms=step_shape[0], pair_blocks_per_sm=step_shape[1])
     pairs = count_pairs(x, box, s["cutoff"], s["excluded_pairs"])
     flop_per_pair = 50
     props = torch.cuda.get_device_properties(dev)
@@ -591,6 +603,9 @@ def main():
                 "traffic": PAIRS_TRAFFIC_BYTES if args.waters == 7850 else None,
                 "pairs_within_cutoff": pairs, "flop_per_pair": flop_per_pair,
                 "launch_ms": round(times[1], 5),
+                "launch_shape": {"sms": props.multi_processor_count, "blocks_per_sm": alone_blocks},
+                "step_shape": {"sms": step_shape[0] or props.multi_processor_count,
+                               "blocks_per_sm": step_shape[1], "launch_ms": round(step_times[1], 5)},
                 "peak_note": "nominal FP32 = SMs x 128 x 2 x max SM clock (no measured FP32 peak exists)",
                 "stage_ms": {"gather": round(times[0], 5), "pairs": round(times[1], 5),
                              "excluded": round(times[2], 5), "pme": round(times[3], 5),
@@ -604,10 +619,12 @@ def main():
             "e2e": {"value": round(e2e, 2), "unit": "ns/day", "h2d_bytes_per_step": 2 * n * 3 * 8,
                     "d2h_bytes_per_step": 2 * n * 3 * 8 + 4},
             "roofline": roofline,
-            # this library's kernels per MD step: noise, spread, convolve, PME
-            # gather, pairs, update (cuFFT's own kernels not counted); 16 per
-            # build (with the frames and the references) and 5 per pruning
-            "gpu_launches": int(args.steps * args.md_steps * 6 + builds * 16 + prunes * 5),
+            # this library's kernels per MD step: the gated pruning, spread,
+            # spectrum scaling, pairs, update (cuFFT's own kernels not
+            # counted), the noise once a graph of `unroll` steps, and 20 per
+            # build (with the frames, the places and the references)
+            "gpu_launches": int(args.steps * args.md_steps * 5 + args.steps * args.md_steps // max(1, args.unroll)
+                                + builds * 20),
             "tuned": tuned,
             "builds": int(builds), "prunes": int(prunes), "regrows": int(regrows), "regrows_total": th1["regrows"],
             "stale_stops": int(stops),
