@@ -477,3 +477,176 @@ void orc_bspline_moduli(int64_t K, int32_t order, double *out) {
       out[m] = 0.5 * (l + r);
     }
 }
+
+/* ------------------------------------------------------------------------
+ * Triclinic cells (docs/neighbor-groups.md, Section 5.1; docs/triclinic.md):
+ * the cell H of rows a = (ax, 0, 0), b = (bx, by, 0), c = (cx, cy, cz),
+ * given as the six numbers (ax, by, cz, bx, cx, cy) of MDIR's
+ * vector<6xf64>; a lattice vector n = (na, nb, nc) is n H.
+ * ---------------------------------------------------------------------- */
+
+/* The positions of test/Runtime/neighbors-groups-triclinic-gpu.mlir:47-100:
+ * fractional coordinates from the generator of orc_lcg_positions, each
+ * moved by (i + 3k) mod 7 - 3 lattice vectors, then x = s H. */
+void orc_lcg_positions_triclinic(int64_t n, const double *cell, double *x) {
+  uint64_t s = 42;
+  double ax = cell[0], by = cell[1], cz = cell[2], bx = cell[3], cx = cell[4], cy = cell[5];
+  for (int64_t i = 0; i < n; ++i) {
+    double f[3];
+    for (int k = 0; k < 3; ++k) {
+      s = (s * 1103515245ull + 12345ull) % 2147483648ull;
+      f[k] = (double)s / 2147483648.0 + ((double)((i + 3 * k) % 7) - 3.0);
+    }
+    x[3 * i] = f[0] * ax + f[1] * bx + f[2] * cx;
+    x[3 * i + 1] = f[1] * by + f[2] * cy;
+    x[3 * i + 2] = f[2] * cz;
+  }
+}
+
+/* The widened reach of a triclinic build: 3e-6 of the sum of the diagonal
+ * and the magnitudes of the three tilts (docs/neighbor-groups.md, 5.1). */
+double orc_widened_reach_triclinic(double reach, const double *cell) {
+  return reach + 3e-6 * (cell[0] + cell[1] + cell[2] + fabs(cell[3]) + fabs(cell[4]) + fabs(cell[5]));
+}
+
+/* Every image of every pair i < j within `reach` in f64: the displacement
+ * reduced once along c, b and a, then the lattice vectors up to `span`
+ * from that image along each of a, b, c.  Pairs with a position that is not
+ * finite and excluded pairs have none.  Writes at most `cap` rows
+ * (i, j, na, nb, nc) of the lattice vector of j's image relative to i (raw
+ * positions), returns the count; *several counts the pairs with more than
+ * one image within the reach. */
+int64_t orc_pairset_triclinic(int64_t n, const double *x, const double *cell, double reach,
+                              const int32_t *excl_off, const int32_t *excl, int32_t span, int64_t cap,
+                              int32_t *out, int64_t *several) {
+  double ax = cell[0], by = cell[1], cz = cell[2], bx = cell[3], cx = cell[4], cy = cell[5];
+  double R2 = reach * reach;
+  int64_t count = 0, multi = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (!finite3(x + 3 * i)) continue;
+    for (int64_t j = i + 1; j < n; ++j) {
+      if (!finite3(x + 3 * j)) continue;
+      if (excluded_pair(excl_off, excl, (int32_t)i, (int32_t)j)) continue;
+      double d[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
+      /* one pass along c, b, a: the lattice vector m of the reduced image */
+      double mc = -rint(d[2] / cz);
+      d[0] += mc * cx; d[1] += mc * cy; d[2] += mc * cz;
+      double mb = -rint(d[1] / by);
+      d[0] += mb * bx; d[1] += mb * by;
+      double ma = -rint(d[0] / ax);
+      d[0] += ma * ax;
+      int found = 0;
+      for (int tc = -span; tc <= span; ++tc)
+        for (int tb = -span; tb <= span; ++tb)
+          for (int ta = -span; ta <= span; ++ta) {
+            double ex = d[0] + ta * ax + tb * bx + tc * cx;
+            double ey = d[1] + tb * by + tc * cy;
+            double ez = d[2] + tc * cz;
+            if (!(ex * ex + ey * ey + ez * ez <= R2)) continue;
+            if (count < cap && out) {
+              out[5 * count] = (int32_t)i;
+              out[5 * count + 1] = (int32_t)j;
+              out[5 * count + 2] = (int32_t)ma + ta;
+              out[5 * count + 3] = (int32_t)mb + tb;
+              out[5 * count + 4] = (int32_t)mc + tc;
+            }
+            ++count;
+            ++found;
+          }
+      if (found > 1) ++multi;
+    }
+  }
+  if (several) *several = multi;
+  return count;
+}
+
+/* The f32 pair test of a triclinic build, as the device computes it:
+ * frames xw = (float)(x + S H), S the lattice vector that brings x into the
+ * brick [0, ax) x [0, by) x [0, cz) (along c, then b, then a; in f64), the
+ * image of an entry n in f32, t = n H with each product and sum rounded
+ * (tx = (na ax + nb bx) + nc cx, ty = nb by + nc cy, tz = nc cz, the cell in
+ * f32), and d = (xw_B + t) - xw_A, A the atom of the smaller number (t
+ * negated when A is j); r2 = (dx dx + dy dy) + dz dz, no fused multiply-add;
+ * the test r2 <= (float)(R'^2), R' the widened reach.  The images are those
+ * of orc_pairset_triclinic's search (span lattice vectors from the reduced
+ * image of the f64 displacement); rows (i, j, na, nb, nc) relative to the
+ * raw positions. */
+static void tri_wrap(const double *x, const double *cell, double *xw, int32_t *S) {
+  double ax = cell[0], by = cell[1], cz = cell[2], bx = cell[3], cx = cell[4], cy = cell[5];
+  double p[3] = {x[0], x[1], x[2]};
+  double sc = -floor(p[2] / cz);
+  p[0] += sc * cx; p[1] += sc * cy; p[2] += sc * cz;
+  double sb = -floor(p[1] / by);
+  p[0] += sb * bx; p[1] += sb * by;
+  double sa = -floor(p[0] / ax);
+  p[0] += sa * ax;
+  xw[0] = p[0]; xw[1] = p[1]; xw[2] = p[2];
+  S[0] = (int32_t)sa; S[1] = (int32_t)sb; S[2] = (int32_t)sc;
+}
+
+int64_t orc_pairset_triclinic_f32(int64_t n, const double *x, const double *cell, double reach,
+                                  const int32_t *excl_off, const int32_t *excl, int32_t span, int64_t cap,
+                                  int32_t *out) {
+  float axf = (float)cell[0], byf = (float)cell[1], czf = (float)cell[2];
+  float bxf = (float)cell[3], cxf = (float)cell[4], cyf = (float)cell[5];
+  double ax = cell[0], by = cell[1], cz = cell[2], bx = cell[3], cx = cell[4], cy = cell[5];
+  double Rw = orc_widened_reach_triclinic(reach, cell);
+  float R2f = (float)(Rw * Rw);
+  double Rs = Rw + 1e-3;  /* the f64 search reach of the candidate images */
+  float *xf = (float *)malloc(sizeof(float) * 3 * (size_t)(n > 0 ? n : 1));
+  double *xd = (double *)malloc(sizeof(double) * 3 * (size_t)(n > 0 ? n : 1));
+  int32_t *S = (int32_t *)malloc(sizeof(int32_t) * 3 * (size_t)(n > 0 ? n : 1));
+  for (int64_t i = 0; i < n; ++i) {
+    if (!finite3(x + 3 * i)) continue;
+    tri_wrap(x + 3 * i, cell, xd + 3 * i, S + 3 * i);
+    for (int k = 0; k < 3; ++k) xf[3 * i + k] = (float)xd[3 * i + k];
+  }
+  int64_t count = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (!finite3(x + 3 * i)) continue;
+    for (int64_t j = i + 1; j < n; ++j) {
+      if (!finite3(x + 3 * j)) continue;
+      if (excluded_pair(excl_off, excl, (int32_t)i, (int32_t)j)) continue;
+      /* candidate images e of wrapped j relative to wrapped i */
+      double d[3] = {xd[3 * j] - xd[3 * i], xd[3 * j + 1] - xd[3 * i + 1], xd[3 * j + 2] - xd[3 * i + 2]};
+      double mc = -rint(d[2] / cz);
+      d[0] += mc * cx; d[1] += mc * cy; d[2] += mc * cz;
+      double mb = -rint(d[1] / by);
+      d[0] += mb * bx; d[1] += mb * by;
+      double ma = -rint(d[0] / ax);
+      d[0] += ma * ax;
+      for (int tc = -span; tc <= span; ++tc)
+        for (int tb = -span; tb <= span; ++tb)
+          for (int ta = -span; ta <= span; ++ta) {
+            double ex = d[0] + ta * ax + tb * bx + tc * cx;
+            double ey = d[1] + tb * by + tc * cy;
+            double ez = d[2] + tc * cz;
+            if (!(ex * ex + ey * ey + ez * ez <= Rs * Rs)) continue;
+            int32_t na = (int32_t)ma + ta, nb = (int32_t)mb + tb, nc = (int32_t)mc + tc;
+            /* the f32 test, A = i (the smaller number), B = j with image n */
+            float fa = (float)na, fb = (float)nb, fc = (float)nc;
+            float tx = (fa * axf + fb * bxf) + fc * cxf;
+            float ty = fb * byf + fc * cyf;
+            float tz = fc * czf;
+            float dx = (xf[3 * j] + tx) - xf[3 * i];
+            float dy = (xf[3 * j + 1] + ty) - xf[3 * i + 1];
+            float dz = (xf[3 * j + 2] + tz) - xf[3 * i + 2];
+            float r2 = (dx * dx + dy * dy) + dz * dz;
+            if (!(r2 <= R2f)) continue;
+            if (count < cap && out) {
+              /* relative to the raw positions: n + S_j - S_i */
+              out[5 * count] = (int32_t)i;
+              out[5 * count + 1] = (int32_t)j;
+              out[5 * count + 2] = na + S[3 * j] - S[3 * i];
+              out[5 * count + 3] = nb + S[3 * j + 1] - S[3 * i + 1];
+              out[5 * count + 4] = nc + S[3 * j + 2] - S[3 * i + 2];
+            }
+            ++count;
+          }
+    }
+  }
+  free(xf);
+  free(xd);
+  free(S);
+  return count;
+}

@@ -58,6 +58,13 @@ def lib():
         _lib.orc_lcg_positions.argtypes = [i64, d, p]
         _lib.orc_widened_reach.restype = d
         _lib.orc_widened_reach.argtypes = [d, p]
+        _lib.orc_lcg_positions_triclinic.argtypes = [i64, p, p]
+        _lib.orc_widened_reach_triclinic.restype = d
+        _lib.orc_widened_reach_triclinic.argtypes = [d, p]
+        _lib.orc_pairset_triclinic.restype = i64
+        _lib.orc_pairset_triclinic.argtypes = [i64, p, p, d, p, p, i32, i64, p, p]
+        _lib.orc_pairset_triclinic_f32.restype = i64
+        _lib.orc_pairset_triclinic_f32.argtypes = [i64, p, p, d, p, p, i32, i64, p]
     return _lib
 
 
@@ -88,6 +95,55 @@ def lcg_positions(n, length):
     x = np.zeros((n, 3))
     lib().orc_lcg_positions(n, length, _ptr(x))
     return x
+
+
+def lcg_positions_triclinic(n, cell):
+    """The positions of MDIR's test/Runtime/neighbors-groups-triclinic-gpu.mlir:47-100
+    in the cell (ax, by, cz, bx, cx, cy)."""
+    x = np.zeros((n, 3))
+    lib().orc_lcg_positions_triclinic(n, _ptr(_c(cell, np.float64)), _ptr(x))
+    return x
+
+
+def cell_matrix(cell):
+    """The rows a, b, c of the lower-triangular cell (ax, by, cz, bx, cx, cy)."""
+    ax, by, cz, bx, cx, cy = [float(v) for v in cell]
+    return np.array([[ax, 0.0, 0.0], [bx, by, 0.0], [cx, cy, cz]])
+
+
+def pairset_triclinic_f32(x, cell, reach, excl=None, want_list=True, span=3):
+    """(count, rows (i, j, na, nb, nc)) of the canonical f32 pair test of a
+    triclinic build (the widened reach; images relative to the raw
+    positions); see oracle.c."""
+    x = _c(x, np.float64)
+    cell = _c(cell, np.float64)
+    n = len(x)
+    off, ex = (None, None) if excl is None else (_c(excl[0], np.int32), _c(excl[1], np.int32))
+    count = lib().orc_pairset_triclinic_f32(n, _ptr(x), _ptr(cell), reach, _ptr(off), _ptr(ex), span, 0, None)
+    if not want_list:
+        return count, None
+    out = np.zeros((max(count, 1), 5), dtype=np.int32)
+    lib().orc_pairset_triclinic_f32(n, _ptr(x), _ptr(cell), reach, _ptr(off), _ptr(ex), span, count, _ptr(out))
+    return count, out[:count]
+
+
+def pairset_triclinic(x, cell, reach, excl=None, want_list=True, span=2):
+    """(count, rows (i, j, na, nb, nc), pairs with several images) of every
+    image of every pair within `reach` in f64 in a triclinic cell; see
+    oracle.c."""
+    x = _c(x, np.float64)
+    cell = _c(cell, np.float64)
+    n = len(x)
+    off, ex = (None, None) if excl is None else (_c(excl[0], np.int32), _c(excl[1], np.int32))
+    several = ctypes.c_int64(0)
+    count = lib().orc_pairset_triclinic(n, _ptr(x), _ptr(cell), reach, _ptr(off), _ptr(ex), span, 0, None,
+                                        ctypes.byref(several))
+    if not want_list:
+        return count, None, several.value
+    out = np.zeros((max(count, 1), 5), dtype=np.int32)
+    lib().orc_pairset_triclinic(n, _ptr(x), _ptr(cell), reach, _ptr(off), _ptr(ex), span, count, _ptr(out),
+                                ctypes.byref(several))
+    return count, out[:count], several.value
 
 
 def chain_exclusions(n, degree):

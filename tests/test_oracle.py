@@ -28,6 +28,53 @@ GROUPS_KAT = [
 ]
 
 
+# test/Runtime/neighbors-groups-triclinic-gpu.mlir:636-812: the cell
+# (ax, by, cz, bx, cx, cy), reach, exclusion degree, a position that is not
+# a number, particles, the bits of the lists, the pairs with several images
+# within the reach (the last line of each case, printed for the 320-particle
+# cases)
+_OCT = (12.0, 11.313708498984761, 9.797958971132712, -4.0, -4.0, -5.656854249492381)
+_DODEC = (12.0, 12.0, 8.485281374238571, 0.0, 6.0, 6.0)
+_SMALL = (4.2, 4.0, 3.9, 1.0, -1.5, 1.2)
+_HEXA = (12.0, 10.392304845413264, 9.0, -6.0, 0.0, 0.0)
+_NDODEC = (4.242640687119286, 4.242640687119286, 3.0, 0.0, 2.121320343559643, 2.121320343559643)
+_NOCT = (3.6742346141747673, 3.4641016151377544, 3.0, -1.224744871391589, -1.224744871391589, -1.7320508075688772)
+_NHEXA = (3.4641016151377544, 3.0, 3.2, -1.7320508075688772, 0.0, 0.0)
+_NBOUNDS = (3.0, 3.0, 3.0, 1.5, -1.5, 1.5)
+TRICLINIC_KAT = [
+    (_OCT, 1.5, 0, False, 2000, 21149, None), (_OCT, 1.5, 1, False, 2000, 21125, None),
+    (_OCT, 1.5, 9, False, 2000, 20953, None), (_OCT, 1.5, 0, True, 2000, 21132, None),
+    (_DODEC, 1.5, 0, False, 2000, 23156, None), (_DODEC, 2.65, 0, False, 2000, 127147, None),
+    (_SMALL, 1.9, 0, False, 2000, 875982, None), (_HEXA, 1.5, 0, False, 2000, 25088, None),
+    (_NDODEC, 1.8, 0, False, 320, 22998, 0), (_NDODEC, 2.55, 1, False, 320, 65313, 15162),
+    (_NDODEC, 2.925, 0, False, 320, 99408, 35791), (_NOCT, 1.8, 0, False, 320, 32533, 0),
+    (_NOCT, 2.55, 1, False, 320, 92527, 33437), (_NOCT, 2.925, 0, False, 320, 140360, 46186),
+    (_NHEXA, 1.8, 0, False, 320, 37351, 889), (_NHEXA, 2.55, 1, False, 320, 105866, 42846),
+    (_NHEXA, 2.925, 0, False, 320, 161158, 50026), (_NBOUNDS, 1.8, 0, False, 320, 46107, 2703),
+    (_NBOUNDS, 2.55, 1, False, 320, 130675, 45014), (_NBOUNDS, 2.925, 0, False, 320, 197964, 50644),
+]
+
+
+def triclinic_case(cell, R, deg, poison, n):
+    x = O.lcg_positions_triclinic(n, cell)
+    if poison:
+        x[7, 0] = np.nan
+    ex = O.chain_exclusions(n, deg) if deg else None
+    return x, ex
+
+
+@pytest.mark.parametrize("cell,R,deg,poison,n,bits,several", TRICLINIC_KAT)
+def test_triclinic_pairset_matches_groups_kat(cell, R, deg, poison, n, bits, several):
+    """The canonical f32 test of a triclinic build gives MDIR's bit counts;
+    the f64 images within the reach give its counts of pairs with several."""
+    x, ex = triclinic_case(cell, R, deg, poison, n)
+    count, _ = O.pairset_triclinic_f32(x, cell, R, ex, want_list=False)
+    assert count == bits
+    if several is not None:
+        _, _, multi = O.pairset_triclinic(x, cell, R, ex, want_list=False)
+        assert multi == several
+
+
 def lcg_case(L, R, deg, poison, n):
     x = O.lcg_positions(n, L)
     if poison:
