@@ -176,6 +176,29 @@ int32_t mdrtNbBuild(mdrtNb *ctx, const double *x, int64_t n, const double box[3]
 int32_t mdrtNbForce(mdrtNb *ctx, const double *x, const double box[3], uint32_t flags,
                     double *forces, void *stream);
 
+/* The build and the force term in a triclinic cell: cell = (ax, by, cz,
+ * bx, cx, cy), the rows a = (ax, 0, 0), b = (bx, by, 0), c = (cx, cy, cz)
+ * of a lower-triangular H in the reduced form |bx|, |cx| <= ax/2,
+ * |cy| <= by/2 (else MDRT_NB_INVALID_BOX; also a reach of 0.999 of the
+ * least of ax, by, cz or more).  Positions are wrapped into the brick
+ * [0, ax) x [0, by) x [0, cz) along c, then b, then a; an entry's image is a
+ * lattice vector n (five bits a component), applied as n H; the reach is
+ * widened by 3e-6 of the sum of the diagonal and the tilts' magnitudes.
+ * The lists hold every image within the reach once (several images of a
+ * pair when the reach exceeds half the cell).  A context built in a
+ * triclinic cell takes its forces from mdrtNbForceTriclinic with the same
+ * cell (mdrtNbForce refuses it); the pruning, energies and constants work
+ * as in an orthorhombic cell (box = the diagonal).  PME, the parameter
+ * gradient, the displacement test, the MD step and batches run in
+ * orthorhombic cells only (MDRT_NB_UNSUPPORTED).
+ * MDIR: mdrt_gpu_build_neighbors_groups_triclinic(x, vector<6xf64>, ...)
+ * (GroupsBuild.cpp:248-345, docs/neighbor-groups.md Section 5.1, D126);
+ * its lists are checked by test/Runtime/neighbors-groups-triclinic-gpu.mlir. */
+int32_t mdrtNbBuildTriclinic(mdrtNb *ctx, const double *x, int64_t n, const double cell[6], double reach,
+                             void *stream, int32_t *sizes_out);
+int32_t mdrtNbForceTriclinic(mdrtNb *ctx, const double *x, const double cell[6], uint32_t flags,
+                             double *forces, void *stream);
+
 /* Copies the energies and virials of the last MDRT_NB_ENERGY evaluation
  * (MDRT_NB_E_COUNT f64) to out (host); waits for `stream`.
  * MDIR: the seven f64 numbers per sum of docs/pme.md, Section 3, and

@@ -40,6 +40,8 @@ SIGNATURES = {
     "mdrtPmeSetup": (_i32, [_p, _i32, _i32, _i32, _i32]),
     "mdrtNbBuild": (_i32, [_p, _p, _i64, _p, _d, _p, _p]),
     "mdrtNbForce": (_i32, [_p, _p, _p, _u32, _p, _p]),
+    "mdrtNbBuildTriclinic": (_i32, [_p, _p, _i64, _p, _d, _p, _p]),
+    "mdrtNbForceTriclinic": (_i32, [_p, _p, _p, _u32, _p, _p]),
     "mdrtNbEnergies": (_i32, [_p, _p, _p]),
     "mdrtNbConstants": (_i32, [_p, _p, _i32, _p]),
     "mdrtPmePotential": (_i32, [_p, _p, _p]),

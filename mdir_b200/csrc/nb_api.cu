@@ -316,9 +316,41 @@ int32_t mdrtPmeSetup(mdrtNb *ctx, int32_t k1, int32_t k2, int32_t k3, int32_t or
   return MDRT_NB_OK;
 }
 
+// The build in the cell of c.tilt (set by the caller): see mdrtNbBuild.
+static int32_t nb_build_entry(mdrtNb *ctx, const double *x, int64_t n, const double box[3], double reach,
+                              void *stream, int32_t *sizes_out);
+
 int32_t mdrtNbBuild(mdrtNb *ctx, const double *x, int64_t n, const double box[3], double reach,
                     void *stream, int32_t *sizes_out) {
   if (!ctx || !x) return MDRT_NB_INVALID_ARGUMENT;
+  for (double &t : ctx->c.tilt) t = 0.0;
+  return nb_build_entry(ctx, x, n, box, reach, stream, sizes_out);
+}
+
+// A triclinic cell (ax, by, cz, bx, cx, cy) in MDIR's reduced form:
+// |bx| <= ax/2, |cx| <= ax/2, |cy| <= by/2.
+static int check_cell(const double cell[6]) {
+  if (!cell) return MDRT_NB_INVALID_ARGUMENT;
+  for (int k = 0; k < 6; ++k)
+    if (!std::isfinite(cell[k])) return MDRT_NB_INVALID_BOX;
+  const double slack = 1.0 + 1e-9;
+  if (std::fabs(cell[3]) > 0.5 * cell[0] * slack || std::fabs(cell[4]) > 0.5 * cell[0] * slack ||
+      std::fabs(cell[5]) > 0.5 * cell[1] * slack)
+    return MDRT_NB_INVALID_BOX;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbBuildTriclinic(mdrtNb *ctx, const double *x, int64_t n, const double cell[6], double reach,
+                             void *stream, int32_t *sizes_out) {
+  if (!ctx || !x) return MDRT_NB_INVALID_ARGUMENT;
+  int s = check_cell(cell);
+  if (s) return s;
+  for (int k = 0; k < 3; ++k) ctx->c.tilt[k] = cell[3 + k];
+  return nb_build_entry(ctx, x, n, cell, reach, stream, sizes_out);
+}
+
+static int32_t nb_build_entry(mdrtNb *ctx, const double *x, int64_t n, const double box[3], double reach,
+                              void *stream, int32_t *sizes_out) {
   NbCtx &c = ctx->c;
   if (n != c.n) return MDRT_NB_INVALID_ARGUMENT;
   if (reach > 0 && reach != c.reach) {
@@ -330,6 +362,7 @@ int32_t mdrtNbBuild(mdrtNb *ctx, const double *x, int64_t n, const double box[3]
   CK(cudaSetDevice(c.device));
   cudaStream_t st = (cudaStream_t)stream;
   if (nb_build_run(c, x, box, st)) return MDRT_NB_CUDA_ERROR;
+  for (int k = 0; k < 3; ++k) c.tilt_built[k] = c.tilt[k];
   if (!c.x_build) CK(cudaMalloc(&c.x_build, sizeof(double) * 3 * c.n));
   CK(cudaMemcpyAsync(c.x_build, x, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToDevice, st));
   if (sizes_out)
@@ -338,9 +371,28 @@ int32_t mdrtNbBuild(mdrtNb *ctx, const double *x, int64_t n, const double box[3]
   return MDRT_NB_OK;
 }
 
+static int32_t nb_force_entry(mdrtNb *ctx, const double *x, const double box[3], uint32_t flags, double *forces,
+                              void *stream);
+
 int32_t mdrtNbForce(mdrtNb *ctx, const double *x, const double box[3], uint32_t flags, double *forces,
                     void *stream) {
   if (!ctx || !x || !forces) return MDRT_NB_INVALID_ARGUMENT;
+  if (nb_triclinic(ctx->c)) return MDRT_NB_INVALID_BOX;  // built in a triclinic cell
+  return nb_force_entry(ctx, x, box, flags, forces, stream);
+}
+
+int32_t mdrtNbForceTriclinic(mdrtNb *ctx, const double *x, const double cell[6], uint32_t flags, double *forces,
+                             void *stream) {
+  if (!ctx || !x || !forces) return MDRT_NB_INVALID_ARGUMENT;
+  int s = check_cell(cell);
+  if (s) return s;
+  for (int k = 0; k < 3; ++k)
+    if (cell[3 + k] != ctx->c.tilt_built[k]) return MDRT_NB_INVALID_BOX;  // a cell change needs a build
+  return nb_force_entry(ctx, x, cell, flags, forces, stream);
+}
+
+static int32_t nb_force_entry(mdrtNb *ctx, const double *x, const double box[3], uint32_t flags, double *forces,
+                              void *stream) {
   NbCtx &c = ctx->c;
   if (!c.built) return MDRT_NB_NOT_BUILT;
   int s = check_box(c, box);
@@ -352,6 +404,7 @@ int32_t mdrtNbForce(mdrtNb *ctx, const double *x, const double box[3], uint32_t 
   bool pairs = !(flags & MDRT_NB_NO_PAIRS);
   bool excluded = !(flags & MDRT_NB_NO_EXCLUDED);
   bool pme = c.pme.on && !(flags & MDRT_NB_NO_PME) && c.beta > 0.0;
+  if (pme && nb_triclinic(c)) return MDRT_NB_UNSUPPORTED;  // PME in orthorhombic cells
   if (!(flags & MDRT_NB_ACCUMULATE)) CK(cudaMemsetAsync(forces, 0, sizeof(double) * 3 * c.n, st));
   if (energy) CK(cudaMemsetAsync(c.energy, 0, sizeof(double) * NB_E_SLOTS, st));
   nb_gather_frames(c, x, box, st);
@@ -374,6 +427,7 @@ int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, con
   if (!ctx || !box || count < 0 || (count > 0 && (!frames || !out))) return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = ctx->c;
   if (!c.built || !c.x_build) return MDRT_NB_NOT_BUILT;
+  if (nb_triclinic(c)) return MDRT_NB_UNSUPPORTED;  // per-axis minimum image
   if (count == 0) return MDRT_NB_OK;
   CK(cudaSetDevice(c.device));
   cudaStream_t st = (cudaStream_t)stream;
@@ -409,6 +463,7 @@ int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3
   if (mode == MDRT_NB_GRAD_PRODUCT && !cotangent) return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = ctx->c;
   if (!c.built) return MDRT_NB_NOT_BUILT;
+  if (nb_triclinic(c)) return MDRT_NB_UNSUPPORTED;  // the adjoint runs in orthorhombic cells
   int s = check_box(c, box);
   if (s) return s;
   for (int k = 0; k < 3; ++k)

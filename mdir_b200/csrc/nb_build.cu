@@ -32,7 +32,11 @@
 
 namespace {
 
+// The brick of a cell: x + S H in [0, ax) x [0, by) x [0, cz), S found
+// along c, then b, then a (with no tilts, per axis), each product and sum
+// of f64 rounded as written.
 __global__ void nb_keys(int64_t n, const double *__restrict__ x, double Lx, double Ly, double Lz,
+                        double bx, double cx, double cy,
                         int Nx, int Ny, int Nz, float inv_wx, float inv_wy, float inv_hz,
                         int32_t *__restrict__ key, int32_t *__restrict__ bin_count,
                         float4 *__restrict__ atom_xw, char4 *__restrict__ atom_shift,
@@ -42,10 +46,16 @@ __global__ void nb_keys(int64_t n, const double *__restrict__ x, double Lx, doub
   double v0 = x[3 * i], v1 = x[3 * i + 1], v2 = x[3 * i + 2];
   bool ok = isfinite(v0) && isfinite(v1) && isfinite(v2);
   double S0 = 0, S1 = 0, S2 = 0;
+  double p0 = 0, p1 = 0, p2 = 0;
   if (ok) {
-    S0 = -floor(v0 / Lx);
-    S1 = -floor(v1 / Ly);
     S2 = -floor(v2 / Lz);
+    p2 = __dadd_rn(v2, __dmul_rn(S2, Lz));
+    p1 = __dadd_rn(v1, __dmul_rn(S2, cy));
+    S1 = -floor(p1 / Ly);
+    p1 = __dadd_rn(p1, __dmul_rn(S1, Ly));
+    p0 = __dadd_rn(__dadd_rn(v0, __dmul_rn(S2, cx)), __dmul_rn(S1, bx));
+    S0 = -floor(p0 / Lx);
+    p0 = __dadd_rn(p0, __dmul_rn(S0, Lx));
     ok = fabs(S0) <= 100.0 && fabs(S1) <= 100.0 && fabs(S2) <= 100.0;
   }
   if (!ok) {
@@ -56,7 +66,7 @@ __global__ void nb_keys(int64_t n, const double *__restrict__ x, double Lx, doub
     atom_shift[i] = make_char4(0, 0, 0, 0);
     return;
   }
-  float w0 = (float)(v0 + S0 * Lx), w1 = (float)(v1 + S1 * Ly), w2 = (float)(v2 + S2 * Lz);
+  float w0 = (float)p0, w1 = (float)p1, w2 = (float)p2;
   int kx = min(max((int)(w0 * inv_wx), 0), Nx - 1);
   int ky = min(max((int)(w1 * inv_wy), 0), Ny - 1);
   int kz = min(max((int)(w2 * inv_hz), 0), Nz - 1);
@@ -177,6 +187,8 @@ __device__ __forceinline__ float nb_pair_r2(float4 xa, float4 xb, float sx, floa
 
 struct SearchParams {
   float Lx, Ly, Lz;
+  float bx, cx, cy;  // the tilts of a triclinic cell (tri != 0), else 0
+  int tri;
   float wx, wy;
   int Nx, Ny;
   float R2f;     // (float)(R'^2)
@@ -337,6 +349,13 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
     bool wide = s_meta[gi][1] != 0;
     int kmin = s_meta[gi][2], kmax = s_meta[gi][3];
     float4 lo = box_lo[g], hi = box_hi[g];
+    NbCell H;
+    H.ax = P.Lx;
+    H.by = P.Ly;
+    H.cz = P.Lz;
+    H.bx = P.bx;
+    H.cx = P.cx;
+    H.cy = P.cy;
     float ci0 = 0.5f * (lo.x + hi.x), ci1 = 0.5f * (lo.y + hi.y), ci2 = 0.5f * (lo.z + hi.z);
     float wi0 = 0.5f * (hi.x - lo.x), wi1 = 0.5f * (hi.y - lo.y), wi2 = 0.5f * (hi.z - lo.z);
     int kx0 = (int)floorf((lo.x - P.Rbox) / P.wx), kx1 = (int)floorf((hi.x + P.Rbox) / P.wx);
@@ -369,7 +388,8 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
         bool same = ((e.w >> 4) & 1) != 0;
         int sx, sy, sz;
         nb_decode_image(code, sx, sy, sz);
-        float fsx = (float)sx * P.Lx, fsy = (float)sy * P.Ly, fsz = (float)sz * P.Lz;
+        float3 t = nb_lattice_shift(sx, sy, sz, H);
+        float fsx = t.x, fsy = t.y, fsz = t.z;
 #pragma unroll 4
         for (int m = 0; m < NB_GROUP; ++m) {
           float4 xm = s_mem[gi][m];
@@ -440,71 +460,123 @@ __global__ void __launch_bounds__(128) nb_search_t(SearchParams P0, const NbFram
       __syncwarp();
     };
 
-    for (int wi = w0; wi < w1; ++wi) {
-      int ky = ky0 + wi / nx, kx = kx0 + wi % nx;
-      int cy = ((ky % P.Ny) + P.Ny) % P.Ny;
-      int sy = (ky - cy) / P.Ny;
-      int cx = ((kx % P.Nx) + P.Nx) % P.Nx;
-      int sx = (kx - cx) / P.Nx;
-      int c = col0 + cy * P.Nx + cx;
+    // The candidate groups of column c seen through the image T (code):
+    // the box test, then the places that pass the test against this group's
+    // box into the queue.
+    auto visit = [&](int c, float fsx, float fsy, float fsz, int code) {
       int hb = max(group_start[c], (int)g), he = group_start[c + 1];
-      if (hb >= he) continue;
-      for (int sz = sz0; sz <= sz1; ++sz) {
-        float fsx = (float)sx * P.Lx, fsy = (float)sy * P.Ly, fsz = (float)sz * P.Lz;
-        int code = nb_image_code(sx, sy, sz);
-        for (int base = hb; base < he; base += 32) {
-          int hc = base + lane;
-          bool pass = false;
-          if (hc < he) {
-            float4 l2 = box_lo[hc], h2 = box_hi[hc];
-            float d0 = fabsf(0.5f * (l2.x + h2.x) + fsx - ci0) - (wi0 + 0.5f * (h2.x - l2.x));
-            float d1 = fabsf(0.5f * (l2.y + h2.y) + fsy - ci1) - (wi1 + 0.5f * (h2.y - l2.y));
-            float d2 = fabsf(0.5f * (l2.z + h2.z) + fsz - ci2) - (wi2 + 0.5f * (h2.z - l2.z));
-            d0 = fmaxf(d0, 0.f);
-            d1 = fmaxf(d1, 0.f);
-            d2 = fmaxf(d2, 0.f);
-            pass = d0 * d0 + d1 * d1 + d2 * d2 <= Rb2;
-          }
-          unsigned bits = __ballot_sync(FULL, pass);
-          while (bits) {
-            int c0 = __ffs(bits) - 1;
+      for (int base = hb; base < he; base += 32) {
+        int hc = base + lane;
+        bool pass = false;
+        if (hc < he) {
+          float4 l2 = box_lo[hc], h2 = box_hi[hc];
+          float d0 = fabsf(0.5f * (l2.x + h2.x) + fsx - ci0) - (wi0 + 0.5f * (h2.x - l2.x));
+          float d1 = fabsf(0.5f * (l2.y + h2.y) + fsy - ci1) - (wi1 + 0.5f * (h2.y - l2.y));
+          float d2 = fabsf(0.5f * (l2.z + h2.z) + fsz - ci2) - (wi2 + 0.5f * (h2.z - l2.z));
+          d0 = fmaxf(d0, 0.f);
+          d1 = fmaxf(d1, 0.f);
+          d2 = fmaxf(d2, 0.f);
+          pass = d0 * d0 + d1 * d1 + d2 * d2 <= Rb2;
+        }
+        unsigned bits = __ballot_sync(FULL, pass);
+        while (bits) {
+          int c0 = __ffs(bits) - 1;
+          bits &= bits - 1;
+          int c1 = -1;
+          if (bits) {
+            c1 = __ffs(bits) - 1;
             bits &= bits - 1;
-            int c1 = -1;
-            if (bits) {
-              c1 = __ffs(bits) - 1;
-              bits &= bits - 1;
-            }
-            int cand = half ? c1 : c0;
-            bool keep = false;
-            int pj = 0, aj = -1;
-            float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
-            bool same = false;
-            if (cand >= 0) {
-              int64_t h = base + cand;
-              pj = (int)(h * NB_GROUP + u);
-              aj = order[pj];
-              if (aj >= 0) {
-                xj = xw[pj];
-                same = h == g;
-                // the place against this group's box, with the margin of the window
-                float xs = xj.x + fsx, ys = xj.y + fsy, zs = xj.z + fsz;
-                float gx = fmaxf(fmaxf(lo.x - xs, xs - hi.x), 0.f);
-                float gy = fmaxf(fmaxf(lo.y - ys, ys - hi.y), 0.f);
-                float gz = fmaxf(fmaxf(lo.z - zs, zs - hi.z), 0.f);
-                keep = gx * gx + gy * gy + gz * gz <= Rb2;
-              }
-            }
-            unsigned kb = __ballot_sync(FULL, keep);
-            if (keep) {
-              int at = (qh + qn + __popc(kb & ((1u << lane) - 1))) & 63;
-              qi[at] = make_int4(pj, aj, code, u | (same ? 16 : 0));
-              qx[at] = xj;
-            }
-            qn += __popc(kb);
-            if (qn >= 32) drain(32);
           }
+          int cand = half ? c1 : c0;
+          bool keep = false;
+          int pj = 0, aj = -1;
+          float4 xj = make_float4(0.f, 0.f, 0.f, 0.f);
+          bool same = false;
+          if (cand >= 0) {
+            int64_t h = base + cand;
+            pj = (int)(h * NB_GROUP + u);
+            aj = order[pj];
+            if (aj >= 0) {
+              xj = xw[pj];
+              same = h == g;
+              // the place against this group's box, with the margin of the window
+              float xs = xj.x + fsx, ys = xj.y + fsy, zs = xj.z + fsz;
+              float gx = fmaxf(fmaxf(lo.x - xs, xs - hi.x), 0.f);
+              float gy = fmaxf(fmaxf(lo.y - ys, ys - hi.y), 0.f);
+              float gz = fmaxf(fmaxf(lo.z - zs, zs - hi.z), 0.f);
+              keep = gx * gx + gy * gy + gz * gz <= Rb2;
+            }
+          }
+          unsigned kb = __ballot_sync(FULL, keep);
+          if (keep) {
+            int at = (qh + qn + __popc(kb & ((1u << lane) - 1))) & 63;
+            qi[at] = make_int4(pj, aj, code, u | (same ? 16 : 0));
+            qx[at] = xj;
+          }
+          qn += __popc(kb);
+          if (qn >= 32) drain(32);
         }
       }
+    };
+
+    if (!P.tri) {
+      // orthorhombic: the window of columns around the box, wrapped per axis
+      for (int wi = w0; wi < w1; ++wi) {
+        int ky = ky0 + wi / nx, kx = kx0 + wi % nx;
+        int cy = ((ky % P.Ny) + P.Ny) % P.Ny;
+        int sy = (ky - cy) / P.Ny;
+        int cx = ((kx % P.Nx) + P.Nx) % P.Nx;
+        int sx = (kx - cx) / P.Nx;
+        int c = col0 + cy * P.Nx + cx;
+        if (max(group_start[c], (int)g) >= group_start[c + 1]) continue;
+        for (int sz = sz0; sz <= sz1; ++sz) {
+          float3 t = nb_lattice_shift(sx, sy, sz, H);
+          visit(c, t.x, t.y, t.z, nb_image_code(sx, sy, sz));
+        }
+      }
+    } else {
+      // triclinic: every lattice vector n that can bring a brick position
+      // within the reach of the box (along c, then b, then a), each with the
+      // brick's columns its window cuts; the (image, column) pairs are
+      // shared among the W warps in this order.
+      const float R = P.Rbox;
+      auto each = [&](auto &&fn) {
+        int nc0 = (int)floorf((lo.z - R) / H.cz), nc1 = (int)floorf((hi.z + R) / H.cz);
+        for (int nc = nc0; nc <= nc1; ++nc) {
+          float yc = (float)nc * H.cy, xc = (float)nc * H.cx;
+          int nb0 = (int)floorf((lo.y - R - yc) / H.by), nb1 = (int)floorf((hi.y + R - yc) / H.by);
+          for (int nb = nb0; nb <= nb1; ++nb) {
+            float xb = xc + (float)nb * H.bx;
+            int na0 = (int)floorf((lo.x - R - xb) / H.ax), na1 = (int)floorf((hi.x + R - xb) / H.ax);
+            for (int na = na0; na <= na1; ++na) {
+              float3 t = nb_lattice_shift(na, nb, nc, H);
+              if (hi.z + R - t.z < 0.f || lo.z - R - t.z >= H.cz) continue;
+              int ax0 = max(0, (int)floorf((lo.x - R - t.x) / P.wx));
+              int ax1 = min(P.Nx - 1, (int)floorf((hi.x + R - t.x) / P.wx));
+              int ay0 = max(0, (int)floorf((lo.y - R - t.y) / P.wy));
+              int ay1 = min(P.Ny - 1, (int)floorf((hi.y + R - t.y) / P.wy));
+              if (ax0 > ax1 || ay0 > ay1) continue;
+              fn(na, nb, nc, t, ax0, ax1, ay0, ay1);
+            }
+          }
+        }
+      };
+      int total = 0;
+      each([&](int, int, int, float3, int ax0, int ax1, int ay0, int ay1) {
+        total += (ax1 - ax0 + 1) * (ay1 - ay0 + 1);
+      });
+      int t0 = (int)((int64_t)total * part / W), t1 = (int)((int64_t)total * (part + 1) / W);
+      int at = 0;
+      each([&](int na, int nb, int nc, float3 t, int ax0, int ax1, int ay0, int ay1) {
+        int nxw = ax1 - ax0 + 1, cnt = nxw * (ay1 - ay0 + 1);
+        int lo_i = max(t0 - at, 0), hi_i = min(t1 - at, cnt);
+        for (int k = lo_i; k < hi_i; ++k) {
+          int c = col0 + (ay0 + k / nxw) * P.Nx + ax0 + k % nxw;
+          if (max(group_start[c], (int)g) >= group_start[c + 1]) continue;
+          visit(c, t.x, t.y, t.z, nb_image_code(na, nb, nc));
+        }
+        at += cnt;
+      });
     }
     if (qn > 0) drain(qn);
   }
@@ -612,7 +684,7 @@ __device__ __forceinline__ bool nb_beyond_box(float3 lo, float3 hi, float jx, fl
 // their order (a warp per group, ballot compaction), so that the inner list
 // of a group is a deterministic function of the outer one and the frames.
 __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_t *__restrict__ sizes,
-                                                float Lx, float Ly, float Lz, float rin2, int64_t list_cap,
+                                                NbCell H, float rin2, int64_t list_cap,
                                                 const int2 *__restrict__ slab, const int32_t *__restrict__ counts,
                                                 const int32_t *__restrict__ order, const float4 *__restrict__ xq,
                                                 int2 *__restrict__ slab_in, int32_t *__restrict__ counts_in,
@@ -648,9 +720,10 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
       en = slab[g * list_cap + e];
       unsigned mm = (unsigned)en.y & live & 0xffffu;
       int sx, sy, sz;
-      nb_decode_image(((unsigned)en.y >> 16) & 31, sx, sy, sz);
+      nb_decode_image(((unsigned)en.y >> 16) & NB_IMAGE_BITS, sx, sy, sz);
       float4 xj = xq[en.x];
-      float jx = xj.x + (float)sx * Lx, jy = xj.y + (float)sy * Ly, jz = xj.z + (float)sz * Lz;
+      float3 t = nb_lattice_shift(sx, sy, sz, H);
+      float jx = xj.x + t.x, jy = xj.y + t.y, jz = xj.z + t.z;
       if (nb_beyond_box(box_lo, box_hi, jx, jy, jz, far2)) mm = 0;
       while (mm) {
         int m = __ffs(mm) - 1;
@@ -688,7 +761,7 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
 // the scan.  Block 0 counts the pruning in *prunes.
 #define NB_PRUNE_WARPS 4
 __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
-    nb_prune_block(int64_t groups_cap, const int32_t *__restrict__ sizes, float Lx, float Ly, float Lz, float rin2,
+    nb_prune_block(int64_t groups_cap, const int32_t *__restrict__ sizes, NbCell H, float rin2,
                    int64_t list_cap, const int2 *__restrict__ slab, const int32_t *__restrict__ counts,
                    const int32_t *__restrict__ order, const float4 *__restrict__ xq, int2 *__restrict__ slab_in,
                    int32_t *__restrict__ counts_in, const int *gate, const double *__restrict__ x,
@@ -789,10 +862,11 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
       float jx = 0.f, jy = 0.f, jz = 0.f;
       if (base + 32 * j + lane < hi && ((unsigned)en[j].y & live & 0xffffu)) {
         int sx, sy, sz;
-        nb_decode_image(((unsigned)en[j].y >> 16) & 31, sx, sy, sz);
-        jx = xj[j].x + (float)sx * Lx;
-        jy = xj[j].y + (float)sy * Ly;
-        jz = xj[j].z + (float)sz * Lz;
+        nb_decode_image(((unsigned)en[j].y >> 16) & NB_IMAGE_BITS, sx, sy, sz);
+        float3 t = nb_lattice_shift(sx, sy, sz, H);
+        jx = xj[j].x + t.x;
+        jy = xj[j].y + t.y;
+        jz = xj[j].z + t.z;
         pass = !nb_beyond_box(box_lo, box_hi, jx, jy, jz, far2);
       }
       unsigned pb = __ballot_sync(FULL, pass);
@@ -957,7 +1031,8 @@ static void nb_build_launch(NbCtx &c, const double *x, const double box[3], cuda
   cudaMemsetAsync(c.bin_count, 0, sizeof(int32_t) * (nbins + 1), s);
   cudaMemsetAsync(c.bin_fill, 0, sizeof(int32_t) * (nbins + 1), s);
   cudaMemsetAsync(c.order, 0xff, sizeof(int32_t) * c.places_cap, s);
-  nb_keys<<<blocks_for(n, 256), 256, 0, s>>>(n, x, box[0], box[1], box[2], G.Nx, G.Ny, G.Nz,
+  nb_keys<<<blocks_for(n, 256), 256, 0, s>>>(n, x, box[0], box[1], box[2], c.tilt[0], c.tilt[1], c.tilt[2],
+                                            G.Nx, G.Ny, G.Nz,
                                             1.0f / G.wx, 1.0f / G.wy, 1.0f / G.hz, c.key,
                                             c.bin_count, c.atom_xw, c.atom_shift, c.sizes);
   nb_scan(c.bin_count, c.bin_start, nbins + 1, nullptr, c.scan_scratch, s);
@@ -976,13 +1051,19 @@ static void nb_build_launch(NbCtx &c, const double *x, const double box[3], cuda
   P.Lx = (float)box[0];
   P.Ly = (float)box[1];
   P.Lz = (float)box[2];
+  P.bx = (float)c.tilt[0];
+  P.cx = (float)c.tilt[1];
+  P.cy = (float)c.tilt[2];
+  P.tri = nb_triclinic(c) ? 1 : 0;
   P.wx = G.wx;
   P.wy = G.wy;
   P.Nx = G.Nx;
   P.Ny = G.Ny;
-  double Rw = c.reach + 3e-6 * (box[0] + box[1] + box[2]);
+  // the widening: 3e-6 of the sum of the diagonal and the tilts' magnitudes
+  double span = box[0] + box[1] + box[2] + fabs(c.tilt[0]) + fabs(c.tilt[1]) + fabs(c.tilt[2]);
+  double Rw = c.reach + 3e-6 * span;
   P.R2f = (float)(Rw * Rw);
-  P.Rbox = (float)(Rw + 2e-5 * (box[0] + box[1] + box[2]) + 1e-6);
+  P.Rbox = (float)(Rw + 2e-5 * span + 1e-6);
   P.groups_cap = c.groups_cap;
   P.list_cap = c.list_cap;
   // four warps a group staging in chunks of the inner slab when it is there
@@ -1032,17 +1113,17 @@ int nb_reserve_inner(NbCtx &c) {
 }
 
 void nb_prune_run(NbCtx &c, const double box[3], cudaStream_t s) {
-  double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2]);
+  double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2] + fabs(c.tilt[0]) + fabs(c.tilt[1]) + fabs(c.tilt[2]));
   size_t stage = sizeof(int2) * (size_t)c.list_cap;
   if (stage <= 200 * 1024) {
     static size_t configured[NB_MAX_DEVICES] = {};
     nb_allow_smem(nb_prune_block, stage, configured);
     nb_prune_block<<<(int)c.groups_cap, NB_PRUNE_WARPS * 32, stage, s>>>(
-        c.groups_cap, c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+        c.groups_cap, c.sizes, nb_cell(c, box), (float)(Rw * Rw), c.list_cap, c.slab,
         c.counts, c.order, c.xq, c.slab_in, c.counts_in, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr);
   } else {
-    nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
-                                                        (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+    nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, nb_cell(c, box),
+                                                        (float)(Rw * Rw), c.list_cap, c.slab,
                                                         c.counts, c.order, c.xq, c.slab_in, c.counts_in, nullptr,
                                                         nullptr, nullptr);
   }
@@ -1098,7 +1179,7 @@ __global__ void __launch_bounds__(1024) nb_units_one_block(int64_t groups_cap, c
 
 void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double *x, double *x_prune,
                     double *prunes, int32_t *unit_counter, cudaStream_t s) {
-  double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2]);
+  double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2] + fabs(c.tilt[0]) + fabs(c.tilt[1]) + fabs(c.tilt[2]));
   size_t stage = sizeof(int2) * (size_t)c.list_cap;
   if (stage <= 200 * 1024) {
     static size_t configured[NB_MAX_DEVICES] = {};
@@ -1107,14 +1188,14 @@ void nb_prune_gated(NbCtx &c, const double box[3], const int *gate, const double
     // (the counter is zeroed by the update that asked for the pruning)
     bool claim = !c.deterministic && unit_counter;
     nb_launch_chained(nb_prune_block, dim3((int)c.groups_cap), dim3(NB_PRUNE_WARPS * 32), stage, s, c.groups_cap,
-                      c.sizes, (float)box[0], (float)box[1], (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+                      c.sizes, nb_cell(c, box), (float)(Rw * Rw), c.list_cap, c.slab,
                       c.counts, c.order, c.xq, c.slab_in, c.counts_in, gate, x, x_prune,
                       claim ? unit_counter : nullptr, claim ? c.units_in : nullptr, c.units_cap,
                       claim ? prunes : nullptr);
     if (claim) return;
   } else {
-    nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, (float)box[0], (float)box[1],
-                                                        (float)box[2], (float)(Rw * Rw), c.list_cap, c.slab,
+    nb_prune<<<blocks_for(c.groups_cap, 4), 128, 0, s>>>(c.groups_cap, c.sizes, nb_cell(c, box),
+                                                        (float)(Rw * Rw), c.list_cap, c.slab,
                                                         c.counts, c.order, c.xq, c.slab_in, c.counts_in, gate, x,
                                                         x_prune);
   }

@@ -55,15 +55,36 @@ struct NbBox {
 // its whole-cell shift less the half cell of the centred frames.
 __host__ __device__ inline double nb_frame_shift(int s) { return (double)s - 0.5; }
 
+// The image of an entry: a lattice vector n = (na, nb, nc) of the cell,
+// each component + 16 in five bits (bits 16-30 of the entry's second word;
+// -16..15, since a triclinic brick spans up to 3.5 periods of a).
+#define NB_IMAGE_BITS 0x7fff
 __host__ __device__ inline int nb_image_code(int sx, int sy, int sz) {
-  return 9 * (sz + 1) + 3 * (sy + 1) + (sx + 1);
+  return (sx + 16) | ((sy + 16) << 5) | ((sz + 16) << 10);
 }
 
 __device__ __forceinline__ void nb_decode_image(int code, int &sx, int &sy, int &sz) {
-  sz = code / 9 - 1;
-  int r = code - 9 * (sz + 1);
-  sy = r / 3 - 1;
-  sx = r - 3 * (sy + 1) - 1;
+  sx = (code & 31) - 16;
+  sy = ((code >> 5) & 31) - 16;
+  sz = ((code >> 10) & 31) - 16;
+}
+
+// The cell: rows a = (ax, 0, 0), b = (bx, by, 0), c = (cx, cy, cz) of a
+// lower-triangular H (an orthorhombic cell has no tilts bx, cx, cy).
+struct NbCell {
+  float ax, by, cz, bx, cx, cy;
+};
+
+// The lattice vector n H in f32, each product and each sum rounded in this
+// order: ((na ax + nb bx) + nc cx, nb by + nc cy, nc cz).  The neighbor
+// test of the build shifts by exactly this (its pair sets are compared bit
+// for bit); without tilts it is (na ax, nb by, nc cz).
+__device__ __forceinline__ float3 nb_lattice_shift(int na, int nb, int nc, const NbCell &H) {
+  float fa = (float)na, fb = (float)nb, fc = (float)nc;
+  float tx = __fadd_rn(__fadd_rn(__fmul_rn(fa, H.ax), __fmul_rn(fb, H.bx)), __fmul_rn(fc, H.cx));
+  float ty = __fadd_rn(__fmul_rn(fb, H.by), __fmul_rn(fc, H.cy));
+  float tz = __fmul_rn(fc, H.cz);
+  return make_float3(tx, ty, tz);
 }
 
 // Fixed-point scale of the deterministic force accumulators: 2^32 units

@@ -60,6 +60,10 @@ struct NbCtx {
   // neighbor structure
   NbGrid grid;
   double box_built[3] = {0, 0, 0};
+  // The tilts (bx, cx, cy) of a triclinic cell whose diagonal is the box
+  // (mdrtNbBuildTriclinic / mdrtNbForceTriclinic); 0 for an orthorhombic one.
+  double tilt[3] = {0, 0, 0};
+  double tilt_built[3] = {0, 0, 0};
   int64_t groups_cap = 0, places_cap = 0, bins_cap = 0, cols_cap = 0;
   int64_t list_cap = 0;    // C: entries per group
   int64_t units_cap = 0;
@@ -279,3 +283,16 @@ int nb_batch_pme_setup(mdrtNbBatch &b, const int32_t *grids, int order);
 void nb_batch_pme_release(mdrtNbBatch &b);
 int nb_batch_pme_run(mdrtNbBatch &b, bool energy, cudaStream_t s);
 void nb_batch_energy_sums(mdrtNbBatch &b, bool pairs, bool excluded, bool pme, cudaStream_t s);
+
+// The f32 cell of a context's box and tilts.
+inline NbCell nb_cell(const NbCtx &c, const double box[3]) {
+  NbCell H;
+  H.ax = (float)box[0];
+  H.by = (float)box[1];
+  H.cz = (float)box[2];
+  H.bx = (float)c.tilt[0];
+  H.cx = (float)c.tilt[1];
+  H.cy = (float)c.tilt[2];
+  return H;
+}
+inline bool nb_triclinic(const NbCtx &c) { return c.tilt[0] != 0.0 || c.tilt[1] != 0.0 || c.tilt[2] != 0.0; }

@@ -32,6 +32,7 @@ namespace {
 
 struct PairParams {
   float Lx, Ly, Lz;
+  float bx, cx, cy;  // tilts of a triclinic cell (0: orthorhombic)
   float rc2;
   float beta;
   float beta_p;         // p beta, p of the erfc approximation below
@@ -169,13 +170,23 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
       int2 en = valid ? slab[(int64_t)g * P.list_cap + e0 + r * 32 + lane] : make_int2(0, 0);
       int q = en.x;
       unsigned mask = valid ? ((unsigned)en.y & 0xffffu) : 0u;
-      int code = ((unsigned)en.y >> 16) & 31;
+      int code = ((unsigned)en.y >> 16) & NB_IMAGE_BITS;
       int sx, sy, sz;
       nb_decode_image(code, sx, sy, sz);
       float4 xj = xq[q];
-      xj.x += (float)sx * Lx;
-      xj.y += (float)sy * Ly;
-      xj.z += (float)sz * Lz;
+      {
+        NbCell H;
+        H.ax = Lx;
+        H.by = Ly;
+        H.cz = Lz;
+        H.bx = P.bx;
+        H.cx = P.cx;
+        H.cy = P.cy;
+        float3 t = nb_lattice_shift(sx, sy, sz, H);
+        xj.x += t.x;
+        xj.y += t.y;
+        xj.z += t.z;
+      }
       int tj = typ[q];
       float2 fj = LJM == 1 ? ljf[tj] : make_float2(0.f, 0.f);
       // bit k of mrot: the pair of this lane's entry with member (lane + k) mod 16
@@ -274,8 +285,8 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
 __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
                           const int32_t *__restrict__ order, const char4 *__restrict__ shift,
                           const double *__restrict__ x, const float *__restrict__ q,
-                          const int32_t *__restrict__ type, double Lx, double Ly, double Lz,
-                          float4 *__restrict__ xq, int32_t *__restrict__ typ_p) {
+                          const int32_t *__restrict__ type, double Lx, double Ly, double Lz, double bx,
+                          double cx, double cy, float4 *__restrict__ xq, int32_t *__restrict__ typ_p) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
   int a = order[p];
@@ -284,8 +295,10 @@ __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
     typ_p[p] = 0;
     return;
   }
+  // x + S H less half the diagonal (a triclinic cell adds S's tilt terms)
   char4 s = shift[p];
-  xq[p] = make_float4((float)(x[3 * a] + nb_frame_shift(s.x) * Lx), (float)(x[3 * a + 1] + nb_frame_shift(s.y) * Ly),
+  xq[p] = make_float4((float)(x[3 * a] + nb_frame_shift(s.x) * Lx + (double)s.y * bx + (double)s.z * cx),
+                      (float)(x[3 * a + 1] + nb_frame_shift(s.y) * Ly + (double)s.z * cy),
                       (float)(x[3 * a + 2] + nb_frame_shift(s.z) * Lz), q[a]);
   typ_p[p] = type[a];
 }
@@ -296,6 +309,7 @@ __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
 template <bool FIXED>
 __device__ __forceinline__ void nb_excluded_pair(int i, int j, const int32_t *__restrict__ place_of,
                                                  const float4 *__restrict__ xq, double Lx, double Ly, double Lz,
+                                                 double bx, double cx, double cy,
                                                  double beta, double coulomb, float4 *__restrict__ acc,
                                                  unsigned long long *__restrict__ accf, int *__restrict__ status,
                                                  double *v) {
@@ -303,9 +317,15 @@ __device__ __forceinline__ void nb_excluded_pair(int i, int j, const int32_t *__
   if (pi < 0 || pj < 0) return;
   float4 a = xq[pi], b = xq[pj];
   double d0 = (double)a.x - b.x, d1 = (double)a.y - b.y, d2 = (double)a.z - b.z;
+  // the minimum image in one pass along c, b, a (per axis without tilts)
+  double nc = rint(d2 / Lz);
+  d0 -= nc * cx;
+  d1 -= nc * cy;
+  d2 -= Lz * nc;
+  double nbv = rint(d1 / Ly);
+  d0 -= nbv * bx;
+  d1 -= Ly * nbv;
   d0 -= Lx * rint(d0 / Lx);
-  d1 -= Ly * rint(d1 / Ly);
-  d2 -= Lz * rint(d2 / Lz);
   double r2 = d0 * d0 + d1 * d1 + d2 * d2;
   double qq = coulomb * (double)a.w * (double)b.w;
   if (qq == 0.0 || r2 <= 0.0) return;
@@ -353,14 +373,15 @@ __device__ __forceinline__ void nb_block_partials8(double *v, double *__restrict
 template <bool FIXED>
 __global__ void nb_excluded(int64_t npairs, const int32_t *__restrict__ pairs,
                             const int32_t *__restrict__ place_of, const float4 *__restrict__ xq,
-                            double Lx, double Ly, double Lz, double beta, double coulomb, bool energy,
+                            double Lx, double Ly, double Lz, double bx, double cx, double cy, double beta,
+                            double coulomb, bool energy,
                             float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
                             double *__restrict__ partials, int *__restrict__ status) {
   int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (k < npairs)
-    nb_excluded_pair<FIXED>(pairs[2 * k], pairs[2 * k + 1], place_of, xq, Lx, Ly, Lz, beta, coulomb, acc, accf,
-                            status, v);
+    nb_excluded_pair<FIXED>(pairs[2 * k], pairs[2 * k + 1], place_of, xq, Lx, Ly, Lz, bx, cx, cy, beta, coulomb,
+                            acc, accf, status, v);
   if (!energy) return;
   nb_block_partials8(v, partials);
 }
@@ -378,8 +399,8 @@ __global__ void nb_batch_excluded(const int32_t *__restrict__ blk_frame, const i
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (k < frame_end[f]) {
     const NbFrameDev &F = frames[f];
-    nb_excluded_pair<false>(pairs[2 * k], pairs[2 * k + 1], place_of, xq, F.L0, F.L1, F.L2, beta, coulomb, acc,
-                            nullptr, nullptr, v);
+    nb_excluded_pair<false>(pairs[2 * k], pairs[2 * k + 1], place_of, xq, F.L0, F.L1, F.L2, 0.0, 0.0, 0.0, beta,
+                            coulomb, acc, nullptr, nullptr, v);
   }
   if (!energy) return;
   nb_block_partials8(v, partials);
@@ -625,13 +646,23 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
       int2 en = valid ? slab[(int64_t)g * P.list_cap + e0 + r * 32 + lane] : make_int2(0, 0);
       int q = en.x;
       unsigned mask = valid ? ((unsigned)en.y & 0xffffu) : 0u;
-      int code = ((unsigned)en.y >> 16) & 31;
+      int code = ((unsigned)en.y >> 16) & NB_IMAGE_BITS;
       int sx, sy, sz;
       nb_decode_image(code, sx, sy, sz);
       float4 xj = xq[q];
-      xj.x += (float)sx * P.Lx;
-      xj.y += (float)sy * P.Ly;
-      xj.z += (float)sz * P.Lz;
+      {
+        NbCell H;
+        H.ax = P.Lx;
+        H.by = P.Ly;
+        H.cz = P.Lz;
+        H.bx = P.bx;
+        H.cx = P.cx;
+        H.cy = P.cy;
+        float3 t = nb_lattice_shift(sx, sy, sz, H);
+        xj.x += t.x;
+        xj.y += t.y;
+        xj.z += t.z;
+      }
       float4 gj = MODE == 0 ? gp[q] : make_float4(0.f, 0.f, 0.f, 0.f);
       int tj = typ[q];
       float fqj = xj.w * P.coulomb;
@@ -784,6 +815,9 @@ PairParams pair_params(const NbCtx &c, const double box[3]) {
   P.Lx = (float)box[0];
   P.Ly = (float)box[1];
   P.Lz = (float)box[2];
+  P.bx = (float)c.tilt[0];
+  P.cx = (float)c.tilt[1];
+  P.cy = (float)c.tilt[2];
   P.rc2 = (float)(c.cutoff * c.cutoff);
   P.beta = (float)c.beta;
   P.beta_p = (float)(0.3275911 * c.beta);
@@ -804,8 +838,8 @@ PairParams pair_params(const NbCtx &c, const double box[3]) {
 
 void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
   nb_gather<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.shift, x,
-                                                          c.q, c.type, box[0], box[1], box[2], c.xq,
-                                                          c.typ_p);
+                                                          c.q, c.type, box[0], box[1], box[2], c.tilt[0],
+                                                          c.tilt[1], c.tilt[2], c.xq, c.typ_p);
 }
 
 void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt) {
@@ -852,10 +886,10 @@ void nb_excluded_list_run(NbCtx &c, const double box[3], const int32_t *pairs, i
   if (npairs == 0 || c.beta == 0.0) return;
   int blocks = blocks_for(npairs, 256);
   if (c.deterministic)
-    nb_excluded<true><<<blocks, 256, 0, s>>>(npairs, pairs, c.place_of, c.xq, box[0], box[1], box[2], c.beta,
+    nb_excluded<true><<<blocks, 256, 0, s>>>(npairs, pairs, c.place_of, c.xq, box[0], box[1], box[2], c.tilt[0], c.tilt[1], c.tilt[2], c.beta,
                                              c.coulomb, false, c.acc, c.acc_fixed, nullptr, c.status);
   else
-    nb_excluded<false><<<blocks, 256, 0, s>>>(npairs, pairs, c.place_of, c.xq, box[0], box[1], box[2], c.beta,
+    nb_excluded<false><<<blocks, 256, 0, s>>>(npairs, pairs, c.place_of, c.xq, box[0], box[1], box[2], c.tilt[0], c.tilt[1], c.tilt[2], c.beta,
                                               c.coulomb, false, c.acc, c.acc_fixed, nullptr, c.status);
 }
 
@@ -864,11 +898,11 @@ void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s)
   int blocks = blocks_for(c.n_excl_pairs, 256);
   if (c.deterministic)
     nb_excluded<true><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, c.place_of, c.xq, box[0],
-                                             box[1], box[2], c.beta, c.coulomb, energy, c.acc,
+                                             box[1], box[2], c.tilt[0], c.tilt[1], c.tilt[2], c.beta, c.coulomb, energy, c.acc,
                                              c.acc_fixed, c.excl_partials, c.status);
   else
     nb_excluded<false><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, c.place_of, c.xq, box[0],
-                                              box[1], box[2], c.beta, c.coulomb, energy, c.acc,
+                                              box[1], box[2], c.tilt[0], c.tilt[1], c.tilt[2], c.beta, c.coulomb, energy, c.acc,
                                               c.acc_fixed, c.excl_partials, c.status);
 }
 

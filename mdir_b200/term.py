@@ -137,11 +137,14 @@ class NonbondedTerm:
             raise ValueError("positions: a contiguous CUDA float64 tensor of shape (n, 3)")
 
     def build(self, x, box, reach=0.0, stream=None, allow_nan=False):
-        """The neighbor build at device positions x; returns the sizes."""
+        """The neighbor build at device positions x; returns the sizes.  `box`
+        is the three edges of an orthorhombic cell or the six numbers
+        (ax, by, cz, bx, cx, cy) of a triclinic one."""
         self._check_x(x)
         b = _host(box, np.float64)
         sizes = np.zeros(L.SIZE_COUNT, dtype=np.int32)
-        s = L.lib().mdrtNbBuild(self._h, _dp(x), self.n, _hp(b), reach, _stream(stream), _hp(sizes))
+        entry = L.lib().mdrtNbBuildTriclinic if len(b) == 6 else L.lib().mdrtNbBuild
+        s = entry(self._h, _dp(x), self.n, _hp(b), reach, _stream(stream), _hp(sizes))
         if not (s == L.NAN_POSITION and allow_nan):
             L.check(s, "mdrtNbBuild")
         self.box = b
@@ -157,8 +160,8 @@ class NonbondedTerm:
         flags = (L.ENERGY if energy else 0) | (L.POTENTIAL if potential else 0) | \
             (L.ACCUMULATE if accumulate else 0) | (0 if pairs else L.NO_PAIRS) | \
             (0 if pme else L.NO_PME) | (0 if excluded else L.NO_EXCLUDED)
-        L.check(L.lib().mdrtNbForce(self._h, _dp(x), _hp(b), flags, _dp(forces), _stream(stream)),
-                "mdrtNbForce")
+        entry = L.lib().mdrtNbForceTriclinic if len(b) == 6 else L.lib().mdrtNbForce
+        L.check(entry(self._h, _dp(x), _hp(b), flags, _dp(forces), _stream(stream)), "mdrtNbForce")
         return forces
 
     def energies(self, stream=None):
@@ -256,14 +259,13 @@ class NonbondedTerm:
         q = E[g_idx, e_idx, 0]
         bits = E[g_idx, e_idx, 1].astype(np.uint32)
         mask = bits & 0xFFFF
-        code = (bits >> 16) & 31
+        code = (bits >> 16) & 0x7FFF  # a lattice vector, five bits a component
         m_bits = (mask[:, None] >> np.arange(16)[None, :]) & 1
         k_idx, m_idx = np.nonzero(m_bits)
         a = order[16 * g_idx[k_idx] + m_idx]
         b = order[q[k_idx]]
         c = code[k_idx].astype(np.int64)
-        sz, r = c // 9 - 1, c % 9
-        sy, sx = r // 3 - 1, r % 3 - 1
+        sx, sy, sz = (c & 31) - 16, ((c >> 5) & 31) - 16, ((c >> 10) & 31) - 16
         swap = b < a
         sx = np.where(swap, -sx, sx)
         sy = np.where(swap, -sy, sy)
@@ -272,6 +274,37 @@ class NonbondedTerm:
         j = np.maximum(a, b)
         out = np.stack([i, j, 9 * (sz + 1) + 3 * (sy + 1) + (sx + 1)], axis=1).astype(np.int32)
         return out
+
+    def pair_images(self, sizes):
+        """The (i, j, na, nb, nc) of every bit of the lists, i < j by atom
+        number: the lattice vector of j's image relative to i in the raw
+        positions (the entry's image plus the places' shifts), for either
+        cell."""
+        order = self.buffer(L.SLOT_ORDER, np.int32)
+        counts = self.buffer(L.SLOT_COUNTS, np.int32)
+        shifts = self.buffer(L.SLOT_SHIFTS, np.int8, 4).astype(np.int64)
+        cap = self.info()["list_capacity"]
+        entries = self.buffer(L.SLOT_ENTRIES, np.int32, 2)
+        G = int(sizes[L.SIZE_GROUPS])
+        counts = counts[:G]
+        E = entries[: G * cap].reshape(G, cap, 2)
+        valid = np.arange(cap)[None, :] < counts[:, None]
+        g_idx, e_idx = np.nonzero(valid)
+        q = E[g_idx, e_idx, 0]
+        bits = E[g_idx, e_idx, 1].astype(np.uint32)
+        mask = bits & 0xFFFF
+        code = ((bits >> 16) & 0x7FFF).astype(np.int64)
+        m_bits = (mask[:, None] >> np.arange(16)[None, :]) & 1
+        k_idx, m_idx = np.nonzero(m_bits)
+        pa = 16 * g_idx[k_idx] + m_idx
+        pb = q[k_idx]
+        a, b = order[pa], order[pb]
+        c = code[k_idx]
+        n = np.stack([(c & 31) - 16, ((c >> 5) & 31) - 16, ((c >> 10) & 31) - 16], 1)
+        n = n + shifts[pb, :3] - shifts[pa, :3]
+        swap = (b < a)[:, None]
+        n = np.where(swap, -n, n)
+        return np.concatenate([np.minimum(a, b)[:, None], np.maximum(a, b)[:, None], n], 1).astype(np.int32)
 
 
 _CUDART = None

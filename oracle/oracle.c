@@ -650,3 +650,94 @@ int64_t orc_pairset_triclinic_f32(int64_t n, const double *x, const double *cell
   free(S);
   return count;
 }
+
+/* The Lennard-Jones + Ewald direct pair term of orc_nonbonded in a
+ * triclinic cell: every image within rc of every pair i < j (the f64
+ * displacement reduced once along c, b, a, then `span` lattice vectors
+ * around it); small systems, O(n^2). */
+void orc_nonbonded_triclinic(int64_t n, const double *x, const double *q, const int32_t *type, int32_t ntypes,
+                             const double *sigma, const double *epsilon, const double *cell, double rc,
+                             double beta, double coulomb, const int32_t *excl_off, const int32_t *excl,
+                             int32_t span, double *forces, double *energies, double *virial) {
+  double ax = cell[0], by = cell[1], cz = cell[2], bx = cell[3], cx = cell[4], cy = cell[5];
+  double rc2 = rc * rc;
+  double twobeta_sqrtpi = 2.0 * beta / sqrt(M_PI);
+  double elj = 0.0, ecoul = 0.0, W[9] = {0};
+  for (int64_t i = 0; i < n; ++i) {
+    if (!finite3(x + 3 * i)) continue;
+    for (int64_t j = i + 1; j < n; ++j) {
+      if (!finite3(x + 3 * j)) continue;
+      if (excluded_pair(excl_off, excl, (int32_t)i, (int32_t)j)) continue;
+      double d0[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+      double mc = -rint(d0[2] / cz);
+      d0[0] += mc * cx; d0[1] += mc * cy; d0[2] += mc * cz;
+      double mb = -rint(d0[1] / by);
+      d0[0] += mb * bx; d0[1] += mb * by;
+      d0[0] += -rint(d0[0] / ax) * ax;
+      for (int tc = -span; tc <= span; ++tc)
+        for (int tb = -span; tb <= span; ++tb)
+          for (int ta = -span; ta <= span; ++ta) {
+            double d[3] = {d0[0] + ta * ax + tb * bx + tc * cx, d0[1] + tb * by + tc * cy, d0[2] + tc * cz};
+            double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (!(r2 < rc2)) continue;
+            double r = sqrt(r2);
+            double fscal = 0.0;
+            int ti = type[i], tj = type[j];
+            double sg = sigma[ti * ntypes + tj], ep = epsilon[ti * ntypes + tj];
+            if (ep != 0.0) {
+              double sr = sg / r, s6 = pow(sr, 6.0), s12 = s6 * s6;
+              elj += 4.0 * ep * (s12 - s6);
+              fscal += -(4.0 * ep * (-12.0 * s12 + 6.0 * s6) / r) / r;
+            }
+            double qq = coulomb * q[i] * q[j];
+            if (qq != 0.0) {
+              double er = erfc(beta * r);
+              ecoul += qq * er / r;
+              fscal += -(qq * (-er / r2 - twobeta_sqrtpi * exp(-beta * beta * r2) / r)) / r;
+            }
+            for (int k = 0; k < 3; ++k) {
+              forces[3 * i + k] += fscal * d[k];
+              forces[3 * j + k] -= fscal * d[k];
+            }
+            for (int a2 = 0; a2 < 3; ++a2)
+              for (int b2 = 0; b2 < 3; ++b2) W[3 * a2 + b2] += d[a2] * fscal * d[b2];
+          }
+    }
+  }
+  energies[0] += elj;
+  energies[1] += ecoul;
+  for (int k = 0; k < 9; ++k) virial[k] += W[k];
+}
+
+/* orc_excluded in a triclinic cell: the minimum image reduced once along
+ * c, b, a. */
+void orc_excluded_triclinic(int64_t npairs, const int32_t *pairs, const double *x, const double *q,
+                            const double *cell, double beta, double coulomb, double *forces, double *energies,
+                            double *virial) {
+  double ax = cell[0], by = cell[1], cz = cell[2], bx = cell[3], cx = cell[4], cy = cell[5];
+  double e = 0.0;
+  double twobeta_sqrtpi = 2.0 * beta / sqrt(M_PI);
+  for (int64_t p = 0; p < npairs; ++p) {
+    int32_t i = pairs[2 * p], j = pairs[2 * p + 1];
+    double d[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+    double mc = -rint(d[2] / cz);
+    d[0] += mc * cx; d[1] += mc * cy; d[2] += mc * cz;
+    double mb = -rint(d[1] / by);
+    d[0] += mb * bx; d[1] += mb * by;
+    d[0] += -rint(d[0] / ax) * ax;
+    double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    double qq = coulomb * q[i] * q[j];
+    if (qq == 0.0 || r2 <= 0.0) continue;
+    double r = sqrt(r2);
+    double ef = erf(beta * r);
+    e += -qq * ef / r;
+    double fs = qq * (twobeta_sqrtpi * exp(-beta * beta * r2) / r2 - ef / (r2 * r));
+    for (int k = 0; k < 3; ++k) {
+      forces[3 * i + k] += fs * d[k];
+      forces[3 * j + k] -= fs * d[k];
+    }
+    for (int a2 = 0; a2 < 3; ++a2)
+      for (int b2 = 0; b2 < 3; ++b2) virial[3 * a2 + b2] += d[a2] * fs * d[b2];
+  }
+  energies[0] += e;
+}

@@ -65,6 +65,10 @@ def lib():
         _lib.orc_pairset_triclinic.argtypes = [i64, p, p, d, p, p, i32, i64, p, p]
         _lib.orc_pairset_triclinic_f32.restype = i64
         _lib.orc_pairset_triclinic_f32.argtypes = [i64, p, p, d, p, p, i32, i64, p]
+        _lib.orc_nonbonded_triclinic.restype = None
+        _lib.orc_nonbonded_triclinic.argtypes = [i64, p, p, p, i32, p, p, p, d, d, d, p, p, i32, p, p, p]
+        _lib.orc_excluded_triclinic.restype = None
+        _lib.orc_excluded_triclinic.argtypes = [i64, p, p, p, p, d, d, p, p, p]
     return _lib
 
 
@@ -125,6 +129,34 @@ def pairset_triclinic_f32(x, cell, reach, excl=None, want_list=True, span=3):
     out = np.zeros((max(count, 1), 5), dtype=np.int32)
     lib().orc_pairset_triclinic_f32(n, _ptr(x), _ptr(cell), reach, _ptr(off), _ptr(ex), span, count, _ptr(out))
     return count, out[:count]
+
+
+def direct_triclinic(system, x, cell, span=2):
+    """FP64 forces and energies of the pair term (every image within the
+    cutoff) and of the excluded-pair correction in a triclinic cell, for a
+    system dict as `evaluate` takes (no reciprocal, self or background
+    terms): {"forces", "lj", "coulomb", "excluded", "virial"}."""
+    x = _c(x, np.float64)
+    cell = _c(cell, np.float64)
+    n = len(x)
+    q = _c(system["charges"], np.float64)
+    t = _c(system["types"], np.int32)
+    sig = _c(system["sigma"], np.float64)  # type-pair tables, as evaluate takes them
+    eps = _c(system["epsilon"], np.float64)
+    pairs = np.asarray(system.get("excluded_pairs", np.zeros((0, 2))), dtype=np.int32).reshape(-1, 2)
+    off, ex = rows_from_pairs(n, pairs) if len(pairs) else (None, None)
+    f = np.zeros((n, 3))
+    e = np.zeros(2)
+    w = np.zeros(9)
+    lib().orc_nonbonded_triclinic(n, _ptr(x), _ptr(q), _ptr(t), sig.shape[0], _ptr(sig), _ptr(eps),
+                                  _ptr(cell), system["cutoff"], system["beta"], system.get("coulomb", COULOMB),
+                                  _ptr(None if off is None else _c(off, np.int32)),
+                                  _ptr(None if ex is None else _c(ex, np.int32)), span, _ptr(f), _ptr(e), _ptr(w))
+    ee = np.zeros(1)
+    pp = _c(pairs, np.int32)
+    lib().orc_excluded_triclinic(len(pp), _ptr(pp), _ptr(x), _ptr(q), _ptr(cell), system["beta"],
+                                 system.get("coulomb", COULOMB), _ptr(f), _ptr(ee), _ptr(w))
+    return {"forces": f, "lj": e[0], "coulomb": e[1], "excluded": ee[0], "virial": w.reshape(3, 3)}
 
 
 def pairset_triclinic(x, cell, reach, excl=None, want_list=True, span=2):
