@@ -187,10 +187,13 @@ int32_t mdrtNbForce(mdrtNb *ctx, const double *x, const double box[3], uint32_t 
  * The lists hold every image within the reach once (several images of a
  * pair when the reach exceeds half the cell).  A context built in a
  * triclinic cell takes its forces from mdrtNbForceTriclinic with the same
- * cell (mdrtNbForce refuses it); the pruning, energies and constants work
- * as in an orthorhombic cell (box = the diagonal).  PME, the parameter
- * gradient, the displacement test, the MD step and batches run in
- * orthorhombic cells only (MDRT_NB_UNSUPPORTED).
+ * cell (mdrtNbForce refuses it); the pruning, energies, constants and
+ * mdrtPmePotential work as in an orthorhombic cell (box = the diagonal).
+ * PME spreads and gathers on the fractional coordinates f = x H^-1 with the
+ * wave vectors m = H^-1 k (docs/pme.md, Section 1; V = ax by cz).  The
+ * parameter gradient and the displacement test run in orthorhombic cells
+ * only (MDRT_NB_UNSUPPORTED); the MD step and batches build orthorhombic
+ * cells.
  * MDIR: mdrt_gpu_build_neighbors_groups_triclinic(x, vector<6xf64>, ...)
  * (GroupsBuild.cpp:248-345, docs/neighbor-groups.md Section 5.1, D126);
  * its lists are checked by test/Runtime/neighbors-groups-triclinic-gpu.mlir. */

@@ -404,7 +404,6 @@ static int32_t nb_force_entry(mdrtNb *ctx, const double *x, const double box[3],
   bool pairs = !(flags & MDRT_NB_NO_PAIRS);
   bool excluded = !(flags & MDRT_NB_NO_EXCLUDED);
   bool pme = c.pme.on && !(flags & MDRT_NB_NO_PME) && c.beta > 0.0;
-  if (pme && nb_triclinic(c)) return MDRT_NB_UNSUPPORTED;  // PME in orthorhombic cells
   if (!(flags & MDRT_NB_ACCUMULATE)) CK(cudaMemsetAsync(forces, 0, sizeof(double) * 3 * c.n, st));
   if (energy) CK(cudaMemsetAsync(c.energy, 0, sizeof(double) * NB_E_SLOTS, st));
   nb_gather_frames(c, x, box, st);

@@ -45,9 +45,7 @@ __global__ void __launch_bounds__(256) nb_spread(GridParams G, int64_t places,
   if (v.w == 0.f) return;
   int k0, k1, k2;
   float t0, t1, t2;
-  nb_frac(v.x, G.invL0, G.K0, k0, t0);
-  nb_frac(v.y, G.invL1, G.K1, k1, t1);
-  nb_frac(v.z, G.invL2, G.K2, k2, t2);
+  nb_frac3(v, G, k0, k1, k2, t0, t1, t2);
   float w0[P], w1[P], w2[P];
   nb_bspline<P>(t0, w0, nullptr);
   nb_bspline<P>(t1, w1, nullptr);
@@ -86,6 +84,7 @@ __global__ void nb_fixed_to_grid(int64_t total, unsigned long long *__restrict__
 struct ConvParams {
   int K0, K1, K2, H2;  // H2 = K2/2 + 1
   double L0, L1, L2;
+  double h10 = 0.0, h20 = 0.0, h21 = 0.0;  // H^-1 (1,0), (2,0), (2,1) of a triclinic cell
   double pref;       // f / (pi V)
   double pi2_beta2;  // pi^2 / beta^2
 };
@@ -98,9 +97,12 @@ __device__ __forceinline__ double nb_bc(const ConvParams &C, const float *__rest
   int64_t r = k / C.H2;
   int i1 = (int)(r % C.K1);
   int i0 = (int)(r / C.K1);
-  m0 = (i0 <= C.K0 / 2 ? i0 : i0 - C.K0) / C.L0;
-  m1 = (i1 <= C.K1 / 2 ? i1 : i1 - C.K1) / C.L1;
-  m2v = (i2 <= C.K2 / 2 ? i2 : i2 - C.K2) / C.L2;
+  // m = k0 a* + k1 b* + k2 c*, the reciprocal vectors the columns of H^-1
+  double k0s = (i0 <= C.K0 / 2 ? i0 : i0 - C.K0), k1s = (i1 <= C.K1 / 2 ? i1 : i1 - C.K1);
+  double k2s = (i2 <= C.K2 / 2 ? i2 : i2 - C.K2);
+  m0 = k0s / C.L0;
+  m1 = k1s / C.L1 + k0s * C.h10;
+  m2v = k2s / C.L2 + k0s * C.h20 + k1s * C.h21;
   mm = m0 * m0 + m1 * m1 + m2v * m2v;
   if (k == 0) return 0.0;
   double B = (double)moduli[i0] * (double)moduli[C.K0 + i1] * (double)moduli[C.K0 + C.K1 + i2];
@@ -212,9 +214,7 @@ __global__ void __launch_bounds__(128) nb_pme_gather(GridParams G, int64_t place
   float4 v = xq[p];
   int k0, k1, k2;
   float t0, t1, t2;
-  nb_frac(v.x, G.invL0, G.K0, k0, t0);
-  nb_frac(v.y, G.invL1, G.K1, k1, t1);
-  nb_frac(v.z, G.invL2, G.K2, k2, t2);
+  nb_frac3(v, G, k0, k1, k2, t0, t1, t2);
   float w0[P], w1[P], w2[P], d0[P], d1[P], d2[P];
   nb_bspline<P>(t0, w0, d0);
   nb_bspline<P>(t1, w1, d1);
@@ -249,8 +249,8 @@ __global__ void __launch_bounds__(128) nb_pme_gather(GridParams G, int64_t place
     }
   }
   float q = v.w;
-  out[p] = make_float4(-q * g0 * (float)G.K0 * G.invL0, -q * g1 * (float)G.K1 * G.invL1,
-                       -q * g2 * (float)G.K2 * G.invL2, 0.f);
+  float3 F = nb_frac_force(G, q, g0, g1, g2);
+  out[p] = make_float4(F.x, F.y, F.z, 0.f);
   if (pot) pot[p] = e;
 }
 
@@ -275,9 +275,7 @@ __global__ void __launch_bounds__(128) nb_pme_gather_split(GridParams G, int64_t
     v = xq[p];
     int k0, k1, k2;
     float t0, t1, t2;
-    nb_frac(v.x, G.invL0, G.K0, k0, t0);
-    nb_frac(v.y, G.invL1, G.K1, k1, t1);
-    nb_frac(v.z, G.invL2, G.K2, k2, t2);
+    nb_frac3(v, G, k0, k1, k2, t0, t1, t2);
     float w0[P], w1[P], w2[P], d0[P], d1[P], d2[P];
     nb_bspline<P>(t0, w0, d0);
     nb_bspline<P>(t1, w1, d1);
@@ -320,8 +318,8 @@ __global__ void __launch_bounds__(128) nb_pme_gather_split(GridParams G, int64_t
     return;
   }
   float q = v.w;
-  out[p] = make_float4(-q * g0 * (float)G.K0 * G.invL0, -q * g1 * (float)G.K1 * G.invL1,
-                       -q * g2 * (float)G.K2 * G.invL2, 0.f);
+  float3 F = nb_frac_force(G, q, g0, g1, g2);
+  out[p] = make_float4(F.x, F.y, F.z, 0.f);
   if (pot) pot[p] = e;
 }
 
@@ -511,6 +509,27 @@ void nb_pme_release(NbCtx &c) {
   P.on = false;
 }
 
+// The tilt terms of a triclinic cell (box = its diagonal, c.tilt = bx, cx,
+// cy) for the fractions, the gradients and the reciprocal vectors: the
+// entries of H^-1 below its diagonal, (1,0) = -bx/(ax by),
+// (2,0) = (bx cy - by cx)/(ax by cz), (2,1) = -cy/(by cz).  Zero in an
+// orthorhombic cell.
+static void nb_cell_tilts(const NbCtx &c, const double box[3], GridParams &G, ConvParams *C) {
+  double ax = box[0], by = box[1], cz = box[2], bx = c.tilt[0], cx = c.tilt[1], cy = c.tilt[2];
+  double h10 = -bx / (ax * by), h20 = (bx * cy - by * cx) / (ax * by * cz), h21 = -cy / (by * cz);
+  G.ta_b = (float)(bx / ax);
+  G.ta_c = (float)(cx / ax);
+  G.tb_c = (float)(cy / by);
+  G.h10 = (float)h10;
+  G.h20 = (float)h20;
+  G.h21 = (float)h21;
+  if (C) {
+    C->h10 = h10;
+    C->h20 = h20;
+    C->h21 = h21;
+  }
+}
+
 int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaStream_t s) {
   NbPme &P = c.pme;
   if (!P.on) return 0;
@@ -521,6 +540,7 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
   G.invL0 = (float)(1.0 / box[0]);
   G.invL1 = (float)(1.0 / box[1]);
   G.invL2 = (float)(1.0 / box[2]);
+  nb_cell_tilts(c, box, G, nullptr);
   int64_t total = (int64_t)G.K0 * G.K1 * G.K2;
   int64_t half = (int64_t)G.K0 * G.K1 * (G.K2 / 2 + 1);
   int64_t threads = c.places_cap * P.order;
@@ -553,6 +573,7 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
   C.L2 = box[2];
   C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
   C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
+  nb_cell_tilts(c, box, G, &C);
   if (energy) {
     nb_convolve<true><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
     nb_pme_sum<<<1, 256, 0, s>>>(P.partials, P.conv_blocks, c.energy);
@@ -824,8 +845,8 @@ __global__ void __launch_bounds__(128) nb_batch_gather_split(int64_t places, con
     return;
   }
   float q = v.w;
-  out[p] = make_float4(-q * g0 * (float)G.K0 * G.invL0, -q * g1 * (float)G.K1 * G.invL1,
-                       -q * g2 * (float)G.K2 * G.invL2, 0.f);
+  float3 F = nb_frac_force(G, q, g0, g1, g2);
+  out[p] = make_float4(F.x, F.y, F.z, 0.f);
 }
 
 }  // namespace

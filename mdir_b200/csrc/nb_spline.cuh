@@ -59,4 +59,50 @@ __device__ __forceinline__ void nb_frac(float x, float invL, int K, int &k0, flo
 struct GridParams {
   int K0, K1, K2;
   float invL0, invL1, invL2;
+  // a triclinic cell (0 in an orthorhombic one): the fractions' tilt terms
+  // bx/ax, cx/ax, cy/by, and the off-diagonal entries (1,0), (2,0), (2,1)
+  // of H^-1, which take the spline slopes to Cartesian gradients
+  float ta_b = 0.f, ta_c = 0.f, tb_c = 0.f;
+  float h10 = 0.f, h20 = 0.f, h21 = 0.f;
 };
+
+// The grid points and fractions of a centred frame v in a triclinic cell
+// (the position p = v + diag/2 = fa a + fb b + fc c): fc = v.z/cz + 1/2,
+// fb = v.y/by + 1/2 - fc cy/by, fa = v.x/ax + 1/2 - fb bx/ax - fc cx/ax; in
+// an orthorhombic cell these are nb_frac's per axis, bit for bit.
+__device__ __forceinline__ void nb_frac3(float4 v, const GridParams &G, int &k0, int &k1, int &k2, float &t0,
+                                         float &t1, float &t2) {
+  float fc = fmaf(v.z, G.invL2, 0.5f);
+  float fb = fmaf(v.y, G.invL1, 0.5f) - fc * G.tb_c;
+  float fa = fmaf(v.x, G.invL0, 0.5f) - (fb * G.ta_b + fc * G.ta_c);
+  float f[3] = {fa, fb, fc};
+  int K[3] = {G.K0, G.K1, G.K2};
+  int kk[3];
+  float tt[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float g = f[a] - floorf(f[a]);
+    float u = g * (float)K[a];
+    float fl = floorf(u);
+    int k = (int)fl;
+    if (k >= K[a]) k -= K[a];
+    if (k < 0) k += K[a];
+    kk[a] = k;
+    float t = u - fl;
+    tt[a] = t >= 1.f ? 0.f : t;
+  }
+  k0 = kk[0];
+  k1 = kk[1];
+  k2 = kk[2];
+  t0 = tt[0];
+  t1 = tt[1];
+  t2 = tt[2];
+}
+
+// The force -q grad(sum phi W) from the spline-slope sums (g0, g1, g2) of
+// the three fractions: -q H^-1 (K0 g0, K1 g1, K2 g2); per axis in an
+// orthorhombic cell.
+__device__ __forceinline__ float3 nb_frac_force(const GridParams &G, float q, float g0, float g1, float g2) {
+  float ga = -q * g0 * (float)G.K0, gb = -q * g1 * (float)G.K1, gc = -q * g2 * (float)G.K2;
+  return make_float3(ga * G.invL0, gb * G.invL1 + ga * G.h10, gc * G.invL2 + ga * G.h20 + gb * G.h21);
+}

@@ -293,6 +293,80 @@ def pme(x, q, box, K, order, beta, coulomb=COULOMB):
     return energy, forces, W, pot
 
 
+def pme_triclinic(x, q, cell, K, order, beta, coulomb=COULOMB):
+    """SPME in a triclinic cell (ax, by, cz, bx, cx, cy): the spreading and
+    gathering of `pme` on the fractional coordinates f = x H^-1, the wave
+    vectors m = H^-1 k (the reciprocal vectors are the columns of H^-1),
+    V = ax by cz; the gathered fractional forces taken to Cartesian ones by
+    H^-1.  Returns (energy, forces, virial, dE/dq) as `pme`."""
+    x = _c(x, np.float64)
+    q = _c(q, np.float64)
+    H = cell_matrix(cell)
+    Hinv = np.linalg.inv(H)
+    f = np.ascontiguousarray(x @ Hinv)
+    unit = _c([1.0, 1.0, 1.0], np.float64)
+    Ka = np.asarray(K, dtype=np.int64)
+    n = len(x)
+    grid = np.zeros(tuple(K))
+    lib().orc_pme_spread(n, _ptr(f), _ptr(q), _ptr(unit), _ptr(Ka), order, _ptr(grid))
+    V = float(cell[0] * cell[1] * cell[2])
+    ks = []
+    for a in range(3):
+        idx = np.arange(K[a]) if a < 2 else np.arange(K[2] // 2 + 1)
+        ks.append(np.where(idx <= K[a] // 2, idx, idx - K[a]).astype(np.float64))
+    k0, k1, k2 = np.meshgrid(ks[0], ks[1], ks[2], indexing="ij")
+    mx = Hinv[0, 0] * k0 + Hinv[0, 1] * k1 + Hinv[0, 2] * k2
+    my = Hinv[1, 0] * k0 + Hinv[1, 1] * k1 + Hinv[1, 2] * k2
+    mz = Hinv[2, 0] * k0 + Hinv[2, 1] * k1 + Hinv[2, 2] * k2
+    m2 = mx * mx + my * my + mz * mz
+    B = (bspline_moduli(K[0], order)[:, None, None] * bspline_moduli(K[1], order)[None, :, None]
+         * bspline_moduli(K[2], order)[None, None, :K[2] // 2 + 1])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        C = coulomb / (math.pi * V) * np.exp(-math.pi ** 2 * m2 / beta ** 2) / m2
+    C[0, 0, 0] = 0.0
+    bc = B * C
+    S = np.fft.rfftn(grid)
+    power = (S.real ** 2 + S.imag ** 2)
+    weight = np.full(bc.shape[2], 2.0)
+    weight[0] = 1.0
+    if K[2] % 2 == 0:
+        weight[-1] = 1.0
+    Em = 0.5 * bc * power * weight[None, None, :]
+    energy = float(Em.sum())
+    with np.errstate(divide="ignore", invalid="ignore"):
+        fm = -2.0 * (1.0 / m2 + math.pi ** 2 / beta ** 2)
+    fm[0, 0, 0] = 0.0
+    mv = (mx, my, mz)
+    W = np.zeros((3, 3))
+    for a in range(3):
+        for b in range(3):
+            W[a, b] = float((Em * ((1.0 if a == b else 0.0) + fm * mv[a] * mv[b])).sum())
+    phi = np.ascontiguousarray(np.fft.irfftn(bc * S, s=tuple(K), axes=(0, 1, 2)) * (K[0] * K[1] * K[2]))
+    ffrac = np.zeros((n, 3))
+    pot = np.zeros(n)
+    lib().orc_pme_gather(n, _ptr(f), _ptr(q), _ptr(unit), _ptr(Ka), order, _ptr(phi), _ptr(ffrac), _ptr(pot))
+    return energy, ffrac @ Hinv.T, W, pot
+
+
+def evaluate_triclinic(system, x, cell):
+    """Every term of a system dict in a triclinic cell (pairs, excluded,
+    reciprocal, self, background): as `evaluate`."""
+    q = np.asarray(system["charges"], dtype=np.float64)
+    d = direct_triclinic(system, x, cell)
+    terms = {"lj": d["lj"], "coulomb": d["coulomb"], "excluded": d["excluded"]}
+    forces = d["forces"].copy()
+    W = d["virial"].copy()
+    e_rec, f_rec, w_rec, pot = pme_triclinic(x, q, cell, system["grid"], system["order"], system["beta"])
+    terms["reciprocal"] = e_rec
+    forces += f_rec
+    W += w_rec
+    terms["self"] = self_energy(q, system["beta"])
+    eb = background_energy(q, cell[:3], system["beta"])
+    terms["background"] = eb
+    W += np.eye(3) * eb
+    return {"energy": sum(terms.values()), "terms": terms, "forces": forces, "virial": W, "potential": pot}
+
+
 def ewald_sum_reciprocal(x, q, box, beta, coulomb=COULOMB, gauss=1e-18):
     """The reciprocal energy by the Ewald sum over wave vectors (the method of
     test/Driver/Inputs/ewald_reference.py), for small systems."""
@@ -308,6 +382,33 @@ def ewald_sum_reciprocal(x, q, box, beta, coulomb=COULOMB, gauss=1e-18):
                 if a == 0 and (b < 0 or (b == 0 and c <= 0)):
                     continue
                 m = np.array([a / box[0], b / box[1], c / box[2]])
+                m2 = float(m @ m)
+                if m2 > limit * limit:
+                    continue
+                ph = 2 * math.pi * (x @ m)
+                re, im = float(q @ np.cos(ph)), float(q @ np.sin(ph))
+                e += 2 * coulomb / (2 * math.pi * V) * math.exp(-math.pi ** 2 * m2 / beta ** 2) / m2 * (re * re + im * im)
+    return e
+
+
+def ewald_sum_reciprocal_triclinic(x, q, cell, beta, coulomb=COULOMB, gauss=1e-18):
+    """The reciprocal energy by the Ewald sum over the wave vectors m = H^-1 k
+    of a triclinic cell, for small systems (the check of pme_triclinic)."""
+    x = np.asarray(x, dtype=np.float64)
+    q = np.asarray(q, dtype=np.float64)
+    H = cell_matrix(cell)
+    Hinv = np.linalg.inv(H)
+    V = float(cell[0] * cell[1] * cell[2])
+    limit = beta * math.sqrt(-math.log(gauss)) / math.pi
+    # |k_a| <= limit |a| bounds every k with |m| <= limit (m . a = k_a)
+    kmax = [int(limit * np.linalg.norm(H[a])) + 1 for a in range(3)]
+    e = 0.0
+    for a in range(0, kmax[0] + 1):
+        for b in range(-kmax[1], kmax[1] + 1):
+            for c in range(-kmax[2], kmax[2] + 1):
+                if a == 0 and (b < 0 or (b == 0 and c <= 0)):
+                    continue
+                m = Hinv @ np.array([a, b, c], dtype=np.float64)
                 m2 = float(m @ m)
                 if m2 > limit * limit:
                     continue

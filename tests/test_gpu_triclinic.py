@@ -101,8 +101,36 @@ def test_triclinic_refusals(cuda):
     with pytest.raises(_lib.NativeError) as e:  # forces of a triclinic build in its own cell only
         t.force(xd, list(CELLS[0])[:3])
     assert e.value.status == _lib.INVALID_BOX
-    t.set_pme([32, 32, 32], 4)
-    with pytest.raises(_lib.NativeError) as e:  # PME runs in orthorhombic cells
-        t.force(xd, list(CELLS[0]))
+    g = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.NativeError) as e:  # the adjoint runs in orthorhombic cells
+        t.parameter_gradient(xd, g, box=list(CELLS[0])[:3])
     assert e.value.status == _lib.UNSUPPORTED
+    t.close()
+
+
+@pytest.mark.parametrize("cell", CELLS)
+def test_triclinic_pme_forces_and_energies_match_fp64(cuda, cell):
+    """The whole term with SPME in a triclinic cell (fractional spreading
+    and gathering, wave vectors H^-1 k) against the FP64 oracle."""
+    from mdir_b200 import NonbondedTerm
+    s = charged_lattice(cell)
+    s["grid"], s["order"] = (36, 36, 32), 4
+    n = len(s["charges"])
+    t = NonbondedTerm(n)
+    t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t.set_exclusions(pairs=s["excluded_pairs"])
+    t.set_interaction(s["cutoff"], s["reach"], s["beta"])
+    t.set_pme(s["grid"], s["order"])
+    xd = torch.tensor(s["positions"], dtype=torch.float64, device="cuda")
+    t.build(xd, list(cell))
+    f = t.force(xd, list(cell), energy=True).cpu().numpy()
+    e = t.energies()
+    ref = O.evaluate_triclinic(s, s["positions"], cell)
+    err = np.sqrt(np.mean(np.sum((f - ref["forces"]) ** 2, 1)) / np.mean(np.sum(ref["forces"] ** 2, 1)))
+    assert err < 1e-5, err
+    scale = sum(abs(v) for v in ref["terms"].values())
+    for name in ("lj", "coulomb", "excluded", "reciprocal"):
+        assert abs(e[name] - ref["terms"][name]) <= 1e-6 * scale, (name, e[name], ref["terms"][name])
+    c = t.constants(list(cell)[:3])
+    assert abs(c["self"] - ref["terms"]["self"]) <= 1e-9 * abs(ref["terms"]["self"])
     t.close()

@@ -158,3 +158,33 @@ def test_beta_and_grid_of_the_water_box():
     L = (7850 / 33.4) ** (1 / 3)
     assert O.pme_grid([L] * 3, 0.1, 4) == [64, 64, 64]
     assert O.pme_grid([22.008] * 3, 0.1, 4) == [224, 224, 224]
+
+
+def test_triclinic_pme_is_the_ewald_sum_and_its_gradient():
+    """SPME in a triclinic cell (fractional spreading, m = H^-1 k): the
+    energy is the Ewald sum over wave vectors, the forces are its central
+    differences, and with no tilts it is the orthorhombic SPME."""
+    rng = np.random.default_rng(11)
+    cell = (2.4, 2.2, 2.1, -0.8, 0.9, -1.0)
+    H = O.cell_matrix(cell)
+    n = 24
+    x = rng.uniform(0, 1, size=(n, 3)) @ H
+    q = rng.normal(0, 0.5, size=n)
+    q -= q.mean()
+    beta, K, order = 3.0, (48, 48, 48), 8
+    e, f, W, pot = O.pme_triclinic(x, q, cell, K, order, beta)
+    e_ref = O.ewald_sum_reciprocal_triclinic(x, q, cell, beta)
+    assert abs(e - e_ref) < 1e-5 * abs(e_ref), (e, e_ref)
+    h = 1e-5
+    for i in (0, 7):
+        for a in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[i, a] += h
+            xm[i, a] -= h
+            fd = -(O.pme_triclinic(xp, q, cell, K, order, beta)[0] - O.pme_triclinic(xm, q, cell, K, order, beta)[0]) / (2 * h)
+            assert abs(f[i, a] - fd) < 1e-6 * max(1.0, np.abs(f).max()), (i, a, f[i, a], fd)
+    box = (2.4, 2.2, 2.1)
+    e0, f0, W0, p0 = O.pme(x, q, box, K, order, beta)
+    e1, f1, W1, p1 = O.pme_triclinic(x, q, box + (0.0, 0.0, 0.0), K, order, beta)
+    assert abs(e0 - e1) < 1e-12 * abs(e0)
+    np.testing.assert_allclose(f1, f0, rtol=1e-10, atol=1e-10)
