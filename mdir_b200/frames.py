@@ -271,16 +271,34 @@ class FrameEvaluator:
         """Energies of the frames and the gradients asked for: "positions"
         (dU/dx, (K, n, 3)) and "tunables" (per frame: sigma (K, nt),
         epsilon (K, nt), charges (K, n)).  MDIR: FrameEvaluator.evaluate,
-        python/mdir/_frames.py:715.  The cell is the system's (orthorhombic);
-        another cell or tilts are refused."""
-        if tilts is not None:
-            raise UnsupportedError("triclinic cells are not implemented")
-        if cells is not None and not np.allclose(np.asarray(cells, dtype=np.float64).reshape(-1, 3), self.box):
-            raise UnsupportedError("frames in another cell than the system's")
+        python/mdir/_frames.py:715.  The cell is the system's edges; `tilts`
+        (bx, cx, cy), one cell for every frame, makes it triclinic (the
+        lists are built for each frame; the tunables' gradient runs in
+        orthorhombic cells only).  Another cell is refused."""
         for g in gradients:
             if g not in ("tunables", "positions"):
                 raise ValueError(f"unknown gradient {g!r}")
+        if cells is not None and not np.allclose(np.asarray(cells, dtype=np.float64).reshape(-1, 3), self.box):
+            raise UnsupportedError("frames in another cell than the system's")
         X = self.frames(positions)
+        if tilts is not None:
+            t = np.asarray(tilts, dtype=np.float64).reshape(-1, 3)
+            if not np.allclose(t, t[0]):
+                raise UnsupportedError("frames in different triclinic cells")
+            if "tunables" in gradients:
+                raise UnsupportedError("parameter gradients in triclinic cells are not implemented")
+            cell = np.concatenate([self.box, t[0]])
+            self._upload()
+            F = torch.empty_like(X)
+            E = np.zeros(X.shape[0])
+            for k in range(X.shape[0]):
+                self.term.build(X[k], cell, self.reach)
+                self.builds += 1
+                self.term.force(X[k], cell, energy=True, forces=F[k])
+                E[k] = self._energy()
+            self._built = False  # the lists are the triclinic build's
+            out = {"positions": -F} if "positions" in gradients else {}
+            return FrameEnergies(self, X, E, out)
         F, E = self.forces(X, energy=True)
         out = {}
         if "positions" in gradients:

@@ -134,3 +134,26 @@ def test_triclinic_pme_forces_and_energies_match_fp64(cuda, cell):
     c = t.constants(list(cell)[:3])
     assert abs(c["self"] - ref["terms"]["self"]) <= 1e-9 * abs(ref["terms"]["self"])
     t.close()
+
+
+def test_frame_evaluator_in_a_triclinic_cell(cuda):
+    """FrameEvaluator.evaluate(positions, tilts=...) gives the FP64 energies
+    and forces of each frame in the triclinic cell."""
+    from mdir_b200 import FrameEvaluator
+    cell = CELLS[1]
+    s = charged_lattice(cell)
+    s["grid"], s["order"] = (36, 36, 32), 4
+    s["box"] = np.array(cell[:3])
+    rng = np.random.default_rng(5)
+    frames = np.stack([s["positions"] + rng.normal(0, 0.002, s["positions"].shape) for _ in range(2)])
+    ev = FrameEvaluator(s)
+    res = ev.evaluate(frames, tilts=cell[3:], gradients=("positions",))
+    for k in range(2):
+        ref = O.evaluate_triclinic(s, frames[k], cell)
+        assert abs(res.energy[k] - ref["energy"]) <= 1e-6 * sum(abs(v) for v in ref["terms"].values())
+        f = -res.gradients["positions"][k].cpu().numpy()
+        err = np.sqrt(np.mean(np.sum((f - ref["forces"]) ** 2, 1)) / np.mean(np.sum(ref["forces"] ** 2, 1)))
+        assert err < 1e-5, err
+    from mdir_b200.api import UnsupportedError
+    with pytest.raises(UnsupportedError):
+        ev.evaluate(frames, tilts=cell[3:])  # the tunables' gradient: orthorhombic cells only
