@@ -563,10 +563,13 @@ def main():
     # grow its lists once ahead of need
     for _ in range(5):
         e2e_step()
-    e_steps = max(3, args.steps // 2)
+    e_steps = max(3, args.steps)
+    step_sec = []
     t0 = time.perf_counter()
     for _ in range(e_steps):
+        t1 = time.perf_counter()
         e2e_step()
+        step_sec.append(time.perf_counter() - t1)
     e2e_sec = (time.perf_counter() - t0)
     if world > 1:
         t = torch.tensor([e2e_sec], device=dev)
@@ -617,7 +620,9 @@ def main():
             "dtype": "f32 pairs / f64 sums (mixed)", "data": "synthetic (seeded TIP3P box, random orientations)",
             "config": config(args, s), "clocks": clk,
             "e2e": {"value": round(e2e, 2), "unit": "ns/day", "h2d_bytes_per_step": 2 * n * 3 * 8,
-                    "d2h_bytes_per_step": 2 * n * 3 * 8 + 4},
+                    "d2h_bytes_per_step": 2 * n * 3 * 8 + 4, "steps": e_steps,
+                    "median_step_ms": round(float(np.median(step_sec)) * 1e3, 3),
+                    "max_step_ms": round(float(np.max(step_sec)) * 1e3, 3)},
             "roofline": roofline,
             # this library's kernels per MD step: the gated pruning, spread,
             # spectrum scaling, pairs, update (cuFFT's own kernels not
