@@ -787,14 +787,19 @@ __global__ void nb_charge_terms(int64_t n, const float *__restrict__ q, double s
   gq[i] += self2 * (double)q[i] + background;
 }
 
-// Fixed-order sum of the per-block type-pair partials, added into out.
+// Fixed-order sum of the per-block type-pair partials, added into out: a
+// warp per value, lane l summing blocks l, l + 32, ... in turn, then the
+// lanes by a fixed shuffle tree (the same order every call, 19 dependent
+// loads a lane where one thread a value took 592).
 __global__ void nb_sum_type_partials(const double *__restrict__ partials, int nblocks, int width,
                                      double *__restrict__ out) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= width) return;
+  int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (k >= width) return;  // whole warps
   double s = 0.0;
-  for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)b * width + k];
-  out[k] += s;
+  for (int b = lane; b < nblocks; b += 32) s += partials[(int64_t)b * width + k];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[k] += s;
 }
 
 inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
@@ -964,7 +969,7 @@ int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double 
     nb_pairs_adjoint<1><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
                                              c.adj_q, c.adj_types);
   int width = 2 * c.ntypes * c.ntypes;
-  nb_sum_type_partials<<<blocks_for(width, 256), 256, 0, s>>>(c.adj_types, grid, width, dtable);
+  nb_sum_type_partials<<<blocks_for((int64_t)width * 32, 256), 256, 0, s>>>(c.adj_types, grid, width, dtable);
   int rc = nb_pme_adjoint_run(c, box, mode, s);
   if (rc) return rc;
   nb_scatter_place_values<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.adj_q,
