@@ -29,6 +29,8 @@ struct NbPme {
   float *potential = nullptr;   // f32 per place: dE_rec/dq
   double *partials = nullptr;   // per-block energy/virial partials of the convolution
   float *adj_grid = nullptr;    // K0*K1*K2: the dipole grid V, then psi (the adjoint)
+  float *influence = nullptr;   // B C per half-complex point (f32) for the sums without energy
+  double infl_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // cell, beta, f, tilts of that table
   int conv_blocks = 0;
   size_t workspace_bytes = 0;
 };

@@ -474,6 +474,8 @@ int nb_pme_setup(NbCtx &c, int k0, int k1, int k2, int order) {
   if (cudaMalloc(&P.moduli, sizeof(float) * (k0 + k1 + k2)) != cudaSuccess) return -1;
   P.conv_blocks = blocks_for(half, 256);
   if (cudaMalloc(&P.partials, sizeof(double) * 7 * P.conv_blocks) != cudaSuccess) return -1;
+  if (cudaMalloc(&P.influence, sizeof(float) * half) != cudaSuccess) return -1;
+  for (double &k : P.infl_key) k = 0.0;
   std::vector<float> mod;
   for (int K : {k0, k1, k2}) {
     std::vector<double> m = host_moduli(K, order);
@@ -496,9 +498,11 @@ void nb_pme_release(NbCtx &c) {
   if (P.bwd) cufftDestroy(P.bwd);
   P.fwd = P.bwd = 0;
   for (void *p : {(void *)P.grid, (void *)P.spec, (void *)P.fixed, (void *)P.moduli,
-                  (void *)P.pme_force, (void *)P.potential, (void *)P.partials, (void *)P.adj_grid})
+                  (void *)P.pme_force, (void *)P.potential, (void *)P.partials, (void *)P.adj_grid,
+                  (void *)P.influence})
     if (p) cudaFree(p);
   P.adj_grid = nullptr;
+  P.influence = nullptr;
   P.grid = nullptr;
   P.spec = nullptr;
   P.fixed = nullptr;
@@ -528,6 +532,20 @@ static void nb_cell_tilts(const NbCtx &c, const double box[3], GridParams &G, Co
     C->h20 = h20;
     C->h21 = h21;
   }
+}
+
+// The influence table of the context's cell for the convolutions that sum
+// no energy (the forces, the adjoint), made again when the cell, the Ewald
+// parameter, the Coulomb factor or the tilts change.
+static int nb_pme_table(NbCtx &c, const double box[3], cudaStream_t s) {
+  NbPme &P = c.pme;
+  double key[8] = {box[0], box[1], box[2], c.beta, c.coulomb, c.tilt[0], c.tilt[1], c.tilt[2]};
+  bool same = true;
+  for (int k = 0; k < 8; ++k) same = same && key[k] == P.infl_key[k];
+  if (same) return 0;
+  if (nb_pme_influence(c, box, P.influence, s)) return -1;
+  for (int k = 0; k < 8; ++k) P.infl_key[k] = key[k];
+  return 0;
 }
 
 int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaStream_t s) {
@@ -578,7 +596,8 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
     nb_convolve<true><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
     nb_pme_sum<<<1, 256, 0, s>>>(P.partials, P.conv_blocks, c.energy);
   } else {
-    nb_convolve<false><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
+    if (nb_pme_table(c, box, s)) return -1;
+    nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, P.influence, P.spec, nullptr, 0, nullptr);
   }
   if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.grid) != CUFFT_SUCCESS) return -3;
   float *pot = potential ? P.potential : nullptr;
@@ -642,7 +661,8 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s) 
   C.L2 = box[2];
   C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
   C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
-  nb_convolve<false><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
+  if (nb_pme_table(c, box, s)) return -1;
+  nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, P.influence, P.spec, nullptr, 0, nullptr);
   if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.adj_grid) != CUFFT_SUCCESS) return -3;
   switch (P.order) {
     case 4: nb_pme_adjoint_gather<4, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
@@ -1047,6 +1067,8 @@ int nb_pme_influence(NbCtx &c, const double box[3], float *influence, cudaStream
   C.L2 = box[2];
   C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
   C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
+  GridParams G;
+  nb_cell_tilts(c, box, G, &C);
   int64_t half = (int64_t)C.K0 * C.K1 * C.H2;
   nb_influence<<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, influence);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
