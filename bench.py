@@ -54,6 +54,8 @@ def parse():
                    help="blocks of the pair kernel an SM with --no-tune (0: the library's default)")
     p.add_argument("--only", choices=["adjoint", "batch", "precision"], help="run one leg alone (profiling)")
     p.add_argument("--adjoint-frames", type=int, default=64)
+    p.add_argument("--frame-lanes", type=int, default=4,
+                   help="contexts that evaluate the gradient leg's frames side by side")
     p.add_argument("--batch-frames", type=int, default=256)
     p.add_argument("--no-adjoint", action="store_true", help="skip the force-matching gradient leg")
     p.add_argument("--no-batch", action="store_true", help="skip the batch-of-frames leg")
@@ -177,7 +179,7 @@ def adjoint_leg(args, dev, flush, world=1, frames=64, reps=5, warmup=3):
     from mdir_b200.ranks import max_over_ranks, sum_gradients
     s, X, target = systems.force_matching(frames=frames, waters=args.waters)
     n = X.shape[1]
-    ev = FrameEvaluator(s, device=dev.index)
+    ev = FrameEvaluator(s, device=dev.index, lanes=args.frame_lanes)
     Xd = torch.tensor(X, device=dev)
     # target forces: the device forward at the perturbed parameters (untimed)
     ev.set_parameters(target["sigma"], target["epsilon"], target["charges"])
@@ -251,7 +253,7 @@ def adjoint_leg(args, dev, flush, world=1, frames=64, reps=5, warmup=3):
             "forward_ms_per_frame": round(fwd_ms, 4),
             "fd_frames_per_s": round(fd_all, 4), "fd_frames_per_s_lj_only": round(fd_lj, 2),
             "speedup_vs_fd": round(adj_fps / fd_all, 1), "speedup_vs_fd_lj_only": round(adj_fps / fd_lj, 2),
-            "builds_in_timed": int(ev.builds - builds0),
+            "builds_in_timed": int(ev.builds - builds0), "frame_lanes": ev.lanes,
             "gradient_error": "adjoint vs FP64 central differences (h = 1e-5) <= 1e-4 per element "
                               "(tests/test_gpu_adjoint.py, 23,550 atoms)",
             "targets": "device forward at parameters x (1 +- 2%)",

@@ -121,9 +121,19 @@ class FrameEnergies:
 
 
 class FrameEvaluator:
-    """Energies, forces and parameter gradients of frames of one system."""
+    """Energies, forces and parameter gradients of frames of one system.
 
-    def __init__(self, system, device=0, sigma=None, epsilon=None, charges=None):
+    `lanes` contexts evaluate the frames of one call side by side, frame i
+    of the call on lane i mod lanes: lane 0 on the caller's current stream,
+    the others on streams of their own, each with its own lists (built at
+    the positions of the build in force when it first gets a frame after
+    that build) and scratch.  The kernels of one 23,550-atom frame leave
+    most of the GPU idle between its two pair launches (FFTs of a 64^3 grid,
+    spreading, gathers, short reductions), which the other lanes fill.
+    Gradient sums are kept per lane and added in lane order at the end of a
+    call, so a result does not depend on how the lanes' work interleaves."""
+
+    def __init__(self, system, device=0, sigma=None, epsilon=None, charges=None, lanes=4):
         self.system = system
         self.n = len(system["charges"])
         self.device = torch.device("cuda", device)
@@ -136,7 +146,26 @@ class FrameEvaluator:
         self.ntypes = len(self.sigma)
         self.cutoff = float(system["cutoff"])
         self.reach = float(system["reach"])
-        term = NonbondedTerm(self.n, device)
+        if int(lanes) < 1:
+            raise ValueError("lanes >= 1")
+        self.lanes = int(lanes)
+        self.term = self._new_term()
+        self.version = 0
+        self._uploaded = -1
+        self._built = False
+        self.builds = 0
+        # lanes 1.. (created at the first call of several frames)
+        self._lane_terms = [self.term]
+        self._lane_streams = [None]
+        self._lane_built = [0]
+        self._lane_uploaded = [-1]
+        self._lane_sums = [None]
+        self._build_id = 0
+        self._build_x = None
+
+    def _new_term(self):
+        system = self.system
+        term = NonbondedTerm(self.n, self.device.index)
         term.set_exclusions(system["excluded_pairs"])
         pme = system.get("pme", True)
         term.set_interaction(self.cutoff, self.reach, system["beta"] if pme else 0.0,
@@ -144,11 +173,7 @@ class FrameEvaluator:
                              lj_switch=system.get("lj_switch", False), switch_distance=system.get("switch", 0.0))
         if pme:
             term.set_pme(system["grid"], system["order"])
-        self.term = term
-        self.version = 0
-        self._uploaded = -1
-        self._built = False
-        self.builds = 0
+        return term
 
     # -- parameters ------------------------------------------------------------
     def set_parameters(self, sigma=None, epsilon=None, charges=None):
@@ -169,9 +194,13 @@ class FrameEvaluator:
 
     def _upload(self):
         if self._uploaded != self.version:
+            if len(self._lane_terms) > 1:
+                # the uploads replace buffers that the lanes' kernels may still read
+                torch.cuda.synchronize(self.device)
             sg, ep = self.tables()
             self.term.set_particles(self.charges, self.types, sg, ep)
             self._uploaded = self.version
+            self._lane_uploaded[0] = self.version
 
     def per_type(self, dq, dtable):
         """{"sigma", "epsilon", "charges"} from the table gradient."""
@@ -218,6 +247,71 @@ class FrameEvaluator:
         self.term.build(x, self.box, self.reach)
         self._built = True
         self.builds += 1
+        self._build_id += 1
+        self._lane_built[0] = self._build_id
+        if self.lanes > 1:
+            self._build_x = x.clone()  # where the other lanes build when they next get a frame
+
+    # -- lanes -----------------------------------------------------------------
+    def _open_lanes(self, frames, sums=False):
+        """The lanes of a call of `frames` frames (with `sums`, the side lanes'
+        gradient sums zeroed); the side lanes' streams wait for the work
+        queued so far on the current stream."""
+        count = max(1, min(self.lanes, frames))
+        while len(self._lane_terms) < count:
+            self._lane_terms.append(self._new_term())
+            self._lane_streams.append(torch.cuda.Stream(device=self.device))
+            self._lane_built.append(0)
+            self._lane_uploaded.append(-1)
+            self._lane_sums.append(None)
+        if sums:
+            for l in range(1, count):
+                self._zero_sums(l)
+        if count > 1:
+            self._fork(range(1, count))
+        return count
+
+    def _fork(self, lanes):
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.device))
+        for l in lanes:
+            self._lane_streams[l].wait_event(ev)
+
+    def _lane(self, i, count):
+        """(term, stream, lane) for frame i of a call over `count` lanes."""
+        l = i % count
+        if l == 0:
+            return self.term, None, 0
+        term, st = self._lane_terms[l], self._lane_streams[l]
+        if self._lane_uploaded[l] != self.version:
+            torch.cuda.synchronize(self.device)
+            sg, ep = self.tables()
+            term.set_particles(self.charges, self.types, sg, ep)
+            self._lane_uploaded[l] = self.version
+        if self._lane_built[l] != self._build_id:
+            self._fork([l])  # the build's positions were made on the current stream
+            term.build(self._build_x, self.box, self.reach, stream=st)
+            self._lane_built[l] = self._build_id
+        return term, st, l
+
+    def _join(self, count):
+        cur = torch.cuda.current_stream(self.device)
+        for l in range(1, count):
+            ev = torch.cuda.Event()
+            ev.record(self._lane_streams[l])
+            cur.wait_event(ev)
+
+    def _zero_sums(self, l):
+        """Lane l's gradient sums (charges (n,), table (2, nt, nt)) set to zero
+        on the current stream."""
+        s = self._lane_sums[l]
+        if s is None:
+            self._lane_sums[l] = (torch.zeros(self.n, dtype=torch.float64, device=self.device),
+                                  torch.zeros((2, self.ntypes, self.ntypes), dtype=torch.float64,
+                                              device=self.device))
+        else:
+            s[0].zero_()
+            s[1].zero_()
 
     def forces(self, positions, energy=False, out=None):
         """Forces (K, n, 3) of every frame (and, with `energy`, the
@@ -225,15 +319,26 @@ class FrameEvaluator:
         X = self.frames(positions)
         F = torch.empty_like(X) if out is None else out
         E = np.zeros(X.shape[0]) if energy else None
-        for k in self.schedule(X):
-            self.term.force(X[k], energy=energy, forces=F[k])
-            if energy:
-                E[k] = self._energy()
+        count = self._open_lanes(X.shape[0])
+        pending = {}  # lane -> the frame whose energies it holds
+        try:
+            for i, k in enumerate(self.schedule(X)):
+                term, st, l = self._lane(i, count)
+                if l in pending:
+                    E[pending.pop(l)] = self._energy(term, st)
+                term.force(X[k], energy=energy, forces=F[k], stream=st)
+                if energy:
+                    pending[l] = k
+            for l, k in pending.items():
+                E[k] = self._energy(self._lane_terms[l], self._lane_streams[l])
+        finally:
+            self._join(count)
         return (F, E) if energy else F
 
-    def _energy(self):
-        e = self.term.energies()
-        c = self.term.constants(dispersion=self.system.get("dispersion", False))
+    def _energy(self, term=None, stream=None):
+        term = self.term if term is None else term
+        e = term.energies(stream=stream)
+        c = term.constants(dispersion=self.system.get("dispersion", False))
         return (e["lj"] + e["coulomb"] + e["excluded"] + e["reciprocal"] + c["self"] + c["background"]
                 + c["dispersion"])
 
@@ -248,8 +353,18 @@ class FrameEvaluator:
             dq = torch.zeros(self.n, dtype=torch.float64, device=self.device)
         if dtable is None:
             dtable = torch.zeros((2, self.ntypes, self.ntypes), dtype=torch.float64, device=self.device)
-        for k in self.schedule(X):
-            self.term.parameter_gradient(X[k], cotangent=G[k], dq=dq, dtable=dtable)
+        count = self._open_lanes(X.shape[0], sums=True)
+        sums = [None] + [self._lane_sums[l] for l in range(1, count)]
+        try:
+            for i, k in enumerate(self.schedule(X)):
+                term, st, l = self._lane(i, count)
+                q, t = (dq, dtable) if l == 0 else sums[l]
+                term.parameter_gradient(X[k], cotangent=G[k], dq=q, dtable=t, stream=st)
+        finally:
+            self._join(count)
+        for l in range(1, count):
+            dq += sums[l][0]
+            dtable += sums[l][1]
         return dq, dtable
 
     def energy_gradient(self, positions):
@@ -261,10 +376,15 @@ class FrameEvaluator:
         disp = None
         if self.system.get("dispersion", False):
             disp = torch.as_tensor(self.dispersion_gradient(), device=self.device)
-        for k in self.schedule(X):
-            self.term.parameter_gradient(X[k], dq=dq[k], dtable=dt[k])
-            if disp is not None:
-                dt[k] += disp
+        count = self._open_lanes(K)
+        try:
+            for i, k in enumerate(self.schedule(X)):
+                term, st, _ = self._lane(i, count)
+                term.parameter_gradient(X[k], dq=dq[k], dtable=dt[k], stream=st)
+        finally:
+            self._join(count)
+        if disp is not None:
+            dt += disp
         return dq, dt
 
     def evaluate(self, positions, cells=None, tilts=None, *, gradients=("tunables",)):

@@ -210,3 +210,28 @@ def test_product_at_the_full_water_box(cuda):
     assert rel_err(got["sigma"][:8], fd["sigma"]) <= GRAD_TOL
     assert rel_err(got["epsilon"][:8], fd["epsilon"]) <= GRAD_TOL
     assert rel_err(got["charges"][atoms], fd["charges"]) <= GRAD_TOL
+
+
+def test_lanes_give_the_results_of_one_lane(cuda):
+    """Frames spread over 4 contexts on their own streams (one moved beyond
+    half the skin, so that the lanes build again in the middle of a call)
+    give the forces, energies and gradients of one context."""
+    s, X, _ = systems.force_matching(frames=7, waters=600, jitter=0.005)
+    X = X.copy()
+    X[4] += np.array([0.08, 0.0, 0.0])
+    Xd = torch.tensor(X, device=cuda)
+    G = torch.tensor(np.random.default_rng(3).normal(size=X.shape), device=cuda)
+    out = []
+    for lanes in (1, 4):
+        ev = FrameEvaluator(s, lanes=lanes)
+        F, E = ev.forces(Xd, energy=True)
+        dq, dt = ev.product(Xd, G)
+        eq, et = ev.energy_gradient(Xd)
+        out.append((F.cpu().numpy(), E, dq.cpu().numpy(), dt.cpu().numpy(), eq.cpu().numpy(), et.cpu().numpy(),
+                    ev.builds))
+    one, four = out
+    # each call: frames 0-3 on the build in force, frame 4 (moved), frame 5 (far from frame 4)
+    assert one[6] == four[6] == 7
+    for a, b in zip(one[:6], four[:6]):
+        scale = np.max(np.abs(a))
+        assert np.max(np.abs(a - b)) <= 1e-6 * scale
