@@ -746,9 +746,11 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
 
 // The same pruning with a block of NB_PRUNE_WARPS warps per group: warp w
 // takes the w-th contiguous share of the outer entries, stages what
-// survives in shared memory, and the block writes the shares in warp order,
-// so the inner list is the one of the warp-per-group kernel, in a quarter of
-// the dependent rounds.  A lane takes four entries a round, their loads and
+// survives in shared memory, and the block writes the shares class by class
+// (entries of more than NB_SPARSE_BITS members first, then by member count,
+// each class in warp order), so the inner list holds the entries of the
+// warp-per-group kernel, in a quarter of the dependent rounds, ordered for
+// the pair kernel's sparse rounds.  A lane takes four entries a round, their loads and
 // their partners' frames all issued before the first test, so a round costs
 // two memory latencies for 128 entries.  Dynamic shared memory: list_cap
 // entries.
@@ -769,7 +771,7 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
                    int64_t units_cap, double *prunes) {
   extern __shared__ int2 s_stage[];
   __shared__ float4 s_m[NB_GROUP];
-  __shared__ int s_cnt[NB_PRUNE_WARPS];
+  __shared__ int s_cls[NB_PRUNE_WARPS][NB_SPARSE_BITS + 1];
   __shared__ int s_unit0, s_nunits;
   __shared__ int2 s_qe[NB_PRUNE_WARPS][64];    // a warp's queue of entries that pass the box test
   __shared__ float4 s_qx[NB_PRUNE_WARPS][64];  // and their partners' images
@@ -880,14 +882,50 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
     }
   }
   if (qn > 0) drain(qn);
-  if (lane == 0) s_cnt[warp] = out;
-  __syncthreads();
-  int at = 0, total = 0;
-  for (int w = 0; w < NB_PRUNE_WARPS; ++w) {
-    if (w < warp) at += s_cnt[w];
-    total += s_cnt[w];
+  // The inner list in classes by member count (class 0: more than
+  // NB_SPARSE_BITS members, class c: c members), class by class, each class
+  // in warp order and within a warp in the order staged.
+  constexpr int NC = NB_SPARSE_BITS + 1;
+  auto entry_class = [](int2 e) {
+    int pc = __popc((unsigned)e.y & 0xffffu);
+    return pc > NB_SPARSE_BITS ? 0 : pc;
+  };
+  int mine[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) mine[c] = 0;
+  for (int i0 = 0; i0 < out; i0 += 32) {
+    int cls = i0 + lane < out ? entry_class(stage[i0 + lane]) : -1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) mine[c] += __popc(__ballot_sync(FULL, cls == c));
   }
-  for (int i = lane; i < out; i += 32) slab_in[g * list_cap + at + i] = stage[i];
+  if (lane == 0) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) s_cls[warp][c] = mine[c];
+  }
+  __syncthreads();
+  int start[NC];
+  int total = 0;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    int before = 0, all = 0;
+    for (int w = 0; w < NB_PRUNE_WARPS; ++w) {
+      int k = s_cls[w][c];
+      if (w < warp) before += k;
+      all += k;
+    }
+    start[c] = total + before;
+    total += all;
+  }
+  for (int i0 = 0; i0 < out; i0 += 32) {
+    int2 en = i0 + lane < out ? stage[i0 + lane] : make_int2(0, 0);
+    int cls = i0 + lane < out ? entry_class(en) : -1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      unsigned b = __ballot_sync(FULL, cls == c);
+      if (cls == c) slab_in[g * list_cap + start[c] + __popc(b & ((1u << lane) - 1))] = en;
+      start[c] += __popc(b);
+    }
+  }
   if (threadIdx.x == 0) {
     counts_in[g] = total;
     if (units) {

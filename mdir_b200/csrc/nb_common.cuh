@@ -13,7 +13,11 @@
 //              of absolute positions (PME) add the half cell back.
 //   lists      one slab of C entries per group: entry = int2(q, bits) with
 //              q the partner place, bits 0-15 the members that pair with it
-//              and bits 16-20 the image code 9(sz+1)+3(sy+1)+(sx+1).
+//              and bits 16-30 the lattice vector of the partner's image, 5
+//              bits a component (NB_IMAGE_BITS below).  A pruned (inner)
+//              list holds its entries in classes: those with more than
+//              NB_SPARSE_BITS members first, then those with 1, 2, ...,
+//              NB_SPARSE_BITS members.
 //   units      (group, ordinal) work items of 64 entries each, in group
 //              order, so that every launch sees them in the same order.
 #pragma once
@@ -23,6 +27,10 @@
 #define NB_GROUP 16
 #define NB_UNIT 64
 #define NB_WARP 32
+// Entries with at most this many members are evaluated member by member
+// (a round of 32 such entries takes as many steps as its largest entry has
+// members) instead of in the 16 rotating steps of a dense round.
+#define NB_SPARSE_BITS 8
 
 // sizes[] slots written by the build (device) and read by the host.
 enum NbSizeSlot {

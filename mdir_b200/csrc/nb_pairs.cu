@@ -19,6 +19,10 @@
 // steps it is home again.  The partner's force stays in its lane and is
 // added once per entry with one float4 atomic (red.global.add.v4.f32), or
 // three 64-bit integer atomics in fixed point in the deterministic mode.
+// A round whose 32 entries all have at most NB_SPARSE_BITS members (the
+// pruned lists put those entries last, by member count) skips the 16 steps:
+// each lane visits its own members only, one a step, and the member forces
+// are summed from shared memory in lane order after the round.
 // Energies and virial go to a per-unit f64 slot, summed later in a fixed
 // order, so they are bitwise reproducible in every mode.
 #include <cmath>
@@ -79,6 +83,34 @@ __device__ __forceinline__ float nb_erfc_from_exp(float pbr, float ex) {
   return poly * ex;
 }
 
+// One pair at r2 with LJ factors cc = (6 c6, 12 c12) and charge product qq
+// (times the Coulomb constant): the force factor fs (the force on the member
+// is fs d, d its displacement from the partner) and, with ENERGY, the LJ and
+// Coulomb energies.  A pair outside (masked, or beyond r_c) computes on its
+// own r^2, finite or not; the caller drops its results.
+template <bool ENERGY, bool SWITCH>
+__device__ __forceinline__ void nb_pair_terms(const PairParams &P, float r2, float2 cc, float qq, float &fs,
+                                              float &ulj, float &uc) {
+  float rinv = nb_rsqrt(r2);
+  float rinv2 = rinv * rinv;
+  float s6 = rinv2 * rinv2 * rinv2;
+  float a12 = cc.y * s6 * s6, a6 = cc.x * s6;  // 12 c12 / r^12, 6 c6 / r^6
+  fs = (a12 - a6) * rinv2;
+  ulj = (ENERGY || SWITCH) ? a12 * (1.f / 12.f) - a6 * (1.f / 6.f) : 0.f;
+  if (SWITCH) {
+    float y = fminf(fmaxf((r2 - P.rs2) * P.winv, 0.f), 1.f);
+    float S = (1.f - y) * (1.f - y) * (1.f + 2.f * y);
+    float dSdr2 = -6.f * y * (1.f - y) * P.winv;
+    fs = fs * S - 2.f * ulj * dSdr2;
+    ulj *= S;
+  }
+  float rr = r2 * rinv;
+  float ex = nb_ex2(r2 * P.nb2_log2e);
+  float erfcv = nb_erfc_from_exp(P.beta_p * rr, ex);
+  fs = fmaf(qq * fmaf(erfcv, rinv, P.two_beta_sqrtpi * ex), rinv2, fs);
+  uc = ENERGY ? qq * (erfcv * rinv - P.coulomb_shift) : 0.f;
+}
+
 __device__ __forceinline__ void nb_red_add_v4(float4 *addr, float x, float y, float z) {
   // one vector reduction instead of three (sm_90 and newer)
   atomicAdd(addr, make_float4(x, y, z, 0.f));
@@ -96,9 +128,9 @@ __device__ __forceinline__ void nb_red_fixed(unsigned long long *addr, float x, 
 // pair in shared memory; 1, the product of per-type factors (sqrt c6,
 // sqrt c12), exact when the table factorizes (one LJ type, or geometric
 // mixing), which needs no dependent lookup.  The members live twice in
-// shared memory (slots u and u + 16), so that lane l reads member
-// (l + k) mod 16 at slot l mod 16 + k: an immediate offset in the unrolled
-// loop, no index arithmetic.
+// shared memory (slots u and u + 16), so that in a dense round lane l reads
+// member (l + k) mod 16 at slot l mod 16 + k: an immediate offset in the
+// unrolled loop, no index arithmetic.
 template <bool ENERGY, bool FIXED, bool SWITCH, int LJM, bool BATCH = false>
 __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *__restrict__ group_L,
                                                 const int32_t *__restrict__ sizes,
@@ -117,6 +149,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   __shared__ float2 s_f[8][2 * NB_GROUP];  // LJM 1: member factors
   __shared__ int s_t[8][2 * NB_GROUP];     // LJM 0: member row offsets in s_lj
   __shared__ float2 s_lj[LJM == 0 ? NB_MAX_TYPES * NB_MAX_TYPES : 1];
+  __shared__ float s_b[8][3][NB_SPARSE_BITS][33];  // member forces of a sparse round (33: no bank conflicts)
   const unsigned FULL = 0xffffffffu;
   if (LJM == 0) {  // (6 c6, 12 c12): the force's factors
     int nt2 = P.ntypes * P.ntypes;
@@ -129,15 +162,27 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int u = lane & 15;
   const int src = (lane & 16) | ((lane + 1) & 15);  // the lane the member accumulators come from
-  const float4 *px = &s_x[warp][u];
-  const float2 *pf = &s_f[warp][u];
-  const int *pt = &s_t[warp][u];
   int nunits = min((int64_t)sizes[NB_SIZE_UNITS], P.units_cap);
   int wstride = gridDim.x * 8;
-  for (int unit = blockIdx.x * 8 + warp; unit < nunits; unit += wstride) {
-    int2 uo = units[unit];
+  // the next unit's header is in flight during this unit (the energy forms,
+  // short of registers, read it when they come to it)
+  int unit = blockIdx.x * 8 + warp;
+  int2 uo_next = !ENERGY && unit < nunits ? units[unit] : make_int2(0, 0);
+  for (; unit < nunits; unit += wstride) {
+    int2 uo = ENERGY ? units[unit] : uo_next;
+    if (!ENERGY && unit + wstride < nunits) uo_next = units[unit + wstride];
     int g = uo.x;
     int64_t pi = (int64_t)g * NB_GROUP + u;
+    // both rounds' entries, in flight with the members' loads (a group's
+    // slab holds a whole number of units, so both reads stay in it; the
+    // lanes past the list's end drop theirs below); the energy forms read
+    // each round's when they come to it
+    const int2 *row = slab + (int64_t)g * P.list_cap + (int64_t)uo.y * NB_UNIT;
+    int2 pre0 = make_int2(0, 0), pre1 = make_int2(0, 0);
+    if (!ENERGY) {
+      pre0 = row[lane];
+      pre1 = row[32 + lane];
+    }
     __syncwarp();
     {
       float4 xi = xq[pi];
@@ -167,7 +212,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
     for (int r = 0; r < 2; ++r) {
       if (r * 32 >= ne) break;
       bool valid = r * 32 + lane < ne;
-      int2 en = valid ? slab[(int64_t)g * P.list_cap + e0 + r * 32 + lane] : make_int2(0, 0);
+      int2 en = valid ? (ENERGY ? row[r * 32 + lane] : (r == 0 ? pre0 : pre1)) : make_int2(0, 0);
       int q = en.x;
       unsigned mask = valid ? ((unsigned)en.y & 0xffffu) : 0u;
       int code = ((unsigned)en.y >> 16) & NB_IMAGE_BITS;
@@ -189,53 +234,32 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
       }
       int tj = typ[q];
       float2 fj = LJM == 1 ? ljf[tj] : make_float2(0.f, 0.f);
-      // bit k of mrot: the pair of this lane's entry with member (lane + k) mod 16
-      unsigned mrot = ((mask >> u) | (mask << (16 - u))) & 0xffffu;
       float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-#pragma unroll
-      for (int k = 0; k < NB_GROUP; ++k) {
-        float4 xm = px[k];
+      // One pair of this lane's entry with the member at slot m: its force
+      // (dropped outside), the partner's share and the energies.
+      auto pair = [&](int m, bool masked_in, float &fx, float &fy, float &fz) {
+        float4 xm = s_x[warp][m];
         float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
         float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        bool inside = (mrot & (1u << k)) && (r2 < P.rc2);
-        // a slot outside (masked, or beyond r_c) computes on its own r^2,
-        // finite or not, and its force and energies are dropped below
-        float r2s = r2;
+        bool inside = masked_in && (r2 < P.rc2);
         float2 cc;  // (6 c6, 12 c12)
         if (LJM == 1) {
-          float2 fm = pf[k];
+          float2 fm = s_f[warp][m];
           cc = make_float2(fm.x * fj.x, fm.y * fj.y);
         } else {
-          cc = s_lj[pt[k] + tj];
-        }
-        float rinv = nb_rsqrt(r2s);
-        float rinv2 = rinv * rinv;
-        float s6 = rinv2 * rinv2 * rinv2;
-        float a12 = cc.y * s6 * s6, a6 = cc.x * s6;  // 12 c12 / r^12, 6 c6 / r^6
-        float fs = (a12 - a6) * rinv2;
-        float ulj = (ENERGY || SWITCH) ? a12 * (1.f / 12.f) - a6 * (1.f / 6.f) : 0.f;
-        if (SWITCH) {
-          float y = fminf(fmaxf((r2s - P.rs2) * P.winv, 0.f), 1.f);
-          float S = (1.f - y) * (1.f - y) * (1.f + 2.f * y);
-          float dSdr2 = -6.f * y * (1.f - y) * P.winv;
-          fs = fs * S - 2.f * ulj * dSdr2;
-          ulj *= S;
+          cc = s_lj[s_t[warp][m] + tj];
         }
         float qq = xm.w * xj.w;
-        float rr = r2s * rinv;
-        float ex = nb_ex2(r2s * P.nb2_log2e);
-        float erfcv = nb_erfc_from_exp(P.beta_p * rr, ex);
-        fs = fmaf(qq * fmaf(erfcv, rinv, P.two_beta_sqrtpi * ex), rinv2, fs);
+        float fs, ulj, uc;
+        nb_pair_terms<ENERGY, SWITCH>(P, r2, cc, qq, fs, ulj, uc);
         fs = inside ? fs : 0.f;
-        float fx = fs * dx, fy = fs * dy, fz = fs * dz;
-        ax += fx;
-        ay += fy;
-        az += fz;
+        fx = fs * dx;
+        fy = fs * dy;
+        fz = fs * dz;
         fjx -= fx;
         fjy -= fy;
         fjz -= fz;
         if (ENERGY) {
-          float uc = qq * (erfcv * rinv - P.coulomb_shift);
           elj += inside ? ulj : 0.f;
           ecl += inside ? uc : 0.f;
           vxx = fmaf(dx, fx, vxx);
@@ -245,9 +269,68 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
           vxz = fmaf(dx, fz, vxz);
           vyz = fmaf(dy, fz, vyz);
         }
-        ax = __shfl_sync(FULL, ax, src);
-        ay = __shfl_sync(FULL, ay, src);
-        az = __shfl_sync(FULL, az, src);
+      };
+      if (__all_sync(FULL, __popc(mask) <= NB_SPARSE_BITS)) {
+        // A sparse round (the pruned lists put such entries last): each lane
+        // visits only its own members, one a step, for as many steps as the
+        // fullest entry of the round has members.  Step i's member force goes
+        // to s_b[.][i][lane]; then lanes u and u + 16 add member u's forces
+        // over the lanes of their half, in lane order.
+        int steps = (int)__reduce_max_sync(FULL, (unsigned)__popc(mask));
+        unsigned mm = mask;
+        // the next member of this lane's entry, or a dropped pair with
+        // member 0 once none is left (a lane with fewer members idles so)
+        auto visit = [&](int i) {
+          bool has = mm != 0u;
+          int m = has ? __ffs(mm) - 1 : 0;
+          mm &= mm - 1;
+          float fx, fy, fz;
+          pair(m, has, fx, fy, fz);
+          if (has) {
+            s_b[warp][0][i][lane] = fx;
+            s_b[warp][1][i][lane] = fy;
+            s_b[warp][2][i][lane] = fz;
+          }
+        };
+        // two members a step, branch-free, so that their chains interleave
+        int i = 0;
+        for (; i + 1 < steps; i += 2) {
+          visit(i);
+          visit(i + 1);
+        }
+        if (i < steps) visit(i);
+        __syncwarp();
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        const unsigned below = (1u << u) - 1u;
+#pragma unroll 4
+        for (int j = 0; j < 16; ++j) {
+          int lp = (lane & 16) | j;
+          unsigned mk = __shfl_sync(FULL, mask, lp);
+          if ((mk >> u) & 1u) {
+            int i = __popc(mk & below);
+            sx += s_b[warp][0][i][lp];
+            sy += s_b[warp][1][i][lp];
+            sz += s_b[warp][2][i][lp];
+          }
+        }
+        __syncwarp();  // the next round writes s_b again
+        ax += sx;
+        ay += sy;
+        az += sz;
+      } else {
+        // bit k of mrot: the pair of this lane's entry with member (lane + k) mod 16
+        unsigned mrot = ((mask >> u) | (mask << (16 - u))) & 0xffffu;
+#pragma unroll
+        for (int k = 0; k < NB_GROUP; ++k) {
+          float fx, fy, fz;
+          pair(u + k, (mrot & (1u << k)) != 0u, fx, fy, fz);
+          ax += fx;
+          ay += fy;
+          az += fz;
+          ax = __shfl_sync(FULL, ax, src);
+          ay = __shfl_sync(FULL, ay, src);
+          az = __shfl_sync(FULL, az, src);
+        }
       }
       if (valid && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
         if (FIXED)
