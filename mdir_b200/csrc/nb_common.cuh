@@ -30,7 +30,7 @@
 // Entries with at most this many members are evaluated member by member
 // (a round of 32 such entries takes as many steps as its largest entry has
 // members) instead of in the 16 rotating steps of a dense round.
-#define NB_SPARSE_BITS 8
+#define NB_SPARSE_BITS 5
 
 // sizes[] slots written by the build (device) and read by the host.
 enum NbSizeSlot {
