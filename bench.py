@@ -607,6 +607,7 @@ def main():
                 # workload, from one ncu capture (profiles/nb_pairs_tip3p23550.md)
                 "traffic": PAIRS_TRAFFIC_BYTES if args.waters == 7850 else None,
                 "pairs_within_cutoff": pairs, "flop_per_pair": flop_per_pair,
+                "pairs_per_s": round(pairs / (times[1] * 1e-3), 0),
                 "launch_ms": round(times[1], 5),
                 "launch_shape": {"sms": props.multi_processor_count, "blocks_per_sm": alone_blocks},
                 "step_shape": {"sms": step_shape[0] or props.multi_processor_count,
