@@ -72,7 +72,7 @@ class Integrator:
         return p.value
 
     def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(1.025, 1.05),
-             pair_sms=(0, 112, 128, 136), pair_blocks=(4, 3), steps=400, reps=3, stream=None):
+             pair_sms=(0, 112, 120, 128, 136), pair_blocks=(4, 3), steps=400, reps=3, stream=None):
         """The autotuner of the step, in two stages: the outer and pruned
         reaches first (the launch shapes as set), then the span of the pair
         grid (SMs; the others are left to the PME kernels beside it) and its
