@@ -131,7 +131,10 @@ class FrameEvaluator:
     most of the GPU idle between its two pair launches (FFTs of a 64^3 grid,
     spreading, gathers, short reductions), which the other lanes fill.
     Gradient sums are kept per lane and added in lane order at the end of a
-    call, so a result does not depend on how the lanes' work interleaves."""
+    call, so a result does not depend on how the lanes' work interleaves.
+    The caller's stream waits for the side lanes before a call returns, so
+    the tensors of a call may be freed or reused on that stream at once
+    (torch's allocator hands a block back only to the stream it was made on)."""
 
     def __init__(self, system, device=0, sigma=None, epsilon=None, charges=None, lanes=4):
         self.system = system
