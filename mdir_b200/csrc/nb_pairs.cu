@@ -272,10 +272,10 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
       };
       if (__all_sync(FULL, __popc(mask) <= NB_SPARSE_BITS)) {
         // A sparse round (the pruned lists put such entries last): each lane
-        // visits only its own members, one a step, for as many steps as the
-        // fullest entry of the round has members.  Step i's member force goes
-        // to s_b[.][i][lane]; then lanes u and u + 16 add member u's forces
-        // over the lanes of their half, in lane order.
+        // visits only its own members, as many as the fullest entry of the
+        // round has.  Its i-th member's force goes to s_b[.][i][lane]; then
+        // lanes u and u + 16 add member u's forces over the lanes of their
+        // half, in lane order.
         int steps = (int)__reduce_max_sync(FULL, (unsigned)__popc(mask));
         unsigned mm = mask;
         // the next member of this lane's entry, or a dropped pair with
