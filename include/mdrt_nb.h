@@ -85,6 +85,12 @@ enum mdrtNbGroupsSlot {
   MDRT_NB_GROUPS_ENTRIES = 2,  /* int32x2 [groups * capacity]: (place, mask | image << 16) */
   MDRT_NB_GROUPS_UNITS = 4,    /* int32x2 [units]: (group, ordinal) */
   MDRT_NB_GROUPS_SHIFTS = 6,   /* int8x4 [places]: whole cells S of each place */
+  /* the pruned (inner) lists of a dual list, valid after a pruning: the
+   * entries of the outer lists with the members within the pruned reach, by
+   * member count (more than NB_SPARSE_BITS = 5 first, then 1, 2, ..., 5), in
+   * the outer order within a count; none without a dual list */
+  MDRT_NB_GROUPS_INNER_ENTRIES = 7, /* int32x2 [groups * capacity] */
+  MDRT_NB_GROUPS_INNER_COUNTS = 9,  /* int32 [groups] */
   MDRT_NB_GROUPS_PLACED = 15,  /* float32x4 [places]: frames (x + (S - 1/2) L, q), centred on the cell */
   MDRT_NB_GROUPS_PLACE_OF = 16 /* int32 [particles]: place of each atom, -1 none */
 };

@@ -19,6 +19,7 @@ SIZE_PLACES, SIZE_LONGEST, SIZE_UNITS, SIZE_EXCL_WIDE, SIZE_NAN, SIZE_OVERFLOW, 
     SIZE_ENTRIES, SIZE_COUNT = range(9)
 SLOT_ORDER, SLOT_COUNTS, SLOT_ENTRIES, SLOT_UNITS, SLOT_SHIFTS, SLOT_PLACED, SLOT_PLACE_OF = \
     0, 1, 2, 4, 6, 15, 16
+SLOT_INNER_ENTRIES, SLOT_INNER_COUNTS = 7, 9
 GRAD_PRODUCT, GRAD_ENERGY = 0, 1
 
 _lib = None

@@ -534,6 +534,8 @@ int32_t mdrtNbGroupsBuffer(mdrtNb *ctx, int32_t slot, void **pointer, int64_t *c
     case MDRT_NB_GROUPS_ENTRIES: p = c.slab; k = c.groups_cap * c.list_cap; break;
     case MDRT_NB_GROUPS_UNITS: p = c.units; k = c.units_cap; break;
     case MDRT_NB_GROUPS_SHIFTS: p = c.shift; k = c.places_cap; break;
+    case MDRT_NB_GROUPS_INNER_ENTRIES: p = c.slab_in; k = c.slab_in ? c.slab_in_entries : 0; break;
+    case MDRT_NB_GROUPS_INNER_COUNTS: p = c.counts_in; k = c.counts_in ? c.groups_cap : 0; break;
     case MDRT_NB_GROUPS_PLACED: p = c.xq; k = c.places_cap; break;
     case MDRT_NB_GROUPS_PLACE_OF: p = c.place_of; k = c.n; break;
     default: return MDRT_NB_INVALID_ARGUMENT;

@@ -677,6 +677,15 @@ __device__ __forceinline__ bool nb_beyond_box(float3 lo, float3 hi, float jx, fl
   return gx * gx + gy * gy + gz * gz > far2;
 }
 
+// The pruning's f32 distance of a member at xm from a partner image at
+// (jx, jy, jz) = frame + lattice shift: each difference, product and sum
+// rounded once in this order (no contraction), so that a host restatement
+// in f32 gets the same bits and the same inner lists.
+__device__ __forceinline__ float nb_prune_r2(float4 xm, float jx, float jy, float jz) {
+  float dx = __fsub_rn(xm.x, jx), dy = __fsub_rn(xm.y, jy), dz = __fsub_rn(xm.z, jz);
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
 // The pruning of the dual list (MDIR: emitGroupsPrune,
 // lib/Conversion/MDExecToGPU/MDExecToGPU.cpp:9588; docs/neighbor-groups.md,
 // Section 6.2): inner mask = outer mask and [r^2 <= R_in'^2] at the current
@@ -723,14 +732,12 @@ __global__ void __launch_bounds__(128) nb_prune(int64_t groups_cap, const int32_
       nb_decode_image(((unsigned)en.y >> 16) & NB_IMAGE_BITS, sx, sy, sz);
       float4 xj = xq[en.x];
       float3 t = nb_lattice_shift(sx, sy, sz, H);
-      float jx = xj.x + t.x, jy = xj.y + t.y, jz = xj.z + t.z;
+      float jx = __fadd_rn(xj.x, t.x), jy = __fadd_rn(xj.y, t.y), jz = __fadd_rn(xj.z, t.z);
       if (nb_beyond_box(box_lo, box_hi, jx, jy, jz, far2)) mm = 0;
       while (mm) {
         int m = __ffs(mm) - 1;
         mm &= mm - 1;
-        float4 xm = s_m[warp][m];
-        float dx = xm.x - jx, dy = xm.y - jy, dz = xm.z - jz;
-        float r2 = dx * dx + dy * dy + dz * dz;
+        float r2 = nb_prune_r2(s_m[warp][m], jx, jy, jz);
         if (r2 <= rin2) inner |= 1u << m;
       }
     }
@@ -825,9 +832,7 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
       unsigned mm = (unsigned)en.y & live;
 #pragma unroll
       for (int m = 0; m < NB_GROUP; ++m) {
-        float4 xm = s_m[m];
-        float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
-        float r2 = dx * dx + dy * dy + dz * dz;
+        float r2 = nb_prune_r2(s_m[m], xj.x, xj.y, xj.z);
         if (((mm >> m) & 1u) && r2 <= rin2) inner |= 1u << m;
       }
     }
@@ -866,9 +871,9 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
         int sx, sy, sz;
         nb_decode_image(((unsigned)en[j].y >> 16) & NB_IMAGE_BITS, sx, sy, sz);
         float3 t = nb_lattice_shift(sx, sy, sz, H);
-        jx = xj[j].x + t.x;
-        jy = xj[j].y + t.y;
-        jz = xj[j].z + t.z;
+        jx = __fadd_rn(xj[j].x, t.x);
+        jy = __fadd_rn(xj[j].y, t.y);
+        jz = __fadd_rn(xj[j].z, t.z);
         pass = !nb_beyond_box(box_lo, box_hi, jx, jy, jz, far2);
       }
       unsigned pb = __ballot_sync(FULL, pass);

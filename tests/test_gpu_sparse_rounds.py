@@ -65,3 +65,93 @@ def test_pruned_lists_give_the_forces_of_one_list(cuda, table, deterministic):
         assert abs(e2[k] - terms[k]) <= 1e-6 * scale, (k, e2[k], terms[k])
     w1, w2 = e1["virial_pair"], e2["virial_pair"]
     assert np.max(np.abs(w1 - w2)) <= 1e-6 * np.max(np.abs(w1))
+
+
+def _inner_reference(t, sizes, rin, cell):
+    """The inner lists the pruning must leave, restated on the host from the
+    outer lists and the frames: an outer entry keeps the members whose f32
+    distance (member frame minus partner frame plus lattice shift, each
+    difference, product and sum rounded once, the shift's products and sums
+    too) is within R_in' = R_in + 3e-6 (ax + by + cz + |bx| + |cx| + |cy|),
+    squared in f64 and rounded to f32; entries left with no member go; the
+    rest come by member count (more than 5 first, then 1, ..., 5), in the
+    outer order within a count."""
+    from mdir_b200 import _lib as L
+    f32 = np.float32
+    ax, by, cz, bx, cx, cy = (list(cell) + [0.0, 0.0, 0.0])[:6]
+    Rw = rin + 3e-6 * (ax + by + cz + abs(bx) + abs(cx) + abs(cy))
+    rin2 = f32(Rw * Rw)
+    G = int(sizes[L.SIZE_GROUPS])
+    cap = t.info()["list_capacity"]
+    counts = t.buffer(L.SLOT_COUNTS, np.int32)[:G]
+    E = t.buffer(L.SLOT_ENTRIES, np.int32, 2)[: G * cap].reshape(G, cap, 2)
+    xq = t.buffer(L.SLOT_PLACED, np.float32, 4)
+    order = t.buffer(L.SLOT_ORDER, np.int32)
+    lists = []
+    for g in range(G):
+        ent = E[g, : counts[g]]
+        q = ent[:, 0]
+        bits = ent[:, 1].astype(np.int64) & 0xFFFFFFFF
+        live = int(sum(1 << m for m in range(16) if order[16 * g + m] >= 0))
+        mask = bits & 0xFFFF & live
+        code = (bits >> 16) & 0x7FFF
+        na, nb, nc = (f32(v) for v in ((code & 31) - 16, ((code >> 5) & 31) - 16, ((code >> 10) & 31) - 16))
+        tx = (na * f32(ax) + nb * f32(bx)) + nc * f32(cx)
+        ty = nb * f32(by) + nc * f32(cy)
+        tz = nc * f32(cz)
+        jx, jy, jz = xq[q, 0] + tx, xq[q, 1] + ty, xq[q, 2] + tz
+        inner = np.zeros(len(q), dtype=np.int64)
+        for m in range(16):
+            xm = xq[16 * g + m]
+            dx, dy, dz = xm[0] - jx, xm[1] - jy, xm[2] - jz
+            r2 = (dx * dx + dy * dy) + dz * dz
+            inner |= (((mask >> m) & 1) & (r2 <= rin2)).astype(np.int64) << m
+        keep = inner != 0
+        kept = np.stack([q[keep], (inner[keep] | (bits[keep] & 0x7FFF0000)).astype(np.int64)], 1)
+        pc = np.array([bin(int(v)).count("1") for v in inner[keep]], dtype=np.int64)
+        cls = np.where(pc > 5, 0, pc)
+        lists.append(np.concatenate([kept[cls == c] for c in range(6)]) if len(kept) else kept)
+    return lists
+
+
+@pytest.mark.parametrize("case", ["water", "triclinic"])
+def test_pruned_lists_are_the_host_restatement(cuda, case):
+    """Bit for bit: the inner lists after a pruning equal the host
+    restatement of the pruning's f32 test, in its order, at the build's
+    positions and again after the atoms moved."""
+    from mdir_b200 import _lib as L
+    if case == "water":
+        s = systems.tip3p(waters=1500, seed=11)
+        cell = list(s["box"])
+    else:
+        from tests.test_gpu_triclinic import CELLS, charged_lattice
+        cell = list(CELLS[0])
+        s = charged_lattice(cell)
+    n = len(s["charges"])
+    t = NonbondedTerm(n)
+    t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t.set_exclusions(pairs=s["excluded_pairs"])
+    rin = 1.0
+    t.set_interaction(0.9, 1.25 if case == "water" else 1.1, 0.0)
+    t.set_pruned_reach(rin)
+    x = np.asarray(s["positions"], dtype=np.float64)
+    rng = np.random.default_rng(4)
+    for step in range(2):
+        xd = torch.tensor(x, device=cuda)
+        if step == 0:
+            sizes = t.build(xd, cell)
+        t.prune(xd, cell[:3])
+        torch.cuda.synchronize()
+        ref = _inner_reference(t, sizes, rin, cell)
+        cap = t.info()["list_capacity"]
+        G = len(ref)
+        got_c = t.buffer(L.SLOT_INNER_COUNTS, np.int32)[:G]
+        got_e = t.buffer(L.SLOT_INNER_ENTRIES, np.int32, 2)[: G * cap].reshape(G, cap, 2)
+        assert sum(len(r) for r in ref) > 0
+        for g in range(G):
+            assert got_c[g] == len(ref[g]), (step, g)
+            got = got_e[g, : got_c[g]].astype(np.int64)
+            got[:, 1] &= 0xFFFFFFFF
+            np.testing.assert_array_equal(got, ref[g])
+        x = x + rng.normal(0.0, 0.01, size=x.shape)  # within half the skin of the build
+    t.close()
