@@ -88,7 +88,9 @@ enum mdrtNbGroupsSlot {
   /* the pruned (inner) lists of a dual list, valid after a pruning: the
    * entries of the outer lists with the members within the pruned reach, by
    * member count (more than NB_SPARSE_BITS = 5 first, then 1, 2, ..., 5), in
-   * the outer order within a count; none without a dual list */
+   * the outer order within a count (lists of more than 25,600 entries, past
+   * the pruning's shared-memory staging, keep the outer order); none
+   * without a dual list */
   MDRT_NB_GROUPS_INNER_ENTRIES = 7, /* int32x2 [groups * capacity] */
   MDRT_NB_GROUPS_INNER_COUNTS = 9,  /* int32 [groups] */
   MDRT_NB_GROUPS_PLACED = 15,  /* float32x4 [places]: frames (x + (S - 1/2) L, q), centred on the cell */

@@ -17,7 +17,9 @@
 //              bits a component (NB_IMAGE_BITS below).  A pruned (inner)
 //              list holds its entries in classes: those with more than
 //              NB_SPARSE_BITS members first, then those with 1, 2, ...,
-//              NB_SPARSE_BITS members.
+//              NB_SPARSE_BITS members (a list too long for the pruning's
+//              shared-memory staging keeps the outer order; the pair kernel
+//              is right in either order).
 //   units      (group, ordinal) work items of 64 entries each, in group
 //              order, so that every launch sees them in the same order.
 #pragma once
