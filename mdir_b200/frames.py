@@ -130,6 +130,8 @@ class FrameEvaluator:
     that build) and scratch.  The kernels of one 23,550-atom frame leave
     most of the GPU idle between its two pair launches (FFTs of a 64^3 grid,
     spreading, gathers, short reductions), which the other lanes fill.
+    Each lane holds the device memory of one context (lists, frames, PME
+    grids); `lanes=1` keeps one.
     Gradient sums are kept per lane and added in lane order at the end of a
     call, so a result does not depend on how the lanes' work interleaves.
     The caller's stream waits for the side lanes before a call returns, so
