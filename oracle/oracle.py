@@ -11,7 +11,10 @@ parts that MDIR computes on the host or through an FFT:
 - beta by bisection of erfc(beta rc) = tol and the smooth grid size
   (lib/Driver/TermNonbonded.cpp:755-795 and 1104-1130);
 - the self, background and dispersion-correction constants
-  (TermNonbonded.cpp:601-637 and 651-668).
+  (TermNonbonded.cpp:601-637 and 651-668);
+- the pruning of a dual list (lib/Conversion/MDExecToGPU/
+  MDExecToGPU.cpp:9588, docs/neighbor-groups.md Section 6.2), restated in
+  f32 on the lists and frames the device holds (`prune_lists`).
 
 Units: nm, ps, kJ/mol, e.  COULOMB is MDIR's COULOMB_NATIVE
 (scripts/mdir_physical_constants.py:16)."""
@@ -176,6 +179,53 @@ def pairset_triclinic(x, cell, reach, excl=None, want_list=True, span=2):
     lib().orc_pairset_triclinic(n, _ptr(x), _ptr(cell), reach, _ptr(off), _ptr(ex), span, count, _ptr(out),
                                 ctypes.byref(several))
     return count, out[:count], several.value
+
+
+def prune_lists(entries, counts, frames, order, cell, pruned, sparse_bits=5):
+    """The inner lists that a pruning leaves (MDIR: the inner mask = the
+    outer mask and [r^2 <= R_in'^2] at the current frames, entries left with
+    no member dropped; MDExecToGPU.cpp:9588), restated in f32 on the device's
+    data: `entries` (G, C, 2) int32 outer entries (partner place, member bits
+    | lattice-vector code << 16), `counts` (G,), `frames` (P, 4) f32 places,
+    `order` (P,) atoms of the places (-1 empty), the cell (ax, by, cz[, bx, cx,
+    cy]) and the pruned reach.  R_in' = R_in + 3e-6 (ax + by + cz + |bx| +
+    |cx| + |cy|), squared in f64 and rounded to f32; the partner's image is
+    its frame plus the lattice shift (na ax + nb bx) + nc cx, nb by + nc cy,
+    nc cz; the distance is (m - j)^2 summed x, y then z; each of these f32
+    operations rounded once.  Each list comes by member count, entries of
+    more than `sparse_bits` members first, then 1, 2, ..., in the outer
+    order within a count.  Returns a list of (n_g, 2) int64 arrays."""
+    f32 = np.float32
+    ax, by, cz, bx, cx, cy = (list(cell) + [0.0, 0.0, 0.0])[:6]
+    Rw = pruned + 3e-6 * (ax + by + cz + abs(bx) + abs(cx) + abs(cy))
+    rin2 = f32(Rw * Rw)
+    frames = np.asarray(frames, dtype=np.float32)
+    lists = []
+    for g in range(len(counts)):
+        ent = np.asarray(entries[g, : counts[g]])
+        q = ent[:, 0].astype(np.int64)
+        bits = ent[:, 1].astype(np.int64) & 0xFFFFFFFF
+        live = int(sum(1 << m for m in range(16) if order[16 * g + m] >= 0))
+        mask = bits & 0xFFFF & live
+        code = (bits >> 16) & 0x7FFF
+        na, nb, nc = (f32(v) for v in ((code & 31) - 16, ((code >> 5) & 31) - 16, ((code >> 10) & 31) - 16))
+        tx = (na * f32(ax) + nb * f32(bx)) + nc * f32(cx)
+        ty = nb * f32(by) + nc * f32(cy)
+        tz = nc * f32(cz)
+        jx, jy, jz = frames[q, 0] + tx, frames[q, 1] + ty, frames[q, 2] + tz
+        inner = np.zeros(len(q), dtype=np.int64)
+        for m in range(16):
+            xm = frames[16 * g + m]
+            dx, dy, dz = xm[0] - jx, xm[1] - jy, xm[2] - jz
+            r2 = (dx * dx + dy * dy) + dz * dz
+            inner |= (((mask >> m) & 1) & (r2 <= rin2)).astype(np.int64) << m
+        keep = inner != 0
+        kept = np.stack([q[keep], inner[keep] | (bits[keep] & 0x7FFF0000)], 1)
+        pc = np.array([bin(int(v)).count("1") for v in inner[keep]], dtype=np.int64)
+        cls = np.where(pc > sparse_bits, 0, pc)
+        lists.append(np.concatenate([kept[cls == c] for c in range(sparse_bits + 1)])
+                     if len(kept) else kept.reshape(0, 2))
+    return lists
 
 
 def chain_exclusions(n, degree):

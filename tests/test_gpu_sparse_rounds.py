@@ -67,58 +67,11 @@ def test_pruned_lists_give_the_forces_of_one_list(cuda, table, deterministic):
     assert np.max(np.abs(w1 - w2)) <= 1e-6 * np.max(np.abs(w1))
 
 
-def _inner_reference(t, sizes, rin, cell):
-    """The inner lists the pruning must leave, restated on the host from the
-    outer lists and the frames: an outer entry keeps the members whose f32
-    distance (member frame minus partner frame plus lattice shift, each
-    difference, product and sum rounded once, the shift's products and sums
-    too) is within R_in' = R_in + 3e-6 (ax + by + cz + |bx| + |cx| + |cy|),
-    squared in f64 and rounded to f32; entries left with no member go; the
-    rest come by member count (more than 5 first, then 1, ..., 5), in the
-    outer order within a count."""
-    from mdir_b200 import _lib as L
-    f32 = np.float32
-    ax, by, cz, bx, cx, cy = (list(cell) + [0.0, 0.0, 0.0])[:6]
-    Rw = rin + 3e-6 * (ax + by + cz + abs(bx) + abs(cx) + abs(cy))
-    rin2 = f32(Rw * Rw)
-    G = int(sizes[L.SIZE_GROUPS])
-    cap = t.info()["list_capacity"]
-    counts = t.buffer(L.SLOT_COUNTS, np.int32)[:G]
-    E = t.buffer(L.SLOT_ENTRIES, np.int32, 2)[: G * cap].reshape(G, cap, 2)
-    xq = t.buffer(L.SLOT_PLACED, np.float32, 4)
-    order = t.buffer(L.SLOT_ORDER, np.int32)
-    lists = []
-    for g in range(G):
-        ent = E[g, : counts[g]]
-        q = ent[:, 0]
-        bits = ent[:, 1].astype(np.int64) & 0xFFFFFFFF
-        live = int(sum(1 << m for m in range(16) if order[16 * g + m] >= 0))
-        mask = bits & 0xFFFF & live
-        code = (bits >> 16) & 0x7FFF
-        na, nb, nc = (f32(v) for v in ((code & 31) - 16, ((code >> 5) & 31) - 16, ((code >> 10) & 31) - 16))
-        tx = (na * f32(ax) + nb * f32(bx)) + nc * f32(cx)
-        ty = nb * f32(by) + nc * f32(cy)
-        tz = nc * f32(cz)
-        jx, jy, jz = xq[q, 0] + tx, xq[q, 1] + ty, xq[q, 2] + tz
-        inner = np.zeros(len(q), dtype=np.int64)
-        for m in range(16):
-            xm = xq[16 * g + m]
-            dx, dy, dz = xm[0] - jx, xm[1] - jy, xm[2] - jz
-            r2 = (dx * dx + dy * dy) + dz * dz
-            inner |= (((mask >> m) & 1) & (r2 <= rin2)).astype(np.int64) << m
-        keep = inner != 0
-        kept = np.stack([q[keep], (inner[keep] | (bits[keep] & 0x7FFF0000)).astype(np.int64)], 1)
-        pc = np.array([bin(int(v)).count("1") for v in inner[keep]], dtype=np.int64)
-        cls = np.where(pc > 5, 0, pc)
-        lists.append(np.concatenate([kept[cls == c] for c in range(6)]) if len(kept) else kept)
-    return lists
-
-
 @pytest.mark.parametrize("case", ["water", "triclinic"])
 def test_pruned_lists_are_the_host_restatement(cuda, case):
-    """Bit for bit: the inner lists after a pruning equal the host
-    restatement of the pruning's f32 test, in its order, at the build's
-    positions and again after the atoms moved."""
+    """Bit for bit: the inner lists after a pruning equal the oracle's
+    restatement of the pruning's f32 test (oracle.prune_lists), in its
+    order, at the build's positions and again after the atoms moved."""
     from mdir_b200 import _lib as L
     if case == "water":
         s = systems.tip3p(waters=1500, seed=11)
@@ -142,9 +95,11 @@ def test_pruned_lists_are_the_host_restatement(cuda, case):
             sizes = t.build(xd, cell)
         t.prune(xd, cell[:3])
         torch.cuda.synchronize()
-        ref = _inner_reference(t, sizes, rin, cell)
         cap = t.info()["list_capacity"]
-        G = len(ref)
+        G = int(sizes[L.SIZE_GROUPS])
+        ref = O.prune_lists(t.buffer(L.SLOT_ENTRIES, np.int32, 2)[: G * cap].reshape(G, cap, 2),
+                            t.buffer(L.SLOT_COUNTS, np.int32)[:G], t.buffer(L.SLOT_PLACED, np.float32, 4),
+                            t.buffer(L.SLOT_ORDER, np.int32), cell, rin)
         got_c = t.buffer(L.SLOT_INNER_COUNTS, np.int32)[:G]
         got_e = t.buffer(L.SLOT_INNER_ENTRIES, np.int32, 2)[: G * cap].reshape(G, cap, 2)
         assert sum(len(r) for r in ref) > 0

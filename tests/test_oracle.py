@@ -188,3 +188,48 @@ def test_triclinic_pme_is_the_ewald_sum_and_its_gradient():
     e1, f1, W1, p1 = O.pme_triclinic(x, q, box + (0.0, 0.0, 0.0), K, order, beta)
     assert abs(e0 - e1) < 1e-12 * abs(e0)
     np.testing.assert_allclose(f1, f0, rtol=1e-10, atol=1e-10)
+
+
+def test_prune_lists_restatement():
+    """oracle.prune_lists against a scalar restatement entry by entry, with
+    empty places, images, entries that lose every member, and all classes."""
+    rng = np.random.default_rng(8)
+    G, C = 3, 40
+    f32 = np.float32
+    cell = (2.9, 3.1, 3.3, 0.4, -0.6, 0.5)
+    frames = rng.uniform(-0.7, 0.7, size=(16 * G, 4)).astype(np.float32)
+    order = np.arange(16 * G, dtype=np.int32)
+    order[[5, 21, 40]] = -1  # empty places
+    entries = np.zeros((G, C, 2), dtype=np.int32)
+    counts = np.array([40, 17, 0], dtype=np.int32)
+    for g in range(G):
+        for e in range(counts[g]):
+            n = rng.choice([-1, 0, 1], size=3, p=[0.1, 0.8, 0.1]) + 16
+            code = int(n[0]) | (int(n[1]) << 5) | (int(n[2]) << 10)
+            mask = int(rng.integers(1, 1 << 16))
+            entries[g, e] = (rng.integers(0, 16 * G), mask | (int(code) << 16))
+    rin = 1.0
+    got = O.prune_lists(entries, counts, frames, order, cell, rin)
+    ax, by, cz, bx, cx, cy = cell
+    Rw = rin + 3e-6 * (ax + by + cz + abs(bx) + abs(cx) + abs(cy))
+    rin2 = f32(Rw * Rw)
+    for g in range(G):
+        rows = []
+        for e in range(counts[g]):
+            q, bits = int(entries[g, e, 0]), int(entries[g, e, 1]) & 0xFFFFFFFF
+            code = (bits >> 16) & 0x7FFF
+            na, nb, nc = (f32((code >> s) & 31) - f32(16) for s in (0, 5, 10))
+            t = ((na * f32(ax) + nb * f32(bx)) + nc * f32(cx), nb * f32(by) + nc * f32(cy), nc * f32(cz))
+            j = [frames[q, k] + t[k] for k in range(3)]
+            inner = 0
+            for m in range(16):
+                if not (bits >> m) & 1 or order[16 * g + m] < 0:
+                    continue
+                d = [frames[16 * g + m, k] - j[k] for k in range(3)]
+                if (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2] <= rin2:
+                    inner |= 1 << m
+            if inner:
+                rows.append((bin(inner).count("1"), q, inner | (bits & 0x7FFF0000)))
+        want = [(q, b) for c in range(6) for (pc, q, b) in rows if (0 if pc > 5 else pc) == c]
+        assert [tuple(map(int, r)) for r in got[g]] == want
+    assert sum(len(r) for r in got) > 0 and any(len(r) < counts[g] for g, r in enumerate(got))
