@@ -216,7 +216,11 @@ int64_t orc_pairset(int64_t n, const double *x, const double *box, double reach,
  *
  * energies[0] = LJ, energies[1] = Coulomb direct.  virial[9] = sum d (x) F
  * with d = x_i - x_j (image) and F the force on i.  forces[3n] += forces.
- * lj_switch: 0 = none, 1 = r^2 cubic switch from rs.
+ * lj_switch: 0 = none, 1 = r^2 cubic switch from rs (MDIR's
+ * SQUARED_DISTANCE_SWITCH modifier), 2 = the potential switch of MDIR's md
+ * dialect, S = 1 - 10 t^3 + 15 t^4 - 6 t^5, t = (r - rs)/(rc - rs), S = 1
+ * for r <= rs (lib/Dialect/MD/Transforms/ExpandTruncation.cpp:19-46; the
+ * expression pairs of examples/argon/argon.toml).
  * ---------------------------------------------------------------------- */
 void orc_nonbonded(int64_t n, const double *x, const double *q,
                    const int32_t *type, int32_t ntypes, const double *sigma,
@@ -277,7 +281,15 @@ void orc_nonbonded(int64_t n, const double *x, const double *q,
                     double sr = sg / r, s6 = pow(sr, 6.0), s12 = s6 * s6;
                     double e = 4.0 * ep * (s12 - s6);
                     double dedr = 4.0 * ep * (-12.0 * s12 + 6.0 * s6) / r;
-                    if (lj_switch) {
+                    if (lj_switch == 2) {
+                      if (r > rs) {
+                        double t = (r - rs) / (rc - rs);
+                        double S = 1.0 + t * t * t * (-10.0 + t * (15.0 - 6.0 * t));
+                        double dSdr = t * t * (-30.0 + t * (60.0 - 30.0 * t)) / (rc - rs);
+                        dedr = dedr * S + e * dSdr;
+                        e *= S;
+                      }
+                    } else if (lj_switch) {
                       double y = (r2 - rs2) * winv;
                       if (y < 0.0) y = 0.0;
                       if (y > 1.0) y = 1.0;

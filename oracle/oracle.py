@@ -498,7 +498,11 @@ def dispersion_energy(types, sigma, epsilon, excluded_pairs, box, rc):
 
 def nonbonded(x, q, types, sigma, epsilon, box, rc, beta, excl=None, coulomb=COULOMB,
               coulomb_shift=False, lj_switch=False, rs=0.0):
-    """f64 LJ + Ewald direct: (energies {'lj', 'coulomb'}, forces, virial)."""
+    """f64 LJ + Ewald direct: (energies {'lj', 'coulomb'}, forces, virial).
+    lj_switch: False / 0 none, True / 1 the cubic switch in r^2 (MDIR's
+    SQUARED_DISTANCE_SWITCH modifier, TermLennardJones.cpp:72-95), 2 the
+    potential switch of MDIR's md dialect, quintic in r (ExpandTruncation.cpp:
+    19-46), both from rs to rc."""
     x = _c(x, np.float64)
     q = _c(q, np.float64)
     t = _c(types, np.int32)

@@ -233,3 +233,35 @@ def test_prune_lists_restatement():
         want = [(q, b) for c in range(6) for (pc, q, b) in rows if (0 if pc > 5 else pc) == c]
         assert [tuple(map(int, r)) for r in got[g]] == want
     assert sum(len(r) for r in got) > 0 and any(len(r) < counts[g] for g, r in enumerate(got))
+
+
+def test_argon_lattice_potential_is_mdir_argon_test():
+    """examples/argon (864 atoms, LJ switched from 7.5 to 8.5 Å by the md
+    dialect's quintic potential switch): step-0 potential -1304.88...
+    kcal/mol (test/Driver/argon.test:9-14; -5459.64 kJ/mol in
+    examples/argon/argon.mlir); fixture from tests/golden/make_argon_lattice.py.
+    The forces are the energy's central differences."""
+    import json
+    d = json.load(open(Path(__file__).resolve().parent / "golden" / "argon_lattice.json"))
+    x = np.array(d["positions_nm"])
+    n = len(x)
+    s = {"charges": np.zeros(n), "types": np.zeros(n, dtype=np.int32), "sigma": np.array([[d["sigma_nm"]]]),
+         "epsilon": np.array([[d["epsilon_kj_mol"]]]), "box": np.array(d["box_nm"]), "cutoff": d["cutoff_nm"],
+         "reach": d["cutoff_nm"] + 0.1, "pme": False, "beta": 0.0, "grid": None, "order": 4,
+         "excluded_pairs": np.zeros((0, 2), dtype=np.int64), "lj_switch": 2, "switch": d["switch_nm"]}
+    r = O.evaluate(s, x)
+    kcal = r["terms"]["lj"] / O.KJ_PER_KCAL
+    assert f"{kcal:.6f}".startswith(d["potential_kcal_mol_prefix"]), kcal
+    assert f"{r['terms']['lj']:.4f}".startswith(f"{d['potential_kj_mol_argon_mlir']:.2f}")
+    # central differences on atoms moved into the switching region
+    rng = np.random.default_rng(2)
+    xj = x + rng.uniform(-0.03, 0.03, size=x.shape)
+    f = O.evaluate(s, xj)["forces"]
+    h = 1e-6
+    for a in (0, 100, 500):
+        for k in range(3):
+            up, dn = xj.copy(), xj.copy()
+            up[a, k] += h
+            dn[a, k] -= h
+            fd = -(O.evaluate(s, up)["terms"]["lj"] - O.evaluate(s, dn)["terms"]["lj"]) / (2 * h)
+            assert abs(fd - f[a, k]) <= 1e-5 * max(1.0, abs(f[a, k])), (a, k, fd, f[a, k])
