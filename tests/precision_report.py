@@ -116,8 +116,11 @@ def main():
     s = systems.argon()
     print(json.dumps({"workload": "argon-864", "force_rms_rel": force_error(s),
                       "nve": nve(s, 0.002, 0, 2000 if not q else 400, 101, 5, temperature=120.0)}), flush=True)
-    # MDIR's argon.test settings: LJ switched from 0.75 to 0.85 nm, 2000 x 5 fs
-    # (its bound: a relative drift of at most 1e-5)
+    # the distances and steps of MDIR's argon.test: LJ switched from 0.75 to
+    # 0.85 nm, 2000 x 5 fs (its bound: a relative drift of at most 1e-5);
+    # the switch is the device's, the cubic in r^2 (MDIR's squared-distance
+    # switch), where argon.test's expression pair takes the md dialect's
+    # quintic potential switch in r
     s = dict(systems.argon(cutoff=0.85, skin=0.1))
     s.update({"lj_switch": True, "switch": 0.75})
     print(json.dumps({"workload": "argon-864-switched", "force_rms_rel": force_error(s),
