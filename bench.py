@@ -9,11 +9,12 @@ path (neighbor build when the test of validity asks, pair kernel, excluded
 correction, PME with cuFFT, leap-frog + SETTLE + thermostat) as a CUDA
 graph.  One bench step = `--md-steps` MD steps (one replay of the step
 graph); the L2 is flushed between bench steps (a 256 MiB write).  Metric:
-ns/day, the aggregate of N independent replicas (one per GPU: the single
-box does not shard).
+ns/day; with N GPUs, N independent replicas (the single box does not
+shard): `value` is their aggregate and `per_replica_ns_day` each box's.
 
 The reference arm (--impl reference) times the OpenMP CPU port of MDIR's
-host algorithm for the same workload on the host cores."""
+host algorithm for the same workload on the host cores, with MDIR's CPU
+neighbor matrix at a reach of r_c + 0.15 nm."""
 
 import argparse
 import json
@@ -31,7 +32,12 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 DT_PS = 0.002
-PAIRS_TRAFFIC_BYTES = 6.19e6  # ncu dram__bytes_read.sum + dram__bytes_write.sum of nb_pairs, 23,550 atoms
+# DRAM bytes read + written by one nb_pairs launch on the 23,550-atom box at
+# the tuned reaches (ncu dram__bytes_read.sum + dram__bytes_write.sum; the
+# counters need a profiler replay, so the figure is from a capture, not this run)
+PAIRS_TRAFFIC_BYTES = 6.93e6
+# MDIR's CPU neighbor matrix: the cutoff plus a 0.15 nm skin
+CPU_SKIN_NM = 0.15
 METRIC = "ns/day water box (TIP3P 23,550 atoms, PME, SETTLE, NVT, 2 fs)"
 
 
@@ -73,9 +79,10 @@ def workload(args):
 
 
 def config(args, s):
+    """The workload (the same for both arms); each arm's own list reaches
+    are tuning and go in its `tuning` key."""
     return {"workload": f"tip3p-{len(s['charges'])}", "atoms": len(s["charges"]),
-            "box_nm": round(float(s["box"][0]), 4), "cutoff_nm": s["cutoff"], "reach_nm": s["reach"],
-            "pruned_reach_nm": s["pruned"],
+            "box_nm": round(float(s["box"][0]), 4), "cutoff_nm": s["cutoff"],
             "pme_grid": list(s["grid"]), "pme_order": s["order"], "dt_ps": DT_PS,
             "md_steps_per_step": args.md_steps, "graph_steps": args.unroll, "ensemble": "NVT Bussi 300 K",
             "l2": "flushed between timed steps (256 MiB write); each step replays md_steps MD steps",
@@ -154,14 +161,30 @@ def ns_per_day(md_steps, seconds):
     return md_steps / seconds * DT_PS * 86400.0 / 1000.0
 
 
+def cpu_system(s):
+    """The workload as the CPU port runs it: one neighbor matrix at MDIR's
+    CPU reach r_c + 0.15 nm (no dual list)."""
+    c = dict(s)
+    c["reach"] = s["cutoff"] + CPU_SKIN_NM
+    return c
+
+
+def cpu_description():
+    from oracle.cpu_port import reference_fft
+    fft = ("MDIR's runtime/mdrt_fft.c + pocketfft built from the reference's sources" if reference_fft()
+           else "numpy's pocketfft (MDIR's mdrt_fft.c not built)")
+    return (f"f32 neighbor matrix at r_c + {CPU_SKIN_NM} nm (cells of half the reach), f32 row loop with MDIR's "
+            f"D90 erfc, f64 excluded pairs, i64 PME spreading, {fft}; one matrix rebuild every 10 steps")
+
+
 def cpu_baseline(s, x, steps=3):
     from oracle.cpu_port import time_md_steps
-    sec, threads, tb, tf = time_md_steps(s, x, steps)
+    c = cpu_system(s)
+    sec, threads, tb, tf = time_md_steps(c, x, steps)
     return {"value": round(ns_per_day(1, sec), 4), "unit": "ns/day", "cores": threads, "kind": "port",
-            "sample": f"{steps} force evaluations of the {len(s['charges'])}-atom box after a warm-up "
-                      f"(f32 neighbor matrix, f32 row loop, i64 PME spreading, pocketfft via numpy), one "
-                      f"matrix rebuild every 10 steps amortised: {tf * 1e3:.1f} ms/eval, "
-                      f"{tb * 1e3:.1f} ms/build"}
+            "sample": f"{steps} force evaluations of the {len(s['charges'])}-atom box after a warm-up, "
+                      f"{cpu_description()} amortised: {tf * 1e3:.1f} ms/eval, {tb * 1e3:.1f} ms/build",
+            "tuning": {"reach_nm": c["reach"], "pruned_reach_nm": 0.0}}
 
 
 def adjoint_leg(args, dev, flush, world=1, frames=64, reps=5, warmup=3):
@@ -405,7 +428,8 @@ def run_reference(args):
         return
     s, v = workload(args)
     from oracle.cpu_port import CpuPort
-    cp = CpuPort(s)
+    c = cpu_system(s)
+    cp = CpuPort(c)
     x = s["positions"].copy()
     cp.build(x)
     for _ in range(max(args.warmup, 1)):
@@ -423,10 +447,10 @@ def run_reference(args):
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 pairs / f64 PME", "data": "synthetic",
-           "config": config(args, s),
+           "config": config(args, s), "tuning": {"reach_nm": c["reach"], "pruned_reach_nm": 0.0},
            "cpu_baseline": {"value": round(value, 4), "unit": "ns/day", "cores": cp.threads, "kind": "port",
-                            "sample": f"{args.steps} MD-step force evaluations (rebuild every 10) of the "
-                                      f"{len(s['charges'])}-atom box; MDIR's CPU path is MLIR-generated and "
+                            "sample": f"{args.steps} MD-step force evaluations of the {len(s['charges'])}-atom "
+                                      f"box, {cpu_description()}; MDIR's CPU path is MLIR-generated and "
                                       "cannot be built here, so this is the OpenMP port of its algorithm"},
            "e2e": {"value": round(value, 4), "unit": "ns/day", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
@@ -603,8 +627,6 @@ def main():
     achieved = pairs * flop_per_pair / (times[1] * 1e-3) / 1e12
     roofline = {"bound": "fp32", "kernel": "nb_pairs", "achieved": round(achieved, 3),
                 "peak": round(peak_fp32, 2), "unit": "TFLOP/s", "frac": round(achieved / peak_fp32, 4),
-                # DRAM bytes read + written per launch of nb_pairs on this
-                # workload, from one ncu capture (profiles/nb_pairs_tip3p23550.md)
                 "traffic": PAIRS_TRAFFIC_BYTES if args.waters == 7850 else None,
                 "pairs_within_cutoff": pairs, "flop_per_pair": flop_per_pair,
                 "pairs_per_s": round(pairs / (times[1] * 1e-3), 0),
@@ -634,6 +656,8 @@ def main():
             "gpu_launches": int(args.steps * args.md_steps * 5 + args.steps * args.md_steps // max(1, args.unroll)
                                 + builds * 20),
             "tuned": tuned,
+            "tuning": {"reach_nm": s["reach"], "pruned_reach_nm": s["pruned"]},
+            "per_replica_ns_day": round(value / world, 2),
             "builds": int(builds), "prunes": int(prunes), "regrows": int(regrows), "regrows_total": th1["regrows"],
             "stale_stops": int(stops),
             "temperature_K": round(temp, 1), "status": status}

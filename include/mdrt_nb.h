@@ -355,16 +355,18 @@ int32_t mdrtMdForces(mdrtMd *md, double **forces);
  * (device f64 [n, 3]) and writes the energy and the virial (xx yy zz xy xz
  * yz) to energy_virial (device f64 [7]); asynchronous on `stream`.
  *
- * For callers that cannot allocate device memory: code recording a CUDA
- * graph by stream capture (cudaMalloc cannot be captured), hosts that own all
- * device memory through a fixed pool, and loops that must not pay the device
+ * For callers that cannot allocate device memory: host programs (and
+ * plugins inside them) that own all device memory through a fixed pool and
+ * forbid other allocations, and loops that must not pay the device
  * synchronization of cudaFree.  It calls no cudaMalloc, cudaFree or
  * allocating library routine: its scratch (the per-block partial sums) is a
  * fixed __device__ array of the library, held on every GPU that loads it
  * until the process exits.  More than MDRT_NB_NOALLOC_MAX_PAIRS pairs is
  * refused with MDRT_NB_INVALID_ARGUMENT (and a message on stderr).  The
  * first call on a device looks up the array's device address (a runtime
- * query, no allocation); make that first call before any stream capture.
+ * query, no allocation) and keeps it for the life of the process; make that
+ * first call before any stream capture, and do not call the entry point on
+ * a device after a cudaDeviceReset of it (the kept address may be stale).
  * Calls share the array: two calls that overlap on the GPU race.
  * No counterpart in MDIR; the allocating path is mdrtNbForce with
  * MDRT_NB_NO_PAIRS | MDRT_NB_NO_PME. */

@@ -15,13 +15,13 @@ direct + PME or no electrostatics, rigid three-site waters, NVE or NVT
 ps, kJ/mol, e, K."""
 
 import enum
-import math
 
 import numpy as np
 import torch
 
 from . import _lib as L
 from .md import Integrator as _Integrator
+from .systems import ewald_beta, pme_grid
 from .term import COULOMB, NonbondedTerm, _dp, _hp
 
 
@@ -157,32 +157,6 @@ class Schedule:
         self.energy_period = 0
 
 
-def _beta(rc, tol):
-    low, high = 0.0, 1.0
-    while math.erfc(high * rc) > tol:
-        high *= 2.0
-    for _ in range(100):
-        mid = 0.5 * (low + high)
-        if math.erfc(mid * rc) > tol:
-            low = mid
-        else:
-            high = mid
-    return 0.5 * (low + high)
-
-
-def _smooth(least):
-    size = max(int(least), 2)
-    while True:
-        if size % 2 == 0:
-            rest = size
-            for f in (2, 3, 5, 7):
-                while rest % f == 0:
-                    rest //= f
-            if rest == 1:
-                return size
-        size += 1
-
-
 class Program:
     """A validated, immutable plan (MDIR: mdir.Program with `plan`)."""
 
@@ -229,10 +203,9 @@ def compile(system, state, integrator, ensemble, execution, schedule):
     plan = {"particles": n, "cutoff": rc, "reach": R, "pruned_reach": Rin, "box": box.tolist(),
             "device": execution.device}
     if system.electrostatics == Electrostatics.PME:
-        beta = system.pme_alpha or _beta(rc, system.pme_tolerance)
-        grid = [int(g) if g else _smooth(math.ceil(L / system.pme_spacing - 1e-9)) for g, L in
-                zip(system.pme_grid, box)]
-        grid = [max(g, 2 * system.pme_order) for g in grid]
+        beta = system.pme_alpha or ewald_beta(rc, system.pme_tolerance)
+        auto = pme_grid(box, system.pme_spacing, system.pme_order)
+        grid = [max(int(g), 2 * system.pme_order) if g else a for g, a in zip(system.pme_grid, auto)]
         if system.pme_order not in (4, 5, 6, 8):
             raise UnsupportedError("pme_order: 4, 5, 6 or 8")
         plan.update({"beta": beta, "pme_grid": grid, "pme_order": system.pme_order})

@@ -1,10 +1,9 @@
 // mdrtNbExcludedNoAlloc: the excluded-pair Ewald correction with no device
 // allocation at all, for callers that cannot allocate.
 //
-// Who needs it: a caller that is recording a CUDA graph by stream capture
-// (cudaMalloc is not a capturable operation and breaks the capture), a host
-// that owns all device memory through its own fixed pool and forbids other
-// allocations, or a real-time loop that must not pay the device-wide
+// Who needs it: a host program that owns all device memory through its own
+// fixed pool and forbids any other allocation, a plugin loaded into such a
+// program, or a real-time loop that must not pay the device-wide
 // synchronization that cudaFree implies.  The regular path (mdrtNbForce)
 // keeps its per-block partial sums in buffers that the context allocates;
 // this variant keeps them in a file-scope __device__ array instead, so that
@@ -32,7 +31,9 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_excl_partials[kMaxBlocks * 8];
 
 // Its device address, found once per device (the host-side name of a
-// __device__ array is not a device address).
+// __device__ array is not a device address) and kept for the life of the
+// process: after a cudaDeviceReset the kept address may be stale, so a
+// program that resets a device does not call this entry point on it again.
 std::mutex g_mutex;
 double *g_partials[kMaxDevices] = {nullptr};
 

@@ -50,4 +50,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_argon_lattice.py <path of an MDIR checkout>")
+    main(sys.argv[1])

@@ -50,7 +50,9 @@ def read_prmtop(path):
 
 
 def main():
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_opc_three.py <path of an MDIR checkout>")
+    root = Path(sys.argv[1])
     inputs = root / "test/Driver/Inputs"
     top = read_prmtop(inputs / "opc/three.prmtop")
     charges = [float(v) / 18.2223 for v in top["CHARGE"]]

@@ -2,8 +2,9 @@
 allocating path (mdrtNbForce with the pairs and PME switched off), called
 through the C ABI twice in a row.
 
-It is for callers that cannot allocate device memory (stream capture, fixed
-memory pools, loops that must not synchronize on cudaFree): its scratch is a
+It is for callers that cannot allocate device memory (programs that own
+all device memory through a fixed pool, loops that must not synchronize on
+cudaFree): its scratch is a
 fixed device array of the library, shared by every call.  This file sorts
 last so that a run stopping at its first failure has run every other test."""
 import ctypes
