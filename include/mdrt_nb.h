@@ -122,7 +122,12 @@ int32_t mdrtNbSetExclusions(mdrtNb *ctx, const int32_t *offsets, const int32_t *
 
 /* Cutoff r_c, reach R (r_c + skin), Ewald beta (0: no Coulomb direct sum),
  * Coulomb constant f, the direct-sum shift erfc(beta r_c)/r_c (0/1), and
- * the LJ switch in r^2 from switch_distance (0/1).
+ * the switch of the LJ potential from switch_distance rs to r_c: 0 none;
+ * 1 the cubic in r^2, S = (1 - y)^2 (1 + 2y), y = (r^2 - rs^2)/(r_c^2 - rs^2)
+ * (MDIR's SQUARED_DISTANCE_SWITCH modifier, TermLennardJones.cpp:72-95);
+ * 2 the quintic in r, S = 1 - 10t^3 + 15t^4 - 6t^5, t = (r - rs)/(r_c - rs)
+ * (the potential switch of MDIR's md dialect, lib/Dialect/MD/Transforms/
+ * ExpandTruncation.cpp:19-46).
  * MDIR: TermNonbonded.cpp:378-470 and TermLennardJones.cpp:26-80. */
 int32_t mdrtNbSetInteraction(mdrtNb *ctx, double cutoff, double reach, double beta, double coulomb,
                              int32_t coulomb_shift, int32_t lj_switch, double switch_distance);
@@ -439,6 +444,119 @@ int32_t mdrtNbBatchConstants(mdrtNbBatch *batch, double *out);
  * launch shapes are fixed by its emitters (DevicePolicy.cpp:72-99). */
 int32_t mdrtNbBatchAutotune(mdrtNbBatch *batch, const double *x, double *forces, void *stream,
                             int32_t *choice);
+
+/* ---- MDIR's own runtime names ----------------------------------------------
+ * The entries an MDIR host program binds for the groups and the cuFFT
+ * transforms, with the memref descriptors of MLIR's C interface (a buffer
+ * of rank 1 or 2: allocated and aligned pointers, offset, sizes, strides;
+ * runtime/mdrt_cuda.c:1530-1582).  Where MDIR aborts (an invalid slot, a
+ * failed allocation, a failed transform), these entries print to stderr,
+ * leave an empty descriptor, and keep the status for mdrtGroupsLastStatus. */
+typedef struct {
+  void *allocated;
+  void *aligned;
+  int64_t offset;
+  int64_t size;
+  int64_t stride;
+} mdrtMemRef1D;
+typedef struct {
+  void *allocated;
+  void *aligned;
+  int64_t offset;
+  int64_t sizes[2];
+  int64_t strides[2];
+} mdrtMemRef2D;
+
+/* The slots of a groups registry, MDIR's stable slot table (ABI version 3,
+ * include/mdir/Runtime/GroupsABI.h:10-44); every slot a buffer of 32-bit
+ * values whose length follows from the registry's places and blocks. */
+#define MDRT_GROUPS_ABI_VERSION 3
+enum mdrtGroupsSlot {
+  MDRT_GROUPS_ORDER = 0,          /* [places] the particle at each place, -1 empty */
+  MDRT_GROUPS_COUNTS = 1,         /* [places / 16] entries of each group's list */
+  MDRT_GROUPS_ENTRIES = 2,        /* [64 blocks] the partner place of each entry, -1 past a list's end */
+  MDRT_GROUPS_MASKS = 3,          /* [64 blocks] members (bits 0-15) | image (bits 16-30, this header's code) */
+  MDRT_GROUPS_UNIT_GROUPS = 4,    /* [blocks] the group of each block */
+  MDRT_GROUPS_UNIT_ORDINALS = 5,  /* [blocks] the block's number in its group's list */
+  MDRT_GROUPS_SHIFTS = 6,         /* [places] whole cells of each place, int8x4 */
+  MDRT_GROUPS_INNER_ENTRIES = 7,  /* [64 blocks] the pruned lists by blocks */
+  MDRT_GROUPS_INNER_MASKS = 8,
+  MDRT_GROUPS_INNER_COUNTS = 9,   /* [blocks] entries of each block of the pruned lists */
+  MDRT_GROUPS_BLOCK_OF = 10,      /* [mdrtGroupsReserveBlockOf's length] */
+  MDRT_GROUPS_ACTIVE_UNITS = 11,  /* [blocks] the blocks of the pruned lists that hold entries */
+  MDRT_GROUPS_ACTIVE_COUNT = 12,  /* [1] their number */
+  MDRT_GROUPS_ACTIVE_RUNS = 13,
+  MDRT_GROUPS_ACTIVE_WIDE_RUNS = 14,
+  MDRT_GROUPS_PLACED = 15,        /* [places, 3] f32 positions of the places in the frames of the build */
+  MDRT_GROUPS_SEGMENT_COUNTS = 16,
+  MDRT_GROUPS_SEGMENT_LAST = 17,
+  MDRT_GROUPS_SEGMENT_ORDER = 18,
+  MDRT_GROUPS_RECORD_ENTRIES = 19,
+  MDRT_GROUPS_RECORD_MASKS = 20,
+  MDRT_GROUPS_RECORD_GROUPS = 21,
+  MDRT_GROUPS_RECORD_COUNTS = 22,
+  MDRT_GROUPS_SEGMENT_OFFSETS = 23,
+  MDRT_GROUPS_BUFFERS = 24
+};
+
+/* A registry with room for `places` places (rounded up to 16) and `blocks`
+ * blocks of 64 entries on the current device; the outer list's slots (0-6)
+ * are allocated now, the others where first asked for.  Returns the handle,
+ * 0 on failure.  MDIR: mdrtGroupsCreate, runtime/mdrt_cuda.c:3087. */
+int64_t mdrtGroupsCreate(int64_t places, int64_t blocks);
+/* The buffer of `slot` as a memref of rank 1 (allocated at its first use).
+ * MDIR: _mlir_ciface_mdrtGroupsBuffer, mdrt_cuda.c:3109. */
+void _mlir_ciface_mdrtGroupsBuffer(mdrtMemRef1D *result, int64_t handle, int64_t slot);
+/* Room for `places` places and `blocks` blocks, a quarter more than asked,
+ * if the registry has less; what the buffers held is lost (waits for the
+ * device).  MDIR: mdrtGroupsGrow, mdrt_cuda.c:3185. */
+void mdrtGroupsGrow(int64_t handle, int64_t places, int64_t blocks);
+/* After a complete build: the growths of the lists since the last call,
+ * and the registry marked built.  MDIR: mdrtGroupsBuilt, mdrt_cuda.c:3208. */
+int64_t mdrtGroupsBuilt(int64_t handle);
+/* Room for `length` values of MDRT_GROUPS_BLOCK_OF, a quarter more than
+ * asked, if it has less.  MDIR: mdrtGroupsReserveBlockOf, mdrt_cuda.c:3218. */
+void mdrtGroupsReserveBlockOf(int64_t handle, int64_t length);
+/* The placed positions as a memref of rank 2, [places, 3] f32.
+ * MDIR: _mlir_ciface_mdrtGroupsPlaced, mdrt_cuda.c:3300. */
+void _mlir_ciface_mdrtGroupsPlaced(mdrtMemRef2D *result, int64_t handle);
+/* Frees a registry (MDIR releases them when its run ends).  No MDIR
+ * counterpart by name. */
+int32_t mdrtGroupsDestroy(int64_t handle);
+/* The status the last failing MDIR-named entry left (MDRT_NB_OK if none
+ * since the last call), then cleared.  No MDIR counterpart: MDIR aborts. */
+int32_t mdrtGroupsLastStatus(void);
+/* Copies the lists of the context's last build into the registry's slots
+ * in MDIR's layout (growing it first as mdrtGroupsGrow does): order,
+ * counts, entries and masks in blocks of 64 with each block's group and
+ * ordinal, shifts, the placed positions, and, after a pruning, the pruned
+ * lists by blocks with the entries each holds, the active blocks (all of
+ * them) and their number.  Asynchronous on `stream` (one host wait for the
+ * count of the pruned blocks).  The values are this library's (partner
+ * places, 16-member masks with this header's image code, centred frames).
+ * No MDIR counterpart by name: MDIR's emitted build writes the registry. */
+int32_t mdrtNbGroupsExport(mdrtNb *ctx, int64_t handle, void *stream);
+/* The stream of the MDIR-named transforms below, which take none (NULL:
+ * the default stream). */
+int32_t mdrtNbSetAbiStream(void *stream);
+/* The forward and the backward (not normalized) 3D real transforms in f32
+ * of a k1 x k2 x k3 grid and its k1 x k2 x (k3/2 + 1) half-complex grid.
+ * MDIR: _mlir_ciface_mdrtCudaFFTForward3DF32 / Backward3DF32,
+ * runtime/mdrt_cuda.c:2942-2979. */
+void _mlir_ciface_mdrtCudaFFTForward3DF32(mdrtMemRef1D *real, mdrtMemRef1D *complex, int64_t k1, int64_t k2,
+                                          int64_t k3);
+void _mlir_ciface_mdrtCudaFFTBackward3DF32(mdrtMemRef1D *complex, mdrtMemRef1D *real, int64_t k1, int64_t k2,
+                                           int64_t k3);
+/* The backward transform of the half-complex grid times the Gaussian
+ * influence of a rectangular cell given by per-axis tables: for axis a of
+ * k_a points, three rows of k_a f32 (its wave numbers, their squares m_a^2
+ * and its factors t_a), the axes one after the other; each point (x, y, z)
+ * is scaled by t_1[x] t_2[y] t_3[z] / (m_1^2[x] + m_2^2[y] + m_3^2[z]) (0
+ * where the squares sum to 0), then transformed back.  MDIR:
+ * _mlir_ciface_mdrtCudaFFTGaussianBackwardF32 (mdrt_cuda.c:2985-2990) with
+ * its load callback (runtime/pme_callback.cu:5-21). */
+void _mlir_ciface_mdrtCudaFFTGaussianBackwardF32(mdrtMemRef1D *complex, mdrtMemRef1D *real, mdrtMemRef1D *tables,
+                                                 int64_t k1, int64_t k2, int64_t k3);
 
 #ifdef __cplusplus
 }

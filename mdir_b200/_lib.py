@@ -75,7 +75,38 @@ SIGNATURES = {
     "mdrtNbBatchAutotune": (_i32, [_p, _p, _p, _p, _p]),
     "mdrtCudaFFTForward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
     "mdrtCudaFFTBackward3DF32": (_i32, [_p, _p, _i64, _i64, _i64, _p]),
+    # MDIR's own names (memref descriptors by pointer)
+    "mdrtGroupsCreate": (_i64, [_i64, _i64]),
+    "_mlir_ciface_mdrtGroupsBuffer": (None, [_p, _i64, _i64]),
+    "mdrtGroupsGrow": (None, [_i64, _i64, _i64]),
+    "mdrtGroupsBuilt": (_i64, [_i64]),
+    "mdrtGroupsReserveBlockOf": (None, [_i64, _i64]),
+    "_mlir_ciface_mdrtGroupsPlaced": (None, [_p, _i64]),
+    "mdrtGroupsDestroy": (_i32, [_i64]),
+    "mdrtGroupsLastStatus": (_i32, []),
+    "mdrtNbGroupsExport": (_i32, [_p, _i64, _p]),
+    "mdrtNbSetAbiStream": (_i32, [_p]),
+    "_mlir_ciface_mdrtCudaFFTForward3DF32": (None, [_p, _p, _i64, _i64, _i64]),
+    "_mlir_ciface_mdrtCudaFFTBackward3DF32": (None, [_p, _p, _i64, _i64, _i64]),
+    "_mlir_ciface_mdrtCudaFFTGaussianBackwardF32": (None, [_p, _p, _p, _i64, _i64, _i64]),
 }
+
+
+class MemRef1D(ctypes.Structure):
+    """MLIR's descriptor of a buffer of rank 1 (mdrtMemRef1D)."""
+    _fields_ = [("allocated", _p), ("aligned", _p), ("offset", _i64), ("size", _i64), ("stride", _i64)]
+
+
+class MemRef2D(ctypes.Structure):
+    """MLIR's descriptor of a buffer of rank 2 (mdrtMemRef2D)."""
+    _fields_ = [("allocated", _p), ("aligned", _p), ("offset", _i64), ("sizes", _i64 * 2), ("strides", _i64 * 2)]
+
+
+# MDIR's slot table of a groups registry (mdrtGroupsSlot)
+GROUPS_ORDER, GROUPS_COUNTS, GROUPS_ENTRIES, GROUPS_MASKS, GROUPS_UNIT_GROUPS, GROUPS_UNIT_ORDINALS, \
+    GROUPS_SHIFTS, GROUPS_INNER_ENTRIES, GROUPS_INNER_MASKS, GROUPS_INNER_COUNTS, GROUPS_BLOCK_OF, \
+    GROUPS_ACTIVE_UNITS, GROUPS_ACTIVE_COUNT = range(13)
+GROUPS_PLACED, GROUPS_BUFFERS = 15, 24
 
 
 class NativeError(RuntimeError):

@@ -63,7 +63,11 @@ class Electrostatics(enum.Enum):
 
 class Truncation(enum.Enum):
     NONE = "NONE"
-    SWITCH = "SWITCH"  # the cubic switch of the potential in r^2 from switch_distance
+    SWITCH = "SWITCH"  # the cubic switch of the LJ potential in r^2 from switch_distance
+    POTENTIAL_SWITCH = "POTENTIAL_SWITCH"  # the quintic switch in r of MDIR's md dialect
+
+
+_SWITCH_FORM = {Truncation.NONE: 0, Truncation.SWITCH: 1, Truncation.POTENTIAL_SWITCH: 2}
 
 
 class System:
@@ -112,7 +116,7 @@ class System:
             s.pme_grid = tuple(d["grid"])
             s.pme_order = d["order"]
         if d.get("lj_switch"):
-            s.truncation = Truncation.SWITCH
+            s.truncation = Truncation.POTENTIAL_SWITCH if d["lj_switch"] == 2 else Truncation.SWITCH
             s.switch_distance = d["switch"]
         return s
 
@@ -230,7 +234,7 @@ def _make_term(program):
     t.set_particles(s.charges, s.types, s.sigma, s.epsilon)
     t.set_exclusions(pairs=s.excluded_pairs)
     t.set_interaction(p["cutoff"], p["reach"], p["beta"], coulomb=COULOMB,
-                      lj_switch=s.truncation == Truncation.SWITCH, switch_distance=s.switch_distance)
+                      lj_switch=_SWITCH_FORM[s.truncation], switch_distance=s.switch_distance)
     if p["pme_grid"]:
         t.set_pme(p["pme_grid"], p["pme_order"])
     t.set_deterministic(program.execution.deterministic)

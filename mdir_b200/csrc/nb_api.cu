@@ -236,6 +236,7 @@ int32_t mdrtNbSetInteraction(mdrtNb *ctx, double cutoff, double reach, double be
                              int32_t coulomb_shift, int32_t lj_switch, double switch_distance) {
   if (!ctx || !(cutoff > 0) || !(reach >= cutoff) || !(beta >= 0) || !std::isfinite(coulomb))
     return MDRT_NB_INVALID_ARGUMENT;
+  if (lj_switch < 0 || lj_switch > 2) return MDRT_NB_INVALID_ARGUMENT;
   if (lj_switch && !(switch_distance >= 0 && switch_distance < cutoff)) return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = ctx->c;
   c.cutoff = cutoff;

@@ -44,7 +44,8 @@ struct PairParams {
   float two_beta_sqrtpi;
   float coulomb;
   float coulomb_shift;  // erfc(beta rc)/rc when the direct sum is shifted, else 0
-  float rs2, winv;      // LJ switch in r^2
+  float rs2, winv;      // LJ switch 1, in r^2: rs^2 and 1 / (rc^2 - rs^2)
+  float rs, winv_r;     // LJ switch 2, in r: rs and 1 / (rc - rs)
   int ntypes;
   int64_t list_cap;
   int64_t units_cap;
@@ -88,7 +89,12 @@ __device__ __forceinline__ float nb_erfc_from_exp(float pbr, float ex) {
 // is fs d, d its displacement from the partner) and, with ENERGY, the LJ and
 // Coulomb energies.  A pair outside (masked, or beyond r_c) computes on its
 // own r^2, finite or not; the caller drops its results.
-template <bool ENERGY, bool SWITCH>
+// SWITCH multiplies the LJ potential by S from rs to rc: 1, the cubic in r^2
+// S = (1 - y)^2 (1 + 2y), y = (r^2 - rs^2)/(rc^2 - rs^2) (MDIR's
+// SQUARED_DISTANCE_SWITCH modifier, TermLennardJones.cpp:72-95); 2, the
+// quintic in r S = 1 - 10t^3 + 15t^4 - 6t^5, t = (r - rs)/(rc - rs) (the
+// potential switch of MDIR's md dialect, ExpandTruncation.cpp:19-46).
+template <bool ENERGY, int SWITCH>
 __device__ __forceinline__ void nb_pair_terms(const PairParams &P, float r2, float2 cc, float qq, float &fs,
                                               float &ulj, float &uc) {
   float rinv = nb_rsqrt(r2);
@@ -97,14 +103,20 @@ __device__ __forceinline__ void nb_pair_terms(const PairParams &P, float r2, flo
   float a12 = cc.y * s6 * s6, a6 = cc.x * s6;  // 12 c12 / r^12, 6 c6 / r^6
   fs = (a12 - a6) * rinv2;
   ulj = (ENERGY || SWITCH) ? a12 * (1.f / 12.f) - a6 * (1.f / 6.f) : 0.f;
-  if (SWITCH) {
+  float rr = r2 * rinv;
+  if (SWITCH == 1) {
     float y = fminf(fmaxf((r2 - P.rs2) * P.winv, 0.f), 1.f);
     float S = (1.f - y) * (1.f - y) * (1.f + 2.f * y);
     float dSdr2 = -6.f * y * (1.f - y) * P.winv;
     fs = fs * S - 2.f * ulj * dSdr2;
     ulj *= S;
+  } else if (SWITCH == 2) {
+    float t = fminf(fmaxf((rr - P.rs) * P.winv_r, 0.f), 1.f);
+    float S = fmaf(t * t * t, fmaf(t, fmaf(-6.f, t, 15.f), -10.f), 1.f);
+    float dSdr = t * t * fmaf(t, fmaf(-30.f, t, 60.f), -30.f) * P.winv_r;
+    fs = fs * S - ulj * dSdr * rinv;  // -(dU/dr S + U dS/dr) / r
+    ulj *= S;
   }
-  float rr = r2 * rinv;
   float ex = nb_ex2(r2 * P.nb2_log2e);
   float erfcv = nb_erfc_from_exp(P.beta_p * rr, ex);
   fs = fmaf(qq * fmaf(erfcv, rinv, P.two_beta_sqrtpi * ex), rinv2, fs);
@@ -131,7 +143,7 @@ __device__ __forceinline__ void nb_red_fixed(unsigned long long *addr, float x, 
 // shared memory (slots u and u + 16), so that in a dense round lane l reads
 // member (l + k) mod 16 at slot l mod 16 + k: an immediate offset in the
 // unrolled loop, no index arithmetic.
-template <bool ENERGY, bool FIXED, bool SWITCH, int LJM, bool BATCH = false>
+template <bool ENERGY, bool FIXED, int SWITCH, int LJM, bool BATCH = false>
 __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *__restrict__ group_L,
                                                 const int32_t *__restrict__ sizes,
                                                 const int2 *__restrict__ units,
@@ -915,7 +927,9 @@ PairParams pair_params(const NbCtx &c, const double box[3]) {
   P.coulomb_shift = c.coulomb_shift ? (float)(erfc(c.beta * c.cutoff) / c.cutoff) : 0.f;
   double rs2 = c.switch_distance * c.switch_distance;
   P.rs2 = (float)rs2;
-  P.winv = c.lj_switch ? (float)(1.0 / (c.cutoff * c.cutoff - rs2)) : 0.f;
+  P.winv = c.lj_switch == 1 ? (float)(1.0 / (c.cutoff * c.cutoff - rs2)) : 0.f;
+  P.rs = (float)c.switch_distance;
+  P.winv_r = c.lj_switch == 2 ? (float)(1.0 / (c.cutoff - c.switch_distance)) : 0.f;
   P.ntypes = c.ntypes;
   P.list_cap = c.list_cap;
   P.units_cap = c.units_cap;
@@ -957,14 +971,22 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, co
     else                        \
       NB_LAUNCH2(E, F, S, 0);   \
   } while (0)
-  bool F = c.deterministic, S = c.lj_switch != 0;
+#define NB_LAUNCH_S(E, F)        \
+  do {                           \
+    if (c.lj_switch == 2)        \
+      NB_LAUNCH(E, F, 2);        \
+    else if (c.lj_switch == 1)   \
+      NB_LAUNCH(E, F, 1);        \
+    else                         \
+      NB_LAUNCH(E, F, 0);        \
+  } while (0)
+  bool F = c.deterministic;
   if (energy) {
-    if (F) { if (S) NB_LAUNCH(true, true, true); else NB_LAUNCH(true, true, false); }
-    else { if (S) NB_LAUNCH(true, false, true); else NB_LAUNCH(true, false, false); }
+    if (F) NB_LAUNCH_S(true, true); else NB_LAUNCH_S(true, false);
   } else {
-    if (F) { if (S) NB_LAUNCH(false, true, true); else NB_LAUNCH(false, true, false); }
-    else { if (S) NB_LAUNCH(false, false, true); else NB_LAUNCH(false, false, false); }
+    if (F) NB_LAUNCH_S(false, true); else NB_LAUNCH_S(false, false);
   }
+#undef NB_LAUNCH_S
 #undef NB_LAUNCH
 #undef NB_LAUNCH2
 }
@@ -1094,7 +1116,7 @@ void nb_batch_pairs_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
   int64_t want = (c.units_cap + 7) / 8;
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)g_sm_count * std::max(1, c.pair_blocks_per_sm)));
 #define NB_BATCH_LAUNCH(E, M)                                                                                \
-  nb_pairs<E, false, false, M, true><<<grid, 256, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq, \
+  nb_pairs<E, false, 0, M, true><<<grid, 256, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq, \
                                                          c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed, c.unit_partials, \
                                                          c.status, nullptr)
   if (energy) {

@@ -29,7 +29,7 @@ def make_term(s, deterministic=False):
     t = NonbondedTerm(n)
     t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
     t.set_exclusions(pairs=s["excluded_pairs"])
-    t.set_interaction(s["cutoff"], s["reach"], s["beta"], lj_switch=s.get("lj_switch", False),
+    t.set_interaction(s["cutoff"], s["reach"], s["beta"], lj_switch=s.get("lj_switch", 0),
                       switch_distance=s.get("switch", 0.0))
     if s["pme"]:
         t.set_pme(s["grid"], s["order"])
@@ -118,3 +118,35 @@ def test_pme_potential_is_dE_dq(cuda):
     got = run(s, potential=True)
     np.testing.assert_allclose(got["potential"], ref["potential"], rtol=1e-4,
                                atol=1e-5 * np.abs(ref["potential"]).max())
+
+
+def test_argon_test_potential_on_the_device(cuda):
+    """MDIR's test/Driver/argon.test:9-14 through the device path: the
+    864-atom lattice of examples/argon with LJ switched from 0.75 to
+    0.85 nm by the md dialect's quintic potential switch (lj_switch 2)
+    gives the step-0 potential -1304.88... kcal/mol; forces against the
+    FP64 oracle, also on positions moved into the switching region."""
+    fx = json.loads((GOLDEN / "argon_lattice.json").read_text())
+    x = np.array(fx["positions_nm"])
+    n = len(x)
+    s = {"positions": x, "charges": np.zeros(n), "types": np.zeros(n, dtype=np.int32),
+         "sigma": np.array([[fx["sigma_nm"]]]), "epsilon": np.array([[fx["epsilon_kj_mol"]]]),
+         "box": np.array(fx["box_nm"]), "cutoff": fx["cutoff_nm"], "reach": fx["cutoff_nm"] + 0.1,
+         "pme": False, "beta": 0.0, "grid": None, "order": 4, "excluded_pairs": np.zeros((0, 2), dtype=np.int64),
+         "dispersion": False, "lj_switch": 2, "switch": fx["switch_nm"]}
+    got = run(s)
+    kcal = got["e"]["lj"] / O.KJ_PER_KCAL
+    assert f"{kcal:.6f}".startswith(fx["potential_kcal_mol_prefix"]), kcal
+    ref = O.evaluate(s, x)
+    assert abs(got["e"]["lj"] - ref["terms"]["lj"]) <= ENERGY_TOL * abs(ref["terms"]["lj"])
+    assert rms_rel(got["forces"], ref["forces"]) < FORCE_RMS_TOL
+    rng = np.random.default_rng(2)
+    s["positions"] = x + rng.uniform(-0.03, 0.03, size=x.shape)
+    got = run(s)
+    ref = O.evaluate(s, s["positions"])
+    assert rms_rel(got["forces"], ref["forces"]) < FORCE_RMS_TOL
+    assert abs(got["e"]["lj"] - ref["terms"]["lj"]) <= ENERGY_TOL * abs(ref["terms"]["lj"])
+    # the two switches are different functions of r: the quintic is not the cubic in r^2
+    s["lj_switch"] = 1
+    cubic = run(s)["e"]["lj"]
+    assert abs(cubic - got["e"]["lj"]) > 1e-3
