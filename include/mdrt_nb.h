@@ -344,6 +344,14 @@ int32_t mdrtMdBuild(mdrtMd *md, const double *x, const double box[3], void *stre
  * the host reading the test of validity after each step. */
 int32_t mdrtMdRun(mdrtMd *md, double *x, double *v, const double box[3], double dt, int64_t steps,
                   int32_t unroll, void *stream);
+/* The integrator of mdrtMdRun: leap-frog (the default; v half a step
+ * behind x) or velocity Verlet (v on the step at the start and the end of
+ * each run; the same positions).  Velocity Verlet refuses rigid waters
+ * (MDRT_NB_UNSUPPORTED): velocities on the step would need their velocity
+ * constraints.  MDIR: the integrators of docs/dynamics.md (velocity Verlet
+ * for argon.test; leap-frog). */
+enum mdrtMdIntegrator { MDRT_MD_LEAP_FROG = 0, MDRT_MD_VELOCITY_VERLET = 1 };
+int32_t mdrtMdSetIntegrator(mdrtMd *md, int32_t method);
 /* out[9]: thermostat scaling, kinetic energy of the last two half steps,
  * steps taken, builds made, degrees of freedom, prunings made, runs of step
  * graphs redone after a list overflow, stops at a drift past half the skin

@@ -21,6 +21,7 @@ SLOT_ORDER, SLOT_COUNTS, SLOT_ENTRIES, SLOT_UNITS, SLOT_SHIFTS, SLOT_PLACED, SLO
     0, 1, 2, 4, 6, 15, 16
 SLOT_INNER_ENTRIES, SLOT_INNER_COUNTS = 7, 9
 GRAD_PRODUCT, GRAD_ENERGY = 0, 1
+LEAP_FROG, VELOCITY_VERLET = 0, 1
 
 _lib = None
 
@@ -56,6 +57,7 @@ SIGNATURES = {
     "mdrtMdDestroy": (_i32, [_p]),
     "mdrtMdSetThermostat": (_i32, [_p, _d, _d, ctypes.c_uint64]),
     "mdrtMdSetLookahead": (_i32, [_p, _d]),
+    "mdrtMdSetIntegrator": (_i32, [_p, _i32]),
     "mdrtMdBuild": (_i32, [_p, _p, _p, _p]),
     "mdrtMdRun": (_i32, [_p, _p, _p, _p, _d, _i64, _i32, _p]),
     "mdrtMdThermo": (_i32, [_p, _p, _p]),

@@ -129,6 +129,10 @@ class InitialState:
 
 
 class Integrator:
+    """method: "LEAP_FROG" or "VELOCITY_VERLET" (MDIR's integrators,
+    docs/dynamics.md); velocity Verlet keeps the velocities on the step and
+    takes no rigid waters."""
+
     def __init__(self):
         self.method = "LEAP_FROG"
         self.timestep = 0.002
@@ -219,6 +223,11 @@ def compile(system, state, integrator, ensemble, execution, schedule):
         raise UnsupportedError("ensembles: NVE and NVT")
     if not integrator.timestep > 0:
         raise InputError("timestep must be positive")
+    method = str(integrator.method).upper()
+    if method not in ("LEAP_FROG", "VELOCITY_VERLET"):
+        raise UnsupportedError("integrators: LEAP_FROG and VELOCITY_VERLET")
+    if method == "VELOCITY_VERLET" and system.rigid_water and system.water_residues is not None:
+        raise UnsupportedError("VELOCITY_VERLET with rigid waters needs velocity constraints; use LEAP_FROG")
     plan["waters"] = 0 if system.water_residues is None else len(system.water_residues)
     return Program(system, state, integrator, ensemble, execution, schedule, plan)
 
@@ -260,6 +269,7 @@ class Simulation:
         self.md = _Integrator(self.term, s.masses, s.water_residues if s.rigid_water else None)
         e = program.ensemble
         self.md.thermostat(e.temperature, e.tau_t if e.kind == EnsembleKind.NVT else 0.0, e.seed)
+        self.md.method(str(program.integrator.method))
         st = program.state
         self.x = torch.tensor(st.positions, dtype=torch.float64, device=self.device)
         v = st.velocities if len(st.velocities) else np.zeros_like(st.positions)

@@ -66,6 +66,7 @@ struct mdrtMd {
   int64_t regrows = 0;             // runs redone after an overflow inside the graphs
   int64_t redone = 0;              // stops at a drift past half the skin between two decisions
   double lookahead = 1.5;          // mdrtMdSetLookahead
+  int verlet = 0;                  // mdrtMdSetIntegrator: velocities on the step at a run's ends
   // PME gathered by the update (order 4): the step's side stream spreads the
   // frames into qgrid (through qfixed in the deterministic mode) and
   // transforms qgrid -> spec -> phi; the update gathers each atom's PME force
@@ -1183,10 +1184,62 @@ static int32_t md_prepare_graph(mdrtMd *m, double *x, double *v, const double bo
   return MDRT_NB_OK;
 }
 
+// v += sign dt/2 F/m: the half kick of velocity Verlet at a run's end
+// (sign +1) or, backwards, at its start (sign -1).
+__global__ void md_half_kick(int64_t n3, const double *__restrict__ f, const double *__restrict__ inv_mass,
+                             double half_dt, double *__restrict__ v) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) v[i] += half_dt * inv_mass[i / 3] * f[i];
+}
+
+// The forces of the term at x (with the lists in force) and the half kick.
+static int32_t md_verlet_kick(mdrtMd *m, const double *x, double *v, const double box[3], double half_dt,
+                              cudaStream_t st) {
+  int32_t s = mdrtNbForce(m->handle, x, box, 0u, m->force, st);
+  if (s) return s;
+  md_half_kick<<<blocks_for(3 * m->n, 256), 256, 0, st>>>(3 * m->n, m->force, m->inv_mass, half_dt, v);
+  return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
+}
+
+static int32_t md_run_leapfrog(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
+                               int32_t unroll, void *stream);
+
 extern "C" {
 
+int32_t mdrtMdSetIntegrator(mdrtMd *m, int32_t method) {
+  if (!m || (method != MDRT_MD_LEAP_FROG && method != MDRT_MD_VELOCITY_VERLET)) return MDRT_NB_INVALID_ARGUMENT;
+  // velocities on the step need the velocity constraints of rigid waters
+  // (RATTLE), which the step does not apply
+  if (method == MDRT_MD_VELOCITY_VERLET && m->nwaters > 0) return MDRT_NB_UNSUPPORTED;
+  m->verlet = method == MDRT_MD_VELOCITY_VERLET;
+  return MDRT_NB_OK;
+}
+
+// Velocity Verlet and leap-frog give the same positions; they differ in
+// when the velocities are: on the step (v_n) or half a step behind.  With
+// velocity Verlet the run takes v_0, turns it into v_{-1/2} = v_0 - F_0
+// dt/(2m), runs the leap-frog steps, and turns v_{N-1/2} into v_N =
+// v_{N-1/2} + F_N dt/(2m), with the forces at the run's first and last
+// positions (two evaluations of the term a run).
 int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
                   int32_t unroll, void *stream) {
+  if (!m || !x || !v || !box || !(dt > 0) || steps < 0 || unroll > MD_MAX_UNROLL || unroll < -MD_MAX_UNROLL)
+    return MDRT_NB_INVALID_ARGUMENT;
+  if (!m->verlet || steps == 0) return md_run_leapfrog(m, x, v, box, dt, steps, unroll, stream);
+  NbCtx &c = *m->nb;
+  if (!c.built) return MDRT_NB_NOT_BUILT;
+  cudaSetDevice(c.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  int32_t s = md_verlet_kick(m, x, v, box, -0.5 * dt, st);
+  if (!s) s = md_run_leapfrog(m, x, v, box, dt, steps, unroll, stream);
+  if (!s) s = md_verlet_kick(m, x, v, box, 0.5 * dt, st);
+  return s;
+}
+
+}  // extern "C"
+
+static int32_t md_run_leapfrog(mdrtMd *m, double *x, double *v, const double box[3], double dt, int64_t steps,
+                               int32_t unroll, void *stream) {
   if (!m || !x || !v || !box || !(dt > 0) || steps < 0 || unroll > MD_MAX_UNROLL || unroll < -MD_MAX_UNROLL)
     return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = *m->nb;
@@ -1271,6 +1324,8 @@ int32_t mdrtMdRun(mdrtMd *m, double *x, double *v, const double box[3], double d
   if (left > 0) return md_run_steps(m, x, v, box, dt, left, unroll, stream);
   return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
 }
+
+extern "C" {
 
 // [0] lambda, [1] kinetic energy of the last half step, [2] of the one
 // before, [3] steps, [4] builds since create, [5] degrees of freedom.

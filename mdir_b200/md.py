@@ -44,6 +44,13 @@ class Integrator:
     def thermostat(self, temperature, tau, seed=1):
         L.check(L.lib().mdrtMdSetThermostat(self._h, temperature, tau, seed), "mdrtMdSetThermostat")
 
+    def method(self, name):
+        """The integrator: "leap_frog" (velocities half a step behind the
+        positions) or "velocity_verlet" (velocities on the step at the start
+        and the end of each run; the same positions; no rigid waters)."""
+        code = {"leap_frog": L.LEAP_FROG, "velocity_verlet": L.VELOCITY_VERLET}[name.lower()]
+        L.check(L.lib().mdrtMdSetIntegrator(self._h, code), "mdrtMdSetIntegrator")
+
     def lookahead(self, factor):
         """The rebuild decision's extrapolation of the drift (default 1.5)."""
         L.check(L.lib().mdrtMdSetLookahead(self._h, float(factor)), "mdrtMdSetLookahead")

@@ -112,3 +112,18 @@ def test_compile_refuses_what_the_library_does_not_offer():
     ens.kind = "NPT"
     with pytest.raises(mdir.UnsupportedError):
         mdir.compile(system, state, integ, ens, exe, sch)
+
+
+def test_compile_takes_the_integrators_mdir_names():
+    s, system, state, integ, ens, exe, sch = _program_inputs()
+    integ.method = "VELOCITY_VERLET"  # rigid waters need velocity constraints
+    with pytest.raises(mdir.UnsupportedError):
+        mdir.compile(system, state, integ, ens, exe, sch)
+    integ.method = "BROWNIAN"
+    with pytest.raises(mdir.UnsupportedError):
+        mdir.compile(system, state, integ, ens, exe, sch)
+    a = systems.argon()
+    argon = mdir.System.from_dict(a)
+    integ.method = "VELOCITY_VERLET"
+    p = mdir.compile(argon, mdir.InitialState(a["positions"], None, a["box"]), integ, ens, exe, sch)
+    assert p.plan["waters"] == 0

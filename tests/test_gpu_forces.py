@@ -139,7 +139,8 @@ def test_argon_test_potential_on_the_device(cuda):
     assert f"{kcal:.6f}".startswith(fx["potential_kcal_mol_prefix"]), kcal
     ref = O.evaluate(s, x)
     assert abs(got["e"]["lj"] - ref["terms"]["lj"]) <= ENERGY_TOL * abs(ref["terms"]["lj"])
-    assert rms_rel(got["forces"], ref["forces"]) < FORCE_RMS_TOL
+    # on the lattice the forces cancel to ~0.01 kJ/mol/nm by symmetry, so
+    # they are compared where the atoms have moved off it
     rng = np.random.default_rng(2)
     s["positions"] = x + rng.uniform(-0.03, 0.03, size=x.shape)
     got = run(s)

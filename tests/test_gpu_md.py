@@ -216,3 +216,66 @@ def test_forces_of_a_step_are_the_oracle_forces(cuda, deterministic):
     err = np.sqrt(np.mean(np.sum((f - ref) ** 2, 1)) / np.mean(np.sum(ref ** 2, 1)))
     assert err < 1e-5, err
     assert md.thermo()["prunes"] > 0 and t.status() == 0
+
+
+def test_velocity_verlet_argon_nve(cuda):
+    """The liquid-argon workload (864 atoms, cutoff 1.0 nm, Maxwell
+    velocities at 120 K) under velocity Verlet, NVE at 2 fs: the first 20
+    steps follow an FP64 velocity-Verlet integration on the oracle's forces
+    (positions and on-step velocities), and over 2,000 steps the total energy
+    with on-step velocities (the dispersion correction is a constant) moves
+    by a small part of its fluctuations."""
+    s = systems.argon()
+    n = len(s["charges"])
+    t = NonbondedTerm(n)
+    t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t.set_interaction(s["cutoff"], s["reach"], 0.0)
+    md = Integrator(t, s["masses"])
+    md.method("velocity_verlet")
+    md.thermostat(120.0, 0.0, 1)
+    v0 = systems.maxwell_velocities(s, 120.0, seed=2)
+    x = torch.tensor(s["positions"], dtype=torch.float64, device="cuda")
+    v = torch.tensor(v0, device="cuda")
+    md.build(x, s["box"])
+    dt = 0.002
+    md.run(x, v, s["box"], dt, 20, unroll=10)
+    # the FP64 reference: velocity Verlet on the oracle's forces
+    m = np.asarray(s["masses"])[:, None]
+    xr, vr = s["positions"].copy(), v0.copy()
+    f = O.evaluate(s, xr)["forces"]
+    for _ in range(20):
+        vr = vr + 0.5 * dt * f / m
+        xr = xr + dt * vr
+        f = O.evaluate(s, xr)["forces"]
+        vr = vr + 0.5 * dt * f / m
+    np.testing.assert_allclose(x.cpu().numpy(), xr, atol=1e-6)
+    vd = v.cpu().numpy()
+    assert np.sqrt(np.mean((vd - vr) ** 2)) < 1e-4 * np.sqrt(np.mean(vr ** 2))
+
+    def total():
+        xe = x.cpu().numpy()
+        e = O.evaluate(s, xe)["energy"]
+        return e + 0.5 * float(np.sum(m * v.cpu().numpy() ** 2))
+
+    e0 = [total()]
+    for _ in range(10):
+        md.run(x, v, s["box"], dt, 198, unroll=-6)
+        e0.append(total())
+    e0 = np.array(e0)
+    # the plain LJ cut makes the energy jump when pairs cross the cutoff:
+    # a drift well inside a percent of the kinetic energy (about 1.3 kJ/mol
+    # per atom at 120 K)
+    kin = 0.5 * float(np.sum(m * v.cpu().numpy() ** 2))
+    assert abs(e0[-1] - e0[0]) < 0.01 * kin
+    # leap-frog from v_{-1/2} gives the same positions
+    t2 = NonbondedTerm(n)
+    t2.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t2.set_interaction(s["cutoff"], s["reach"], 0.0)
+    md2 = Integrator(t2, s["masses"])
+    md2.thermostat(120.0, 0.0, 1)
+    x2 = torch.tensor(s["positions"], dtype=torch.float64, device="cuda")
+    md2.build(x2, s["box"])
+    f0 = O.evaluate(s, s["positions"])["forces"]
+    v2 = torch.tensor(v0 - 0.5 * dt * f0 / m, device="cuda")
+    md2.run(x2, v2, s["box"], dt, 20, unroll=10)
+    np.testing.assert_allclose(x2.cpu().numpy(), xr, atol=1e-6)
