@@ -777,7 +777,9 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
                    double *__restrict__ x_prune, int32_t *unit_counter, int2 *__restrict__ units,
                    int64_t units_cap, double *prunes) {
   extern __shared__ int2 s_stage[];
-  __shared__ float4 s_m[NB_GROUP];
+  // members m and m + 8 side by side for the packed tests: (x, x', y, y'), (z, z')
+  __shared__ float4 s_mxy[NB_GROUP / 2];
+  __shared__ float2 s_mz[NB_GROUP / 2];
   __shared__ int s_cls[NB_PRUNE_WARPS][NB_SPARSE_BITS + 1];
   __shared__ int s_unit0, s_nunits;
   __shared__ int2 s_qe[NB_PRUNE_WARPS][64];    // a warp's queue of entries that pass the box test
@@ -796,7 +798,12 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
   }
   if (warp == 0) {
     float4 xme = xq[g * NB_GROUP + (lane & 15)];
-    if (lane < NB_GROUP) s_m[lane] = xme;
+    float ox = __shfl_sync(FULL, xme.x, lane + 8), oy = __shfl_sync(FULL, xme.y, lane + 8);
+    float oz = __shfl_sync(FULL, xme.z, lane + 8);
+    if (lane < NB_GROUP / 2) {
+      s_mxy[lane] = make_float4(xme.x, ox, xme.y, oy);
+      s_mz[lane] = make_float2(xme.z, oz);
+    }
     bool on = lane < NB_GROUP && order[g * NB_GROUP + (lane & 15)] >= 0;
     unsigned live = __ballot_sync(FULL, on) & 0xffffu;
     float3 blo, bhi;
@@ -830,10 +837,18 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
       en = qe[lane];
       float4 xj = qx[lane];
       unsigned mm = (unsigned)en.y & live;
+      // members m and m + 8 at once in packed f32x2 arithmetic, with the
+      // roundings of nb_prune_r2 (x - y is x + (-y) exactly; products and
+      // sums rounded once, in its order), so the bits are the same
+      const float2 nx = make_float2(-xj.x, -xj.x), ny = make_float2(-xj.y, -xj.y), nz = make_float2(-xj.z, -xj.z);
 #pragma unroll
-      for (int m = 0; m < NB_GROUP; ++m) {
-        float r2 = nb_prune_r2(s_m[m], xj.x, xj.y, xj.z);
-        if (((mm >> m) & 1u) && r2 <= rin2) inner |= 1u << m;
+      for (int m = 0; m < NB_GROUP / 2; ++m) {
+        const float4 a = s_mxy[m];
+        const float2 dx = __fadd2_rn(make_float2(a.x, a.y), nx), dy = __fadd2_rn(make_float2(a.z, a.w), ny);
+        const float2 dz = __fadd2_rn(s_mz[m], nz);
+        const float2 r2 = __fadd2_rn(__fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy)), __fmul2_rn(dz, dz));
+        if (((mm >> m) & 1u) && r2.x <= rin2) inner |= 1u << m;
+        if (((mm >> (m + 8)) & 1u) && r2.y <= rin2) inner |= 1u << (m + 8);
       }
     }
     unsigned has = __ballot_sync(FULL, inner != 0);

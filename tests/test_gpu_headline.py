@@ -198,3 +198,49 @@ def test_the_256_frame_batch_frame_by_frame(cuda):
     F2 = ev.force(energy=True, graph=True).cpu().numpy()
     assert rms_rel(F2, F) < 1e-6
     ev.close()
+
+
+@pytest.mark.parametrize("x_kind", ["start", "moved"])
+def test_tuned_reaches_leave_the_pairs_and_forces_unchanged(cuda, box23550, x_kind):
+    """Every (outer reach, pruned reach) the step autotuner tries (Integrator.
+    tune's candidates, MDIR's skins search D281) gives the same pairs within
+    the cutoff, and forces and energies equal to the FP64 oracle's: the
+    reaches change the work, never the result."""
+    s, x1 = box23550
+    x = s["positions"] if x_kind == "start" else x1
+    ref = O.evaluate(s, x)
+    scale = sum(abs(v) for v in ref["terms"].values())
+    rc = s["cutoff"]
+    within = None
+    forces = []
+    for R, Rin in ((1.3, 1.025), (1.5, 1.05), (1.7, 1.025), (1.7, 1.05), (1.0, 0.0)):
+        t = NonbondedTerm(len(s["charges"]))
+        t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+        t.set_exclusions(pairs=s["excluded_pairs"])
+        t.set_interaction(rc, R, s["beta"])
+        t.set_pruned_reach(Rin)
+        t.set_pme(s["grid"], s["order"])
+        t.build(torch.tensor(s["positions"], device=cuda), s["box"])
+        xd = torch.tensor(x, device=cuda)
+        if Rin:
+            t.prune(xd, s["box"])
+        f = t.force(xd, energy=True).cpu().numpy()
+        e = t.energies()
+        assert rms_rel(f, ref["forces"]) < FORCE_RMS_TOL, (R, Rin)
+        for name in ("lj", "coulomb"):
+            assert abs(e[name] - ref["terms"][name]) <= ENERGY_TOL * scale, (R, Rin, name)
+        forces.append(f)
+        # the pairs of the build's lists within the cutoff (at the build's positions)
+        if x_kind == "start":
+            p = t.pair_set(t.build(torch.tensor(s["positions"], device=cuda), s["box"]))
+            xs = s["positions"]
+            d = xs[p[:, 1]] - xs[p[:, 0]]
+            d -= s["box"] * np.round(d / s["box"])
+            inside = canon(p[np.sum(d * d, 1) < rc * rc])
+            if within is None:
+                within = inside
+            else:
+                np.testing.assert_array_equal(inside, within)
+        t.close()
+    for f in forces[1:]:
+        assert rms_rel(f, forces[0]) < 1e-6

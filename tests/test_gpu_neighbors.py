@@ -47,13 +47,19 @@ def test_build_is_deterministic(cuda):
     t1, s1, p1 = device_pairs(x, 7.0, 1.0, None)
     e1 = t1.buffer(L.SLOT_ENTRIES, np.int32, 2).copy()
     o1 = t1.buffer(L.SLOT_ORDER, np.int32).copy()
+    c1 = t1.buffer(L.SLOT_COUNTS, np.int32).copy()
     t2, s2, p2 = device_pairs(x, 7.0, 1.0, None)
     e2 = t2.buffer(L.SLOT_ENTRIES, np.int32, 2)
     o2 = t2.buffer(L.SLOT_ORDER, np.int32)
+    c2 = t2.buffer(L.SLOT_COUNTS, np.int32)
     np.testing.assert_array_equal(o1, o2)
     G = s1[6]
     cap = t1.info()["list_capacity"]
-    np.testing.assert_array_equal(e1[: G * cap], e2[: G * cap])
+    assert cap == t2.info()["list_capacity"]
+    np.testing.assert_array_equal(c1[:G], c2[:G])
+    # every list entry for entry (the slab past a list's end is not written)
+    for g in range(G):
+        np.testing.assert_array_equal(e1[g * cap: g * cap + c1[g]], e2[g * cap: g * cap + c2[g]])
 
 
 def test_capacity_grows_and_retries(cuda):
