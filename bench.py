@@ -576,6 +576,7 @@ def main():
     exe.device, exe.graph_steps = local, args.unroll
     exe.pair_sms = tuned["pair_sms"] if tuned else args.pair_sms
     exe.pair_blocks_per_sm = tuned["pair_blocks_per_sm"] if tuned else args.pair_blocks
+    exe.fused_prune = tuned["fused_prune"] if tuned else 0
     sim = mdir.Simulation(mdir.compile(system, st, integ, ens, exe, sch))
 
     def e2e_step():

@@ -49,7 +49,11 @@ enum mdrtNbFlags {
   MDRT_NB_NO_PAIRS = 8u,     /* skip the pair term */
   MDRT_NB_NO_PME = 16u,      /* skip the reciprocal sum */
   MDRT_NB_NO_EXCLUDED = 32u, /* skip the excluded-pair correction */
-  MDRT_NB_GRAPH = 64u        /* mdrtNbBatchForce: replay the launches as a CUDA graph */
+  MDRT_NB_GRAPH = 64u,       /* mdrtNbBatchForce: replay the launches as a CUDA graph */
+  /* prune the dual list at x first, as mdrtNbPrune does; for forces
+   * without energies outside the deterministic mode the pruning and the
+   * pairs of the fresh inner lists run as one kernel (MDIR D284) */
+  MDRT_NB_PRUNE = 128u
 };
 
 /* Slots of the energies of mdrtNbEnergies (f64). */
@@ -153,7 +157,11 @@ int32_t mdrtNbPrune(mdrtNb *ctx, const double *x, const double box[3], void *str
 enum mdrtNbTuneKey {
   MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM = 0,
   MDRT_NB_TUNE_SEARCH_WARPS = 1,  /* batches only */
-  MDRT_NB_TUNE_PAIR_SMS = 2       /* SMs the pair grid spans (0: all); the others stay free for PME */
+  MDRT_NB_TUNE_PAIR_SMS = 2,      /* SMs the pair grid spans (0: all); the others stay free for PME */
+  /* the MD step's pruning of the dual list in its pair kernel (MDIR D284,
+   * lib/Dialect/MDExec/DevicePolicy.cpp:70-99): 0 from 4096 groups on (the
+   * default), 1 always, 2 never; never in the deterministic mode */
+  MDRT_NB_TUNE_FUSED_PRUNE = 3
 };
 int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value);
 

@@ -133,7 +133,7 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   nb_free(c.xq); nb_free(c.typ_p); nb_free(c.acc); nb_free(c.acc_fixed);
   nb_free(c.unit_partials); nb_free(c.energy);
   nb_free(c.slab_in); nb_free(c.counts_in); nb_free(c.unit_n_in); nb_free(c.unit_start_in);
-  nb_free(c.units_in); nb_free(c.sizes_in);
+  nb_free(c.units_in); nb_free(c.sizes_in); nb_free(c.one);
   if (c.h_sizes) cudaFreeHost(c.h_sizes);
   if (c.h_energy) cudaFreeHost(c.h_energy);
   delete ctx;
@@ -256,6 +256,10 @@ int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value) {
     case MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM:
       if (value < 1 || value > 4) return MDRT_NB_INVALID_ARGUMENT;
       ctx->c.pair_blocks_per_sm = value;
+      return MDRT_NB_OK;
+    case MDRT_NB_TUNE_FUSED_PRUNE:
+      if (value < 0 || value > 2) return MDRT_NB_INVALID_ARGUMENT;
+      ctx->c.fused_prune = value;
       return MDRT_NB_OK;
     case MDRT_NB_TUNE_PAIR_SMS:
       if (value < 0 || value > 4096) return MDRT_NB_INVALID_ARGUMENT;
@@ -408,7 +412,26 @@ static int32_t nb_force_entry(mdrtNb *ctx, const double *x, const double box[3],
   if (!(flags & MDRT_NB_ACCUMULATE)) CK(cudaMemsetAsync(forces, 0, sizeof(double) * 3 * c.n, st));
   if (energy) CK(cudaMemsetAsync(c.energy, 0, sizeof(double) * NB_E_SLOTS, st));
   nb_gather_frames(c, x, box, st);
-  if (pairs) nb_pairs_run(c, box, energy, st);
+  bool pairs_done = false;
+  if ((flags & MDRT_NB_PRUNE) && c.inner_reach > 0.0) {
+    // the pruning at x, and, for forces outside the deterministic mode, the
+    // pairs of the pruned lists in the same kernel (MDIR D284)
+    if (pairs && !energy && !c.deterministic && sizeof(int2) * (size_t)c.list_cap <= NB_FUSED_STAGE_MAX) {
+      if (!c.one) {
+        CK(cudaMalloc(&c.one, sizeof(int32_t)));
+        int32_t h_one = 1;
+        CK(cudaMemcpy(c.one, &h_one, sizeof(int32_t), cudaMemcpyHostToDevice));
+      }
+      CK(cudaMemsetAsync(c.sizes_in + NB_SIZE_UNITS, 0, sizeof(int32_t), st));  // the blocks claim their units
+      nb_prune_pairs_run(c, box, c.one, x, nullptr, nullptr, c.sizes_in + NB_SIZE_UNITS, st, nullptr);
+      pairs_done = true;
+    } else {
+      nb_prune_run(c, box, st);
+    }
+    c.inner_valid = true;
+    c.prunes++;
+  }
+  if (pairs && !pairs_done) nb_pairs_run(c, box, energy, st);
   if (excluded) nb_excluded_run(c, box, energy, st);
   if (energy && (pairs || excluded)) nb_reduce_energy(c, pairs, excluded, st);
   if (pme) {

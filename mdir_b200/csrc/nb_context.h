@@ -115,6 +115,8 @@ struct NbCtx {
   // tuning (mdrtNbSetTuning): blocks of 8 warps per SM of the pair kernel
   int pair_blocks_per_sm = 4;
   int pair_sms = 0;  // SMs the persistent pair grid spans (0: all); the rest are left to PME
+  int fused_prune = 0;  // the MD step's pruning in the pair kernel: 0 by group count, 1 always, 2 never
+  int32_t *one = nullptr;  // a device 1: the gate of a pruning a force call asks for (MDRT_NB_PRUNE)
   // parameter gradient scratch (mdrtNbParameterGradient), allocated at the first call
   float4 *adj_g = nullptr;        // per place: the cotangent on the forces (f32)
   double *adj_q = nullptr;        // per place: the charge gradient, kept zero between calls
@@ -246,7 +248,23 @@ int nb_grow_lists_keep(NbCtx &c, int64_t longest, cudaStream_t s);
 #define NB_GROW_AHEAD 0.85
 void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
 // With `halt` (device), nothing when *halt is set (the MD step's stop).
-void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt = nullptr);
+// With `skip` (device), nothing when *skip is set (a pruning step whose
+// pairs nb_prune_pairs_run computed).
+void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt = nullptr,
+                  const int *skip = nullptr);
+// The pruning of a pruning step with the pairs of its fresh inner lists in
+// one kernel (MDIR D284), when *gate (device) is set: the same inner lists
+// and claimed units as nb_prune_gated, the forces of the pairs added.
+// Forces only, outside the deterministic mode.
+void nb_prune_pairs_run(NbCtx &c, const double box[3], const int *gate, const double *x, double *x_prune,
+                        double *prunes, int32_t *unit_counter, cudaStream_t s, const int *halt);
+// Whether the MD step prunes in its pair kernel: the tuning (fused_prune),
+// by default from NB_FUSED_PRUNE_GROUPS groups of the last build on (MDIR's
+// threshold, DevicePolicy.cpp:70-99); never in the deterministic mode or
+// with lists too long for the kernel's shared-memory staging.
+bool nb_fused_prune(const NbCtx &c);
+#define NB_FUSED_PRUNE_GROUPS 4096
+#define NB_FUSED_STAGE_MAX (160 * 1024)
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);
 // The correction over a given list of pairs (i < j), forces only.
 void nb_excluded_list_run(NbCtx &c, const double box[3], const int32_t *pairs, int64_t npairs,

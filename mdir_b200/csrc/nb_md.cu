@@ -693,8 +693,15 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
   }
   // the pruning that the last update asked for, beside the PME chain (it
   // needs only the frames, and the pair kernel after it needs its lists)
-  md_prune_step(m, x, box, s);
-  nb_pairs_run(c, box, false, s, flag + 3);
+  if (nb_fused_prune(c) && md_unit_counter(m)) {
+    // a pruning step prunes and computes its pairs in one kernel (MDIR
+    // D284); the pair kernel after it then returns at once
+    nb_prune_pairs_run(c, box, m.flag + 1, x, m.x_prune, m.thermo + 5, md_unit_counter(m), s, flag + 3);
+    nb_pairs_run(c, box, false, s, flag + 3, m.flag + 1);
+  } else {
+    md_prune_step(m, x, box, s);
+    nb_pairs_run(c, box, false, s, flag + 3);
+  }
   if (m.n_excl_other > 0) nb_excluded_list_run(c, box, m.excl_other, m.n_excl_other, s);
   if (pme) {
     cudaEventRecord(m.ev_join, m.side);
@@ -1128,7 +1135,7 @@ static int32_t md_prepare_graph(mdrtMd *m, double *x, double *v, const double bo
   NbCtx &c = *m->nb;
   int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap + (int64_t)(c.inner_reach * 1e9) +
                 (c.inner_valid ? 1 : 0) + (c.deterministic ? 2 : 0) + ((int64_t)c.pair_blocks_per_sm << 40) +
-                ((int64_t)c.pair_sms << 44) + (int64_t)(uintptr_t)m->qgrid;
+                ((int64_t)c.pair_sms << 44) + (int64_t)(uintptr_t)m->qgrid + ((int64_t)nb_fused_prune(c) << 56);
   bool stale = !m->exec || m->gx != x || m->gv != v || m->gdt != dt || m->gunroll != unroll ||
                m->gbox[0] != box[0] || m->gbox[1] != box[1] || m->gbox[2] != box[2] || m->gcap_key != key;
   if (stale) {

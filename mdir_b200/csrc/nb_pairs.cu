@@ -29,6 +29,7 @@
 #include <cstdio>
 
 #include "nb_context.h"
+#include "nb_prune.cuh"
 
 #define NB_MAX_TYPES 32
 
@@ -136,6 +137,215 @@ __device__ __forceinline__ void nb_red_fixed(unsigned long long *addr, float x, 
   atomicAdd(addr + 2, (unsigned long long)__float2ll_rn(z * 4294967296.0f));
 }
 
+// One unit of a list (group g = uo.x, entries 64 uo.y ... 64 uo.y + 63) by
+// one warp: the rounds of 32 entries (dense, or sparse for entries of at
+// most NB_SPARSE_BITS members), the members' and partners' forces, and with
+// ENERGY the unit's energy and virial partials at `unit`.  s_xw, s_fw, s_tw
+// and s_bw are the warp's shared arrays (the 16 members twice; the sparse
+// round's member forces).
+template <bool ENERGY, bool FIXED, int SWITCH, int LJM, bool BATCH>
+__device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64_t unit,
+                                             const float4 *__restrict__ group_L, const int2 *__restrict__ slab,
+                                             const int32_t *__restrict__ counts, const float4 *__restrict__ xq,
+                                             const int32_t *__restrict__ typ, const float2 *__restrict__ ljf,
+                                             const float2 *s_lj, float4 *s_xw, float2 *s_fw, int *s_tw,
+                                             float (*s_bw)[NB_SPARSE_BITS][33], float4 *__restrict__ acc,
+                                             unsigned long long *__restrict__ accf, double *__restrict__ partials,
+                                             int *__restrict__ status) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, u = lane & 15;
+  const int src = (lane & 16) | ((lane + 1) & 15);  // the lane the member accumulators come from
+  int g = uo.x;
+  int64_t pi = (int64_t)g * NB_GROUP + u;
+  // both rounds' entries, in flight with the members' loads (a group's
+  // slab holds a whole number of units, so both reads stay in it; the
+  // lanes past the list's end drop theirs below); the energy forms read
+  // each round's when they come to it
+  const int2 *row = slab + (int64_t)g * P.list_cap + (int64_t)uo.y * NB_UNIT;
+  int2 pre0 = make_int2(0, 0), pre1 = make_int2(0, 0);
+  if (!ENERGY) {
+    pre0 = row[lane];
+    pre1 = row[32 + lane];
+  }
+  __syncwarp();
+  {
+    float4 xi = xq[pi];
+    xi.w *= P.coulomb;
+    int ti = typ[pi];
+    s_xw[lane] = xi;
+    if (LJM == 1) {  // the member's factors times 6 and 12: the force's factors
+      float2 f = ljf[ti];
+      s_fw[lane] = make_float2(6.f * f.x, 12.f * f.y);
+    } else
+      s_tw[lane] = ti * P.ntypes;
+  }
+  __syncwarp();
+  int cnt = (int)min((int64_t)counts[g], P.list_cap);
+  int e0 = uo.y * NB_UNIT;
+  int ne = min(NB_UNIT, cnt - e0);
+  float Lx = P.Lx, Ly = P.Ly, Lz = P.Lz;
+  if (BATCH) {  // the cell of the group's frame
+    float4 Lg = group_L[g];
+    Lx = Lg.x;
+    Ly = Lg.y;
+    Lz = Lg.z;
+  }
+  float ax = 0.f, ay = 0.f, az = 0.f;  // the accumulator of member (lane + k) mod 16
+  float elj = 0.f, ecl = 0.f;
+  float vxx = 0.f, vyy = 0.f, vzz = 0.f, vxy = 0.f, vxz = 0.f, vyz = 0.f;
+  for (int r = 0; r < 2; ++r) {
+    if (r * 32 >= ne) break;
+    bool valid = r * 32 + lane < ne;
+    int2 en = valid ? (ENERGY ? row[r * 32 + lane] : (r == 0 ? pre0 : pre1)) : make_int2(0, 0);
+    int q = en.x;
+    unsigned mask = valid ? ((unsigned)en.y & 0xffffu) : 0u;
+    int code = ((unsigned)en.y >> 16) & NB_IMAGE_BITS;
+    int sx, sy, sz;
+    nb_decode_image(code, sx, sy, sz);
+    float4 xj = xq[q];
+    {
+      NbCell H;
+      H.ax = Lx;
+      H.by = Ly;
+      H.cz = Lz;
+      H.bx = P.bx;
+      H.cx = P.cx;
+      H.cy = P.cy;
+      float3 t = nb_lattice_shift(sx, sy, sz, H);
+      xj.x += t.x;
+      xj.y += t.y;
+      xj.z += t.z;
+    }
+    int tj = typ[q];
+    float2 fj = LJM == 1 ? ljf[tj] : make_float2(0.f, 0.f);
+    float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+    // One pair of this lane's entry with the member at slot m: its force
+    // (dropped outside), the partner's share and the energies.
+    auto pair = [&](int m, bool masked_in, float &fx, float &fy, float &fz) {
+      float4 xm = s_xw[m];
+      float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
+      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      bool inside = masked_in && (r2 < P.rc2);
+      float2 cc;  // (6 c6, 12 c12)
+      if (LJM == 1) {
+        float2 fm = s_fw[m];
+        cc = make_float2(fm.x * fj.x, fm.y * fj.y);
+      } else {
+        cc = s_lj[s_tw[m] + tj];
+      }
+      float qq = xm.w * xj.w;
+      float fs, ulj, uc;
+      nb_pair_terms<ENERGY, SWITCH>(P, r2, cc, qq, fs, ulj, uc);
+      fs = inside ? fs : 0.f;
+      fx = fs * dx;
+      fy = fs * dy;
+      fz = fs * dz;
+      fjx -= fx;
+      fjy -= fy;
+      fjz -= fz;
+      if (ENERGY) {
+        elj += inside ? ulj : 0.f;
+        ecl += inside ? uc : 0.f;
+        vxx = fmaf(dx, fx, vxx);
+        vyy = fmaf(dy, fy, vyy);
+        vzz = fmaf(dz, fz, vzz);
+        vxy = fmaf(dx, fy, vxy);
+        vxz = fmaf(dx, fz, vxz);
+        vyz = fmaf(dy, fz, vyz);
+      }
+    };
+    if (__all_sync(FULL, __popc(mask) <= NB_SPARSE_BITS)) {
+      // A sparse round (the pruned lists put such entries last): each lane
+      // visits only its own members, as many as the fullest entry of the
+      // round has.  Its i-th member's force goes to s_b[.][i][lane]; then
+      // lanes u and u + 16 add member u's forces over the lanes of their
+      // half, in lane order.
+      int steps = (int)__reduce_max_sync(FULL, (unsigned)__popc(mask));
+      unsigned mm = mask;
+      // the next member of this lane's entry, or a dropped pair with
+      // member 0 once none is left (a lane with fewer members idles so)
+      auto visit = [&](int i) {
+        bool has = mm != 0u;
+        int m = has ? __ffs(mm) - 1 : 0;
+        mm &= mm - 1;
+        float fx, fy, fz;
+        pair(m, has, fx, fy, fz);
+        if (has) {
+          s_bw[0][i][lane] = fx;
+          s_bw[1][i][lane] = fy;
+          s_bw[2][i][lane] = fz;
+        }
+      };
+      // two members a step, branch-free, so that their chains interleave
+      int i = 0;
+      for (; i + 1 < steps; i += 2) {
+        visit(i);
+        visit(i + 1);
+      }
+      if (i < steps) visit(i);
+      __syncwarp();
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+      const unsigned below = (1u << u) - 1u;
+#pragma unroll 4
+      for (int j = 0; j < 16; ++j) {
+        int lp = (lane & 16) | j;
+        unsigned mk = __shfl_sync(FULL, mask, lp);
+        if ((mk >> u) & 1u) {
+          int i = __popc(mk & below);
+          sx += s_bw[0][i][lp];
+          sy += s_bw[1][i][lp];
+          sz += s_bw[2][i][lp];
+        }
+      }
+      __syncwarp();  // the next round writes s_b again
+      ax += sx;
+      ay += sy;
+      az += sz;
+    } else {
+      // bit k of mrot: the pair of this lane's entry with member (lane + k) mod 16
+      unsigned mrot = ((mask >> u) | (mask << (16 - u))) & 0xffffu;
+#pragma unroll
+      for (int k = 0; k < NB_GROUP; ++k) {
+        float fx, fy, fz;
+        pair(u + k, (mrot & (1u << k)) != 0u, fx, fy, fz);
+        ax += fx;
+        ay += fy;
+        az += fz;
+        ax = __shfl_sync(FULL, ax, src);
+        ay = __shfl_sync(FULL, ay, src);
+        az = __shfl_sync(FULL, az, src);
+      }
+    }
+    if (valid && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
+      if (FIXED)
+        nb_red_fixed(accf + 3 * (int64_t)q, fjx, fjy, fjz, status);
+      else
+        nb_red_add_v4(acc + q, fjx, fjy, fjz);
+    }
+  }
+  ax += __shfl_xor_sync(FULL, ax, 16);
+  ay += __shfl_xor_sync(FULL, ay, 16);
+  az += __shfl_xor_sync(FULL, az, 16);
+  if (lane < 16 && (ax != 0.f || ay != 0.f || az != 0.f)) {
+    if (FIXED)
+      nb_red_fixed(accf + 3 * pi, ax, ay, az, status);
+    else
+      nb_red_add_v4(acc + pi, ax, ay, az);
+  }
+  if (ENERGY) {
+    double v[8] = {elj, ecl, vxx, vyy, vzz, vxy, vxz, vyz};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(FULL, v[k], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) partials[(int64_t)unit * 8 + k] = v[k];
+    }
+  }
+}
+
 // LJM selects the Lennard-Jones coefficients: 0, a (c6, c12) table by type
 // pair in shared memory; 1, the product of per-type factors (sqrt c6,
 // sqrt c12), exact when the table factorizes (one LJ type, or geometric
@@ -154,15 +364,15 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
                                                 const float2 *__restrict__ lj, const float2 *__restrict__ ljf,
                                                 float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
                                                 double *__restrict__ partials, int *__restrict__ status,
-                                                const int *halt) {
+                                                const int *halt, const int *skip) {
   nb_grid_wait();  // the lists and frames of the kernels before (a chained launch)
   if (halt && *halt) return;  // the MD step stopped at a stale list (its host rebuilds)
+  if (skip && *skip) return;  // a pruning step: the pruning kernel computed the pairs
   __shared__ float4 s_x[8][2 * NB_GROUP];
   __shared__ float2 s_f[8][2 * NB_GROUP];  // LJM 1: member factors
   __shared__ int s_t[8][2 * NB_GROUP];     // LJM 0: member row offsets in s_lj
   __shared__ float2 s_lj[LJM == 0 ? NB_MAX_TYPES * NB_MAX_TYPES : 1];
   __shared__ float s_b[8][3][NB_SPARSE_BITS][33];  // member forces of a sparse round (33: no bank conflicts)
-  const unsigned FULL = 0xffffffffu;
   if (LJM == 0) {  // (6 c6, 12 c12): the force's factors
     int nt2 = P.ntypes * P.ntypes;
     for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
@@ -171,9 +381,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
     }
     __syncthreads();
   }
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int u = lane & 15;
-  const int src = (lane & 16) | ((lane + 1) & 15);  // the lane the member accumulators come from
+  int warp = threadIdx.x >> 5;
   int nunits = min((int64_t)sizes[NB_SIZE_UNITS], P.units_cap);
   int wstride = gridDim.x * 8;
   // the next unit's header is in flight during this unit (the energy forms,
@@ -183,196 +391,57 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   for (; unit < nunits; unit += wstride) {
     int2 uo = ENERGY ? units[unit] : uo_next;
     if (!ENERGY && unit + wstride < nunits) uo_next = units[unit + wstride];
-    int g = uo.x;
-    int64_t pi = (int64_t)g * NB_GROUP + u;
-    // both rounds' entries, in flight with the members' loads (a group's
-    // slab holds a whole number of units, so both reads stay in it; the
-    // lanes past the list's end drop theirs below); the energy forms read
-    // each round's when they come to it
-    const int2 *row = slab + (int64_t)g * P.list_cap + (int64_t)uo.y * NB_UNIT;
-    int2 pre0 = make_int2(0, 0), pre1 = make_int2(0, 0);
-    if (!ENERGY) {
-      pre0 = row[lane];
-      pre1 = row[32 + lane];
-    }
-    __syncwarp();
-    {
-      float4 xi = xq[pi];
-      xi.w *= P.coulomb;
-      int ti = typ[pi];
-      s_x[warp][lane] = xi;
-      if (LJM == 1) {  // the member's factors times 6 and 12: the force's factors
-        float2 f = ljf[ti];
-        s_f[warp][lane] = make_float2(6.f * f.x, 12.f * f.y);
-      } else
-        s_t[warp][lane] = ti * P.ntypes;
-    }
-    __syncwarp();
-    int cnt = (int)min((int64_t)counts[g], P.list_cap);
-    int e0 = uo.y * NB_UNIT;
-    int ne = min(NB_UNIT, cnt - e0);
-    float Lx = P.Lx, Ly = P.Ly, Lz = P.Lz;
-    if (BATCH) {  // the cell of the group's frame
-      float4 Lg = group_L[g];
-      Lx = Lg.x;
-      Ly = Lg.y;
-      Lz = Lg.z;
-    }
-    float ax = 0.f, ay = 0.f, az = 0.f;  // the accumulator of member (lane + k) mod 16
-    float elj = 0.f, ecl = 0.f;
-    float vxx = 0.f, vyy = 0.f, vzz = 0.f, vxy = 0.f, vxz = 0.f, vyz = 0.f;
-    for (int r = 0; r < 2; ++r) {
-      if (r * 32 >= ne) break;
-      bool valid = r * 32 + lane < ne;
-      int2 en = valid ? (ENERGY ? row[r * 32 + lane] : (r == 0 ? pre0 : pre1)) : make_int2(0, 0);
-      int q = en.x;
-      unsigned mask = valid ? ((unsigned)en.y & 0xffffu) : 0u;
-      int code = ((unsigned)en.y >> 16) & NB_IMAGE_BITS;
-      int sx, sy, sz;
-      nb_decode_image(code, sx, sy, sz);
-      float4 xj = xq[q];
-      {
-        NbCell H;
-        H.ax = Lx;
-        H.by = Ly;
-        H.cz = Lz;
-        H.bx = P.bx;
-        H.cx = P.cx;
-        H.cy = P.cy;
-        float3 t = nb_lattice_shift(sx, sy, sz, H);
-        xj.x += t.x;
-        xj.y += t.y;
-        xj.z += t.z;
-      }
-      int tj = typ[q];
-      float2 fj = LJM == 1 ? ljf[tj] : make_float2(0.f, 0.f);
-      float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-      // One pair of this lane's entry with the member at slot m: its force
-      // (dropped outside), the partner's share and the energies.
-      auto pair = [&](int m, bool masked_in, float &fx, float &fy, float &fz) {
-        float4 xm = s_x[warp][m];
-        float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
-        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        bool inside = masked_in && (r2 < P.rc2);
-        float2 cc;  // (6 c6, 12 c12)
-        if (LJM == 1) {
-          float2 fm = s_f[warp][m];
-          cc = make_float2(fm.x * fj.x, fm.y * fj.y);
-        } else {
-          cc = s_lj[s_t[warp][m] + tj];
-        }
-        float qq = xm.w * xj.w;
-        float fs, ulj, uc;
-        nb_pair_terms<ENERGY, SWITCH>(P, r2, cc, qq, fs, ulj, uc);
-        fs = inside ? fs : 0.f;
-        fx = fs * dx;
-        fy = fs * dy;
-        fz = fs * dz;
-        fjx -= fx;
-        fjy -= fy;
-        fjz -= fz;
-        if (ENERGY) {
-          elj += inside ? ulj : 0.f;
-          ecl += inside ? uc : 0.f;
-          vxx = fmaf(dx, fx, vxx);
-          vyy = fmaf(dy, fy, vyy);
-          vzz = fmaf(dz, fz, vzz);
-          vxy = fmaf(dx, fy, vxy);
-          vxz = fmaf(dx, fz, vxz);
-          vyz = fmaf(dy, fz, vyz);
-        }
-      };
-      if (__all_sync(FULL, __popc(mask) <= NB_SPARSE_BITS)) {
-        // A sparse round (the pruned lists put such entries last): each lane
-        // visits only its own members, as many as the fullest entry of the
-        // round has.  Its i-th member's force goes to s_b[.][i][lane]; then
-        // lanes u and u + 16 add member u's forces over the lanes of their
-        // half, in lane order.
-        int steps = (int)__reduce_max_sync(FULL, (unsigned)__popc(mask));
-        unsigned mm = mask;
-        // the next member of this lane's entry, or a dropped pair with
-        // member 0 once none is left (a lane with fewer members idles so)
-        auto visit = [&](int i) {
-          bool has = mm != 0u;
-          int m = has ? __ffs(mm) - 1 : 0;
-          mm &= mm - 1;
-          float fx, fy, fz;
-          pair(m, has, fx, fy, fz);
-          if (has) {
-            s_b[warp][0][i][lane] = fx;
-            s_b[warp][1][i][lane] = fy;
-            s_b[warp][2][i][lane] = fz;
-          }
-        };
-        // two members a step, branch-free, so that their chains interleave
-        int i = 0;
-        for (; i + 1 < steps; i += 2) {
-          visit(i);
-          visit(i + 1);
-        }
-        if (i < steps) visit(i);
-        __syncwarp();
-        float sx = 0.f, sy = 0.f, sz = 0.f;
-        const unsigned below = (1u << u) - 1u;
-#pragma unroll 4
-        for (int j = 0; j < 16; ++j) {
-          int lp = (lane & 16) | j;
-          unsigned mk = __shfl_sync(FULL, mask, lp);
-          if ((mk >> u) & 1u) {
-            int i = __popc(mk & below);
-            sx += s_b[warp][0][i][lp];
-            sy += s_b[warp][1][i][lp];
-            sz += s_b[warp][2][i][lp];
-          }
-        }
-        __syncwarp();  // the next round writes s_b again
-        ax += sx;
-        ay += sy;
-        az += sz;
-      } else {
-        // bit k of mrot: the pair of this lane's entry with member (lane + k) mod 16
-        unsigned mrot = ((mask >> u) | (mask << (16 - u))) & 0xffffu;
-#pragma unroll
-        for (int k = 0; k < NB_GROUP; ++k) {
-          float fx, fy, fz;
-          pair(u + k, (mrot & (1u << k)) != 0u, fx, fy, fz);
-          ax += fx;
-          ay += fy;
-          az += fz;
-          ax = __shfl_sync(FULL, ax, src);
-          ay = __shfl_sync(FULL, ay, src);
-          az = __shfl_sync(FULL, az, src);
-        }
-      }
-      if (valid && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
-        if (FIXED)
-          nb_red_fixed(accf + 3 * (int64_t)q, fjx, fjy, fjz, status);
-        else
-          nb_red_add_v4(acc + q, fjx, fjy, fjz);
-      }
-    }
-    ax += __shfl_xor_sync(FULL, ax, 16);
-    ay += __shfl_xor_sync(FULL, ay, 16);
-    az += __shfl_xor_sync(FULL, az, 16);
-    if (lane < 16 && (ax != 0.f || ay != 0.f || az != 0.f)) {
-      if (FIXED)
-        nb_red_fixed(accf + 3 * pi, ax, ay, az, status);
-      else
-        nb_red_add_v4(acc + pi, ax, ay, az);
-    }
-    if (ENERGY) {
-      double v[8] = {elj, ecl, vxx, vyy, vzz, vxy, vxz, vyz};
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(FULL, v[k], o);
-      }
-      if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) partials[(int64_t)unit * 8 + k] = v[k];
-      }
+    nb_pair_unit<ENERGY, FIXED, SWITCH, LJM, BATCH>(P, uo, unit, group_L, slab, counts, xq, typ, ljf, s_lj,
+                                                    s_x[warp], s_f[warp], s_t[warp], s_b[warp], acc, accf,
+                                                    partials, status);
+  }
+}
+
+// The pruning step of the dual list with its pairs in one kernel (MDIR
+// D284: the loop over pairs that first takes a pruning prunes for it): a
+// block of NB_PRUNE_WARPS warps a group prunes the group's outer list at the
+// step's frames exactly as the pruning kernel does (nb_prune_group: the same
+// inner list, counts and claimed units, and the positions of the pruning),
+// then its warps evaluate the units of that fresh inner list at once, while
+// other blocks are still pruning.  Forces only, outside the deterministic
+// mode (the claimed units come in block order); nothing unless *gate is set
+// (the update before asked for a pruning) and the step goes on.
+template <int SWITCH, int LJM>
+__global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
+    nb_prune_pairs(PairParams P, int64_t groups_cap, const int32_t *__restrict__ sizes, NbCell H, float rin2,
+                   const int2 *__restrict__ slab, const int32_t *__restrict__ counts,
+                   const int32_t *__restrict__ order, const float4 *__restrict__ xq,
+                   const int32_t *__restrict__ typ, const float2 *__restrict__ lj, const float2 *__restrict__ ljf,
+                   int2 *__restrict__ slab_in, int32_t *__restrict__ counts_in, const int *gate,
+                   const double *__restrict__ x, double *__restrict__ x_prune, int32_t *unit_counter,
+                   int2 *__restrict__ units, double *prunes, float4 *__restrict__ acc, int *__restrict__ status,
+                   const int *halt) {
+  __shared__ float4 s_x[NB_PRUNE_WARPS][2 * NB_GROUP];
+  __shared__ float2 s_f[NB_PRUNE_WARPS][2 * NB_GROUP];
+  __shared__ int s_t[NB_PRUNE_WARPS][2 * NB_GROUP];
+  __shared__ float2 s_lj[LJM == 0 ? NB_MAX_TYPES * NB_MAX_TYPES : 1];
+  __shared__ float s_b[NB_PRUNE_WARPS][3][NB_SPARSE_BITS][33];
+  int64_t g = blockIdx.x;
+  nb_grid_wait();  // the gate and the frames of the kernels before (a chained launch)
+  if (halt && *halt) return;
+  if (*gate == 0) return;  // no pruning due: the pair kernel after this one does the pairs
+  if (g >= groups_cap || g >= sizes[NB_SIZE_GROUPS]) return;
+  if (LJM == 0) {
+    int nt2 = P.ntypes * P.ntypes;
+    for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
+      float2 c = lj[k];
+      s_lj[k] = make_float2(6.f * c.x, 12.f * c.y);
     }
   }
+  int total = nb_prune_group(g, H, rin2, P.list_cap, slab, counts, order, xq, slab_in, counts_in, x, x_prune,
+                             unit_counter, units, P.units_cap, prunes);
+  __syncthreads();  // the block's inner list and its count, written to global memory, and s_lj
+  int warp = threadIdx.x >> 5;
+  int nu = (total + NB_UNIT - 1) / NB_UNIT;
+  for (int o = warp; o < nu; o += NB_PRUNE_WARPS)
+    nb_pair_unit<false, false, SWITCH, LJM, false>(P, make_int2((int)g, o), 0, nullptr, slab_in, counts_in, xq, typ,
+                                                   ljf, s_lj, s_x[warp], s_f[warp], s_t[warp], s_b[warp], acc,
+                                                   nullptr, nullptr, status);
 }
 
 // Frames: xq[p] = ((float)(x_a + (S_p - 1/2) L), q_a) for the atom a at place p;
@@ -944,7 +1013,52 @@ void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream
                                                           c.tilt[1], c.tilt[2], c.xq, c.typ_p);
 }
 
-void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt) {
+bool nb_fused_prune(const NbCtx &c) {
+  if (c.deterministic || !(c.inner_reach > 0.0) || sizeof(int2) * (size_t)c.list_cap > NB_FUSED_STAGE_MAX)
+    return false;
+  if (c.fused_prune == 1) return true;
+  if (c.fused_prune == 2) return false;
+  return c.h_sizes && c.h_sizes[NB_SIZE_GROUPS] >= NB_FUSED_PRUNE_GROUPS;
+}
+
+void nb_prune_pairs_run(NbCtx &c, const double box[3], const int *gate, const double *x, double *x_prune,
+                        double *prunes, int32_t *unit_counter, cudaStream_t s, const int *halt) {
+  PairParams P = pair_params(c, box);
+  double Rw = c.inner_reach + 3e-6 * (box[0] + box[1] + box[2] + fabs(c.tilt[0]) + fabs(c.tilt[1]) + fabs(c.tilt[2]));
+  size_t stage = sizeof(int2) * (size_t)c.list_cap;
+  NbCell H = nb_cell(c, box);
+#define NB_FUSED_LAUNCH(S, M)                                                                                    \
+  do {                                                                                                          \
+    static size_t configured[64] = {};                                                                          \
+    int dev = 0;                                                                                                \
+    cudaGetDevice(&dev);                                                                                        \
+    if (dev >= 0 && dev < 64 && configured[dev] < stage) {                                                       \
+      cudaFuncSetAttribute(nb_prune_pairs<S, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);      \
+      configured[dev] = stage;                                                                                  \
+    }                                                                                                           \
+    nb_launch_chained(nb_prune_pairs<S, M>, dim3((int)c.groups_cap), dim3(NB_PRUNE_WARPS * 32), stage, s, P,     \
+                      c.groups_cap, c.sizes, H, (float)(Rw * Rw), c.slab, c.counts, c.order, c.xq, c.typ_p,    \
+                      c.lj, c.ljf, c.slab_in, c.counts_in, gate, x, x_prune, unit_counter, c.units_in, prunes,   \
+                      c.acc, c.status, halt);                                                                   \
+  } while (0)
+#define NB_FUSED_M(S)           \
+  do {                          \
+    if (c.lj_geom)              \
+      NB_FUSED_LAUNCH(S, 1);    \
+    else                        \
+      NB_FUSED_LAUNCH(S, 0);    \
+  } while (0)
+  if (c.lj_switch == 2)
+    NB_FUSED_M(2);
+  else if (c.lj_switch == 1)
+    NB_FUSED_M(1);
+  else
+    NB_FUSED_M(0);
+#undef NB_FUSED_M
+#undef NB_FUSED_LAUNCH
+}
+
+void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt, const int *skip) {
   ensure_sm_count();
   PairParams P = pair_params(c, box);
   // persistent grid: enough warps for the units, `pair_blocks_per_sm`
@@ -963,7 +1077,7 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, co
 #define NB_LAUNCH2(E, F, S, M)                                                                            \
   nb_launch_chained(nb_pairs<E, F, S, M>, dim3(grid), dim3(256), 0, s, P, (const float4 *)nullptr, lsizes,  \
                     lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed, c.unit_partials, \
-                    c.status, halt)
+                    c.status, halt, skip)
 #define NB_LAUNCH(E, F, S)      \
   do {                          \
     if (c.lj_geom)              \
@@ -1118,7 +1232,7 @@ void nb_batch_pairs_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
 #define NB_BATCH_LAUNCH(E, M)                                                                                \
   nb_pairs<E, false, 0, M, true><<<grid, 256, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq, \
                                                          c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed, c.unit_partials, \
-                                                         c.status, nullptr)
+                                                         c.status, nullptr, nullptr)
   if (energy) {
     if (c.lj_geom) NB_BATCH_LAUNCH(true, 1); else NB_BATCH_LAUNCH(true, 0);
   } else {

@@ -79,11 +79,12 @@ class Integrator:
         return p.value
 
     def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(1.025, 1.05),
-             pair_sms=(0, 112, 120, 128, 136), pair_blocks=(4, 3), steps=400, reps=3, stream=None):
-        """The autotuner of the step, in two stages: the outer and pruned
+             pair_sms=(0, 112, 120, 128, 136), pair_blocks=(4, 3), fused=(2, 1), steps=400, reps=3, stream=None):
+        """The autotuner of the step, in three stages: the outer and pruned
         reaches first (the launch shapes as set), then the span of the pair
         grid (SMs; the others are left to the PME kernels beside it) and its
-        blocks per SM at the reaches kept.  Each choice is timed as `reps`
+        blocks per SM at the reaches kept, then the pruning inside the pair
+        kernel (MDIR D284) or in a launch of its own.  Each choice is timed as `reps`
         runs of `steps` steps after a build and half as many untimed steps;
         the fastest is kept and built for.  x and v are put back; the step
         counter and the thermostat's noise move on.  MDIR searches its
@@ -117,6 +118,7 @@ class Integrator:
 
         sms0 = getattr(t, "pair_sms", 0)
         blocks0 = getattr(t, "pair_blocks_per_sm", 4)
+        fused0 = getattr(t, "fused_prune", 0)
         trials = []
         for R in reaches:
             if not R < 0.999 * least:
@@ -130,6 +132,18 @@ class Integrator:
                 if (sms, blocks) != (sms0, blocks0):
                     trials.append((trial(R, Rin, sms, blocks), R, Rin, sms, blocks))
         us, R, Rin, sms, blocks = min(t_ for t_ in trials if t_[1] == R and t_[2] == Rin)
+        # the pruning in the pair kernel (MDIR D284) or in a launch of its
+        # own, at the shape kept
+        fused_trials = []
+        for f in fused:
+            t.set_tuning(fused_prune=f)
+            fused_trials.append((trial(R, Rin, sms, blocks), f))
+        fus, fchoice = min(fused_trials)
+        if fus < us:
+            us = fus
+        else:
+            fchoice = fused0
+        t.set_tuning(fused_prune=fchoice)
         t.set_reach(R)
         t.set_pruned_reach(Rin)
         t.set_tuning(pair_sms=sms, pair_blocks_per_sm=blocks)
@@ -137,7 +151,7 @@ class Integrator:
         v.copy_(keep_v)
         self.build(x, box, stream=st)
         return {"reach": R, "pruned_reach": Rin, "pair_sms": sms, "pair_blocks_per_sm": blocks,
-                "us_per_step": round(us, 2), "trials": len(trials)}
+                "fused_prune": fchoice, "us_per_step": round(us, 2), "trials": len(trials) + len(fused_trials)}
 
     def temperature(self, stream=None):
         t = self.thermo(stream)

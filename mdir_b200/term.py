@@ -61,6 +61,7 @@ class NonbondedTerm:
         self.pruned = 0.0
         self.pair_sms = 0
         self.pair_blocks_per_sm = 4
+        self.fused_prune = 0
 
     def close(self):
         if getattr(self, "_h", None):
@@ -118,8 +119,10 @@ class NonbondedTerm:
         b = _host(self.box if box is None else box, np.float64)
         L.check(L.lib().mdrtNbPrune(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtNbPrune")
 
-    def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None):
-        """Launch shapes (the autotuner's knobs); results do not depend on them."""
+    def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None, fused_prune=None):
+        """Launch shapes and the MD step's pruning in the pair kernel (0 by
+        group count, 1 always, 2 never): the autotuner's knobs; results do
+        not depend on them beyond the order of f32 sums."""
         if pair_blocks_per_sm is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_BLOCKS_PER_SM, int(pair_blocks_per_sm)),
                     "mdrtNbSetTuning")
@@ -127,6 +130,9 @@ class NonbondedTerm:
         if pair_sms is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_SMS, int(pair_sms)), "mdrtNbSetTuning")
             self.pair_sms = int(pair_sms)
+        if fused_prune is not None:
+            L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_FUSED_PRUNE, int(fused_prune)), "mdrtNbSetTuning")
+            self.fused_prune = int(fused_prune)
 
     def set_deterministic(self, on=True):
         L.check(L.lib().mdrtNbSetDeterministic(self._h, int(bool(on))), "mdrtNbSetDeterministic")
@@ -151,15 +157,16 @@ class NonbondedTerm:
         return sizes
 
     def force(self, x, box=None, energy=False, potential=False, forces=None, accumulate=False,
-              pairs=True, pme=True, excluded=True, stream=None):
-        """Forces (device f64 (n, 3)) of the term at x."""
+              pairs=True, pme=True, excluded=True, prune=False, stream=None):
+        """Forces (device f64 (n, 3)) of the term at x; `prune` prunes the
+        dual list at x first (in the pair kernel itself for forces alone)."""
         self._check_x(x)
         b = _host(self.box if box is None else box, np.float64)
         if forces is None:
             forces = torch.empty((self.n, 3), dtype=torch.float64, device=x.device)
         flags = (L.ENERGY if energy else 0) | (L.POTENTIAL if potential else 0) | \
             (L.ACCUMULATE if accumulate else 0) | (0 if pairs else L.NO_PAIRS) | \
-            (0 if pme else L.NO_PME) | (0 if excluded else L.NO_EXCLUDED)
+            (0 if pme else L.NO_PME) | (0 if excluded else L.NO_EXCLUDED) | (L.PRUNE if prune else 0)
         entry = L.lib().mdrtNbForceTriclinic if len(b) == 6 else L.lib().mdrtNbForce
         L.check(entry(self._h, _dp(x), _hp(b), flags, _dp(forces), _stream(stream)), "mdrtNbForce")
         return forces

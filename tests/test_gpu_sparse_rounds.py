@@ -110,3 +110,80 @@ def test_pruned_lists_are_the_host_restatement(cuda, case):
             np.testing.assert_array_equal(got, ref[g])
         x = x + rng.normal(0.0, 0.01, size=x.shape)  # within half the skin of the build
     t.close()
+
+
+def test_pruning_in_the_pair_kernel_is_the_pruning_then_the_pairs(cuda):
+    """MDRT_NB_PRUNE on a force call: the pruning and the pairs of the fresh
+    inner lists in one kernel (MDIR D284) leave the inner lists of the
+    pruning kernel bit for bit, and the forces of pruning then pairing."""
+    from mdir_b200 import _lib as L
+    s = systems.tip3p(waters=1500, seed=17)
+    box = list(s["box"])
+    x0 = np.asarray(s["positions"])
+    x1 = x0 + np.random.default_rng(6).normal(0.0, 0.01, size=x0.shape)
+
+    def term():
+        t = NonbondedTerm(len(s["charges"]))
+        t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+        t.set_exclusions(pairs=s["excluded_pairs"])
+        t.set_interaction(s["cutoff"], 1.3, s["beta"])
+        t.set_pruned_reach(1.0)
+        t.set_pme(s["grid"], s["order"])
+        sizes = t.build(torch.tensor(x0, device=cuda), box)
+        return t, int(sizes[L.SIZE_GROUPS])
+
+    (a, G), (b, _) = term(), term()
+    for x in (x0, x1):
+        xd = torch.tensor(x, device=cuda)
+        a.prune(xd, box)
+        fa = a.force(xd).cpu().numpy()
+        fb = b.force(xd, prune=True).cpu().numpy()
+        ca = a.buffer(L.SLOT_INNER_COUNTS, np.int32)[:G]
+        cb = b.buffer(L.SLOT_INNER_COUNTS, np.int32)[:G]
+        np.testing.assert_array_equal(ca, cb)
+        cap = a.info()["list_capacity"]
+        ea = a.buffer(L.SLOT_INNER_ENTRIES, np.int32, 2)
+        eb = b.buffer(L.SLOT_INNER_ENTRIES, np.int32, 2)
+        for g in range(G):
+            np.testing.assert_array_equal(ea[g * cap: g * cap + ca[g]], eb[g * cap: g * cap + cb[g]])
+        err = np.sqrt(np.mean(np.sum((fb - fa) ** 2, 1)) / np.mean(np.sum(fa ** 2, 1)))
+        assert err < 1e-6, err
+        ref = O.evaluate(s, x)["forces"]
+        assert np.sqrt(np.mean(np.sum((fb - ref) ** 2, 1)) / np.mean(np.sum(ref ** 2, 1))) < 1e-5
+        # the next force call without a pruning reads the inner lists and units the kernel left
+        fc = b.force(xd).cpu().numpy()
+        assert np.sqrt(np.mean(np.sum((fc - fa) ** 2, 1)) / np.mean(np.sum(fa ** 2, 1))) < 1e-6
+    a.close()
+    b.close()
+
+
+def test_md_step_with_the_pruning_in_the_pair_kernel(cuda):
+    """The MD step with its prunings inside the pair kernel (tuning
+    fused_prune 1) follows the step with a pruning launch of its own (2):
+    the same prunings and rebuilds, and positions that part no faster than
+    two runs of the step with its own pruning launch part from each other
+    (f32 sums in the order the atomics land, amplified by the dynamics)."""
+    from mdir_b200.md import Integrator
+    s = systems.tip3p(waters=1500, seed=19)
+    out = []
+    for fused in (2, 2, 1):
+        t = NonbondedTerm(len(s["charges"]))
+        t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+        t.set_exclusions(pairs=s["excluded_pairs"])
+        t.set_interaction(s["cutoff"], 1.3, s["beta"])
+        t.set_pruned_reach(0.95)
+        t.set_pme(s["grid"], s["order"])
+        t.set_tuning(fused_prune=fused)
+        md = Integrator(t, s["masses"], s["waters"])
+        md.thermostat(300.0, 0.0, 1)
+        x = torch.tensor(s["positions"], device=cuda)
+        v = torch.tensor(systems.maxwell_velocities(s, 300.0, seed=2), device=cuda)
+        md.build(x, s["box"])
+        md.run(x, v, s["box"], 0.002, 60, unroll=10)
+        th = md.thermo()
+        out.append((x.cpu().numpy(), th["prunes"], th["builds"]))
+        assert t.status() == 0
+    (xa, pa, ba), (xc, pc, bc), (xb, pb, bb) = out
+    assert pa == pb == pc and pa >= 10 and ba == bb == bc
+    control = np.abs(xa - xc).max()
+    assert np.abs(xa - xb).max() < 1e-4 or np.abs(xa - xb).max() < 10 * control, (np.abs(xa - xb).max(), control)
