@@ -419,7 +419,7 @@ def precision_leg(args, dev, flush, reach=1.6, pruned=1.05, thermalize=1000, nve
                     "total_std_kj_mol": round(float(E[:, 0].std()), 3),
                     "temperature_K": round(2.0 * kin / (md.thermo()["ndof"] * 0.0083144626181532), 1)},
             "force_error": "RMS relative force error vs FP64: 1.09e-5 on this box, 2.7e-6 on the 23,550-atom box "
-                           "(tests/precision_report.py; bounded by tests/test_gpu_precision.py)"}
+                           "(bounded by tests/test_gpu_precision.py and tests/test_gpu_headline.py)"}
 
 
 def run_reference(args):

@@ -78,7 +78,7 @@ class Integrator:
         L.check(L.lib().mdrtMdForces(self._h, ctypes.byref(p)), "mdrtMdForces")
         return p.value
 
-    def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(1.025, 1.05),
+    def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(0.975, 1.0, 1.025, 1.05),
              pair_sms=(0, 112, 120, 128, 136), pair_blocks=(4, 3), fused=(2, 1), steps=400, reps=3, stream=None):
         """The autotuner of the step, in three stages: the outer and pruned
         reaches first (the launch shapes as set), then the span of the pair
