@@ -577,6 +577,7 @@ def main():
     exe.pair_sms = tuned["pair_sms"] if tuned else args.pair_sms
     exe.pair_blocks_per_sm = tuned["pair_blocks_per_sm"] if tuned else args.pair_blocks
     exe.fused_prune = tuned["fused_prune"] if tuned else 0
+    exe.staging_depth = tuned["staging_depth"] if tuned else 1
     sim = mdir.Simulation(mdir.compile(system, st, integ, ens, exe, sch))
 
     def e2e_step():

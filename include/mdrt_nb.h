@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define MDRT_NB_ABI_VERSION 1
+#define MDRT_NB_ABI_VERSION 2
 
 typedef struct mdrtNb mdrtNb;
 
@@ -161,7 +161,10 @@ enum mdrtNbTuneKey {
   /* the MD step's pruning of the dual list in its pair kernel (MDIR D284,
    * lib/Dialect/MDExec/DevicePolicy.cpp:70-99): 0 from 4096 groups on (the
    * default), 1 always, 2 never; never in the deterministic mode */
-  MDRT_NB_TUNE_FUSED_PRUNE = 3
+  MDRT_NB_TUNE_FUSED_PRUNE = 3,
+  /* the pair kernel's staging depth: 1, a unit's entries are read as the
+   * unit starts; 2, the next unit's entries are in flight during a unit */
+  MDRT_NB_TUNE_STAGING_DEPTH = 4
 };
 int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value);
 
@@ -453,9 +456,12 @@ int32_t mdrtNbBatchEnergies(mdrtNbBatch *batch, void *stream, double *out);
  * term (host, f64), in the cells of the last build. */
 int32_t mdrtNbBatchConstants(mdrtNbBatch *batch, double *out);
 /* The project's autotuner: times a build and an evaluation with energies
- * for every search width (4, 1 warps a group) and pair-kernel occupancy
- * (4..1 blocks per SM), keeps the fastest, and writes it to choice[2] =
- * {search warps, pair blocks per SM}.  Needs a build (for the cells);
+ * for every search width (4, 1 warps a group), pair-kernel occupancy (4..1
+ * blocks per SM) and staging depth (1, 2), keeps the fastest, and writes it
+ * to choice[3] = {search warps, pair blocks per SM, staging depth}.  The
+ * members of a group (16, the column places of the build) and the threads
+ * an i-cluster's accumulators rotate over (16, a half-warp) are fixed by
+ * the layout.  Needs a build (for the cells);
  * `forces` is scratch (device f64 [n, 3]).  No MDIR counterpart: MDIR's
  * launch shapes are fixed by its emitters (DevicePolicy.cpp:72-99). */
 int32_t mdrtNbBatchAutotune(mdrtNbBatch *batch, const double *x, double *forces, void *stream,

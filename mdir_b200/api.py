@@ -158,6 +158,7 @@ class Execution:
         self.pair_sms = 0  # SMs the pair kernel spans (0: all); the others are left to PME
         self.pair_blocks_per_sm = 0  # blocks of the pair kernel an SM (0: the library's default, 4)
         self.fused_prune = 0  # the pruning inside the pair kernel: 0 by group count, 1 always, 2 never
+        self.staging_depth = 1  # the pair kernel's staging depth (1 or 2)
 
 
 class Schedule:
@@ -256,6 +257,8 @@ def _make_term(program):
         t.set_tuning(pair_blocks_per_sm=program.execution.pair_blocks_per_sm)
     if getattr(program.execution, "fused_prune", 0):
         t.set_tuning(fused_prune=program.execution.fused_prune)
+    if getattr(program.execution, "staging_depth", 1) != 1:
+        t.set_tuning(staging_depth=program.execution.staging_depth)
     return t
 
 

@@ -118,7 +118,10 @@ class BatchEvaluator:
         self.built = True
         return sizes
 
-    def set_tuning(self, pair_blocks_per_sm=None, search_warps=None):
+    def set_tuning(self, pair_blocks_per_sm=None, search_warps=None, staging_depth=None):
+        if staging_depth is not None:
+            L.check(L.lib().mdrtNbBatchSetTuning(self._h, L.TUNE_STAGING_DEPTH, int(staging_depth)),
+                    "mdrtNbBatchSetTuning")
         if pair_blocks_per_sm is not None:
             L.check(L.lib().mdrtNbBatchSetTuning(self._h, L.TUNE_PAIR_BLOCKS_PER_SM, int(pair_blocks_per_sm)),
                     "mdrtNbBatchSetTuning")
@@ -128,13 +131,16 @@ class BatchEvaluator:
 
     def autotune(self, stream=None):
         """Times every launch shape of the build and the pair kernel on this
-        batch and keeps the fastest: {"search_warps", "pair_blocks_per_sm"}."""
+        batch (search warps a group, pair blocks an SM, staging depth) and
+        keeps the fastest; returns the choice, with the group's members and
+        the threads its accumulators rotate over, which the layout fixes."""
         if not self.built:
             self.build(stream)
-        choice = np.zeros(2, dtype=np.int32)
+        choice = np.zeros(3, dtype=np.int32)
         L.check(L.lib().mdrtNbBatchAutotune(self._h, _dp(self.x), _dp(self.forces_out), _stream(stream),
                                             _hp(choice)), "mdrtNbBatchAutotune")
-        return {"search_warps": int(choice[0]), "pair_blocks_per_sm": int(choice[1])}
+        return {"search_warps": int(choice[0]), "pair_blocks_per_sm": int(choice[1]),
+                "staging_depth": int(choice[2]), "members_per_group": 16, "threads_per_group": 16}
 
     def force(self, energy=True, graph=False, stream=None):
         """The forces of all frames (device f64 (n, 3), the evaluator's

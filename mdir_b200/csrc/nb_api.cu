@@ -130,7 +130,7 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   nb_free(c.key); nb_free(c.bin_count); nb_free(c.bin_start); nb_free(c.bin_fill);
   nb_free(c.sorted); nb_free(c.col_groups); nb_free(c.scan_scratch);
   nb_free(c.atom_xw); nb_free(c.atom_shift);
-  nb_free(c.xq); nb_free(c.typ_p); nb_free(c.acc); nb_free(c.acc_fixed);
+  nb_free(c.xq); nb_free(c.xq_lo); nb_free(c.typ_p); nb_free(c.acc); nb_free(c.acc_fixed);
   nb_free(c.unit_partials); nb_free(c.energy);
   nb_free(c.slab_in); nb_free(c.counts_in); nb_free(c.unit_n_in); nb_free(c.unit_start_in);
   nb_free(c.units_in); nb_free(c.sizes_in); nb_free(c.one);
@@ -256,6 +256,10 @@ int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value) {
     case MDRT_NB_TUNE_PAIR_BLOCKS_PER_SM:
       if (value < 1 || value > 4) return MDRT_NB_INVALID_ARGUMENT;
       ctx->c.pair_blocks_per_sm = value;
+      return MDRT_NB_OK;
+    case MDRT_NB_TUNE_STAGING_DEPTH:
+      if (value != 1 && value != 2) return MDRT_NB_INVALID_ARGUMENT;
+      ctx->c.staging_depth = value;
       return MDRT_NB_OK;
     case MDRT_NB_TUNE_FUSED_PRUNE:
       if (value < 0 || value > 2) return MDRT_NB_INVALID_ARGUMENT;

@@ -235,6 +235,11 @@ int32_t mdrtNbBatchSetTuning(mdrtNbBatch *b, int32_t key, int32_t value) {
       if (value != 1 && value != 4) return MDRT_NB_INVALID_ARGUMENT;
       b->search_warps = value;
       return MDRT_NB_OK;
+    case MDRT_NB_TUNE_STAGING_DEPTH:
+      if (value != 1 && value != 2) return MDRT_NB_INVALID_ARGUMENT;
+      b->nb->c.staging_depth = value;
+      drop_graph(b);
+      return MDRT_NB_OK;
   }
   return MDRT_NB_INVALID_ARGUMENT;
 }
@@ -334,12 +339,14 @@ int32_t mdrtNbBatchAutotune(mdrtNbBatch *b, const double *x, double *forces, voi
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   float best = 1e30f;
-  int best_w = b->search_warps, best_p = c.pair_blocks_per_sm;
+  int best_w = b->search_warps, best_p = c.pair_blocks_per_sm, best_d = c.staging_depth;
   int32_t status = MDRT_NB_OK;
   for (int w : {4, 1}) {
-    for (int pb : {4, 3, 2, 1}) {
+    for (int trial = 0; trial < 8; ++trial) {
+      int pb = 4 - trial / 2, depth = 1 + trial % 2;
       b->search_warps = w;
       c.pair_blocks_per_sm = pb;
+      c.staging_depth = depth;
       drop_graph(b);
       // a warm-up, then three timed builds + evaluations
       status = mdrtNbBatchBuild(b, x, b->h_boxes.data(), stream, nullptr);
@@ -358,6 +365,7 @@ int32_t mdrtNbBatchAutotune(mdrtNbBatch *b, const double *x, double *forces, voi
         best = ms;
         best_w = w;
         best_p = pb;
+        best_d = depth;
       }
     }
     if (status) break;
@@ -366,6 +374,7 @@ int32_t mdrtNbBatchAutotune(mdrtNbBatch *b, const double *x, double *forces, voi
   cudaEventDestroy(e1);
   b->search_warps = best_w;
   c.pair_blocks_per_sm = best_p;
+  c.staging_depth = best_d;
   if (best_w == 1) {  // a warp a group stages nothing
     bfree(b->search_scratch);
     b->search_scratch_entries = 0;
@@ -374,6 +383,7 @@ int32_t mdrtNbBatchAutotune(mdrtNbBatch *b, const double *x, double *forces, voi
   if (choice) {
     choice[0] = best_w;
     choice[1] = best_p;
+    choice[2] = best_d;
   }
   return status;
 }

@@ -797,6 +797,7 @@ static int nb_reserve(NbCtx &c, int64_t list_cap) {
         nb_realloc(c.xw, cap * NB_GROUP) || nb_realloc(c.box_lo, cap) || nb_realloc(c.box_hi, cap) ||
         nb_realloc(c.group_col, cap) || nb_realloc(c.counts, cap) || nb_realloc(c.unit_n, cap) ||
         nb_realloc(c.unit_start, cap + 1) || nb_realloc(c.xq, cap * NB_GROUP) ||
+        nb_realloc(c.xq_lo, cap * NB_GROUP) ||
         nb_realloc(c.typ_p, cap * NB_GROUP) || nb_realloc(c.acc, cap * NB_GROUP) ||
         nb_realloc(c.acc_fixed, cap * NB_GROUP * 3))
       return -1;

@@ -89,6 +89,7 @@ struct NbCtx {
   char4 *atom_shift = nullptr;
   // per-step frames and accumulators (place order)
   float4 *xq = nullptr;
+  float4 *xq_lo = nullptr;               // the f32 residual of each frame (deterministic mode: split frames)
   int32_t *typ_p = nullptr;
   float4 *acc = nullptr;                 // pair + excluded forces, f32 atomics
   unsigned long long *acc_fixed = nullptr;  // 3 per place, deterministic mode
@@ -116,6 +117,7 @@ struct NbCtx {
   int pair_blocks_per_sm = 4;
   int pair_sms = 0;  // SMs the persistent pair grid spans (0: all); the rest are left to PME
   int fused_prune = 0;  // the MD step's pruning in the pair kernel: 0 by group count, 1 always, 2 never
+  int staging_depth = 1;  // the pair kernel's force forms: 1, a unit's entries read as it starts; 2, during the unit before
   int32_t *one = nullptr;  // a device 1: the gate of a pruning a force call asks for (MDRT_NB_PRUNE)
   // parameter gradient scratch (mdrtNbParameterGradient), allocated at the first call
   float4 *adj_g = nullptr;        // per place: the cotangent on the forces (f32)

@@ -217,15 +217,23 @@ __device__ __forceinline__ Vec3 take_force(int p, float4 *acc, unsigned long lon
   return f;
 }
 
-__device__ __forceinline__ float4 write_frame(int p, Vec3 x, const char4 *__restrict__ shift, const double *L,
-                                              float4 *xq) {
-  if (p < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
-  char4 s = shift[p];
-  float4 o = xq[p];
-  float4 nf = make_float4((float)(x.x + nb_frame_shift(s.x) * L[0]), (float)(x.y + nb_frame_shift(s.y) * L[1]),
-                          (float)(x.z + nb_frame_shift(s.z) * L[2]), o.w);
+// The frame of place p at x (the charge kept), and with xq_lo its f32
+// residual (the split frames of the deterministic mode).
+__device__ __forceinline__ float4 md_frame(int p, Vec3 x, char4 s, const double *L, float q, float4 *xq,
+                                           float4 *xq_lo) {
+  double fx = x.x + nb_frame_shift(s.x) * L[0], fy = x.y + nb_frame_shift(s.y) * L[1];
+  double fz = x.z + nb_frame_shift(s.z) * L[2];
+  float4 nf = make_float4((float)fx, (float)fy, (float)fz, q);
   xq[p] = nf;
+  if (xq_lo)
+    xq_lo[p] = make_float4((float)(fx - (double)nf.x), (float)(fy - (double)nf.y), (float)(fz - (double)nf.z), 0.f);
   return nf;
+}
+
+__device__ __forceinline__ float4 write_frame(int p, Vec3 x, const char4 *__restrict__ shift, const double *L,
+                                              float4 *xq, float4 *xq_lo) {
+  if (p < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+  return md_frame(p, x, shift[p], L, xq[p].w, xq, xq_lo);
 }
 
 // The PME force on the atom at frame fr (charge fr.w), gathered from the
@@ -300,7 +308,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     UpdateParams U, const double *__restrict__ inv_mass, const double *__restrict__ mass,
     const float *__restrict__ charge, const int32_t *__restrict__ wplace, const int32_t *__restrict__ fplace,
     const char4 *__restrict__ shift, float4 *acc, unsigned long long *accf, const float4 *__restrict__ pme,
-    float4 *xq, double *__restrict__ x, double *__restrict__ v, double *__restrict__ fout,
+    float4 *xq, float4 *xq_lo, double *__restrict__ x, double *__restrict__ v, double *__restrict__ fout,
     const double *__restrict__ x_ref, const double *__restrict__ x_prune, double *thermo, double *ke_part,
     float2 *blk_max, unsigned int *counter) {
   __shared__ double s_ke[MD_UPDATE_THREADS / 32];
@@ -394,10 +402,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
       store3(v, a, vn);
       store3(fout, a, f);
       if (p >= 0) {
-        float4 nf = make_float4((float)(xn.x + nb_frame_shift(sh.x) * U.L[0]),
-                                (float)(xn.y + nb_frame_shift(sh.y) * U.L[1]),
-                                (float)(xn.z + nb_frame_shift(sh.z) * U.L[2]), qw);
-        xq[p] = nf;
+        md_frame(p, xn, sh, U.L, qw, xq, xq_lo);
         if (U.fixed) {
           accf[3 * p] = 0ull;
           accf[3 * p + 1] = 0ull;
@@ -430,7 +435,7 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     store3(x, i, xi);
     store3(v, i, vi);
     store3(fout, i, fi);
-    write_frame(pi, xi, shift, U.L, xq);
+    write_frame(pi, xi, shift, U.L, xq, xq_lo);
     ke = 0.5 * mass[i] * dot(vi, vi);
     Vec3 di = xi - load3(x_ref, i);
     d2max = (float)dot(di, di);
@@ -744,7 +749,8 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
   U.unit_counter = c.inner_reach > 0.0 ? md_unit_counter(m) : nullptr;
   nb_launch_chained(md_update, dim3(m.ke_blocks), dim3(MD_UPDATE_THREADS), 0, s, m.nwaters, m.nfree, m.waters,
                     m.free_atoms, U, m.inv_mass, m.mass, c.q, m.wplace, m.fplace, c.shift, c.acc, c.acc_fixed,
-                    (pme && !fused) ? (const float4 *)c.pme.pme_force : nullptr, c.xq, x, v, m.force, m.x_ref,
+                    (pme && !fused) ? (const float4 *)c.pme.pme_force : nullptr, c.xq,
+                    c.deterministic ? c.xq_lo : nullptr, x, v, m.force, m.x_ref,
                     m.x_prune, m.thermo, m.ke_part, m.blk_max, m.done_blocks);
 }
 

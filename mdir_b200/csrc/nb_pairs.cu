@@ -38,6 +38,7 @@ namespace {
 struct PairParams {
   float Lx, Ly, Lz;
   float bx, cx, cy;  // tilts of a triclinic cell (0: orthorhombic)
+  double Ld[6];      // the cell in f64 (ax, by, cz, bx, cx, cy): the exact image shifts of the split frames
   float rc2;
   float beta;
   float beta_p;         // p beta, p of the erfc approximation below
@@ -142,11 +143,22 @@ __device__ __forceinline__ void nb_red_fixed(unsigned long long *addr, float x, 
 // most NB_SPARSE_BITS members), the members' and partners' forces, and with
 // ENERGY the unit's energy and virial partials at `unit`.  s_xw, s_fw, s_tw
 // and s_bw are the warp's shared arrays (the 16 members twice; the sparse
-// round's member forces).
-template <bool ENERGY, bool FIXED, int SWITCH, int LJM, bool BATCH>
-__device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64_t unit,
+// round's member forces).  With STAGED the caller has read the unit's two
+// rounds of entries ahead (pre0, pre1: the staging depth 2 of the pair
+// kernel); else the force forms read them here, in flight with the
+// members' loads.
+//
+// FIXED (the deterministic mode) takes split frames: the f32 frame xq and
+// its rounding residual xq_lo ((x + (S - 1/2) L) - xq in f32), the
+// partner's image shift exact in f64 and split the same way, so that a
+// pair's displacement is (xm - xj) + (xm_lo - xj_lo): no bits lost to the
+// size of the cell (a 22 nm box has f32 frames of up to 11 nm).  s_lw is
+// the warp's shared array of the members' residuals.
+template <bool ENERGY, bool FIXED, int SWITCH, int LJM, bool BATCH, bool STAGED = false>
+__device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64_t unit, int2 pre0, int2 pre1,
                                              const float4 *__restrict__ group_L, const int2 *__restrict__ slab,
                                              const int32_t *__restrict__ counts, const float4 *__restrict__ xq,
+                                             const float4 *__restrict__ xq_lo, float4 *s_lw,
                                              const int32_t *__restrict__ typ, const float2 *__restrict__ ljf,
                                              const float2 *s_lj, float4 *s_xw, float2 *s_fw, int *s_tw,
                                              float (*s_bw)[NB_SPARSE_BITS][33], float4 *__restrict__ acc,
@@ -162,8 +174,7 @@ __device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64
   // lanes past the list's end drop theirs below); the energy forms read
   // each round's when they come to it
   const int2 *row = slab + (int64_t)g * P.list_cap + (int64_t)uo.y * NB_UNIT;
-  int2 pre0 = make_int2(0, 0), pre1 = make_int2(0, 0);
-  if (!ENERGY) {
+  if (!ENERGY && !STAGED) {
     pre0 = row[lane];
     pre1 = row[32 + lane];
   }
@@ -173,6 +184,7 @@ __device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64
     xi.w *= P.coulomb;
     int ti = typ[pi];
     s_xw[lane] = xi;
+    if (FIXED) s_lw[lane] = xq_lo[pi];
     if (LJM == 1) {  // the member's factors times 6 and 12: the force's factors
       float2 f = ljf[ti];
       s_fw[lane] = make_float2(6.f * f.x, 12.f * f.y);
@@ -196,14 +208,26 @@ __device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64
   for (int r = 0; r < 2; ++r) {
     if (r * 32 >= ne) break;
     bool valid = r * 32 + lane < ne;
-    int2 en = valid ? (ENERGY ? row[r * 32 + lane] : (r == 0 ? pre0 : pre1)) : make_int2(0, 0);
+    int2 en = valid ? ((ENERGY && !STAGED) ? row[r * 32 + lane] : (r == 0 ? pre0 : pre1)) : make_int2(0, 0);
     int q = en.x;
     unsigned mask = valid ? ((unsigned)en.y & 0xffffu) : 0u;
     int code = ((unsigned)en.y >> 16) & NB_IMAGE_BITS;
     int sx, sy, sz;
     nb_decode_image(code, sx, sy, sz);
     float4 xj = xq[q];
-    {
+    float3 jl = make_float3(0.f, 0.f, 0.f);  // FIXED: the residual of the partner's image
+    if (FIXED) {
+      // the image x_j + n H in f64 from the split frame, split again
+      float4 lo = xq_lo[q];
+      double na = sx, nbv = sy, nc = sz;
+      double X = (double)xj.x + (double)lo.x + ((na * P.Ld[0] + nbv * P.Ld[3]) + nc * P.Ld[4]);
+      double Y = (double)xj.y + (double)lo.y + (nbv * P.Ld[1] + nc * P.Ld[5]);
+      double Z = (double)xj.z + (double)lo.z + nc * P.Ld[2];
+      xj.x = (float)X;
+      xj.y = (float)Y;
+      xj.z = (float)Z;
+      jl = make_float3((float)(X - (double)xj.x), (float)(Y - (double)xj.y), (float)(Z - (double)xj.z));
+    } else {
       NbCell H;
       H.ax = Lx;
       H.by = Ly;
@@ -224,6 +248,12 @@ __device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64
     auto pair = [&](int m, bool masked_in, float &fx, float &fy, float &fz) {
       float4 xm = s_xw[m];
       float dx = xm.x - xj.x, dy = xm.y - xj.y, dz = xm.z - xj.z;
+      if (FIXED) {
+        float4 ml = s_lw[m];
+        dx += ml.x - jl.x;
+        dy += ml.y - jl.y;
+        dz += ml.z - jl.z;
+      }
       float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       bool inside = masked_in && (r2 < P.rc2);
       float2 cc;  // (6 c6, 12 c12)
@@ -353,13 +383,18 @@ __device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64
 // shared memory (slots u and u + 16), so that in a dense round lane l reads
 // member (l + k) mod 16 at slot l mod 16 + k: an immediate offset in the
 // unrolled loop, no index arithmetic.
-template <bool ENERGY, bool FIXED, int SWITCH, int LJM, bool BATCH = false>
+// DEPTH is the staging depth: 1, a unit's entries are read when it starts
+// (the force forms read the next unit's header during a unit, the energy
+// forms each round's entries when they come to it); 2, the next unit's
+// header and entries are in flight during a unit (four more registers).
+template <bool ENERGY, bool FIXED, int SWITCH, int LJM, bool BATCH = false, int DEPTH = 1>
 __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *__restrict__ group_L,
                                                 const int32_t *__restrict__ sizes,
                                                 const int2 *__restrict__ units,
                                                 const int2 *__restrict__ slab,
                                                 const int32_t *__restrict__ counts,
                                                 const float4 *__restrict__ xq,
+                                                const float4 *__restrict__ xq_lo,
                                                 const int32_t *__restrict__ typ,
                                                 const float2 *__restrict__ lj, const float2 *__restrict__ ljf,
                                                 float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
@@ -369,6 +404,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   if (halt && *halt) return;  // the MD step stopped at a stale list (its host rebuilds)
   if (skip && *skip) return;  // a pruning step: the pruning kernel computed the pairs
   __shared__ float4 s_x[8][2 * NB_GROUP];
+  __shared__ float4 s_l[8][FIXED ? 2 * NB_GROUP : 1];  // FIXED: the members' frame residuals
   __shared__ float2 s_f[8][2 * NB_GROUP];  // LJM 1: member factors
   __shared__ int s_t[8][2 * NB_GROUP];     // LJM 0: member row offsets in s_lj
   __shared__ float2 s_lj[LJM == 0 ? NB_MAX_TYPES * NB_MAX_TYPES : 1];
@@ -387,13 +423,40 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   // the next unit's header is in flight during this unit (the energy forms,
   // short of registers, read it when they come to it)
   int unit = blockIdx.x * 8 + warp;
+  const int lane = threadIdx.x & 31;
+  if (DEPTH == 2) {
+    // the unit's entries were read during the unit before
+    int2 uo = unit < nunits ? units[unit] : make_int2(0, 0);
+    int2 e0 = make_int2(0, 0), e1 = make_int2(0, 0);
+    if (unit < nunits) {
+      const int2 *row = slab + (int64_t)uo.x * P.list_cap + (int64_t)uo.y * NB_UNIT;
+      e0 = row[lane];
+      e1 = row[32 + lane];
+    }
+    for (; unit < nunits; unit += wstride) {
+      int2 un = make_int2(0, 0), n0 = make_int2(0, 0), n1 = make_int2(0, 0);
+      if (unit + wstride < nunits) {
+        un = units[unit + wstride];
+        const int2 *row = slab + (int64_t)un.x * P.list_cap + (int64_t)un.y * NB_UNIT;
+        n0 = row[lane];
+        n1 = row[32 + lane];
+      }
+      nb_pair_unit<ENERGY, FIXED, SWITCH, LJM, BATCH, true>(P, uo, unit, e0, e1, group_L, slab, counts, xq, xq_lo,
+                                                            s_l[warp], typ, ljf, s_lj, s_x[warp], s_f[warp],
+                                                            s_t[warp], s_b[warp], acc, accf, partials, status);
+      uo = un;
+      e0 = n0;
+      e1 = n1;
+    }
+    return;
+  }
   int2 uo_next = !ENERGY && unit < nunits ? units[unit] : make_int2(0, 0);
   for (; unit < nunits; unit += wstride) {
     int2 uo = ENERGY ? units[unit] : uo_next;
     if (!ENERGY && unit + wstride < nunits) uo_next = units[unit + wstride];
-    nb_pair_unit<ENERGY, FIXED, SWITCH, LJM, BATCH>(P, uo, unit, group_L, slab, counts, xq, typ, ljf, s_lj,
-                                                    s_x[warp], s_f[warp], s_t[warp], s_b[warp], acc, accf,
-                                                    partials, status);
+    nb_pair_unit<ENERGY, FIXED, SWITCH, LJM, BATCH>(P, uo, unit, make_int2(0, 0), make_int2(0, 0), group_L, slab,
+                                                    counts, xq, xq_lo, s_l[warp], typ, ljf, s_lj, s_x[warp],
+                                                    s_f[warp], s_t[warp], s_b[warp], acc, accf, partials, status);
   }
 }
 
@@ -439,9 +502,10 @@ __global__ void __launch_bounds__(NB_PRUNE_WARPS * 32)
   int warp = threadIdx.x >> 5;
   int nu = (total + NB_UNIT - 1) / NB_UNIT;
   for (int o = warp; o < nu; o += NB_PRUNE_WARPS)
-    nb_pair_unit<false, false, SWITCH, LJM, false>(P, make_int2((int)g, o), 0, nullptr, slab_in, counts_in, xq, typ,
-                                                   ljf, s_lj, s_x[warp], s_f[warp], s_t[warp], s_b[warp], acc,
-                                                   nullptr, nullptr, status);
+    nb_pair_unit<false, false, SWITCH, LJM, false>(P, make_int2((int)g, o), 0, make_int2(0, 0), make_int2(0, 0),
+                                                   nullptr, slab_in, counts_in, xq, nullptr, nullptr, typ, ljf, s_lj,
+                                                   s_x[warp], s_f[warp], s_t[warp], s_b[warp], acc, nullptr,
+                                                   nullptr, status);
 }
 
 // Frames: xq[p] = ((float)(x_a + (S_p - 1/2) L), q_a) for the atom a at place p;
@@ -450,20 +514,27 @@ __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
                           const int32_t *__restrict__ order, const char4 *__restrict__ shift,
                           const double *__restrict__ x, const float *__restrict__ q,
                           const int32_t *__restrict__ type, double Lx, double Ly, double Lz, double bx,
-                          double cx, double cy, float4 *__restrict__ xq, int32_t *__restrict__ typ_p) {
+                          double cx, double cy, float4 *__restrict__ xq, int32_t *__restrict__ typ_p,
+                          float4 *__restrict__ xq_lo) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
   int a = order[p];
   if (a < 0) {
     xq[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (xq_lo) xq_lo[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     typ_p[p] = 0;
     return;
   }
-  // x + S H less half the diagonal (a triclinic cell adds S's tilt terms)
+  // x + S H less half the diagonal (a triclinic cell adds S's tilt terms),
+  // and with xq_lo the f32 residual of each coordinate
   char4 s = shift[p];
-  xq[p] = make_float4((float)(x[3 * a] + nb_frame_shift(s.x) * Lx + (double)s.y * bx + (double)s.z * cx),
-                      (float)(x[3 * a + 1] + nb_frame_shift(s.y) * Ly + (double)s.z * cy),
-                      (float)(x[3 * a + 2] + nb_frame_shift(s.z) * Lz), q[a]);
+  double fx = x[3 * a] + nb_frame_shift(s.x) * Lx + (double)s.y * bx + (double)s.z * cx;
+  double fy = x[3 * a + 1] + nb_frame_shift(s.y) * Ly + (double)s.z * cy;
+  double fz = x[3 * a + 2] + nb_frame_shift(s.z) * Lz;
+  float4 hi = make_float4((float)fx, (float)fy, (float)fz, q[a]);
+  xq[p] = hi;
+  if (xq_lo)
+    xq_lo[p] = make_float4((float)(fx - (double)hi.x), (float)(fy - (double)hi.y), (float)(fz - (double)hi.z), 0.f);
   typ_p[p] = type[a];
 }
 
@@ -987,6 +1058,12 @@ PairParams pair_params(const NbCtx &c, const double box[3]) {
   P.bx = (float)c.tilt[0];
   P.cx = (float)c.tilt[1];
   P.cy = (float)c.tilt[2];
+  P.Ld[0] = box[0];
+  P.Ld[1] = box[1];
+  P.Ld[2] = box[2];
+  P.Ld[3] = c.tilt[0];
+  P.Ld[4] = c.tilt[1];
+  P.Ld[5] = c.tilt[2];
   P.rc2 = (float)(c.cutoff * c.cutoff);
   P.beta = (float)c.beta;
   P.beta_p = (float)(0.3275911 * c.beta);
@@ -1010,7 +1087,8 @@ PairParams pair_params(const NbCtx &c, const double box[3]) {
 void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
   nb_gather<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.shift, x,
                                                           c.q, c.type, box[0], box[1], box[2], c.tilt[0],
-                                                          c.tilt[1], c.tilt[2], c.xq, c.typ_p);
+                                                          c.tilt[1], c.tilt[2], c.xq, c.typ_p,
+                                                          c.deterministic ? c.xq_lo : nullptr);
 }
 
 bool nb_fused_prune(const NbCtx &c) {
@@ -1074,10 +1152,17 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, co
   const int2 *lunits = inner ? c.units_in : c.units;
   const int2 *lslab = inner ? c.slab_in : c.slab;
   const int32_t *lcounts = inner ? c.counts_in : c.counts;
-#define NB_LAUNCH2(E, F, S, M)                                                                            \
-  nb_launch_chained(nb_pairs<E, F, S, M>, dim3(grid), dim3(256), 0, s, P, (const float4 *)nullptr, lsizes,  \
-                    lunits, lslab, lcounts, c.xq, c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed, c.unit_partials, \
-                    c.status, halt, skip)
+#define NB_LAUNCH3(E, F, S, M, D)                                                                          \
+  nb_launch_chained(nb_pairs<E, F, S, M, false, D>, dim3(grid), dim3(256), 0, s, P, (const float4 *)nullptr,  \
+                    lsizes, lunits, lslab, lcounts, c.xq, c.xq_lo, c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed,  \
+                    c.unit_partials, c.status, halt, skip)
+#define NB_LAUNCH2(E, F, S, M)                     \
+  do {                                             \
+    if (c.staging_depth == 2)                      \
+      NB_LAUNCH3(E, F, S, M, 2);                   \
+    else                                           \
+      NB_LAUNCH3(E, F, S, M, 1);                   \
+  } while (0)
 #define NB_LAUNCH(E, F, S)      \
   do {                          \
     if (c.lj_geom)              \
@@ -1103,6 +1188,7 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, co
 #undef NB_LAUNCH_S
 #undef NB_LAUNCH
 #undef NB_LAUNCH2
+#undef NB_LAUNCH3
 }
 
 void nb_excluded_list_run(NbCtx &c, const double box[3], const int32_t *pairs, int64_t npairs,
@@ -1229,14 +1315,20 @@ void nb_batch_pairs_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
   PairParams P = pair_params(c, unit_box);
   int64_t want = (c.units_cap + 7) / 8;
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)g_sm_count * std::max(1, c.pair_blocks_per_sm)));
-#define NB_BATCH_LAUNCH(E, M)                                                                                \
-  nb_pairs<E, false, 0, M, true><<<grid, 256, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq, \
-                                                         c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed, c.unit_partials, \
-                                                         c.status, nullptr, nullptr)
+#define NB_BATCH_LAUNCH(E, M, D)                                                                               \
+  nb_pairs<E, false, 0, M, true, D><<<grid, 256, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq,  \
+                                                            nullptr, c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed,     \
+                                                            c.unit_partials, c.status, nullptr, nullptr)
   if (energy) {
-    if (c.lj_geom) NB_BATCH_LAUNCH(true, 1); else NB_BATCH_LAUNCH(true, 0);
+    if (c.staging_depth == 2) {
+      if (c.lj_geom) NB_BATCH_LAUNCH(true, 1, 2); else NB_BATCH_LAUNCH(true, 0, 2);
+    } else {
+      if (c.lj_geom) NB_BATCH_LAUNCH(true, 1, 1); else NB_BATCH_LAUNCH(true, 0, 1);
+    }
+  } else if (c.staging_depth == 2) {
+    if (c.lj_geom) NB_BATCH_LAUNCH(false, 1, 2); else NB_BATCH_LAUNCH(false, 0, 2);
   } else {
-    if (c.lj_geom) NB_BATCH_LAUNCH(false, 1); else NB_BATCH_LAUNCH(false, 0);
+    if (c.lj_geom) NB_BATCH_LAUNCH(false, 1, 1); else NB_BATCH_LAUNCH(false, 0, 1);
   }
 #undef NB_BATCH_LAUNCH
 }

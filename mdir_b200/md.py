@@ -79,11 +79,13 @@ class Integrator:
         return p.value
 
     def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(0.975, 1.0, 1.025, 1.05),
-             pair_sms=(0, 112, 120, 128, 136), pair_blocks=(4, 3), fused=(2, 1), steps=400, reps=3, stream=None):
+             pair_sms=(0, 112, 120, 128, 136), pair_blocks=(4, 3), depths=(1, 2), fused=(2, 1), steps=400, reps=3,
+             stream=None):
         """The autotuner of the step, in three stages: the outer and pruned
         reaches first (the launch shapes as set), then the span of the pair
-        grid (SMs; the others are left to the PME kernels beside it) and its
-        blocks per SM at the reaches kept, then the pruning inside the pair
+        grid (SMs; the others are left to the PME kernels beside it), its
+        blocks per SM and its staging depth at the reaches kept, then the
+        pruning inside the pair
         kernel (MDIR D284) or in a launch of its own.  Each choice is timed as `reps`
         runs of `steps` steps after a build and half as many untimed steps;
         the fastest is kept and built for.  x and v are put back; the step
@@ -97,10 +99,10 @@ class Integrator:
         keep_x, keep_v = x.clone(), v.clone()
         st = stream if stream is not None else torch.cuda.current_stream(x.device)
 
-        def trial(R, Rin, sms, blocks):
+        def trial(R, Rin, sms, blocks, depth=None):
             t.set_reach(R)
             t.set_pruned_reach(Rin)
-            t.set_tuning(pair_sms=sms, pair_blocks_per_sm=blocks)
+            t.set_tuning(pair_sms=sms, pair_blocks_per_sm=blocks, staging_depth=depth)
             x.copy_(keep_x)
             v.copy_(keep_v)
             self.build(x, box, stream=st)
@@ -119,19 +121,22 @@ class Integrator:
         sms0 = getattr(t, "pair_sms", 0)
         blocks0 = getattr(t, "pair_blocks_per_sm", 4)
         fused0 = getattr(t, "fused_prune", 0)
+        depth0 = getattr(t, "staging_depth", 1)
         trials = []
         for R in reaches:
             if not R < 0.999 * least:
                 continue
             for Rin in pruned:
                 if cutoff <= Rin < R:
-                    trials.append((trial(R, Rin, sms0, blocks0), R, Rin, sms0, blocks0))
-        _, R, Rin, _, _ = min(trials)
+                    trials.append((trial(R, Rin, sms0, blocks0, depth0), R, Rin, sms0, blocks0, depth0))
+        _, R, Rin, _, _, _ = min(trials)
         for sms in pair_sms:
             for blocks in pair_blocks:
-                if (sms, blocks) != (sms0, blocks0):
-                    trials.append((trial(R, Rin, sms, blocks), R, Rin, sms, blocks))
-        us, R, Rin, sms, blocks = min(t_ for t_ in trials if t_[1] == R and t_[2] == Rin)
+                for depth in depths:
+                    if (sms, blocks, depth) != (sms0, blocks0, depth0):
+                        trials.append((trial(R, Rin, sms, blocks, depth), R, Rin, sms, blocks, depth))
+        us, R, Rin, sms, blocks, depth = min(t_ for t_ in trials if t_[1] == R and t_[2] == Rin)
+        t.set_tuning(staging_depth=depth)
         # the pruning in the pair kernel (MDIR D284) or in a launch of its
         # own, at the shape kept
         fused_trials = []
@@ -151,7 +156,7 @@ class Integrator:
         v.copy_(keep_v)
         self.build(x, box, stream=st)
         return {"reach": R, "pruned_reach": Rin, "pair_sms": sms, "pair_blocks_per_sm": blocks,
-                "fused_prune": fchoice, "us_per_step": round(us, 2), "trials": len(trials) + len(fused_trials)}
+                "staging_depth": depth, "fused_prune": fchoice, "us_per_step": round(us, 2), "trials": len(trials) + len(fused_trials)}
 
     def temperature(self, stream=None):
         t = self.thermo(stream)

@@ -62,6 +62,7 @@ class NonbondedTerm:
         self.pair_sms = 0
         self.pair_blocks_per_sm = 4
         self.fused_prune = 0
+        self.staging_depth = 1
 
     def close(self):
         if getattr(self, "_h", None):
@@ -119,7 +120,7 @@ class NonbondedTerm:
         b = _host(self.box if box is None else box, np.float64)
         L.check(L.lib().mdrtNbPrune(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtNbPrune")
 
-    def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None, fused_prune=None):
+    def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None, fused_prune=None, staging_depth=None):
         """Launch shapes and the MD step's pruning in the pair kernel (0 by
         group count, 1 always, 2 never): the autotuner's knobs; results do
         not depend on them beyond the order of f32 sums."""
@@ -130,6 +131,9 @@ class NonbondedTerm:
         if pair_sms is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_SMS, int(pair_sms)), "mdrtNbSetTuning")
             self.pair_sms = int(pair_sms)
+        if staging_depth is not None:
+            L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_STAGING_DEPTH, int(staging_depth)), "mdrtNbSetTuning")
+            self.staging_depth = int(staging_depth)
         if fused_prune is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_FUSED_PRUNE, int(fused_prune)), "mdrtNbSetTuning")
             self.fused_prune = int(fused_prune)

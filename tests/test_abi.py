@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 def test_version_and_status_strings_need_no_device():
     from mdir_b200 import _lib
     lib = _lib.lib()
-    assert lib.mdrtNbVersion() == 1
+    assert lib.mdrtNbVersion() == 2
     assert b"reach" in lib.mdrtNbStatusString(_lib.INVALID_BOX)
 
 

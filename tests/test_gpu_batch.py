@@ -82,6 +82,14 @@ def test_graph_replay_and_autotuned_shapes_give_the_same_forces(cuda, frames):
     assert np.allclose(E1, E0, rtol=1e-7, atol=1e-6)
     choice = ev.autotune()
     assert choice["search_warps"] in (1, 4) and 1 <= choice["pair_blocks_per_sm"] <= 4
+    assert choice["staging_depth"] in (1, 2)
+    # every shape the autotuner chooses among gives the same forces
+    for depth in (1, 2):
+        for blocks in (4, 1):
+            ev.set_tuning(pair_blocks_per_sm=blocks, staging_depth=depth)
+            Fd = ev.force(energy=True).clone()
+            assert rms_rel(Fd.cpu().numpy(), F0.cpu().numpy()) < 1e-6, (depth, blocks)
+    ev.set_tuning(pair_blocks_per_sm=choice["pair_blocks_per_sm"], staging_depth=choice["staging_depth"])
     F2 = ev.force(energy=True).clone()
     assert rms_rel(F2.cpu().numpy(), F0.cpu().numpy()) < 1e-6
     # new positions: the graph reads them from the same buffer

@@ -187,3 +187,29 @@ def test_md_step_with_the_pruning_in_the_pair_kernel(cuda):
     assert pa == pb == pc and pa >= 10 and ba == bb == bc
     control = np.abs(xa - xc).max()
     assert np.abs(xa - xb).max() < 1e-4 or np.abs(xa - xb).max() < 10 * control, (np.abs(xa - xb).max(), control)
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_staging_depth_changes_no_force(cuda, deterministic):
+    """The pair kernel's staging depth 2 (the next unit's entries in flight)
+    gives the forces and energies of depth 1: bit for bit in the
+    deterministic mode, to the order of f32 sums otherwise."""
+    s = systems.tip3p(waters=1500, seed=23)
+    box = list(s["box"])
+    xd = torch.tensor(s["positions"], device=cuda)
+    out = []
+    for depth in (1, 2):
+        t = _term(s, s["sigma"], s["epsilon"], 1.3, 1.0, deterministic)
+        t.set_tuning(staging_depth=depth)
+        t.build(xd, box)
+        t.prune(xd, box)
+        f = t.force(xd, energy=True).cpu().numpy()
+        out.append((f, t.energies()))
+        t.close()
+    (f1, e1), (f2, e2) = out
+    if deterministic:
+        np.testing.assert_array_equal(f1, f2)
+        assert e1["lj"] == e2["lj"] and e1["coulomb"] == e2["coulomb"]
+    else:
+        assert np.sqrt(np.mean(np.sum((f2 - f1) ** 2, 1)) / np.mean(np.sum(f1 ** 2, 1))) < 1e-6
+        assert abs(e1["coulomb"] - e2["coulomb"]) <= 1e-9 * abs(e1["coulomb"])
