@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--pair-sms", type=int, default=0, help="span of the pair grid with --no-tune (0: all SMs)")
     p.add_argument("--pair-blocks", type=int, default=0,
                    help="blocks of the pair kernel an SM with --no-tune (0: the library's default)")
+    p.add_argument("--pme-fft", default="own", choices=["own", "cufft"],
+                   help="the PME transforms: the library's three kernels, or cuFFT")
     p.add_argument("--only", choices=["adjoint", "batch", "precision"], help="run one leg alone (profiling)")
     p.add_argument("--adjoint-frames", type=int, default=64)
     p.add_argument("--frame-lanes", type=int, default=4,
@@ -501,6 +503,7 @@ def main():
     term.set_interaction(s["cutoff"], s["reach"], s["beta"])
     term.set_pruned_reach(s["pruned"])
     term.set_pme(s["grid"], s["order"])
+    term.set_tuning(pme_fft=args.pme_fft)
     if args.no_tune and args.pair_sms:
         term.set_tuning(pair_sms=args.pair_sms)
     if args.no_tune and args.pair_blocks:
@@ -578,6 +581,7 @@ def main():
     exe.pair_blocks_per_sm = tuned["pair_blocks_per_sm"] if tuned else args.pair_blocks
     exe.fused_prune = tuned["fused_prune"] if tuned else 0
     exe.staging_depth = tuned["staging_depth"] if tuned else 1
+    exe.pme_fft = args.pme_fft
     sim = mdir.Simulation(mdir.compile(system, st, integ, ens, exe, sch))
 
     def e2e_step():

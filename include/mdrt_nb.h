@@ -164,7 +164,11 @@ enum mdrtNbTuneKey {
   MDRT_NB_TUNE_FUSED_PRUNE = 3,
   /* the pair kernel's staging depth: 1, a unit's entries are read as the
    * unit starts; 2, the next unit's entries are in flight during a unit */
-  MDRT_NB_TUNE_STAGING_DEPTH = 4
+  MDRT_NB_TUNE_STAGING_DEPTH = 4,
+  /* the PME transforms: 0, the library's own three-kernel convolution when
+   * every grid dimension is 32, 64 or 128 (the default), cuFFT otherwise;
+   * 1, cuFFT always (MDIR's cuFFT path, runtime/mdrt_cuda.c:2942-2990) */
+  MDRT_NB_TUNE_PME_FFT = 5
 };
 int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value);
 

@@ -159,6 +159,7 @@ class Execution:
         self.pair_blocks_per_sm = 0  # blocks of the pair kernel an SM (0: the library's default, 4)
         self.fused_prune = 0  # the pruning inside the pair kernel: 0 by group count, 1 always, 2 never
         self.staging_depth = 1  # the pair kernel's staging depth (1 or 2)
+        self.pme_fft = "own"  # the PME transforms: "own" (three kernels where the grid allows) or "cufft"
 
 
 class Schedule:
@@ -230,6 +231,8 @@ def compile(system, state, integrator, ensemble, execution, schedule):
         raise UnsupportedError("integrators: LEAP_FROG and VELOCITY_VERLET")
     if method == "VELOCITY_VERLET" and system.rigid_water and system.water_residues is not None:
         raise UnsupportedError("VELOCITY_VERLET with rigid waters needs velocity constraints; use LEAP_FROG")
+    if getattr(execution, "pme_fft", "own") not in ("own", "cufft"):
+        raise InputError("pme_fft: \"own\" or \"cufft\"")
     plan["waters"] = 0 if system.water_residues is None else len(system.water_residues)
     return Program(system, state, integrator, ensemble, execution, schedule, plan)
 
@@ -259,6 +262,8 @@ def _make_term(program):
         t.set_tuning(fused_prune=program.execution.fused_prune)
     if getattr(program.execution, "staging_depth", 1) != 1:
         t.set_tuning(staging_depth=program.execution.staging_depth)
+    if getattr(program.execution, "pme_fft", "own") != "own":
+        t.set_tuning(pme_fft=program.execution.pme_fft)
     return t
 
 

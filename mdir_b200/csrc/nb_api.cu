@@ -269,6 +269,10 @@ int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value) {
       if (value < 0 || value > 4096) return MDRT_NB_INVALID_ARGUMENT;
       ctx->c.pair_sms = value;
       return MDRT_NB_OK;
+    case MDRT_NB_TUNE_PME_FFT:
+      if (value != 0 && value != 1) return MDRT_NB_INVALID_ARGUMENT;
+      ctx->c.pme_fft = value;
+      return MDRT_NB_OK;
   }
   return MDRT_NB_INVALID_ARGUMENT;
 }

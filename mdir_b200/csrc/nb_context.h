@@ -33,6 +33,7 @@ struct NbPme {
   double infl_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // cell, beta, f, tilts of that table
   int conv_blocks = 0;
   size_t workspace_bytes = 0;
+  float2 *fft_tw = nullptr;     // twiddles of the own transforms (nb_fft.cuh), when every K is 32, 64 or 128
 };
 
 struct NbCtx {
@@ -117,6 +118,7 @@ struct NbCtx {
   int pair_blocks_per_sm = 4;
   int pair_sms = 0;  // SMs the persistent pair grid spans (0: all); the rest are left to PME
   int fused_prune = 0;  // the MD step's pruning in the pair kernel: 0 by group count, 1 always, 2 never
+  int pme_fft = 0;  // the PME transforms: 0, the own three-kernel convolution where the grid allows; 1, cuFFT
   int staging_depth = 1;  // the pair kernel's force forms: 1, a unit's entries read as it starts; 2, during the unit before
   int32_t *one = nullptr;  // a device 1: the gate of a pruning a force call asks for (MDRT_NB_PRUNE)
   // parameter gradient scratch (mdrtNbParameterGradient), allocated at the first call
@@ -265,6 +267,9 @@ void nb_prune_pairs_run(NbCtx &c, const double box[3], const int *gate, const do
 // threshold, DevicePolicy.cpp:70-99); never in the deterministic mode or
 // with lists too long for the kernel's shared-memory staging.
 bool nb_fused_prune(const NbCtx &c);
+// The PME convolution runs on the own three kernels (nb_fft.cuh): every
+// grid dimension 32, 64 or 128 and cuFFT not asked for.
+bool nb_fft_own(const NbCtx &c);
 #define NB_FUSED_PRUNE_GROUPS 4096
 #define NB_FUSED_STAGE_MAX (160 * 1024)
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);

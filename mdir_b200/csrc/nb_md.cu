@@ -817,8 +817,9 @@ static int md_pme_buffers(mdrtMd *m) {
       cudaMalloc(&m->spec, sizeof(float2) * half) != cudaSuccess ||
       cudaMalloc(&m->influence, sizeof(float) * half) != cudaSuccess)
     return -1;
-  // the grids start empty; each chain empties them again (the fixed-point
-  // grid by its conversion, the f32 grid by the spectrum scaling)
+  // the grids start empty; each chain empties the grid it spread (the
+  // forward plane kernel of the own transforms; with cuFFT the conversion
+  // of the fixed-point grid or the spectrum scaling)
   if (cudaMemset(m->qfixed, 0, sizeof(unsigned long long) * pts) != cudaSuccess ||
       cudaMemset(m->qgrid, 0, sizeof(float) * pts) != cudaSuccess)
     return -1;
@@ -1141,7 +1142,8 @@ static int32_t md_prepare_graph(mdrtMd *m, double *x, double *v, const double bo
   NbCtx &c = *m->nb;
   int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap + (int64_t)(c.inner_reach * 1e9) +
                 (c.inner_valid ? 1 : 0) + (c.deterministic ? 2 : 0) + ((int64_t)c.pair_blocks_per_sm << 40) +
-                ((int64_t)c.pair_sms << 44) + (int64_t)(uintptr_t)m->qgrid + ((int64_t)nb_fused_prune(c) << 56);
+                ((int64_t)c.pair_sms << 44) + (int64_t)(uintptr_t)m->qgrid + ((int64_t)nb_fused_prune(c) << 56) +
+                ((int64_t)c.staging_depth << 58) + ((int64_t)nb_fft_own(c) << 61);
   bool stale = !m->exec || m->gx != x || m->gv != v || m->gdt != dt || m->gunroll != unroll ||
                m->gbox[0] != box[0] || m->gbox[1] != box[1] || m->gbox[2] != box[2] || m->gcap_key != key;
   if (stale) {

@@ -22,7 +22,10 @@
 #include <cstdio>
 #include <vector>
 
+#include <type_traits>
+
 #include "nb_context.h"
+#include "nb_fft.cuh"
 #include "nb_spline.cuh"
 
 namespace {
@@ -193,6 +196,324 @@ __global__ void nb_pme_sum(const double *__restrict__ partials, int nblocks, dou
   if (threadIdx.x == 0) {
     energy[NB_E_REC] = s[0][0];
     for (int k = 0; k < 6; ++k) energy[NB_W_REC + k] = s[0][1 + k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The convolution on power-of-two grids in three kernels (nb_fft.cuh): the
+// grid g[x][y][z] (z fastest) and the half-complex spectrum S[kx][ky][kz]
+// (kz = 0..K2/2 fastest, cuFFT's R2C layout, so the influence table and the
+// gathers are shared with the cuFFT chain).
+//
+//   nb_fft_planes_fwd   a block per x plane: rows y, y+1 go through one
+//                       complex z transform as real and imaginary parts and
+//                       are separated after it; the K2/2 + 1 z frequencies
+//                       then take a y transform each, the real DC and
+//                       Nyquist lines together as one complex line.  Empties
+//                       the charge grid it read for the next spreading.
+//   nb_fft_columns      a block per L columns (ky, kz): the x transform, the
+//                       influence function B C (with the energy and virial
+//                       sums when asked), the inverse x transform.
+//   nb_fft_planes_inv   a block per x plane: the inverse y transforms, then
+//                       the pairs of rows through one inverse z transform.
+//
+// Every array stays in L2 on the MD step's grid (1 MiB at 64^3).
+
+template <int K>
+__device__ __forceinline__ void nb_fft_load_tw(float2 *dst, const float2 *__restrict__ tw_all) {
+  for (int i = threadIdx.x; i < K; i += blockDim.x) dst[i] = tw_all[nb_fft_tw_offset(K) + i];
+}
+
+// Shared memory of the plane kernels: twiddles, the row pairs S (lines of
+// K2 + 1), the z frequencies T (lines of K1 + 1); lines rounded up to whole
+// passes of the block's threads.
+template <int K1, int K2>
+struct NbFftPlane {
+  static constexpr int H = K2 / 2, PR = K1 / 2;
+  static constexpr int LA = NB_FFT_BLOCK / nb_fft_threads(K2), LB = NB_FFT_BLOCK / nb_fft_threads(K1);
+  static constexpr int SL = (PR + LA - 1) / LA * LA, TL = (H + LB - 1) / LB * LB;
+  static constexpr int S1 = K1 + 1, S2 = K2 + 1;
+  static constexpr size_t bytes = sizeof(float2) * (size_t)(K1 + K2 + SL * S2 + TL * S1);
+};
+
+template <int K1, int K2, bool FIXED>
+__global__ void __launch_bounds__(NB_FFT_BLOCK) nb_fft_planes_fwd(float *__restrict__ grid,
+                                                                  unsigned long long *__restrict__ fixed,
+                                                                  float2 *__restrict__ spec,
+                                                                  const float2 *__restrict__ tw_all,
+                                                                  const int *halt) {
+  using Q = NbFftPlane<K1, K2>;
+  constexpr int H = Q::H, S1 = Q::S1, S2 = Q::S2;
+  extern __shared__ float2 nb_fft_sm[];
+  float2 *tw1 = nb_fft_sm, *tw2 = tw1 + K1, *S = tw2 + K2, *T = S + Q::SL * S2;
+  nb_fft_load_tw<K1>(tw1, tw_all);
+  nb_fft_load_tw<K2>(tw2, tw_all);
+  nb_grid_wait();
+  const int stop = halt ? *halt : 0;  // the MD step stopped at a stale list
+  const int tid = threadIdx.x;
+  const int64_t plane = (int64_t)blockIdx.x * K1 * K2;
+  // rows 2p and 2p + 1 as the real and imaginary parts of line p: every
+  // load of a chunk in flight before the grid is emptied behind them
+  constexpr int NA = Q::PR * K2 / NB_FFT_BLOCK, CH = NA < 8 ? NA : 8;
+  static_assert(Q::PR * K2 % NB_FFT_BLOCK == 0, "whole rows per pass");
+#pragma unroll 1
+  for (int r0 = 0; r0 < NA; r0 += CH) {
+    float va[CH], vb[CH];
+#pragma unroll
+    for (int r = 0; r < CH; ++r) {
+      int i = tid + (r0 + r) * NB_FFT_BLOCK, p = i / K2, z = i - p * K2;
+      int64_t a = plane + (int64_t)(2 * p) * K2 + z;
+      if (FIXED) {
+        va[r] = (float)((double)(long long)fixed[a] * (1.0 / NB_GRID_SCALE));
+        vb[r] = (float)((double)(long long)fixed[a + K2] * (1.0 / NB_GRID_SCALE));
+      } else {
+        va[r] = grid[a];
+        vb[r] = grid[a + K2];
+      }
+    }
+    if (stop) return;
+#pragma unroll
+    for (int r = 0; r < CH; ++r) {
+      int i = tid + (r0 + r) * NB_FFT_BLOCK, p = i / K2, z = i - p * K2;
+      int64_t a = plane + (int64_t)(2 * p) * K2 + z;
+      if (FIXED) {
+        fixed[a] = 0ull;
+        fixed[a + K2] = 0ull;
+      } else {
+        grid[a] = 0.f;
+        grid[a + K2] = 0.f;
+      }
+      S[p * S2 + z] = make_float2(va[r], vb[r]);
+    }
+  }
+  __syncthreads();
+  {
+    constexpr int TH = nb_fft_threads(K2);
+    int g = tid / TH, t = tid - g * TH;
+    for (int l = g; l < Q::SL; l += Q::LA) nb_fft_line<K2, false>(S + l * S2, t, tw2);
+  }
+  __syncthreads();
+  // separate the pairs: A = (Z(k) + conj Z(K2-k))/2, B = (Z(k) - conj Z(K2-k))/2i;
+  // line 0 of T holds DC + i Nyquist (both real) of each row
+  for (int i = tid; i < Q::PR * H; i += NB_FFT_BLOCK) {
+    int p = i / H, kz = i - p * H;
+    float2 z = S[p * S2 + kz], a, b;
+    if (kz == 0) {
+      float2 nq = S[p * S2 + H];
+      a = make_float2(z.x, nq.x);
+      b = make_float2(z.y, nq.y);
+    } else {
+      float2 zc = S[p * S2 + K2 - kz];
+      a = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+      b = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    }
+    T[kz * S1 + 2 * p] = a;
+    T[kz * S1 + 2 * p + 1] = b;
+  }
+  __syncthreads();
+  {
+    constexpr int TH = nb_fft_threads(K1);
+    int g = tid / TH, t = tid - g * TH;
+    for (int l = g; l < Q::TL; l += Q::LB) nb_fft_line<K1, false>(T + l * S1, t, tw1);
+  }
+  __syncthreads();
+  float2 *out = spec + (int64_t)blockIdx.x * K1 * (H + 1);
+#pragma unroll 4
+  for (int i = tid; i < K1 * (H + 1); i += NB_FFT_BLOCK) {
+    int ky = i / (H + 1), kz = i - ky * (H + 1);
+    float2 v;
+    if (kz == 0 || kz == H) {
+      // the two real lines out of their complex sum U = F0 + i FN
+      float2 u = T[ky], w = T[(K1 - ky) & (K1 - 1)];
+      v = kz == 0 ? make_float2(0.5f * (u.x + w.x), 0.5f * (u.y - w.y))
+                  : make_float2(0.5f * (u.y + w.y), -0.5f * (u.x - w.x));
+    } else {
+      v = T[kz * S1 + ky];
+    }
+    out[i] = v;
+  }
+}
+
+template <int K0>
+struct NbFftColumns {
+  static constexpr int L = NB_FFT_BLOCK / nb_fft_threads(K0), S0 = K0 + 1;
+  static constexpr size_t bytes = sizeof(float2) * (size_t)(K0 + L * S0);
+};
+
+// ncols = K1 (K2/2 + 1) columns; block b takes columns b L .. b L + L - 1.
+// Without ENERGY the spectrum is scaled by the f32 table `influence`; with
+// it B C is formed in f64 per point as nb_convolve does and the block's
+// energy and virial go to partials[7 b ..].
+template <int K0, bool ENERGY>
+__global__ void __launch_bounds__(NB_FFT_BLOCK) nb_fft_columns(int64_t ncols, float2 *__restrict__ spec,
+                                                               const float *__restrict__ influence, ConvParams C,
+                                                               const float *__restrict__ moduli,
+                                                               double *__restrict__ partials,
+                                                               const float2 *__restrict__ tw_all,
+                                                               const int *halt) {
+  using Q = NbFftColumns<K0>;
+  constexpr int L = Q::L, S0 = Q::S0;
+  extern __shared__ float2 nb_fft_sm[];
+  float2 *tw = nb_fft_sm, *D = tw + K0;
+  const int tid = threadIdx.x;
+  const int64_t c0 = (int64_t)blockIdx.x * L;
+  static_assert(K0 * L % NB_FFT_BLOCK == 0, "whole columns per pass");
+  constexpr int NB = K0 * L / NB_FFT_BLOCK;  // 8: every load in flight at once
+  // point r of this thread: kx = i / L, column c0 + i % L, i = tid + r NB_FFT_BLOCK
+  float bc[NB];
+  if (!ENERGY) {
+    // the influence table is not written by the kernels before: read before the wait
+#pragma unroll
+    for (int r = 0; r < NB; ++r) {
+      int i = tid + r * NB_FFT_BLOCK, kx = i / L, c = i - kx * L;
+      bc[r] = c0 + c < ncols ? influence[(int64_t)kx * ncols + c0 + c] : 0.f;
+    }
+  }
+  nb_fft_load_tw<K0>(tw, tw_all);
+  nb_grid_wait();
+  const int stop = halt ? *halt : 0;
+  float2 v0[NB];
+#pragma unroll
+  for (int r = 0; r < NB; ++r) {
+    int i = tid + r * NB_FFT_BLOCK, x = i / L, c = i - x * L;
+    v0[r] = c0 + c < ncols ? spec[(int64_t)x * ncols + c0 + c] : make_float2(0.f, 0.f);
+  }
+  if (stop) return;
+#pragma unroll
+  for (int r = 0; r < NB; ++r) {
+    int i = tid + r * NB_FFT_BLOCK, x = i / L, c = i - x * L;
+    D[c * S0 + x] = v0[r];
+  }
+  __syncthreads();
+  constexpr int TH = nb_fft_threads(K0);
+  const int g = tid / TH, t = tid - g * TH;
+  nb_fft_line<K0, false>(D + g * S0, t, tw);
+  __syncthreads();
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int r = 0; r < NB; ++r) {
+    int i = tid + r * NB_FFT_BLOCK, kx = i / L, c = i - kx * L;
+    if (c0 + c >= ncols) continue;
+    int64_t k = (int64_t)kx * ncols + c0 + c;
+    float2 s = D[c * S0 + kx];
+    if (ENERGY) {
+      double m0, m1, m2v, mm;
+      double b = nb_bc(C, moduli, k, m0, m1, m2v, mm);
+      D[c * S0 + kx] = make_float2((float)(s.x * b), (float)(s.y * b));
+      if (k != 0) {
+        int i2 = (int)(k % C.H2);
+        double wgt = (i2 == 0 || (C.K2 % 2 == 0 && i2 == C.K2 / 2)) ? 1.0 : 2.0;
+        double em = 0.5 * wgt * b * ((double)s.x * s.x + (double)s.y * s.y);
+        double f = -2.0 * (1.0 / mm + C.pi2_beta2);
+        v[0] += em;
+        v[1] += em * (1.0 + f * m0 * m0);
+        v[2] += em * (1.0 + f * m1 * m1);
+        v[3] += em * (1.0 + f * m2v * m2v);
+        v[4] += em * f * m0 * m1;
+        v[5] += em * f * m0 * m2v;
+        v[6] += em * f * m1 * m2v;
+      }
+    } else {
+      D[c * S0 + kx] = make_float2(s.x * bc[r], s.y * bc[r]);
+    }
+  }
+  __syncthreads();
+  nb_fft_line<K0, true>(D + g * S0, t, tw);
+  __syncthreads();
+#pragma unroll 4
+  for (int i = tid; i < K0 * L; i += NB_FFT_BLOCK) {
+    int x = i / L, c = i - x * L;
+    if (c0 + c < ncols) spec[(int64_t)x * ncols + c0 + c] = D[c * S0 + x];
+  }
+  if (!ENERGY) return;
+  __shared__ double s_part[NB_FFT_BLOCK / 32][7];
+  int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  }
+  if (lane == 0)
+    for (int k = 0; k < 7; ++k) s_part[warp][k] = v[k];
+  __syncthreads();
+  if (tid < 7) {
+    double s = 0.0;
+    for (int w = 0; w < NB_FFT_BLOCK / 32; ++w) s += s_part[w][tid];
+    partials[(int64_t)blockIdx.x * 7 + tid] = s;
+  }
+}
+
+template <int K1, int K2>
+__global__ void __launch_bounds__(NB_FFT_BLOCK) nb_fft_planes_inv(const float2 *__restrict__ spec,
+                                                                  float *__restrict__ phi,
+                                                                  const float2 *__restrict__ tw_all,
+                                                                  const int *halt) {
+  using Q = NbFftPlane<K1, K2>;
+  constexpr int H = Q::H, S1 = Q::S1, S2 = Q::S2;
+  extern __shared__ float2 nb_fft_sm[];
+  float2 *tw1 = nb_fft_sm, *tw2 = tw1 + K1, *S = tw2 + K2, *T = S + Q::SL * S2;
+  nb_fft_load_tw<K1>(tw1, tw_all);
+  nb_fft_load_tw<K2>(tw2, tw_all);
+  nb_grid_wait();
+  const int stop = halt ? *halt : 0;
+  const int tid = threadIdx.x;
+  const float2 *in = spec + (int64_t)blockIdx.x * K1 * (H + 1);
+  // the plane's spectrum, a chunk of loads in flight at a time
+  constexpr int NC = (K1 * (H + 1) + NB_FFT_BLOCK - 1) / NB_FFT_BLOCK, CH = NC < 9 ? NC : 9;
+#pragma unroll 1
+  for (int r0 = 0; r0 < NC; r0 += CH) {
+    float2 v[CH];
+#pragma unroll
+    for (int r = 0; r < CH; ++r) {
+      int i = tid + (r0 + r) * NB_FFT_BLOCK;
+      v[r] = i < K1 * (H + 1) ? in[i] : make_float2(0.f, 0.f);
+    }
+    if (stop) return;
+#pragma unroll
+    for (int r = 0; r < CH; ++r) {
+      int i = tid + (r0 + r) * NB_FFT_BLOCK, ky = i / (H + 1), kz = i - ky * (H + 1);
+      if (i < K1 * (H + 1) && kz != 0 && kz != H) T[kz * S1 + ky] = v[r];
+    }
+  }
+  for (int ky = tid; ky < K1; ky += NB_FFT_BLOCK) {
+    // the DC and Nyquist lines as one: F0 + i FN
+    float2 f0 = in[ky * (H + 1)], fn = in[ky * (H + 1) + H];
+    T[ky] = make_float2(f0.x - fn.y, f0.y + fn.x);
+  }
+  __syncthreads();
+  {
+    constexpr int TH = nb_fft_threads(K1);
+    int g = tid / TH, t = tid - g * TH;
+    for (int l = g; l < Q::TL; l += Q::LB) nb_fft_line<K1, true>(T + l * S1, t, tw1);
+  }
+  __syncthreads();
+  // rows 2p, 2p + 1 as one line: Z(k) = A(k) + i B(k), Z(K2-k) = conj A(k) + i conj B(k)
+  for (int i = tid; i < Q::PR * H; i += NB_FFT_BLOCK) {
+    int p = i / H, kz = i - p * H;
+    float2 a = T[kz * S1 + 2 * p], b = T[kz * S1 + 2 * p + 1];
+    if (kz == 0) {
+      S[p * S2] = make_float2(a.x, b.x);
+      S[p * S2 + H] = make_float2(a.y, b.y);
+    } else {
+      S[p * S2 + kz] = make_float2(a.x - b.y, a.y + b.x);
+      S[p * S2 + K2 - kz] = make_float2(a.x + b.y, b.x - a.y);
+    }
+  }
+  __syncthreads();
+  {
+    constexpr int TH = nb_fft_threads(K2);
+    int g = tid / TH, t = tid - g * TH;
+    for (int l = g; l < Q::SL; l += Q::LA) nb_fft_line<K2, true>(S + l * S2, t, tw2);
+  }
+  __syncthreads();
+  const int64_t plane = (int64_t)blockIdx.x * K1 * K2;
+#pragma unroll 4
+  for (int i = tid; i < Q::PR * K2; i += NB_FFT_BLOCK) {
+    int p = i / K2, z = i - p * K2;
+    float2 v = S[p * S2 + z];
+    int64_t a = plane + (int64_t)(2 * p) * K2 + z;
+    phi[a] = v.x;
+    phi[a + K2] = v.y;
   }
 }
 
@@ -455,7 +776,114 @@ std::vector<double> host_moduli(int K, int order) {
   return out;
 }
 
+// ---- host side of the three-kernel convolution -----------------------------
+
+template <int K>
+using NbK = std::integral_constant<int, K>;
+
+bool nb_fft_size_ok(int k) { return k == 32 || k == 64 || k == 128; }
+
+// f(NbK<K1>, NbK<K2>) for the plane sizes of the grid.
+template <typename F>
+bool nb_fft_planes(int k1, int k2, F &&f) {
+#define NB_FFT_CASE(A, B)      \
+  if (k1 == A && k2 == B) {    \
+    f(NbK<A>(), NbK<B>());     \
+    return true;               \
+  }
+  NB_FFT_CASE(32, 32) NB_FFT_CASE(32, 64) NB_FFT_CASE(32, 128)
+  NB_FFT_CASE(64, 32) NB_FFT_CASE(64, 64) NB_FFT_CASE(64, 128)
+  NB_FFT_CASE(128, 32) NB_FFT_CASE(128, 64) NB_FFT_CASE(128, 128)
+#undef NB_FFT_CASE
+  return false;
+}
+
+template <typename F>
+bool nb_fft_column(int k0, F &&f) {
+  if (k0 == 32) f(NbK<32>());
+  else if (k0 == 64) f(NbK<64>());
+  else if (k0 == 128) f(NbK<128>());
+  else return false;
+  return true;
+}
+
+template <typename Kern>
+void nb_fft_smem(Kern kernel, size_t bytes) {
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// The shared-memory opt-in of the kernels of a grid (once, at setup: not a
+// stream operation, so not inside a captured step).
+void nb_fft_prepare(const int K[3]) {
+  nb_fft_planes(K[1], K[2], [](auto a, auto b) {
+    constexpr int K1 = decltype(a)::value, K2 = decltype(b)::value;
+    size_t bytes = NbFftPlane<K1, K2>::bytes;
+    nb_fft_smem(nb_fft_planes_fwd<K1, K2, false>, bytes);
+    nb_fft_smem(nb_fft_planes_fwd<K1, K2, true>, bytes);
+    nb_fft_smem(nb_fft_planes_inv<K1, K2>, bytes);
+  });
+  nb_fft_column(K[0], [](auto a) {
+    constexpr int K0 = decltype(a)::value;
+    nb_fft_smem(nb_fft_columns<K0, false>, NbFftColumns<K0>::bytes);
+    nb_fft_smem(nb_fft_columns<K0, true>, NbFftColumns<K0>::bytes);
+  });
+}
+
+// Blocks of the column kernel on a grid.
+int64_t nb_fft_column_blocks(const int K[3]) {
+  int64_t ncols = (int64_t)K[1] * (K[2] / 2 + 1);
+  int L = NB_FFT_BLOCK / nb_fft_threads(K[0]);
+  return (ncols + L - 1) / L;
+}
+
+// The convolution of `grid` (or of the 2^40 fixed-point `fixed`, when
+// non-null) into the potential `phi`, through `spec`; empties the grid it
+// read.  energy: B C formed per point with the sums into partials (one
+// block of seven per column block); else the table `influence`.  Launched
+// chained after the spreading on s.
+int nb_fft_convolve(const NbPme &P, float *grid, unsigned long long *fixed, float2 *spec, float *phi,
+                    const float *influence, bool energy, const ConvParams &C, double *partials, const int *halt,
+                    cudaStream_t s) {
+  const int *K = P.K;
+  const float2 *tw = P.fft_tw;
+  int64_t ncols = (int64_t)K[1] * (K[2] / 2 + 1);
+  cudaError_t e = cudaSuccess;
+  bool ok = nb_fft_planes(K[1], K[2], [&](auto a, auto b) {
+    constexpr int K1 = decltype(a)::value, K2 = decltype(b)::value;
+    size_t bytes = NbFftPlane<K1, K2>::bytes;
+    if (fixed)
+      e = nb_launch_chained(nb_fft_planes_fwd<K1, K2, true>, dim3(K[0]), dim3(NB_FFT_BLOCK), bytes, s, grid, fixed,
+                            spec, tw, halt);
+    else
+      e = nb_launch_chained(nb_fft_planes_fwd<K1, K2, false>, dim3(K[0]), dim3(NB_FFT_BLOCK), bytes, s, grid, fixed,
+                            spec, tw, halt);
+  });
+  if (!ok || e != cudaSuccess) return -3;
+  ok = nb_fft_column(K[0], [&](auto a) {
+    constexpr int K0 = decltype(a)::value;
+    dim3 blocks((unsigned)nb_fft_column_blocks(K));
+    size_t bytes = NbFftColumns<K0>::bytes;
+    if (energy)
+      e = nb_launch_chained(nb_fft_columns<K0, true>, blocks, dim3(NB_FFT_BLOCK), bytes, s, ncols, spec, influence,
+                            C, (const float *)P.moduli, partials, tw, halt);
+    else
+      e = nb_launch_chained(nb_fft_columns<K0, false>, blocks, dim3(NB_FFT_BLOCK), bytes, s, ncols, spec, influence,
+                            C, (const float *)P.moduli, partials, tw, halt);
+  });
+  if (!ok || e != cudaSuccess) return -3;
+  nb_fft_planes(K[1], K[2], [&](auto a, auto b) {
+    constexpr int K1 = decltype(a)::value, K2 = decltype(b)::value;
+    e = nb_launch_chained(nb_fft_planes_inv<K1, K2>, dim3(K[0]), dim3(NB_FFT_BLOCK), NbFftPlane<K1, K2>::bytes, s,
+                          (const float2 *)spec, phi, tw, halt);
+  });
+  return e == cudaSuccess ? 0 : -3;
+}
+
 }  // namespace
+
+// The own transforms serve this context's grid (every K 32, 64 or 128) and
+// are not switched off.
+bool nb_fft_own(const NbCtx &c) { return c.pme.fft_tw != nullptr && c.pme_fft == 0; }
 
 int nb_pme_setup(NbCtx &c, int k0, int k1, int k2, int order) {
   nb_pme_release(c);
@@ -484,6 +912,18 @@ int nb_pme_setup(NbCtx &c, int k0, int k1, int k2, int order) {
   cudaMemcpy(P.moduli, mod.data(), sizeof(float) * mod.size(), cudaMemcpyHostToDevice);
   if (cufftPlan3d(&P.fwd, k0, k1, k2, CUFFT_R2C) != CUFFT_SUCCESS) return -3;
   if (cufftPlan3d(&P.bwd, k0, k1, k2, CUFFT_C2R) != CUFFT_SUCCESS) return -3;
+  if (nb_fft_size_ok(k0) && nb_fft_size_ok(k1) && nb_fft_size_ok(k2)) {
+    // e^(-2 pi i e/K) for K = 32, 64, 128, formed in f64
+    std::vector<float2> tw(NB_FFT_TW_TOTAL);
+    for (int K : {32, 64, 128})
+      for (int e = 0; e < K; ++e) {
+        double a = -2.0 * M_PI * (double)e / (double)K;
+        tw[nb_fft_tw_offset(K) + e] = make_float2((float)std::cos(a), (float)std::sin(a));
+      }
+    if (cudaMalloc(&P.fft_tw, sizeof(float2) * NB_FFT_TW_TOTAL) != cudaSuccess) return -1;
+    cudaMemcpy(P.fft_tw, tw.data(), sizeof(float2) * NB_FFT_TW_TOTAL, cudaMemcpyHostToDevice);
+    nb_fft_prepare(P.K);
+  }
   if (c.places_cap > 0) {
     if (cudaMalloc(&P.pme_force, sizeof(float4) * c.places_cap) != cudaSuccess) return -1;
     if (cudaMalloc(&P.potential, sizeof(float) * c.places_cap) != cudaSuccess) return -1;
@@ -499,8 +939,9 @@ void nb_pme_release(NbCtx &c) {
   P.fwd = P.bwd = 0;
   for (void *p : {(void *)P.grid, (void *)P.spec, (void *)P.fixed, (void *)P.moduli,
                   (void *)P.pme_force, (void *)P.potential, (void *)P.partials, (void *)P.adj_grid,
-                  (void *)P.influence})
+                  (void *)P.influence, (void *)P.fft_tw})
     if (p) cudaFree(p);
+  P.fft_tw = nullptr;
   P.adj_grid = nullptr;
   P.influence = nullptr;
   P.grid = nullptr;
@@ -577,10 +1018,8 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
     case 8: SPREAD(8); break;
   }
 #undef SPREAD
-  if (c.deterministic) nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, P.fixed, P.grid);
-  cufftSetStream(P.fwd, s);
-  cufftSetStream(P.bwd, s);
-  if (cufftExecR2C(P.fwd, P.grid, (cufftComplex *)P.spec) != CUFFT_SUCCESS) return -3;
+  bool own = nb_fft_own(c);
+  if (c.deterministic && !own) nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, P.fixed, P.grid);
   ConvParams C;
   C.K0 = G.K0;
   C.K1 = G.K1;
@@ -592,14 +1031,26 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
   C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
   C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
   nb_cell_tilts(c, box, G, &C);
-  if (energy) {
-    nb_convolve<true><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
-    nb_pme_sum<<<1, 256, 0, s>>>(P.partials, P.conv_blocks, c.energy);
+  if (own) {
+    // spread grid -> potential in P.grid, the fixed-point grid read directly
+    if (!energy && nb_pme_table(c, box, s)) return -1;
+    if (nb_fft_convolve(P, P.grid, c.deterministic ? P.fixed : nullptr, P.spec, P.grid, P.influence, energy, C,
+                        P.partials, nullptr, s))
+      return -3;
+    if (energy) nb_pme_sum<<<1, 256, 0, s>>>(P.partials, (int)nb_fft_column_blocks(P.K), c.energy);
   } else {
-    if (nb_pme_table(c, box, s)) return -1;
-    nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, P.influence, P.spec, nullptr, 0, nullptr);
+    cufftSetStream(P.fwd, s);
+    cufftSetStream(P.bwd, s);
+    if (cufftExecR2C(P.fwd, P.grid, (cufftComplex *)P.spec) != CUFFT_SUCCESS) return -3;
+    if (energy) {
+      nb_convolve<true><<<blocks_for(half, 256), 256, 0, s>>>(C, P.moduli, P.spec, P.partials);
+      nb_pme_sum<<<1, 256, 0, s>>>(P.partials, P.conv_blocks, c.energy);
+    } else {
+      if (nb_pme_table(c, box, s)) return -1;
+      nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, P.influence, P.spec, nullptr, 0, nullptr);
+    }
+    if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.grid) != CUFFT_SUCCESS) return -3;
   }
-  if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.grid) != CUFFT_SUCCESS) return -3;
   float *pot = potential ? P.potential : nullptr;
   int blocks = blocks_for(c.places_cap, 128);
   float4 *pf = (float4 *)P.pme_force;
@@ -650,7 +1101,6 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s) 
     case 6: nb_spread_dipole<6><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.adj_grid); break;
     case 8: nb_spread_dipole<8><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.adj_grid); break;
   }
-  if (cufftExecR2C(P.fwd, P.adj_grid, (cufftComplex *)P.spec) != CUFFT_SUCCESS) return -3;
   ConvParams C;
   C.K0 = G.K0;
   C.K1 = G.K1;
@@ -662,8 +1112,15 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s) 
   C.pref = c.coulomb / (M_PI * box[0] * box[1] * box[2]);
   C.pi2_beta2 = M_PI * M_PI / (c.beta * c.beta);
   if (nb_pme_table(c, box, s)) return -1;
-  nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, P.influence, P.spec, nullptr, 0, nullptr);
-  if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.adj_grid) != CUFFT_SUCCESS) return -3;
+  if (nb_fft_own(c)) {
+    // V -> psi in place, three kernels
+    if (nb_fft_convolve(P, P.adj_grid, nullptr, P.spec, P.adj_grid, P.influence, false, C, nullptr, nullptr, s))
+      return -3;
+  } else {
+    if (cufftExecR2C(P.fwd, P.adj_grid, (cufftComplex *)P.spec) != CUFFT_SUCCESS) return -3;
+    nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, P.influence, P.spec, nullptr, 0, nullptr);
+    if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.adj_grid) != CUFFT_SUCCESS) return -3;
+  }
   switch (P.order) {
     case 4: nb_pme_adjoint_gather<4, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
     case 5: nb_pme_adjoint_gather<5, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
@@ -1033,16 +1490,23 @@ int nb_pme_md_chain(NbCtx &c, const double box[3], float *qgrid, unsigned long l
   int64_t total = (int64_t)G.K0 * G.K1 * G.K2;
   int64_t half = (int64_t)G.K0 * G.K1 * (G.K2 / 2 + 1);
   int64_t threads = c.places_cap * 4;
-  if (c.deterministic) {
-    // the fixed-point grid is empty: its conversion empties it
+  if (c.deterministic)
     nb_spread<4, true><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, qgrid,
                                                                 qfixed, halt);
-    nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, qfixed, qgrid);
-  } else {
-    // the grid is empty: the spectrum scaling of the last chain emptied it
+  else
     nb_spread<4, false><<<blocks_for(threads, 256), 256, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, qgrid,
                                                                  qfixed, halt);
+  if (nb_fft_own(c)) {
+    // the spread grid (empty before the spreading: this chain's forward
+    // plane kernel empties it, or in the deterministic mode the fixed-point
+    // grid, read directly) -> spectrum -> phi in three kernels
+    ConvParams C{};
+    return nb_fft_convolve(P, qgrid, c.deterministic ? qfixed : nullptr, spec, phi, influence, false, C, nullptr,
+                           halt, s);
   }
+  // the grid is empty: the conversion of the fixed-point grid empties that
+  // one, the spectrum scaling of the last chain this one
+  if (c.deterministic) nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, qfixed, qgrid);
   cufftSetStream(P.fwd, s);
   cufftSetStream(P.bwd, s);
   if (cufftExecR2C(P.fwd, qgrid, (cufftComplex *)spec) != CUFFT_SUCCESS) return -3;

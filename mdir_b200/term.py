@@ -120,10 +120,13 @@ class NonbondedTerm:
         b = _host(self.box if box is None else box, np.float64)
         L.check(L.lib().mdrtNbPrune(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtNbPrune")
 
-    def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None, fused_prune=None, staging_depth=None):
-        """Launch shapes and the MD step's pruning in the pair kernel (0 by
-        group count, 1 always, 2 never): the autotuner's knobs; results do
-        not depend on them beyond the order of f32 sums."""
+    def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None, fused_prune=None, staging_depth=None,
+                   pme_fft=None):
+        """Launch shapes, the MD step's pruning in the pair kernel (0 by
+        group count, 1 always, 2 never) and the PME transforms ("own", the
+        library's three-kernel convolution where every grid dimension is 32,
+        64 or 128; "cufft"): the autotuner's knobs; results do not depend on
+        them beyond the order of f32 sums."""
         if pair_blocks_per_sm is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_BLOCKS_PER_SM, int(pair_blocks_per_sm)),
                     "mdrtNbSetTuning")
@@ -137,6 +140,10 @@ class NonbondedTerm:
         if fused_prune is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_FUSED_PRUNE, int(fused_prune)), "mdrtNbSetTuning")
             self.fused_prune = int(fused_prune)
+        if pme_fft is not None:
+            code = {"own": 0, "cufft": 1}[pme_fft]
+            L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PME_FFT, code), "mdrtNbSetTuning")
+            self.pme_fft = pme_fft
 
     def set_deterministic(self, on=True):
         L.check(L.lib().mdrtNbSetDeterministic(self._h, int(bool(on))), "mdrtNbSetDeterministic")
