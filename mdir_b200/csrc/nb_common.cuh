@@ -113,6 +113,13 @@ __device__ __forceinline__ float3 nb_lattice_shift(int na, int nb, int nc, const
 // becomes a programmatic edge, which hides most of the launch gap between
 // the dependent kernels of the MD step.
 __device__ __forceinline__ void nb_grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the chained kernel after this one launch once every block of this
+// grid has called it (or exited): the dependent's blocks then run their work
+// before nb_grid_wait() beside this kernel's.  Called by a persistent kernel
+// whose blocks are all resident, it cannot hold back blocks of its own grid.
+__device__ __forceinline__ void nb_grid_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 template <typename... KArgs, typename... Args>
 static inline cudaError_t nb_launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,

@@ -332,18 +332,42 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     int p = act ? wplace[3 * w + k] : -1;
     int base = 3 * wl, s1 = base + (k + 1) % 3, s2 = base + (k + 2) % 3;
     if (lane >= 30) s1 = s2 = base = lane;
-    // every load that the pair kernel before does not write first (on a
-    // chained launch they overlap its last blocks), then the wait
+    // every load of data that no kernel of this step writes (the pair
+    // kernel lets this launch start beside it, so the step's pruning may not
+    // have flushed), then the wait
     Vec3 x0 = load3(x, a), v0 = load3(v, a);
     double q = charge[a], im = inv_mass[a], ms = mass[a];
     Vec3 xr = load3(x_ref, a);
-    Vec3 xpr = U.prune_half2 > 0.0 ? load3(x_prune, a) : xr;
     char4 sh = p >= 0 ? shift[p] : make_char4(0, 0, 0, 0);
     float4 fr = p >= 0 ? xq[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float qw = p >= 0 ? fr.w : 0.f;
+    // the PME gather (the potential comes from the reciprocal chain, which
+    // the launch depends on in full) and the excluded pair (k, k+1) of this
+    // water (positions only) need nothing of the pair kernel: both run
+    // before the wait, beside that kernel's last units
+    Vec3 fg = {0.0, 0.0, 0.0};
+    if (p >= 0 && U.pme_fused && qw != 0.f) fg = md_pme_gather(fr, U.phi, U.G);
+    Vec3 x1 = shfl3(x0, s1);
+    double q1 = __shfl_sync(0xffffffffu, q, s1);
+    Vec3 fp = {0.0, 0.0, 0.0};
+    if (U.water_excl && act) {
+      Vec3 d = x0 - x1;
+      d.x -= U.L[0] * rint(d.x / U.L[0]);
+      d.y -= U.L[1] * rint(d.y / U.L[1]);
+      d.z -= U.L[2] * rint(d.z / U.L[2]);
+      double r2 = dot(d, d), qq = U.coulomb * q * q1;
+      if (qq != 0.0 && r2 > 0.0) {
+        double r = sqrt(r2);
+        double fs = qq * (U.two_beta_sqrtpi * exp(-U.beta * U.beta * r2) / r2 - erf(U.beta * r) / (r2 * r));
+        fp = fs * d;
+      }
+    }
     nb_grid_wait();
     if (halt) return;
+    // the positions of the last pruning: a pruning of this step (before the
+    // pair kernel) writes them
+    Vec3 xpr = U.prune_half2 > 0.0 ? load3(x_prune, a) : xr;
     Vec3 f = {0.0, 0.0, 0.0};
-    float qw = 0.f;
     if (p >= 0) {
       if (U.fixed) {
         long long fx = (long long)accf[3 * p], fy = (long long)accf[3 * p + 1], fz = (long long)accf[3 * p + 2];
@@ -358,28 +382,10 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
         f.y += w4.y;
         f.z += w4.z;
       }
-      qw = fr.w;
       if (U.pme_fused && qw != 0.f) {
-        Vec3 fg = md_pme_gather(fr, U.phi, U.G);
         f.x += fg.x;
         f.y += fg.y;
         f.z += fg.z;
-      }
-    }
-    // the excluded pair (k, k+1) of this water
-    Vec3 x1 = shfl3(x0, s1);
-    double q1 = __shfl_sync(0xffffffffu, q, s1);
-    Vec3 fp = {0.0, 0.0, 0.0};
-    if (U.water_excl && act) {
-      Vec3 d = x0 - x1;
-      d.x -= U.L[0] * rint(d.x / U.L[0]);
-      d.y -= U.L[1] * rint(d.y / U.L[1]);
-      d.z -= U.L[2] * rint(d.z / U.L[2]);
-      double r2 = dot(d, d), qq = U.coulomb * q * q1;
-      if (qq != 0.0 && r2 > 0.0) {
-        double r = sqrt(r2);
-        double fs = qq * (U.two_beta_sqrtpi * exp(-U.beta * U.beta * r2) / r2 - erf(U.beta * r) / (r2 * r));
-        fp = fs * d;
       }
     }
     // this atom: + its own pair, - the pair (k-1, k) of the lane before
@@ -423,13 +429,17 @@ __global__ void __launch_bounds__(MD_UPDATE_THREADS) md_update(
     int64_t t = (int64_t)(blockIdx.x - water_blocks) * blockDim.x + threadIdx.x;
     int i = free_atoms[t];
     int pi = fplace[t];
+    Vec3 fg = {0.0, 0.0, 0.0};
+    bool gather = false;
+    if (U.pme_fused && pi >= 0) {
+      float4 fr = xq[pi];
+      gather = fr.w != 0.f;
+      if (gather) fg = md_pme_gather(fr, U.phi, U.G);
+    }
     nb_grid_wait();
     if (halt) return;
     Vec3 fi = take_force(pi, acc, accf, pme, U.fixed);
-    if (U.pme_fused && pi >= 0) {
-      float4 fr = xq[pi];
-      if (fr.w != 0.f) fi = fi + md_pme_gather(fr, U.phi, U.G);
-    }
+    if (gather) fi = fi + fg;
     Vec3 vi = lambda * load3(v, i) + (dt * inv_mass[i]) * fi;
     Vec3 xi = load3(x, i) + dt * vi;
     store3(x, i, xi);
@@ -533,11 +543,23 @@ __device__ void md_last_block(const UpdateParams &U, const double *ke_part, cons
   __shared__ float s_m[MD_UPDATE_THREADS / 32][2];
   double v = 0.0;
   float dmax = 0.f, pmax = 0.f;
-  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-    v += __ldcg(ke_part + b);
-    float2 mb = __ldcg(blk_max + b);
-    dmax = fmaxf(dmax, mb.x);
-    pmax = fmaxf(pmax, mb.y);
+  // eight partials a thread in flight at a time, summed in the order of b
+  constexpr int CH = 8;
+  for (int b0 = threadIdx.x; b0 < nblocks; b0 += CH * blockDim.x) {
+    double kp[CH];
+    float2 mb[CH];
+#pragma unroll
+    for (int r = 0; r < CH; ++r) {
+      int b = b0 + r * blockDim.x;
+      kp[r] = b < nblocks ? __ldcg(ke_part + b) : 0.0;
+      mb[r] = b < nblocks ? __ldcg(blk_max + b) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int r = 0; r < CH; ++r) {
+      if (b0 + r * (int)blockDim.x < nblocks) v += kp[r];
+      dmax = fmaxf(dmax, mb[r].x);
+      pmax = fmaxf(pmax, mb[r].y);
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {

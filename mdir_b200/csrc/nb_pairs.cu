@@ -400,6 +400,9 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
                                                 float4 *__restrict__ acc, unsigned long long *__restrict__ accf,
                                                 double *__restrict__ partials, int *__restrict__ status,
                                                 const int *halt, const int *skip) {
+  // the MD step's update may start its loads, its PME gather and its
+  // excluded pairs beside this kernel; it waits for these forces
+  nb_grid_launch_dependents();
   nb_grid_wait();  // the lists and frames of the kernels before (a chained launch)
   if (halt && *halt) return;  // the MD step stopped at a stale list (its host rebuilds)
   if (skip && *skip) return;  // a pruning step: the pruning kernel computed the pairs
