@@ -254,8 +254,11 @@ void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream
 // With `halt` (device), nothing when *halt is set (the MD step's stop).
 // With `skip` (device), nothing when *skip is set (a pruning step whose
 // pairs nb_prune_pairs_run computed).
+// With `update_after`, the kernel lets the chained launch after it (the MD
+// step's update) start beside it once its persistent blocks are resident;
+// kept off where pair launches follow one another.
 void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt = nullptr,
-                  const int *skip = nullptr);
+                  const int *skip = nullptr, bool update_after = false);
 // The pruning of a pruning step with the pairs of its fresh inner lists in
 // one kernel (MDIR D284), when *gate (device) is set: the same inner lists
 // and claimed units as nb_prune_gated, the forces of the pairs added.

@@ -724,10 +724,10 @@ static void md_step_body(mdrtMd &m, double *x, double *v, const double box[3], d
     // a pruning step prunes and computes its pairs in one kernel (MDIR
     // D284); the pair kernel after it then returns at once
     nb_prune_pairs_run(c, box, m.flag + 1, x, m.x_prune, m.thermo + 5, md_unit_counter(m), s, flag + 3);
-    nb_pairs_run(c, box, false, s, flag + 3, m.flag + 1);
+    nb_pairs_run(c, box, false, s, flag + 3, m.flag + 1, m.n_excl_other == 0);
   } else {
     md_prune_step(m, x, box, s);
-    nb_pairs_run(c, box, false, s, flag + 3);
+    nb_pairs_run(c, box, false, s, flag + 3, nullptr, m.n_excl_other == 0);
   }
   if (m.n_excl_other > 0) nb_excluded_list_run(c, box, m.excl_other, m.n_excl_other, s);
   if (pme) {

@@ -39,6 +39,7 @@ struct PairParams {
   float Lx, Ly, Lz;
   float bx, cx, cy;  // tilts of a triclinic cell (0: orthorhombic)
   double Ld[6];      // the cell in f64 (ax, by, cz, bx, cx, cy): the exact image shifts of the split frames
+  int update_after;  // the MD step: the update chained after the kernel may start beside it
   float rc2;
   float beta;
   float beta_p;         // p beta, p of the erfc approximation below
@@ -402,7 +403,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
                                                 const int *halt, const int *skip) {
   // the MD step's update may start its loads, its PME gather and its
   // excluded pairs beside this kernel; it waits for these forces
-  nb_grid_launch_dependents();
+  if (P.update_after) nb_grid_launch_dependents();
   nb_grid_wait();  // the lists and frames of the kernels before (a chained launch)
   if (halt && *halt) return;  // the MD step stopped at a stale list (its host rebuilds)
   if (skip && *skip) return;  // a pruning step: the pruning kernel computed the pairs
@@ -1055,6 +1056,7 @@ void ensure_sm_count() {
 
 PairParams pair_params(const NbCtx &c, const double box[3]) {
   PairParams P;
+  P.update_after = 0;
   P.Lx = (float)box[0];
   P.Ly = (float)box[1];
   P.Lz = (float)box[2];
@@ -1139,9 +1141,11 @@ void nb_prune_pairs_run(NbCtx &c, const double box[3], const int *gate, const do
 #undef NB_FUSED_LAUNCH
 }
 
-void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt, const int *skip) {
+void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, const int *halt, const int *skip,
+                  bool update_after) {
   ensure_sm_count();
   PairParams P = pair_params(c, box);
+  P.update_after = update_after ? 1 : 0;
   // persistent grid: enough warps for the units, `pair_blocks_per_sm`
   // blocks of 8 warps per SM (4 fit at 64 registers; fewer leave room for
   // the PME kernels that run beside it on another stream)

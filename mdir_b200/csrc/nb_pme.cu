@@ -75,13 +75,26 @@ __global__ void __launch_bounds__(256) nb_spread(GridParams G, int64_t places,
   }
 }
 
+// The fixed-point grid to f32, emptied behind: four points a thread with
+// 16-byte loads and stores (the last total % 4 points one at a time).
 __global__ void nb_fixed_to_grid(int64_t total, unsigned long long *__restrict__ fixed,
                                  float *__restrict__ grid) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= total) return;
-  long long v = (long long)fixed[k];
-  fixed[k] = 0ull;
-  grid[k] = (float)((double)v * (1.0 / NB_GRID_SCALE));
+  int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (k + 4 <= total) {
+    ulonglong2 a = *(const ulonglong2 *)(fixed + k), b = *(const ulonglong2 *)(fixed + k + 2);
+    *(ulonglong2 *)(fixed + k) = make_ulonglong2(0ull, 0ull);
+    *(ulonglong2 *)(fixed + k + 2) = make_ulonglong2(0ull, 0ull);
+    *(float4 *)(grid + k) = make_float4((float)((double)(long long)a.x * (1.0 / NB_GRID_SCALE)),
+                                        (float)((double)(long long)a.y * (1.0 / NB_GRID_SCALE)),
+                                        (float)((double)(long long)b.x * (1.0 / NB_GRID_SCALE)),
+                                        (float)((double)(long long)b.y * (1.0 / NB_GRID_SCALE)));
+  } else {
+    for (; k < total; ++k) {
+      long long v = (long long)fixed[k];
+      fixed[k] = 0ull;
+      grid[k] = (float)((double)v * (1.0 / NB_GRID_SCALE));
+    }
+  }
 }
 
 struct ConvParams {
@@ -1019,7 +1032,7 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
   }
 #undef SPREAD
   bool own = nb_fft_own(c);
-  if (c.deterministic && !own) nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, P.fixed, P.grid);
+  if (c.deterministic && !own) nb_fixed_to_grid<<<blocks_for((total + 3) / 4, 256), 256, 0, s>>>(total, P.fixed, P.grid);
   ConvParams C;
   C.K0 = G.K0;
   C.K1 = G.K1;
@@ -1506,7 +1519,7 @@ int nb_pme_md_chain(NbCtx &c, const double box[3], float *qgrid, unsigned long l
   }
   // the grid is empty: the conversion of the fixed-point grid empties that
   // one, the spectrum scaling of the last chain this one
-  if (c.deterministic) nb_fixed_to_grid<<<blocks_for(total, 256), 256, 0, s>>>(total, qfixed, qgrid);
+  if (c.deterministic) nb_fixed_to_grid<<<blocks_for((total + 3) / 4, 256), 256, 0, s>>>(total, qfixed, qgrid);
   cufftSetStream(P.fwd, s);
   cufftSetStream(P.bwd, s);
   if (cufftExecR2C(P.fwd, qgrid, (cufftComplex *)spec) != CUFFT_SUCCESS) return -3;
