@@ -284,6 +284,24 @@ int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3
                                 const double *cotangent, int32_t mode, double *dq,
                                 double *dtable, void *stream);
 
+/* The reciprocal potential grid phi of the last force evaluation that ran
+ * PME (K1 x K2 x K3 f32 in the grid's layout, the third index fastest) to
+ * `grid` (device), asynchronous on `stream`; MDRT_NB_INVALID_ARGUMENT
+ * without PME.  Kept for each frame, it spares the parameter gradient the
+ * reciprocal forward (mdrtNbParameterGradientPotential).
+ * MDIR: the potential grid of the PME stages (D231), which the vjp of
+ * python/mdir/_frames.py:327 recomputes. */
+int32_t mdrtPmePotentialGrid(mdrtNb *ctx, float *grid, void *stream);
+
+/* mdrtNbParameterGradient with the potential grid phi that
+ * mdrtPmePotentialGrid kept from the force evaluation at the same x,
+ * charges and cell: the reciprocal forward is not run again.  phi NULL:
+ * the same as mdrtNbParameterGradient.  A phi of other positions or
+ * charges gives a wrong gradient; nothing checks it. */
+int32_t mdrtNbParameterGradientPotential(mdrtNb *ctx, const double *x, const double box[3],
+                                         const double *cotangent, int32_t mode, const float *phi,
+                                         double *dq, double *dtable, void *stream);
+
 /* A device pointer to a buffer of the neighbor structure and its element
  * count (a view; invalidated by the next build that grows).
  * MDIR: _mlir_ciface_mdrtGroupsBuffer(result, handle, slot),

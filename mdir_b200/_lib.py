@@ -50,6 +50,8 @@ SIGNATURES = {
     "mdrtPmePotential": (_i32, [_p, _p, _p]),
     "mdrtNbDisplacement": (_i32, [_p, _p, _i64, _p, _p, _p]),
     "mdrtNbParameterGradient": (_i32, [_p, _p, _p, _p, _i32, _p, _p, _p]),
+    "mdrtNbParameterGradientPotential": (_i32, [_p, _p, _p, _p, _i32, _p, _p, _p, _p]),
+    "mdrtPmePotentialGrid": (_i32, [_p, _p, _p]),
     "mdrtNbGroupsBuffer": (_i32, [_p, _i32, ctypes.POINTER(_p), ctypes.POINTER(_i64)]),
     "mdrtNbGroupsInfo": (_i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "mdrtNbStatus": (_i32, [_p, _p, _i32, ctypes.POINTER(_i32)]),

@@ -489,6 +489,19 @@ int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, con
 
 int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3], const double *cotangent,
                                 int32_t mode, double *dq, double *dtable, void *stream) {
+  return mdrtNbParameterGradientPotential(ctx, x, box, cotangent, mode, nullptr, dq, dtable, stream);
+}
+
+int32_t mdrtPmePotentialGrid(mdrtNb *ctx, float *grid, void *stream) {
+  if (!ctx || !grid || !ctx->c.pme.on) return MDRT_NB_INVALID_ARGUMENT;
+  CK(cudaSetDevice(ctx->c.device));
+  if (nb_pme_potential_grid(ctx->c, grid, (cudaStream_t)stream)) return MDRT_NB_CUDA_ERROR;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbParameterGradientPotential(mdrtNb *ctx, const double *x, const double box[3],
+                                         const double *cotangent, int32_t mode, const float *phi, double *dq,
+                                         double *dtable, void *stream) {
   if (!ctx || !x || !box || !dq || !dtable) return MDRT_NB_INVALID_ARGUMENT;
   if (mode != MDRT_NB_GRAD_PRODUCT && mode != MDRT_NB_GRAD_ENERGY) return MDRT_NB_INVALID_ARGUMENT;
   if (mode == MDRT_NB_GRAD_PRODUCT && !cotangent) return MDRT_NB_INVALID_ARGUMENT;
@@ -503,7 +516,8 @@ int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3
   if (c.lj_switch) return MDRT_NB_UNSUPPORTED;
   CK(cudaSetDevice(c.device));
   if (nb_adjoint_reserve(c)) return MDRT_NB_CUDA_ERROR;
-  if (nb_adjoint_run(c, x, box, cotangent, mode, dq, dtable, (cudaStream_t)stream)) return MDRT_NB_CUDA_ERROR;
+  if (phi && !c.pme.on) return MDRT_NB_INVALID_ARGUMENT;
+  if (nb_adjoint_run(c, x, box, cotangent, mode, dq, dtable, (cudaStream_t)stream, phi)) return MDRT_NB_CUDA_ERROR;
   CK(cudaGetLastError());
   return MDRT_NB_OK;
 }

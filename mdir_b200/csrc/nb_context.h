@@ -291,9 +291,12 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
 // epsilon entries).  Needs the adjoint scratch (nb_adjoint_reserve).
 int nb_adjoint_reserve(NbCtx &c);
 int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double *cotangent, int mode,
-                   double *dq, double *dtable, cudaStream_t s);
+                   double *dq, double *dtable, cudaStream_t s, const float *phi = nullptr);
 // The reciprocal part of the charge gradient, added per place into c.adj_q.
-int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s);
+int nb_pme_potential_grid(NbCtx &c, float *out, cudaStream_t s);
+// With phi (a potential grid kept from the force evaluation at the same
+// frames and charges), the reciprocal forward is not run again.
+int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s, const float *phi = nullptr);
 
 // The MD step's reciprocal chain when the update gathers (order 4): the
 // frames spread into qgrid (through qfixed, empty, in the deterministic

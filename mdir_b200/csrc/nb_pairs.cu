@@ -1262,7 +1262,7 @@ int nb_adjoint_reserve(NbCtx &c) {
 }
 
 int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double *cot, int mode, double *dq,
-                   double *dtable, cudaStream_t s) {
+                   double *dtable, cudaStream_t s, const float *phi) {
   PairParams P = pair_params(c, box);
   nb_gather_frames(c, x, box, s);
   if (mode == 0)
@@ -1282,7 +1282,7 @@ int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double 
                                              c.adj_q, c.adj_types);
   int width = 2 * c.ntypes * c.ntypes;
   nb_sum_type_partials<<<blocks_for((int64_t)width * 32, 256), 256, 0, s>>>(c.adj_types, grid, width, dtable);
-  int rc = nb_pme_adjoint_run(c, box, mode, s);
+  int rc = nb_pme_adjoint_run(c, box, mode, s, phi);
   if (rc) return rc;
   nb_scatter_place_values<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.adj_q,
                                                                         dq);

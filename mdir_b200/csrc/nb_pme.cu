@@ -1081,7 +1081,7 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
 // influence, inverse FFT); in mode 0 the dipole grid V goes through the same
 // FFT pair and influence to give psi.  The dipole spread uses f32 atomics
 // in both modes of the forward (deterministic or not).
-int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s) {
+int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s, const float *phi) {
   NbPme &P = c.pme;
   if (!P.on) return 0;
   GridParams G;
@@ -1094,15 +1094,18 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s) 
   int64_t total = (int64_t)G.K0 * G.K1 * G.K2;
   int64_t half = (int64_t)G.K0 * G.K1 * (G.K2 / 2 + 1);
   if (!P.adj_grid && cudaMalloc(&P.adj_grid, sizeof(float) * total) != cudaSuccess) return -2;
-  int rc = nb_pme_run(c, box, false, false, s);  // phi in P.grid
-  if (rc) return rc;
+  if (!phi) {
+    int rc = nb_pme_run(c, box, false, false, s);  // phi in P.grid
+    if (rc) return rc;
+    phi = P.grid;
+  }
   int blocks = blocks_for(c.places_cap, 128);
   if (mode == 1) {
     switch (P.order) {
-      case 4: nb_pme_adjoint_gather<4, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, P.grid, nullptr, c.adj_q); break;
-      case 5: nb_pme_adjoint_gather<5, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, P.grid, nullptr, c.adj_q); break;
-      case 6: nb_pme_adjoint_gather<6, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, P.grid, nullptr, c.adj_q); break;
-      case 8: nb_pme_adjoint_gather<8, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, P.grid, nullptr, c.adj_q); break;
+      case 4: nb_pme_adjoint_gather<4, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
+      case 5: nb_pme_adjoint_gather<5, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
+      case 6: nb_pme_adjoint_gather<6, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
+      case 8: nb_pme_adjoint_gather<8, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
     }
     return 0;
   }
@@ -1135,10 +1138,10 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s) 
     if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.adj_grid) != CUFFT_SUCCESS) return -3;
   }
   switch (P.order) {
-    case 4: nb_pme_adjoint_gather<4, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
-    case 5: nb_pme_adjoint_gather<5, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
-    case 6: nb_pme_adjoint_gather<6, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
-    case 8: nb_pme_adjoint_gather<8, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, P.grid, P.adj_grid, c.adj_q); break;
+    case 4: nb_pme_adjoint_gather<4, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
+    case 5: nb_pme_adjoint_gather<5, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
+    case 6: nb_pme_adjoint_gather<6, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
+    case 8: nb_pme_adjoint_gather<8, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
   }
   return 0;
 }
@@ -1481,6 +1484,15 @@ int nb_batch_pme_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
     nb_batch_gather_split<8><<<blocks_for(c.places_cap * 8, 128), 128, 0, s>>>(
         c.places_cap, c.sizes, c.order, b.atom_frame, b.frames_dev, c.xq, P.grid, pf);
   return 0;
+}
+
+// The potential grid of the last force evaluation (K0 K1 K2 f32, in P.grid)
+// to `out` (device), on s.
+int nb_pme_potential_grid(NbCtx &c, float *out, cudaStream_t s) {
+  NbPme &P = c.pme;
+  if (!P.on) return -2;
+  int64_t total = (int64_t)P.K[0] * P.K[1] * P.K[2];
+  return cudaMemcpyAsync(out, P.grid, sizeof(float) * total, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? 0 : -1;
 }
 
 // ---------------------------------------------------------------------------

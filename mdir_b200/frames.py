@@ -138,7 +138,7 @@ class FrameEvaluator:
     the tensors of a call may be freed or reused on that stream at once
     (torch's allocator hands a block back only to the stream it was made on)."""
 
-    def __init__(self, system, device=0, sigma=None, epsilon=None, charges=None, lanes=4):
+    def __init__(self, system, device=0, sigma=None, epsilon=None, charges=None, lanes=4, keep_potentials=True):
         self.system = system
         self.n = len(system["charges"])
         self.device = torch.device("cuda", device)
@@ -154,6 +154,10 @@ class FrameEvaluator:
         if int(lanes) < 1:
             raise ValueError("lanes >= 1")
         self.lanes = int(lanes)
+        # the forces of the differentiable op keep each frame's reciprocal
+        # potential grid (4 bytes a grid point a frame) for the adjoint
+        self.grid = list(system["grid"]) if system.get("pme", True) else None
+        self.keep_potentials = bool(keep_potentials) and self.grid is not None
         self.term = self._new_term()
         self.version = 0
         self._uploaded = -1
@@ -318,9 +322,18 @@ class FrameEvaluator:
             s[0].zero_()
             s[1].zero_()
 
-    def forces(self, positions, energy=False, out=None):
+    def potential_buffers(self, frames):
+        """A device f32 (frames, K1, K2, K3) buffer for the potential grids of
+        `frames` frames (forces(potentials=...)), or None without PME."""
+        if self.grid is None:
+            return None
+        return torch.empty((frames, *self.grid), dtype=torch.float32, device=self.device)
+
+    def forces(self, positions, energy=False, out=None, potentials=None):
         """Forces (K, n, 3) of every frame (and, with `energy`, the
-        potential energies (K,) as a host array)."""
+        potential energies (K,) as a host array).  With `potentials` (from
+        potential_buffers), each frame's reciprocal potential grid is kept
+        there for product(..., potentials=)."""
         X = self.frames(positions)
         F = torch.empty_like(X) if out is None else out
         E = np.zeros(X.shape[0]) if energy else None
@@ -332,6 +345,8 @@ class FrameEvaluator:
                 if l in pending:
                     E[pending.pop(l)] = self._energy(term, st)
                 term.force(X[k], energy=energy, forces=F[k], stream=st)
+                if potentials is not None:
+                    term.potential_grid(out=potentials[k], stream=st)
                 if energy:
                     pending[l] = k
             for l, k in pending.items():
@@ -347,11 +362,13 @@ class FrameEvaluator:
         return (e["lj"] + e["coulomb"] + e["excluded"] + e["reciprocal"] + c["self"] + c["background"]
                 + c["dispersion"])
 
-    def product(self, positions, cotangent, dq=None, dtable=None):
+    def product(self, positions, cotangent, dq=None, dtable=None, potentials=None):
         """sum over frames of sum_i g_ni . dF_ni/dtheta for a cotangent g
         (K, n, 3) on the forces: the charge gradient (n,) and the table
         gradient (2, ntypes, ntypes), device f64, accumulated into dq and
-        dtable when given."""
+        dtable when given.  `potentials`: the grids that forces() kept for
+        these frames at these parameters (the reciprocal forward is then
+        not run again)."""
         X = self.frames(positions)
         G = torch.as_tensor(cotangent, dtype=torch.float64, device=self.device).reshape(X.shape).contiguous()
         if dq is None:
@@ -364,7 +381,8 @@ class FrameEvaluator:
             for i, k in enumerate(self.schedule(X)):
                 term, st, l = self._lane(i, count)
                 q, t = (dq, dtable) if l == 0 else sums[l]
-                term.parameter_gradient(X[k], cotangent=G[k], dq=q, dtable=t, stream=st)
+                term.parameter_gradient(X[k], cotangent=G[k], dq=q, dtable=t, stream=st,
+                                        potential=None if potentials is None else potentials[k])
         finally:
             self._join(count)
         for l in range(1, count):

@@ -110,6 +110,7 @@ class NonbondedTerm:
     def set_pme(self, grid, order=4):
         k = [0, 0, 0] if grid is None else [int(v) for v in grid]
         L.check(L.lib().mdrtPmeSetup(self._h, k[0], k[1], k[2], int(order)), "mdrtPmeSetup")
+        self.pme_grid = k
 
     def set_pruned_reach(self, pruned_distance):
         """The dual list: prune the lists to this reach (0: one list)."""
@@ -214,13 +215,28 @@ class NonbondedTerm:
                 "mdrtNbDisplacement")
         return out
 
+    def potential_grid(self, out=None, stream=None):
+        """The reciprocal potential grid of the last force evaluation (device
+        f32 of the grid's shape), into `out` when given."""
+        if out is None:
+            out = torch.empty(tuple(self.pme_grid), dtype=torch.float32, device=self.device)
+        if not (out.is_cuda and out.dtype == torch.float32 and out.is_contiguous()
+                and out.numel() == int(np.prod(self.pme_grid))):
+            raise ValueError("out: a contiguous CUDA float32 tensor of the grid's size")
+        L.check(L.lib().mdrtPmePotentialGrid(self._h, ctypes.c_void_p(out.data_ptr()), _stream(stream)),
+                "mdrtPmePotentialGrid")
+        return out
+
     def parameter_gradient(self, x, cotangent=None, box=None, dq=None, dtable=None, ntypes=None,
-                           stream=None):
+                           stream=None, potential=None):
         """The gradient in the charges and the sigma / epsilon table at x:
         with a cotangent g (device f64 (n, 3)) on the forces, the product
         sum_k g_k . dF_k/dtheta, else dE/dtheta (without the dispersion
         correction).  Adds into dq (device f64 (n,)) and dtable (device f64
-        (2, ntypes, ntypes)), created as zeros when not given; returns both."""
+        (2, ntypes, ntypes)), created as zeros when not given; returns both.
+        `potential`: the potential grid that potential_grid() kept from the
+        force evaluation at the same x and charges, so that the reciprocal
+        forward is not run again."""
         self._check_x(x)
         b = _host(self.box if box is None else box, np.float64)
         if dq is None:
@@ -234,8 +250,15 @@ class NonbondedTerm:
             self._check_x(cotangent)
             mode = L.GRAD_PRODUCT
             g = _dp(cotangent)
-        L.check(L.lib().mdrtNbParameterGradient(self._h, _dp(x), _hp(b), g, mode, _dp(dq), _dp(dtable),
-                                                _stream(stream)), "mdrtNbParameterGradient")
+        phi = None
+        if potential is not None:
+            if not (potential.is_cuda and potential.dtype == torch.float32 and potential.is_contiguous()
+                    and potential.numel() == int(np.prod(self.pme_grid))):
+                raise ValueError("potential: a contiguous CUDA float32 tensor of the grid's size")
+            phi = ctypes.c_void_p(potential.data_ptr())
+        L.check(L.lib().mdrtNbParameterGradientPotential(self._h, _dp(x), _hp(b), g, mode, phi, _dp(dq),
+                                                         _dp(dtable), _stream(stream)),
+                "mdrtNbParameterGradientPotential")
         return dq, dtable
 
     def status(self, clear=False, stream=None):

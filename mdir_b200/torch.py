@@ -3,10 +3,12 @@
 `forces(evaluator, sigma, epsilon, charges, positions)` returns the forces
 (K, n, 3) of the frames; autograd differentiates them in the per-type LJ
 sigma / epsilon and the per-atom charges through the hand-written adjoint
-of libmdrt_nb.so (`mdrtNbParameterGradient`, the product mode), which
-recomputes the pair geometry and the reciprocal grids instead of storing
-them.  A force-matching loss (1/K) sum |F - F_ref|^2 therefore costs one
-forward and one adjoint pass per frame.
+of libmdrt_nb.so (`mdrtNbParameterGradientPotential`, the product mode),
+which recomputes the pair geometry and reads each frame's reciprocal
+potential grid as the forward kept it (4 bytes a grid point a frame;
+`FrameEvaluator(keep_potentials=False)` recomputes it instead).  A
+force-matching loss (1/K) sum |F - F_ref|^2 therefore costs one forward and
+one adjoint pass per frame.
 
 `evaluate(evaluator, theta, positions)` returns the energies (K,),
 differentiable in theta = {"sigma", "epsilon", "charges"} (the energy mode)
@@ -33,9 +35,11 @@ class _Forces(torch.autograd.Function):
     def forward(ctx, evaluator, positions, sigma, epsilon, charges):
         evaluator.set_parameters(_host(sigma), _host(epsilon), _host(charges))
         X = evaluator.frames(positions.detach())
-        F = evaluator.forces(X)
+        P = evaluator.potential_buffers(X.shape[0]) if evaluator.keep_potentials else None
+        F = evaluator.forces(X, potentials=P)
         ctx.evaluator = evaluator
         ctx.params = (_host(sigma), _host(epsilon), _host(charges))
+        ctx.potentials = P
         ctx.save_for_backward(X)
         return F.reshape(positions.shape)
 
@@ -46,7 +50,8 @@ class _Forces(torch.autograd.Function):
         ev = ctx.evaluator
         (X,) = ctx.saved_tensors
         ev.set_parameters(*ctx.params)
-        dq, dt = ev.product(X, grad.reshape(X.shape))
+        dq, dt = ev.product(X, grad.reshape(X.shape), potentials=ctx.potentials)
+        ctx.potentials = None
         ds, de = lorentz_berthelot_chain(dt.cpu().numpy(), ev.sigma, ev.epsilon)
         dev = grad.device
         return (None, None, torch.as_tensor(ds, device=dev) if ctx.needs_input_grad[2] else None,

@@ -235,3 +235,35 @@ def test_lanes_give_the_results_of_one_lane(cuda):
     for a, b in zip(one[:6], four[:6]):
         scale = np.max(np.abs(a))
         assert np.max(np.abs(a - b)) <= 1e-6 * scale
+
+
+def test_kept_potential_grids_give_the_recomputed_gradient(cuda):
+    """The product with each frame's reciprocal potential grid kept from the
+    forward (mdrtPmePotentialGrid, mdrtNbParameterGradientPotential) against
+    the product that runs the reciprocal forward again, over 4 lanes with a
+    build in the middle of the call; and the autograd op both ways."""
+    s, X, _ = systems.force_matching(frames=7, waters=600, jitter=0.005)
+    X = X.copy()
+    X[4] += np.array([0.08, 0.0, 0.0])
+    Xd = torch.tensor(X, device=cuda)
+    G = torch.tensor(np.random.default_rng(5).normal(size=X.shape), device=cuda)
+    ev = FrameEvaluator(s, lanes=4)
+    P = ev.potential_buffers(len(X))
+    ev.forces(Xd, potentials=P)
+    kept = ev.product(Xd, G, potentials=P)
+    again = ev.product(Xd, G)
+    for a, b in zip(kept, again):
+        a, b = a.cpu().numpy(), b.cpu().numpy()
+        assert np.max(np.abs(a - b)) <= 1e-6 * np.max(np.abs(b))
+    sig, eps, q = _params(s)
+    grads = []
+    for keep in (True, False):
+        ev = FrameEvaluator(s, lanes=4, keep_potentials=keep)
+        ts = torch.tensor(sig, device=cuda, requires_grad=True)
+        te = torch.tensor(eps, device=cuda, requires_grad=True)
+        tq = torch.tensor(q, device=cuda, requires_grad=True)
+        Fk = mtorch.forces(ev, ts, te, tq, Xd)
+        (Fk ** 2).sum().backward()
+        grads.append([ts.grad.cpu().numpy(), te.grad.cpu().numpy(), tq.grad.cpu().numpy()])
+    for a, b in zip(*grads):
+        assert np.max(np.abs(a - b)) <= 1e-6 * np.max(np.abs(b))
