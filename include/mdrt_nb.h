@@ -168,7 +168,14 @@ enum mdrtNbTuneKey {
   /* the PME transforms: 0, the library's own three-kernel convolution when
    * every grid dimension is 32, 64 or 128 (the default), cuFFT otherwise;
    * 1, cuFFT always (MDIR's cuFFT path, runtime/mdrt_cuda.c:2942-2990) */
-  MDRT_NB_TUNE_PME_FFT = 5
+  MDRT_NB_TUNE_PME_FFT = 5,
+  /* the PME spreading: 0 (the default) and 1, global atomics; 2, through
+   * shared-memory tiles of 8^3 grid points in the mixed mode (MDIR D282,
+   * lib/Dialect/MDExec/DevicePolicy.cpp:105-124, which tiles grids of
+   * 500,000 points by default on its devices; on the B200 the global atomics
+   * measured faster at 224^3).  The deterministic mode spreads in fixed
+   * point with global atomics. */
+  MDRT_NB_TUNE_PME_SPREAD = 6
 };
 int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value);
 

@@ -15,6 +15,7 @@ OK, GROW, NAN_POSITION, INVALID_BOX, CUDA_ERROR, TIMEOUT, INVALID_ARGUMENT, UNSU
 ENERGY, ACCUMULATE, POTENTIAL, NO_PAIRS, NO_PME, NO_EXCLUDED, GRAPH, PRUNE = 1, 2, 4, 8, 16, 32, 64, 128
 TUNE_PAIR_BLOCKS_PER_SM, TUNE_SEARCH_WARPS, TUNE_PAIR_SMS, TUNE_FUSED_PRUNE, TUNE_STAGING_DEPTH = 0, 1, 2, 3, 4
 TUNE_PME_FFT = 5
+TUNE_PME_SPREAD = 6
 E_LJ, E_COULOMB, E_EXCLUDED, E_RECIPROCAL, W_PAIR, W_RECIPROCAL, E_COUNT = 0, 1, 2, 3, 4, 10, 16
 SIZE_PLACES, SIZE_LONGEST, SIZE_UNITS, SIZE_EXCL_WIDE, SIZE_NAN, SIZE_OVERFLOW, SIZE_GROUPS, \
     SIZE_ENTRIES, SIZE_COUNT = range(9)

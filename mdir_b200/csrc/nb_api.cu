@@ -273,6 +273,10 @@ int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value) {
       if (value != 0 && value != 1) return MDRT_NB_INVALID_ARGUMENT;
       ctx->c.pme_fft = value;
       return MDRT_NB_OK;
+    case MDRT_NB_TUNE_PME_SPREAD:
+      if (value < 0 || value > 2) return MDRT_NB_INVALID_ARGUMENT;
+      ctx->c.pme_spread = value;
+      return MDRT_NB_OK;
   }
   return MDRT_NB_INVALID_ARGUMENT;
 }

@@ -802,7 +802,9 @@ static int nb_reserve(NbCtx &c, int64_t list_cap) {
         nb_realloc(c.acc_fixed, cap * NB_GROUP * 3))
       return -1;
     if (c.pme.on) {
-      if (nb_realloc(c.pme.pme_force, cap * NB_GROUP * 4) || nb_realloc(c.pme.potential, cap * NB_GROUP))
+      if (nb_realloc(c.pme.pme_force, cap * NB_GROUP * 4) || nb_realloc(c.pme.potential, cap * NB_GROUP) ||
+          nb_realloc(c.pme.tile_bin, cap * NB_GROUP) || nb_realloc(c.pme.tile_rank, cap * NB_GROUP) ||
+          nb_realloc(c.pme.tile_sorted, cap * NB_GROUP))
         return -1;
     }
     NB_CHECK(cudaMemset(c.acc, 0, sizeof(float4) * cap * NB_GROUP));

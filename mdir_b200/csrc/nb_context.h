@@ -34,7 +34,19 @@ struct NbPme {
   int conv_blocks = 0;
   size_t workspace_bytes = 0;
   float2 *fft_tw = nullptr;     // twiddles of the own transforms (nb_fft.cuh), when every K is 32, 64 or 128
+  // the tiled spreading (large grids in the mixed mode): bins of
+  // NB_TILE_EDGE^3 grid points, their counts (zero between spreadings) and
+  // starts, and per place its bin, its rank in the bin and the places in
+  // bin order
+  int tile_bins[3] = {0, 0, 0};
+  int32_t *tile_count = nullptr, *tile_start = nullptr, *tile_scratch = nullptr;
+  int32_t *tile_bin = nullptr, *tile_rank = nullptr, *tile_sorted = nullptr;
 };
+
+// Tiles of the spreading: NB_TILE_EDGE grid points a side, in the mixed
+// mode when tuned (MDIR D282: lib/Dialect/MDExec/DevicePolicy.cpp:105-124,
+// bins of 8 points; not in the deterministic mode, as MDIR).
+#define NB_TILE_EDGE 8
 
 struct NbCtx {
   int device = 0;
@@ -118,6 +130,7 @@ struct NbCtx {
   int pair_blocks_per_sm = 4;
   int pair_sms = 0;  // SMs the persistent pair grid spans (0: all); the rest are left to PME
   int fused_prune = 0;  // the MD step's pruning in the pair kernel: 0 by group count, 1 always, 2 never
+  int pme_spread = 0;  // the spreading: 0 (the default) and 1, global atomics; 2, tiles (mixed mode)
   int pme_fft = 0;  // the PME transforms: 0, the own three-kernel convolution where the grid allows; 1, cuFFT
   int staging_depth = 1;  // the pair kernel's force forms: 1, a unit's entries read as it starts; 2, during the unit before
   int32_t *one = nullptr;  // a device 1: the gate of a pruning a force call asks for (MDRT_NB_PRUNE)
@@ -273,6 +286,8 @@ bool nb_fused_prune(const NbCtx &c);
 // The PME convolution runs on the own three kernels (nb_fft.cuh): every
 // grid dimension 32, 64 or 128 and cuFFT not asked for.
 bool nb_fft_own(const NbCtx &c);
+// The spreading takes tiles (large grids in the mixed mode, or as tuned).
+bool nb_pme_tiled(const NbCtx &c);
 #define NB_FUSED_PRUNE_GROUPS 4096
 #define NB_FUSED_STAGE_MAX (160 * 1024)
 void nb_excluded_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s);

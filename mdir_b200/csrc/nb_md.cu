@@ -1165,7 +1165,8 @@ static int32_t md_prepare_graph(mdrtMd *m, double *x, double *v, const double bo
   int64_t key = c.groups_cap * 1000003 + c.list_cap * 7 + c.units_cap + (int64_t)(c.inner_reach * 1e9) +
                 (c.inner_valid ? 1 : 0) + (c.deterministic ? 2 : 0) + ((int64_t)c.pair_blocks_per_sm << 40) +
                 ((int64_t)c.pair_sms << 44) + (int64_t)(uintptr_t)m->qgrid + ((int64_t)nb_fused_prune(c) << 56) +
-                ((int64_t)c.staging_depth << 58) + ((int64_t)nb_fft_own(c) << 61);
+                ((int64_t)c.staging_depth << 58) + ((int64_t)nb_fft_own(c) << 61) +
+                ((int64_t)nb_pme_tiled(c) << 62);
   bool stale = !m->exec || m->gx != x || m->gv != v || m->gdt != dt || m->gunroll != unroll ||
                m->gbox[0] != box[0] || m->gbox[1] != box[1] || m->gbox[2] != box[2] || m->gcap_key != key;
   if (stale) {

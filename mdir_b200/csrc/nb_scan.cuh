@@ -10,6 +10,10 @@
 #define NB_SCAN_PER_THREAD 4
 #define NB_SCAN_TILE (NB_SCAN_THREADS * NB_SCAN_PER_THREAD)
 
+// Internal to each file that includes it (the build and the tiled PME
+// spreading both scan).
+namespace {
+
 __device__ __forceinline__ int nb_block_exclusive_scan(int v, int *smem_warp, int &total) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int x = v;
@@ -104,3 +108,5 @@ inline void nb_scan(const int *in, int *out, int n_max, const int *n_ptr, int *s
   nb_scan_sums<<<1, NB_SCAN_THREADS, 0, stream>>>(scratch, nblocks);
   nb_scan_final<<<nblocks, NB_SCAN_THREADS, 0, stream>>>(in, n_ptr, n_max, scratch, nblocks, out);
 }
+
+}  // namespace

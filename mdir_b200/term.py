@@ -122,12 +122,14 @@ class NonbondedTerm:
         L.check(L.lib().mdrtNbPrune(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtNbPrune")
 
     def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None, fused_prune=None, staging_depth=None,
-                   pme_fft=None):
+                   pme_fft=None, pme_spread=None):
         """Launch shapes, the MD step's pruning in the pair kernel (0 by
         group count, 1 always, 2 never) and the PME transforms ("own", the
         library's three-kernel convolution where every grid dimension is 32,
         64 or 128; "cufft"): the autotuner's knobs; results do not depend on
-        them beyond the order of f32 sums."""
+        them beyond the order of f32 sums.  pme_spread: "auto" (global
+        atomics, measured faster on the B200), "global" or "tiles"
+        (shared-memory tiles, the mixed mode)."""
         if pair_blocks_per_sm is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_BLOCKS_PER_SM, int(pair_blocks_per_sm)),
                     "mdrtNbSetTuning")
@@ -145,6 +147,10 @@ class NonbondedTerm:
             code = {"own": 0, "cufft": 1}[pme_fft]
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PME_FFT, code), "mdrtNbSetTuning")
             self.pme_fft = pme_fft
+        if pme_spread is not None:
+            code = {"auto": 0, "global": 1, "tiles": 2}[pme_spread]
+            L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PME_SPREAD, code), "mdrtNbSetTuning")
+            self.pme_spread = pme_spread
 
     def set_deterministic(self, on=True):
         L.check(L.lib().mdrtNbSetDeterministic(self._h, int(bool(on))), "mdrtNbSetDeterministic")
