@@ -172,7 +172,7 @@ def test_fft_entries_with_descriptors(cuda):
     sq = mx[:, None, None] ** 2 + my[None, :, None] ** 2 + mz[None, None, :hz] ** 2
     prod = fx[:, None, None] * fy[None, :, None] * fz[None, None, :hz]
     factor = np.where(sq == 0, 0.0, prod / np.where(sq == 0, 1.0, sq))
-    ref = np.fft.irfftn(want * factor, s=(k1, k2, k3)) * (k1 * k2 * k3)  # not normalized
+    ref = np.fft.irfftn(want * factor, s=(k1, k2, k3), axes=(0, 1, 2)) * (k1 * k2 * k3)  # not normalized
     np.testing.assert_allclose(out.cpu().numpy(), ref, atol=3e-4 * np.abs(ref).max())
     # the plain backward transform, not normalized, gives the grid back
     spec2 = torch.zeros_like(spec)
