@@ -1,6 +1,6 @@
 /* OpenMP CPU port of MDIR's host path for the short-range nonbonded + PME
  * term: the timed CPU baseline that bench.py reports beside the device path
- * (TEST / BASELINE INFRASTRUCTURE; the product never loads it).
+ * (test and CPU-baseline infrastructure; the product never loads it).
  *
  * MDIR's own CPU path is MLIR-generated code that needs LLVM/MLIR to build,
  * so this is a restatement of its algorithm in its mixed-precision roles
