@@ -87,8 +87,15 @@ def test_compile_refuses_bad_inputs():
     system.types[0] = system.sigma.shape[0]
     with pytest.raises(mdir.InputError):
         mdir.compile(system, state, integ, ens, exe, sch)
-    # the program is fine again once the inputs are
     system.types[0] = 0
+    # the PME transforms: the library's own kernels or cuFFT
+    exe.pme_fft = "vkfft"
+    with pytest.raises(mdir.InputError):
+        mdir.compile(system, state, integ, ens, exe, sch)
+    exe.pme_fft = "cufft"
+    mdir.compile(system, state, integ, ens, exe, sch)
+    # the program is fine again once the inputs are
+    exe.pme_fft = "own"
     mdir.compile(system, state, integ, ens, exe, sch)
 
 
