@@ -569,10 +569,12 @@ def main():
 
     # ---- end to end through the public API, host buffers ---------------------
     # The equilibrated state of the device run goes to pinned host buffers;
-    # each e2e step uploads it, runs md_steps through the public API (a new
-    # state: the lists are built again) and reads the new positions and
-    # velocities back into the same buffers, so that the steps chain through
-    # host memory like a checkpoint-restart loop.
+    # each e2e step uploads it, runs md_steps through the public API and
+    # reads the new positions and velocities back into the same buffers, so
+    # that the steps chain through host memory like a checkpoint-restart
+    # loop.  Each upload is a new state to the library: it tests the drift
+    # from the lists' build on the device (mdrtMdRefresh) and keeps them when
+    # they serve it, as they do for the state the last step read back.
     system = mdir.System.from_dict(s)
     system.pruned_distance = s["pruned"]
     hx = x.detach().cpu().pin_memory()

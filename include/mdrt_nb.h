@@ -363,6 +363,16 @@ int32_t mdrtMdSetLookahead(mdrtMd *md, double factor);
 /* A neighbor build at device positions x that also resets the reference
  * positions of the test of validity (D80). */
 int32_t mdrtMdBuild(mdrtMd *md, const double *x, const double box[3], void *stream);
+/* A new state x for mdrtMdRun (after the caller wrote new positions): when
+ * every atom of x lies within half the skin of the positions of the last
+ * build (the test that every step makes), the lists serve x; its frames are
+ * made again, and the pruning that the step's update would ask for after
+ * this drift is set (*built = 0).  Otherwise, or in another cell, a build
+ * as mdrtMdBuild (*built = 1).  A state that the last run left, read back
+ * and written again, keeps the lists, so that the run goes on as one
+ * longer run would.  Waits for `stream`.  MDIR: the validity test of
+ * ExposeValidity.cpp before its host loop rebuilds (D80). */
+int32_t mdrtMdRefresh(mdrtMd *md, const double *x, const double box[3], void *stream, int32_t *built);
 /* `steps` leap-frog steps of dt (ps) on the device state x, v (f64 [n, 3]).
  * The lists are pruned on the device whenever 2 max|x - x_prune| > R_in - r_c
  * (gated launches in every step) and rebuilt at the end of each window of

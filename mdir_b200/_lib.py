@@ -63,6 +63,7 @@ SIGNATURES = {
     "mdrtMdSetLookahead": (_i32, [_p, _d]),
     "mdrtMdSetIntegrator": (_i32, [_p, _i32]),
     "mdrtMdBuild": (_i32, [_p, _p, _p, _p]),
+    "mdrtMdRefresh": (_i32, [_p, _p, _p, _p, _p]),
     "mdrtMdRun": (_i32, [_p, _p, _p, _p, _d, _i64, _i32, _p]),
     "mdrtMdThermo": (_i32, [_p, _p, _p]),
     "mdrtMdForces": (_i32, [_p, ctypes.POINTER(_p)]),

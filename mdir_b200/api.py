@@ -303,8 +303,9 @@ class Simulation:
         return self.md.tune(self.x, self.v, self.box, self.program.integrator.timestep, **kw)
 
     def set_state(self, positions, velocities=None, non_blocking=False):
-        """New positions (and velocities) from host or device arrays; the
-        lists are rebuilt at the next run."""
+        """New positions (and velocities) from host or device arrays.  The
+        next run keeps the lists when the new positions lie within half the
+        skin of their build, and builds otherwise (mdrtMdRefresh)."""
         self.x.copy_(torch.as_tensor(positions), non_blocking=non_blocking)
         if velocities is not None:
             self.v.copy_(torch.as_tensor(velocities), non_blocking=non_blocking)
@@ -314,7 +315,12 @@ class Simulation:
         if steps < 0:
             raise InputError("steps must be nonnegative")
         if getattr(self, "_stale", False):
-            self._build()
+            try:
+                self.md.refresh(self.x, self.box)
+            except L.NativeError as e:
+                if e.status == L.NAN_POSITION:
+                    raise SimulationError("positions that are not numbers or are far outside the cell") from e
+                raise
             self._stale = False
         ex = self.program.execution
         unroll = ex.graph_steps if ex.step_graph else 0

@@ -21,6 +21,7 @@
 //          the test of validity that sets the conditional rebuild
 //   if rebuild: the neighbor build, the frames, the reference positions
 #include <cmath>
+#include <cstring>
 #include <cstdio>
 #include <vector>
 
@@ -29,6 +30,10 @@
 #include "nb_spline.cuh"
 
 #define MD_MAX_UNROLL 256  // steps of one replayed graph
+#define MD_CK(x)                                      \
+  do {                                                \
+    if ((x) != cudaSuccess) return MDRT_NB_CUDA_ERROR; \
+  } while (0)
 #define MD_IN_FLIGHT 2     // step graphs queued ahead of the one the host checks
 
 struct mdrtMd {
@@ -51,6 +56,7 @@ struct mdrtMd {
   int ke_blocks = 0;
   unsigned int *done_blocks = nullptr;  // blocks of md_update finished (the last one reduces)
   float2 *blk_max = nullptr;       // per block of md_update: max |x - x_ref|^2, max |x - x_prune|^2
+  unsigned int *drift = nullptr;   // mdrtMdRefresh: the same two maxima of a new state (f32 bits)
   int32_t *wplace = nullptr;       // the place of each water atom, by slot 3 w + k (after each build)
   int32_t *fplace = nullptr;       // the place of each free atom, by its slot
   double *thermo = nullptr;        // [0] lambda, [1] KE, [2] KE before, [3] steps, [4] builds, [5] prunes
@@ -221,8 +227,10 @@ __device__ __forceinline__ Vec3 take_force(int p, float4 *acc, unsigned long lon
 // residual (the split frames of the deterministic mode).
 __device__ __forceinline__ float4 md_frame(int p, Vec3 x, char4 s, const double *L, float q, float4 *xq,
                                            float4 *xq_lo) {
-  double fx = x.x + nb_frame_shift(s.x) * L[0], fy = x.y + nb_frame_shift(s.y) * L[1];
-  double fz = x.z + nb_frame_shift(s.z) * L[2];
+  // rounded as nb_gather rounds the frames of a build (no contraction)
+  double fx = __dadd_rn(x.x, __dmul_rn(nb_frame_shift(s.x), L[0]));
+  double fy = __dadd_rn(x.y, __dmul_rn(nb_frame_shift(s.y), L[1]));
+  double fz = __dadd_rn(x.z, __dmul_rn(nb_frame_shift(s.z), L[2]));
   float4 nf = make_float4((float)fx, (float)fy, (float)fz, q);
   xq[p] = nf;
   if (xq_lo)
@@ -664,6 +672,36 @@ __global__ void md_after_build(int64_t n3, const double *__restrict__ x, double 
 
 __global__ void md_clear_status(int *status, int bits) { atomicAnd(status, ~bits); }
 
+// The largest squared drift of x from the positions of the last build and
+// of the last pruning, each rounded to f32 as the update rounds its own
+// (the bits of non-negative floats order as the floats): out[0], out[1].
+__global__ void md_drift(int64_t n, const double *__restrict__ x, const double *__restrict__ x_ref,
+                         const double *__restrict__ x_prune, unsigned int *out) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float d2 = 0.f, p2 = 0.f;
+  if (i < n) {
+    Vec3 xi = load3(x, i);
+    Vec3 dr = xi - load3(x_ref, i);
+    d2 = (float)dot(dr, dr);
+    if (x_prune) {
+      dr = xi - load3(x_prune, i);
+      p2 = (float)dot(dr, dr);
+    }
+    // a coordinate that is not finite counts as beyond any skin
+    if (!(d2 <= 3.0e38f)) d2 = 3.0e38f;
+    if (!(p2 <= 3.0e38f)) p2 = 3.0e38f;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+    p2 = fmaxf(p2, __shfl_xor_sync(0xffffffffu, p2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, __float_as_uint(d2));
+    atomicMax(out + 1, __float_as_uint(p2));
+  }
+}
+
 // After a pruning: the reference positions of the inner list.
 __global__ void md_after_prune(int64_t n3, const double *__restrict__ x, double *__restrict__ x_prune,
                                double *thermo) {
@@ -876,7 +914,7 @@ static void md_free(mdrtMd *m) {
   if (m->side) cudaStreamDestroy(m->side);
   for (void *p : {(void *)m->inv_mass, (void *)m->mass, (void *)m->waters, (void *)m->free_atoms,
                   (void *)m->excl_other, (void *)m->force, (void *)m->x_ref, (void *)m->x_prune,
-                  (void *)m->ke_part, (void *)m->done_blocks, (void *)m->blk_max,
+                  (void *)m->ke_part, (void *)m->done_blocks, (void *)m->blk_max, (void *)m->drift,
                   (void *)m->wplace, (void *)m->fplace, (void *)m->thermo, (void *)m->flag,
                   (void *)m->noise, (void *)m->x_ck, (void *)m->v_ck, (void *)m->thermo_ck, (void *)m->peak,
                   (void *)m->xref_ck, (void *)m->xprune_ck, (void *)m->qgrid, (void *)m->phi, (void *)m->qfixed,
@@ -975,6 +1013,7 @@ int32_t mdrtMdCreate(mdrtMd **out, mdrtNb *nb, const double *masses, int64_t nwa
             cudaMalloc(&m->ke_part, sizeof(double) * m->ke_blocks) == cudaSuccess &&
             cudaMalloc(&m->done_blocks, sizeof(unsigned int)) == cudaSuccess &&
             cudaMalloc(&m->blk_max, sizeof(float2) * m->ke_blocks) == cudaSuccess &&
+            cudaMalloc(&m->drift, sizeof(unsigned int) * 2) == cudaSuccess &&
             cudaMalloc(&m->wplace, sizeof(int32_t) * std::max<int64_t>(3 * nwaters, 1)) == cudaSuccess &&
             cudaMalloc(&m->fplace, sizeof(int32_t) * std::max<int64_t>(m->nfree, 1)) == cudaSuccess &&
             cudaMalloc(&m->thermo, sizeof(double) * 8) == cudaSuccess &&
@@ -1067,6 +1106,42 @@ int32_t mdrtMdBuild(mdrtMd *m, const double *x, const double box[3], void *strea
   }
   cudaMemsetAsync(m->flag + 1, 0, sizeof(int), st);  // pruned here: none due
   return cudaGetLastError() == cudaSuccess ? MDRT_NB_OK : MDRT_NB_CUDA_ERROR;
+}
+
+int32_t mdrtMdRefresh(mdrtMd *m, const double *x, const double box[3], void *stream, int32_t *built) {
+  if (!m || !x || !box) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = *m->nb;
+  cudaStream_t st = (cudaStream_t)stream;
+  bool dual = c.inner_reach > 0.0;
+  bool same_cell = c.built && box[0] == c.box_built[0] && box[1] == c.box_built[1] && box[2] == c.box_built[2];
+  if (same_cell && (!dual || c.inner_valid)) {
+    MD_CK(cudaSetDevice(m->device));
+    MD_CK(cudaMemsetAsync(m->drift, 0, sizeof(unsigned int) * 2, st));
+    md_drift<<<blocks_for(m->n, 256), 256, 0, st>>>(m->n, x, m->x_ref, dual ? m->x_prune : nullptr, m->drift);
+    unsigned int h[2] = {0u, 0u};
+    MD_CK(cudaMemcpyAsync(h, m->drift, sizeof(h), cudaMemcpyDeviceToHost, st));
+    MD_CK(cudaStreamSynchronize(st));
+    float d2, p2;
+    std::memcpy(&d2, &h[0], sizeof(float));
+    std::memcpy(&p2, &h[1], sizeof(float));
+    double half = 0.5 * (c.reach - c.cutoff), half_in = 0.5 * (c.inner_reach - c.cutoff);
+    // the test of every step of the update: the lists serve x while the
+    // largest drift from their build stays within half the skin
+    if ((double)d2 <= half * half) {
+      nb_gather_frames(c, x, box, st);
+      // the pruning that the update would ask for after this drift
+      int prune = (dual && (double)p2 > half_in * half_in) ? 1 : 0;
+      int flags[4] = {0, prune, 0, 0};
+      MD_CK(cudaMemcpyAsync(m->flag, flags, sizeof(flags), cudaMemcpyHostToDevice, st));
+      int32_t *counter = md_unit_counter(*m);
+      if (prune && counter) MD_CK(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
+      MD_CK(cudaStreamSynchronize(st));
+      if (built) *built = 0;
+      return MDRT_NB_OK;
+    }
+  }
+  if (built) *built = 1;
+  return mdrtMdBuild(m, x, box, stream);
 }
 
 }  // extern "C"

@@ -532,9 +532,12 @@ __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
   // x + S H less half the diagonal (a triclinic cell adds S's tilt terms),
   // and with xq_lo the f32 residual of each coordinate
   char4 s = shift[p];
-  double fx = x[3 * a] + nb_frame_shift(s.x) * Lx + (double)s.y * bx + (double)s.z * cx;
-  double fy = x[3 * a + 1] + nb_frame_shift(s.y) * Ly + (double)s.z * cy;
-  double fz = x[3 * a + 2] + nb_frame_shift(s.z) * Lz;
+  // each product and sum rounded once, in this order (no contraction), as
+  // the MD step's update makes the frames of the next step (md_frame)
+  double fx = __dadd_rn(__dadd_rn(__dadd_rn(x[3 * a], __dmul_rn(nb_frame_shift(s.x), Lx)), __dmul_rn((double)s.y, bx)),
+                        __dmul_rn((double)s.z, cx));
+  double fy = __dadd_rn(__dadd_rn(x[3 * a + 1], __dmul_rn(nb_frame_shift(s.y), Ly)), __dmul_rn((double)s.z, cy));
+  double fz = __dadd_rn(x[3 * a + 2], __dmul_rn(nb_frame_shift(s.z), Lz));
   float4 hi = make_float4((float)fx, (float)fy, (float)fz, q[a]);
   xq[p] = hi;
   if (xq_lo)

@@ -60,6 +60,17 @@ class Integrator:
         self.term.box = b
         L.check(L.lib().mdrtMdBuild(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtMdBuild")
 
+    def refresh(self, x, box, stream=None):
+        """Positions x written anew: keeps the lists when x lies within half
+        the skin of their build (the test of every step), else builds.
+        Returns True when it built."""
+        b = _host(box, np.float64)
+        self.term.box = b
+        built = ctypes.c_int32()
+        L.check(L.lib().mdrtMdRefresh(self._h, _dp(x), _hp(b), _stream(stream), ctypes.byref(built)),
+                "mdrtMdRefresh")
+        return bool(built.value)
+
     def run(self, x, v, box, dt, steps, unroll=10, stream=None):
         b = _host(box, np.float64)
         L.check(L.lib().mdrtMdRun(self._h, _dp(x), _dp(v), _hp(b), dt, int(steps), int(unroll), _stream(stream)),

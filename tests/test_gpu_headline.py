@@ -142,7 +142,12 @@ def test_simulation_run_is_the_integrator_run_bitwise(cuda, tau):
     program, v0 = _program(s, deterministic=True, tau=tau)
     sim = mdir.Simulation(program)
     sim.run(40)
-    sim.run(35)  # a second call goes on from the first's state
+    # the state read back and written again (a checkpoint-restart loop, as
+    # the bench's e2e leg runs): the lists are kept and the run goes on as
+    # one run would
+    mid = sim.state()
+    sim.set_state(mid.positions, mid.velocities)
+    sim.run(35)
     got = sim.state()
     assert got.step == 75
     # the same run through the integrator directly

@@ -279,3 +279,31 @@ def test_velocity_verlet_argon_nve(cuda):
     v2 = torch.tensor(v0 - 0.5 * dt * f0 / m, device="cuda")
     md2.run(x2, v2, s["box"], dt, 20, unroll=10)
     np.testing.assert_allclose(x2.cpu().numpy(), xr, atol=1e-6)
+
+
+def test_a_state_written_back_keeps_the_lists_and_the_trajectory(cuda):
+    """Positions and velocities read back after a run and written again
+    (a checkpoint-restart loop): mdrtMdRefresh keeps the lists, and the two
+    runs give the trajectory of one run of their length bit for bit
+    (deterministic mode); a state beyond half the skin builds."""
+    s = systems.tip3p(waters=600, seed=51)
+    t1, md1, x1, v1 = setup(s, deterministic=True, tau=0.1)
+    md1.run(x1, v1, s["box"], 0.002, 200, unroll=10)
+    t2, md2, x2, v2 = setup(s, deterministic=True, tau=0.1)
+    md2.run(x2, v2, s["box"], 0.002, 100, unroll=10)
+    hx, hv = x2.cpu(), v2.cpu()
+    x2.zero_()
+    v2.zero_()
+    x2.copy_(hx)
+    v2.copy_(hv)
+    builds = md2.thermo()["builds"]
+    assert md2.refresh(x2, s["box"]) is False
+    assert md2.thermo()["builds"] == builds
+    md2.run(x2, v2, s["box"], 0.002, 100, unroll=10)
+    assert torch.equal(x1, x2) and torch.equal(v1, v2)
+    assert md1.thermo()["builds"] == md2.thermo()["builds"]
+    # an atom moved by more than half the skin: the lists are built again
+    x2[5, 0] += 0.6 * (s["reach"] - s["cutoff"])
+    assert md2.refresh(x2, s["box"]) is True
+    md2.run(x2, v2, s["box"], 0.002, 20, unroll=10)
+    assert t2.status() == 0
