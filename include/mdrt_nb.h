@@ -291,6 +291,27 @@ int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3
                                 const double *cotangent, int32_t mode, double *dq,
                                 double *dtable, void *stream);
 
+/* The force term of `count` frames, frame k at device positions
+ * x + k x_stride (f64 [n, 3]) into forces + k f_stride, one after another
+ * on `stream`, with the lists of the last build (valid for every frame):
+ * the loop of mdrtNbForce calls of a frame evaluator in one call, since the
+ * host's launch rate bounds a small frame's evaluation.  With `potentials`,
+ * frame k's reciprocal potential grid goes to potentials + k p_stride (as
+ * mdrtPmePotentialGrid).  MDRT_NB_ENERGY only with count 1 (the energies
+ * are one evaluation's).  MDIR: FrameEvaluator's loop over the frames of a
+ * call (python/mdir/_frames.py:769, D251). */
+int32_t mdrtNbForceFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_t count, const double box[3],
+                          uint32_t flags, double *forces, int64_t f_stride, float *potentials, int64_t p_stride,
+                          void *stream);
+
+/* mdrtNbParameterGradientPotential over `count` frames (positions
+ * x + k x_stride, cotangents cotangent + k c_stride, potential grids
+ * potentials + k p_stride or NULL), accumulating into dq and dtable. */
+int32_t mdrtNbParameterGradientFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_t count,
+                                      const double box[3], const double *cotangent, int64_t c_stride, int32_t mode,
+                                      const float *potentials, int64_t p_stride, double *dq, double *dtable,
+                                      void *stream);
+
 /* The reciprocal potential grid phi of the last force evaluation that ran
  * PME (K1 x K2 x K3 f32 in the grid's layout, the third index fastest) to
  * `grid` (device), asynchronous on `stream`; MDRT_NB_INVALID_ARGUMENT

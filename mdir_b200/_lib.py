@@ -53,6 +53,8 @@ SIGNATURES = {
     "mdrtNbParameterGradient": (_i32, [_p, _p, _p, _p, _i32, _p, _p, _p]),
     "mdrtNbParameterGradientPotential": (_i32, [_p, _p, _p, _p, _i32, _p, _p, _p, _p]),
     "mdrtPmePotentialGrid": (_i32, [_p, _p, _p]),
+    "mdrtNbForceFrames": (_i32, [_p, _p, _i64, _i64, _p, _u32, _p, _i64, _p, _i64, _p]),
+    "mdrtNbParameterGradientFrames": (_i32, [_p, _p, _i64, _i64, _p, _p, _i64, _i32, _p, _i64, _p, _p, _p]),
     "mdrtNbGroupsBuffer": (_i32, [_p, _i32, ctypes.POINTER(_p), ctypes.POINTER(_i64)]),
     "mdrtNbGroupsInfo": (_i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "mdrtNbStatus": (_i32, [_p, _p, _i32, ctypes.POINTER(_i32)]),

@@ -457,6 +457,37 @@ static int32_t nb_force_entry(mdrtNb *ctx, const double *x, const double box[3],
   return MDRT_NB_OK;
 }
 
+int32_t mdrtNbForceFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_t count, const double box[3],
+                          uint32_t flags, double *forces, int64_t f_stride, float *potentials, int64_t p_stride,
+                          void *stream) {
+  if (!ctx || count < 0 || (count > 0 && (!x || !forces))) return MDRT_NB_INVALID_ARGUMENT;
+  if (nb_triclinic(ctx->c)) return MDRT_NB_INVALID_BOX;
+  if (count > 1 && (flags & MDRT_NB_ENERGY)) return MDRT_NB_INVALID_ARGUMENT;  // one frame's energies at a time
+  if (potentials && !ctx->c.pme.on) return MDRT_NB_INVALID_ARGUMENT;
+  for (int64_t k = 0; k < count; ++k) {
+    int32_t s = nb_force_entry(ctx, x + k * x_stride, box, flags, forces + k * f_stride, stream);
+    if (s) return s;
+    if (potentials && nb_pme_potential_grid(ctx->c, potentials + k * p_stride, (cudaStream_t)stream))
+      return MDRT_NB_CUDA_ERROR;
+  }
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbParameterGradientFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_t count,
+                                      const double box[3], const double *cotangent, int64_t c_stride, int32_t mode,
+                                      const float *potentials, int64_t p_stride, double *dq, double *dtable,
+                                      void *stream) {
+  if (!ctx || count < 0) return MDRT_NB_INVALID_ARGUMENT;
+  for (int64_t k = 0; k < count; ++k) {
+    int32_t s = mdrtNbParameterGradientPotential(ctx, x + k * x_stride, box,
+                                                 cotangent ? cotangent + k * c_stride : nullptr, mode,
+                                                 potentials ? potentials + k * p_stride : nullptr, dq, dtable,
+                                                 stream);
+    if (s) return s;
+  }
+  return MDRT_NB_OK;
+}
+
 int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, const double box[3], double *out,
                            void *stream) {
   if (!ctx || !box || count < 0 || (count > 0 && (!frames || !out))) return MDRT_NB_INVALID_ARGUMENT;

@@ -230,11 +230,12 @@ class FrameEvaluator:
             raise ValueError(f"positions: (K, {self.n}, 3)")
         return X.contiguous()
 
-    def schedule(self, X):
-        """Yields the frame numbers in order, each with a build whose lists
-        serve it: the frames ahead are tested against the positions of the
-        current build in one launch, and a frame that moved more than half
-        the skin gets a new build first."""
+    def runs(self, X):
+        """Yields runs (k0, k1) of consecutive frames that one build serves,
+        in order, building before a run where needed: the frames ahead are
+        tested against the positions of the current build in one launch,
+        and a frame that moved more than half the skin gets a new build
+        first."""
         self._upload()
         K = X.shape[0]
         half_skin = 0.5 * (self.reach - self.cutoff)
@@ -248,9 +249,31 @@ class FrameEvaluator:
             if run == 0:
                 self._build(X[k])
                 continue
-            for j in range(k, k + run):
-                yield j
+            yield k, k + run
             k += run
+
+    def schedule(self, X):
+        """Yields the frame numbers in order, each with a build whose lists
+        serve it (the frames of runs())."""
+        for k0, k1 in self.runs(X):
+            yield from range(k0, k1)
+
+    # frames a lane takes in one native call before the next lane's turn:
+    # every lane gets work early, and the host still makes few calls
+    LANE_CHUNK = 2
+
+    def _lanes_of_run(self, k0, k1, count):
+        """(term, stream, first frame, end) of the native calls of the run
+        [k0, k1): frame k goes to lane k mod count, as schedule() hands them
+        out, LANE_CHUNK frames of a lane a call, the lanes in turn."""
+        span = count * self.LANE_CHUNK
+        for c0 in range(k0, k1, span):
+            c1 = min(k1, c0 + span)
+            for l in range(count):
+                first = c0 + (l - c0) % count
+                if first < c1:
+                    term, st, _ = self._lane(first, count)
+                    yield term, st, first, c1
 
     def _build(self, x):
         self.term.build(x, self.box, self.reach)
@@ -338,6 +361,17 @@ class FrameEvaluator:
         F = torch.empty_like(X) if out is None else out
         E = np.zeros(X.shape[0]) if energy else None
         count = self._open_lanes(X.shape[0])
+        if not energy:
+            # each lane's frames of a run in one native call (the host's
+            # launch rate, not the GPU, bounds a call of many small frames)
+            try:
+                for k0, k1 in self.runs(X):
+                    for term, st, first, end in self._lanes_of_run(k0, k1, count):
+                        term.force_frames(X[:end], first, count, F[:end],
+                                          potentials=None if potentials is None else potentials[:end], stream=st)
+            finally:
+                self._join(count)
+            return F
         pending = {}  # lane -> the frame whose energies it holds
         try:
             for i, k in enumerate(self.schedule(X)):
@@ -378,11 +412,13 @@ class FrameEvaluator:
         count = self._open_lanes(X.shape[0], sums=True)
         sums = [None] + [self._lane_sums[l] for l in range(1, count)]
         try:
-            for i, k in enumerate(self.schedule(X)):
-                term, st, l = self._lane(i, count)
-                q, t = (dq, dtable) if l == 0 else sums[l]
-                term.parameter_gradient(X[k], cotangent=G[k], dq=q, dtable=t, stream=st,
-                                        potential=None if potentials is None else potentials[k])
+            for k0, k1 in self.runs(X):
+                for term, st, first, end in self._lanes_of_run(k0, k1, count):
+                    l = first % count
+                    q, t = (dq, dtable) if l == 0 else sums[l]
+                    term.parameter_gradient_frames(X[:end], first, count, G[:end], q, t,
+                                                   potentials=None if potentials is None else potentials[:end],
+                                                   stream=st)
         finally:
             self._join(count)
         for l in range(1, count):

@@ -189,6 +189,45 @@ class NonbondedTerm:
         L.check(entry(self._h, _dp(x), _hp(b), flags, _dp(forces), _stream(stream)), "mdrtNbForce")
         return forces
 
+    def force_frames(self, X, first, step, F, potentials=None, box=None, stream=None):
+        """Forces of the frames first, first + step, ... of X (device f64
+        (K, n, 3)) into the same frames of F, one native call
+        (mdrtNbForceFrames); with `potentials` (device f32 (K, K1, K2, K3))
+        each frame's reciprocal potential grid is kept there."""
+        K = X.shape[0]
+        count = len(range(first, K, step))
+        if count == 0:
+            return
+        b = _host(self.box if box is None else box, np.float64)
+        frame = 3 * self.n
+        phi, pstride = None, 0
+        if potentials is not None:
+            pstride = step * potentials[0].numel()
+            phi = ctypes.c_void_p(potentials.data_ptr() + 4 * first * potentials[0].numel())
+        L.check(L.lib().mdrtNbForceFrames(self._h, ctypes.c_void_p(X.data_ptr() + 8 * first * frame), step * frame,
+                                          count, _hp(b), 0, ctypes.c_void_p(F.data_ptr() + 8 * first * frame),
+                                          step * frame, phi, pstride, _stream(stream)), "mdrtNbForceFrames")
+
+    def parameter_gradient_frames(self, X, first, step, G, dq, dtable, potentials=None, box=None, stream=None):
+        """parameter_gradient over the frames first, first + step, ... of X
+        with their cotangents in G (device f64 (K, n, 3)) and, when given,
+        their kept potential grids; one native call
+        (mdrtNbParameterGradientFrames), accumulating into dq and dtable."""
+        K = X.shape[0]
+        count = len(range(first, K, step))
+        if count == 0:
+            return
+        b = _host(self.box if box is None else box, np.float64)
+        frame = 3 * self.n
+        phi, pstride = None, 0
+        if potentials is not None:
+            pstride = step * potentials[0].numel()
+            phi = ctypes.c_void_p(potentials.data_ptr() + 4 * first * potentials[0].numel())
+        L.check(L.lib().mdrtNbParameterGradientFrames(
+            self._h, ctypes.c_void_p(X.data_ptr() + 8 * first * frame), step * frame, count, _hp(b),
+            ctypes.c_void_p(G.data_ptr() + 8 * first * frame), step * frame, L.GRAD_PRODUCT, phi, pstride,
+            _dp(dq), _dp(dtable), _stream(stream)), "mdrtNbParameterGradientFrames")
+
     def energies(self, stream=None):
         out = np.zeros(L.E_COUNT)
         L.check(L.lib().mdrtNbEnergies(self._h, _stream(stream), _hp(out)), "mdrtNbEnergies")
