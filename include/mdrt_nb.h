@@ -175,7 +175,11 @@ enum mdrtNbTuneKey {
    * 500,000 points by default on its devices; on the B200 the global atomics
    * measured faster at 224^3).  The deterministic mode spreads in fixed
    * point with global atomics. */
-  MDRT_NB_TUNE_PME_SPREAD = 6
+  MDRT_NB_TUNE_PME_SPREAD = 6,
+  /* the frames entries (mdrtNbForceFrames, mdrtNbParameterGradientFrames):
+   * 1, their launches kept and replayed as CUDA graphs (the default); 0,
+   * launched on each call */
+  MDRT_NB_TUNE_FRAME_GRAPHS = 7
 };
 int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value);
 
@@ -299,14 +303,27 @@ int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3
  * frame k's reciprocal potential grid goes to potentials + k p_stride (as
  * mdrtPmePotentialGrid).  MDRT_NB_ENERGY only with count 1 (the energies
  * are one evaluation's).  MDIR: FrameEvaluator's loop over the frames of a
- * call (python/mdir/_frames.py:769, D251). */
+ * call (python/mdir/_frames.py:769, D251).
+ *
+ * The launches of a call are kept as a CUDA graph (MDRT_NB_TUNE_FRAME_GRAPHS,
+ * on by default) under a key of the call's arguments (pointers, strides,
+ * count, cell, flags) and the state of the context (every buffer, capacity,
+ * tuning value and build count): a call that repeats a key seen before is
+ * one graph launch on `stream`.  A key is captured at its second call (the
+ * first makes the lazy allocations outside any capture), and a context
+ * keeps its 8 most recent keys.  The graph reads the inputs, the particle
+ * tables and the lists at its launch, so new positions or parameters in the
+ * same buffers need no new capture.  A call on a stream that is itself
+ * being captured launches directly. */
 int32_t mdrtNbForceFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_t count, const double box[3],
                           uint32_t flags, double *forces, int64_t f_stride, float *potentials, int64_t p_stride,
                           void *stream);
 
 /* mdrtNbParameterGradientPotential over `count` frames (positions
  * x + k x_stride, cotangents cotangent + k c_stride, potential grids
- * potentials + k p_stride or NULL), accumulating into dq and dtable. */
+ * potentials + k p_stride or NULL), accumulating into dq and dtable.  In
+ * the product mode the launches are kept as a graph, as those of
+ * mdrtNbForceFrames. */
 int32_t mdrtNbParameterGradientFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_t count,
                                       const double box[3], const double *cotangent, int64_t c_stride, int32_t mode,
                                       const float *potentials, int64_t p_stride, double *dq, double *dtable,
@@ -335,6 +352,9 @@ int32_t mdrtNbParameterGradientPotential(mdrtNb *ctx, const double *x, const dou
  * MDIR: _mlir_ciface_mdrtGroupsBuffer(result, handle, slot),
  * runtime/mdrt_cuda.c:3109. */
 int32_t mdrtNbGroupsBuffer(mdrtNb *ctx, int32_t slot, void **pointer, int64_t *count);
+
+/* The graphs of the frames entries: captures and replays so far. */
+int32_t mdrtNbFrameGraphInfo(mdrtNb *ctx, int64_t *captures, int64_t *replays);
 
 /* The capacity C of a list (entries a group) and the builds / growths so far.
  * MDIR: mdrtGroupsBuilt, mdrt_cuda.c:3208. */

@@ -16,6 +16,7 @@ ENERGY, ACCUMULATE, POTENTIAL, NO_PAIRS, NO_PME, NO_EXCLUDED, GRAPH, PRUNE = 1, 
 TUNE_PAIR_BLOCKS_PER_SM, TUNE_SEARCH_WARPS, TUNE_PAIR_SMS, TUNE_FUSED_PRUNE, TUNE_STAGING_DEPTH = 0, 1, 2, 3, 4
 TUNE_PME_FFT = 5
 TUNE_PME_SPREAD = 6
+TUNE_FRAME_GRAPHS = 7
 E_LJ, E_COULOMB, E_EXCLUDED, E_RECIPROCAL, W_PAIR, W_RECIPROCAL, E_COUNT = 0, 1, 2, 3, 4, 10, 16
 SIZE_PLACES, SIZE_LONGEST, SIZE_UNITS, SIZE_EXCL_WIDE, SIZE_NAN, SIZE_OVERFLOW, SIZE_GROUPS, \
     SIZE_ENTRIES, SIZE_COUNT = range(9)
@@ -57,6 +58,7 @@ SIGNATURES = {
     "mdrtNbParameterGradientFrames": (_i32, [_p, _p, _i64, _i64, _p, _p, _i64, _i32, _p, _i64, _p, _p, _p]),
     "mdrtNbGroupsBuffer": (_i32, [_p, _i32, ctypes.POINTER(_p), ctypes.POINTER(_i64)]),
     "mdrtNbGroupsInfo": (_i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "mdrtNbFrameGraphInfo": (_i32, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "mdrtNbStatus": (_i32, [_p, _p, _i32, ctypes.POINTER(_i32)]),
     "mdrtNbTimeKernels": (_i32, [_p, _p, _p, _i32, _p, _p]),
     "mdrtMdCreate": (_i32, [ctypes.POINTER(_p), _p, _p, _i64, _p, _d, _d]),

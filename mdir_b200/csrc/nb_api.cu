@@ -1,4 +1,5 @@
 // The C ABI of include/mdrt_nb.h over the host context NbCtx.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -61,6 +62,101 @@ __global__ void nb_frame_drift(int64_t n, const double *__restrict__ frames, con
   if ((threadIdx.x & 31) == 0) atomicMax(out + blockIdx.y, (unsigned long long)__double_as_longlong(m));
 }
 
+// ---- the graphs of the frames entries ----
+// A frames call launches about a dozen kernels a frame, and for a frame of a
+// few ten thousand atoms the host's launch rate, not the GPU, bounds it.
+// The launches of a call are therefore kept as a CUDA graph under a key of
+// the call's arguments and the bytes of the context as the call found it:
+// every buffer pointer, capacity, tuning value, interaction parameter and
+// build count of NbCtx, so that any change of the context that alters what
+// the launches are (a build, a growth, new tuning, a new cell) changes the
+// key.  The graph reads the frames, the particle tables and the lists at its
+// launch.  The host arrays of NbCtx (h_q and the like) are not in the key:
+// the launches kept here take no argument computed from them.
+#define NB_FRAME_GRAPHS 8
+
+std::vector<unsigned char> nb_frames_key(const NbCtx &c, const uint64_t *args, int nargs) {
+  std::vector<unsigned char> key(sizeof(uint64_t) * nargs + sizeof(NbCtx));
+  std::memcpy(key.data(), args, sizeof(uint64_t) * nargs);
+  const unsigned char *b = reinterpret_cast<const unsigned char *>(&c);
+  std::copy(b, b + sizeof(NbCtx), key.begin() + sizeof(uint64_t) * nargs);
+  return key;
+}
+
+uint64_t nb_bits(double v) {
+  uint64_t u;
+  std::memcpy(&u, &v, sizeof(u));
+  return u;
+}
+
+uint64_t nb_bits(const void *p) { return (uint64_t)(uintptr_t)p; }
+
+// Runs `run(stream)` (the launches of one frames call) for the caller's
+// stream st: a key met before with a graph is one graph launch; a key met
+// once before is captured now, on the context's own stream, and launched;
+// a new key runs directly (its lazy allocations and tables then happen
+// outside any capture) and is remembered.  The least recently used of more
+// than NB_FRAME_GRAPHS keys is dropped (a graph still running is freed when
+// it completes).
+template <class Run>
+int32_t nb_frames_graph(mdrtNb *ctx, const uint64_t *args, int nargs, cudaStream_t st, Run &&run) {
+  NbCtx &c = ctx->c;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (!c.frame_graphs) return run(st);
+  CK(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return run(st);
+  std::vector<unsigned char> key = nb_frames_key(c, args, nargs);
+  NbFrameGraph *hit = nullptr;
+  for (auto &g : ctx->graphs)
+    if (g.key == key) hit = &g;
+  if (!hit) {
+    int32_t s = run(st);
+    if (s) return s;
+    if ((int)ctx->graphs.size() >= NB_FRAME_GRAPHS) {
+      auto old = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                  [](const NbFrameGraph &a, const NbFrameGraph &b) { return a.used < b.used; });
+      if (old->exec) cudaGraphExecDestroy(old->exec);
+      ctx->graphs.erase(old);
+    }
+    NbFrameGraph g;
+    g.key = std::move(key);
+    g.used = ++ctx->graph_clock;
+    ctx->graphs.push_back(std::move(g));
+    return MDRT_NB_OK;
+  }
+  hit->used = ++ctx->graph_clock;
+  if (!hit->exec) {
+    if (!ctx->capture) CK(cudaStreamCreateWithFlags(&ctx->capture, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(ctx->capture, cudaStreamCaptureModeThreadLocal));
+    int32_t s = run(ctx->capture);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->capture, &graph);
+    if (s || e != cudaSuccess || !graph) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      return s ? s : cuda_status(e, "cudaStreamEndCapture");
+    }
+    e = cudaGraphInstantiate(&hit->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      hit->exec = nullptr;
+      return cuda_status(e, "cudaGraphInstantiate");
+    }
+    ctx->graph_captures++;
+    CK(cudaGraphLaunch(hit->exec, st));
+    // the capture ran as the call before it, so it left the context as it
+    // was; if not, the graph holds work of that change and is not kept
+    if (nb_frames_key(c, args, nargs) != hit->key) {
+      cudaGraphExecDestroy(hit->exec);
+      hit->exec = nullptr;
+    }
+    return MDRT_NB_OK;
+  }
+  CK(cudaGraphLaunch(hit->exec, st));
+  ctx->graph_replays++;
+  return MDRT_NB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -119,8 +215,13 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   if (!ctx) return MDRT_NB_OK;
   NbCtx &c = ctx->c;
   cudaSetDevice(c.device);
+  for (auto &g : ctx->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  ctx->graphs.clear();
+  if (ctx->capture) cudaStreamDestroy(ctx->capture);
   nb_pme_release(c);
   nb_free(c.q); nb_free(c.type); nb_free(c.lj); nb_free(c.ljf); nb_free(c.sigeps);
+  nb_free(c.lj_on); nb_free(c.counts_lj);
   nb_free(c.adj_g); nb_free(c.adj_q); nb_free(c.adj_types); nb_free(c.x_build); nb_free(c.drift);
   nb_free(c.excl_off); nb_free(c.excl); nb_free(c.excl_pairs); nb_free(c.excl_partials);
   nb_free(c.order); nb_free(c.place_of); nb_free(c.shift); nb_free(c.xw);
@@ -179,15 +280,26 @@ int32_t mdrtNbSetParticles(mdrtNb *ctx, const double *charges, const int32_t *ty
     }
   c.lj_geom = geom;
   std::vector<float> qf(charges, charges + c.n);
+  // the tables keep their buffers (sized for 32 types) from one call to the
+  // next, so that new parameters leave the kernels' arguments as they were
+  // (and the frames entries' graphs valid); the work in flight on any
+  // stream finishes before they are written
+  CK(cudaDeviceSynchronize());
   if (!c.q) CK(cudaMalloc(&c.q, sizeof(float) * c.n));
   if (!c.type) CK(cudaMalloc(&c.type, sizeof(int32_t) * c.n));
-  nb_free(c.lj);
-  nb_free(c.ljf);
-  CK(cudaMalloc(&c.ljf, sizeof(float2) * ntypes));
+  if (!c.ljf) CK(cudaMalloc(&c.ljf, sizeof(float2) * 32));
+  if (!c.lj) CK(cudaMalloc(&c.lj, sizeof(float2) * 32 * 32));
+  if (!c.sigeps) CK(cudaMalloc(&c.sigeps, sizeof(float2) * 32 * 32));
+  if (!c.lj_on) CK(cudaMalloc(&c.lj_on, sizeof(int32_t) * 32));
+  int32_t on[32] = {0};
+  uint32_t mask = 0;
+  for (int a = 0; a < ntypes; ++a)
+    for (int b = 0; b < ntypes; ++b)
+      if (epsilon[a * ntypes + b] != 0.0) on[a] = 1;
+  for (int a = 0; a < ntypes; ++a) mask |= on[a] ? (1u << a) : 0u;
+  CK(cudaMemcpy(c.lj_on, on, sizeof(on), cudaMemcpyHostToDevice));
+  c.lj_mask = mask;
   CK(cudaMemcpy(c.ljf, factors.data(), sizeof(float2) * ntypes, cudaMemcpyHostToDevice));
-  CK(cudaMalloc(&c.lj, sizeof(float2) * ntypes * ntypes));
-  nb_free(c.sigeps);
-  CK(cudaMalloc(&c.sigeps, sizeof(float2) * ntypes * ntypes));
   CK(cudaMemcpy(c.sigeps, se.data(), sizeof(float2) * ntypes * ntypes, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c.q, qf.data(), sizeof(float) * c.n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c.type, types, sizeof(int32_t) * c.n, cudaMemcpyHostToDevice));
@@ -276,6 +388,10 @@ int32_t mdrtNbSetTuning(mdrtNb *ctx, int32_t key, int32_t value) {
     case MDRT_NB_TUNE_PME_SPREAD:
       if (value < 0 || value > 2) return MDRT_NB_INVALID_ARGUMENT;
       ctx->c.pme_spread = value;
+      return MDRT_NB_OK;
+    case MDRT_NB_TUNE_FRAME_GRAPHS:
+      if (value != 0 && value != 1) return MDRT_NB_INVALID_ARGUMENT;
+      ctx->c.frame_graphs = value;
       return MDRT_NB_OK;
   }
   return MDRT_NB_INVALID_ARGUMENT;
@@ -379,6 +495,7 @@ static int32_t nb_build_entry(mdrtNb *ctx, const double *x, int64_t n, const dou
   CK(cudaSetDevice(c.device));
   cudaStream_t st = (cudaStream_t)stream;
   if (nb_build_run(c, x, box, st)) return MDRT_NB_CUDA_ERROR;
+  if (nb_lj_partition_run(c, st)) return MDRT_NB_CUDA_ERROR;
   for (int k = 0; k < 3; ++k) c.tilt_built[k] = c.tilt[k];
   if (!c.x_build) CK(cudaMalloc(&c.x_build, sizeof(double) * 3 * c.n));
   CK(cudaMemcpyAsync(c.x_build, x, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToDevice, st));
@@ -457,6 +574,28 @@ static int32_t nb_force_entry(mdrtNb *ctx, const double *x, const double box[3],
   return MDRT_NB_OK;
 }
 
+// The checks of the gradient entries and the adjoint's scratch (allocated
+// here, outside any capture).
+static int32_t nb_gradient_ready(mdrtNb *ctx, const double *x, const double box[3], const double *cotangent,
+                                 int32_t mode, const float *phi, double *dq, double *dtable) {
+  if (!ctx || !x || !box || !dq || !dtable) return MDRT_NB_INVALID_ARGUMENT;
+  if (mode != MDRT_NB_GRAD_PRODUCT && mode != MDRT_NB_GRAD_ENERGY) return MDRT_NB_INVALID_ARGUMENT;
+  if (mode == MDRT_NB_GRAD_PRODUCT && !cotangent) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (!c.built) return MDRT_NB_NOT_BUILT;
+  if (nb_triclinic(c)) return MDRT_NB_UNSUPPORTED;  // the adjoint runs in orthorhombic cells
+  int s = check_box(c, box);
+  if (s) return s;
+  for (int k = 0; k < 3; ++k)
+    if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;
+  // the switched Lennard-Jones form has no adjoint here
+  if (c.lj_switch) return MDRT_NB_UNSUPPORTED;
+  if (phi && !c.pme.on) return MDRT_NB_INVALID_ARGUMENT;
+  CK(cudaSetDevice(c.device));
+  if (nb_adjoint_reserve(c)) return MDRT_NB_CUDA_ERROR;
+  return MDRT_NB_OK;
+}
+
 int32_t mdrtNbForceFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_t count, const double box[3],
                           uint32_t flags, double *forces, int64_t f_stride, float *potentials, int64_t p_stride,
                           void *stream) {
@@ -464,13 +603,22 @@ int32_t mdrtNbForceFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_
   if (nb_triclinic(ctx->c)) return MDRT_NB_INVALID_BOX;
   if (count > 1 && (flags & MDRT_NB_ENERGY)) return MDRT_NB_INVALID_ARGUMENT;  // one frame's energies at a time
   if (potentials && !ctx->c.pme.on) return MDRT_NB_INVALID_ARGUMENT;
-  for (int64_t k = 0; k < count; ++k) {
-    int32_t s = nb_force_entry(ctx, x + k * x_stride, box, flags, forces + k * f_stride, stream);
-    if (s) return s;
-    if (potentials && nb_pme_potential_grid(ctx->c, potentials + k * p_stride, (cudaStream_t)stream))
-      return MDRT_NB_CUDA_ERROR;
-  }
-  return MDRT_NB_OK;
+  if (count == 0) return MDRT_NB_OK;
+  if (!box) return MDRT_NB_INVALID_ARGUMENT;
+  auto run = [&](cudaStream_t s) -> int32_t {
+    for (int64_t k = 0; k < count; ++k) {
+      int32_t r = nb_force_entry(ctx, x + k * x_stride, box, flags, forces + k * f_stride, s);
+      if (r) return r;
+      if (potentials && nb_pme_potential_grid(ctx->c, potentials + k * p_stride, s)) return MDRT_NB_CUDA_ERROR;
+    }
+    return MDRT_NB_OK;
+  };
+  // a pruning changes the context at every call: launched directly
+  if (flags & MDRT_NB_PRUNE) return run((cudaStream_t)stream);
+  const uint64_t args[] = {1, nb_bits(x), (uint64_t)x_stride, (uint64_t)count, nb_bits(box[0]), nb_bits(box[1]),
+                           nb_bits(box[2]), flags, nb_bits(forces), (uint64_t)f_stride, nb_bits(potentials),
+                           (uint64_t)p_stride};
+  return nb_frames_graph(ctx, args, (int)(sizeof(args) / sizeof(args[0])), (cudaStream_t)stream, run);
 }
 
 int32_t mdrtNbParameterGradientFrames(mdrtNb *ctx, const double *x, int64_t x_stride, int64_t count,
@@ -478,13 +626,29 @@ int32_t mdrtNbParameterGradientFrames(mdrtNb *ctx, const double *x, int64_t x_st
                                       const float *potentials, int64_t p_stride, double *dq, double *dtable,
                                       void *stream) {
   if (!ctx || count < 0) return MDRT_NB_INVALID_ARGUMENT;
-  for (int64_t k = 0; k < count; ++k) {
-    int32_t s = mdrtNbParameterGradientPotential(ctx, x + k * x_stride, box,
-                                                 cotangent ? cotangent + k * c_stride : nullptr, mode,
-                                                 potentials ? potentials + k * p_stride : nullptr, dq, dtable,
-                                                 stream);
-    if (s) return s;
-  }
+  if (count == 0) return MDRT_NB_OK;
+  int32_t ready = nb_gradient_ready(ctx, x, box, cotangent, mode, potentials, dq, dtable);
+  if (ready) return ready;
+  auto run = [&](cudaStream_t s) -> int32_t {
+    if (nb_adjoint_run(ctx->c, x, x_stride, count, box, cotangent, c_stride, mode, potentials, p_stride, dq, dtable,
+                       s))
+      return MDRT_NB_CUDA_ERROR;
+    CK(cudaGetLastError());
+    return MDRT_NB_OK;
+  };
+  // the energy mode's charge terms take the net charge from the host
+  // charges, which the key does not hold: launched directly
+  if (mode != MDRT_NB_GRAD_PRODUCT || !x || !box) return run((cudaStream_t)stream);
+  const uint64_t args[] = {2, nb_bits(x), (uint64_t)x_stride, (uint64_t)count, nb_bits(box[0]), nb_bits(box[1]),
+                           nb_bits(box[2]), nb_bits(cotangent), (uint64_t)c_stride, (uint64_t)mode,
+                           nb_bits(potentials), (uint64_t)p_stride, nb_bits(dq), nb_bits(dtable)};
+  return nb_frames_graph(ctx, args, (int)(sizeof(args) / sizeof(args[0])), (cudaStream_t)stream, run);
+}
+
+int32_t mdrtNbFrameGraphInfo(mdrtNb *ctx, int64_t *captures, int64_t *replays) {
+  if (!ctx || !captures || !replays) return MDRT_NB_INVALID_ARGUMENT;
+  *captures = ctx->graph_captures;
+  *replays = ctx->graph_replays;
   return MDRT_NB_OK;
 }
 
@@ -537,22 +701,10 @@ int32_t mdrtPmePotentialGrid(mdrtNb *ctx, float *grid, void *stream) {
 int32_t mdrtNbParameterGradientPotential(mdrtNb *ctx, const double *x, const double box[3],
                                          const double *cotangent, int32_t mode, const float *phi, double *dq,
                                          double *dtable, void *stream) {
-  if (!ctx || !x || !box || !dq || !dtable) return MDRT_NB_INVALID_ARGUMENT;
-  if (mode != MDRT_NB_GRAD_PRODUCT && mode != MDRT_NB_GRAD_ENERGY) return MDRT_NB_INVALID_ARGUMENT;
-  if (mode == MDRT_NB_GRAD_PRODUCT && !cotangent) return MDRT_NB_INVALID_ARGUMENT;
-  NbCtx &c = ctx->c;
-  if (!c.built) return MDRT_NB_NOT_BUILT;
-  if (nb_triclinic(c)) return MDRT_NB_UNSUPPORTED;  // the adjoint runs in orthorhombic cells
-  int s = check_box(c, box);
+  int32_t s = nb_gradient_ready(ctx, x, box, cotangent, mode, phi, dq, dtable);
   if (s) return s;
-  for (int k = 0; k < 3; ++k)
-    if (box[k] != c.box_built[k]) return MDRT_NB_INVALID_BOX;
-  // the switched Lennard-Jones form has no adjoint here
-  if (c.lj_switch) return MDRT_NB_UNSUPPORTED;
-  CK(cudaSetDevice(c.device));
-  if (nb_adjoint_reserve(c)) return MDRT_NB_CUDA_ERROR;
-  if (phi && !c.pme.on) return MDRT_NB_INVALID_ARGUMENT;
-  if (nb_adjoint_run(c, x, box, cotangent, mode, dq, dtable, (cudaStream_t)stream, phi)) return MDRT_NB_CUDA_ERROR;
+  if (nb_adjoint_run(ctx->c, x, 0, 1, box, cotangent, 0, mode, phi, 0, dq, dtable, (cudaStream_t)stream))
+    return MDRT_NB_CUDA_ERROR;
   CK(cudaGetLastError());
   return MDRT_NB_OK;
 }

@@ -63,6 +63,8 @@ struct NbCtx {
   std::vector<int32_t> h_type;
   std::vector<float2> h_lj;
   float2 *sigeps = nullptr;    // (sigma, epsilon) per type pair, for the parameter gradient
+  int32_t *lj_on = nullptr;    // per type: 1 when an epsilon of its row is not 0 (device, 32 types)
+  uint32_t lj_mask = 0;        // the same, a bit per type
   // exclusions: ragged rows (atom order) and the list of pairs i < j
   int32_t *excl_off = nullptr, *excl = nullptr;
   int32_t *excl_pairs = nullptr;
@@ -133,6 +135,7 @@ struct NbCtx {
   int pme_spread = 0;  // the spreading: 0 (the default) and 1, global atomics; 2, tiles (mixed mode)
   int pme_fft = 0;  // the PME transforms: 0, the own three-kernel convolution where the grid allows; 1, cuFFT
   int staging_depth = 1;  // the pair kernel's force forms: 1, a unit's entries read as it starts; 2, during the unit before
+  int frame_graphs = 1;  // the frames entries replay their launches as CUDA graphs (1) or launch them (0)
   int32_t *one = nullptr;  // a device 1: the gate of a pruning a force call asks for (MDRT_NB_PRUNE)
   // parameter gradient scratch (mdrtNbParameterGradient), allocated at the first call
   float4 *adj_g = nullptr;        // per place: the cotangent on the forces (f32)
@@ -140,6 +143,14 @@ struct NbCtx {
   double *adj_types = nullptr;    // per block of the adjoint kernel: 2 ntypes^2 partials
   int64_t adj_places = 0;         // places_cap the per-place arrays were sized for
   int adj_blocks = 0;
+  // the outer lists of a build without a pruned reach with each group's
+  // entries of a partner with Lennard-Jones terms first (nb_lj_partition_run):
+  // their count per group, for the build `lj_part_build` and the types of
+  // `lj_part_mask`; the adjoint's rounds after them skip their LJ terms
+  int32_t *counts_lj = nullptr;
+  int64_t counts_lj_cap = 0;
+  int64_t lj_part_build = -1;
+  uint32_t lj_part_mask = 0;
   // the columns and bins the buffers are planned for (one grid, or the
   // frames of a batch laid end to end)
   int64_t plan_cols = 0, plan_bins = 0;
@@ -161,9 +172,22 @@ enum NbEnergySlot {
   NB_E_SLOTS = 16
 };
 
+// The launches of one frames call kept as a CUDA graph (nb_api.cu): the
+// key is the call's arguments followed by the bytes of the context it ran
+// in; exec is null for a key seen once and not yet captured.
+struct NbFrameGraph {
+  std::vector<unsigned char> key;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t used = 0;
+};
+
 // The opaque handle of the C ABI.
 struct mdrtNb {
   NbCtx c;
+  std::vector<NbFrameGraph> graphs;
+  uint64_t graph_clock = 0;
+  cudaStream_t capture = nullptr;  // the frames graphs are captured on this stream
+  int64_t graph_captures = 0, graph_replays = 0;
 };
 
 // One frame of a batch, as the kernels read it: the cell, its grid of
@@ -263,7 +287,10 @@ int nb_grow_lists_keep(NbCtx &c, int64_t longest, cudaStream_t s);
 // Lists longer than this fraction of the capacity are grown ahead, before a
 // rebuild inside the step graphs overflows.
 #define NB_GROW_AHEAD 0.85
-void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s);
+// With `cot` (f64 [n,3], atom order), its f32 copy in place order goes to
+// c.adj_g as well (the adjoint's cotangent).
+void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s,
+                      const double *cot = nullptr);
 // With `halt` (device), nothing when *halt is set (the MD step's stop).
 // With `skip` (device), nothing when *skip is set (a pruning step whose
 // pairs nb_prune_pairs_run computed).
@@ -299,14 +326,21 @@ void nb_reduce_energy(NbCtx &c, bool pairs, bool excluded, cudaStream_t s);
 int nb_pme_setup(NbCtx &c, int k0, int k1, int k2, int order);
 void nb_pme_release(NbCtx &c);
 int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaStream_t s);
-// The parameter gradient (mdrtNbParameterGradient).  mode 0: the product
-// sum_k g_k . dF_k/dtheta for the cotangent g (f64 [n,3], atom order); mode 1:
-// dE/dtheta.  Adds the charge gradient to dq (f64 [n], atom order) and the
-// type-pair gradient to dtable (f64, ntypes^2 sigma entries then ntypes^2
-// epsilon entries).  Needs the adjoint scratch (nb_adjoint_reserve).
+// The parameter gradient (mdrtNbParameterGradient) summed over `count`
+// frames (x + k x_stride; cotangent + k c_stride; phi + k p_stride when phi
+// is given).  mode 0: the product sum_k g_k . dF_k/dtheta for the cotangent
+// g (f64 [n,3], atom order); mode 1: dE/dtheta.  Adds the charge gradient to
+// dq (f64 [n], atom order) and the type-pair gradient to dtable (f64,
+// ntypes^2 sigma entries then ntypes^2 epsilon entries), each reduced once
+// at the end of the call.  Needs the adjoint scratch (nb_adjoint_reserve).
 int nb_adjoint_reserve(NbCtx &c);
-int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double *cotangent, int mode,
-                   double *dq, double *dtable, cudaStream_t s, const float *phi = nullptr);
+// After a build (host, stream s): the stable partition of each group's
+// entries by whether the partner's type has LJ terms, when the lists are
+// the ones the kernels walk (no pruned reach) and fit the kernel's staging.
+int nb_lj_partition_run(NbCtx &c, cudaStream_t s);
+int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, const double box[3],
+                   const double *cotangent, int64_t c_stride, int mode, const float *phi, int64_t p_stride,
+                   double *dq, double *dtable, cudaStream_t s);
 // The reciprocal part of the charge gradient, added per place into c.adj_q.
 int nb_pme_potential_grid(NbCtx &c, float *out, cudaStream_t s);
 // With phi (a potential grid kept from the force evaluation at the same

@@ -519,16 +519,19 @@ __global__ void nb_gather(int64_t places, const int32_t *__restrict__ sizes,
                           const double *__restrict__ x, const float *__restrict__ q,
                           const int32_t *__restrict__ type, double Lx, double Ly, double Lz, double bx,
                           double cx, double cy, float4 *__restrict__ xq, int32_t *__restrict__ typ_p,
-                          float4 *__restrict__ xq_lo) {
+                          float4 *__restrict__ xq_lo, const double *__restrict__ cot, float4 *__restrict__ gp) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
   int a = order[p];
   if (a < 0) {
     xq[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (xq_lo) xq_lo[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (gp) gp[p] = make_float4(0.f, 0.f, 0.f, 0.f);
     typ_p[p] = 0;
     return;
   }
+  // with cot, the cotangent on the forces (the adjoint's g, f32 per place)
+  if (gp) gp[p] = make_float4((float)cot[3 * a], (float)cot[3 * a + 1], (float)cot[3 * a + 2], 0.f);
   // x + S H less half the diagonal (a triclinic cell adds S's tilt terms),
   // and with xq_lo the f32 residual of each coordinate
   char4 s = shift[p];
@@ -835,7 +838,9 @@ __global__ void nb_sum_partials(const double *__restrict__ unit_partials,
 // geometry (nothing of the forward pass is stored).  The member's G_q
 // travels with it like its force accumulator; the partner's stays in its
 // lane and is added once per entry (f64 atomics); the type-pair sums go to
-// shared memory and per-block partials, summed later in a fixed order.
+// shared memory and are added to per-block partials (the frames of a call
+// accumulate there), summed later in a fixed order.  The shared table holds
+// (sigma, eps/sigma) per type pair, so the sigma term needs no division.
 // MDIR's counterpart is the IR-derived product of md-differentiate (D381,
 // docs/python-frames.md:203-260), which walks the neighbor matrix.
 template <int MODE>
@@ -843,16 +848,16 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
     PairParams P, const int32_t *__restrict__ sizes, const int2 *__restrict__ units, const int2 *__restrict__ slab,
     const int32_t *__restrict__ counts, const float4 *__restrict__ xq, const int32_t *__restrict__ typ,
     const float2 *__restrict__ sigeps, const float4 *__restrict__ gp, double *__restrict__ gq,
-    double *__restrict__ type_partials) {
+    double *__restrict__ type_partials, const int32_t *__restrict__ counts_lj) {
   __shared__ float4 s_x[8][2 * NB_GROUP];
-  __shared__ float4 s_g[8][2 * NB_GROUP];
-  __shared__ int s_t[8][2 * NB_GROUP];
+  __shared__ float4 s_g[8][2 * NB_GROUP];  // the cotangent, and in w the member's type row (ntypes t)
   __shared__ float2 s_se[NB_MAX_TYPES * NB_MAX_TYPES];
   __shared__ float s_acc[2 * NB_MAX_TYPES * NB_MAX_TYPES];
   const unsigned FULL = 0xffffffffu;
   int nt2 = P.ntypes * P.ntypes;
   for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
-    s_se[k] = sigeps[k];
+    float2 se = sigeps[k];
+    s_se[k] = make_float2(se.x, se.x > 0.f ? se.y / se.x : 0.f);
     s_acc[k] = 0.f;
     s_acc[nt2 + k] = 0.f;
   }
@@ -862,7 +867,6 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
   const int src = (lane & 16) | ((lane + 1) & 15);
   const float4 *px = &s_x[warp][u];
   const float4 *pg = &s_g[warp][u];
-  const int *pt = &s_t[warp][u];
   int nunits = min((int64_t)sizes[NB_SIZE_UNITS], P.units_cap);
   int wstride = gridDim.x * 8;
   for (int unit = blockIdx.x * 8 + warp; unit < nunits; unit += wstride) {
@@ -874,16 +878,21 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
       float4 xi = xq[pi];
       xi.w *= P.coulomb;
       s_x[warp][lane] = xi;
-      s_g[warp][lane] = MODE == 0 ? gp[pi] : make_float4(0.f, 0.f, 0.f, 0.f);
-      s_t[warp][lane] = typ[pi] * P.ntypes;
+      float4 gi = MODE == 0 ? gp[pi] : make_float4(0.f, 0.f, 0.f, 0.f);
+      gi.w = __int_as_float(typ[pi] * P.ntypes);
+      s_g[warp][lane] = gi;
     }
     __syncwarp();
     int cnt = (int)min((int64_t)counts[g], P.list_cap);
     int e0 = uo.y * NB_UNIT;
     int ne = min(NB_UNIT, cnt - e0);
+    // with the lists partitioned (counts_lj), the rounds that start past a
+    // group's LJ partners have none (the same for the whole warp)
+    int nlj = counts_lj ? counts_lj[g] : cnt;
     float ai = 0.f;  // G_q of member (lane + k) mod 16
     for (int r = 0; r < 2; ++r) {
       if (r * 32 >= ne) break;
+      const bool lj_round = e0 + r * 32 < nlj;
       bool valid = r * 32 + lane < ne;
       int2 en = valid ? slab[(int64_t)g * P.list_cap + e0 + r * 32 + lane] : make_int2(0, 0);
       int q = en.x;
@@ -924,8 +933,8 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
         float erfcv = nb_erfc_from_exp(P.beta_p * rr, ex);
         // w: the factor of the pair's term; cq: its Coulomb part per unit f q_i q_j
         float w, cq;
+        float4 gm = pg[k];
         if (MODE == 0) {
-          float4 gm = pg[k];
           float h = ((gm.x - gj.x) * dx + (gm.y - gj.y) * dy + (gm.z - gj.z) * dz) * rinv;
           w = inside ? h : 0.f;
           // -h D, D = -(erfc(beta r)/r^2 + 2 beta/sqrt(pi) exp(-beta^2 r^2)/r)
@@ -936,23 +945,26 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
         }
         ai = fmaf(cq, fqj, ai);
         aj = fmaf(cq, xm.w, aj);
-        int tp = pt[k] + tj;
-        float2 se = s_se[tp];
-        if (w != 0.f && se.y != 0.f) {
+        if (lj_round && w != 0.f) {
+          int tp = __float_as_int(gm.w) + tj;
+          float2 se = s_se[tp];  // (sigma, eps / sigma)
+          if (se.y != 0.f) {
           float s1 = se.x * rinv;
           float s2 = s1 * s1;
           float s6 = s2 * s2 * s2;
           float s12 = s6 * s6;
           float ds, de;
           if (MODE == 0) {
-            de = -w * 4.f * (6.f * s6 - 12.f * s12) * rinv;
-            ds = -w * 4.f * se.y * (36.f * s6 - 144.f * s12) * rinv / se.x;
+            float a = -4.f * w * rinv;
+            de = a * (6.f * s6 - 12.f * s12);
+            ds = a * se.y * (36.f * s6 - 144.f * s12);
           } else {
             de = 4.f * (s12 - s6);
-            ds = 4.f * se.y * (12.f * s12 - 6.f * s6) / se.x;
+            ds = 4.f * se.y * (12.f * s12 - 6.f * s6);
           }
           atomicAdd(&s_acc[tp], ds);
           atomicAdd(&s_acc[nt2 + tp], de);
+          }
         }
         ai = __shfl_sync(FULL, ai, src);
       }
@@ -963,18 +975,7 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
   }
   __syncthreads();
   for (int k = threadIdx.x; k < 2 * nt2; k += blockDim.x)
-    type_partials[(int64_t)blockIdx.x * 2 * nt2 + k] = (double)s_acc[k];
-}
-
-// g of each place (f32), gathered from the atom-order cotangent (f64).
-__global__ void nb_gather_cotangent(int64_t places, const int32_t *__restrict__ sizes,
-                                    const int32_t *__restrict__ order, const double *__restrict__ g,
-                                    float4 *__restrict__ gp) {
-  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= places || p >= sizes[NB_SIZE_PLACES]) return;
-  int a = order[p];
-  gp[p] = a < 0 ? make_float4(0.f, 0.f, 0.f, 0.f)
-                : make_float4((float)g[3 * a], (float)g[3 * a + 1], (float)g[3 * a + 2], 0.f);
+    type_partials[(int64_t)blockIdx.x * 2 * nt2 + k] += (double)s_acc[k];
 }
 
 // The per-place charge gradient (f64) added to atom order; the place
@@ -990,6 +991,45 @@ __global__ void nb_scatter_place_values(int64_t places, const int32_t *__restric
     if (a >= 0) out[a] += v;
     vp[p] = 0.0;
   }
+}
+
+// The stable partition of each group's list by the partner's LJ terms: the
+// entries whose partner's type has any, then the others, each in their
+// order; counts_lj[g] gets the number of the first.  One warp a group, its
+// entries staged in shared memory (list_cap of them).
+__global__ void __launch_bounds__(32) nb_lj_partition(const int32_t *__restrict__ sizes, int64_t list_cap,
+                                                      const int32_t *__restrict__ counts, int2 *__restrict__ slab,
+                                                      const int32_t *__restrict__ order,
+                                                      const int32_t *__restrict__ type,
+                                                      const int32_t *__restrict__ lj_on,
+                                                      int32_t *__restrict__ counts_lj) {
+  extern __shared__ int2 s_e[];
+  int64_t g = blockIdx.x;
+  if (g >= sizes[NB_SIZE_GROUPS]) return;
+  int lane = threadIdx.x;
+  int cnt = (int)min((int64_t)counts[g], list_cap);
+  int2 *row = slab + g * list_cap;
+  for (int e = lane; e < cnt; e += 32) s_e[e] = row[e];
+  __syncwarp();
+  auto lj = [&](int e) {
+    int a = order[s_e[e].x];
+    return a >= 0 && lj_on[type[a]] != 0;
+  };
+  int nlj = 0;
+  for (int e0 = 0; e0 < cnt; e0 += 32) nlj += __popc(__ballot_sync(0xffffffffu, e0 + lane < cnt && lj(e0 + lane)));
+  int pl = 0, pn = nlj;
+  unsigned below = (1u << lane) - 1u;
+  for (int e0 = 0; e0 < cnt; e0 += 32) {
+    int e = e0 + lane;
+    bool in = e < cnt;
+    bool f = in && lj(e);
+    unsigned bl = __ballot_sync(0xffffffffu, f);
+    unsigned bn = __ballot_sync(0xffffffffu, in && !f);
+    if (in) row[f ? pl + __popc(bl & below) : pn + __popc(bn & below)] = s_e[e];
+    pl += __popc(bl);
+    pn += __popc(bn);
+  }
+  if (lane == 0) counts_lj[g] = nlj;
 }
 
 // The excluded pairs, u = -f q_i q_j erf(beta r)/r, in f64 and atom order.
@@ -1092,11 +1132,12 @@ PairParams pair_params(const NbCtx &c, const double box[3]) {
 
 }  // namespace
 
-void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s) {
+void nb_gather_frames(NbCtx &c, const double *x, const double box[3], cudaStream_t s, const double *cot) {
   nb_gather<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.shift, x,
                                                           c.q, c.type, box[0], box[1], box[2], c.tilt[0],
                                                           c.tilt[1], c.tilt[2], c.xq, c.typ_p,
-                                                          c.deterministic ? c.xq_lo : nullptr);
+                                                          c.deterministic ? c.xq_lo : nullptr, cot,
+                                                          cot ? c.adj_g : nullptr);
 }
 
 bool nb_fused_prune(const NbCtx &c) {
@@ -1264,12 +1305,29 @@ int nb_adjoint_reserve(NbCtx &c) {
   return 0;
 }
 
-int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double *cot, int mode, double *dq,
-                   double *dtable, cudaStream_t s, const float *phi) {
+int nb_lj_partition_run(NbCtx &c, cudaStream_t s) {
+  c.lj_part_build = -1;
+  size_t stage = sizeof(int2) * (size_t)c.list_cap;
+  if (c.inner_reach > 0.0 || !c.lj_on || c.groups_cap <= 0 || c.list_cap <= 0 || stage > 48 * 1024) return 0;
+  if (c.counts_lj_cap < c.groups_cap) {
+    if (c.counts_lj) cudaFree(c.counts_lj);
+    c.counts_lj = nullptr;
+    c.counts_lj_cap = 0;
+    if (cudaMalloc(&c.counts_lj, sizeof(int32_t) * c.groups_cap) != cudaSuccess) return -1;
+    c.counts_lj_cap = c.groups_cap;
+  }
+  nb_lj_partition<<<(unsigned)c.groups_cap, 32, stage, s>>>(c.sizes, c.list_cap, c.counts, c.slab, c.order, c.type,
+                                                            c.lj_on, c.counts_lj);
+  if (cudaGetLastError() != cudaSuccess) return -1;
+  c.lj_part_build = c.builds;
+  c.lj_part_mask = c.lj_mask;
+  return 0;
+}
+
+int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, const double box[3],
+                   const double *cot, int64_t c_stride, int mode, const float *phi, int64_t p_stride, double *dq,
+                   double *dtable, cudaStream_t s) {
   PairParams P = pair_params(c, box);
-  nb_gather_frames(c, x, box, s);
-  if (mode == 0)
-    nb_gather_cotangent<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, cot, c.adj_g);
   bool inner = c.inner_reach > 0.0 && c.inner_valid;
   const int32_t *lsizes = inner ? c.sizes_in : c.sizes;
   const int2 *lunits = inner ? c.units_in : c.units;
@@ -1277,35 +1335,46 @@ int nb_adjoint_run(NbCtx &c, const double *x, const double box[3], const double 
   const int32_t *lcounts = inner ? c.counts_in : c.counts;
   int64_t want = (c.units_cap + 7) / 8;
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, c.adj_blocks));
-  if (mode == 0)
-    nb_pairs_adjoint<0><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
-                                             c.adj_q, c.adj_types);
-  else
-    nb_pairs_adjoint<1><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
-                                             c.adj_q, c.adj_types);
   int width = 2 * c.ntypes * c.ntypes;
+  const int32_t *lj_counts =
+      !inner && c.lj_part_build == c.builds && c.lj_part_mask == c.lj_mask ? c.counts_lj : nullptr;
+  // the blocks' type-pair partials and the places' charge gradient (kept
+  // zero between calls) sum the frames; both go out once at the end
+  if (cudaMemsetAsync(c.adj_types, 0, sizeof(double) * grid * width, s) != cudaSuccess) return -1;
+  double net = 0.0;
+  if (mode == 1)
+    for (double v : c.h_q) net += v;
+  for (int64_t k = 0; k < count; ++k) {
+    const double *xk = x + k * x_stride;
+    const double *ck = mode == 0 ? cot + k * c_stride : nullptr;
+    nb_gather_frames(c, xk, box, s, ck);
+    if (mode == 0)
+      nb_pairs_adjoint<0><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
+                                               c.adj_q, c.adj_types, lj_counts);
+    else
+      nb_pairs_adjoint<1><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
+                                               c.adj_q, c.adj_types, lj_counts);
+    int rc = nb_pme_adjoint_run(c, box, mode, s, phi ? phi + k * p_stride : nullptr);
+    if (rc) return rc;
+    if (c.n_excl_pairs > 0 && c.beta != 0.0) {
+      int blocks = blocks_for(c.n_excl_pairs, 256);
+      if (mode == 0)
+        nb_excluded_adjoint<0><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, xk, c.q, ck, box[0], box[1],
+                                                      box[2], c.beta, c.coulomb, dq);
+      else
+        nb_excluded_adjoint<1><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, xk, c.q, ck, box[0], box[1],
+                                                      box[2], c.beta, c.coulomb, dq);
+    }
+    if (mode == 1 && c.beta > 0.0) {
+      double V = box[0] * box[1] * box[2];
+      double self2 = -2.0 * c.coulomb * c.beta / sqrt(M_PI);
+      double background = -c.coulomb * M_PI * net / (V * c.beta * c.beta);
+      nb_charge_terms<<<blocks_for(c.n, 256), 256, 0, s>>>(c.n, c.q, self2, background, dq);
+    }
+  }
   nb_sum_type_partials<<<blocks_for((int64_t)width * 32, 256), 256, 0, s>>>(c.adj_types, grid, width, dtable);
-  int rc = nb_pme_adjoint_run(c, box, mode, s, phi);
-  if (rc) return rc;
   nb_scatter_place_values<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.adj_q,
                                                                         dq);
-  if (c.n_excl_pairs > 0 && c.beta != 0.0) {
-    int blocks = blocks_for(c.n_excl_pairs, 256);
-    if (mode == 0)
-      nb_excluded_adjoint<0><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, x, c.q, cot, box[0], box[1],
-                                                    box[2], c.beta, c.coulomb, dq);
-    else
-      nb_excluded_adjoint<1><<<blocks, 256, 0, s>>>(c.n_excl_pairs, c.excl_pairs, x, c.q, cot, box[0], box[1],
-                                                    box[2], c.beta, c.coulomb, dq);
-  }
-  if (mode == 1 && c.beta > 0.0) {
-    double net = 0.0;
-    for (double v : c.h_q) net += v;
-    double V = box[0] * box[1] * box[2];
-    double self2 = -2.0 * c.coulomb * c.beta / sqrt(M_PI);
-    double background = -c.coulomb * M_PI * net / (V * c.beta * c.beta);
-    nb_charge_terms<<<blocks_for(c.n, 256), 256, 0, s>>>(c.n, c.q, self2, background, dq);
-  }
   return 0;
 }
 

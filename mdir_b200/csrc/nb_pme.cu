@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(256) nb_spread(GridParams G, int64_t places,
   nb_bspline<P>(t2, w2, nullptr);
   int gz = k2 - c;
   if (gz < 0) gz += G.K2;
-  float qz = v.w * w2[c];
+  float qz = v.w * nb_pick(w2, c);
 #pragma unroll
   for (int jx = 0; jx < P; ++jx) {
     int gx = k0 - jx;
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(128) nb_tile_spread(GridParams G, int nb1, int
     nb_bspline<P>(t0, w0, nullptr);
     nb_bspline<P>(t1, w1, nullptr);
     nb_bspline<P>(t2, w2, nullptr);
-    float qz = v.w * w2[c];
+    float qz = v.w * nb_pick(w2, c);
     int lz = k2 - c - o2;
 #pragma unroll
     for (int jx = 0; jx < P; ++jx) {
@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(128) nb_pme_gather_split(GridParams G, int64_t
     nb_bspline<P>(t2, w2, d2);
     int gz = k2 - c;
     if (gz < 0) gz += G.K2;
-    float wz = w2[c], dz = d2[c];
+    float wz = nb_pick(w2, c), dz = nb_pick(d2, c);
 #pragma unroll
     for (int jx = 0; jx < P; ++jx) {
       int gx = k0 - jx;
@@ -815,7 +815,7 @@ __global__ void __launch_bounds__(256) nb_spread_dipole(GridParams G, int64_t pl
         a2 = v.w * g.z * (float)G.K2 * G.invL2;
   int gz = k2 - c;
   if (gz < 0) gz += G.K2;
-  float wz = w2[c], dz = d2[c];
+  float wz = nb_pick(w2, c), dz = nb_pick(d2, c);
 #pragma unroll
   for (int jx = 0; jx < P; ++jx) {
     int gx = k0 - jx;
@@ -880,6 +880,85 @@ __global__ void __launch_bounds__(128) nb_pme_adjoint_gather(GridParams G, int64
   }
   double grad = g.x * g0 * G.K0 * G.invL0 + g.y * g1 * G.K1 * G.invL1 + g.z * g2 * G.K2 * G.invL2;
   out[p] += -grad - s;
+}
+
+// The same two terms with P threads per atom, one z point each (P a power
+// of two dividing 32), in f32 partial sums over each thread's P x P points,
+// summed over the P lanes by shuffles and added to the place's f64 value by
+// its first lane.
+template <int P, int MODE>
+__global__ void __launch_bounds__(128) nb_pme_adjoint_gather_split(GridParams G, int64_t places,
+                                                                   const int32_t *__restrict__ sizes,
+                                                                   const int32_t *__restrict__ order,
+                                                                   const float4 *__restrict__ xq,
+                                                                   const float4 *__restrict__ gp,
+                                                                   const float *__restrict__ phi,
+                                                                   const float *__restrict__ psi,
+                                                                   double *__restrict__ out) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t p = t / P;
+  int c = (int)(t & (P - 1));
+  bool live = p < places && p < sizes[NB_SIZE_PLACES];
+  bool atom = live && order[p] >= 0;
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f, sv = 0.f;
+  float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (atom) {
+    float4 v = xq[p];
+    if (MODE == 0) g = gp[p];
+    int k0, k1, k2;
+    float t0, t1, t2;
+    nb_frac(v.x, G.invL0, G.K0, k0, t0);
+    nb_frac(v.y, G.invL1, G.K1, k1, t1);
+    nb_frac(v.z, G.invL2, G.K2, k2, t2);
+    float w0[P], w1[P], w2[P], d0[P], d1[P], d2[P];
+    nb_bspline<P>(t0, w0, d0);
+    nb_bspline<P>(t1, w1, d1);
+    nb_bspline<P>(t2, w2, d2);
+    int gz = k2 - c;
+    if (gz < 0) gz += G.K2;
+    const float *sgrid = MODE == 0 ? psi : phi;
+#pragma unroll
+    for (int jx = 0; jx < P; ++jx) {
+      int gx = k0 - jx;
+      if (gx < 0) gx += G.K0;
+#pragma unroll
+      for (int jy = 0; jy < P; ++jy) {
+        int gy = k1 - jy;
+        if (gy < 0) gy += G.K1;
+        int64_t idx = ((int64_t)gx * G.K1 + gy) * G.K2 + gz;
+        float wxy = w0[jx] * w1[jy];
+        sv = fmaf(wxy, __ldg(sgrid + idx), sv);
+        if (MODE == 0) {
+          float f = __ldg(phi + idx);
+          g0 = fmaf(d0[jx] * w1[jy], f, g0);
+          g1 = fmaf(w0[jx] * d1[jy], f, g1);
+          g2 = fmaf(wxy, f, g2);
+        }
+      }
+    }
+    float wz = nb_pick(w2, c), dz = nb_pick(d2, c);
+    g0 *= wz;
+    g1 *= wz;
+    g2 *= dz;
+    sv *= wz;
+  }
+#pragma unroll
+  for (int o = P / 2; o > 0; o >>= 1) {
+    sv += __shfl_xor_sync(0xffffffffu, sv, o);
+    if (MODE == 0) {
+      g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+      g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+      g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+    }
+  }
+  if (!atom || c != 0) return;
+  if (MODE == 1) {
+    out[p] += (double)sv;
+    return;
+  }
+  double grad = (double)g.x * g0 * G.K0 * G.invL0 + (double)g.y * g1 * G.K1 * G.invL1 +
+                (double)g.z * g2 * G.K2 * G.invL2;
+  out[p] += -grad - (double)sv;
 }
 
 inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
@@ -1289,10 +1368,10 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s, 
   int blocks = blocks_for(c.places_cap, 128);
   if (mode == 1) {
     switch (P.order) {
-      case 4: nb_pme_adjoint_gather<4, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
+      case 4: nb_pme_adjoint_gather_split<4, 1><<<blocks_for(c.places_cap * 4, 128), 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
       case 5: nb_pme_adjoint_gather<5, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
       case 6: nb_pme_adjoint_gather<6, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
-      case 8: nb_pme_adjoint_gather<8, 1><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
+      case 8: nb_pme_adjoint_gather_split<8, 1><<<blocks_for(c.places_cap * 8, 128), 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, nullptr, phi, nullptr, c.adj_q); break;
     }
     return 0;
   }
@@ -1320,15 +1399,18 @@ int nb_pme_adjoint_run(NbCtx &c, const double box[3], int mode, cudaStream_t s, 
     if (nb_fft_convolve(P, P.adj_grid, nullptr, P.spec, P.adj_grid, P.influence, false, C, nullptr, nullptr, s))
       return -3;
   } else {
+    // the plans run on this call's stream (a forward may have left them on another)
+    cufftSetStream(P.fwd, s);
+    cufftSetStream(P.bwd, s);
     if (cufftExecR2C(P.fwd, P.adj_grid, (cufftComplex *)P.spec) != CUFFT_SUCCESS) return -3;
     nb_scale_spectrum<<<blocks_for(half, 256), 256, 0, s>>>(half, P.influence, P.spec, nullptr, 0, nullptr);
     if (cufftExecC2R(P.bwd, (cufftComplex *)P.spec, P.adj_grid) != CUFFT_SUCCESS) return -3;
   }
   switch (P.order) {
-    case 4: nb_pme_adjoint_gather<4, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
+    case 4: nb_pme_adjoint_gather_split<4, 0><<<blocks_for(c.places_cap * 4, 128), 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
     case 5: nb_pme_adjoint_gather<5, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
     case 6: nb_pme_adjoint_gather<6, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
-    case 8: nb_pme_adjoint_gather<8, 0><<<blocks, 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
+    case 8: nb_pme_adjoint_gather_split<8, 0><<<blocks_for(c.places_cap * 8, 128), 128, 0, s>>>(G, c.places_cap, c.sizes, c.order, c.xq, c.adj_g, phi, P.adj_grid, c.adj_q); break;
   }
   return 0;
 }
@@ -1384,7 +1466,7 @@ __global__ void __launch_bounds__(256) nb_batch_spread(int64_t places, const int
   nb_bspline<P>(t2, w2, nullptr);
   int gz = k2 - c;
   if (gz < 0) gz += G.K2;
-  float qz = v.w * w2[c];
+  float qz = v.w * nb_pick(w2, c);
 #pragma unroll
   for (int jx = 0; jx < P; ++jx) {
     int gx = k0 - jx;
@@ -1494,7 +1576,7 @@ __global__ void __launch_bounds__(128) nb_batch_gather_split(int64_t places, con
     nb_bspline<P>(t2, w2, d2);
     int gz = k2 - c;
     if (gz < 0) gz += G.K2;
-    float wz = w2[c], dz = d2[c];
+    float wz = nb_pick(w2, c), dz = nb_pick(d2, c);
 #pragma unroll
     for (int jx = 0; jx < P; ++jx) {
       int gx = k0 - jx;

@@ -106,3 +106,13 @@ __device__ __forceinline__ float3 nb_frac_force(const GridParams &G, float q, fl
   float ga = -q * g0 * (float)G.K0, gb = -q * g1 * (float)G.K1, gc = -q * g2 * (float)G.K2;
   return make_float3(ga * G.invL0, gb * G.invL1 + ga * G.h10, gc * G.invL2 + ga * G.h20 + gb * G.h21);
 }
+
+// a[c] for a lane-dependent c, picked by selects: a dynamic index would
+// put the array (registers of an unrolled spline) in local memory.
+template <int P>
+__device__ __forceinline__ float nb_pick(const float (&a)[P], int c) {
+  float v = 0.f;
+#pragma unroll
+  for (int j = 0; j < P; ++j) v = j == c ? a[j] : v;
+  return v;
+}

@@ -136,9 +136,15 @@ class FrameEvaluator:
     call, so a result does not depend on how the lanes' work interleaves.
     The caller's stream waits for the side lanes before a call returns, so
     the tensors of a call may be freed or reused on that stream at once
-    (torch's allocator hands a block back only to the stream it was made on)."""
+    (torch's allocator hands a block back only to the stream it was made on).
 
-    def __init__(self, system, device=0, sigma=None, epsilon=None, charges=None, lanes=4, keep_potentials=True):
+    With `frame_graphs` (the default) the library keeps the launches of each
+    lane's frames as a CUDA graph and replays it when a call repeats the
+    same buffers (mdrtNbForceFrames): a lane then takes all its frames of a
+    run in one native call."""
+
+    def __init__(self, system, device=0, sigma=None, epsilon=None, charges=None, lanes=4, keep_potentials=True,
+                 frame_graphs=True):
         self.system = system
         self.n = len(system["charges"])
         self.device = torch.device("cuda", device)
@@ -158,6 +164,7 @@ class FrameEvaluator:
         # potential grid (4 bytes a grid point a frame) for the adjoint
         self.grid = list(system["grid"]) if system.get("pme", True) else None
         self.keep_potentials = bool(keep_potentials) and self.grid is not None
+        self.frame_graphs = bool(frame_graphs)
         self.term = self._new_term()
         self.version = 0
         self._uploaded = -1
@@ -168,9 +175,14 @@ class FrameEvaluator:
         self._lane_streams = [None]
         self._lane_built = [0]
         self._lane_uploaded = [-1]
-        self._lane_sums = [None]
+        # the side lanes' gradient sums: charges (lanes - 1, n) and tables
+        # (lanes - 1, 2, nt, nt), made at the first product over several lanes
+        self._side_sums = None
         self._build_id = 0
         self._build_x = None
+        # (build, frames) of the last forces() call when one run served all
+        # its frames: the autograd op hands it to its product
+        self.last_run = None
 
     def _new_term(self):
         system = self.system
@@ -182,6 +194,8 @@ class FrameEvaluator:
                              lj_switch=system.get("lj_switch", False), switch_distance=system.get("switch", 0.0))
         if pme:
             term.set_pme(system["grid"], system["order"])
+        if not self.frame_graphs:
+            term.set_tuning(frame_graphs=False)
         return term
 
     # -- parameters ------------------------------------------------------------
@@ -211,6 +225,22 @@ class FrameEvaluator:
             self._uploaded = self.version
             self._lane_uploaded[0] = self.version
 
+    def lorentz_berthelot_chain_device(self, dtable):
+        """lorentz_berthelot_chain of a device table gradient (2, nt, nt), on
+        the device: the sigma and epsilon gradients (nt,) each, f64.  The
+        epsilon weights eps_ab / (2 eps_a) are uploaded once per set of
+        parameters."""
+        key = (self.version, self.device)
+        if getattr(self, "_lb_weights", (None,))[0] != key:
+            e = np.asarray(self.epsilon, dtype=np.float64)
+            eab = np.sqrt(e[:, None] * e[None, :])
+            with np.errstate(divide="ignore", invalid="ignore"):
+                w = np.where(e[:, None] > 0, eab / (2.0 * e[:, None]), 0.0)
+            self._lb_weights = (key, torch.as_tensor(w, dtype=torch.float64, device=self.device))
+        w = self._lb_weights[1]
+        S = dtable + dtable.transpose(1, 2)
+        return 0.5 * S[0].sum(dim=1), (S[1] * w).sum(dim=1)
+
     def per_type(self, dq, dtable):
         """{"sigma", "epsilon", "charges"} from the table gradient."""
         ds, de = lorentz_berthelot_chain(dtable.cpu().numpy(), self.sigma, self.epsilon)
@@ -230,14 +260,19 @@ class FrameEvaluator:
             raise ValueError(f"positions: (K, {self.n}, 3)")
         return X.contiguous()
 
-    def runs(self, X):
+    def runs(self, X, reuse=None):
         """Yields runs (k0, k1) of consecutive frames that one build serves,
         in order, building before a run where needed: the frames ahead are
         tested against the positions of the current build in one launch,
         and a frame that moved more than half the skin gets a new build
-        first."""
+        first.  `reuse`: the last_run of a forces() call on these same
+        frames, taken as it is (no displacement test) while its build is
+        still the one in force."""
         self._upload()
         K = X.shape[0]
+        if reuse is not None and reuse == (self._build_id, K) and self._built:
+            yield 0, K
+            return
         half_skin = 0.5 * (self.reach - self.cutoff)
         k = 0
         while k < K:
@@ -258,15 +293,19 @@ class FrameEvaluator:
         for k0, k1 in self.runs(X):
             yield from range(k0, k1)
 
-    # frames a lane takes in one native call before the next lane's turn:
-    # every lane gets work early, and the host still makes few calls
+    # frames a lane takes in one native call before the next lane's turn
+    # when the launches are not kept as graphs: every lane gets work early,
+    # and the host still makes few calls
     LANE_CHUNK = 2
 
     def _lanes_of_run(self, k0, k1, count):
         """(term, stream, first frame, end) of the native calls of the run
         [k0, k1): frame k goes to lane k mod count, as schedule() hands them
-        out, LANE_CHUNK frames of a lane a call, the lanes in turn."""
-        span = count * self.LANE_CHUNK
+        out, LANE_CHUNK frames of a lane a call, the lanes in turn; with
+        frame graphs a lane's frames of the run in one call (one graph
+        launch once its buffers repeat)."""
+        chunk = -(-(k1 - k0) // count) if self.frame_graphs else self.LANE_CHUNK
+        span = count * chunk
         for c0 in range(k0, k1, span):
             c1 = min(k1, c0 + span)
             for l in range(count):
@@ -295,10 +334,8 @@ class FrameEvaluator:
             self._lane_streams.append(torch.cuda.Stream(device=self.device))
             self._lane_built.append(0)
             self._lane_uploaded.append(-1)
-            self._lane_sums.append(None)
-        if sums:
-            for l in range(1, count):
-                self._zero_sums(l)
+        if sums and count > 1:
+            self._zero_sums(count)
         if count > 1:
             self._fork(range(1, count))
         return count
@@ -333,17 +370,16 @@ class FrameEvaluator:
             ev.record(self._lane_streams[l])
             cur.wait_event(ev)
 
-    def _zero_sums(self, l):
-        """Lane l's gradient sums (charges (n,), table (2, nt, nt)) set to zero
-        on the current stream."""
-        s = self._lane_sums[l]
-        if s is None:
-            self._lane_sums[l] = (torch.zeros(self.n, dtype=torch.float64, device=self.device),
-                                  torch.zeros((2, self.ntypes, self.ntypes), dtype=torch.float64,
-                                              device=self.device))
+    def _zero_sums(self, count):
+        """The side lanes' gradient sums of a call over `count` lanes, set to
+        zero on the current stream (two launches)."""
+        if self._side_sums is None or self._side_sums[0].shape[0] < count - 1:
+            self._side_sums = (torch.zeros((self.lanes - 1, self.n), dtype=torch.float64, device=self.device),
+                               torch.zeros((self.lanes - 1, 2, self.ntypes, self.ntypes), dtype=torch.float64,
+                                           device=self.device))
         else:
-            s[0].zero_()
-            s[1].zero_()
+            self._side_sums[0][:count - 1].zero_()
+            self._side_sums[1][:count - 1].zero_()
 
     def potential_buffers(self, frames):
         """A device f32 (frames, K1, K2, K3) buffer for the potential grids of
@@ -361,16 +397,21 @@ class FrameEvaluator:
         F = torch.empty_like(X) if out is None else out
         E = np.zeros(X.shape[0]) if energy else None
         count = self._open_lanes(X.shape[0])
+        self.last_run = None
         if not energy:
             # each lane's frames of a run in one native call (the host's
             # launch rate, not the GPU, bounds a call of many small frames)
+            done = []
             try:
                 for k0, k1 in self.runs(X):
+                    done.append((k0, k1))
                     for term, st, first, end in self._lanes_of_run(k0, k1, count):
                         term.force_frames(X[:end], first, count, F[:end],
                                           potentials=None if potentials is None else potentials[:end], stream=st)
             finally:
                 self._join(count)
+            if done == [(0, X.shape[0])]:
+                self.last_run = (self._build_id, X.shape[0])
             return F
         pending = {}  # lane -> the frame whose energies it holds
         try:
@@ -396,13 +437,14 @@ class FrameEvaluator:
         return (e["lj"] + e["coulomb"] + e["excluded"] + e["reciprocal"] + c["self"] + c["background"]
                 + c["dispersion"])
 
-    def product(self, positions, cotangent, dq=None, dtable=None, potentials=None):
+    def product(self, positions, cotangent, dq=None, dtable=None, potentials=None, run=None):
         """sum over frames of sum_i g_ni . dF_ni/dtheta for a cotangent g
         (K, n, 3) on the forces: the charge gradient (n,) and the table
         gradient (2, ntypes, ntypes), device f64, accumulated into dq and
         dtable when given.  `potentials`: the grids that forces() kept for
         these frames at these parameters (the reciprocal forward is then
-        not run again)."""
+        not run again); `run`: that call's last_run (the frames' test
+        against the build is then not made again)."""
         X = self.frames(positions)
         G = torch.as_tensor(cotangent, dtype=torch.float64, device=self.device).reshape(X.shape).contiguous()
         if dq is None:
@@ -410,9 +452,10 @@ class FrameEvaluator:
         if dtable is None:
             dtable = torch.zeros((2, self.ntypes, self.ntypes), dtype=torch.float64, device=self.device)
         count = self._open_lanes(X.shape[0], sums=True)
-        sums = [None] + [self._lane_sums[l] for l in range(1, count)]
+        side = self._side_sums
+        sums = [None] + [(side[0][l - 1], side[1][l - 1]) for l in range(1, count)]
         try:
-            for k0, k1 in self.runs(X):
+            for k0, k1 in self.runs(X, reuse=run):
                 for term, st, first, end in self._lanes_of_run(k0, k1, count):
                     l = first % count
                     q, t = (dq, dtable) if l == 0 else sums[l]
@@ -421,9 +464,10 @@ class FrameEvaluator:
                                                    stream=st)
         finally:
             self._join(count)
-        for l in range(1, count):
-            dq += sums[l][0]
-            dtable += sums[l][1]
+        if count > 1:
+            # the lanes' sums in a fixed order (one reduction each)
+            dq += side[0][:count - 1].sum(dim=0)
+            dtable += side[1][:count - 1].sum(dim=0)
         return dq, dtable
 
     def energy_gradient(self, positions):

@@ -63,6 +63,7 @@ class NonbondedTerm:
         self.pair_blocks_per_sm = 4
         self.fused_prune = 0
         self.staging_depth = 1
+        self.frame_graphs = True
 
     def close(self):
         if getattr(self, "_h", None):
@@ -122,14 +123,16 @@ class NonbondedTerm:
         L.check(L.lib().mdrtNbPrune(self._h, _dp(x), _hp(b), _stream(stream)), "mdrtNbPrune")
 
     def set_tuning(self, pair_blocks_per_sm=None, pair_sms=None, fused_prune=None, staging_depth=None,
-                   pme_fft=None, pme_spread=None):
+                   pme_fft=None, pme_spread=None, frame_graphs=None):
         """Launch shapes, the MD step's pruning in the pair kernel (0 by
         group count, 1 always, 2 never) and the PME transforms ("own", the
         library's three-kernel convolution where every grid dimension is 32,
         64 or 128; "cufft"): the autotuner's knobs; results do not depend on
         them beyond the order of f32 sums.  pme_spread: "auto" (global
         atomics, measured faster on the B200), "global" or "tiles"
-        (shared-memory tiles, the mixed mode)."""
+        (shared-memory tiles, the mixed mode).  frame_graphs: whether
+        force_frames and parameter_gradient_frames keep their launches as
+        CUDA graphs (True, the default)."""
         if pair_blocks_per_sm is not None:
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PAIR_BLOCKS_PER_SM, int(pair_blocks_per_sm)),
                     "mdrtNbSetTuning")
@@ -151,6 +154,16 @@ class NonbondedTerm:
             code = {"auto": 0, "global": 1, "tiles": 2}[pme_spread]
             L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_PME_SPREAD, code), "mdrtNbSetTuning")
             self.pme_spread = pme_spread
+        if frame_graphs is not None:
+            L.check(L.lib().mdrtNbSetTuning(self._h, L.TUNE_FRAME_GRAPHS, int(bool(frame_graphs))),
+                    "mdrtNbSetTuning")
+            self.frame_graphs = bool(frame_graphs)
+
+    def frame_graph_info(self):
+        """(captures, replays) of the frames entries' graphs so far."""
+        a, b = ctypes.c_int64(0), ctypes.c_int64(0)
+        L.check(L.lib().mdrtNbFrameGraphInfo(self._h, ctypes.byref(a), ctypes.byref(b)), "mdrtNbFrameGraphInfo")
+        return a.value, b.value
 
     def set_deterministic(self, on=True):
         L.check(L.lib().mdrtNbSetDeterministic(self._h, int(bool(on))), "mdrtNbSetDeterministic")

@@ -30,16 +30,29 @@ def _host(t):
     return t.detach().to("cpu", torch.float64).numpy()
 
 
+def _host_params(sigma, epsilon, charges):
+    """The three parameter tensors on the host, in one device-to-host copy."""
+    parts = [t.detach().reshape(-1).to(torch.float64) for t in (sigma, epsilon, charges)]
+    flat = torch.cat(parts).cpu().numpy()
+    a, b = parts[0].numel(), parts[0].numel() + parts[1].numel()
+    return flat[:a], flat[a:b], flat[b:]
+
+
 class _Forces(torch.autograd.Function):
     @staticmethod
     def forward(ctx, evaluator, positions, sigma, epsilon, charges):
-        evaluator.set_parameters(_host(sigma), _host(epsilon), _host(charges))
+        # the host copies are taken once, before the forward is queued, so
+        # that the host goes on to queue the loss and the backward while the
+        # forward runs
+        params = _host_params(sigma, epsilon, charges)
+        evaluator.set_parameters(*params)
         X = evaluator.frames(positions.detach())
         P = evaluator.potential_buffers(X.shape[0]) if evaluator.keep_potentials else None
         F = evaluator.forces(X, potentials=P)
         ctx.evaluator = evaluator
-        ctx.params = (_host(sigma), _host(epsilon), _host(charges))
+        ctx.params = params
         ctx.potentials = P
+        ctx.run = evaluator.last_run
         ctx.save_for_backward(X)
         return F.reshape(positions.shape)
 
@@ -50,12 +63,12 @@ class _Forces(torch.autograd.Function):
         ev = ctx.evaluator
         (X,) = ctx.saved_tensors
         ev.set_parameters(*ctx.params)
-        dq, dt = ev.product(X, grad.reshape(X.shape), potentials=ctx.potentials)
+        dq, dt = ev.product(X, grad.reshape(X.shape), potentials=ctx.potentials, run=ctx.run)
         ctx.potentials = None
-        ds, de = lorentz_berthelot_chain(dt.cpu().numpy(), ev.sigma, ev.epsilon)
-        dev = grad.device
-        return (None, None, torch.as_tensor(ds, device=dev) if ctx.needs_input_grad[2] else None,
-                torch.as_tensor(de, device=dev) if ctx.needs_input_grad[3] else None,
+        # the per-type gradients on the device (no wait for the product)
+        ds, de = ev.lorentz_berthelot_chain_device(dt)
+        return (None, None, ds.to(grad.dtype) if ctx.needs_input_grad[2] else None,
+                de.to(grad.dtype) if ctx.needs_input_grad[3] else None,
                 dq if ctx.needs_input_grad[4] else None)
 
 

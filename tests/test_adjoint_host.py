@@ -38,6 +38,27 @@ def test_lorentz_berthelot_chain_matches_differences():
             assert de[a] == 0.0
 
 
+def test_lorentz_berthelot_chain_on_the_device_side_is_the_host_chain():
+    """FrameEvaluator.lorentz_berthelot_chain_device (the autograd op's chain,
+    torch ops on the evaluator's device; here the CPU) equals the host chain,
+    and takes new weights when the parameters change."""
+    import types
+    import torch
+    from mdir_b200.frames import FrameEvaluator
+    rng = np.random.default_rng(12)
+    nt = 6
+    ev = types.SimpleNamespace(version=0, device=torch.device("cpu"), epsilon=rng.uniform(0.2, 1.0, nt))
+    ev.epsilon[2] = 0.0
+    for version in range(2):
+        ev.version = version
+        ev.epsilon = ev.epsilon * (1.0 + 0.1 * version)
+        A = rng.normal(size=(2, nt, nt))
+        ds, de = FrameEvaluator.lorentz_berthelot_chain_device(ev, torch.tensor(A))
+        hs, he = lorentz_berthelot_chain(A, np.full(nt, 0.3), ev.epsilon)
+        assert np.allclose(ds.numpy(), hs, rtol=1e-14, atol=0)
+        assert np.allclose(de.numpy(), he, rtol=1e-14, atol=0)
+
+
 def test_dispersion_gradient_matches_oracle_differences():
     s = systems.solvated_frame(1200, seed=3)
     s["dispersion"] = True
