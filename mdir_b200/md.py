@@ -92,14 +92,17 @@ class Integrator:
     def tune(self, x, v, box, dt, reaches=(1.3, 1.4, 1.5, 1.6, 1.7), pruned=(0.975, 1.0, 1.025, 1.05),
              pair_sms=(0, 112, 120, 128, 136), pair_blocks=(4, 3), depths=(1, 2), fused=(2, 1), steps=400, reps=3,
              stream=None):
-        """The autotuner of the step, in three stages: the outer and pruned
+        """The autotuner of the step, in four stages: the outer and pruned
         reaches first (the launch shapes as set), then the span of the pair
         grid (SMs; the others are left to the PME kernels beside it), its
         blocks per SM and its staging depth at the reaches kept, then the
-        pruning inside the pair
-        kernel (MDIR D284) or in a launch of its own.  Each choice is timed as `reps`
-        runs of `steps` steps after a build and half as many untimed steps;
-        the fastest is kept and built for.  x and v are put back; the step
+        three leading pairs of reaches again at that shape in runs twice as
+        long and more of them (the leaders differ by about the noise of the
+        short runs, and the best reaches depend on the shape), then the
+        pruning inside the pair kernel (MDIR D284) or in a launch of its
+        own.  Each choice is timed as `reps` runs of `steps` steps after a
+        build and half as many untimed steps; the fastest is kept and built
+        for.  x and v are put back; the step
         counter and the thermostat's noise move on.  MDIR searches its
         reaches the same way (the skins search, D281,
         lib/Compiler/Skins.cpp).  Returns the choice with its time per step
@@ -110,7 +113,7 @@ class Integrator:
         keep_x, keep_v = x.clone(), v.clone()
         st = stream if stream is not None else torch.cuda.current_stream(x.device)
 
-        def trial(R, Rin, sms, blocks, depth=None):
+        def trial(R, Rin, sms, blocks, depth=None, steps=steps, reps=reps):
             t.set_reach(R)
             t.set_pruned_reach(Rin)
             t.set_tuning(pair_sms=sms, pair_blocks_per_sm=blocks, staging_depth=depth)
@@ -147,6 +150,14 @@ class Integrator:
                     if (sms, blocks, depth) != (sms0, blocks0, depth0):
                         trials.append((trial(R, Rin, sms, blocks, depth), R, Rin, sms, blocks, depth))
         us, R, Rin, sms, blocks, depth = min(t_ for t_ in trials if t_[1] == R and t_[2] == Rin)
+        first = sorted((t_[0], t_[1], t_[2]) for t_ in trials if t_[3:] == (sms0, blocks0, depth0))
+        leaders = []
+        for _, R_, Rin_ in first:
+            if (R_, Rin_) not in leaders:
+                leaders.append((R_, Rin_))
+        final = [(trial(R_, Rin_, sms, blocks, depth, steps=2 * steps, reps=reps + 2), R_, Rin_)
+                 for R_, Rin_ in leaders[:3]]
+        us, R, Rin = min(final)
         t.set_tuning(staging_depth=depth)
         # the pruning in the pair kernel (MDIR D284) or in a launch of its
         # own, at the shape kept
@@ -167,7 +178,8 @@ class Integrator:
         v.copy_(keep_v)
         self.build(x, box, stream=st)
         return {"reach": R, "pruned_reach": Rin, "pair_sms": sms, "pair_blocks_per_sm": blocks,
-                "staging_depth": depth, "fused_prune": fchoice, "us_per_step": round(us, 2), "trials": len(trials) + len(fused_trials)}
+                "staging_depth": depth, "fused_prune": fchoice, "us_per_step": round(us, 2),
+                "trials": len(trials) + len(final) + len(fused_trials)}
 
     def temperature(self, stream=None):
         t = self.thermo(stream)
