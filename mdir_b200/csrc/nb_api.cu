@@ -223,6 +223,7 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   nb_free(c.q); nb_free(c.type); nb_free(c.lj); nb_free(c.ljf); nb_free(c.sigeps);
   nb_free(c.lj_on); nb_free(c.counts_lj);
   nb_free(c.adj_g); nb_free(c.adj_q); nb_free(c.adj_types); nb_free(c.x_build); nb_free(c.drift);
+  if (c.h_drift) cudaFreeHost(c.h_drift);
   nb_free(c.excl_off); nb_free(c.excl); nb_free(c.excl_pairs); nb_free(c.excl_partials);
   nb_free(c.order); nb_free(c.place_of); nb_free(c.shift); nb_free(c.xw);
   nb_free(c.box_lo); nb_free(c.box_hi); nb_free(c.group_start); nb_free(c.group_col);
@@ -663,9 +664,13 @@ int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, con
   cudaStream_t st = (cudaStream_t)stream;
   if (c.drift_cap < count) {
     nb_free(c.drift);
+    if (c.h_drift) cudaFreeHost(c.h_drift);
+    c.h_drift = nullptr;
     c.drift_cap = 0;
-    CK(cudaMalloc(&c.drift, sizeof(unsigned long long) * count));
-    c.drift_cap = count;
+    int64_t cap = std::max<int64_t>(count, 64);
+    CK(cudaMalloc(&c.drift, sizeof(unsigned long long) * cap));
+    CK(cudaMallocHost(&c.h_drift, sizeof(unsigned long long) * cap));
+    c.drift_cap = cap;
   }
   CK(cudaMemsetAsync(c.drift, 0, sizeof(unsigned long long) * count, st));
   int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (c.n + 255) / 256));
@@ -675,12 +680,11 @@ int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, con
                                                          box[2], c.drift + f0);
   }
   CK(cudaGetLastError());
-  std::vector<unsigned long long> bits(count);
-  CK(cudaMemcpyAsync(bits.data(), c.drift, sizeof(unsigned long long) * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c.h_drift, c.drift, sizeof(unsigned long long) * count, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   for (int64_t f = 0; f < count; ++f) {
     double d2;
-    std::memcpy(&d2, &bits[f], sizeof(double));
+    std::memcpy(&d2, &c.h_drift[f], sizeof(double));
     out[f] = std::sqrt(d2);
   }
   return MDRT_NB_OK;

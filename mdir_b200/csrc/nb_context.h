@@ -141,6 +141,7 @@ struct NbCtx {
   float4 *adj_g = nullptr;        // per place: the cotangent on the forces (f32)
   double *adj_q = nullptr;        // per place: the charge gradient, kept zero between calls
   double *adj_types = nullptr;    // per block of the adjoint kernel: 2 ntypes^2 partials
+  int adj_width = 0;              // the 2 ntypes^2 adj_types was sized for
   int64_t adj_places = 0;         // places_cap the per-place arrays were sized for
   int adj_blocks = 0;
   // the outer lists of a build without a pruned reach with each group's
@@ -158,6 +159,7 @@ struct NbCtx {
   // displacement maxima of mdrtNbDisplacement
   double *x_build = nullptr;
   unsigned long long *drift = nullptr;
+  unsigned long long *h_drift = nullptr;  // pinned mirror
   int64_t drift_cap = 0;
 };
 

@@ -843,18 +843,27 @@ __global__ void nb_sum_partials(const double *__restrict__ unit_partials,
 // (sigma, eps/sigma) per type pair, so the sigma term needs no division.
 // MDIR's counterpart is the IR-derived product of md-differentiate (D381,
 // docs/python-frames.md:203-260), which walks the neighbor matrix.
+// Warps a block of the adjoint kernel: few, so that a block whose warps
+// finish early (each takes a fixed share of units) soon frees its SM for
+// the kernels of the other frames running beside it.
+#ifndef NB_ADJ_WARPS
+#define NB_ADJ_WARPS 2
+#endif
+
 template <int MODE>
-__global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
+__global__ void __launch_bounds__(NB_ADJ_WARPS * 32, 32 / NB_ADJ_WARPS) nb_pairs_adjoint(
     PairParams P, const int32_t *__restrict__ sizes, const int2 *__restrict__ units, const int2 *__restrict__ slab,
     const int32_t *__restrict__ counts, const float4 *__restrict__ xq, const int32_t *__restrict__ typ,
     const float2 *__restrict__ sigeps, const float4 *__restrict__ gp, double *__restrict__ gq,
     double *__restrict__ type_partials, const int32_t *__restrict__ counts_lj) {
-  __shared__ float4 s_x[8][2 * NB_GROUP];
-  __shared__ float4 s_g[8][2 * NB_GROUP];  // the cotangent, and in w the member's type row (ntypes t)
-  __shared__ float2 s_se[NB_MAX_TYPES * NB_MAX_TYPES];
-  __shared__ float s_acc[2 * NB_MAX_TYPES * NB_MAX_TYPES];
+  __shared__ float4 s_x[NB_ADJ_WARPS][2 * NB_GROUP];
+  __shared__ float4 s_g[NB_ADJ_WARPS][2 * NB_GROUP];  // the cotangent, and in w the member's type row (ntypes t)
+  // (sigma, eps/sigma) per type pair, then the 2 ntypes^2 sums (dynamic: ntypes^2 x 16 bytes)
+  extern __shared__ float2 s_dyn[];
   const unsigned FULL = 0xffffffffu;
   int nt2 = P.ntypes * P.ntypes;
+  float2 *s_se = s_dyn;
+  float *s_acc = reinterpret_cast<float *>(s_dyn + nt2);
   for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
     float2 se = sigeps[k];
     s_se[k] = make_float2(se.x, se.x > 0.f ? se.y / se.x : 0.f);
@@ -868,8 +877,8 @@ __global__ void __launch_bounds__(256, 4) nb_pairs_adjoint(
   const float4 *px = &s_x[warp][u];
   const float4 *pg = &s_g[warp][u];
   int nunits = min((int64_t)sizes[NB_SIZE_UNITS], P.units_cap);
-  int wstride = gridDim.x * 8;
-  for (int unit = blockIdx.x * 8 + warp; unit < nunits; unit += wstride) {
+  int wstride = gridDim.x * NB_ADJ_WARPS;
+  for (int unit = blockIdx.x * NB_ADJ_WARPS + warp; unit < nunits; unit += wstride) {
     int2 uo = units[unit];
     int g = uo.x;
     int64_t pi = (int64_t)g * NB_GROUP + u;
@@ -1286,10 +1295,15 @@ void nb_reduce_energy(NbCtx &c, bool pairs, bool excluded, cudaStream_t s) {
 
 int nb_adjoint_reserve(NbCtx &c) {
   ensure_sm_count();
-  if (!c.adj_types) {
-    c.adj_blocks = g_sm_count * 4;
-    if (cudaMalloc(&c.adj_types, sizeof(double) * c.adj_blocks * 2 * NB_MAX_TYPES * NB_MAX_TYPES) != cudaSuccess)
-      return -1;
+  // per block of the adjoint kernel, the 2 ntypes^2 type-pair sums
+  int width = 2 * c.ntypes * c.ntypes;
+  if (!c.adj_types || c.adj_width < width) {
+    if (c.adj_types) cudaFree(c.adj_types);
+    c.adj_types = nullptr;
+    c.adj_width = 0;
+    c.adj_blocks = g_sm_count * (32 / NB_ADJ_WARPS);
+    if (cudaMalloc(&c.adj_types, sizeof(double) * c.adj_blocks * width) != cudaSuccess) return -1;
+    c.adj_width = width;
   }
   if (c.adj_places < c.places_cap) {
     if (c.adj_g) cudaFree(c.adj_g);
@@ -1333,9 +1347,10 @@ int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, c
   const int2 *lunits = inner ? c.units_in : c.units;
   const int2 *lslab = inner ? c.slab_in : c.slab;
   const int32_t *lcounts = inner ? c.counts_in : c.counts;
-  int64_t want = (c.units_cap + 7) / 8;
+  int64_t want = (c.units_cap + NB_ADJ_WARPS - 1) / NB_ADJ_WARPS;
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, c.adj_blocks));
   int width = 2 * c.ntypes * c.ntypes;
+  size_t smem = sizeof(float2) * c.ntypes * c.ntypes * 2;
   const int32_t *lj_counts =
       !inner && c.lj_part_build == c.builds && c.lj_part_mask == c.lj_mask ? c.counts_lj : nullptr;
   // the blocks' type-pair partials and the places' charge gradient (kept
@@ -1349,11 +1364,11 @@ int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, c
     const double *ck = mode == 0 ? cot + k * c_stride : nullptr;
     nb_gather_frames(c, xk, box, s, ck);
     if (mode == 0)
-      nb_pairs_adjoint<0><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
-                                               c.adj_q, c.adj_types, lj_counts);
+      nb_pairs_adjoint<0><<<grid, NB_ADJ_WARPS * 32, smem, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p,
+                                                                c.sigeps, c.adj_g, c.adj_q, c.adj_types, lj_counts);
     else
-      nb_pairs_adjoint<1><<<grid, 256, 0, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p, c.sigeps, c.adj_g,
-                                               c.adj_q, c.adj_types, lj_counts);
+      nb_pairs_adjoint<1><<<grid, NB_ADJ_WARPS * 32, smem, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p,
+                                                                c.sigeps, c.adj_g, c.adj_q, c.adj_types, lj_counts);
     int rc = nb_pme_adjoint_run(c, box, mode, s, phi ? phi + k * p_stride : nullptr);
     if (rc) return rc;
     if (c.n_excl_pairs > 0 && c.beta != 0.0) {

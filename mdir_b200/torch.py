@@ -30,12 +30,28 @@ def _host(t):
     return t.detach().to("cpu", torch.float64).numpy()
 
 
+_PINNED = {}
+
+
 def _host_params(sigma, epsilon, charges):
-    """The three parameter tensors on the host, in one device-to-host copy."""
-    parts = [t.detach().reshape(-1).to(torch.float64) for t in (sigma, epsilon, charges)]
-    flat = torch.cat(parts).cpu().numpy()
-    a, b = parts[0].numel(), parts[0].numel() + parts[1].numel()
-    return flat[:a], flat[a:b], flat[b:]
+    """The three parameter tensors on the host (f64 copies): three
+    asynchronous copies into a pinned buffer and one wait."""
+    parts = [t.detach().reshape(-1) for t in (sigma, epsilon, charges)]
+    sizes = [p.numel() for p in parts]
+    total = sum(sizes)
+    key = (total, parts[0].device)
+    buf = _PINNED.get(key)
+    if buf is None:
+        buf = torch.empty(total, dtype=torch.float64, pin_memory=parts[0].is_cuda)
+        _PINNED[key] = buf
+    at = 0
+    for p, k in zip(parts, sizes):
+        buf[at:at + k].copy_(p, non_blocking=True)
+        at += k
+    if parts[0].is_cuda:
+        torch.cuda.current_stream(parts[0].device).synchronize()
+    flat = buf.numpy().copy()
+    return flat[:sizes[0]], flat[sizes[0]:sizes[0] + sizes[1]], flat[sizes[0] + sizes[1]:]
 
 
 class _Forces(torch.autograd.Function):
