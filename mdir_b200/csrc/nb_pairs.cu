@@ -843,11 +843,13 @@ __global__ void nb_sum_partials(const double *__restrict__ unit_partials,
 // (sigma, eps/sigma) per type pair, so the sigma term needs no division.
 // MDIR's counterpart is the IR-derived product of md-differentiate (D381,
 // docs/python-frames.md:203-260), which walks the neighbor matrix.
-// Warps a block of the adjoint kernel: few, so that a block whose warps
-// finish early (each takes a fixed share of units) soon frees its SM for
-// the kernels of the other frames running beside it.
+// Warps a block of the adjoint kernel: one, so that a warp that finishes
+// early (each takes a fixed share of units) frees its place on the SM for
+// the kernels of the other frames running beside it at once, rather than
+// wait at the block's barrier (1, 2, 4 and 8 measured 2.78-2.81, 2.82-2.86,
+// 2.84-2.87 and 2.93 ms for the product of 64 frames on four lanes).
 #ifndef NB_ADJ_WARPS
-#define NB_ADJ_WARPS 2
+#define NB_ADJ_WARPS 1
 #endif
 
 template <int MODE>
