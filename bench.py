@@ -7,8 +7,10 @@ Workload: 7,850 rigid TIP3P waters (23,550 atoms) at 33.4 nm^-3, cutoff
 300 K (Bussi, 0.1 ps), dt 2 fs, mixed precision: the MD step of the device
 path (neighbor build when the test of validity asks, pair kernel, excluded
 correction, PME with cuFFT, leap-frog + SETTLE + thermostat) as a CUDA
-graph.  One bench step = `--md-steps` MD steps (one replay of the step
-graph); the L2 is flushed between bench steps (a 256 MiB write).  Metric:
+graph.  One bench step = `--md-steps` MD steps (1,000 by default, 2 ps:
+the interval at which a run usually writes a frame; replays of the step
+graph, then one read of the run's status); the L2 is flushed between bench
+steps (a 256 MiB write).  Metric:
 ns/day; with N GPUs, N independent replicas (the single box does not
 shard): `value` is their aggregate and `per_replica_ns_day` each box's.
 
@@ -47,7 +49,8 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--md-steps", type=int, default=100, help="MD steps per bench step")
+    p.add_argument("--md-steps", type=int, default=1000,
+                   help="MD steps per bench step (2 ps; a trajectory frame's usual interval)")
     p.add_argument("--unroll", type=int, default=10, help="MD steps per graph")
     p.add_argument("--waters", type=int, default=7850)
     p.add_argument("--reach", type=float, default=1.2, help="reach of the outer lists (nm)")
