@@ -221,6 +221,7 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   if (ctx->capture) cudaStreamDestroy(ctx->capture);
   nb_pme_release(c);
   nb_free(c.q); nb_free(c.type); nb_free(c.lj); nb_free(c.ljf); nb_free(c.sigeps);
+  nb_free(c.lj_on); nb_free(c.counts_lj);
   nb_free(c.adj_g); nb_free(c.adj_q); nb_free(c.adj_types); nb_free(c.x_build); nb_free(c.drift);
   if (c.h_drift) cudaFreeHost(c.h_drift);
   nb_free(c.excl_off); nb_free(c.excl); nb_free(c.excl_pairs); nb_free(c.excl_partials);
@@ -290,7 +291,15 @@ int32_t mdrtNbSetParticles(mdrtNb *ctx, const double *charges, const int32_t *ty
   if (!c.ljf) CK(cudaMalloc(&c.ljf, sizeof(float2) * 32));
   if (!c.lj) CK(cudaMalloc(&c.lj, sizeof(float2) * 32 * 32));
   if (!c.sigeps) CK(cudaMalloc(&c.sigeps, sizeof(float2) * 32 * 32));
-
+  if (!c.lj_on) CK(cudaMalloc(&c.lj_on, sizeof(int32_t) * 32));
+  int32_t on[32] = {0};
+  uint32_t mask = 0;
+  for (int a = 0; a < ntypes; ++a)
+    for (int b = 0; b < ntypes; ++b)
+      if (epsilon[a * ntypes + b] != 0.0) on[a] = 1;
+  for (int a = 0; a < ntypes; ++a) mask |= on[a] ? (1u << a) : 0u;
+  CK(cudaMemcpy(c.lj_on, on, sizeof(on), cudaMemcpyHostToDevice));
+  c.lj_mask = mask;
   CK(cudaMemcpy(c.ljf, factors.data(), sizeof(float2) * ntypes, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c.sigeps, se.data(), sizeof(float2) * ntypes * ntypes, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c.q, qf.data(), sizeof(float) * c.n, cudaMemcpyHostToDevice));
@@ -487,6 +496,7 @@ static int32_t nb_build_entry(mdrtNb *ctx, const double *x, int64_t n, const dou
   CK(cudaSetDevice(c.device));
   cudaStream_t st = (cudaStream_t)stream;
   if (nb_build_run(c, x, box, st)) return MDRT_NB_CUDA_ERROR;
+  if (nb_lj_partition_run(c, st)) return MDRT_NB_CUDA_ERROR;
   for (int k = 0; k < 3; ++k) c.tilt_built[k] = c.tilt[k];
   if (!c.x_build) CK(cudaMalloc(&c.x_build, sizeof(double) * 3 * c.n));
   CK(cudaMemcpyAsync(c.x_build, x, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToDevice, st));

@@ -252,6 +252,8 @@ int32_t mdrtNbBatchBuild(mdrtNbBatch *b, const double *x, const double *boxes, v
   CK(cudaSetDevice(c.device));
   if (boxes != b->h_boxes.data()) std::memcpy(b->h_boxes.data(), boxes, sizeof(double) * 3 * b->frames);
   if (nb_batch_build_run(*b, x, (cudaStream_t)stream)) return MDRT_NB_CUDA_ERROR;
+  // the lists ordered as a single system's build orders them
+  if (nb_lj_partition_run(c, (cudaStream_t)stream)) return MDRT_NB_CUDA_ERROR;
   if (sizes_out)
     for (int k = 0; k < NB_SIZE_COUNT; ++k) sizes_out[k] = c.h_sizes[k];
   if (c.h_sizes[NB_SIZE_NAN] > 0) return MDRT_NB_NAN_POSITION;

@@ -63,6 +63,8 @@ struct NbCtx {
   std::vector<int32_t> h_type;
   std::vector<float2> h_lj;
   float2 *sigeps = nullptr;    // (sigma, epsilon) per type pair, for the parameter gradient
+  int32_t *lj_on = nullptr;    // per type: 1 when an epsilon of its row is not 0 (device, 32 types)
+  uint32_t lj_mask = 0;        // the same, a bit per type
   // exclusions: ragged rows (atom order) and the list of pairs i < j
   int32_t *excl_off = nullptr, *excl = nullptr;
   int32_t *excl_pairs = nullptr;
@@ -142,6 +144,14 @@ struct NbCtx {
   int adj_width = 0;              // the 2 ntypes^2 adj_types was sized for
   int64_t adj_places = 0;         // places_cap the per-place arrays were sized for
   int adj_blocks = 0;
+  // the outer lists of a build without a pruned reach with each group's
+  // entries of a partner with Lennard-Jones terms first (nb_lj_partition_run):
+  // their count per group, for the build `lj_part_build` and the types of
+  // `lj_part_mask`; the adjoint's rounds after them skip their LJ terms
+  int32_t *counts_lj = nullptr;
+  int64_t counts_lj_cap = 0;
+  int64_t lj_part_build = -1;
+  uint32_t lj_part_mask = 0;
   // the columns and bins the buffers are planned for (one grid, or the
   // frames of a batch laid end to end)
   int64_t plan_cols = 0, plan_bins = 0;
@@ -326,6 +336,10 @@ int nb_pme_run(NbCtx &c, const double box[3], bool energy, bool potential, cudaS
 // ntypes^2 sigma entries then ntypes^2 epsilon entries), each reduced once
 // at the end of the call.  Needs the adjoint scratch (nb_adjoint_reserve).
 int nb_adjoint_reserve(NbCtx &c);
+// After a build (host, stream s): the stable partition of each group's
+// entries by whether the partner's type has LJ terms, when the lists are
+// the ones the kernels walk (no pruned reach) and fit the kernel's staging.
+int nb_lj_partition_run(NbCtx &c, cudaStream_t s);
 int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, const double box[3],
                    const double *cotangent, int64_t c_stride, int mode, const float *phi, int64_t p_stride,
                    double *dq, double *dtable, cudaStream_t s);

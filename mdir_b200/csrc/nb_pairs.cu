@@ -857,7 +857,7 @@ __global__ void __launch_bounds__(NB_ADJ_WARPS * 32, 32 / NB_ADJ_WARPS) nb_pairs
     PairParams P, const int32_t *__restrict__ sizes, const int2 *__restrict__ units, const int2 *__restrict__ slab,
     const int32_t *__restrict__ counts, const float4 *__restrict__ xq, const int32_t *__restrict__ typ,
     const float2 *__restrict__ sigeps, const float4 *__restrict__ gp, double *__restrict__ gq,
-    double *__restrict__ type_partials) {
+    double *__restrict__ type_partials, const int32_t *__restrict__ counts_lj) {
   __shared__ float4 s_x[NB_ADJ_WARPS][2 * NB_GROUP];
   __shared__ float4 s_g[NB_ADJ_WARPS][2 * NB_GROUP];  // the cotangent, and in w the member's type row (ntypes t)
   // (sigma, eps/sigma) per type pair, then the 2 ntypes^2 sums (dynamic: ntypes^2 x 16 bytes)
@@ -897,9 +897,13 @@ __global__ void __launch_bounds__(NB_ADJ_WARPS * 32, 32 / NB_ADJ_WARPS) nb_pairs
     int cnt = (int)min((int64_t)counts[g], P.list_cap);
     int e0 = uo.y * NB_UNIT;
     int ne = min(NB_UNIT, cnt - e0);
+    // with the lists partitioned (counts_lj), the rounds that start past a
+    // group's LJ partners have none (the same for the whole warp)
+    int nlj = counts_lj ? counts_lj[g] : cnt;
     float ai = 0.f;  // G_q of member (lane + k) mod 16
     for (int r = 0; r < 2; ++r) {
       if (r * 32 >= ne) break;
+      const bool lj_round = e0 + r * 32 < nlj;
       bool valid = r * 32 + lane < ne;
       int2 en = valid ? slab[(int64_t)g * P.list_cap + e0 + r * 32 + lane] : make_int2(0, 0);
       int q = en.x;
@@ -952,7 +956,7 @@ __global__ void __launch_bounds__(NB_ADJ_WARPS * 32, 32 / NB_ADJ_WARPS) nb_pairs
         }
         ai = fmaf(cq, fqj, ai);
         aj = fmaf(cq, xm.w, aj);
-        if (w != 0.f) {
+        if (lj_round && w != 0.f) {
           int tp = __float_as_int(gm.w) + tj;
           float2 se = s_se[tp];  // (sigma, eps / sigma)
           if (se.y != 0.f) {
@@ -998,6 +1002,45 @@ __global__ void nb_scatter_place_values(int64_t places, const int32_t *__restric
     if (a >= 0) out[a] += v;
     vp[p] = 0.0;
   }
+}
+
+// The stable partition of each group's list by the partner's LJ terms: the
+// entries whose partner's type has any, then the others, each in their
+// order; counts_lj[g] gets the number of the first.  One warp a group, its
+// entries staged in shared memory (list_cap of them).
+__global__ void __launch_bounds__(32) nb_lj_partition(const int32_t *__restrict__ sizes, int64_t list_cap,
+                                                      const int32_t *__restrict__ counts, int2 *__restrict__ slab,
+                                                      const int32_t *__restrict__ order,
+                                                      const int32_t *__restrict__ type,
+                                                      const int32_t *__restrict__ lj_on,
+                                                      int32_t *__restrict__ counts_lj) {
+  extern __shared__ int2 s_e[];
+  int64_t g = blockIdx.x;
+  if (g >= sizes[NB_SIZE_GROUPS]) return;
+  int lane = threadIdx.x;
+  int cnt = (int)min((int64_t)counts[g], list_cap);
+  int2 *row = slab + g * list_cap;
+  for (int e = lane; e < cnt; e += 32) s_e[e] = row[e];
+  __syncwarp();
+  auto lj = [&](int e) {
+    int a = order[s_e[e].x];
+    return a >= 0 && lj_on[type[a]] != 0;
+  };
+  int nlj = 0;
+  for (int e0 = 0; e0 < cnt; e0 += 32) nlj += __popc(__ballot_sync(0xffffffffu, e0 + lane < cnt && lj(e0 + lane)));
+  int pl = 0, pn = nlj;
+  unsigned below = (1u << lane) - 1u;
+  for (int e0 = 0; e0 < cnt; e0 += 32) {
+    int e = e0 + lane;
+    bool in = e < cnt;
+    bool f = in && lj(e);
+    unsigned bl = __ballot_sync(0xffffffffu, f);
+    unsigned bn = __ballot_sync(0xffffffffu, in && !f);
+    if (in) row[f ? pl + __popc(bl & below) : pn + __popc(bn & below)] = s_e[e];
+    pl += __popc(bl);
+    pn += __popc(bn);
+  }
+  if (lane == 0) counts_lj[g] = nlj;
 }
 
 // The excluded pairs, u = -f q_i q_j erf(beta r)/r, in f64 and atom order.
@@ -1278,6 +1321,25 @@ int nb_adjoint_reserve(NbCtx &c) {
   return 0;
 }
 
+int nb_lj_partition_run(NbCtx &c, cudaStream_t s) {
+  c.lj_part_build = -1;
+  size_t stage = sizeof(int2) * (size_t)c.list_cap;
+  if (c.inner_reach > 0.0 || !c.lj_on || c.groups_cap <= 0 || c.list_cap <= 0 || stage > 48 * 1024) return 0;
+  if (c.counts_lj_cap < c.groups_cap) {
+    if (c.counts_lj) cudaFree(c.counts_lj);
+    c.counts_lj = nullptr;
+    c.counts_lj_cap = 0;
+    if (cudaMalloc(&c.counts_lj, sizeof(int32_t) * c.groups_cap) != cudaSuccess) return -1;
+    c.counts_lj_cap = c.groups_cap;
+  }
+  nb_lj_partition<<<(unsigned)c.groups_cap, 32, stage, s>>>(c.sizes, c.list_cap, c.counts, c.slab, c.order, c.type,
+                                                            c.lj_on, c.counts_lj);
+  if (cudaGetLastError() != cudaSuccess) return -1;
+  c.lj_part_build = c.builds;
+  c.lj_part_mask = c.lj_mask;
+  return 0;
+}
+
 int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, const double box[3],
                    const double *cot, int64_t c_stride, int mode, const float *phi, int64_t p_stride, double *dq,
                    double *dtable, cudaStream_t s) {
@@ -1291,6 +1353,8 @@ int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, c
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, c.adj_blocks));
   int width = 2 * c.ntypes * c.ntypes;
   size_t smem = sizeof(float2) * c.ntypes * c.ntypes * 2;
+  const int32_t *lj_counts =
+      !inner && c.lj_part_build == c.builds && c.lj_part_mask == c.lj_mask ? c.counts_lj : nullptr;
   // the blocks' type-pair partials and the places' charge gradient (kept
   // zero between calls) sum the frames; both go out once at the end
   if (cudaMemsetAsync(c.adj_types, 0, sizeof(double) * grid * width, s) != cudaSuccess) return -1;
@@ -1303,10 +1367,10 @@ int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, c
     nb_gather_frames(c, xk, box, s, ck);
     if (mode == 0)
       nb_pairs_adjoint<0><<<grid, NB_ADJ_WARPS * 32, smem, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p,
-                                                                c.sigeps, c.adj_g, c.adj_q, c.adj_types);
+                                                                c.sigeps, c.adj_g, c.adj_q, c.adj_types, lj_counts);
     else
       nb_pairs_adjoint<1><<<grid, NB_ADJ_WARPS * 32, smem, s>>>(P, lsizes, lunits, lslab, lcounts, c.xq, c.typ_p,
-                                                                c.sigeps, c.adj_g, c.adj_q, c.adj_types);
+                                                                c.sigeps, c.adj_g, c.adj_q, c.adj_types, lj_counts);
     int rc = nb_pme_adjoint_run(c, box, mode, s, phi ? phi + k * p_stride : nullptr);
     if (rc) return rc;
     if (c.n_excl_pairs > 0 && c.beta != 0.0) {

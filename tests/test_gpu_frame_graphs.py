@@ -107,3 +107,42 @@ def test_loss_gradient_with_and_without_graphs():
     for a, b in zip(*grads):
         assert np.max(np.abs(a - b)) <= 1e-5 * np.max(np.abs(b))
 
+
+def test_lists_put_lj_partners_first():
+    """A build without a pruned reach orders each group's entries with the
+    partners that have Lennard-Jones terms first (the adjoint skips its LJ
+    terms in the rounds after them), and the pair set stays the oracle's."""
+    from mdir_b200 import NonbondedTerm
+    from mdir_b200 import _lib as L
+    from oracle import oracle as O
+    s = systems.tip3p(waters=600)
+    x = np.asarray(s["positions"])
+    t = NonbondedTerm(len(x))
+    t.set_particles(s["charges"], s["types"], s["sigma"], s["epsilon"])
+    t.set_exclusions(pairs=s["excluded_pairs"])
+    t.set_interaction(s["cutoff"], s["reach"], s["beta"])
+    sizes = t.build(torch.tensor(x, device="cuda"), s["box"])
+    G = int(sizes[L.SIZE_GROUPS])
+    cap = t.info()["list_capacity"]
+    entries = t.buffer(L.SLOT_ENTRIES, np.int32, 2)[: G * cap].reshape(G, cap, 2)
+    counts = t.buffer(L.SLOT_COUNTS, np.int32)[:G]
+    order = t.buffer(L.SLOT_ORDER, np.int32)
+    eps = np.asarray(s["epsilon"])
+    lj_type = np.any(eps != 0.0, axis=1)
+    types = np.asarray(s["types"])
+    assert lj_type.any() and not lj_type.all()
+    mixed = 0
+    for g in range(G):
+        partners = entries[g, : counts[g], 0]
+        flags = lj_type[types[order[partners]]]
+        # every LJ partner before every other one
+        assert not np.any(flags[1:] & ~flags[:-1]), g
+        mixed += bool(flags.any() and not flags.all())
+    assert mixed > 0
+    got = np.asarray(t.pair_set(sizes), dtype=np.int64)
+    count, ref = O.pairset(x, s["box"], s["reach"], O.rows_from_pairs(len(x), s["excluded_pairs"]))
+    ref = np.asarray(ref, dtype=np.int64)
+    assert len(got) == count
+    key = lambda p: p[np.lexsort((p[:, 2], p[:, 1], p[:, 0]))]
+    np.testing.assert_array_equal(key(got), key(ref))
+    t.close()
