@@ -1081,18 +1081,26 @@ __global__ void nb_charge_terms(int64_t n, const float *__restrict__ q, double s
 }
 
 // Fixed-order sum of the per-block type-pair partials, added into out: a
-// warp per value, lane l summing blocks l, l + 32, ... in turn, then the
-// lanes by a fixed shuffle tree (the same order every call, 19 dependent
-// loads a lane where one thread a value took 592).
-__global__ void nb_sum_type_partials(const double *__restrict__ partials, int nblocks, int width,
-                                     double *__restrict__ out) {
-  int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (k >= width) return;  // whole warps
+// block of NB_SUM_THREADS per value, thread t summing blocks t, t + 256, ...
+// in turn, then the threads by a fixed tree (the same order every call).
+// The partials are block-major (each adjoint block writes its row whole).
+#define NB_SUM_THREADS 256
+__global__ void __launch_bounds__(NB_SUM_THREADS) nb_sum_type_partials(const double *__restrict__ partials,
+                                                                      int nblocks, int width,
+                                                                      double *__restrict__ out) {
+  __shared__ double s_sum[NB_SUM_THREADS / 32];
+  const int k = blockIdx.x, t = threadIdx.x;
   double s = 0.0;
-  for (int b = lane; b < nblocks; b += 32) s += partials[(int64_t)b * width + k];
+  for (int b = t; b < nblocks; b += NB_SUM_THREADS) s += partials[(int64_t)b * width + k];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) out[k] += s;
+  if ((t & 31) == 0) s_sum[t >> 5] = s;
+  __syncthreads();
+  if (t == 0) {
+    double total = 0.0;
+    for (int w = 0; w < NB_SUM_THREADS / 32; ++w) total += s_sum[w];
+    out[k] += total;
+  }
 }
 
 inline int blocks_for(int64_t n, int t) { return (int)std::max<int64_t>(1, (n + t - 1) / t); }
@@ -1324,7 +1332,20 @@ int nb_adjoint_reserve(NbCtx &c) {
 int nb_lj_partition_run(NbCtx &c, cudaStream_t s) {
   c.lj_part_build = -1;
   size_t stage = sizeof(int2) * (size_t)c.list_cap;
-  if (c.inner_reach > 0.0 || !c.lj_on || c.groups_cap <= 0 || c.list_cap <= 0 || stage > 48 * 1024) return 0;
+  if (c.inner_reach > 0.0 || !c.lj_on || c.groups_cap <= 0 || c.list_cap <= 0 || stage > 227 * 1024) return 0;
+  if (stage > 48 * 1024) {
+    // the shared-memory opt-in for this list capacity (once per device and size)
+    static size_t configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 0;
+    if (configured[dev] < stage) {
+      if (cudaFuncSetAttribute(nb_lj_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage) !=
+          cudaSuccess)
+        return -1;
+      configured[dev] = stage;
+    }
+  }
   if (c.counts_lj_cap < c.groups_cap) {
     if (c.counts_lj) cudaFree(c.counts_lj);
     c.counts_lj = nullptr;
@@ -1389,7 +1410,7 @@ int nb_adjoint_run(NbCtx &c, const double *x, int64_t x_stride, int64_t count, c
       nb_charge_terms<<<blocks_for(c.n, 256), 256, 0, s>>>(c.n, c.q, self2, background, dq);
     }
   }
-  nb_sum_type_partials<<<blocks_for((int64_t)width * 32, 256), 256, 0, s>>>(c.adj_types, grid, width, dtable);
+  nb_sum_type_partials<<<width, NB_SUM_THREADS, 0, s>>>(c.adj_types, grid, width, dtable);
   nb_scatter_place_values<<<blocks_for(c.places_cap, 256), 256, 0, s>>>(c.places_cap, c.sizes, c.order, c.adj_q,
                                                                         dq);
   return 0;
