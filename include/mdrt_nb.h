@@ -268,6 +268,17 @@ int32_t mdrtPmePotential(mdrtNb *ctx, double *potential, void *stream);
 int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, const double box[3],
                            double *out, void *stream);
 
+/* The same test in two halves, so that the caller can queue work between
+ * them: mdrtNbDisplacementStart queues the test and the copy of its result
+ * on `stream` without waiting; mdrtNbDisplacementResult waits for that copy
+ * (not for the rest of the stream) and writes out[count] as
+ * mdrtNbDisplacement.  A frames call queued in between reads the lists as
+ * they are; the caller evaluates again, after a build, the frames that the
+ * result puts past half the skin. */
+int32_t mdrtNbDisplacementStart(mdrtNb *ctx, const double *frames, int64_t count, const double box[3],
+                                void *stream);
+int32_t mdrtNbDisplacementResult(mdrtNb *ctx, double *out);
+
 /* Modes of mdrtNbParameterGradient. */
 enum mdrtNbGradientMode {
   MDRT_NB_GRAD_PRODUCT = 0,  /* sum_k g_k . dF_k/dtheta for a cotangent g on the forces */

@@ -51,6 +51,8 @@ SIGNATURES = {
     "mdrtNbConstants": (_i32, [_p, _p, _i32, _p]),
     "mdrtPmePotential": (_i32, [_p, _p, _p]),
     "mdrtNbDisplacement": (_i32, [_p, _p, _i64, _p, _p, _p]),
+    "mdrtNbDisplacementStart": (_i32, [_p, _p, _i64, _p, _p]),
+    "mdrtNbDisplacementResult": (_i32, [_p, _p]),
     "mdrtNbParameterGradient": (_i32, [_p, _p, _p, _p, _i32, _p, _p, _p]),
     "mdrtNbParameterGradientPotential": (_i32, [_p, _p, _p, _p, _i32, _p, _p, _p, _p]),
     "mdrtPmePotentialGrid": (_i32, [_p, _p, _p]),

@@ -224,6 +224,7 @@ int32_t mdrtNbDestroy(mdrtNb *ctx) {
   nb_free(c.lj_on); nb_free(c.counts_lj);
   nb_free(c.adj_g); nb_free(c.adj_q); nb_free(c.adj_types); nb_free(c.x_build); nb_free(c.drift);
   if (c.h_drift) cudaFreeHost(c.h_drift);
+  if (ctx->drift_done) cudaEventDestroy(ctx->drift_done);
   nb_free(c.excl_off); nb_free(c.excl); nb_free(c.excl_pairs); nb_free(c.excl_partials);
   nb_free(c.order); nb_free(c.place_of); nb_free(c.shift); nb_free(c.xw);
   nb_free(c.box_lo); nb_free(c.box_hi); nb_free(c.group_start); nb_free(c.group_col);
@@ -653,14 +654,18 @@ int32_t mdrtNbFrameGraphInfo(mdrtNb *ctx, int64_t *captures, int64_t *replays) {
   return MDRT_NB_OK;
 }
 
-int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, const double box[3], double *out,
-                           void *stream) {
-  if (!ctx || !box || count < 0 || (count > 0 && (!frames || !out))) return MDRT_NB_INVALID_ARGUMENT;
+int32_t mdrtNbDisplacementStart(mdrtNb *ctx, const double *frames, int64_t count, const double box[3],
+                                void *stream) {
+  if (!ctx || !box || count < 0 || (count > 0 && !frames)) return MDRT_NB_INVALID_ARGUMENT;
   NbCtx &c = ctx->c;
   if (!c.built || !c.x_build) return MDRT_NB_NOT_BUILT;
   if (nb_triclinic(c)) return MDRT_NB_UNSUPPORTED;  // per-axis minimum image
-  if (count == 0) return MDRT_NB_OK;
   CK(cudaSetDevice(c.device));
+  ctx->drift_count = -1;
+  if (count == 0) {
+    ctx->drift_count = 0;
+    return MDRT_NB_OK;
+  }
   cudaStream_t st = (cudaStream_t)stream;
   if (c.drift_cap < count) {
     nb_free(c.drift);
@@ -672,6 +677,7 @@ int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, con
     CK(cudaMallocHost(&c.h_drift, sizeof(unsigned long long) * cap));
     c.drift_cap = cap;
   }
+  if (!ctx->drift_done) CK(cudaEventCreateWithFlags(&ctx->drift_done, cudaEventDisableTiming));
   CK(cudaMemsetAsync(c.drift, 0, sizeof(unsigned long long) * count, st));
   int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (c.n + 255) / 256));
   for (int64_t f0 = 0; f0 < count; f0 += 65535) {
@@ -681,13 +687,34 @@ int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, con
   }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c.h_drift, c.drift, sizeof(unsigned long long) * count, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  CK(cudaEventRecord(ctx->drift_done, st));
+  ctx->drift_count = count;
+  return MDRT_NB_OK;
+}
+
+int32_t mdrtNbDisplacementResult(mdrtNb *ctx, double *out) {
+  if (!ctx) return MDRT_NB_INVALID_ARGUMENT;
+  NbCtx &c = ctx->c;
+  if (ctx->drift_count < 0) return MDRT_NB_INVALID_ARGUMENT;  // no test started
+  int64_t count = ctx->drift_count;
+  ctx->drift_count = -1;
+  if (count == 0) return MDRT_NB_OK;
+  if (!out) return MDRT_NB_INVALID_ARGUMENT;
+  CK(cudaEventSynchronize(ctx->drift_done));
   for (int64_t f = 0; f < count; ++f) {
     double d2;
     std::memcpy(&d2, &c.h_drift[f], sizeof(double));
     out[f] = std::sqrt(d2);
   }
   return MDRT_NB_OK;
+}
+
+int32_t mdrtNbDisplacement(mdrtNb *ctx, const double *frames, int64_t count, const double box[3], double *out,
+                           void *stream) {
+  if (!ctx || !box || count < 0 || (count > 0 && (!frames || !out))) return MDRT_NB_INVALID_ARGUMENT;
+  int32_t s = mdrtNbDisplacementStart(ctx, frames, count, box, stream);
+  if (s) return s;
+  return mdrtNbDisplacementResult(ctx, out);
 }
 
 int32_t mdrtNbParameterGradient(mdrtNb *ctx, const double *x, const double box[3], const double *cotangent,

@@ -190,6 +190,11 @@ struct mdrtNb {
   uint64_t graph_clock = 0;
   cudaStream_t capture = nullptr;  // the frames graphs are captured on this stream
   int64_t graph_captures = 0, graph_replays = 0;
+  // a started displacement test (mdrtNbDisplacementStart): the event after
+  // the copy of its result and its frames (-1 when none is pending); kept
+  // out of NbCtx, whose bytes key the frames graphs
+  cudaEvent_t drift_done = nullptr;
+  int64_t drift_count = -1;
 };
 
 // One frame of a batch, as the kernels read it: the cell, its grid of

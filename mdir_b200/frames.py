@@ -401,17 +401,42 @@ class FrameEvaluator:
         if not energy:
             # each lane's frames of a run in one native call (the host's
             # launch rate, not the GPU, bounds a call of many small frames)
+            K = X.shape[0]
+
+            def launch(k0, k1):
+                for term, st, first, end in self._lanes_of_run(k0, k1, count):
+                    term.force_frames(X[:end], first, count, F[:end],
+                                      potentials=None if potentials is None else potentials[:end], stream=st)
+
             done = []
             try:
-                for k0, k1 in self.runs(X):
-                    done.append((k0, k1))
-                    for term, st, first, end in self._lanes_of_run(k0, k1, count):
-                        term.force_frames(X[:end], first, count, F[:end],
-                                          potentials=None if potentials is None else potentials[:end], stream=st)
+                start = 0
+                if self._built:
+                    # the frames go on the build in force while their test
+                    # runs ahead of them on the device; its result, read
+                    # after they are queued, sends the frames from the first
+                    # that moved past half the skin round again after a build
+                    self._upload()
+                    pending = self.term.displacement_start(X)
+                    launch(0, K)
+                    d = self.term.displacement_result(pending)
+                    bad = np.nonzero(~(d < 0.5 * (self.reach - self.cutoff)))[0]
+                    start = int(bad[0]) if len(bad) else K
+                    if start == K:
+                        done.append((0, K))
+                    else:
+                        # the lanes' frames read the old lists: they finish
+                        # before a build writes new ones
+                        self._join(count)
+                        self._fork(range(1, count))
+                if start < K:
+                    for k0, k1 in self.runs(X[start:]):
+                        done.append((start + k0, start + k1))
+                        launch(start + k0, start + k1)
             finally:
                 self._join(count)
-            if done == [(0, X.shape[0])]:
-                self.last_run = (self._build_id, X.shape[0])
+            if done == [(0, K)]:
+                self.last_run = (self._build_id, K)
             return F
         pending = {}  # lane -> the frame whose energies it holds
         try:

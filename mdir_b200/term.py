@@ -273,6 +273,25 @@ class NonbondedTerm:
                 "mdrtNbDisplacement")
         return out
 
+    def displacement_start(self, frames, box=None, stream=None):
+        """Queues the test of displacement() without waiting; returns the
+        frame count for displacement_result()."""
+        if not (frames.is_cuda and frames.dtype == torch.float64 and frames.is_contiguous()
+                and frames.shape[-2:] == (self.n, 3)):
+            raise ValueError("frames: a contiguous CUDA float64 tensor of shape (K, n, 3)")
+        count = frames.numel() // (3 * self.n)
+        b = _host(self.box if box is None else box, np.float64)
+        L.check(L.lib().mdrtNbDisplacementStart(self._h, _dp(frames), count, _hp(b), _stream(stream)),
+                "mdrtNbDisplacementStart")
+        return count
+
+    def displacement_result(self, count):
+        """The result of the test displacement_start() queued (host f64
+        (count,)); waits for that test only."""
+        out = np.zeros(count)
+        L.check(L.lib().mdrtNbDisplacementResult(self._h, _hp(out)), "mdrtNbDisplacementResult")
+        return out
+
     def potential_grid(self, out=None, stream=None):
         """The reciprocal potential grid of the last force evaluation (device
         f32 of the grid's shape), into `out` when given."""

@@ -146,3 +146,23 @@ def test_lists_put_lj_partners_first():
     key = lambda p: p[np.lexsort((p[:, 2], p[:, 1], p[:, 0]))]
     np.testing.assert_array_equal(key(got), key(ref))
     t.close()
+
+
+def test_frames_past_the_skin_mid_call_are_evaluated_again():
+    """The frames of a call go on the build in force while their test runs;
+    when frames from the middle of the call on moved past half the skin,
+    those are evaluated again after a build.  Each frame's forces equal
+    those of the frame evaluated alone, with lists built at it."""
+    s, X, target = systems.force_matching(frames=8, waters=900)
+    X = X.copy()
+    X[5:] += 0.3  # every atom of frames 5.. moved 0.52 nm, past half the skin
+    ev = FrameEvaluator(s, lanes=3)
+    Xd = torch.tensor(X, device="cuda")
+    for _ in range(2):
+        ev.forces(Xd[:1])  # a build at frame 0
+        F = ev.forces(Xd).cpu().numpy()
+    for k in range(8):
+        one = FrameEvaluator(s, lanes=1, frame_graphs=False)
+        ref = one.forces(Xd[k:k + 1]).cpu().numpy()[0]
+        err = np.sqrt(np.mean(np.sum((F[k] - ref) ** 2, 1)) / np.mean(np.sum(ref ** 2, 1)))
+        assert err < 1e-6, (k, err)
