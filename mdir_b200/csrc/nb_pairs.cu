@@ -388,8 +388,16 @@ __device__ __forceinline__ void nb_pair_unit(const PairParams &P, int2 uo, int64
 // (the force forms read the next unit's header during a unit, the energy
 // forms each round's entries when they come to it); 2, the next unit's
 // header and entries are in flight during a unit (four more registers).
+// Warps a block of the pair kernel (a persistent grid of
+// pair_blocks_per_sm x 8 / NB_PAIR_WARPS blocks an SM).  The MD step of the
+// 23,550-atom box measured 54.2-54.3 µs with 8, 54.9-55.2 with 2 and
+// 55.9-56.7 with 1, side by side (unlike the adjoint, no other kernel waits
+// for the SMs its early warps would free).
+#ifndef NB_PAIR_WARPS
+#define NB_PAIR_WARPS 8
+#endif
 template <bool ENERGY, bool FIXED, int SWITCH, int LJM, bool BATCH = false, int DEPTH = 1>
-__global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *__restrict__ group_L,
+__global__ void __launch_bounds__(NB_PAIR_WARPS * 32, 32 / NB_PAIR_WARPS) nb_pairs(PairParams P, const float4 *__restrict__ group_L,
                                                 const int32_t *__restrict__ sizes,
                                                 const int2 *__restrict__ units,
                                                 const int2 *__restrict__ slab,
@@ -407,12 +415,12 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   nb_grid_wait();  // the lists and frames of the kernels before (a chained launch)
   if (halt && *halt) return;  // the MD step stopped at a stale list (its host rebuilds)
   if (skip && *skip) return;  // a pruning step: the pruning kernel computed the pairs
-  __shared__ float4 s_x[8][2 * NB_GROUP];
-  __shared__ float4 s_l[8][FIXED ? 2 * NB_GROUP : 1];  // FIXED: the members' frame residuals
-  __shared__ float2 s_f[8][2 * NB_GROUP];  // LJM 1: member factors
-  __shared__ int s_t[8][2 * NB_GROUP];     // LJM 0: member row offsets in s_lj
+  __shared__ float4 s_x[NB_PAIR_WARPS][2 * NB_GROUP];
+  __shared__ float4 s_l[NB_PAIR_WARPS][FIXED ? 2 * NB_GROUP : 1];  // FIXED: the members' frame residuals
+  __shared__ float2 s_f[NB_PAIR_WARPS][2 * NB_GROUP];  // LJM 1: member factors
+  __shared__ int s_t[NB_PAIR_WARPS][2 * NB_GROUP];     // LJM 0: member row offsets in s_lj
   __shared__ float2 s_lj[LJM == 0 ? NB_MAX_TYPES * NB_MAX_TYPES : 1];
-  __shared__ float s_b[8][3][NB_SPARSE_BITS][33];  // member forces of a sparse round (33: no bank conflicts)
+  __shared__ float s_b[NB_PAIR_WARPS][3][NB_SPARSE_BITS][33];  // member forces of a sparse round (33: no bank conflicts)
   if (LJM == 0) {  // (6 c6, 12 c12): the force's factors
     int nt2 = P.ntypes * P.ntypes;
     for (int k = threadIdx.x; k < nt2; k += blockDim.x) {
@@ -423,10 +431,10 @@ __global__ void __launch_bounds__(256, 4) nb_pairs(PairParams P, const float4 *_
   }
   int warp = threadIdx.x >> 5;
   int nunits = min((int64_t)sizes[NB_SIZE_UNITS], P.units_cap);
-  int wstride = gridDim.x * 8;
+  int wstride = gridDim.x * NB_PAIR_WARPS;
   // the next unit's header is in flight during this unit (the energy forms,
   // short of registers, read it when they come to it)
-  int unit = blockIdx.x * 8 + warp;
+  int unit = blockIdx.x * NB_PAIR_WARPS + warp;
   const int lane = threadIdx.x & 31;
   if (DEPTH == 2) {
     // the unit's entries were read during the unit before
@@ -1212,9 +1220,9 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, co
   // persistent grid: enough warps for the units, `pair_blocks_per_sm`
   // blocks of 8 warps per SM (4 fit at 64 registers; fewer leave room for
   // the PME kernels that run beside it on another stream)
-  int64_t want = (c.units_cap + 7) / 8;
+  int64_t want = (c.units_cap + NB_PAIR_WARPS - 1) / NB_PAIR_WARPS;
   int sms = c.pair_sms > 0 ? std::min(c.pair_sms, g_sm_count) : g_sm_count;
-  int grid = (int)std::min<int64_t>(want, (int64_t)sms * std::max(1, c.pair_blocks_per_sm));
+  int grid = (int)std::min<int64_t>(want, (int64_t)sms * std::max(1, c.pair_blocks_per_sm) * (8 / NB_PAIR_WARPS));
   if (grid < 1) grid = 1;
   // the inner list of the dual list once it has been pruned, else the outer
   bool inner = c.inner_reach > 0.0 && c.inner_valid;
@@ -1223,7 +1231,8 @@ void nb_pairs_run(NbCtx &c, const double box[3], bool energy, cudaStream_t s, co
   const int2 *lslab = inner ? c.slab_in : c.slab;
   const int32_t *lcounts = inner ? c.counts_in : c.counts;
 #define NB_LAUNCH3(E, F, S, M, D)                                                                          \
-  nb_launch_chained(nb_pairs<E, F, S, M, false, D>, dim3(grid), dim3(256), 0, s, P, (const float4 *)nullptr,  \
+  nb_launch_chained(nb_pairs<E, F, S, M, false, D>, dim3(grid), dim3(NB_PAIR_WARPS * 32), 0, s, P,             \
+                    (const float4 *)nullptr,                                                                 \
                     lsizes, lunits, lslab, lcounts, c.xq, c.xq_lo, c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed,  \
                     c.unit_partials, c.status, halt, skip)
 #define NB_LAUNCH2(E, F, S, M)                     \
@@ -1430,10 +1439,11 @@ void nb_batch_pairs_run(mdrtNbBatch &b, bool energy, cudaStream_t s) {
   ensure_sm_count();
   double unit_box[3] = {1.0, 1.0, 1.0};  // the cells come from group_L
   PairParams P = pair_params(c, unit_box);
-  int64_t want = (c.units_cap + 7) / 8;
-  int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)g_sm_count * std::max(1, c.pair_blocks_per_sm)));
+  int64_t want = (c.units_cap + NB_PAIR_WARPS - 1) / NB_PAIR_WARPS;
+  int grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>(want, (int64_t)g_sm_count * std::max(1, c.pair_blocks_per_sm) * (8 / NB_PAIR_WARPS)));
 #define NB_BATCH_LAUNCH(E, M, D)                                                                               \
-  nb_pairs<E, false, 0, M, true, D><<<grid, 256, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq,  \
+  nb_pairs<E, false, 0, M, true, D><<<grid, NB_PAIR_WARPS * 32, 0, s>>>(P, b.group_L, c.sizes, c.units, c.slab, c.counts, c.xq,  \
                                                             nullptr, c.typ_p, c.lj, c.ljf, c.acc, c.acc_fixed,     \
                                                             c.unit_partials, c.status, nullptr, nullptr)
   if (energy) {
