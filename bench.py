@@ -623,8 +623,9 @@ def main():
         torch.cuda.synchronize(dev)
 
     # warm-up: the first runs of a new context capture its step graph and may
-    # grow its lists once ahead of need
-    for _ in range(5):
+    # grow its lists once ahead of need (a growth captures the graph again,
+    # a few hundred ms once; 10 runs of 1,000 steps let the lists settle)
+    for _ in range(max(10, args.warmup)):
         e2e_step()
     e_steps = max(3, args.steps)
     step_sec = []

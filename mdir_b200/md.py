@@ -96,9 +96,10 @@ class Integrator:
         reaches first (the launch shapes as set), then the span of the pair
         grid (SMs; the others are left to the PME kernels beside it), its
         blocks per SM and its staging depth at the reaches kept, then the
-        three leading pairs of reaches again at that shape in runs twice as
-        long and more of them (the leaders differ by about the noise of the
-        short runs, and the best reaches depend on the shape), then the
+        three leading pairs of reaches at each of the two leading shapes
+        again, in runs twice as long and more of them (the leaders differ by
+        about the noise of the short runs, and the best reaches depend on
+        the shape), then the
         pruning inside the pair kernel (MDIR D284) or in a launch of its
         own.  Each choice is timed as `reps` runs of `steps` steps after a
         build and half as many untimed steps; the fastest is kept and built
@@ -155,9 +156,15 @@ class Integrator:
         for _, R_, Rin_ in first:
             if (R_, Rin_) not in leaders:
                 leaders.append((R_, Rin_))
-        final = [(trial(R_, Rin_, sms, blocks, depth, steps=2 * steps, reps=reps + 2), R_, Rin_)
-                 for R_, Rin_ in leaders[:3]]
-        us, R, Rin = min(final)
+        # the two leading shapes at the reaches kept, each with the three
+        # leading reaches, in the longer runs
+        shapes = []
+        for t_ in sorted(t_ for t_ in trials if t_[1] == R and t_[2] == Rin):
+            if t_[3:] not in shapes:
+                shapes.append(t_[3:])
+        final = [(trial(R_, Rin_, sh[0], sh[1], sh[2], steps=2 * steps, reps=reps + 2), R_, Rin_) + sh
+                 for sh in shapes[:2] for R_, Rin_ in leaders[:3]]
+        us, R, Rin, sms, blocks, depth = min(final)
         t.set_tuning(staging_depth=depth)
         # the pruning in the pair kernel (MDIR D284) or in a launch of its
         # own, at the shape kept
